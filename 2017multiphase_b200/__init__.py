@@ -1,0 +1,411 @@
+"""B200 multiphase FLIP step — Python host mirror of the reference's `cspray`.
+
+The simulation runs in ``libmp.so`` (hand-written sm_100a CUDA behind the C ABI
+declared in ``include/mp.h``). This module binds that ABI with ctypes and mirrors
+the reference's stage methods (Multiphase/Multiphase/spray.h:21-337) under
+their reference names, so a caller of ``cspray`` finds the same operations:
+
+    sim = Sim.from_config(1)            # scene set-up (cspray::initparam + init)
+    sim.bubblesim()                     # one time step (spray.cpp:979-1233)
+    sim.hashAndSortParticles()          # or one stage at a time
+    p = sim.get_field("press")
+
+There is no CPU fallback: if the library or a GPU is missing, construction
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import warnings
+from typing import Dict, Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmp.so")
+INCLUDE_H = os.path.join(os.path.dirname(_HERE), "include", "mp.h")
+
+# status codes (mp.h)
+MP_OK, MP_ERR_CUDA, MP_ERR_CAPACITY, MP_ERR_NOCONVERGE, MP_ERR_TIMEOUT, MP_ERR_ARG, MP_ERR_STATE = range(7)
+_ERR_NAMES = {1: "MP_ERR_CUDA", 2: "MP_ERR_CAPACITY", 3: "MP_ERR_NOCONVERGE", 4: "MP_ERR_TIMEOUT",
+              5: "MP_ERR_ARG", 6: "MP_ERR_STATE"}
+
+# particle and cell types (utility.h:13-19)
+TYPEFLUID, TYPEAIR, TYPEBOUNDARY, TYPEVACUUM, TYPEAIRSOLO, TYPESOLID = range(6)
+MC_SOLID, MC_FLUID, MC_GAS = 0, 1, 2
+PREC_MIXED, PREC_FP64 = 0, 1
+TOL_REF_ABS, TOL_REL = 0, 1
+KT_CG_STENCIL, KT_CG_UPDATE, KT_P2G, KT_G2P, KT_SORT, KT_LEVELSET, KT_MC_DENS = range(7)
+
+# field ids in the order of enum mp_field (mp.h)
+FIELDS = [
+    "press", "div", "lsfluid", "lsair", "lsmerge", "phifluid", "phiair", "phisolid",
+    "phigrax", "phigray", "phigraz", "phigrax_air", "phigray_air", "phigraz_air",
+    "surftension", "tp", "tp_save", "tp_old", "fixedheat", "mark",
+    "waterux", "wateruy", "wateruz", "waterux_old", "wateruy_old", "wateruz_old",
+    "airux", "airuy", "airuz", "airux_old", "airuy_old", "airuz_old",
+    "solidux", "soliduy", "soliduz", "cellstart", "cellend",
+    "pos", "vel", "flag", "mass", "temp", "lheat", "solubility", "gascontain",
+]
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+_DTYPE = {"mark": np.int8, "flag": np.int8, "cellstart": np.uint32, "cellend": np.uint32}
+
+
+class MPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class MPState(C.Structure):
+    _fields_ = [("frame", C.c_int32), ("par_num_now", C.c_int32), ("n_real_solpoint", C.c_int32),
+                ("last_cg_iters", C.c_int32), ("last_cg_residual", C.c_double),
+                ("last_heat_cg_iters", C.c_int32), ("last_heat_cg_residual", C.c_double),
+                ("mc_verts", C.c_int32 * 3), ("mc_indices", C.c_int32 * 3), ("mc_active_voxels", C.c_int32 * 3),
+                ("reserved", C.c_int32 * 6)]
+
+
+_lib = None
+_Params = None
+
+
+def load_library() -> C.CDLL:
+    """Loads libmp.so; raises if it has not been built."""
+    global _lib, _Params
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() (make -C csrc)")
+    lib = C.CDLL(LIB_PATH)
+    lib.mp_params_describe.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.mp_params_size.restype = C.c_int
+    fields = []
+    i = 0
+    while True:
+        name = C.c_char_p(); off = C.c_int(); kind = C.c_int()
+        if lib.mp_params_describe(i, C.byref(name), C.byref(off), C.byref(kind)) != 0:
+            break
+        fields.append((name.value.decode(), off.value, kind.value))
+        i += 1
+    # rebuild the struct from the library's own table (offsets checked below)
+    members = []
+    for nm, off, kind in fields:
+        members.append((nm, C.c_float if kind == 1 else C.c_int32))
+    size = lib.mp_params_size()
+    pad = (size - (fields[-1][1] + 4)) // 4
+    members.append(("reserved", C.c_int32 * pad))
+
+    class Params(C.Structure):
+        _fields_ = members
+
+    for nm, off, _ in fields:
+        if getattr(Params, nm).offset != off:
+            raise ImportError(f"mp_params layout mismatch at {nm}")
+    if C.sizeof(Params) != size:
+        raise ImportError("mp_params size mismatch")
+    _Params = Params
+    vp = C.c_void_p
+    P = C.POINTER(Params)
+    sig = {
+        "mp_params_default": ([P, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "mp_params_derive": ([P], C.c_int),
+        "mp_create": ([P, C.POINTER(vp)], C.c_int),
+        "mp_destroy": ([vp], C.c_int),
+        "mp_set_params": ([vp, P], C.c_int),
+        "mp_get_params": ([vp, P], C.c_int),
+        "mp_get_state": ([vp, C.POINTER(MPState)], C.c_int),
+        "mp_set_state": ([vp, C.POINTER(MPState)], C.c_int),
+        "mp_last_error": ([vp, C.c_char_p, C.c_size_t], C.c_int),
+        "mp_set_stream": ([vp, vp], C.c_int),
+        "mp_get_stream": ([vp, C.POINTER(vp)], C.c_int),
+        "mp_synchronize": ([vp], C.c_int),
+        "mp_upload_particles": ([vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "mp_download_particles": ([vp, C.POINTER(C.c_int), vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "mp_field_info": ([vp, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)], C.c_int),
+        "mp_get_field": ([vp, C.c_int, vp, C.c_size_t], C.c_int),
+        "mp_set_field": ([vp, C.c_int, vp, C.c_size_t], C.c_int),
+        "mp_set_tables": ([vp, vp, C.c_int, vp, C.c_int], C.c_int),
+        "mp_mc_tables": ([vp, vp, vp], C.c_int),
+        "mp_init_particle_heat": ([vp], C.c_int),
+        "mp_levelset": ([vp, C.c_float], C.c_int),
+        "mp_sweep_phi": ([vp, C.c_int], C.c_int),
+        "mp_sweep_u": ([vp, C.c_int], C.c_int),
+        "mp_set_boundary_u": ([vp, C.c_int], C.c_int),
+        "mp_project": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
+        "mp_mc": ([vp, C.c_int], C.c_int),
+        "mp_mc_download": ([vp, C.c_int, vp, vp, vp, C.c_int, C.c_int], C.c_int),
+        "mp_mc_download_field": ([vp, vp, vp], C.c_int),
+        "mp_kernel_timing": ([vp, C.c_int, C.c_int], C.c_int),
+        "mp_kernel_timing_read": ([vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)], C.c_int),
+        "mp_kernel_timing_reset": ([vp], C.c_int),
+        "mp_launch_count": ([vp], C.c_int64),
+        "mp_scene_params": ([C.c_int, C.c_int, P], C.c_int),
+        "mp_scene_particles": ([P, C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_int), vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "mp_scene_tables": ([P, C.c_int, C.c_uint64, vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
+        "mp_scene_fixed_heat": ([P, C.c_int, vp], C.c_int),
+    }
+    for nm, (args, res) in sig.items():
+        f = getattr(lib, nm)
+        f.argtypes = args
+        f.restype = res
+    for nm in ["mp_hash_sort", "mp_external_force", "mp_sweep_ls_mark", "mp_mark_solo_air", "mp_surface_tension",
+               "mp_markgrid_bubble", "mp_p2g", "mp_drag", "mp_g2p", "mp_solid_motion", "mp_solo_air_update",
+               "mp_collide_advect", "mp_correct_pos", "mp_correct_pos_bubble", "mp_heat", "mp_gen_gas", "mp_delete",
+               "mp_melt", "mp_freeze", "mp_mc_presort", "mp_step"]:
+        f = getattr(lib, nm)
+        f.argtypes = [vp]
+        f.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def Params():
+    """The ctypes mirror of mp_params, built from the library's field table."""
+    load_library()
+    return _Params()
+
+
+def params_to_dict(p) -> Dict[str, float]:
+    return {nm: getattr(p, nm) for nm, _ in p._fields_ if nm != "reserved"}
+
+
+def scene_params(config: int, n: int = 0):
+    """Parameters of benchmark configuration 1..5 (mp_scene_params)."""
+    lib = load_library()
+    p = Params()
+    _check(lib.mp_scene_params(config, n, C.byref(p)), None)
+    return p
+
+
+def default_params(nx: int, ny: int, nz: int, par_num_max: int):
+    lib = load_library()
+    p = Params()
+    _check(lib.mp_params_default(C.byref(p), nx, ny, nz, par_num_max), None)
+    return p
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc: int, ctx, allow_noconverge=False) -> int:
+    if rc == MP_OK:
+        return rc
+    if rc == MP_ERR_NOCONVERGE and allow_noconverge:
+        warnings.warn("CG stopped at its iteration limit", RuntimeWarning)
+        return rc
+    buf = C.create_string_buffer(512)
+    load_library().mp_last_error(ctx, buf, 512)
+    raise MPError(rc, buf.value.decode(errors="replace"))
+
+
+def scene_particles(p, config: int, seed: int) -> Dict[str, np.ndarray]:
+    """Initial particles of a configuration (mp_scene_particles), as numpy arrays."""
+    lib = load_library()
+    n = C.c_int()
+    _check(lib.mp_scene_particles(C.byref(p), config, seed, 0, C.byref(n), None, None, None, None, None, None, None,
+                                  None), None)
+    cnt = n.value
+    out = {"pos": np.zeros((cnt, 3), np.float32), "vel": np.zeros((cnt, 3), np.float32),
+           "flag": np.zeros(cnt, np.int8), "mass": np.zeros(cnt, np.float32), "temp": np.zeros(cnt, np.float32),
+           "lheat": np.zeros(cnt, np.float32), "solubility": np.zeros(cnt, np.float32),
+           "gascontain": np.zeros(cnt, np.float32)}
+    _check(lib.mp_scene_particles(C.byref(p), config, seed, cnt, C.byref(n), *[_ptr(out[k]) for k in
+                                  ["pos", "vel", "flag", "mass", "temp", "lheat", "solubility", "gascontain"]]), None)
+    return out
+
+
+def scene_tables(p, config: int, seed: int, nrand: int = 10000):
+    lib = load_library()
+    rf = np.zeros(nrand, np.float32)
+    seeds = np.zeros(64, np.int32)
+    ns = C.c_int()
+    _check(lib.mp_scene_tables(C.byref(p), config, seed, _ptr(rf), nrand, _ptr(seeds), 64, C.byref(ns)), None)
+    return rf, seeds[:ns.value].copy()
+
+
+def scene_fixed_heat(p, config: int) -> np.ndarray:
+    lib = load_library()
+    fh = np.zeros(p.nx * p.ny * p.nz, np.float32)
+    _check(lib.mp_scene_fixed_heat(C.byref(p), config, _ptr(fh)), None)
+    return fh
+
+
+def mc_tables():
+    lib = load_library()
+    nv = np.zeros(256, np.int32); tri = np.zeros(256 * 16, np.int32); edge = np.zeros(256, np.int32)
+    lib.mp_mc_tables(_ptr(nv), _ptr(tri), _ptr(edge))
+    return nv, tri, edge
+
+
+class Sim:
+    """One simulation context on the current CUDA device (the reference's cspray)."""
+
+    def __init__(self, params):
+        self.lib = load_library()
+        self.params = params
+        self.ctx = C.c_void_p()
+        _check(self.lib.mp_create(C.byref(params), C.byref(self.ctx)), None)
+
+    @classmethod
+    def from_config(cls, config: int, n: int = 0, seed: int = 2017000, params=None, **overrides):
+        """cspray::initparam + init for benchmark configuration `config`."""
+        p = params if params is not None else scene_params(config, n)
+        for k, v in overrides.items():
+            setattr(p, k, v)
+        parts = scene_particles(p, config, seed)
+        sim = cls(p)
+        sim.upload_particles(**parts)
+        rf, seeds = scene_tables(p, config, seed)
+        sim.set_tables(rf, seeds)
+        sim.set_field("fixedheat", scene_fixed_heat(p, config))
+        st = sim.state()
+        st.n_real_solpoint = int((parts["flag"] == TYPESOLID).sum())
+        sim.set_state(st)
+        sim.config, sim.seed = config, seed
+        return sim
+
+    def close(self):
+        if self.ctx:
+            self.lib.mp_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- data -------------------------------------------------------------
+    def upload_particles(self, pos, flag, mass, vel=None, temp=None, lheat=None, solubility=None, gascontain=None):
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        n = pos.shape[0]
+        arrs = [pos, None if vel is None else np.ascontiguousarray(vel, np.float32).reshape(-1, 3),
+                np.ascontiguousarray(flag, np.int8), np.ascontiguousarray(mass, np.float32)]
+        arrs += [None if a is None else np.ascontiguousarray(a, np.float32) for a in (temp, lheat, solubility, gascontain)]
+        _check(self.lib.mp_upload_particles(self.ctx, n, *[_ptr(a) for a in arrs]), self.ctx)
+
+    def download_particles(self) -> Dict[str, np.ndarray]:
+        n = self.state().par_num_now
+        out = {"pos": np.zeros((n, 3), np.float32), "vel": np.zeros((n, 3), np.float32), "flag": np.zeros(n, np.int8),
+               "mass": np.zeros(n, np.float32), "temp": np.zeros(n, np.float32), "lheat": np.zeros(n, np.float32),
+               "solubility": np.zeros(n, np.float32), "gascontain": np.zeros(n, np.float32)}
+        cnt = C.c_int()
+        _check(self.lib.mp_download_particles(self.ctx, C.byref(cnt), *[_ptr(out[k]) for k in
+               ["pos", "vel", "flag", "mass", "temp", "lheat", "solubility", "gascontain"]]), self.ctx)
+        return out
+
+    def field_info(self, name: str):
+        cnt = C.c_size_t(); eb = C.c_size_t()
+        _check(self.lib.mp_field_info(self.ctx, FIELD_ID[name], C.byref(cnt), C.byref(eb)), self.ctx)
+        return cnt.value, eb.value
+
+    def get_field(self, name: str) -> np.ndarray:
+        cnt, eb = self.field_info(name)
+        a = np.zeros(cnt, _DTYPE.get(name, np.float32))
+        _check(self.lib.mp_get_field(self.ctx, FIELD_ID[name], _ptr(a), a.nbytes), self.ctx)
+        return a
+
+    def set_field(self, name: str, a: np.ndarray):
+        a = np.ascontiguousarray(a, _DTYPE.get(name, np.float32)).ravel()
+        _check(self.lib.mp_set_field(self.ctx, FIELD_ID[name], _ptr(a), a.nbytes), self.ctx)
+
+    def set_tables(self, randfloat: np.ndarray, seeds: np.ndarray):
+        rf = np.ascontiguousarray(randfloat, np.float32)
+        sd = np.ascontiguousarray(seeds, np.int32)
+        _check(self.lib.mp_set_tables(self.ctx, _ptr(rf), rf.size, _ptr(sd), sd.size), self.ctx)
+
+    def state(self) -> MPState:
+        s = MPState()
+        _check(self.lib.mp_get_state(self.ctx, C.byref(s)), self.ctx)
+        return s
+
+    def set_state(self, s: MPState):
+        _check(self.lib.mp_set_state(self.ctx, C.byref(s)), self.ctx)
+
+    def set_params(self, p):
+        _check(self.lib.mp_set_params(self.ctx, C.byref(p)), self.ctx)
+        self.params = p
+
+    def synchronize(self):
+        _check(self.lib.mp_synchronize(self.ctx), self.ctx)
+
+    # ---- stages, under the reference's method names (spray.h) ------------
+    def _stage(self, name, *args, allow_noconverge=False):
+        return _check(getattr(self.lib, name)(self.ctx, *args), self.ctx, allow_noconverge)
+
+    def initHeatAndSolubility(self): return self._stage("mp_init_particle_heat")
+    def hashAndSortParticles(self): return self._stage("mp_hash_sort")
+    def addexternalforce(self): return self._stage("mp_external_force")
+    def computeLevelset(self, offset=0.0): return self._stage("mp_levelset", C.c_float(offset))
+    def sweepLSAndMardGrid(self): return self._stage("mp_sweep_ls_mark")
+    def markSoloAirParticle(self): return self._stage("mp_mark_solo_air")
+    def computesurfacetension(self): return self._stage("mp_surface_tension")
+    def markgrid_bubble(self): return self._stage("mp_markgrid_bubble")
+    def mapvelp2g_bubble(self): return self._stage("mp_p2g")
+    def enforceDragForce(self): return self._stage("mp_drag")
+    def sweepPhi(self, phase): return self._stage("mp_sweep_phi", phase)
+    def sweepU(self, phase): return self._stage("mp_sweep_u", phase)
+    def setWaterBoundaryU(self, phase): return self._stage("mp_set_boundary_u", phase)
+
+    def project_CG_bubble(self):
+        it = C.c_int(); res = C.c_double()
+        rc = _check(self.lib.mp_project(self.ctx, C.byref(it), C.byref(res)), self.ctx, allow_noconverge=True)
+        return it.value, res.value, rc
+
+    def mapvelg2p_bubble(self): return self._stage("mp_g2p")
+    def solidmotion(self): return self._stage("mp_solid_motion")
+    def updateSoloAirParticle(self): return self._stage("mp_solo_air_update")
+    def CollisionSolid(self): return self._stage("mp_collide_advect")
+    def correctpos(self): return self._stage("mp_correct_pos")
+    def correctpos_bubble(self): return self._stage("mp_correct_pos_bubble")
+    def updateTemperature(self): return self._stage("mp_heat", allow_noconverge=True)
+    def GenerateGasParticle(self): return self._stage("mp_gen_gas")
+    def deleteAirFluidParticle(self): return self._stage("mp_delete")
+    def MeltSolid(self): return self._stage("mp_melt")
+    def Freezing(self): return self._stage("mp_freeze")
+    def preMC(self): return self._stage("mp_mc_presort")
+    def runMC(self, surface): return self._stage("mp_mc", surface)
+    def bubblesim(self): return self._stage("mp_step", allow_noconverge=True)
+    simstep = bubblesim
+
+    def mc_mesh(self, surface: int):
+        s = self.state()
+        nv, ni = s.mc_verts[surface], s.mc_indices[surface]
+        v = np.zeros((nv, 3), np.float32); nr = np.zeros((nv, 3), np.float32); ix = np.zeros(ni, np.uint32)
+        _check(self.lib.mp_mc_download(self.ctx, surface, _ptr(v), _ptr(nr), _ptr(ix), nv, ni), self.ctx)
+        return v, nr, ix
+
+    def mc_field(self):
+        p = self.params
+        dens = np.zeros((2 * p.nx + 1) * (2 * p.ny + 1) * (2 * p.nz + 1), np.float32)
+        cube = np.zeros(8 * p.nx * p.ny * p.nz, np.uint8)
+        _check(self.lib.mp_mc_download_field(self.ctx, _ptr(dens), _ptr(cube)), self.ctx)
+        return dens, cube
+
+    # ---- measurement ------------------------------------------------------
+    def kernel_timing(self, cls: int, enable: bool = True):
+        _check(self.lib.mp_kernel_timing(self.ctx, cls, int(enable)), self.ctx)
+
+    def kernel_timing_read(self, cls: int):
+        ms = C.c_double(); n = C.c_int64()
+        _check(self.lib.mp_kernel_timing_read(self.ctx, cls, C.byref(ms), C.byref(n)), self.ctx)
+        return ms.value, n.value
+
+    def kernel_timing_reset(self):
+        _check(self.lib.mp_kernel_timing_reset(self.ctx), self.ctx)
+
+    def launch_count(self) -> int:
+        return int(self.lib.mp_launch_count(self.ctx))
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        _check(self.lib.mp_get_stream(self.ctx, C.byref(s)), self.ctx)
+        return s.value or 0

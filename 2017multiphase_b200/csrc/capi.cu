@@ -1,0 +1,727 @@
+// capi.cu — the C ABI (include/mp.h): context life cycle, data movement,
+// stage entry points and the full bubblesim step.
+//
+// The context replaces the state of the reference's cspray class
+// (Multiphase/Multiphase/spray.h:153-389); mp_create is its initmem_bubble
+// (spray.cu:25-218) plus initMC (spray.cu:709-757); mp_step is bubblesim
+// (spray.cpp:979-1233).
+#include "ctx.cuh"
+#include <cmath>
+#include <cstring>
+#include <cstddef>
+#include <algorithm>
+#include <new>
+
+extern "C" void mp_internal_mc_tables(int32_t* nv, int32_t* tri, int32_t* edge);
+
+// ---------------------------------------------------------------------------
+// parameters
+// ---------------------------------------------------------------------------
+struct ParamField { const char* name; int offset; int kind; };
+#define PF_I(f) {#f, (int)offsetof(mp_params, f), 0}
+#define PF_F(f) {#f, (int)offsetof(mp_params, f), 1}
+static const ParamField kParamFields[] = {
+    PF_I(version), PF_I(nx), PF_I(ny), PF_I(nz), PF_I(par_num_max), PF_I(scene),
+    PF_F(cellsize), PF_F(dt), PF_F(gravity_x), PF_F(gravity_y), PF_F(gravity_z),
+    PF_F(gmin_x), PF_F(gmin_y), PF_F(gmin_z), PF_F(samplespace),
+    PF_F(m0), PF_F(airm0), PF_F(waterrho), PF_F(solidrho), PF_F(pradius),
+    PF_F(poly6kern), PF_F(spikykern), PF_F(lapkern),
+    PF_I(b_solid), PF_I(b_melt), PF_I(b_freeze), PF_I(b_fix_solid), PF_I(b_gen_gas), PF_I(b_heat_trans),
+    PF_I(b_add_heat_bottom), PF_I(b_extend_heat_to_boundary), PF_I(b_correct_position),
+    PF_I(b_smooth_mc), PF_I(b_run_mc), PF_I(mc_every), PF_I(smooth_iters),
+    PF_F(surfacetension_sigma), PF_F(heatalpha_fluid), PF_F(heatalpha_air), PF_F(heatalpha_solid),
+    PF_F(heatalpha_vacuum), PF_F(default_temperature), PF_F(temperature0), PF_F(melting_point),
+    PF_F(boiling_point), PF_F(drag_param_solo), PF_F(drag_param_grid), PF_F(viscosity_sph),
+    PF_F(default_solid_T), PF_F(default_liquid_T), PF_F(liquid_heat_th), PF_F(alpha_temp_trans),
+    PF_F(bounce_vel_param), PF_F(bounce_pos_param), PF_F(heat_increase_bottom),
+    PF_F(bubble_max_vel), PF_F(max_vel_for_bubble), PF_F(buoyance_rate_air), PF_F(buoyance_rate_solo),
+    PF_F(vapor_gen_rate), PF_F(init_dissolve_gas_rate), PF_F(init_gas_rate),
+    PF_F(correction_spring), PF_F(correction_radius), PF_F(mc_density), PF_F(heat_clamp),
+    PF_F(solubility_coef), PF_F(solid_bounce_param), PF_F(flip_alpha), PF_I(cg_tol_mode), PF_F(cg_tol),
+    PF_I(cg_max_iter), PF_I(heat_cg_max_iter), PF_I(cg_true_residual_every), PF_I(precision),
+    PF_I(coef_mode), PF_F(density_ratio), PF_I(mc_max_verts), PF_I(mc_max_tris), PF_I(seed_redraw),
+    PF_I(update_seed_frame_delta), PF_I(b_fixed_heat),
+};
+
+extern "C" int mp_params_size(void) { return (int)sizeof(mp_params); }
+
+extern "C" int mp_params_describe(int index, const char** name, int* offset, int* kind) {
+    int cnt = (int)(sizeof(kParamFields) / sizeof(kParamFields[0]));
+    if (index < 0 || index >= cnt) return MP_ERR_ARG;
+    if (name) *name = kParamFields[index].name;
+    if (offset) *offset = kParamFields[index].offset;
+    if (kind) *kind = kParamFields[index].kind;
+    return MP_OK;
+}
+
+// spray.cpp:573-588: m0 from the sample spacing, SPH kernel constants from the cell size
+extern "C" int mp_params_derive(mp_params* p) {
+    if (!p) return MP_ERR_ARG;
+    p->m0 = (1.0f * p->waterrho) / powf(1.0f / p->samplespace, 3.0f);
+    p->airm0 = p->m0;
+    p->pradius = (float)pow((double)(p->m0 / p->waterrho * 3.0f / 4.0f) / M_PI, 1.0 / 3.0f);
+    p->poly6kern = 315.0f / (64.0f * 3.141592f * powf(p->cellsize, 9.0f));
+    p->spikykern = -45.0f / (3.141592f * powf(p->cellsize, 6.0f));
+    p->lapkern = 45.0f / (3.141592f * powf(p->cellsize, 6.0f));
+    p->max_vel_for_bubble = p->cellsize / p->dt;
+    return MP_OK;
+}
+
+// cspray::initparam defaults (spray.cpp:29-78, 573-626) with the MULTIBUBBLE
+// scene switches (spray.cpp:191-214)
+extern "C" int mp_params_default(mp_params* p, int nx, int ny, int nz, int par_num_max) {
+    if (!p || nx < 4 || ny < 4 || nz < 4 || par_num_max < 0) return MP_ERR_ARG;
+    memset(p, 0, sizeof(*p));
+    p->version = MP_PARAMS_VERSION;
+    p->nx = nx; p->ny = ny; p->nz = nz; p->par_num_max = par_num_max;
+    p->scene = MP_SCENE_MULTIBUBBLE;
+    p->cellsize = 1.0f / 64;
+    p->dt = 0.003f;
+    p->gravity_x = 0; p->gravity_y = 0; p->gravity_z = -9.8f;
+    p->samplespace = 0.5f * p->cellsize;
+    p->waterrho = 1000.0f; p->solidrho = 800.0f;
+    p->b_solid = 0; p->b_melt = 0; p->b_freeze = 0; p->b_fix_solid = 0; p->b_gen_gas = 0; p->b_heat_trans = 0;
+    p->b_add_heat_bottom = 0; p->b_extend_heat_to_boundary = 0; p->b_correct_position = 1;
+    p->b_smooth_mc = 1; p->b_run_mc = 1; p->mc_every = 2; p->smooth_iters = 5;
+    p->surfacetension_sigma = 0.0f;
+    p->heatalpha_fluid = 0.02f; p->heatalpha_air = 0.008f; p->heatalpha_solid = 0.2f; p->heatalpha_vacuum = 0.0001f;
+    p->default_temperature = 293.15f; p->temperature0 = 273.15f;
+    p->melting_point = 273.15f; p->boiling_point = 373.15f;
+    p->drag_param_solo = 10; p->drag_param_grid = 0.05f; p->viscosity_sph = 1.8f;
+    p->default_solid_T = 263.15f; p->default_liquid_T = 293.15f; p->liquid_heat_th = 10; p->alpha_temp_trans = 0.0f;
+    p->bounce_vel_param = 1.0f; p->bounce_pos_param = 0;
+    p->heat_increase_bottom = 0.0f;
+    p->bubble_max_vel = 6.5f;
+    p->buoyance_rate_air = 1.25f; p->buoyance_rate_solo = 1.05f;
+    p->vapor_gen_rate = 0.01f; p->init_dissolve_gas_rate = 1.0f; p->init_gas_rate = 0.7f;
+    p->correction_spring = 500000.0f; p->correction_radius = 0.5f;
+    p->mc_density = 0.5f;
+    p->heat_clamp = 378.0f;
+    p->solubility_coef = 1018.9f;
+    p->solid_bounce_param = 0.5f;
+    p->flip_alpha = 1.0f;
+    p->cg_tol_mode = MP_TOL_REF_ABS; p->cg_tol = 0.01f;
+    p->cg_max_iter = 800; p->heat_cg_max_iter = 3800; p->cg_true_residual_every = 0;
+    p->precision = MP_PREC_MIXED; p->coef_mode = MP_COEF_REF; p->density_ratio = 1000.0f;
+    // the reference fixes 6e6 vertices / 12e6 triangles (spray.cu:721-722); here the
+    // caps scale with the 2x grid's cross-section (a few surface layers)
+    long long mv = std::max(100000LL, 24LL * (2 * nx) * (2 * ny));
+    mv = std::min(mv, 64000000LL);
+    p->mc_max_verts = (int)mv; p->mc_max_tris = (int)std::min(2 * mv, 128000000LL);
+    p->seed_redraw = 0; p->update_seed_frame_delta = 15;
+    p->b_fixed_heat = 0;
+    return mp_params_derive(p);
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+static int dalloc(MpCtx* c, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        c->err = std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
+        return MP_ERR_CUDA;
+    }
+    return MP_OK;
+}
+template <class T>
+static int dalloc_t(MpCtx* c, T** p, size_t count) { return dalloc(c, (void**)p, sizeof(T) * count); }
+
+static void free_all(MpCtx* c) {
+    void* ptrs[] = {c->press, c->divg, c->lsfluid, c->lsair, c->lsmerge, c->phifluid, c->phiair, c->phisolid,
+                    c->gx, c->gy, c->gz, c->gxa, c->gya, c->gza, c->sf, c->Tp, c->Tp_save, c->Tp_old, c->fixedheat,
+                    c->cell_tmp, c->mark, c->mark_tmp, c->cg_r, c->cg_p, c->cg_z, c->cg64, c->red, c->scal, c->red_count,
+                    c->pos, c->vel, c->heat, c->pos2, c->vel2, c->heat2, c->pdens, c->pprs, c->pscr, c->pscr2,
+                    c->flag_snap, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->scan_tmp, c->u32_scratch,
+                    c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_cube, c->mc_vflag, c->mc_vscan,
+                    c->mc_compact, c->mc_vverts, c->mc_vvscan, c->mc_emark, c->mc_escan, c->mc_vstart, c->mc_inc,
+                    c->mc_fill, c->mc_tmpv};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    for (int a = 0; a < 3; a++) {
+        for (float* p : {c->wu[a], c->wuo[a], c->au[a], c->auo[a], c->su[a], c->tmpu[a]}) if (p) cudaFree(p);
+        if (c->mc[a].verts) cudaFree(c->mc[a].verts);
+        if (c->mc[a].normals) cudaFree(c->mc[a].normals);
+        if (c->mc[a].indices) cudaFree(c->mc[a].indices);
+    }
+    for (auto& e : c->kt_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    for (int k = 0; k < MP_KT_COUNT; k++)
+        for (auto& e : c->kt_pending[k]) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+static size_t scan_scratch(size_t n) {
+    size_t tot = 64;
+    while (n > 4096) { size_t nb = (n + 4095) / 4096; tot += 2 * nb + 2; n = nb; }
+    return tot;
+}
+
+static int create_impl(MpCtx* c, const mp_params* p) {
+    c->P = *p;
+    memset(&c->S, 0, sizeof(c->S));
+    MP_CUDA(c, cudaGetDevice(&c->device));
+    MP_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+    mpk::Grid& g = c->G;
+    g.NX = p->nx; g.NY = p->ny; g.NZ = p->nz;
+    g.n = g.NX * g.NY * g.NZ;
+    g.nfx = (g.NX + 1) * g.NY * g.NZ; g.nfy = g.NX * (g.NY + 1) * g.NZ; g.nfz = g.NX * g.NY * (g.NZ + 1);
+    g.h = p->cellsize; g.gx0 = p->gmin_x; g.gy0 = p->gmin_y; g.gz0 = p->gmin_z;
+    size_t n = g.n;
+    float** cellf[] = {&c->press, &c->divg, &c->lsfluid, &c->lsair, &c->lsmerge, &c->phifluid, &c->phiair, &c->phisolid,
+                       &c->gx, &c->gy, &c->gz, &c->gxa, &c->gya, &c->gza, &c->sf, &c->Tp, &c->Tp_save, &c->Tp_old,
+                       &c->fixedheat, &c->cell_tmp, &c->cg_r, &c->cg_p, &c->cg_z};
+    for (float** f : cellf) { MP_TRY(dalloc_t(c, f, n)); MP_CUDA(c, cudaMemset(*f, 0, sizeof(float) * n)); }
+    MP_TRY(dalloc_t(c, &c->mark, n)); MP_TRY(dalloc_t(c, &c->mark_tmp, n));
+    MP_CUDA(c, cudaMemset(c->mark, 0, n));
+    {   // fixed heat defaults to "not fixed"
+        std::vector<float> u(n, MP_UNDEF_TEMPERATURE);
+        MP_CUDA(c, cudaMemcpy(c->fixedheat, u.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    }
+    size_t nf[3] = {(size_t)g.nfx, (size_t)g.nfy, (size_t)g.nfz};
+    for (int a = 0; a < 3; a++) {
+        for (float** f : {&c->wu[a], &c->wuo[a], &c->au[a], &c->auo[a], &c->su[a], &c->tmpu[a]}) {
+            MP_TRY(dalloc_t(c, f, nf[a]));
+            MP_CUDA(c, cudaMemset(*f, 0, sizeof(float) * nf[a]));
+        }
+    }
+    MP_TRY(dalloc_t(c, &c->cg64, 5 * n));
+    c->red_blocks = mp_blocks((long long)n, 256);
+    MP_TRY(dalloc_t(c, &c->red, (size_t)148 * 32 * 6));
+    MP_TRY(dalloc_t(c, &c->scal, 16));
+    MP_TRY(dalloc_t(c, &c->red_count, 16));
+    MP_CUDA(c, cudaMemset(c->red_count, 0, 16 * sizeof(unsigned int)));
+    MP_CUDA(c, cudaMemset(c->scal, 0, 16 * sizeof(double)));
+    size_t cap = (size_t)std::max(p->par_num_max, 1);
+    for (float4** f : {&c->pos, &c->vel, &c->heat, &c->pos2, &c->vel2, &c->heat2, &c->pscr, &c->pscr2})
+        MP_TRY(dalloc_t(c, f, cap));
+    MP_TRY(dalloc_t(c, &c->pdens, cap)); MP_TRY(dalloc_t(c, &c->pprs, cap));
+    size_t n8 = c->P.b_run_mc ? 8 * n : n;
+    size_t kcap = std::max(cap, n) + 1;
+    MP_TRY(dalloc_t(c, &c->keys, kcap)); MP_TRY(dalloc_t(c, &c->perm, kcap));
+    MP_TRY(dalloc_t(c, &c->cell_cnt, n8 + 1)); MP_TRY(dalloc_t(c, &c->cell_off, n8 + 1));
+    MP_CUDA(c, cudaMemset(c->cell_cnt, 0, sizeof(uint32_t) * (n8 + 1)));
+    MP_CUDA(c, cudaMemset(c->cell_off, 0, sizeof(uint32_t) * (n8 + 1)));
+    MP_TRY(dalloc_t(c, &c->tmask, n8));
+    MP_CUDA(c, cudaMemset(c->tmask, 0, n8));
+    MP_TRY(dalloc_t(c, &c->u32_scratch, 16));
+    // marching cubes tables and buffers
+    MP_TRY(dalloc_t(c, &c->mc_numverts, 256)); MP_TRY(dalloc_t(c, &c->mc_tri, 256 * 16));
+    {
+        int32_t nv[256], tri[256 * 16];
+        mp_internal_mc_tables(nv, tri, nullptr);
+        MP_CUDA(c, cudaMemcpy(c->mc_numverts, nv, sizeof(nv), cudaMemcpyHostToDevice));
+        MP_CUDA(c, cudaMemcpy(c->mc_tri, tri, sizeof(tri), cudaMemcpyHostToDevice));
+    }
+    size_t scan_max = std::max(kcap, n8 + 1);
+    if (c->P.b_run_mc) {
+        size_t nnode = (size_t)(2 * g.NX + 1) * (2 * g.NY + 1) * (2 * g.NZ + 1);
+        size_t nvox = 8 * n;
+        c->mc_edges = 3 * nnode;
+        MP_TRY(dalloc_t(c, &c->mc_dens, nnode));
+        MP_TRY(dalloc_t(c, &c->mc_cube, nvox));
+        MP_TRY(dalloc_t(c, &c->mc_vflag, nvox)); MP_TRY(dalloc_t(c, &c->mc_vscan, nvox + 1));
+        MP_TRY(dalloc_t(c, &c->mc_compact, nvox));
+        MP_TRY(dalloc_t(c, &c->mc_vverts, nvox)); MP_TRY(dalloc_t(c, &c->mc_vvscan, nvox + 1));
+        MP_TRY(dalloc_t(c, &c->mc_emark, c->mc_edges)); MP_TRY(dalloc_t(c, &c->mc_escan, c->mc_edges + 1));
+        size_t mv = (size_t)c->P.mc_max_verts, mi = 3 * (size_t)c->P.mc_max_tris;
+        MP_TRY(dalloc_t(c, &c->mc_vstart, mv + 1)); MP_TRY(dalloc_t(c, &c->mc_fill, mv + 1));
+        MP_TRY(dalloc_t(c, &c->mc_inc, mi)); MP_TRY(dalloc_t(c, &c->mc_tmpv, mv));
+        for (int a = 0; a < 3; a++) {
+            MP_TRY(dalloc_t(c, &c->mc[a].verts, mv)); MP_TRY(dalloc_t(c, &c->mc[a].normals, mv));
+            MP_TRY(dalloc_t(c, &c->mc[a].indices, mi));
+        }
+        scan_max = std::max(scan_max, std::max(c->mc_edges + 1, mv + 1));
+    }
+    c->scan_tmp_elems = scan_scratch(scan_max);
+    MP_TRY(dalloc_t(c, &c->scan_tmp, c->scan_tmp_elems));
+    MP_CUDA(c, cudaDeviceSynchronize());
+    return MP_OK;
+}
+
+static MpCtx* C(void* ctx) { return reinterpret_cast<MpCtx*>(ctx); }
+#define CTX_OR_ARG(c) do { if (!(c)) return MP_ERR_ARG; } while (0)
+
+static int check_params(const mp_params* p, std::string& err) {
+    if (!p) { err = "null params"; return MP_ERR_ARG; }
+    if (p->version != MP_PARAMS_VERSION) { err = "params version mismatch"; return MP_ERR_ARG; }
+    if (p->nx < 4 || p->ny < 4 || p->nz < 4) { err = "grid must be at least 4^3"; return MP_ERR_ARG; }
+    long long n = (long long)p->nx * p->ny * p->nz;
+    if (8 * n + 1 > 0x7fffffffLL || 3LL * (2 * p->nx + 1) * (2 * p->ny + 1) * (2 * p->nz + 1) > 0x7fffffffLL) {
+        err = "grid too large for 32-bit indexing"; return MP_ERR_ARG;
+    }
+    if (p->par_num_max < 0) { err = "par_num_max < 0"; return MP_ERR_ARG; }
+    if (!(p->cellsize > 0) || !(p->dt > 0)) { err = "cellsize and dt must be positive"; return MP_ERR_ARG; }
+    if (p->mc_every < 0 || p->smooth_iters < 0 || p->cg_max_iter < 0 || p->heat_cg_max_iter < 0) { err = "negative count"; return MP_ERR_ARG; }
+    if (p->scene < 0 || p->scene > MP_SCENE_ALL) { err = "bad scene"; return MP_ERR_ARG; }
+    if (p->precision != MP_PREC_MIXED && p->precision != MP_PREC_FP64) { err = "bad precision"; return MP_ERR_ARG; }
+    if (p->cg_tol_mode != MP_TOL_REF_ABS && p->cg_tol_mode != MP_TOL_REL) { err = "bad cg_tol_mode"; return MP_ERR_ARG; }
+    if (p->coef_mode != MP_COEF_REF) { err = "only MP_COEF_REF is implemented"; return MP_ERR_ARG; }
+    if (p->mc_max_verts < 1 || p->mc_max_tris < 1) { err = "marching-cubes caps must be positive"; return MP_ERR_ARG; }
+    return MP_OK;
+}
+
+static thread_local std::string g_create_err;
+
+extern "C" int mp_create(const mp_params* p, void** ctx) {
+    if (!ctx) return MP_ERR_ARG;
+    *ctx = nullptr;
+    int rc = check_params(p, g_create_err);
+    if (rc) return rc;
+    MpCtx* c = new (std::nothrow) MpCtx();
+    if (!c) return MP_ERR_CAPACITY;
+    rc = create_impl(c, p);
+    if (rc != MP_OK) { g_create_err = c->err; free_all(c); delete c; return rc; }
+    *ctx = c;
+    return MP_OK;
+}
+
+extern "C" int mp_destroy(void* ctx) {
+    MpCtx* c = C(ctx);
+    CTX_OR_ARG(c);
+    cudaStreamSynchronize(c->stream);
+    free_all(c);
+    delete c;
+    return MP_OK;
+}
+
+extern "C" int mp_set_params(void* ctx, const mp_params* p) {
+    MpCtx* c = C(ctx);
+    CTX_OR_ARG(c);
+    int rc = check_params(p, c->err);
+    if (rc) return rc;
+    if (p->nx != c->P.nx || p->ny != c->P.ny || p->nz != c->P.nz || p->par_num_max != c->P.par_num_max ||
+        p->b_run_mc != c->P.b_run_mc || p->mc_max_verts != c->P.mc_max_verts || p->mc_max_tris != c->P.mc_max_tris) {
+        c->err = "grid size, capacity and marching-cubes buffers are fixed at mp_create";
+        return MP_ERR_ARG;
+    }
+    c->P = *p;
+    c->G.h = p->cellsize; c->G.gx0 = p->gmin_x; c->G.gy0 = p->gmin_y; c->G.gz0 = p->gmin_z;
+    return MP_OK;
+}
+extern "C" int mp_get_params(void* ctx, mp_params* p) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); if (!p) return MP_ERR_ARG;
+    *p = c->P; return MP_OK;
+}
+extern "C" int mp_get_state(void* ctx, mp_state* s) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); if (!s) return MP_ERR_ARG;
+    *s = c->S; return MP_OK;
+}
+extern "C" int mp_set_state(void* ctx, const mp_state* s) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); if (!s) return MP_ERR_ARG;
+    if (s->par_num_now < 0 || s->par_num_now > c->P.par_num_max) { c->err = "par_num_now out of range"; return MP_ERR_ARG; }
+    c->S.frame = s->frame; c->S.par_num_now = s->par_num_now; c->S.n_real_solpoint = s->n_real_solpoint;
+    return MP_OK;
+}
+extern "C" int mp_last_error(void* ctx, char* buf, size_t len) {
+    if (!buf || len == 0) return MP_ERR_ARG;
+    const std::string& e = ctx ? C(ctx)->err : g_create_err;
+    size_t k = std::min(len - 1, e.size());
+    memcpy(buf, e.data(), k);
+    buf[k] = 0;
+    return MP_OK;
+}
+extern "C" int mp_set_stream(void* ctx, void* stream) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->own_stream) { cudaStreamDestroy(c->stream); c->own_stream = false; }
+    c->stream = (cudaStream_t)stream;
+    return MP_OK;
+}
+extern "C" int mp_get_stream(void* ctx, void** stream) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); if (!stream) return MP_ERR_ARG;
+    *stream = (void*)c->stream; return MP_OK;
+}
+extern "C" int mp_synchronize(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+extern "C" int mp_get_device(void* ctx, int* device) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); if (!device) return MP_ERR_ARG;
+    *device = c->device; return MP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// data in / out
+// ---------------------------------------------------------------------------
+extern "C" int mp_upload_particles(void* ctx, int n, const float* pos3, const float* vel3, const int8_t* flag,
+                                   const float* mass, const float* temp, const float* lheat, const float* sol,
+                                   const float* gas) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (n < 0 || (n > 0 && (!pos3 || !flag || !mass))) { c->err = "upload: bad arguments"; return MP_ERR_ARG; }
+    if (n > c->P.par_num_max) { c->err = "upload: more particles than par_num_max"; return MP_ERR_CAPACITY; }
+    MP_TRY(k_pack_particles(c, n, pos3, vel3, flag, mass, temp, lheat, sol, gas));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->S.par_num_now = n;
+    c->mc_sorted = 0;
+    return MP_OK;
+}
+extern "C" int mp_download_particles(void* ctx, int* n, float* pos3, float* vel3, int8_t* flag, float* mass,
+                                     float* temp, float* lheat, float* sol, float* gas) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (n) *n = c->np();
+    return k_unpack_particles(c, c->np(), pos3, vel3, flag, mass, temp, lheat, sol, gas);
+}
+
+static void* field_dev(MpCtx* c, int f, size_t& count, size_t& eb) {
+    const mpk::Grid& g = c->G;
+    eb = 4;
+    switch (f) {
+    case MP_F_PRESS: count = g.n; return c->press;
+    case MP_F_DIV: count = g.n; return c->divg;
+    case MP_F_LSFLUID: count = g.n; return c->lsfluid;
+    case MP_F_LSAIR: count = g.n; return c->lsair;
+    case MP_F_LSMERGE: count = g.n; return c->lsmerge;
+    case MP_F_PHIFLUID: count = g.n; return c->phifluid;
+    case MP_F_PHIAIR: count = g.n; return c->phiair;
+    case MP_F_PHISOLID: count = g.n; return c->phisolid;
+    case MP_F_PHIGRAX: count = g.n; return c->gx;
+    case MP_F_PHIGRAY: count = g.n; return c->gy;
+    case MP_F_PHIGRAZ: count = g.n; return c->gz;
+    case MP_F_PHIGRAX_AIR: count = g.n; return c->gxa;
+    case MP_F_PHIGRAY_AIR: count = g.n; return c->gya;
+    case MP_F_PHIGRAZ_AIR: count = g.n; return c->gza;
+    case MP_F_SURFTENSION: count = g.n; return c->sf;
+    case MP_F_TP: count = g.n; return c->Tp;
+    case MP_F_TP_SAVE: count = g.n; return c->Tp_save;
+    case MP_F_TP_OLD: count = g.n; return c->Tp_old;
+    case MP_F_FIXEDHEAT: count = g.n; return c->fixedheat;
+    case MP_F_MARK: count = g.n; eb = 1; return c->mark;
+    case MP_F_WATERUX: count = g.nfx; return c->wu[0];
+    case MP_F_WATERUY: count = g.nfy; return c->wu[1];
+    case MP_F_WATERUZ: count = g.nfz; return c->wu[2];
+    case MP_F_WATERUX_OLD: count = g.nfx; return c->wuo[0];
+    case MP_F_WATERUY_OLD: count = g.nfy; return c->wuo[1];
+    case MP_F_WATERUZ_OLD: count = g.nfz; return c->wuo[2];
+    case MP_F_AIRUX: count = g.nfx; return c->au[0];
+    case MP_F_AIRUY: count = g.nfy; return c->au[1];
+    case MP_F_AIRUZ: count = g.nfz; return c->au[2];
+    case MP_F_AIRUX_OLD: count = g.nfx; return c->auo[0];
+    case MP_F_AIRUY_OLD: count = g.nfy; return c->auo[1];
+    case MP_F_AIRUZ_OLD: count = g.nfz; return c->auo[2];
+    case MP_F_SOLIDUX: count = g.nfx; return c->su[0];
+    case MP_F_SOLIDUY: count = g.nfy; return c->su[1];
+    case MP_F_SOLIDUZ: count = g.nfz; return c->su[2];
+    default: count = 0; return nullptr;
+    }
+}
+
+extern "C" int mp_field_info(void* ctx, int f, size_t* count, size_t* eb) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    size_t cnt = 0, e = 4;
+    if (f == MP_F_CELLSTART || f == MP_F_CELLEND) { cnt = c->G.n; e = 4; }
+    else if (f == MP_P_POS || f == MP_P_VEL) { cnt = 3 * (size_t)c->np(); e = 4; }
+    else if (f == MP_P_FLAG) { cnt = c->np(); e = 1; }
+    else if (f >= MP_P_MASS && f <= MP_P_GASCONTAIN) { cnt = c->np(); e = 4; }
+    else if (!field_dev(c, f, cnt, e)) { c->err = "unknown field"; return MP_ERR_ARG; }
+    if (count) *count = cnt;
+    if (eb) *eb = e;
+    return MP_OK;
+}
+
+// particle attribute <-> (float4 stream, component)
+static bool pattr(int f, int& stream, int& comp) {
+    switch (f) {
+    case MP_P_MASS: stream = 1; comp = 3; return true;
+    case MP_P_TEMP: stream = 2; comp = 0; return true;
+    case MP_P_LHEAT: stream = 2; comp = 1; return true;
+    case MP_P_SOLUBILITY: stream = 2; comp = 2; return true;
+    case MP_P_GASCONTAIN: stream = 2; comp = 3; return true;
+    default: return false;
+    }
+}
+
+extern "C" int mp_get_field(void* ctx, int f, void* dst, size_t bytes) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    size_t cnt, e;
+    MP_TRY(mp_field_info(ctx, f, &cnt, &e));
+    if (bytes != cnt * e || (bytes && !dst)) { c->err = "get_field: size mismatch"; return MP_ERR_ARG; }
+    if (!bytes) return MP_OK;
+    if (c->mc_sorted && (f == MP_F_CELLSTART || f == MP_F_CELLEND)) { c->err = "cell ranges are on the 2x grid"; return MP_ERR_STATE; }
+    int np = c->np();
+    if (f == MP_F_CELLSTART || f == MP_F_CELLEND) {
+        uint32_t* st = c->keys; uint32_t* en = c->perm;   // scratch, n entries each
+        MP_TRY(k_cells_to_startend(c, st, en));
+        MP_CUDA(c, cudaMemcpyAsync(dst, f == MP_F_CELLSTART ? st : en, bytes, cudaMemcpyDeviceToHost, c->stream));
+    } else if (f >= MP_P_POS && f <= MP_P_GASCONTAIN) {
+        std::vector<float> p3, v3, m, T, L, so, ga;
+        std::vector<int8_t> fl;
+        p3.resize(3 * (size_t)np); v3.resize(3 * (size_t)np); fl.resize(np); m.resize(np); T.resize(np);
+        L.resize(np); so.resize(np); ga.resize(np);
+        MP_TRY(k_unpack_particles(c, np, p3.data(), v3.data(), fl.data(), m.data(), T.data(), L.data(), so.data(), ga.data()));
+        const void* src = nullptr;
+        switch (f) {
+        case MP_P_POS: src = p3.data(); break;
+        case MP_P_VEL: src = v3.data(); break;
+        case MP_P_FLAG: src = fl.data(); break;
+        case MP_P_MASS: src = m.data(); break;
+        case MP_P_TEMP: src = T.data(); break;
+        case MP_P_LHEAT: src = L.data(); break;
+        case MP_P_SOLUBILITY: src = so.data(); break;
+        default: src = ga.data(); break;
+        }
+        memcpy(dst, src, bytes);
+        return MP_OK;
+    } else {
+        void* d = field_dev(c, f, cnt, e);
+        MP_CUDA(c, cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+    }
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+
+extern "C" int mp_set_field(void* ctx, int f, const void* src, size_t bytes) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    size_t cnt, e;
+    MP_TRY(mp_field_info(ctx, f, &cnt, &e));
+    if (bytes != cnt * e || (bytes && !src)) { c->err = "set_field: size mismatch"; return MP_ERR_ARG; }
+    if (f == MP_F_CELLSTART || f == MP_F_CELLEND) { c->err = "cell ranges are derived by mp_hash_sort"; return MP_ERR_ARG; }
+    if (!bytes) return MP_OK;
+    if (f >= MP_P_POS && f <= MP_P_GASCONTAIN) {
+        int np = c->np();
+        std::vector<float> p3(3 * (size_t)np), v3(3 * (size_t)np), m(np), T(np), L(np), so(np), ga(np);
+        std::vector<int8_t> fl(np);
+        MP_TRY(k_unpack_particles(c, np, p3.data(), v3.data(), fl.data(), m.data(), T.data(), L.data(), so.data(), ga.data()));
+        void* dstp = nullptr;
+        switch (f) {
+        case MP_P_POS: dstp = p3.data(); break;
+        case MP_P_VEL: dstp = v3.data(); break;
+        case MP_P_FLAG: dstp = fl.data(); break;
+        case MP_P_MASS: dstp = m.data(); break;
+        case MP_P_TEMP: dstp = T.data(); break;
+        case MP_P_LHEAT: dstp = L.data(); break;
+        case MP_P_SOLUBILITY: dstp = so.data(); break;
+        default: dstp = ga.data(); break;
+        }
+        memcpy(dstp, src, bytes);
+        MP_TRY(k_pack_particles(c, np, p3.data(), v3.data(), fl.data(), m.data(), T.data(), L.data(), so.data(), ga.data()));
+    } else {
+        void* d = field_dev(c, f, cnt, e);
+        MP_CUDA(c, cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+
+extern "C" int mp_set_tables(void* ctx, const float* randfloat, int nrand, const int32_t* seeds, int nseed) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (nrand <= 200 || !randfloat || nseed < 0 || (nseed > 0 && !seeds)) { c->err = "set_tables: need > 200 random values"; return MP_ERR_ARG; }
+    if (nrand != c->nrand) {
+        if (c->randf) cudaFree(c->randf);
+        c->randf = nullptr;
+        MP_TRY(dalloc_t(c, &c->randf, nrand));
+        c->nrand = nrand;
+    }
+    if (nseed != c->nseed || !c->seeds) {
+        if (c->seeds) cudaFree(c->seeds);
+        c->seeds = nullptr;
+        MP_TRY(dalloc_t(c, &c->seeds, std::max(nseed, 1)));
+        c->nseed = nseed;
+    }
+    MP_CUDA(c, cudaMemcpyAsync(c->randf, randfloat, sizeof(float) * nrand, cudaMemcpyHostToDevice, c->stream));
+    if (nseed) MP_CUDA(c, cudaMemcpyAsync(c->seeds, seeds, sizeof(int32_t) * nseed, cudaMemcpyHostToDevice, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+
+extern "C" int mp_mc_tables(int32_t* num_verts, int32_t* tri, int32_t* edge) {
+    mp_internal_mc_tables(num_verts, tri, edge);
+    return MP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernel timing
+// ---------------------------------------------------------------------------
+static void kt_harvest(MpCtx* c, int cls) {
+    auto& pend = c->kt_pending[cls];
+    size_t keep = 0;
+    for (size_t q = 0; q < pend.size(); q++) {
+        if (cudaEventQuery(pend[q].second) == cudaSuccess) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, pend[q].first, pend[q].second);
+            c->kt_ms[cls] += ms;
+            c->kt_launch[cls]++;
+            c->kt_pool.push_back(pend[q]);
+        } else pend[keep++] = pend[q];
+    }
+    pend.resize(keep);
+}
+void kt_begin(MpCtx* c, int cls, cudaEvent_t* ev_end) {
+    *ev_end = 0;
+    if (cls < 0 || cls >= MP_KT_COUNT || !c->kt_on[cls]) return;
+    std::pair<cudaEvent_t, cudaEvent_t> e;
+    if (!c->kt_pool.empty()) { e = c->kt_pool.back(); c->kt_pool.pop_back(); }
+    else { cudaEventCreate(&e.first); cudaEventCreate(&e.second); }
+    cudaEventRecord(e.first, c->stream);
+    c->kt_pending[cls].push_back(e);
+    *ev_end = e.second;
+}
+void kt_end(MpCtx* c, int cls, cudaEvent_t ev_end) {
+    if (!ev_end) return;
+    cudaEventRecord(ev_end, c->stream);
+    if (c->kt_pending[cls].size() > 4096) { cudaStreamSynchronize(c->stream); kt_harvest(c, cls); }
+}
+extern "C" int mp_kernel_timing(void* ctx, int cls, int enable) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (cls < 0 || cls >= MP_KT_COUNT) return MP_ERR_ARG;
+    c->kt_on[cls] = enable != 0;
+    return MP_OK;
+}
+extern "C" int mp_kernel_timing_read(void* ctx, int cls, double* ms, int64_t* launches) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (cls < 0 || cls >= MP_KT_COUNT) return MP_ERR_ARG;
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    kt_harvest(c, cls);
+    if (ms) *ms = c->kt_ms[cls];
+    if (launches) *launches = c->kt_launch[cls];
+    return MP_OK;
+}
+extern "C" int mp_kernel_timing_reset(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < MP_KT_COUNT; k++) { kt_harvest(c, k); c->kt_ms[k] = 0; c->kt_launch[k] = 0; }
+    c->launches = 0;
+    return MP_OK;
+}
+extern "C" int64_t mp_launch_count(void* ctx) {
+    MpCtx* c = C(ctx);
+    return c ? c->launches : -1;
+}
+
+// ---------------------------------------------------------------------------
+// stages
+// ---------------------------------------------------------------------------
+static int need_cells(MpCtx* c) {
+    if (c->mc_sorted) { c->err = "particles are sorted on the marching-cubes grid; call mp_hash_sort first"; return MP_ERR_STATE; }
+    return MP_OK;
+}
+#define STAGE(name, body)                                  \
+    extern "C" int name(void* ctx) {                       \
+        MpCtx* c = C(ctx); CTX_OR_ARG(c);                  \
+        body;                                              \
+    }
+
+extern "C" int mp_init_particle_heat(void* ctx) { MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_init_particle_heat(c); }
+STAGE(mp_hash_sort, return k_hash_sort(c))
+STAGE(mp_external_force, return k_external_force(c))
+extern "C" int mp_levelset(void* ctx, float offset) {
+    (void)offset;   // ignored by genlevelset (spray_k.cu:2803-2804)
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); MP_TRY(need_cells(c)); return k_levelset(c);
+}
+STAGE(mp_sweep_ls_mark, return k_sweep_ls_mark(c))
+STAGE(mp_mark_solo_air, MP_TRY(need_cells(c)); return k_mark_solo_air(c))
+STAGE(mp_surface_tension, return k_surface_tension(c))
+STAGE(mp_markgrid_bubble, MP_TRY(need_cells(c)); return k_markgrid_bubble(c))
+STAGE(mp_p2g, MP_TRY(need_cells(c)); return k_p2g(c))
+STAGE(mp_drag, MP_TRY(need_cells(c)); return k_drag(c))
+extern "C" int mp_sweep_phi(void* ctx, int ph) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (ph != MP_TYPEFLUID && ph != MP_TYPEAIR) return MP_ERR_ARG;
+    return k_sweep_phi(c, ph);
+}
+extern "C" int mp_sweep_u(void* ctx, int ph) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (ph != MP_TYPEFLUID && ph != MP_TYPEAIR) return MP_ERR_ARG;
+    return k_sweep_u(c, ph);
+}
+extern "C" int mp_set_boundary_u(void* ctx, int ph) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (ph != MP_TYPEFLUID && ph != MP_TYPEAIR) return MP_ERR_ARG;
+    return k_set_boundary_u(c, ph);
+}
+extern "C" int mp_project(void* ctx, int* iters, double* residual) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    return k_project(c, iters, residual);
+}
+STAGE(mp_g2p, return k_g2p(c))
+STAGE(mp_solid_motion, return k_solid_motion(c))
+STAGE(mp_solo_air_update, MP_TRY(need_cells(c)); return k_solo_air_update(c))
+STAGE(mp_collide_advect, MP_TRY(need_cells(c)); return k_collide_advect(c))
+STAGE(mp_correct_pos, MP_TRY(need_cells(c)); return k_correct_pos(c))
+STAGE(mp_correct_pos_bubble, return k_correct_pos_bubble(c))
+STAGE(mp_heat, MP_TRY(need_cells(c)); return k_heat(c))
+STAGE(mp_gen_gas, MP_TRY(need_cells(c)); return k_gen_gas(c))
+STAGE(mp_delete, return k_delete(c))
+STAGE(mp_melt, return k_melt(c))
+STAGE(mp_freeze, MP_TRY(need_cells(c)); return k_freeze(c))
+STAGE(mp_mc_presort, if (!c->P.b_run_mc) { c->err = "marching cubes disabled at mp_create"; return MP_ERR_STATE; } return k_mc_presort(c))
+extern "C" int mp_mc(void* ctx, int surface) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (surface < 0 || surface > 2) return MP_ERR_ARG;
+    if (!c->P.b_run_mc) { c->err = "marching cubes disabled at mp_create"; return MP_ERR_STATE; }
+    return k_mc(c, surface);
+}
+extern "C" int mp_mc_download(void* ctx, int surface, float* verts, float* normals, uint32_t* indices, int max_verts,
+                              int max_indices) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (surface < 0 || surface > 2 || !c->P.b_run_mc) return MP_ERR_ARG;
+    McSurface& m = c->mc[surface];
+    if (m.nverts > max_verts || m.nindices > max_indices) { c->err = "mc_download: buffers too small"; return MP_ERR_CAPACITY; }
+    if (verts && m.nverts) MP_CUDA(c, cudaMemcpyAsync(verts, m.verts, 12 * (size_t)m.nverts, cudaMemcpyDeviceToHost, c->stream));
+    if (normals && m.nverts) MP_CUDA(c, cudaMemcpyAsync(normals, m.normals, 12 * (size_t)m.nverts, cudaMemcpyDeviceToHost, c->stream));
+    if (indices && m.nindices) MP_CUDA(c, cudaMemcpyAsync(indices, m.indices, 4 * (size_t)m.nindices, cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+extern "C" int mp_mc_download_field(void* ctx, float* dens, uint8_t* cube) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!c->P.b_run_mc) return MP_ERR_STATE;
+    size_t nnode = (size_t)(2 * c->G.NX + 1) * (2 * c->G.NY + 1) * (2 * c->G.NZ + 1), nvox = 8 * (size_t)c->G.n;
+    if (dens) MP_CUDA(c, cudaMemcpyAsync(dens, c->mc_dens, 4 * nnode, cudaMemcpyDeviceToHost, c->stream));
+    if (cube) MP_CUDA(c, cudaMemcpyAsync(cube, c->mc_cube, nvox, cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+
+// bubblesim (spray.cpp:979-1233): the stage order and cadence of the reference.
+// Scene-scripted flag toggles of SCENE_ALL / MELTANDBOIL / INTERACTION frames
+// (spray.cpp:1007-1047), pouring (spray.cpp:999-1002) and seed re-draws with
+// the host rand() are not part of this step.
+extern "C" int mp_step(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    const mp_params& P = c->P;
+    int sc = P.scene;
+    int warn = MP_OK, st;
+    MP_TRY(k_hash_sort(c));
+    MP_TRY(k_external_force(c));
+    MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
+    MP_TRY(k_mark_solo_air(c));
+    MP_TRY(k_surface_tension(c));
+    if (sc == MP_SCENE_MELTING || sc == MP_SCENE_FREEZING) MP_TRY(k_markgrid_bubble(c));
+    MP_TRY(k_p2g(c));
+    MP_TRY(k_drag(c));
+    MP_TRY(k_sweep_phi(c, MP_TYPEAIR)); MP_TRY(k_sweep_u(c, MP_TYPEAIR));
+    MP_TRY(k_sweep_phi(c, MP_TYPEFLUID)); MP_TRY(k_sweep_u(c, MP_TYPEFLUID));
+    MP_TRY(k_set_boundary_u(c, MP_TYPEAIR)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+    st = k_project(c, nullptr, nullptr);
+    if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st);
+    MP_TRY(k_sweep_u(c, MP_TYPEAIR)); MP_TRY(k_sweep_u(c, MP_TYPEFLUID));
+    MP_TRY(k_set_boundary_u(c, MP_TYPEAIR)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+    MP_TRY(k_g2p(c));
+    MP_TRY(k_solid_motion(c));
+    MP_TRY(k_solo_air_update(c));
+    MP_TRY(k_hash_sort(c)); MP_TRY(k_collide_advect(c));
+    if (P.b_correct_position) {
+        MP_TRY(k_hash_sort(c)); MP_TRY(k_correct_pos(c));
+        MP_TRY(k_hash_sort(c)); MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c)); MP_TRY(k_correct_pos_bubble(c));
+    } else {
+        MP_TRY(k_hash_sort(c)); MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
+    }
+    MP_TRY(k_hash_sort(c));
+    if (P.b_heat_trans) { st = k_heat(c); if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st); }
+    if (P.b_gen_gas && c->S.frame % 2 == 0) MP_TRY(k_gen_gas(c));
+    MP_TRY(k_hash_sort(c)); MP_TRY(k_delete(c));
+    MP_TRY(k_hash_sort(c));
+    if (P.b_melt) MP_TRY(k_melt(c));
+    if (P.b_freeze) MP_TRY(k_freeze(c));
+    if (P.b_run_mc && P.mc_every > 0 && c->S.frame % P.mc_every == 0) {
+        MP_TRY(k_mc_presort(c));
+        for (int s = 0; s < 3; s++) MP_TRY(k_mc(c, s));
+    }
+    c->S.frame++;
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    MP_CHECK_LAUNCH(c);
+    return warn;
+}

@@ -1,0 +1,473 @@
+// k_cg.cu — two-phase divergence, conjugate-gradient pressure and heat solves,
+// pressure gradient, heat-grid bookkeeping.
+//
+// Reference: cptdivergence_bubble2 (Multiphase/Multiphase/spray_k.cu:3138-3263),
+// solver_cg_bubble (spray.cu:1613-1687) with computeAx_bubble / pcg_op_bubble
+// (spray_k.cu:3423-3460) and product()/arrayproduct_k (spray.cu:1101-1116,
+// spray_k.cu:2279-2297), subGradPress (spray_k.cu:198-224); solver_cg_heat
+// (spray.cu:1780-1852) with computeAx_heat / pcg_op_heat (spray_k.cu:4526-4583),
+// addHeatAtBottom, compb_heat, setBoundaryHeat, compTpChange (spray_k.cu:4492-4617).
+//
+// The reference's "preconditioner" is the identity (z = r copies, spray.cu:1632,1671).
+// It runs 3 host round trips per iteration (dot products summed on the host in
+// FP32). Here alpha, beta and the residual live on the device in FP64; each
+// iteration is two kernels, both recomputing A p from p instead of storing it:
+//   k_cg_dir : p <- r + beta p (masked, double-buffered), z = A p, p.z
+//   k_cg_upd : z = A p, x <- x + alpha p, r <- r - alpha z, r.r, stop test
+// Dot products are FP64 block sums finished by the last block in block order,
+// so they are deterministic. Vectors are FP32 (MP_PREC_MIXED) or FP64.
+#include "ctx.cuh"
+
+using namespace mpk;
+
+namespace {
+
+constexpr int CG_T = 256;
+
+// device scalar slots
+enum { S_A = 0, S_RR = 1, S_ALPHA = 2, S_BETA = 3, S_EPS = 4, S_ZP = 5 };
+// flag slots (unsigned int): done state and iteration count
+enum { F_DONE = 0, F_ITERS = 1, F_COUNT = 2 };
+enum { DONE_RUN = 0, DONE_CONV = 1, DONE_CAP = 2, DONE_ZP0 = 3 };
+
+struct Red {
+    double* part;           // gridDim.x partials
+    unsigned int* count;    // last-block counter
+    double* scal;
+    unsigned int* flag;
+};
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double ws[CG_T / 32];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < CG_T / 32; w++) s += ws[w];
+    return s;   // valid in thread 0
+}
+// returns true in thread 0 of the last block, with the total in *tot
+__device__ __forceinline__ bool finish_sum(const Red& R, double mine, double* tot) {
+    __shared__ bool last;
+    double s = block_sum(mine);
+    if (threadIdx.x == 0) {
+        R.part[blockIdx.x] = s;
+        __threadfence();
+        unsigned int t = atomicAdd(R.count, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    if (threadIdx.x < 32) {
+        double a = 0;
+        for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32) a += ((volatile double*)R.part)[b];
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (threadIdx.x == 0) { *tot = a; *R.count = 0; }
+    }
+    return threadIdx.x == 0;
+}
+
+// ---- matrices --------------------------------------------------------------
+// computeAx_bubble (spray_k.cu:3423-3447): rows over FLUID and AIR cells
+struct PressOp {
+    Grid g;
+    const int8_t* __restrict__ mark;
+    __device__ __forceinline__ bool mask(int idx) const {
+        int m = mark[idx];
+        return (m == MP_TYPEFLUID || m == MP_TYPEAIR) && interior(g, idx);
+    }
+    template <class R, class F>
+    __device__ __forceinline__ R apply(int idx, F val) const {
+        int i, j, k; getijk(g, idx, i, j, k);
+        R c = val(idx);
+        R s = (R)(-6.0f) * c;
+        R h2 = (R)g.h * (R)g.h;
+        int q;
+        q = cid(g, i + 1, j, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = cid(g, i, j + 1, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = cid(g, i, j, k + 1); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = cid(g, i - 1, j, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = cid(g, i, j - 1, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = cid(g, i, j, k - 1); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        return s / h2;
+    }
+};
+// computeAx_heat (spray_k.cu:4526-4568): rows over non-BOUNDARY cells
+struct HeatOp {
+    Grid g;
+    const int8_t* __restrict__ mark;
+    float alpha[MP_TYPECNT];
+    float dt;
+    int boil;    // VACUUM neighbours also take the centre value in boiling scenes
+    __device__ __forceinline__ bool mask(int idx) const { return mark[idx] != MP_TYPEBOUNDARY && interior(g, idx); }
+    template <class R, class F>
+    __device__ __forceinline__ R apply(int idx, F val) const {
+        int i, j, k; getijk(g, idx, i, j, k);
+        float al = alpha[mark[idx]];
+        float h = g.h;
+        R c = val(idx);
+        R s = (R)(h * h / al / dt + 6.0f) * c;
+        int q;
+        auto fix = [&](int qq) { int m = mark[qq]; return boil ? (m == MP_TYPEBOUNDARY || m == MP_TYPEVACUUM) : (m == MP_TYPEBOUNDARY); };
+        q = cid(g, i + 1, j, k); s -= fix(q) ? c : val(q);
+        q = cid(g, i, j + 1, k); s -= fix(q) ? c : val(q);
+        q = cid(g, i, j, k + 1); s -= fix(q) ? c : val(q);
+        q = cid(g, i - 1, j, k); s -= fix(q) ? c : val(q);
+        q = cid(g, i, j - 1, k); s -= fix(q) ? c : val(q);
+        q = cid(g, i, j, k - 1); s -= fix(q) ? c : val(q);
+        return s;
+    }
+};
+
+// r = mask ? b : 0 (x = 0, so b - A x = b); rr; a = rr; eps; stop if converged
+template <class R, class Op>
+__global__ void __launch_bounds__(CG_T) k_cg_init(Op op, int n, const R* __restrict__ b, R* __restrict__ r, Red Rd,
+                                                  int tolmode, float tol) {
+    double acc = 0;
+    MP_GRID_LOOP(idx, n) {
+        R v = op.mask((int)idx) ? (R)(b[idx] + (R)(-1.0f) * (R)0) : (R)0;
+        r[idx] = v;
+        acc += (double)v * (double)v;
+    }
+    double tot;
+    if (finish_sum(Rd, acc, &tot)) {
+        double eps = tolmode == MP_TOL_REF_ABS ? (double)(tol * (float)n) : (double)tol * (double)tol * tot;
+        Rd.scal[S_RR] = tot; Rd.scal[S_A] = tot; Rd.scal[S_EPS] = eps;
+        Rd.flag[F_ITERS] = 0;
+        Rd.flag[F_DONE] = (tot < eps || (tolmode == MP_TOL_REL && eps == 0.0)) ? DONE_CONV : DONE_RUN;
+    }
+}
+
+// p_new = mask ? r + beta p_old : 0 (first iteration: p = r), z = A p_new, p_new . z
+template <class R, class Op>
+__global__ void __launch_bounds__(CG_T) k_cg_dir(Op op, int n, const R* __restrict__ r, const R* __restrict__ pold,
+                                                 R* __restrict__ pnew, Red Rd, int first) {
+    if (Rd.flag[F_DONE] != DONE_RUN) return;
+    R bf = first ? (R)0 : (R)Rd.scal[S_BETA];
+    auto pv = [&](int q) -> R {
+        if (!op.mask(q)) return (R)0;
+        return first ? r[q] : (R)(r[q] + bf * pold[q]);
+    };
+    double acc = 0;
+    MP_GRID_LOOP(idx, n) {
+        int id = (int)idx;
+        R pc = pv(id);
+        pnew[idx] = pc;
+        if (op.mask(id)) {
+            R z = op.template apply<R>(id, pv);
+            acc += (double)z * (double)pc;
+        }
+    }
+    double tot;
+    if (finish_sum(Rd, acc, &tot)) {
+        Rd.scal[S_ZP] = tot;
+        if (tot == 0) Rd.flag[F_DONE] = DONE_ZP0;
+        else Rd.scal[S_ALPHA] = Rd.scal[S_A] / tot;
+    }
+}
+
+// z = A p, x += alpha p, r -= alpha z (masked), r.r, stop test, beta
+template <class R, class Op>
+__global__ void __launch_bounds__(CG_T) k_cg_upd(Op op, int n, const R* __restrict__ p, R* __restrict__ x,
+                                                 R* __restrict__ r, Red Rd, int it, int maxiter, int skip_dot) {
+    if (Rd.flag[F_DONE] != DONE_RUN) return;
+    R af = (R)Rd.scal[S_ALPHA];
+    auto pv = [&](int q) -> R { return p[q]; };
+    double acc = 0;
+    MP_GRID_LOOP(idx, n) {
+        int id = (int)idx;
+        if (op.mask(id)) {
+            R z = op.template apply<R>(id, pv);
+            R xv = x[idx] + af * p[idx];
+            R rv = r[idx] + (-af) * z;
+            x[idx] = xv; r[idx] = rv;
+            acc += (double)rv * (double)rv;
+        } else {
+            x[idx] = (R)0; r[idx] = (R)0;
+        }
+    }
+    if (skip_dot) return;   // a true-residual pass follows
+    double tot;
+    if (finish_sum(Rd, acc, &tot)) {
+        Rd.scal[S_RR] = tot;
+        Rd.flag[F_ITERS] = it + 1;
+        if (tot < Rd.scal[S_EPS]) Rd.flag[F_DONE] = DONE_CONV;
+        else if (it + 1 >= maxiter) Rd.flag[F_DONE] = DONE_CAP;
+        else { Rd.scal[S_BETA] = tot / Rd.scal[S_A]; Rd.scal[S_A] = tot; }
+    }
+}
+
+// periodic true residual: r = mask ? b - A x : 0, then the same stop test
+template <class R, class Op>
+__global__ void __launch_bounds__(CG_T) k_cg_true(Op op, int n, const R* __restrict__ b, const R* __restrict__ x,
+                                                  R* __restrict__ r, Red Rd, int it, int maxiter) {
+    if (Rd.flag[F_DONE] != DONE_RUN) return;
+    auto xv = [&](int q) -> R { return x[q]; };
+    double acc = 0;
+    MP_GRID_LOOP(idx, n) {
+        int id = (int)idx;
+        R v = (R)0;
+        if (op.mask(id)) v = (R)(b[idx] + (R)(-1.0f) * op.template apply<R>(id, xv));
+        r[idx] = v;
+        acc += (double)v * (double)v;
+    }
+    double tot;
+    if (finish_sum(Rd, acc, &tot)) {
+        Rd.scal[S_RR] = tot;
+        Rd.flag[F_ITERS] = it + 1;
+        if (tot < Rd.scal[S_EPS]) Rd.flag[F_DONE] = DONE_CONV;
+        else if (it + 1 >= maxiter) Rd.flag[F_DONE] = DONE_CAP;
+        else { Rd.scal[S_BETA] = tot / Rd.scal[S_A]; Rd.scal[S_A] = tot; }
+    }
+}
+
+// cptdivergence_bubble2 (spray_k.cu:3138-3263)
+template <class R>
+__global__ void k_divergence(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ ls,
+                             const float* __restrict__ wx, const float* __restrict__ wy, const float* __restrict__ wz,
+                             const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ az,
+                             R* __restrict__ b, float* __restrict__ divf) {
+    MP_GRID_LOOP(idx, g.n) {
+        int m = mark[idx];
+        R out = 0;
+        if ((m == MP_TYPEFLUID || m == MP_TYPEAIR) && interior(g, (int)idx)) {
+            int i, j, k; getijk(g, (int)idx, i, j, k);
+            R lc = (R)ls[idx];
+            auto face = [&](int a, int bb, int cc, R wv, R av) -> R {
+                int q = cid(g, a, bb, cc);
+                int mn = mark[q];
+                if (m == MP_TYPEFLUID && mn != MP_TYPEAIR) return wv;
+                if (m == MP_TYPEAIR && mn != MP_TYPEFLUID) return av;
+                R th = ((R)0 - lc) / ((R)ls[q] - lc);
+                if (m == MP_TYPEFLUID) return th * wv + (1 - th) * av;
+                return th * av + (1 - th) * wv;
+            };
+            int f;
+            f = fxi(g, i + 1, j, k); R ux1 = face(i + 1, j, k, (R)wx[f], (R)ax[f]);
+            f = fxi(g, i, j, k);     R ux0 = face(i - 1, j, k, (R)wx[f], (R)ax[f]);
+            f = fyi(g, i, j + 1, k); R uy1 = face(i, j + 1, k, (R)wy[f], (R)ay[f]);
+            f = fyi(g, i, j, k);     R uy0 = face(i, j - 1, k, (R)wy[f], (R)ay[f]);
+            f = fzi(g, i, j, k + 1); R uz1 = face(i, j, k + 1, (R)wz[f], (R)az[f]);
+            f = fzi(g, i, j, k);     R uz0 = face(i, j, k - 1, (R)wz[f], (R)az[f]);
+            out = (ux1 - ux0 + uy1 - uy0 + uz1 - uz0) / (R)g.h;
+        }
+        b[idx] = out;
+        if (divf) divf[idx] = (float)out;
+    }
+}
+
+// subGradPress on the water and the air face fields
+template <class R>
+__global__ void k_subgrad(Grid g, const R* __restrict__ p, float* wx, float* wy, float* wz, float* ax, float* ay, float* az,
+                          float* __restrict__ pf) {
+    long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    R hh = (R)g.h;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k;
+        if (t < g.nfx) {
+            int idx = (int)t; getijk3(idx, g.NY, g.NZ, i, j, k);
+            if (i > 0 && i < g.NX) {
+                R d = (p[cid(g, i, j, k)] - p[cid(g, i - 1, j, k)]) / hh;
+                wx[idx] = (float)((R)wx[idx] - d); ax[idx] = (float)((R)ax[idx] - d);
+            }
+        } else if (t < (long long)g.nfx + g.nfy) {
+            int idx = (int)(t - g.nfx); getijk3(idx, g.NY + 1, g.NZ, i, j, k);
+            if (j > 0 && j < g.NY) {
+                R d = (p[cid(g, i, j, k)] - p[cid(g, i, j - 1, k)]) / hh;
+                wy[idx] = (float)((R)wy[idx] - d); ay[idx] = (float)((R)ay[idx] - d);
+            }
+        } else if (t < (long long)g.nfx + g.nfy + g.nfz) {
+            int idx = (int)(t - g.nfx - g.nfy); getijk3(idx, g.NY, g.NZ + 1, i, j, k);
+            if (k > 0 && k < g.NZ) {
+                R d = (p[cid(g, i, j, k)] - p[cid(g, i, j, k - 1)]) / hh;
+                wz[idx] = (float)((R)wz[idx] - d); az[idx] = (float)((R)az[idx] - d);
+            }
+        }
+        if (pf && t < g.n) pf[t] = (float)p[t];
+    }
+}
+
+// ---- heat grid ----------------------------------------------------------------
+__global__ void k_heat_bottom(Grid g, float* __restrict__ Tp, float inc, float clampv) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        float v = Tp[idx];
+        if (i >= 1 && i < g.NX - 1 && j >= 1 && j < g.NY - 1 && k <= 3) v += inc;
+        Tp[idx] = fminf(clampv, v);
+    }
+}
+// Tp_save copy + compb_heat; with fixed heat the held value feeds the
+// right-hand side (the dormant branch of compb_heat, spray_k.cu:4515-4519)
+__global__ void k_heat_rhs(Grid g, const float* __restrict__ Tp, float* __restrict__ save, float* __restrict__ bo,
+                           const int8_t* __restrict__ mark, const float* __restrict__ fixedheat, HeatOp op) {
+    MP_GRID_LOOP(idx, g.n) {
+        float t = Tp[idx];
+        save[idx] = t;
+        float al = op.alpha[mark[idx]];
+        if (fixedheat && fixedheat[idx] != MP_UNDEF_TEMPERATURE) t = fixedheat[idx];
+        bo[idx] = t * g.h * g.h / al / op.dt;
+    }
+}
+__global__ void k_heat_bound(Grid g, const float* __restrict__ in, float* __restrict__ out) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        float v = in[idx];
+        if (i == g.NX - 1) v = in[cid(g, i - 1, j, k)];
+        else if (i == 0) v = in[cid(g, i + 1, j, k)];
+        else if (j == g.NY - 1) v = in[cid(g, i, j - 1, k)];
+        else if (j == 0) v = in[cid(g, i, j + 1, k)];
+        else if (k == g.NZ - 1) v = in[cid(g, i, j, k - 1)];
+        else if (k == 0) v = in[cid(g, i, j, k + 1)];
+        out[idx] = v;
+    }
+}
+__global__ void k_tp_change(int n, const float* __restrict__ Tp, float* __restrict__ save, const int8_t* __restrict__ mark) {
+    MP_GRID_LOOP(idx, n) save[idx] = (mark[idx] != MP_TYPEBOUNDARY) ? Tp[idx] - save[idx] : 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+static Red red_of(MpCtx* c) {
+    return Red{c->red, c->red_count, c->scal, reinterpret_cast<unsigned int*>(c->red_count + 1)};
+}
+
+// Runs CG on x (zeroed here) for A x = b. Batches iterations between host
+// checks of the device stop flag; launches after the stop exit at once.
+template <class R, class Op>
+static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, int maxiter, int tolmode, float tol,
+                  int true_every, int* iters_out, double* res_out, int kt_stencil) {
+    int n = c->G.n;
+    int nb = c->red_blocks;
+    Red Rd = red_of(c);
+    cudaStream_t s = c->stream;
+    MP_CUDA(c, cudaMemsetAsync(x, 0, sizeof(R) * n, s));
+    k_cg_init<R, Op><<<nb, CG_T, 0, s>>>(op, n, b, r, Rd, tolmode, tol);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    unsigned int hflag[F_COUNT] = {0, 0};
+    MP_CUDA(c, cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(c, cudaStreamSynchronize(s));
+    int it = 0, batch = 8;
+    R* pa = p0; R* pb = p1;
+    while (hflag[F_DONE] == DONE_RUN && it < maxiter) {
+        int end = std::min(maxiter, it + batch);
+        for (; it < end; it++) {
+            {
+                KtScope kt(c, kt_stencil);
+                k_cg_dir<R, Op><<<nb, CG_T, 0, s>>>(op, n, r, pa, pb, Rd, it == 0 ? 1 : 0);
+            }
+            bool tr = true_every > 0 && (it + 1) % true_every == 0;
+            {
+                KtScope kt(c, MP_KT_CG_UPDATE);
+                k_cg_upd<R, Op><<<nb, CG_T, 0, s>>>(op, n, pb, x, r, Rd, it, maxiter, tr ? 1 : 0);
+            }
+            if (tr) k_cg_true<R, Op><<<nb, CG_T, 0, s>>>(op, n, b, x, r, Rd, it, maxiter);
+            c->launches += tr ? 3 : 2;
+            std::swap(pa, pb);
+        }
+        MP_CHECK_LAUNCH(c);
+        MP_CUDA(c, cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(c, cudaStreamSynchronize(s));
+        if (batch < 64) batch *= 2;
+    }
+    double rr = 0;
+    MP_CUDA(c, cudaMemcpyAsync(&rr, Rd.scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(c, cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(c, cudaStreamSynchronize(s));
+    *iters_out = (int)hflag[F_ITERS];
+    *res_out = rr;
+    return hflag[F_DONE] == DONE_CAP ? MP_ERR_NOCONVERGE : MP_OK;
+}
+
+// project_CG_bubble (spray.cu:1590-1611)
+int k_project(MpCtx* c, int* iters, double* res) {
+    const Grid& g = c->G;
+    PressOp op{g, c->mark};
+    int nbk = mp_blocks(g.n, 256);
+    long long ftot = (long long)g.nfx + g.nfy + g.nfz;
+    long long gtot = std::max(ftot, (long long)g.n);
+    int it = 0; double rr = 0; int rc;
+    if (c->P.precision == MP_PREC_FP64) {
+        double* x = c->cg64;
+        double* b = x + g.n; double* r = b + g.n; double* p0 = r + g.n; double* p1 = p0 + g.n;
+        k_divergence<double><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
+                                                         c->au[0], c->au[1], c->au[2], b, c->divg);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        rc = run_cg<double>(c, op, x, b, r, p0, p1, c->P.cg_max_iter, c->P.cg_tol_mode, c->P.cg_tol,
+                            c->P.cg_true_residual_every, &it, &rr, MP_KT_CG_STENCIL);
+        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+        k_subgrad<double><<<mp_blocks(gtot, 256), 256, 0, c->stream>>>(g, x, c->wu[0], c->wu[1], c->wu[2], c->au[0],
+                                                                       c->au[1], c->au[2], c->press);
+    } else {
+        float* x = c->press;
+        k_divergence<float><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
+                                                        c->au[0], c->au[1], c->au[2], c->divg, nullptr);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        rc = run_cg<float>(c, op, x, c->divg, c->cg_r, c->cg_p, c->cg_z, c->P.cg_max_iter, c->P.cg_tol_mode,
+                           c->P.cg_tol, c->P.cg_true_residual_every, &it, &rr, MP_KT_CG_STENCIL);
+        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+        k_subgrad<float><<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, x, c->wu[0], c->wu[1], c->wu[2], c->au[0],
+                                                                      c->au[1], c->au[2], nullptr);
+    }
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    c->S.last_cg_iters = it;
+    c->S.last_cg_residual = rr;
+    if (iters) *iters = it;
+    if (res) *res = rr;
+    return rc;
+}
+
+int k_heat_p2g_launch(MpCtx* c);
+int k_heat_g2p_launch(MpCtx* c);
+int k_latent_heat(MpCtx* c);
+
+// updateTemperature (spray.cu:1889-1947)
+int k_heat(MpCtx* c) {
+    const Grid& g = c->G;
+    const mp_params& P = c->P;
+    int nb = mp_blocks(g.n, 256);
+    MP_TRY(k_heat_p2g_launch(c));
+    if (P.b_add_heat_bottom) {
+        k_heat_bottom<<<nb, 256, 0, c->stream>>>(g, c->Tp, P.heat_increase_bottom, P.heat_clamp);
+        c->launches++;
+    }
+    HeatOp op;
+    op.g = g; op.mark = c->mark; op.dt = P.dt;
+    op.alpha[MP_TYPEFLUID] = P.heatalpha_fluid; op.alpha[MP_TYPEAIR] = P.heatalpha_air;
+    op.alpha[MP_TYPEVACUUM] = P.heatalpha_vacuum; op.alpha[MP_TYPESOLID] = P.heatalpha_solid;
+    op.alpha[MP_TYPEAIRSOLO] = P.heatalpha_air; op.alpha[MP_TYPEBOUNDARY] = 0;
+    int sc = P.scene;
+    op.boil = (sc == MP_SCENE_BOILING || sc == MP_SCENE_BOILING_HIGHRES || sc == MP_SCENE_MELTANDBOIL ||
+               sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL) ? 1 : 0;
+    k_heat_rhs<<<nb, 256, 0, c->stream>>>(g, c->Tp, c->Tp_save, c->Tp_old, c->mark,
+                                          P.b_fixed_heat ? c->fixedheat : nullptr, op);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    int it = 0; double rr = 0;
+    int rc = run_cg<float>(c, op, c->Tp, c->Tp_old, c->cg_r, c->cg_p, c->cg_z, P.heat_cg_max_iter, MP_TOL_REF_ABS,
+                           0.01f, 0, &it, &rr, MP_KT_CG_STENCIL);
+    if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+    c->S.last_heat_cg_iters = it;
+    c->S.last_heat_cg_residual = rr;
+    if (P.b_extend_heat_to_boundary) {
+        k_heat_bound<<<nb, 256, 0, c->stream>>>(g, c->Tp, c->cell_tmp);
+        c->launches++;
+        std::swap(c->Tp, c->cell_tmp);
+    }
+    k_tp_change<<<nb, 256, 0, c->stream>>>(g.n, c->Tp, c->Tp_save, c->mark);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    MP_TRY(k_heat_g2p_launch(c));
+    MP_TRY(k_latent_heat(c));
+    return rc;
+}

@@ -1,0 +1,429 @@
+// k_fields.cu — level set, Eikonal sweeps, cell marks, velocity extrapolation
+// and boundary conditions on the staggered grid.
+//
+// Reference kernels (Multiphase/Multiphase/spray_k.cu): genlevelset 2753-2806,
+// sweepphibytype/sweepphi/solvedistance 746-788, markLS_bigpositive 3683,
+// setLSback_bigpositive 3699, preparels 3708, setLSback 3724,
+// mergeLSAndMarkGrid 3733, computePhigra 3994, sweepu_k_bubble 3779,
+// setWaterBoundaryU_k 956, initphi 712, initSolidPhi 724, markfluid_dense 506,
+// markBoundaryCell 535, compsurfacetension_k 3543.
+// The reference updates the sweeps in place while neighbours read them (a
+// data race); here every pass reads the previous pass (Jacobi) through a
+// second buffer, so results do not depend on thread scheduling.
+#include "ctx.cuh"
+
+using namespace mpk;
+
+namespace {
+
+// genlevelset: unsigned distance to the nearest air / liquid particle in a
+// 5x5x5 cell window, minus half a cell. min over sqrt(d2) == sqrt(min d2)
+// because sqrtf is correctly rounded and monotone, so one sqrt per cell and
+// phase gives the reference's value bit for bit.
+__global__ void __launch_bounds__(256) k_genlevelset(Grid g, Cells cl, const float4* __restrict__ pos,
+                                                     float* __restrict__ lsf, float* __restrict__ lsa,
+                                                     int8_t* __restrict__ mark) {
+    MP_GRID_LOOP(idx, g.n) {
+        mark[idx] = MP_TYPEVACUUM;
+        float h = g.h;
+        float r = 0.5f * h;
+        int i, j, k; getijk3((int)idx, g.NY, g.NZ, i, j, k);
+        float3 gp = (mk3((float)i, (float)j, (float)k) + mk3(0.5f, 0.5f, 0.5f)) * h;
+        float ma2 = __int_as_float(0x7f800000), mf2 = __int_as_float(0x7f800000);
+        for (int di = -2; di <= 2; ++di) {
+            int a = i + di; if (a < 0 || a > g.NX - 1) continue;
+            for (int dj = -2; dj <= 2; ++dj) {
+                int b = j + dj; if (b < 0 || b > g.NY - 1) continue;
+                int k0 = max(k - 2, 0), k1 = min(k + 2, g.NZ - 1);
+                int c0 = cid(g, a, b, k0), c1 = cid(g, a, b, k1);
+                uint32_t s0 = __ldg(cl.off + c0), s1 = __ldg(cl.off + c1 + 1);
+                // cells of one (a,b) column are contiguous in the sorted array
+                for (uint32_t p = s0; p < s1; ++p) {
+                    float4 q = __ldg(pos + p);
+                    float3 d = mk3(q.x, q.y, q.z) - gp;
+                    float d2 = dot(d, d);
+                    int f = pflag(q);
+                    if (f == MP_TYPEAIR || f == MP_TYPEAIRSOLO) ma2 = fminf(ma2, d2);
+                    else if (f == MP_TYPEFLUID || f == MP_TYPESOLID) mf2 = fminf(mf2, d2);
+                }
+            }
+        }
+        float mair = 2.5f * h, mfl = 2.5f * h;
+        float da = sqrtf(ma2), df = sqrtf(mf2);
+        mair = (da < mair) ? da : mair;
+        mfl = (df < mfl) ? df : mfl;
+        mair -= r; mfl -= r;
+        lsf[idx] = mfl;
+        lsa[idx] = mair;
+    }
+}
+
+__device__ __forceinline__ void solvedistance(float a, float b, float c, float& x) {
+    float d = fminf(a, fminf(b, c)) + 1;
+    if (d > fmaxf(a, fmaxf(b, c)))
+        d = (a + b + c + sqrtf(3 - (a - b) * (a - b) - (a - c) * (a - c) - (b - c) * (b - c))) / 3;
+    if (d < x) x = d;
+}
+// one Jacobi pass of sweepphibytype (typeflag >= 0) or sweepphi (typeflag < 0)
+__global__ void k_sweep(Grid g, const float* __restrict__ in, float* __restrict__ out,
+                        const int8_t* __restrict__ mark, int typeflag) {
+    MP_GRID_LOOP(idx, g.n) {
+        float res = in[idx];
+        if (!(typeflag >= 0 && mark[idx] == typeflag)) {
+            int i, j, k; getijk(g, (int)idx, i, j, k);
+            #pragma unroll
+            for (int di = -1; di <= 1; di += 2)
+            #pragma unroll
+            for (int dj = -1; dj <= 1; dj += 2)
+            #pragma unroll
+            for (int dk = -1; dk <= 1; dk += 2) {
+                if (vc(g, i + di, j, k) && vc(g, i, j + dj, k) && vc(g, i, j, k + dk))
+                    solvedistance(__ldg(in + cid(g, i + di, j, k)), __ldg(in + cid(g, i, j + dj, k)),
+                                  __ldg(in + cid(g, i, j, k + dk)), res);
+            }
+        }
+        out[idx] = res;
+    }
+}
+// markLS_bigpositive (mode 0), setLSback_bigpositive (1), preparels (2), setLSback (3)
+__global__ void k_ls_prep(int n, float h, float* __restrict__ ls, int8_t* __restrict__ mark, int mode) {
+    MP_GRID_LOOP(idx, n) {
+        float v = ls[idx];
+        if (mode == 0) {
+            v = v / h;
+            if (v > 1.99f) { v = 5.0f; mark[idx] = MP_TYPEAIR; } else mark[idx] = MP_TYPEFLUID;
+        } else if (mode == 1) {
+            v = v * h;
+        } else if (mode == 2) {
+            v = -v / h;
+            if (v > 0) { v = 5.0f; mark[idx] = MP_TYPEAIR; } else mark[idx] = MP_TYPEFLUID;
+        } else {
+            v = -v * h;
+        }
+        ls[idx] = v;
+    }
+}
+__global__ void k_merge_ls(Grid g, float* __restrict__ lsm, int8_t* __restrict__ mark,
+                           const float* __restrict__ lsf, const float* __restrict__ lsa) {
+    MP_GRID_LOOP(idx, g.n) {
+        float h = g.h;
+        float lf = lsf[idx], la = lsa[idx], out;
+        int8_t m;
+        if (la > 4.99f * h) { out = lf; m = (lf > 0) ? MP_TYPEVACUUM : MP_TYPEFLUID; }
+        else if (lf > 4.99f * h) { out = la; m = (la > 0) ? MP_TYPEVACUUM : MP_TYPEAIR; }
+        else if (la > 0.8f * h && lf > 0.8f * h) { m = MP_TYPEVACUUM; out = fminf(lf, la); }
+        else { out = (lf - la) * 0.5f; m = (out > 0) ? MP_TYPEAIR : MP_TYPEFLUID; }
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        if (i == 0 || i == g.NX - 1 || j == 0 || j == g.NY - 1 || k == 0 || k == g.NZ - 1) {
+            m = MP_TYPEBOUNDARY; out = -0.5f * h;
+        }
+        mark[idx] = m;
+        lsm[idx] = out;
+    }
+}
+__global__ void k_phigra(Grid g, const float* __restrict__ ls, float* __restrict__ ax, float* __restrict__ ay,
+                         float* __restrict__ az) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        float c = ls[idx], h = g.h;
+        float x1 = vc(g, i + 1, j, k) ? ls[cid(g, i + 1, j, k)] : c;
+        float x0 = vc(g, i - 1, j, k) ? ls[cid(g, i - 1, j, k)] : c;
+        float y1 = vc(g, i, j + 1, k) ? ls[cid(g, i, j + 1, k)] : c;
+        float y0 = vc(g, i, j - 1, k) ? ls[cid(g, i, j - 1, k)] : c;
+        float z1 = vc(g, i, j, k + 1) ? ls[cid(g, i, j, k + 1)] : c;
+        float z0 = vc(g, i, j, k - 1) ? ls[cid(g, i, j, k - 1)] : c;
+        ax[idx] = ((x1 - x0) * 0.5f) / h;
+        ay[idx] = ((y1 - y0) * 0.5f) / h;
+        az[idx] = ((z1 - z0) * 0.5f) / h;
+    }
+}
+// initphi (spray_k.cu:712-722)
+__global__ void k_initphi(int n, int NX, float* __restrict__ phi, const int8_t* __restrict__ mark, int type) {
+    MP_GRID_LOOP(idx, n) phi[idx] = (mark[idx] == type) ? -0.5f : (float)(NX * 3);
+}
+
+// sweepu_k_bubble (spray_k.cu:3779-3880): one pass over all three face sets
+__global__ void k_sweepu(Grid g, const float* __restrict__ ix, const float* __restrict__ iy, const float* __restrict__ iz,
+                         float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
+                         const float* __restrict__ ls, const int8_t* __restrict__ mark, int fl) {
+    long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k;
+        if (t < g.nfx) {
+            int idx = (int)t;
+            float res = ix[idx];
+            getijk3(idx, g.NY, g.NZ, i, j, k);
+            if (i > 1 && i < g.NX - 1 && mark[cid(g, i, j, k)] != fl && mark[cid(g, i - 1, j, k)] != fl) {
+                float l0 = ls[cid(g, i, j, k)], l1 = ls[cid(g, i - 1, j, k)];
+                for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
+                    if (j + dj < 0 || j + dj > g.NY - 1 || k + dk < 0 || k + dk > g.NZ - 1) continue;
+                    float wx = (float)(-di) * (l0 - l1);
+                    if (wx < 0) continue;
+                    float wy = (l0 + l1 - ls[cid(g, i, j + dj, k)] - ls[cid(g, i - 1, j + dj, k)]) * 0.5f;
+                    if (wy < 0) continue;
+                    float wz = (l0 + l1 - ls[cid(g, i, j, k + dk)] - ls[cid(g, i - 1, j, k + dk)]) * 0.5f;
+                    if (wz < 0) continue;
+                    float ws = wx + wy + wz;
+                    if (ws == 0) wx = wy = wz = 1.0f / 3;
+                    else { wx /= ws; wy /= ws; wz /= ws; }
+                    res = wx * ix[fxi(g, i + di, j, k)] + wy * ix[fxi(g, i, j + dj, k)] + wz * ix[fxi(g, i, j, k + dk)];
+                }
+            }
+            ox[idx] = res;
+        } else if (t < (long long)g.nfx + g.nfy) {
+            int idx = (int)(t - g.nfx);
+            float res = iy[idx];
+            getijk3(idx, g.NY + 1, g.NZ, i, j, k);
+            if (j > 1 && j < g.NY - 1 && mark[cid(g, i, j, k)] != fl && mark[cid(g, i, j - 1, k)] != fl) {
+                float l0 = ls[cid(g, i, j, k)], l1 = ls[cid(g, i, j - 1, k)];
+                for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
+                    if (i + di < 0 || i + di > g.NX - 1 || k + dk < 0 || k + dk > g.NZ - 1) continue;
+                    float wy = (float)(-dj) * (l0 - l1);
+                    if (wy < 0) continue;
+                    float wx = (l0 + l1 - ls[cid(g, i + di, j, k)] - ls[cid(g, i + di, j - 1, k)]) * 0.5f;
+                    if (wx < 0) continue;
+                    float wz = (l0 + l1 - ls[cid(g, i, j, k + dk)] - ls[cid(g, i, j - 1, k + dk)]) * 0.5f;
+                    if (wz < 0) continue;
+                    float ws = wx + wy + wz;
+                    if (ws == 0) wx = wy = wz = 1.0f / 3;
+                    else { wx /= ws; wy /= ws; wz /= ws; }
+                    res = wx * iy[fyi(g, i + di, j, k)] + wy * iy[fyi(g, i, j + dj, k)] + wz * iy[fyi(g, i, j, k + dk)];
+                }
+            }
+            oy[idx] = res;
+        } else {
+            int idx = (int)(t - g.nfx - g.nfy);
+            float res = iz[idx];
+            getijk3(idx, g.NY, g.NZ + 1, i, j, k);
+            if (k > 1 && k < g.NZ - 1 && mark[cid(g, i, j, k)] != fl && mark[cid(g, i, j, k - 1)] != fl) {
+                float l0 = ls[cid(g, i, j, k)], l1 = ls[cid(g, i, j, k - 1)];
+                for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
+                    if (i + di < 0 || i + di > g.NX - 1 || j + dj < 0 || j + dj > g.NY - 1) continue;
+                    float wz = (float)(-dk) * (l0 - l1);
+                    if (wz < 0) continue;
+                    float wy = (l0 + l1 - ls[cid(g, i, j + dj, k)] - ls[cid(g, i, j + dj, k - 1)]) * 0.5f;
+                    if (wy < 0) continue;
+                    float wx = (l0 + l1 - ls[cid(g, i + di, j, k)] - ls[cid(g, i + di, j, k - 1)]) * 0.5f;
+                    if (wx < 0) continue;
+                    float ws = wx + wy + wz;
+                    if (ws == 0) wx = wy = wz = 1.0f / 3;
+                    else { wx /= ws; wy /= ws; wz /= ws; }
+                    res = wx * iz[fzi(g, i + di, j, k)] + wy * iz[fzi(g, i, j + dj, k)] + wz * iz[fzi(g, i, j, k + dk)];
+                }
+            }
+            oz[idx] = res;
+        }
+    }
+}
+
+// setWaterBoundaryU_k (spray_k.cu:956-995). Faces below the ceiling are only
+// ever zeroed, so the ceiling rule's read of the face below sees either the
+// old value (then re-applies that face's rule) or the zero it was set to.
+__device__ __forceinline__ float zrule(const Grid& g, const int8_t* mark, int i, int j, int k, float v) {
+    if (k <= 1) return 0.0f;
+    if (k > 0 && k < g.NZ && ((mark[cid(g, i, j, k)] == MP_TYPEBOUNDARY) != (mark[cid(g, i, j, k - 1)] == MP_TYPEBOUNDARY)))
+        return 0.0f;
+    return v;
+}
+__global__ void k_bound_u(Grid g, float* __restrict__ ux, float* __restrict__ uy, float* __restrict__ uz,
+                          const int8_t* __restrict__ mark) {
+    long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k;
+        if (t < g.nfx) {
+            int idx = (int)t;
+            getijk3(idx, g.NY, g.NZ, i, j, k);
+            if (i <= 1 || i >= g.NX + 1 - 2) ux[idx] = 0.0f;
+            else if (i > 1 && i < g.NX - 1 &&
+                     ((mark[cid(g, i, j, k)] == MP_TYPEBOUNDARY) != (mark[cid(g, i - 1, j, k)] == MP_TYPEBOUNDARY)))
+                ux[idx] = 0.0f;
+        } else if (t < (long long)g.nfx + g.nfy) {
+            int idx = (int)(t - g.nfx);
+            getijk3(idx, g.NY + 1, g.NZ, i, j, k);
+            if (j <= 1 || j >= g.NY + 1 - 2) uy[idx] = 0.0f;
+            else if (j > 0 && j < g.NY &&
+                     ((mark[cid(g, i, j, k)] == MP_TYPEBOUNDARY) != (mark[cid(g, i, j - 1, k)] == MP_TYPEBOUNDARY)))
+                uy[idx] = 0.0f;
+        } else {
+            int idx = (int)(t - g.nfx - g.nfy);
+            getijk3(idx, g.NY, g.NZ + 1, i, j, k);
+            if (k <= 1 || k >= g.NZ + 1 - 1) uz[idx] = 0.0f;
+            else if (k == g.NZ + 1 - 2) {
+                float below = zrule(g, mark, i, j, k - 1, uz[fzi(g, i, j, k - 1)]);
+                uz[idx] = (below < 0) ? below : 0;
+            } else if (k > 0 && k < g.NZ &&
+                       ((mark[cid(g, i, j, k)] == MP_TYPEBOUNDARY) != (mark[cid(g, i, j, k - 1)] == MP_TYPEBOUNDARY))) {
+                uz[idx] = 0.0f;
+            }
+        }
+    }
+}
+
+// markfluid_dense over the first `lim` cells (spray_k.cu:506-533) then
+// markBoundaryCell (spray_k.cu:535-545)
+__global__ void k_markfluid_dense(Grid g, Cells cl, const float4* __restrict__ pos, int8_t* __restrict__ mark, int lim) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        if (idx < lim) {
+            int cfs = 0, ca = 0;
+            for (uint32_t p = cl.off[idx]; p < cl.off[idx + 1]; ++p) {
+                int f = pflag(pos[p]);
+                if (f == MP_TYPEFLUID || f == MP_TYPESOLID) cfs++;
+                else if (f == MP_TYPEAIR) ca++;
+            }
+            mark[idx] = (cfs == 0 && ca == 0) ? MP_TYPEVACUUM : (cfs > ca ? MP_TYPEFLUID : MP_TYPEAIR);
+        }
+        if (i == 0 || i == g.NX - 1 || j == 0 || j == g.NY - 1 || k == 0 || k == g.NZ - 1) mark[idx] = MP_TYPEBOUNDARY;
+    }
+}
+
+// compsurfacetension_k (spray_k.cu:3543-3637)
+__device__ __forceinline__ float st_comp(const Grid& g, const float* gx, const float* gy, const float* gz,
+                                         int i, int j, int k, int axis, float dflt) {
+    if (!vc(g, i, j, k)) return dflt;
+    int q = cid(g, i, j, k);
+    float a = gx[q], b = gy[q], c = gz[q];
+    float l = length(mk3(a, b, c));
+    if (l == 0) return dflt;
+    float v = axis == 0 ? a : (axis == 1 ? b : c);
+    return v / l;
+}
+__global__ void k_surftension(Grid g, float* __restrict__ sf, const int8_t* __restrict__ mark, const float* __restrict__ gx,
+                              const float* __restrict__ gy, const float* __restrict__ gz, float sigma) {
+    MP_GRID_LOOP(idx, g.n) {
+        if (mark[idx] == MP_TYPEBOUNDARY) { sf[idx] = 0; continue; }
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        float3 c = mk3(gx[idx], gy[idx], gz[idx]);
+        float len = length(c), res;
+        if (len == 0) res = 0;
+        else {
+            c /= len;
+            float x1 = st_comp(g, gx, gy, gz, i + 1, j, k, 0, c.x), x0 = st_comp(g, gx, gy, gz, i - 1, j, k, 0, c.x);
+            float y1 = st_comp(g, gx, gy, gz, i, j + 1, k, 1, c.y), y0 = st_comp(g, gx, gy, gz, i, j - 1, k, 1, c.y);
+            float z1 = st_comp(g, gx, gy, gz, i, j, k + 1, 2, c.z), z0 = st_comp(g, gx, gy, gz, i, j, k - 1, 2, c.z);
+            res = (x1 - x0 + y1 - y0 + z1 - z0) / g.h * 0.5f;
+        }
+        sf[idx] = res * sigma;
+    }
+}
+
+// initSolidPhi (spray_k.cu:724-744)
+__global__ void k_init_solid_phi(Grid g, Cells cl, float* __restrict__ phi) {
+    MP_GRID_LOOP(idx, g.n) {
+        bool f = (cl.tmask[idx] >> MP_TYPESOLID) & 1;
+        phi[idx] = f ? -0.5f : (float)(3 * g.NX);
+    }
+}
+
+}  // namespace
+
+static Cells cells_of(MpCtx* c) { return Cells{c->cell_off, c->tmask}; }
+
+int k_sweep_pass_swap(MpCtx* c, float** phi, int typeflag) {
+    k_sweep<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, *phi, c->cell_tmp, c->mark, typeflag);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    std::swap(*phi, c->cell_tmp);
+    return MP_OK;
+}
+
+int k_levelset(MpCtx* c) {
+    KtScope kt(c, MP_KT_LEVELSET);
+    k_genlevelset<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, cells_of(c), c->pos, c->lsfluid, c->lsair, c->mark);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+int k_phigra(MpCtx* c, float* ax, float* ay, float* az, const float* ls) {
+    k_phigra<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, ls, ax, ay, az);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+// sweepLSAndMardGrid (spray.cu:2011-2065)
+static int sweep_ls_one(MpCtx* c, float** ls) {
+    int n = c->G.n, nb = mp_blocks(n, 256);
+    k_ls_prep<<<nb, 256, 0, c->stream>>>(n, c->G.h, *ls, c->mark, 0); c->launches++;
+    MP_CHECK_LAUNCH(c);
+    for (int it = 0; it < 5; it++) MP_TRY(k_sweep_pass_swap(c, ls, MP_TYPEFLUID));
+    k_ls_prep<<<nb, 256, 0, c->stream>>>(n, c->G.h, *ls, c->mark, 1); c->launches++;
+    k_ls_prep<<<nb, 256, 0, c->stream>>>(n, c->G.h, *ls, c->mark, 2); c->launches++;
+    MP_CHECK_LAUNCH(c);
+    for (int it = 0; it < 5; it++) MP_TRY(k_sweep_pass_swap(c, ls, MP_TYPEFLUID));
+    k_ls_prep<<<nb, 256, 0, c->stream>>>(n, c->G.h, *ls, c->mark, 3); c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+int k_sweep_ls_mark(MpCtx* c) {
+    MP_TRY(sweep_ls_one(c, &c->lsfluid));
+    MP_TRY(sweep_ls_one(c, &c->lsair));
+    k_merge_ls<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, c->lsmerge, c->mark, c->lsfluid, c->lsair);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return k_phigra(c, c->gx, c->gy, c->gz, c->lsmerge);
+}
+
+// sweepPhi (spray.cu:570-583)
+int k_sweep_phi(MpCtx* c, int phase) {
+    float** phi = (phase == MP_TYPEAIR) ? &c->phiair : &c->phifluid;
+    k_initphi<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G.n, c->G.NX, *phi, c->mark, phase);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    for (int it = 0; it < 3; it++) MP_TRY(k_sweep_pass_swap(c, phi, phase));
+    return MP_OK;
+}
+
+// sweepU (spray.cu:585-598): two double-buffered passes
+int k_sweep_u(MpCtx* c, int phase) {
+    float** u = (phase == MP_TYPEAIR) ? c->au : c->wu;
+    const float* phi = (phase == MP_TYPEAIR) ? c->phiair : c->phifluid;
+    long long tot = (long long)c->G.nfx + c->G.nfy + c->G.nfz;
+    for (int it = 0; it < 2; it++) {
+        k_sweepu<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(c->G, u[0], u[1], u[2], c->tmpu[0], c->tmpu[1], c->tmpu[2],
+                                                             phi, c->mark, phase);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        for (int a = 0; a < 3; a++) std::swap(u[a], c->tmpu[a]);
+    }
+    return MP_OK;
+}
+
+// setWaterBoundaryU (spray.cu:605-610)
+int k_set_boundary_u(MpCtx* c, int phase) {
+    float** u = (phase == MP_TYPEAIR) ? c->au : c->wu;
+    long long tot = (long long)c->G.nfx + c->G.nfy + c->G.nfz;
+    k_bound_u<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(c->G, u[0], u[1], u[2], c->mark);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+// markgrid_bubble (spray.cu:511-518): the reference launches markfluid_dense
+// with the particle grid, so only cells below ceil(np/512)*512 are marked
+int k_markgrid_bubble(MpCtx* c) {
+    int np = c->np();
+    long long lim = (long long)std::max(1, (np + 511) / 512) * 512;
+    if (lim > c->G.n) lim = c->G.n;
+    k_markfluid_dense<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, cells_of(c), c->pos, c->mark, (int)lim);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+int k_surface_tension_grid(MpCtx* c) {
+    k_surftension<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, c->sf, c->mark, c->gx, c->gy, c->gz,
+                                                                 c->P.surfacetension_sigma);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+int k_solid_phi(MpCtx* c) {
+    k_init_solid_phi<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, cells_of(c), c->phisolid);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    for (int it = 0; it < 3; it++) MP_TRY(k_sweep_pass_swap(c, &c->phisolid, -1));
+    return MP_OK;
+}

@@ -1,0 +1,312 @@
+"""Benchmark: bubblesim steps/s of the bubble-column configuration (256^3).
+
+One step = one full multiphase FLIP time step (cspray::bubblesim,
+spray.cpp:979-1233) with marching cubes every step, on ~105M particles.
+The path does not shard across GPUs (it is one coupled grid solve), so with
+N GPUs every rank runs an independent replica with its own seed ("replicas
+only"); value = N*K / max-over-ranks time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FLIP steps/s at 256³ (fwd, fwd+adjoint) at ≤1e-5 rel err; PCG HBM GB/s"
+FALLBACK_HBM_GBS = 6650.0
+# Algorithmic bytes per cell per launch of the two CG kernels (FP32 vectors,
+# int8 marks): k_cg_dir reads r, p_old, mark and writes p_new; k_cg_upd reads
+# p, x, r, mark and writes x, r.
+CG_DIR_BYTES_PER_CELL = 13
+CG_UPD_BYTES_PER_CELL = 21
+# DRAM bytes per cell per launch measured by ncu on the same kernels
+# (profiles/cg_kernels_bubble_column.md); None until captured.
+CG_DIR_TRAFFIC_PER_CELL = None
+CG_UPD_TRAFFIC_PER_CELL = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=5)
+    ap.add_argument("--n", type=int, default=0, help="grid size (0: the configuration's own, 256)")
+    ap.add_argument("--seed", type=int, default=2017005)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-n", type=int, default=64, help="grid of the bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def replica_seed(base: int, rank: int) -> int:
+    """Each rank simulates its own replica of the workload."""
+    return base + rank
+
+
+def aggregate_steps_per_s(world: int, steps: int, max_ms: float) -> float:
+    """Whole-job throughput: all ranks' steps over the slowest rank's time."""
+    return world * steps / (max_ms / 1e3)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush(); self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1])); mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(config, n_cpu, seed, steps=1, warm=1):
+    """The CPU oracle (the reference step restated, OpenMP over all host cores) on a
+    bounded sample of the workload: the same configuration on an n_cpu^3 grid."""
+    import importlib
+    mp = importlib.import_module("2017multiphase_b200")
+    from oracle import oracle as oracle_mod
+    threads = os.cpu_count() or 1
+    p = mp.scene_params(config, n_cpu)
+    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables(), threads=threads)
+    parts = mp.scene_particles(p, config, seed)
+    orc.upload_particles(**parts)
+    rf, seeds = mp.scene_tables(p, config, seed)
+    orc.set_tables(rf, seeds)
+    orc.set_field("fixedheat", mp.scene_fixed_heat(p, config))
+    for _ in range(warm):
+        orc.bubblesim()
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        orc.bubblesim()
+        times.append(time.perf_counter() - t)
+    return times, threads, len(parts["flag"])
+
+
+def run_reference(args, rank):
+    n_full = args.n or 256
+    if rank != 0:
+        return
+    times, threads, npart = cpu_sample(args.config, args.cpu_n, args.seed, steps=args.steps, warm=args.warmup)
+    scale = (n_full / args.cpu_n) ** 3
+    per_step = sum(times) / len(times) * scale
+    value = 1.0 / per_step
+    sample = (f"oracle step of the same configuration on a {args.cpu_n}^3 grid ({npart} particles), "
+              f"time scaled by the cell ratio ({scale:.0f}x) to {n_full}^3")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": f"bubble column {n_full}^3 (CPU oracle sample)", "grid": n_full},
+           "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import importlib
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    mp = importlib.import_module("2017multiphase_b200")
+
+    sim = mp.Sim.from_config(args.config, args.n, replica_seed(args.seed, rank))
+    p = sim.params
+    n = p.nx * p.ny * p.nz
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    for _ in range(args.warmup):
+        sim.bubblesim()
+    torch.cuda.synchronize()
+
+    classes = [mp.KT_CG_STENCIL, mp.KT_CG_UPDATE, mp.KT_P2G, mp.KT_G2P, mp.KT_SORT, mp.KT_LEVELSET, mp.KT_MC_DENS]
+    sim.kernel_timing_reset()
+    for k in classes:
+        sim.kernel_timing(k, True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    cg_iters = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sim.bubblesim()
+        cg_iters += sim.state().last_cg_iters
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = sim.launch_count()
+    kt = {k: sim.kernel_timing_read(k) for k in classes}
+    for k in classes:
+        sim.kernel_timing(k, False)
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = aggregate_steps_per_s(world, args.steps, t_max)
+
+    # end to end through the public API with host buffers: the step's host
+    # inputs (random table and nucleation cells) go up, the extracted meshes
+    # come back, every step
+    rf, seeds = mp.scene_tables(p, args.config, replica_seed(args.seed, rank))
+    rf_pin = torch.empty(rf.size, dtype=torch.float32, pin_memory=True).numpy(); rf_pin[:] = rf
+    sd_pin = torch.empty(max(seeds.size, 1), dtype=torch.int32, pin_memory=True).numpy()[:seeds.size]; sd_pin[:] = seeds
+    cap_v = p.mc_max_verts; cap_i = 3 * p.mc_max_tris
+    vbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
+    nbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
+    ibuf = torch.empty(cap_i, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    import ctypes as C
+    h2d = rf_pin.nbytes + sd_pin.nbytes
+    d2h = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        sim.set_tables(rf_pin, sd_pin)
+        sim.bubblesim()
+        st = sim.state()
+        for s in range(3):
+            nv, ni = st.mc_verts[s], st.mc_indices[s]
+            rc = sim.lib.mp_mc_download(sim.ctx, s, vbuf.ctypes.data_as(C.c_void_p), nbuf.ctypes.data_as(C.c_void_p),
+                                        ibuf.ctypes.data_as(C.c_void_p), cap_v, cap_i)
+            if rc:
+                raise RuntimeError(f"mesh download failed {rc}")
+            d2h += 24 * nv + 4 * ni
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h / max(args.e2e_steps, 1))}
+
+    # roofline of the dominant kernel class (by device time in the timed region)
+    peak, peak_kind = peaks()
+    dom = max([mp.KT_CG_STENCIL, mp.KT_CG_UPDATE], key=lambda k: kt[k][0])
+    bpc = CG_DIR_BYTES_PER_CELL if dom == mp.KT_CG_STENCIL else CG_UPD_BYTES_PER_CELL
+    tpc = CG_DIR_TRAFFIC_PER_CELL if dom == mp.KT_CG_STENCIL else CG_UPD_TRAFFIC_PER_CELL
+    ms_k, nl = kt[dom]
+    per_launch_s = ms_k / 1e3 / max(nl, 1)
+    achieved = bpc * n / per_launch_s / 1e9
+    cg_ms = kt[mp.KT_CG_STENCIL][0] + kt[mp.KT_CG_UPDATE][0]
+    cg_launch_pairs = max(kt[mp.KT_CG_STENCIL][1], 1)
+    pcg_gbs = (CG_DIR_BYTES_PER_CELL + CG_UPD_BYTES_PER_CELL) * n * cg_launch_pairs / (cg_ms / 1e3) / 1e9
+    names = {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g_faces",
+             mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
+    roof = {"kernel": names[dom], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "traffic": (tpc * n if tpc else None), "algorithmic_bytes_per_launch": bpc * n,
+            "avg_launch_ms": per_launch_s * 1e3}
+
+    st = sim.state()
+    out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (CG dots, alpha/beta in f64)", "data": "synthetic",
+           "config": {"workload": f"bubble column {p.nx}^3: liquid z<0.8, 200 air bubbles r~U[0.01,0.04], "
+                                  f"8 jittered particles/cell, dt=1/240, FLIP 0.95, CG rel 1e-6 (FP32 vectors, "
+                                  f"FP64 dots), marching cubes every step",
+                      "grid": p.nx, "particles": int(st.par_num_now), "seed": args.seed,
+                      "l2": "inputs larger than L2 (particle streams alone are ~5 GB)",
+                      "parallelism": f"replicas x{world}"},
+           "roofline": roof, "pcg_hbm_gbs": pcg_gbs,
+           "cg_iters_per_step": cg_iters / max(args.steps, 1),
+           "kernel_ms": {names[k]: {"ms": kt[k][0], "launches": kt[k][1]} for k in classes},
+           "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            times, threads, npart = cpu_sample(args.config, args.cpu_n, args.seed)
+            scale = (p.nx / args.cpu_n) ** 3
+            out["cpu_baseline"] = {"value": 1.0 / (times[0] * scale), "unit": "steps/s", "cores": threads,
+                                   "kind": "port",
+                                   "sample": f"one oracle step of the same configuration on a {args.cpu_n}^3 grid "
+                                             f"({npart} particles, {times[0]:.2f} s), scaled by the cell ratio "
+                                             f"{scale:.0f}x to {p.nx}^3"}
+        except Exception as e:   # the baseline is reported, not required
+            out["cpu_baseline"] = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                                   "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    sim.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,337 @@
+/*
+ * mp.h — C ABI of the B200 multiphase FLIP step.
+ *
+ * One entry point per stage method of the reference's `cspray` class
+ * (Multiphase/Multiphase/spray.h:18-389), plus the full time step
+ * (`cspray::bubblesim`, spray.cpp:979-1233). Plain C types only: host
+ * pointers and sizes, an opaque context, `int` status codes.
+ *
+ * Layouts follow the reference:
+ *   cells  idx = i*NY*NZ + j*NZ + k                    (utility.h:55-58)
+ *   x-faces (NX+1)*NY*NZ, y-faces NX*(NY+1)*NZ, z-faces NX*NY*(NZ+1)
+ *   particles as structure-of-arrays: pos float3, vel float3, flag int8,
+ *   mass, temperature, latent heat, solubility, gas content (float each)
+ *                                                      (spray.h:165-170,278)
+ * Particle and cell type codes are the reference's TYPE* values
+ * (utility.h:13-19).
+ *
+ * Error convention (replaces getLastCudaError/exit and `mpause`):
+ * every function returns MP_OK or one MP_ERR_* code; mp_last_error()
+ * gives the message. Nothing calls exit().
+ *
+ * Threading: one context per host thread; all device work of a context is
+ * ordered on its stream (mp_set_stream). Entry points return after the
+ * work is enqueued unless stated; functions that hand data to the host
+ * synchronise the stream.
+ */
+#ifndef MP_H
+#define MP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define MP_OK              0
+#define MP_ERR_CUDA        1   /* a CUDA runtime call failed                 */
+#define MP_ERR_CAPACITY    2   /* par_num_max or a marching-cubes cap hit    */
+#define MP_ERR_NOCONVERGE  3   /* CG stopped at its iteration limit          */
+#define MP_ERR_TIMEOUT     4   /* a bounded device-side wait gave up         */
+#define MP_ERR_ARG         5   /* bad argument (null, size, id)              */
+#define MP_ERR_STATE       6   /* call not valid in the current state        */
+
+/* ---- particle / cell types (utility.h:13-19) ------------------------- */
+#define MP_TYPEFLUID    0
+#define MP_TYPEAIR      1
+#define MP_TYPEBOUNDARY 2
+#define MP_TYPEVACUUM   3
+#define MP_TYPEAIRSOLO  4
+#define MP_TYPESOLID    5
+#define MP_TYPECNT      6
+#define MP_CELL_UNDEF   0xffffffffu   /* empty cell marker (utility.h:22) */
+
+/* ---- scenes (utility.h:114-131); only the branches the step takes ---- */
+#define MP_SCENE_FLUIDSPHERE            0
+#define MP_SCENE_SMOKE                  1
+#define MP_SCENE_BOILING                2
+#define MP_SCENE_BOILING_HIGHRES        3
+#define MP_SCENE_MULTIBUBBLE            4
+#define MP_SCENE_DAMBREAK               5
+#define MP_SCENE_MELTING                6
+#define MP_SCENE_MELTINGPOUR            7
+#define MP_SCENE_FREEZING               8
+#define MP_SCENE_INTERACTION            9
+#define MP_SCENE_INTERACTION_HIGHRES   10
+#define MP_SCENE_MELTANDBOIL           11
+#define MP_SCENE_MELTANDBOIL_HIGHRES   12
+#define MP_SCENE_HEATTRANSFER          13
+#define MP_SCENE_ALL                   15
+
+/* ---- solver modes ----------------------------------------------------- */
+#define MP_TOL_REF_ABS   0   /* stop when r.r < cg_tol*n  (spray.cu:1619,1666) */
+#define MP_TOL_REL       1   /* stop when |r| <= cg_tol*|b|                    */
+#define MP_PREC_MIXED    0   /* FP32 vectors, FP64 dots/alpha/beta            */
+#define MP_PREC_FP64     1   /* divergence, CG and gradient in FP64           */
+#define MP_COEF_REF      0   /* constant-coefficient Laplacian (reference)    */
+#define MP_COEF_GFM      1   /* variable density, ghost-fluid face weights    */
+
+#define MP_PARAMS_VERSION 3
+
+/*
+ * Runtime parameters: the reference's FlipConstant (utility.h:26-46), the
+ * per-scene members set by cspray::initparam (spray.cpp:23-626) and the
+ * solver switches this implementation adds. All fields are 4 bytes.
+ * Fill with mp_params_default(), then edit.
+ */
+typedef struct mp_params {
+    int32_t version;
+    int32_t nx, ny, nz;              /* grid (spray.h:14, now runtime)        */
+    int32_t par_num_max;             /* particle capacity (spray.h:170)       */
+    int32_t scene;                   /* MP_SCENE_* (spray.h:191)              */
+    float   cellsize;                /* hparam.cellsize.x                     */
+    float   dt;                      /* hparam.dt                             */
+    float   gravity_x, gravity_y, gravity_z;
+    float   gmin_x, gmin_y, gmin_z;  /* domain origin (hparam.gmin)           */
+    float   samplespace;             /* hparam.samplespace                    */
+    float   m0, airm0, waterrho, solidrho, pradius;
+    float   poly6kern, spikykern, lapkern;
+    /* scene switches (spray.h:344-358) */
+    int32_t b_solid, b_melt, b_freeze, b_fix_solid, b_gen_gas, b_heat_trans;
+    int32_t b_add_heat_bottom, b_extend_heat_to_boundary, b_correct_position;
+    int32_t b_smooth_mc, b_run_mc;
+    int32_t mc_every;                /* outputframeDelta                      */
+    int32_t smooth_iters;            /* smoothIterTimes                       */
+    /* scene constants (spray.h:275-293, spray.cpp:31-78) */
+    float   surfacetension_sigma;
+    float   heatalpha_fluid, heatalpha_air, heatalpha_solid, heatalpha_vacuum;
+    float   default_temperature, temperature0, melting_point, boiling_point;
+    float   drag_param_solo, drag_param_grid, viscosity_sph;
+    float   default_solid_T, default_liquid_T, liquid_heat_th, alpha_temp_trans;
+    float   bounce_vel_param, bounce_pos_param, heat_increase_bottom;
+    float   bubble_max_vel, max_vel_for_bubble;
+    float   buoyance_rate_air, buoyance_rate_solo;
+    float   vapor_gen_rate, init_dissolve_gas_rate, init_gas_rate;
+    float   correction_spring, correction_radius;
+    float   mc_density;              /* fMCDensity                            */
+    float   heat_clamp;              /* 378.0 in addHeatAtBottom (spray_k.cu:4502) */
+    float   solubility_coef;         /* 1018.9 in updatesolubility (spray_k.cu:4725) */
+    float   solid_bounce_param;      /* SolidbounceParam                      */
+    /* solver switches (new) */
+    float   flip_alpha;              /* 1.0 = pure FLIP as bubblesim ships    */
+    int32_t cg_tol_mode;             /* MP_TOL_*                              */
+    float   cg_tol;                  /* 0.01 (ref_abs) or 1e-6 (rel)          */
+    int32_t cg_max_iter;             /* 800 (spray.cu:1642)                   */
+    int32_t heat_cg_max_iter;        /* 3800 (spray.cu:1804)                  */
+    int32_t cg_true_residual_every;  /* recompute r = b - A x every k its     */
+    int32_t precision;               /* MP_PREC_*                             */
+    int32_t coef_mode;               /* MP_COEF_*                             */
+    float   density_ratio;           /* rho_liquid / rho_air for MP_COEF_GFM  */
+    int32_t mc_max_verts, mc_max_tris;
+    int32_t seed_redraw;             /* 1: updateSeedCell cadence is on       */
+    int32_t update_seed_frame_delta;
+    /* 1: cells whose MP_F_FIXEDHEAT value is not MP_UNDEF_TEMPERATURE are held
+     * at it, the reference's dormant Dirichlet path (compb_heat,
+     * spray_k.cu:4515-4519, updateFixedHeat spray_k.cu:4478) */
+    int32_t b_fixed_heat;
+    int32_t reserved[7];
+} mp_params;
+
+#define MP_UNDEF_TEMPERATURE (-10000.0f)   /* utility.h:24 */
+
+/* Field identifiers for mp_get_field / mp_set_field. */
+enum mp_field {
+    /* cell fields, float[n] */
+    MP_F_PRESS = 0, MP_F_DIV, MP_F_LSFLUID, MP_F_LSAIR, MP_F_LSMERGE,
+    MP_F_PHIFLUID, MP_F_PHIAIR, MP_F_PHISOLID,
+    MP_F_PHIGRAX, MP_F_PHIGRAY, MP_F_PHIGRAZ,
+    MP_F_PHIGRAX_AIR, MP_F_PHIGRAY_AIR, MP_F_PHIGRAZ_AIR,
+    MP_F_SURFTENSION, MP_F_TP, MP_F_TP_SAVE, MP_F_TP_OLD, MP_F_FIXEDHEAT,
+    /* cell marks, int8[n] */
+    MP_F_MARK,
+    /* face fields, float[(nx+1)ny nz] / [nx(ny+1)nz] / [nx ny(nz+1)] */
+    MP_F_WATERUX, MP_F_WATERUY, MP_F_WATERUZ,
+    MP_F_WATERUX_OLD, MP_F_WATERUY_OLD, MP_F_WATERUZ_OLD,
+    MP_F_AIRUX, MP_F_AIRUY, MP_F_AIRUZ,
+    MP_F_AIRUX_OLD, MP_F_AIRUY_OLD, MP_F_AIRUZ_OLD,
+    MP_F_SOLIDUX, MP_F_SOLIDUY, MP_F_SOLIDUZ,
+    /* cell ranges of the last particle sort, uint32[n] (read only) */
+    MP_F_CELLSTART, MP_F_CELLEND,
+    /* particle attributes, [par_num_now] */
+    MP_P_POS,        /* float[3*np] */
+    MP_P_VEL,        /* float[3*np] */
+    MP_P_FLAG,       /* int8[np]    */
+    MP_P_MASS, MP_P_TEMP, MP_P_LHEAT, MP_P_SOLUBILITY, MP_P_GASCONTAIN,
+    MP_FIELD_COUNT
+};
+
+/* Step-level scalars carried between stages. */
+typedef struct mp_state {
+    int32_t frame;            /* mframe                                        */
+    int32_t par_num_now;      /* parNumNow                                     */
+    int32_t n_real_solpoint;  /* nRealSolpoint                                 */
+    int32_t last_cg_iters;    /* pressure CG iterations of the last projection */
+    double  last_cg_residual; /* its final r.r                                 */
+    int32_t last_heat_cg_iters;
+    double  last_heat_cg_residual;
+    int32_t mc_verts[3];      /* last marching-cubes vertex counts per surface */
+    int32_t mc_indices[3];    /* last index counts (3 per triangle)            */
+    int32_t mc_active_voxels[3];
+    int32_t reserved[6];
+} mp_state;
+
+/* Marching-cubes surfaces, in the order bubblesim extracts them
+ * (spray.cpp:1192-1201). */
+#define MP_MC_SOLID 0
+#define MP_MC_FLUID 1
+#define MP_MC_GAS   2
+
+/* Kernel classes whose launches can be timed with CUDA events. */
+#define MP_KT_CG_STENCIL   0   /* pressure CG: A p and p.Ap                */
+#define MP_KT_CG_UPDATE    1   /* pressure CG: x, r update and r.r          */
+#define MP_KT_P2G          2   /* water + air particle-to-grid gather       */
+#define MP_KT_G2P          3   /* FLIP grid-to-particle                     */
+#define MP_KT_SORT         4   /* hash + counting sort + reorder            */
+#define MP_KT_LEVELSET     5   /* genlevelset                               */
+#define MP_KT_MC_DENS      6   /* marching-cubes density field              */
+#define MP_KT_COUNT        7
+
+/* ---- parameters ------------------------------------------------------- */
+
+/* Defaults of the reference (spray.cpp:29-78, 573-626) for a grid of
+ * nx,ny,nz cells with cellsize 1/64, scene MULTIBUBBLE. */
+int mp_params_default(mp_params* p, int nx, int ny, int nz, int par_num_max);
+/* Recompute the derived constants m0, airm0, pradius, *kern from
+ * cellsize/samplespace/waterrho exactly as initparam does (spray.cpp:573-588). */
+int mp_params_derive(mp_params* p);
+/* Field table of mp_params for bindings: name, byte offset, kind (0 int32, 1 float). */
+int mp_params_describe(int index, const char** name, int* offset, int* kind);
+int mp_params_size(void);
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Allocates every device buffer (replaces cspray::initmem_bubble,
+ * spray.cu:25-218, and initMC, spray.cu:709-757). */
+int mp_create(const mp_params* p, void** ctx);
+int mp_destroy(void* ctx);
+int mp_set_params(void* ctx, const mp_params* p);
+int mp_get_params(void* ctx, mp_params* p);
+int mp_get_state(void* ctx, mp_state* s);
+int mp_set_state(void* ctx, const mp_state* s);
+int mp_last_error(void* ctx, char* buf, size_t len);
+/* Stream the context enqueues on (a cudaStream_t passed as a pointer). */
+int mp_set_stream(void* ctx, void* stream);
+int mp_get_stream(void* ctx, void** stream);
+int mp_synchronize(void* ctx);
+/* Device id the context was created on. */
+int mp_get_device(void* ctx, int* device);
+
+/* ---- data in / out ---------------------------------------------------- */
+
+/* Copies n particles from HOST arrays (structure of arrays as in the
+ * reference; any of T/L/sol/gas may be NULL = zero). Sets par_num_now.
+ * Replaces the H2D copies of initparticle_solidCoupling (spray.cu:465-470). */
+int mp_upload_particles(void* ctx, int n, const float* pos3, const float* vel3,
+                        const int8_t* flag, const float* mass, const float* temp,
+                        const float* lheat, const float* solubility,
+                        const float* gascontain);
+int mp_download_particles(void* ctx, int* n, float* pos3, float* vel3,
+                          int8_t* flag, float* mass, float* temp, float* lheat,
+                          float* solubility, float* gascontain);
+/* Element count and element size of a field (particle fields: per current np). */
+int mp_field_info(void* ctx, int field, size_t* count, size_t* elem_bytes);
+int mp_get_field(void* ctx, int field, void* host_dst, size_t bytes);
+int mp_set_field(void* ctx, int field, const void* host_src, size_t bytes);
+/* The random table (spray.cu:180-190) and nucleation seed cells
+ * (spray.cu:2907-2933) are inputs, so every implementation sees the same. */
+int mp_set_tables(void* ctx, const float* randfloat, int nrand,
+                  const int32_t* seedcells, int nseed);
+/* Marching-cubes case tables this build uses (numVerts[256], tri[256*16],
+ * edge[256]); generated, not copied (see mc_tables.cpp). */
+int mp_mc_tables(int32_t* num_verts, int32_t* tri, int32_t* edge);
+
+/* ---- scene set-up (cspray::init, spray.cpp:628-670) -------------------- */
+
+/* Parameters of benchmark configuration `config` (1..5: rising bubble 32^3,
+ * pool boiling 64^3, melting/freezing 128^3, dam break 64^3, bubble column
+ * 256^3) on an n^3 grid (n = 0: the configuration's own size). Replaces the
+ * per-scene branches of cspray::initparam (spray.cpp:83-547). */
+int mp_scene_params(int config, int n, mp_params* p);
+/* Seeds the configuration's particles (cspray::initparticle_solidCoupling,
+ * spray.cu:395-484, with jittered 2x2x2 sub-cell sampling): writes up to cap
+ * particles into the host arrays and their count into *n; with pos3 == NULL
+ * only counts. Temperatures, latent heat, solubility and gas content follow
+ * initTemperature/initSolubility (spray.cu:1989-1999) with the
+ * configuration's per-particle noise. */
+int mp_scene_particles(const mp_params* p, int config, uint64_t seed, int cap, int* n,
+                       float* pos3, float* vel3, int8_t* flag, float* mass, float* temp,
+                       float* lheat, float* solubility, float* gascontain);
+/* Random table (nrand uniforms in [0,1)) and nucleation seed cells of the
+ * configuration; *nseed is set to the number written (at most maxseed). */
+int mp_scene_tables(const mp_params* p, int config, uint64_t seed, float* randfloat, int nrand,
+                    int32_t* seeds, int maxseed, int* nseed);
+/* Fixed-temperature plate of the configuration (MP_F_FIXEDHEAT, n floats). */
+int mp_scene_fixed_heat(const mp_params* p, int config, float* fixedheat);
+
+/* initTemperature + initSolubility (spray.cu:1989-1999) on the uploaded
+ * particles; sets n_real_solpoint to the number of SOLID particles. */
+int mp_init_particle_heat(void* ctx);
+
+/* ---- stages, one per cspray method (spray.h:21-337) -------------------- */
+
+int mp_hash_sort(void* ctx);                 /* hashAndSortParticles  spray.cu:614  */
+int mp_external_force(void* ctx);            /* addexternalforce      spray.cu:376  */
+int mp_levelset(void* ctx, float offset);    /* computeLevelset       spray.cu:1465 */
+int mp_sweep_ls_mark(void* ctx);             /* sweepLSAndMardGrid    spray.cu:2011 */
+int mp_mark_solo_air(void* ctx);             /* markSoloAirParticle   spray.cu:2614 */
+int mp_surface_tension(void* ctx);           /* computesurfacetension spray.cu:2001 */
+int mp_markgrid_bubble(void* ctx);           /* markgrid_bubble       spray.cu:511  */
+int mp_p2g(void* ctx);                       /* mapvelp2g_bubble      spray.cu:1562 */
+int mp_drag(void* ctx);                      /* enforceDragForce      spray.cu:2953 */
+int mp_sweep_phi(void* ctx, int phase);      /* sweepPhi  (phase = MP_TYPEFLUID|MP_TYPEAIR) spray.cu:570 */
+int mp_sweep_u(void* ctx, int phase);        /* sweepU                spray.cu:585  */
+int mp_set_boundary_u(void* ctx, int phase); /* setWaterBoundaryU     spray.cu:605  */
+int mp_project(void* ctx, int* iters, double* residual); /* project_CG_bubble spray.cu:1590 */
+int mp_g2p(void* ctx);                       /* mapvelg2p_bubble      spray.cu:1689 */
+int mp_solid_motion(void* ctx);              /* solidmotion[_fixed]   spray.cu:2685 */
+int mp_solo_air_update(void* ctx);           /* updateSoloAirParticle spray.cu:2620 */
+int mp_collide_advect(void* ctx);            /* CollisionSolid        spray.cu:2959 */
+int mp_correct_pos(void* ctx);               /* correctpos            spray.cu:328  */
+int mp_correct_pos_bubble(void* ctx);        /* correctpos_bubble     spray.cu:2067 */
+int mp_heat(void* ctx);                      /* updateTemperature     spray.cu:1889 */
+int mp_gen_gas(void* ctx);                   /* GenerateGasParticle   spray.cu:2653 */
+int mp_delete(void* ctx);                    /* deleteAirFluidParticle spray.cu:2194 */
+int mp_melt(void* ctx);                      /* MeltSolid             spray.cu:2816 */
+int mp_freeze(void* ctx);                    /* Freezing              spray.cu:2860 */
+/* preMC + one runMC_smooth surface (spray.cu:759-979); the 2x re-sort is
+ * done by mp_mc_presort (hashAndSortParticles_MC, spray.cu:639). */
+int mp_mc_presort(void* ctx);
+int mp_mc(void* ctx, int surface);
+/* Vertex positions (float3), normals (float3) and uint32 indices of the
+ * last extraction of `surface`; counts from mp_state. */
+int mp_mc_download(void* ctx, int surface, float* verts, float* normals,
+                   uint32_t* indices, int max_verts, int max_indices);
+/* MC density field (float[(2nx+1)(2ny+1)(2nz+1)]) and per-voxel case index
+ * (uint8[8n]) of the last extraction. */
+int mp_mc_download_field(void* ctx, float* dens, uint8_t* cubeindex);
+
+/* The whole bubblesim step in the reference's order and cadence
+ * (spray.cpp:979-1233). Synchronous at exit. */
+int mp_step(void* ctx);
+
+/* ---- measurement -------------------------------------------------------- */
+
+/* Record CUDA events around every launch of a kernel class on the context
+ * stream; read back the summed device time (ms) and the launch count. */
+int mp_kernel_timing(void* ctx, int kernel_class, int enable);
+int mp_kernel_timing_read(void* ctx, int kernel_class, double* ms, int64_t* launches);
+int mp_kernel_timing_reset(void* ctx);
+/* Number of this library's kernel launches since the last reset. */
+int64_t mp_launch_count(void* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MP_H */

@@ -1,0 +1,81 @@
+/*
+ * oracle.h — TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the reference's multiphase FLIP step
+ * (gaoyangVR/2017Multiphase, Multiphase/Multiphase/spray.cpp:979-1233 and
+ * the kernels of spray_k.cu it launches). It is the checker for the CUDA
+ * path: only tests/, __graft_entry__.smoke() and bench.py's CPU baseline
+ * may load it. Nothing in the product links or calls it.
+ *
+ * Parity status: the reference cannot be compiled or run here (Windows,
+ * GL, CUDA texture references removed in CUDA 12, missing CUDA-samples
+ * headers), and it ships no tests, golden vectors or fixtures. The only
+ * known-answer data it contains is the marching-cubes edge table, which
+ * the tests check against. Everything else in this file is "parity
+ * unpinned": it restates the reference's arithmetic, operation by
+ * operation, with the deterministic semantics listed in DESIGN.md where
+ * the reference races (in-place sweeps, float atomics, atomic appends).
+ *
+ * Build: g++ -O2 -fopenmp -ffp-contract=off (see oracle/Makefile).
+ */
+#ifndef MP_ORACLE_H
+#define MP_ORACLE_H
+#include <stdint.h>
+#include <stddef.h>
+#include "../include/mp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int  or_create(const mp_params* p, void** out);
+void or_destroy(void* o);
+int  or_set_params(void* o, const mp_params* p);
+int  or_get_state(void* o, mp_state* s);
+int  or_set_state(void* o, const mp_state* s);
+int  or_upload_particles(void* o, int n, const float* pos3, const float* vel3,
+                         const int8_t* flag, const float* mass, const float* temp,
+                         const float* lheat, const float* sol, const float* gas);
+int  or_field_info(void* o, int field, size_t* count, size_t* elem_bytes);
+int  or_get_field(void* o, int field, void* dst, size_t bytes);
+int  or_set_field(void* o, int field, const void* src, size_t bytes);
+int  or_set_tables(void* o, const float* randfloat, int nrand, const int32_t* seeds, int nseed);
+int  or_set_mc_tables(void* o, const int32_t* num_verts, const int32_t* tri);
+int  or_init_particle_heat(void* o);
+
+int or_hash_sort(void* o);
+int or_external_force(void* o);
+int or_levelset(void* o, float offset);
+int or_sweep_ls_mark(void* o);
+int or_mark_solo_air(void* o);
+int or_surface_tension(void* o);
+int or_markgrid_bubble(void* o);
+int or_p2g(void* o);
+int or_drag(void* o);
+int or_sweep_phi(void* o, int phase);
+int or_sweep_u(void* o, int phase);
+int or_set_boundary_u(void* o, int phase);
+int or_project(void* o, int* iters, double* residual);
+int or_g2p(void* o);
+int or_solid_motion(void* o);
+int or_solo_air_update(void* o);
+int or_collide_advect(void* o);
+int or_correct_pos(void* o);
+int or_correct_pos_bubble(void* o);
+int or_heat(void* o);
+int or_gen_gas(void* o);
+int or_delete(void* o);
+int or_melt(void* o);
+int or_freeze(void* o);
+int or_mc_presort(void* o);
+int or_mc(void* o, int surface);
+int or_mc_get(void* o, int surface, float* verts, float* normals, uint32_t* indices,
+              int max_verts, int max_indices);
+int or_mc_get_field(void* o, float* dens, uint8_t* cubeindex);
+int or_step(void* o);
+void or_set_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

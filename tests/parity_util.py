@@ -1,0 +1,114 @@
+"""Helpers for GPU-vs-oracle parity: the same scene on both sides, state transplant
+(GPU state copied into the oracle so one stage can be checked in isolation), and
+field comparison."""
+import numpy as np
+
+CELL_FIELDS = ["press", "div", "lsfluid", "lsair", "lsmerge", "phifluid", "phiair", "phisolid",
+               "phigrax", "phigray", "phigraz", "phigrax_air", "phigray_air", "phigraz_air",
+               "surftension", "tp", "tp_save", "tp_old", "fixedheat", "mark"]
+FACE_FIELDS = ["waterux", "wateruy", "wateruz", "waterux_old", "wateruy_old", "wateruz_old",
+               "airux", "airuy", "airuz", "airux_old", "airuy_old", "airuz_old",
+               "solidux", "soliduy", "soliduz"]
+PART_FIELDS = ["pos", "vel", "flag", "mass", "temp", "lheat", "solubility", "gascontain"]
+
+
+def bubblesim_stages(p, frame):
+    """The stage sequence of one bubblesim step (spray.cpp:979-1233) for params p."""
+    s = [("hashAndSortParticles",), ("addexternalforce",), ("computeLevelset", 0.0), ("sweepLSAndMardGrid",),
+         ("markSoloAirParticle",), ("computesurfacetension",)]
+    if p.scene in (6, 8):   # MELTING, FREEZING
+        s.append(("markgrid_bubble",))
+    s += [("mapvelp2g_bubble",), ("enforceDragForce",), ("sweepPhi", 1), ("sweepU", 1), ("sweepPhi", 0), ("sweepU", 0),
+          ("setWaterBoundaryU", 1), ("setWaterBoundaryU", 0), ("project_CG_bubble",), ("sweepU", 1), ("sweepU", 0),
+          ("setWaterBoundaryU", 1), ("setWaterBoundaryU", 0), ("mapvelg2p_bubble",), ("solidmotion",),
+          ("updateSoloAirParticle",), ("hashAndSortParticles",), ("CollisionSolid",)]
+    if p.b_correct_position:
+        s += [("hashAndSortParticles",), ("correctpos",), ("hashAndSortParticles",), ("computeLevelset", 0.15),
+              ("sweepLSAndMardGrid",), ("correctpos_bubble",)]
+    else:
+        s += [("hashAndSortParticles",), ("computeLevelset", 0.15), ("sweepLSAndMardGrid",)]
+    s.append(("hashAndSortParticles",))
+    if p.b_heat_trans:
+        s.append(("updateTemperature",))
+    if p.b_gen_gas and frame % 2 == 0:
+        s.append(("GenerateGasParticle",))
+    s += [("hashAndSortParticles",), ("deleteAirFluidParticle",), ("hashAndSortParticles",)]
+    if p.b_melt:
+        s.append(("MeltSolid",))
+    if p.b_freeze:
+        s.append(("Freezing",))
+    return s
+
+
+def make_pair(mp, oracle_mod, config, n, seed, **overrides):
+    """A GPU Sim and an oracle with identical parameters, particles and tables."""
+    p = mp.scene_params(config, n)
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    sim = mp.Sim.from_config(config, n, seed, params=p)
+    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    parts = mp.scene_particles(p, config, seed)
+    orc.upload_particles(**parts)
+    rf, seeds = mp.scene_tables(p, config, seed)
+    orc.set_tables(rf, seeds)
+    orc.set_field("fixedheat", mp.scene_fixed_heat(p, config))
+    orc.set_state(sim.state())
+    return sim, orc
+
+
+def transplant(sim, orc, with_cells=True):
+    """Copies the complete GPU state into the oracle."""
+    for f in CELL_FIELDS + FACE_FIELDS:
+        orc.set_field(f, sim.get_field(f))
+    parts = sim.download_particles()
+    st = sim.state()
+    orc.set_state(st)
+    orc.upload_particles(**parts)
+    if with_cells:
+        orc.set_field("cellstart", sim.get_field("cellstart"))
+        orc.set_field("cellend", sim.get_field("cellend"))
+
+
+def snapshot(obj):
+    out = {f: obj.get_field(f) for f in CELL_FIELDS + FACE_FIELDS}
+    out.update(obj.download_particles())
+    return out
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64); b = np.asarray(b, np.float64)
+    if a.shape != b.shape:
+        return np.inf
+    if a.size == 0:
+        return 0.0
+    fin = np.isfinite(b) & np.isfinite(a)
+    if not np.array_equal(np.isfinite(a), np.isfinite(b)):
+        return np.inf
+    scale = max(np.abs(b[fin]).max() if fin.any() else 0.0, 1e-30)
+    return float(np.abs(a[fin] - b[fin]).max() / scale) if fin.any() else 0.0
+
+
+def compare(gpu, ref, exact=True, rtol=1e-5, skip=()):
+    """Returns a list of (field, problem) for fields that differ."""
+    bad = []
+    for k, v in ref.items():
+        if k in skip:
+            continue
+        g = gpu[k]
+        if np.asarray(g).shape != np.asarray(v).shape:
+            bad.append((k, f"shape {np.asarray(g).shape} vs {np.asarray(v).shape}"))
+            continue
+        if exact or v.dtype.kind in "iu":
+            same = np.array_equal(g, v, equal_nan=v.dtype.kind == "f")
+            if not same:
+                if v.dtype.kind == "f":
+                    d = np.abs(g.astype(np.float64) - v.astype(np.float64))
+                    bad.append((k, f"not bit-exact: {int((g != v).sum())} differ, max |d| {np.nanmax(d):.3e}, "
+                                   f"rel {rel_err(g, v):.3e}"))
+                else:
+                    bad.append((k, f"not equal: {int((g != v).sum())} of {v.size} differ"))
+        else:
+            e = rel_err(g, v)
+            if e > rtol:
+                bad.append((k, f"rel err {e:.3e} > {rtol}"))
+    return bad

