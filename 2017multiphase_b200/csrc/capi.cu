@@ -105,7 +105,7 @@ extern "C" int mp_params_default(mp_params* p, int nx, int ny, int nz, int par_n
     p->precision = MP_PREC_MIXED; p->coef_mode = MP_COEF_REF; p->density_ratio = 1000.0f;
     // the reference fixes 6e6 vertices / 12e6 triangles (spray.cu:721-722); here the
     // caps scale with the 2x grid's cross-section (a few surface layers)
-    long long mv = std::max(100000LL, 24LL * (2 * nx) * (2 * ny));
+    long long mv = std::max(100000LL, 64LL * (2 * nx) * (2 * ny));
     mv = std::min(mv, 64000000LL);
     p->mc_max_verts = (int)mv; p->mc_max_tris = (int)std::min(2 * mv, 128000000LL);
     p->seed_redraw = 0; p->update_seed_frame_delta = 15;

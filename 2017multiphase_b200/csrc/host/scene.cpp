@@ -146,6 +146,9 @@ extern "C" int mp_scene_params(int config, int n, mp_params* p) {
         p->scene = MP_SCENE_MULTIBUBBLE;
         p->mc_every = 1;
         p->cg_max_iter = 3000;
+        // hundreds of bubbles: the three meshes are far larger than a few
+        // surface layers of the 2x grid
+        p->mc_max_verts = 64000000; p->mc_max_tris = 128000000;
         break;
     }
     return mp_params_derive(p);

@@ -61,40 +61,51 @@ __device__ __forceinline__ bool finish_sum(const Red& R, double mine, double* to
     __syncthreads();
     if (!last) return false;
     __threadfence();
-    if (threadIdx.x < 32) {
-        double a = 0;
-        for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32) a += ((volatile double*)R.part)[b];
-        #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
-        if (threadIdx.x == 0) { *tot = a; *R.count = 0; }
-    }
+    double a = 0;   // fixed strided subsets, then a fixed tree (deterministic)
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += CG_T) a += __ldcg(R.part + b);
+    double t2 = block_sum(a);
+    if (threadIdx.x == 0) { *tot = t2; *R.count = 0; }
     return threadIdx.x == 0;
 }
 
 // ---- matrices --------------------------------------------------------------
+// Both operators are applied to vectors that are exactly zero outside their
+// unknowns (the reference's pcg_op writes 0 there), so a non-BOUNDARY
+// neighbour that is not an unknown contributes its stored zero, as in the
+// reference, without a test. (i,j,k) is decoded once per cell; neighbours are
+// flat offsets. Unknowns are interior cells (the shell is BOUNDARY in a valid
+// state; the interior test only keeps memory accesses in bounds otherwise).
+__device__ __forceinline__ bool inner(const Grid& g, int i, int j, int k) {
+    return i > 0 && i < g.NX - 1 && j > 0 && j < g.NY - 1 && k > 0 && k < g.NZ - 1;
+}
 // computeAx_bubble (spray_k.cu:3423-3447): rows over FLUID and AIR cells
 struct PressOp {
     Grid g;
     const int8_t* __restrict__ mark;
-    __device__ __forceinline__ bool mask(int idx) const {
+    __device__ __forceinline__ bool mask(int idx, int i, int j, int k) const {
         int m = mark[idx];
-        return (m == MP_TYPEFLUID || m == MP_TYPEAIR) && interior(g, idx);
+        return (m == MP_TYPEFLUID || m == MP_TYPEAIR) && inner(g, i, j, k);
     }
     template <class R, class F>
     __device__ __forceinline__ R apply(int idx, F val) const {
-        int i, j, k; getijk(g, idx, i, j, k);
+        const int sI = g.NY * g.NZ, sJ = g.NZ;
         R c = val(idx);
         R s = (R)(-6.0f) * c;
         R h2 = (R)g.h * (R)g.h;
         int q;
-        q = cid(g, i + 1, j, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
-        q = cid(g, i, j + 1, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
-        q = cid(g, i, j, k + 1); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
-        q = cid(g, i - 1, j, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
-        q = cid(g, i, j - 1, k); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
-        q = cid(g, i, j, k - 1); s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = idx + sI; s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = idx + sJ; s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = idx + 1;  s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = idx - sI; s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = idx - sJ; s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
+        q = idx - 1;  s += (mark[q] == MP_TYPEBOUNDARY) ? c : val(q);
         return s / h2;
     }
+    // the same row, piecewise, for the plane-marching kernels
+    __device__ __forceinline__ bool fixed(int q) const { return mark[q] == MP_TYPEBOUNDARY; }
+    template <class R> __device__ __forceinline__ R start(int, R c) const { return (R)(-6.0f) * c; }
+    template <class R> __device__ __forceinline__ R comb(R s, R v) const { return s + v; }
+    template <class R> __device__ __forceinline__ R finish(R s) const { return s / ((R)g.h * (R)g.h); }
 };
 // computeAx_heat (spray_k.cu:4526-4568): rows over non-BOUNDARY cells
 struct HeatOp {
@@ -103,33 +114,51 @@ struct HeatOp {
     float alpha[MP_TYPECNT];
     float dt;
     int boil;    // VACUUM neighbours also take the centre value in boiling scenes
-    __device__ __forceinline__ bool mask(int idx) const { return mark[idx] != MP_TYPEBOUNDARY && interior(g, idx); }
+    __device__ __forceinline__ bool mask(int idx, int i, int j, int k) const {
+        return mark[idx] != MP_TYPEBOUNDARY && inner(g, i, j, k);
+    }
+    __device__ __forceinline__ bool fix(int q) const {
+        int m = mark[q];
+        return boil ? (m == MP_TYPEBOUNDARY || m == MP_TYPEVACUUM) : (m == MP_TYPEBOUNDARY);
+    }
     template <class R, class F>
     __device__ __forceinline__ R apply(int idx, F val) const {
-        int i, j, k; getijk(g, idx, i, j, k);
+        const int sI = g.NY * g.NZ, sJ = g.NZ;
         float al = alpha[mark[idx]];
         float h = g.h;
         R c = val(idx);
         R s = (R)(h * h / al / dt + 6.0f) * c;
         int q;
-        auto fix = [&](int qq) { int m = mark[qq]; return boil ? (m == MP_TYPEBOUNDARY || m == MP_TYPEVACUUM) : (m == MP_TYPEBOUNDARY); };
-        q = cid(g, i + 1, j, k); s -= fix(q) ? c : val(q);
-        q = cid(g, i, j + 1, k); s -= fix(q) ? c : val(q);
-        q = cid(g, i, j, k + 1); s -= fix(q) ? c : val(q);
-        q = cid(g, i - 1, j, k); s -= fix(q) ? c : val(q);
-        q = cid(g, i, j - 1, k); s -= fix(q) ? c : val(q);
-        q = cid(g, i, j, k - 1); s -= fix(q) ? c : val(q);
+        q = idx + sI; s -= fix(q) ? c : val(q);
+        q = idx + sJ; s -= fix(q) ? c : val(q);
+        q = idx + 1;  s -= fix(q) ? c : val(q);
+        q = idx - sI; s -= fix(q) ? c : val(q);
+        q = idx - sJ; s -= fix(q) ? c : val(q);
+        q = idx - 1;  s -= fix(q) ? c : val(q);
         return s;
     }
+    __device__ __forceinline__ bool fixed(int q) const { return fix(q); }
+    template <class R> __device__ __forceinline__ R start(int idx, R c) const {
+        float al = alpha[mark[idx]];
+        float h = g.h;
+        return (R)(h * h / al / dt + 6.0f) * c;
+    }
+    template <class R> __device__ __forceinline__ R comb(R s, R v) const { return s - v; }
+    template <class R> __device__ __forceinline__ R finish(R s) const { return s; }
 };
+
+#define CG_CELL_LOOP(idx, n, i, j, k)                                                  \
+    MP_GRID_LOOP(idx, n)                                                               \
+        for (int row_ = idx / op.g.NZ, k = idx - row_ * op.g.NZ,                        \
+                 i = row_ / op.g.NY, j = row_ - i * op.g.NY, once_ = 1; once_; once_ = 0)
 
 // r = mask ? b : 0 (x = 0, so b - A x = b); rr; a = rr; eps; stop if converged
 template <class R, class Op>
 __global__ void __launch_bounds__(CG_T) k_cg_init(Op op, int n, const R* __restrict__ b, R* __restrict__ r, Red Rd,
                                                   int tolmode, float tol) {
     double acc = 0;
-    MP_GRID_LOOP(idx, n) {
-        R v = op.mask((int)idx) ? (R)(b[idx] + (R)(-1.0f) * (R)0) : (R)0;
+    CG_CELL_LOOP(idx, n, i, j, k) {
+        R v = op.mask((int)idx, i, j, k) ? (R)(b[idx] + (R)(-1.0f) * (R)0) : (R)0;
         r[idx] = v;
         acc += (double)v * (double)v;
     }
@@ -142,22 +171,21 @@ __global__ void __launch_bounds__(CG_T) k_cg_init(Op op, int n, const R* __restr
     }
 }
 
-// p_new = mask ? r + beta p_old : 0 (first iteration: p = r), z = A p_new, p_new . z
+// p_new = r + beta p_old (first iteration: p = r), zero off the unknowns since
+// r and p_old are; z = A p_new; p_new . z
 template <class R, class Op>
 __global__ void __launch_bounds__(CG_T) k_cg_dir(Op op, int n, const R* __restrict__ r, const R* __restrict__ pold,
                                                  R* __restrict__ pnew, Red Rd, int first) {
     if (Rd.flag[F_DONE] != DONE_RUN) return;
-    R bf = first ? (R)0 : (R)Rd.scal[S_BETA];
-    auto pv = [&](int q) -> R {
-        if (!op.mask(q)) return (R)0;
-        return first ? r[q] : (R)(r[q] + bf * pold[q]);
-    };
+    const R bf = first ? (R)0 : (R)Rd.scal[S_BETA];
+    auto pv = [&](int q) -> R { return first ? __ldg(r + q) : (R)(__ldg(r + q) + bf * __ldg(pold + q)); };
     double acc = 0;
-    MP_GRID_LOOP(idx, n) {
+    CG_CELL_LOOP(idx, n, i, j, k) {
         int id = (int)idx;
-        R pc = pv(id);
+        bool m = op.mask(id, i, j, k);
+        R pc = m ? pv(id) : (R)0;
         pnew[idx] = pc;
-        if (op.mask(id)) {
+        if (m) {
             R z = op.template apply<R>(id, pv);
             acc += (double)z * (double)pc;
         }
@@ -175,12 +203,12 @@ template <class R, class Op>
 __global__ void __launch_bounds__(CG_T) k_cg_upd(Op op, int n, const R* __restrict__ p, R* __restrict__ x,
                                                  R* __restrict__ r, Red Rd, int it, int maxiter, int skip_dot) {
     if (Rd.flag[F_DONE] != DONE_RUN) return;
-    R af = (R)Rd.scal[S_ALPHA];
-    auto pv = [&](int q) -> R { return p[q]; };
+    const R af = (R)Rd.scal[S_ALPHA];
+    auto pv = [&](int q) -> R { return __ldg(p + q); };
     double acc = 0;
-    MP_GRID_LOOP(idx, n) {
+    CG_CELL_LOOP(idx, n, i, j, k) {
         int id = (int)idx;
-        if (op.mask(id)) {
+        if (op.mask(id, i, j, k)) {
             R z = op.template apply<R>(id, pv);
             R xv = x[idx] + af * p[idx];
             R rv = r[idx] + (-af) * z;
@@ -206,12 +234,12 @@ template <class R, class Op>
 __global__ void __launch_bounds__(CG_T) k_cg_true(Op op, int n, const R* __restrict__ b, const R* __restrict__ x,
                                                   R* __restrict__ r, Red Rd, int it, int maxiter) {
     if (Rd.flag[F_DONE] != DONE_RUN) return;
-    auto xv = [&](int q) -> R { return x[q]; };
+    auto xv = [&](int q) -> R { return __ldg(x + q); };
     double acc = 0;
-    MP_GRID_LOOP(idx, n) {
+    CG_CELL_LOOP(idx, n, i, j, k) {
         int id = (int)idx;
         R v = (R)0;
-        if (op.mask(id)) v = (R)(b[idx] + (R)(-1.0f) * op.template apply<R>(id, xv));
+        if (op.mask(id, i, j, k)) v = (R)(b[idx] + (R)(-1.0f) * op.template apply<R>(id, xv));
         r[idx] = v;
         acc += (double)v * (double)v;
     }
@@ -222,6 +250,152 @@ __global__ void __launch_bounds__(CG_T) k_cg_true(Op op, int n, const R* __restr
         if (tot < Rd.scal[S_EPS]) Rd.flag[F_DONE] = DONE_CONV;
         else if (it + 1 >= maxiter) Rd.flag[F_DONE] = DONE_CAP;
         else { Rd.scal[S_BETA] = tot / Rd.scal[S_A]; Rd.scal[S_A] = tot; }
+    }
+}
+
+// ---- plane-marching stencil kernels -------------------------------------------
+// A 32x8 thread tile covers (k, j) and marches along i over a chunk of planes.
+// The value at (i+1) and (i-1) of a thread's own column lives in registers,
+// the +-j / +-k neighbours of plane i come from a shared-memory tile with a
+// one-cell halo, and a per-cell byte (built once per solve, k_nb8) says whether
+// the cell is an unknown (bit 7) and which of its six neighbours take the
+// centre value (bits 0-5, in the reference's order +x +y +z -x -y -z). Each
+// value is read from HBM about once; the arithmetic and its order are those
+// of PressOp/HeatOp::apply.
+constexpr int PM_X = 32, PM_Y = 8;
+struct PmGeom { int chunk; };
+
+template <class Op>
+__global__ void k_nb8(Op op, int n, uint8_t* __restrict__ nb8) {
+    const int sI = op.g.NY * op.g.NZ, sJ = op.g.NZ;
+    CG_CELL_LOOP(idx, n, i, j, k) {
+        uint8_t m = 0;
+        if (op.mask(idx, i, j, k)) {
+            m = 0x80;
+            if (op.fixed(idx + sI)) m |= 1;
+            if (op.fixed(idx + sJ)) m |= 2;
+            if (op.fixed(idx + 1)) m |= 4;
+            if (op.fixed(idx - sI)) m |= 8;
+            if (op.fixed(idx - sJ)) m |= 16;
+            if (op.fixed(idx - 1)) m |= 32;
+        }
+        nb8[idx] = m;
+    }
+}
+
+__device__ __forceinline__ bool pm_finish(const Red& R, double mine, double* tot) {
+    __shared__ double ws[PM_X * PM_Y / 32];
+    __shared__ bool last;
+    const int tid = threadIdx.x + PM_X * threadIdx.y;
+    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    double v = mine;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((tid & 31) == 0) ws[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0;
+        for (int w = 0; w < PM_X * PM_Y / 32; w++) s += ws[w];
+        R.part[bid] = s;
+        __threadfence();
+        unsigned int t = atomicAdd(R.count, 1u);
+        last = (t == nblk - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    // the last block adds the partials: every thread a fixed strided subset
+    // (independent L2 loads), then a fixed tree, so the sum is deterministic
+    double a = 0;
+    for (unsigned int b = tid; b < nblk; b += PM_X * PM_Y) a += __ldcg(R.part + b);
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    __syncthreads();
+    if ((tid & 31) == 0) ws[tid >> 5] = a;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0;
+        for (int w = 0; w < PM_X * PM_Y / 32; w++) s += ws[w];
+        *tot = s; *R.count = 0;
+    }
+    return tid == 0;
+}
+
+// MODE 0 (direction): value = r + beta p_old (first: r); writes p_new; sums p.Ap
+// MODE 1 (update):    value = p; x += alpha p, r -= alpha Ap; sums r.r
+template <class R, class Op, int MODE>
+__global__ void __launch_bounds__(PM_X * PM_Y) k_cg_pm(Op op, PmGeom pg, const uint8_t* __restrict__ nb8,
+                                                      const R* __restrict__ va, const R* __restrict__ vb,
+                                                      R* __restrict__ pout, R* __restrict__ x, R* __restrict__ r,
+                                                      Red Rd, int first, int it, int maxiter, int skip_dot) {
+    if (Rd.flag[F_DONE] != DONE_RUN) return;
+    __shared__ R tile[PM_Y + 2][PM_X + 2];
+    const Grid& g = op.g;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int k = blockIdx.x * PM_X + tx, j = blockIdx.y * PM_Y + ty;
+    const int i0 = blockIdx.z * pg.chunk, i1 = min(i0 + pg.chunk, g.NX);
+    const bool inb = k < g.NZ && j < g.NY;
+    const R bf = (MODE == 0 && !first) ? (R)Rd.scal[S_BETA] : (R)0;
+    const R af = MODE == 1 ? (R)Rd.scal[S_ALPHA] : (R)0;
+    auto ld = [&](int i, int jj, int kk) -> R {
+        if (i < 0 || i >= g.NX || jj < 0 || jj >= g.NY || kk < 0 || kk >= g.NZ) return (R)0;
+        int q = (i * g.NY + jj) * g.NZ + kk;
+        if (MODE == 1 || first) return __ldg(va + q);
+        return (R)(__ldg(va + q) + bf * __ldg(vb + q));
+    };
+    R behind = ld(i0 - 1, j, k), cur = ld(i0, j, k);
+    double acc = 0;
+    for (int i = i0; i < i1; i++) {
+        R front = ld(i + 1, j, k);
+        __syncthreads();
+        tile[ty + 1][tx + 1] = cur;
+        if (ty == 0) tile[0][tx + 1] = ld(i, j - 1, k);
+        if (ty == PM_Y - 1) tile[PM_Y + 1][tx + 1] = ld(i, j + 1, k);
+        if (tx == 0) tile[ty + 1][0] = ld(i, j, k - 1);
+        if (tx == PM_X - 1) tile[ty + 1][PM_X + 1] = ld(i, j, k + 1);
+        __syncthreads();
+        if (inb) {
+            const int c = (i * g.NY + j) * g.NZ + k;
+            const uint32_t m = nb8[c];
+            if (MODE == 0) pout[c] = (m & 0x80) ? cur : (R)0;
+            if (m & 0x80) {
+                R s = op.template start<R>(c, cur);
+                s = op.template comb<R>(s, (m & 1) ? cur : front);
+                s = op.template comb<R>(s, (m & 2) ? cur : tile[ty + 2][tx + 1]);
+                s = op.template comb<R>(s, (m & 4) ? cur : tile[ty + 1][tx + 2]);
+                s = op.template comb<R>(s, (m & 8) ? cur : behind);
+                s = op.template comb<R>(s, (m & 16) ? cur : tile[ty][tx + 1]);
+                s = op.template comb<R>(s, (m & 32) ? cur : tile[ty + 1][tx]);
+                R z = op.template finish<R>(s);
+                if (MODE == 0) {
+                    acc += (double)z * (double)cur;
+                } else {
+                    R xv = x[c] + af * cur;
+                    R rv = r[c] + (-af) * z;
+                    x[c] = xv; r[c] = rv;
+                    acc += (double)rv * (double)rv;
+                }
+            } else if (MODE == 1) {
+                x[c] = (R)0; r[c] = (R)0;
+            }
+        }
+        behind = cur; cur = front;
+    }
+    if (MODE == 1 && skip_dot) return;
+    double tot;
+    if (pm_finish(Rd, acc, &tot)) {
+        if (MODE == 0) {
+            Rd.scal[S_ZP] = tot;
+            if (tot == 0) Rd.flag[F_DONE] = DONE_ZP0;
+            else Rd.scal[S_ALPHA] = Rd.scal[S_A] / tot;
+        } else {
+            Rd.scal[S_RR] = tot;
+            Rd.flag[F_ITERS] = it + 1;
+            if (tot < Rd.scal[S_EPS]) Rd.flag[F_DONE] = DONE_CONV;
+            else if (it + 1 >= maxiter) Rd.flag[F_DONE] = DONE_CAP;
+            else { Rd.scal[S_BETA] = tot / Rd.scal[S_A]; Rd.scal[S_A] = tot; }
+        }
     }
 }
 
@@ -351,6 +525,17 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     k_cg_init<R, Op><<<nb, CG_T, 0, s>>>(op, n, b, r, Rd, tolmode, tol);
     c->launches++;
     MP_CHECK_LAUNCH(c);
+    // neighbour bytes for the plane-marching kernels (mark_tmp is free scratch here)
+    uint8_t* nb8 = reinterpret_cast<uint8_t*>(c->mark_tmp);
+    k_nb8<Op><<<mp_blocks(n, 256), 256, 0, s>>>(op, n, nb8);
+    c->launches++;
+    const Grid& gg = c->G;
+    dim3 pmb(PM_X, PM_Y);
+    int tiles = ((gg.NZ + PM_X - 1) / PM_X) * ((gg.NY + PM_Y - 1) / PM_Y);
+    int chunk = std::max(4, (int)((gg.NX * (long long)tiles + 4095) / 4096));   // <= 4096 blocks (partials buffer)
+    PmGeom pg{chunk};
+    dim3 pmg((gg.NZ + PM_X - 1) / PM_X, (gg.NY + PM_Y - 1) / PM_Y, (gg.NX + chunk - 1) / chunk);
+    if ((long long)pmg.x * pmg.y * pmg.z > 148LL * 32) { c->err = "cg: tiling exceeds partials buffer"; return MP_ERR_CAPACITY; }
     unsigned int hflag[F_COUNT] = {0, 0};
     MP_CUDA(c, cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s));
     MP_CUDA(c, cudaStreamSynchronize(s));
@@ -359,14 +544,16 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     while (hflag[F_DONE] == DONE_RUN && it < maxiter) {
         int end = std::min(maxiter, it + batch);
         for (; it < end; it++) {
-            {
-                KtScope kt(c, kt_stencil);
-                k_cg_dir<R, Op><<<nb, CG_T, 0, s>>>(op, n, r, pa, pb, Rd, it == 0 ? 1 : 0);
-            }
             bool tr = true_every > 0 && (it + 1) % true_every == 0;
             {
+                KtScope kt(c, kt_stencil);
+                k_cg_pm<R, Op, 0><<<pmg, pmb, 0, s>>>(op, pg, nb8, r, pa, pb, nullptr, nullptr, Rd,
+                                                      it == 0 ? 1 : 0, it, maxiter, 0);
+            }
+            {
                 KtScope kt(c, MP_KT_CG_UPDATE);
-                k_cg_upd<R, Op><<<nb, CG_T, 0, s>>>(op, n, pb, x, r, Rd, it, maxiter, tr ? 1 : 0);
+                k_cg_pm<R, Op, 1><<<pmg, pmb, 0, s>>>(op, pg, nb8, pb, nullptr, nullptr, x, r, Rd, 0, it, maxiter,
+                                                      tr ? 1 : 0);
             }
             if (tr) k_cg_true<R, Op><<<nb, CG_T, 0, s>>>(op, n, b, x, r, Rd, it, maxiter);
             c->launches += tr ? 3 : 2;

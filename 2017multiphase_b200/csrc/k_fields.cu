@@ -20,32 +20,49 @@ namespace {
 // 5x5x5 cell window, minus half a cell. min over sqrt(d2) == sqrt(min d2)
 // because sqrtf is correctly rounded and monotone, so one sqrt per cell and
 // phase gives the reference's value bit for bit.
+// The window is visited nearest cells first and a cell is skipped when no
+// particle in it can lower either minimum: a particle keyed to window cell
+// (di,dj,dk) is at least (|d|-0.5)h away from the centre along each axis
+// (particles keyed to cell 0 from outside the domain are further still), and
+// distances of 2.5h or more are clamped anyway. The bound is shrunk by 1e-4
+// relative so that float rounding of d2 can never make a skipped particle the
+// minimum; the result is therefore identical to visiting every particle.
+__constant__ signed char kWin[125][3] = {
+    {0,0,0}, {-1,0,0}, {0,-1,0}, {0,0,-1}, {0,0,1}, {0,1,0}, {1,0,0}, {-1,-1,0}, {-1,0,-1}, {-1,0,1}, {-1,1,0}, {0,-1,-1}, {0,-1,1}, {0,1,-1}, {0,1,1}, {1,-1,0}, {1,0,-1}, {1,0,1}, {1,1,0}, {-1,-1,-1}, {-1,-1,1}, {-1,1,-1}, {-1,1,1}, {1,-1,-1}, {1,-1,1}, {1,1,-1}, {1,1,1}, {-2,0,0}, {0,-2,0}, {0,0,-2}, {0,0,2}, {0,2,0}, {2,0,0}, {-2,-1,0}, {-2,0,-1}, {-2,0,1}, {-2,1,0}, {-1,-2,0}, {-1,0,-2}, {-1,0,2}, {-1,2,0}, {0,-2,-1}, {0,-2,1}, {0,-1,-2}, {0,-1,2}, {0,1,-2}, {0,1,2}, {0,2,-1}, {0,2,1}, {1,-2,0}, {1,0,-2}, {1,0,2}, {1,2,0}, {2,-1,0}, {2,0,-1}, {2,0,1}, {2,1,0}, {-2,-1,-1}, {-2,-1,1}, {-2,1,-1}, {-2,1,1}, {-1,-2,-1}, {-1,-2,1}, {-1,-1,-2}, {-1,-1,2}, {-1,1,-2}, {-1,1,2}, {-1,2,-1}, {-1,2,1}, {1,-2,-1}, {1,-2,1}, {1,-1,-2}, {1,-1,2}, {1,1,-2}, {1,1,2}, {1,2,-1}, {1,2,1}, {2,-1,-1}, {2,-1,1}, {2,1,-1}, {2,1,1}, {-2,-2,0}, {-2,0,-2}, {-2,0,2}, {-2,2,0}, {0,-2,-2}, {0,-2,2}, {0,2,-2}, {0,2,2}, {2,-2,0}, {2,0,-2}, {2,0,2}, {2,2,0}, {-2,-2,-1}, {-2,-2,1}, {-2,-1,-2}, {-2,-1,2}, {-2,1,-2}, {-2,1,2}, {-2,2,-1}, {-2,2,1}, {-1,-2,-2}, {-1,-2,2}, {-1,2,-2}, {-1,2,2}, {1,-2,-2}, {1,-2,2}, {1,2,-2}, {1,2,2}, {2,-2,-1}, {2,-2,1}, {2,-1,-2}, {2,-1,2}, {2,1,-2}, {2,1,2}, {2,2,-1}, {2,2,1}, {-2,-2,-2}, {-2,-2,2}, {-2,2,-2}, {-2,2,2}, {2,-2,-2}, {2,-2,2}, {2,2,-2}, {2,2,2}};
+
 __global__ void __launch_bounds__(256) k_genlevelset(Grid g, Cells cl, const float4* __restrict__ pos,
                                                      float* __restrict__ lsf, float* __restrict__ lsa,
                                                      int8_t* __restrict__ mark) {
+    const uint32_t AIRB = (1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO);
+    const uint32_t FLB = (1u << MP_TYPEFLUID) | (1u << MP_TYPESOLID);
     MP_GRID_LOOP(idx, g.n) {
         mark[idx] = MP_TYPEVACUUM;
         float h = g.h;
         float r = 0.5f * h;
         int i, j, k; getijk3((int)idx, g.NY, g.NZ, i, j, k);
         float3 gp = (mk3((float)i, (float)j, (float)k) + mk3(0.5f, 0.5f, 0.5f)) * h;
+        const float cap2 = 6.25f * h * h * 1.001f;       // beyond 2.5h nothing changes
         float ma2 = __int_as_float(0x7f800000), mf2 = __int_as_float(0x7f800000);
-        for (int di = -2; di <= 2; ++di) {
-            int a = i + di; if (a < 0 || a > g.NX - 1) continue;
-            for (int dj = -2; dj <= 2; ++dj) {
-                int b = j + dj; if (b < 0 || b > g.NY - 1) continue;
-                int k0 = max(k - 2, 0), k1 = min(k + 2, g.NZ - 1);
-                int c0 = cid(g, a, b, k0), c1 = cid(g, a, b, k1);
-                uint32_t s0 = __ldg(cl.off + c0), s1 = __ldg(cl.off + c1 + 1);
-                // cells of one (a,b) column are contiguous in the sorted array
-                for (uint32_t p = s0; p < s1; ++p) {
-                    float4 q = __ldg(pos + p);
-                    float3 d = mk3(q.x, q.y, q.z) - gp;
-                    float d2 = dot(d, d);
-                    int f = pflag(q);
-                    if (f == MP_TYPEAIR || f == MP_TYPEAIRSOLO) ma2 = fminf(ma2, d2);
-                    else if (f == MP_TYPEFLUID || f == MP_TYPESOLID) mf2 = fminf(mf2, d2);
-                }
+        for (int w = 0; w < 125; ++w) {
+            int di = kWin[w][0], dj = kWin[w][1], dk = kWin[w][2];
+            int a = i + di, b = j + dj, cc = k + dk;
+            if (a < 0 || a > g.NX - 1 || b < 0 || b > g.NY - 1 || cc < 0 || cc > g.NZ - 1) continue;
+            float bx = di == 0 ? 0.f : ((float)abs(di) - 0.5f), by = dj == 0 ? 0.f : ((float)abs(dj) - 0.5f);
+            float bz = dk == 0 ? 0.f : ((float)abs(dk) - 0.5f);
+            float lb2 = (bx * bx + by * by + bz * bz) * h * h * 0.9999f;
+            bool wantA = lb2 < fminf(ma2, cap2), wantF = lb2 < fminf(mf2, cap2);
+            if (!wantA && !wantF) continue;
+            int c = cid(g, a, b, cc);
+            uint32_t tm = __ldg(cl.tmask + c);
+            if (!((wantA && (tm & AIRB)) || (wantF && (tm & FLB)))) continue;
+            uint32_t s0 = __ldg(cl.off + c), s1 = __ldg(cl.off + c + 1);
+            for (uint32_t p = s0; p < s1; ++p) {
+                float4 q = __ldg(pos + p);
+                float3 d = mk3(q.x, q.y, q.z) - gp;
+                float d2 = dot(d, d);
+                int f = pflag(q);
+                if (f == MP_TYPEAIR || f == MP_TYPEAIRSOLO) ma2 = fminf(ma2, d2);
+                else if (f == MP_TYPEFLUID || f == MP_TYPESOLID) mf2 = fminf(mf2, d2);
             }
         }
         float mair = 2.5f * h, mfl = 2.5f * h;
@@ -67,20 +84,23 @@ __device__ __forceinline__ void solvedistance(float a, float b, float c, float& 
 // one Jacobi pass of sweepphibytype (typeflag >= 0) or sweepphi (typeflag < 0)
 __global__ void k_sweep(Grid g, const float* __restrict__ in, float* __restrict__ out,
                         const int8_t* __restrict__ mark, int typeflag) {
+    const int sI = g.NY * g.NZ, sJ = g.NZ;
     MP_GRID_LOOP(idx, g.n) {
         float res = in[idx];
         if (!(typeflag >= 0 && mark[idx] == typeflag)) {
             int i, j, k; getijk(g, (int)idx, i, j, k);
+            // the six neighbours, each loaded once; octants in the reference's order
+            const bool vx[2] = {i > 0, i < g.NX - 1}, vy[2] = {j > 0, j < g.NY - 1}, vz[2] = {k > 0, k < g.NZ - 1};
+            const float nx[2] = {vx[0] ? __ldg(in + idx - sI) : 0.f, vx[1] ? __ldg(in + idx + sI) : 0.f};
+            const float ny[2] = {vy[0] ? __ldg(in + idx - sJ) : 0.f, vy[1] ? __ldg(in + idx + sJ) : 0.f};
+            const float nz[2] = {vz[0] ? __ldg(in + idx - 1) : 0.f, vz[1] ? __ldg(in + idx + 1) : 0.f};
             #pragma unroll
-            for (int di = -1; di <= 1; di += 2)
+            for (int a = 0; a < 2; a++)
             #pragma unroll
-            for (int dj = -1; dj <= 1; dj += 2)
+            for (int b = 0; b < 2; b++)
             #pragma unroll
-            for (int dk = -1; dk <= 1; dk += 2) {
-                if (vc(g, i + di, j, k) && vc(g, i, j + dj, k) && vc(g, i, j, k + dk))
-                    solvedistance(__ldg(in + cid(g, i + di, j, k)), __ldg(in + cid(g, i, j + dj, k)),
-                                  __ldg(in + cid(g, i, j, k + dk)), res);
-            }
+            for (int e = 0; e < 2; e++)
+                if (vx[a] && vy[b] && vz[e]) solvedistance(nx[a], ny[b], nz[e], res);
         }
         out[idx] = res;
     }

@@ -26,18 +26,19 @@ struct McGrid {
     int NXMC, NYMC, NZMC;   // voxels
     int W, H, D;            // nodes
     float hm;               // node spacing
+    Tiles T;                // 3-D tiling of the nodes for the density gather
 };
 
 template <int SURF>
 __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const float4* __restrict__ pos, float* __restrict__ dens,
                                                     int scene) {
-    long long tot = (long long)m.W * m.H * m.D;
+    const Tiles T = m.T;
     const float hm = m.hm;
     const uint32_t need = SURF == MP_MC_SOLID ? (1u << MP_TYPESOLID)
                         : SURF == MP_MC_FLUID ? ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO) | (1u << MP_TYPEFLUID))
                                               : ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO));
-    MP_GRID_LOOP(t, tot) {
-        int i, j, k; getijk3((int)t, m.H, m.D, i, j, k);
+    MP_GRID_LOOP(t, T.threads()) {
+        int i, j, k; if (!tile_ijk(T, t, i, j, k)) continue;
         float3 p = mk3((float)i, (float)j, (float)k) * hm;
         float3 center = mk3(0.0f);
         float wsum = 0.0f;
@@ -54,8 +55,13 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
                         float4 o = __ldg(pos + q);
                         int f = pflag(o);
                         float3 op = xyz(o);
+                        // beyond the kernel radius the weight is exactly zero and the pair
+                        // adds nothing: skip it before the sqrt (exact test with margin)
+                        float3 dd = op - p;
+                        float d2 = dot(dd, dd);
                         if (SURF == MP_MC_SOLID) {
                             if (f != MP_TYPESOLID) continue;
+                            if (d2 > hm * hm * 1.001f) continue;
                             float dis = length(op - p);
                             if (dis < hm) {
                                 float w = dis / (4 * hm);
@@ -68,6 +74,7 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
                                                           : (f == MP_TYPEAIR || (f == MP_TYPEAIRSOLO && scene != MP_SCENE_INTERACTION));
                             if (!ok) continue;
                             float R = hm * 2;
+                            if (d2 > R * R * 1.001f) continue;
                             float dis = length(op - p);
                             if (dis < R) {
                                 float w = R * R - dis * dis;
@@ -98,7 +105,7 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
             else phi = -r;
             if (border) phi = -1000.0f;
         }
-        dens[t] = phi;
+        dens[(i * m.H + j) * m.D + k] = phi;
     }
 }
 
@@ -246,6 +253,7 @@ int k_mc(MpCtx* c, int surface) {
     m.NXMC = 2 * c->G.NX; m.NYMC = 2 * c->G.NY; m.NZMC = 2 * c->G.NZ;
     m.W = m.NXMC + 1; m.H = m.NYMC + 1; m.D = m.NZMC + 1;
     m.hm = c->G.h / (float)(m.NXMC / c->G.NX);
+    m.T = make_tiles(m.W, m.H, m.D);
     Cells cl{c->cell_off, c->tmask};
     long long nnode = (long long)m.W * m.H * m.D;
     long long nvox = (long long)m.NXMC * m.NYMC * m.NZMC;
@@ -254,9 +262,9 @@ int k_mc(MpCtx* c, int surface) {
     out.nverts = out.nindices = out.active = 0;
     {
         KtScope kt(c, MP_KT_MC_DENS);
-        if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(nnode, 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
-        else if (surface == MP_MC_FLUID) k_mc_density<MP_MC_FLUID><<<mp_blocks(nnode, 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
-        else k_mc_density<MP_MC_GAS><<<mp_blocks(nnode, 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
+        if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
+        else if (surface == MP_MC_FLUID) k_mc_density<MP_MC_FLUID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
+        else k_mc_density<MP_MC_GAS><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
     }
     k_mc_classify<<<mp_blocks(nvox, 256), 256, 0, s>>>(m, c->mc_dens, c->mc_numverts, c->mc_cube, c->mc_vverts, c->mc_vflag);
     c->launches += 2;

@@ -27,11 +27,10 @@ __global__ void __launch_bounds__(256) k_p2g_faces(Grid g, Cells cl, const float
                                                    float* __restrict__ uy, float* __restrict__ uz) {
     constexpr int R = WHICH == 0 ? 1 : 2;      // union window -R..R
     constexpr int HI = WHICH == 0 ? 0 : 1;     // upper bound along the face normal
-    const int W = g.NX + 1, Hh = g.NY + 1, D = g.NZ + 1;
-    long long tot = (long long)W * Hh * D;
+    const Tiles T = make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1);
     const float scale = 1.0f / g.h;
-    MP_GRID_LOOP(t, tot) {
-        int i, j, k; getijk3((int)t, Hh, D, i, j, k);
+    MP_GRID_LOOP(t, T.threads()) {
+        int i, j, k; if (!tile_ijk(T, t, i, j, k)) continue;
         bool hx = (j < g.NY && k < g.NZ), hy = (i < g.NX && k < g.NZ), hz = (i < g.NX && j < g.NY);
         float wx = 0, sx = 0, wy = 0, sy = 0, wz = 0, sz = 0;
         const float3 gpx = mk3((float)i, (float)j + 0.5f, (float)k + 0.5f);
@@ -50,7 +49,9 @@ __global__ void __launch_bounds__(256) k_p2g_faces(Grid g, Cells cl, const float
                     bool az = hz && dk <= HI;
                     if (!(ax || ay || az)) continue;
                     int c = cid(g, a, b, cc);
-                    if (WHICH == 1 && !((__ldg(cl.tmask + c) >> MP_TYPEAIR) & 1)) continue;
+                    // the type mask is built at sort time; AIR <-> AIRSOLO flips since then
+                    // (markSoloAirParticle) keep the union bit valid
+                    if (WHICH == 1 && !(__ldg(cl.tmask + c) & ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO)))) continue;
                     if (WHICH == 0 && !(__ldg(cl.tmask + c) & ((1u << MP_TYPEFLUID) | (1u << MP_TYPESOLID)))) continue;
                     uint32_t s0 = __ldg(cl.off + c), s1 = __ldg(cl.off + c + 1);
                     for (uint32_t p = s0; p < s1; ++p) {
@@ -58,22 +59,34 @@ __global__ void __launch_bounds__(256) k_p2g_faces(Grid g, Cells cl, const float
                         int f = pflag(q);
                         bool ok = WHICH == 0 ? (f == MP_TYPEFLUID || f == MP_TYPESOLID) : (f == MP_TYPEAIR);
                         if (!ok) continue;
+                        // sharp_kernel(r2, 1.4) is exactly zero once r2 exceeds 1.4^2, and a
+                        // zero weight adds +-0 to both sums: such pairs are skipped
+                        const float cut = (1.4f * 1.4f) * 1.0001f;
                         float4 v = __ldg(vel + p);
                         float3 ps = mk3(q.x, q.y, q.z) * scale;
                         if (ax) {
                             float3 d = ps - gpx;
-                            float w = v.w * sharp_kernel(dot(d, d), 1.4f);
-                            wx += w; sx += w * v.x;
+                            float r2 = dot(d, d);
+                            if (r2 <= cut) {
+                                float w = v.w * sharp_kernel(r2, 1.4f);
+                                wx += w; sx += w * v.x;
+                            }
                         }
                         if (ay) {
                             float3 d = ps - gpy;
-                            float w = v.w * sharp_kernel(dot(d, d), 1.4f);
-                            wy += w; sy += w * v.y;
+                            float r2 = dot(d, d);
+                            if (r2 <= cut) {
+                                float w = v.w * sharp_kernel(r2, 1.4f);
+                                wy += w; sy += w * v.y;
+                            }
                         }
                         if (az) {
                             float3 d = ps - gpz;
-                            float w = v.w * sharp_kernel(dot(d, d), 1.4f);
-                            wz += w; sz += w * v.z;
+                            float r2 = dot(d, d);
+                            if (r2 <= cut) {
+                                float w = v.w * sharp_kernel(r2, 1.4f);
+                                wz += w; sz += w * v.z;
+                            }
                         }
                     }
                 }
@@ -126,7 +139,8 @@ __global__ void k_drag_faces(Grid g, Cells cl, const float4* __restrict__ pos, c
                              float* __restrict__ uz) {
     const int W = g.NX + 1, Hh = g.NY + 1, D = g.NZ + 1;
     long long tot = (long long)W * Hh * D;
-    const uint32_t bit = 1u << MP_TYPEAIRSOLO;
+    // union with AIR: the mask predates markSoloAirParticle's AIR -> AIRSOLO flips
+    const uint32_t bit = (1u << MP_TYPEAIRSOLO) | (1u << MP_TYPEAIR);
     MP_GRID_LOOP(t, tot) {
         int i, j, k; getijk3((int)t, Hh, D, i, j, k);
         #pragma unroll
@@ -246,7 +260,7 @@ static Cells cells_of(MpCtx* c) { return Cells{c->cell_off, c->tmask}; }
 
 int k_p2g_faces(MpCtx* c, float** out, int which) {
     const Grid& g = c->G;
-    long long tot = (long long)(g.NX + 1) * (g.NY + 1) * (g.NZ + 1);
+    long long tot = make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1).threads();
     if (which == 0)
         k_p2g_faces<0><<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g, cells_of(c), c->pos, c->vel, out[0], out[1], out[2]);
     else

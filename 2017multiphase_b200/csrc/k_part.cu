@@ -297,6 +297,7 @@ __global__ void k_correct_pos(Grid g, Cells cl, int np, const float4* __restrict
     const float3 g1 = g0 + mk3((float)g.NX, (float)g.NY, (float)g.NZ) * h;
     const float3 tmin = g0 + (mk3(h, h, h) + mk3(0.5f * samplespace));
     const float3 tmax = g1 - (mk3(h, h, h) + mk3(0.5f * samplespace));
+    const float re2_skip = re * re * 1.001f;
     MP_GRID_LOOP(p, np) {
         float4 q = pos[p];
         int f = pflag(q);
@@ -304,18 +305,31 @@ __global__ void k_correct_pos(Grid g, Cells cl, int np, const float4* __restrict
         float3 ip = xyz(q);
         int i, j, k; ijkpos(g, ip, i, j, k);
         float3 spring = mk3(0.0f);
-        for (int di = -1; di <= 1; di++) for (int dj = -1; dj <= 1; dj++) for (int dk = -1; dk <= 1; dk++) {
-            if (!vc(g, i + di, j + dj, k + dk)) continue;
-            int c = cid(g, i + di, j + dj, k + dk);
+        // the three cells of a (di,dj) column are contiguous: their four range
+        // bounds are read together, then each cell is summed on its own
+        const int k0 = max(k - 1, 0), k1 = min(k + 1, g.NZ - 1);
+        for (int di = -1; di <= 1; di++) for (int dj = -1; dj <= 1; dj++) {
+            if (!vc(g, i + di, j + dj, k)) continue;
+            const int cb = cid(g, i + di, j + dj, k0);
+            uint32_t bnd[4];
+            #pragma unroll
+            for (int q = 0; q < 4; q++) bnd[q] = (q <= k1 - k0 + 1) ? __ldg(cl.off + cb + q) : 0u;
+            for (int cc = 0; cc <= k1 - k0; cc++) {
             float3 s = mk3(0.0f);
-            for (uint32_t t = __ldg(cl.off + c); t < __ldg(cl.off + c + 1); ++t) {
+            for (uint32_t t = bnd[cc]; t < bnd[cc + 1]; ++t) {
                 float3 o = xyz(__ldg(pos + t));
+                float3 dd = o - ip;
+                // beyond re the kernel weight is exactly zero and the pair adds a
+                // signed zero, which leaves the sum unchanged: skip it (exact test
+                // with margin: dist*dist >= re*re whenever d2 > 1.001 re*re)
+                if (dot(dd, dd) > re2_skip) continue;
                 float m = __ldg(&vel[t].w);
-                float dist = length(o - ip);
+                float dist = length(dd);
                 float w = m * smooth_kernel(dist * dist, re);
                 if (dist > 0.1f * re) s += w * (ip - o) / dist;
             }
             spring += s;
+            }
         }
         spring *= spring_k * re;
         if (length(dt * spring) > 0.3f * h) ip += h * 0.3f * spring / length(spring);

@@ -149,17 +149,25 @@ int mp_scan_u32(MpCtx* c, const uint32_t* in, uint32_t* out, size_t n) {
 namespace {
 // calcHashD (spray_k.cu:1010-1028) / calcHashD_MC (:1030-1048): cell id on a
 // grid of (w,hh,d) cells of size dx; an axis outside maps to 0.
+__device__ __forceinline__ uint32_t hash_key(float4 q, float gx0, float gy0, float gz0, float dx, int w, int hh, int d) {
+    float3 r = (mk3(q.x, q.y, q.z) - mk3(gx0, gy0, gz0)) / mk3(dx, dx, dx);
+    int i = (r.x >= 0 && r.x < w) ? (int)r.x : 0;
+    int j = (r.y >= 0 && r.y < hh) ? (int)r.y : 0;
+    int k = (r.z >= 0 && r.z < d) ? (int)r.z : 0;
+    return (uint32_t)(i * hh * d + j * d + k);
+}
+// keys, per-cell counts, and a flag raised when the keys are not already in
+// order (then the stable sort is the identity and the gather can be skipped)
 __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, float gy0, float gz0, float dx,
-                             int w, int hh, int d, uint32_t* __restrict__ keys, uint32_t* __restrict__ cnt) {
+                             int w, int hh, int d, uint32_t* __restrict__ keys, uint32_t* __restrict__ cnt,
+                             uint32_t* __restrict__ unsorted) {
     MP_GRID_LOOP(p, np) {
-        float4 q = pos[p];
-        float3 r = (mk3(q.x, q.y, q.z) - mk3(gx0, gy0, gz0)) / mk3(dx, dx, dx);
-        int i = (r.x >= 0 && r.x < w) ? (int)r.x : 0;
-        int j = (r.y >= 0 && r.y < hh) ? (int)r.y : 0;
-        int k = (r.z >= 0 && r.z < d) ? (int)r.z : 0;
-        uint32_t key = (uint32_t)(i * hh * d + j * d + k);
+        uint32_t key = hash_key(pos[p], gx0, gy0, gz0, dx, w, hh, d);
+        if (p > 0 && hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d) > key) *unsorted = 1u;
         keys[p] = key;
-        atomicAdd(cnt + key, 1u);
+        // one atomic per run of equal keys in the warp (particles arrive nearly sorted)
+        unsigned peers = __match_any_sync(__activemask(), key);
+        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(cnt + key, (uint32_t)__popc(peers));
     }
 }
 // place each particle index in its cell's range (order inside a cell fixed later);
@@ -168,7 +176,13 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, int np, const uint3
                           uint32_t* __restrict__ cnt, uint32_t* __restrict__ perm) {
     MP_GRID_LOOP(p, np) {
         uint32_t key = keys[p];
-        uint32_t r = atomicSub(cnt + key, 1u) - 1u;
+        // a warp's run of equal keys takes consecutive slots in lane (= index) order
+        unsigned peers = __match_any_sync(__activemask(), key);
+        int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+        uint32_t cntp = (uint32_t)__popc(peers), base = 0;
+        if (lane == leader) base = atomicSub(cnt + key, cntp) - cntp;
+        base = __shfl_sync(peers, base, leader);
+        uint32_t r = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
         perm[off[key] + r] = (uint32_t)p;
     }
 }
@@ -189,6 +203,15 @@ __global__ void k_segsort(const uint32_t* __restrict__ off, int ncell, uint32_t*
         tmask[cc] = (uint8_t)m;
     }
 }
+// type mask of each cell when the particles are already in cell order
+__global__ void k_tmask_sorted(const uint32_t* __restrict__ off, int ncell, const float4* __restrict__ pos,
+                               uint8_t* __restrict__ tmask) {
+    MP_GRID_LOOP(cc, ncell) {
+        uint32_t m = 0;
+        for (uint32_t s = off[cc]; s < off[cc + 1]; s++) m |= 1u << (pflag(__ldg(pos + s)) & 7);
+        tmask[cc] = (uint8_t)m;
+    }
+}
 __global__ void k_reorder(const uint32_t* __restrict__ perm, int np,
                           const float4* __restrict__ p0, const float4* __restrict__ v0, const float4* __restrict__ h0,
                           float4* __restrict__ p1, float4* __restrict__ v1, float4* __restrict__ h1) {
@@ -204,13 +227,27 @@ __global__ void k_reorder(const uint32_t* __restrict__ perm, int np,
 static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     int np = c->np();
     int ncell = w * hh * d;
+    uint32_t* unsorted = c->u32_scratch + 1;
+    MP_CUDA(c, cudaMemsetAsync(unsorted, 0, sizeof(uint32_t), c->stream));
     if (np > 0) {
         k_hash_count<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->pos, np, c->G.gx0, c->G.gy0, c->G.gz0, dx, w, hh, d,
-                                                                c->keys, c->cell_cnt);
+                                                                c->keys, c->cell_cnt, unsorted);
         c->launches++;
         MP_CHECK_LAUNCH(c);
     }
     MP_TRY(mp_scan_u32(c, c->cell_cnt, c->cell_off, (size_t)ncell));
+    uint32_t h_unsorted = 1;
+    MP_CUDA(c, cudaMemcpyAsync(&h_unsorted, unsorted, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (!h_unsorted) {
+        // already in cell order: the stable sort is the identity permutation;
+        // the counts still have to run back to zero for the next sort
+        MP_CUDA(c, cudaMemsetAsync(c->cell_cnt, 0, sizeof(uint32_t) * ncell, c->stream));
+        k_tmask_sorted<<<mp_blocks(ncell, 256), 256, 0, c->stream>>>(c->cell_off, ncell, c->pos, c->tmask);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        return MP_OK;
+    }
     if (np > 0) {
         k_scatter<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->keys, np, c->cell_off, c->cell_cnt, c->perm);
         c->launches++;

@@ -127,7 +127,30 @@ struct Cells {
     const uint8_t* __restrict__ tmask;   // bit t set if the cell holds a particle of type t
 };
 
-// typed grid-stride loops
-#define MP_GRID_LOOP(idx, N) for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < (long long)(N); idx += (long long)gridDim.x * blockDim.x)
+// 3-D tiles of 2 x 4 x 32 (i, j, k) points per 256-thread block, k fastest, so a
+// warp covers 32 consecutive k and a block's gather window (the union of its
+// points' neighbour cells) is compact, which lets L1 serve most re-reads.
+constexpr int TILE_I = 2, TILE_J = 4, TILE_K = 32;
+struct Tiles {
+    int W, H, D;        // points along i, j, k
+    int ti, tj, tk;     // tiles along i, j, k
+    __host__ __device__ long long threads() const { return (long long)ti * tj * tk * 256; }
+};
+__host__ __device__ inline Tiles make_tiles(int W, int H, int D) {
+    return Tiles{W, H, D, (W + TILE_I - 1) / TILE_I, (H + TILE_J - 1) / TILE_J, (D + TILE_K - 1) / TILE_K};
+}
+MPD bool tile_ijk(const Tiles& T, int t, int& i, int& j, int& k) {
+    int tile = t >> 8, o = t & 255;
+    int a = tile % T.tk, r = tile / T.tk;
+    int b = r % T.tj, c = r / T.tj;
+    k = a * TILE_K + (o & 31);
+    j = b * TILE_J + ((o >> 5) & 3);
+    i = c * TILE_I + (o >> 7);
+    return i < T.W && j < T.H && k < T.D;
+}
+
+// grid-stride loop with a 32-bit index (every element count here is below 2^31
+// minus one grid stride; mp_create rejects grids that could exceed it)
+#define MP_GRID_LOOP(idx, N) for (int idx = (int)(blockIdx.x * blockDim.x + threadIdx.x); idx < (int)(N); idx += (int)(gridDim.x * blockDim.x))
 
 }  // namespace mpk

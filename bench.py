@@ -226,7 +226,11 @@ def main():
     rf, seeds = mp.scene_tables(p, args.config, replica_seed(args.seed, rank))
     rf_pin = torch.empty(rf.size, dtype=torch.float32, pin_memory=True).numpy(); rf_pin[:] = rf
     sd_pin = torch.empty(max(seeds.size, 1), dtype=torch.int32, pin_memory=True).numpy()[:seeds.size]; sd_pin[:] = seeds
-    cap_v = p.mc_max_verts; cap_i = 3 * p.mc_max_tris
+    # host mesh buffers: twice the largest mesh of the timed steps (the
+    # download reports a capacity error if a later mesh were larger)
+    st0 = sim.state()
+    cap_v = min(p.mc_max_verts, max(2 * max(st0.mc_verts), 1024))
+    cap_i = min(3 * p.mc_max_tris, max(2 * max(st0.mc_indices), 3072))
     vbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
     nbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
     ibuf = torch.empty(cap_i, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
@@ -287,6 +291,7 @@ def main():
                       "parallelism": f"replicas x{world}"},
            "roofline": roof, "pcg_hbm_gbs": pcg_gbs,
            "cg_iters_per_step": cg_iters / max(args.steps, 1),
+           "mesh": {"verts": [int(v) for v in st.mc_verts], "triangles": [int(v) // 3 for v in st.mc_indices]},
            "kernel_ms": {names[k]: {"ms": kt[k][0], "launches": kt[k][1]} for k in classes},
            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -1815,6 +1815,11 @@ int or_set_field(void* v, int f, const void* src, size_t bytes) {
     Oracle* o = (Oracle*)v;
     size_t c, e; void* ptr = o->field_ptr(f, c, e);
     if (bytes != c * e) return MP_ERR_ARG;
+    if (f == MP_F_CELLSTART || f == MP_F_CELLEND) {   // cell ranges must stay inside the particle array
+        const uint32_t* s = (const uint32_t*)src;
+        for (size_t q = 0; q < c; q++)
+            if (s[q] != UNDEF && s[q] > (uint32_t)o->np) return MP_ERR_ARG;
+    }
     if (bytes) memcpy(ptr, src, bytes);
     return MP_OK;
 }

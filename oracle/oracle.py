@@ -121,7 +121,7 @@ class Oracle:
         return a
 
     def set_field(self, name: str, a: np.ndarray):
-        dt = {"mark": np.int8, "flag": np.int8}.get(name, np.float32)
+        dt = {"mark": np.int8, "flag": np.int8, "cellstart": np.uint32, "cellend": np.uint32}.get(name, np.float32)
         a = np.ascontiguousarray(a, dt).ravel()
         self._rc(self.lib.or_set_field(self.h, self.FIELD_ID[name], _ptr(a), a.nbytes))
 
@@ -143,8 +143,11 @@ class Oracle:
         self.params = p
 
     def download_particles(self) -> Dict[str, np.ndarray]:
-        return {k: self.get_field(k) for k in ["pos", "vel", "flag", "mass", "temp", "lheat", "solubility",
-                                               "gascontain"]}
+        out = {k: self.get_field(k) for k in ["pos", "vel", "flag", "mass", "temp", "lheat", "solubility",
+                                              "gascontain"]}
+        out["pos"] = out["pos"].reshape(-1, 3)
+        out["vel"] = out["vel"].reshape(-1, 3)
+        return out
 
     # stages under the reference's names
     def initHeatAndSolubility(self): return self._rc(self.lib.or_init_particle_heat(self.h))
