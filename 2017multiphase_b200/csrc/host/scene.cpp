@@ -146,6 +146,12 @@ extern "C" int mp_scene_params(int config, int n, mp_params* p) {
         p->scene = MP_SCENE_MULTIBUBBLE;
         p->mc_every = 1;
         p->cg_max_iter = 3000;
+        // The solo-air SPH force (enforceForceSoloAirP) is explicit and its
+        // viscous part grows as 1/h^2, so a fixed step that is stable on 64^3
+        // is not on finer grids: at 256^3 and 1/240 the bubbles' particles
+        // reach hundreds of units/s within ten steps. The step shrinks with
+        // h^2 from 1/240 at 64^3 (1/3840 at 256^3).
+        if (n > 64) p->dt = (1.0f / 240.0f) * (64.0f / (float)n) * (64.0f / (float)n);
         // hundreds of bubbles: the three meshes are far larger than a few
         // surface layers of the 2x grid
         p->mc_max_verts = 64000000; p->mc_max_tris = 128000000;

@@ -114,6 +114,14 @@ struct HeatOp {
     float alpha[MP_TYPECNT];
     float dt;
     int boil;    // VACUUM neighbours also take the centre value in boiling scenes
+    // alpha of a cell type by selects (a dynamic index into the parameter
+    // array would copy it to local memory)
+    __device__ __forceinline__ float al_of(int m) const {
+        float a = alpha[0];
+        #pragma unroll
+        for (int t = 1; t < MP_TYPECNT; t++) a = (m == t) ? alpha[t] : a;
+        return a;
+    }
     __device__ __forceinline__ bool mask(int idx, int i, int j, int k) const {
         return mark[idx] != MP_TYPEBOUNDARY && inner(g, i, j, k);
     }
@@ -124,7 +132,7 @@ struct HeatOp {
     template <class R, class F>
     __device__ __forceinline__ R apply(int idx, F val) const {
         const int sI = g.NY * g.NZ, sJ = g.NZ;
-        float al = alpha[mark[idx]];
+        float al = al_of(mark[idx]);
         float h = g.h;
         R c = val(idx);
         R s = (R)(h * h / al / dt + 6.0f) * c;
@@ -139,7 +147,7 @@ struct HeatOp {
     }
     __device__ __forceinline__ bool fixed(int q) const { return fix(q); }
     template <class R> __device__ __forceinline__ R start(int idx, R c) const {
-        float al = alpha[mark[idx]];
+        float al = al_of(mark[idx]);
         float h = g.h;
         return (R)(h * h / al / dt + 6.0f) * c;
     }
@@ -344,20 +352,40 @@ __global__ void __launch_bounds__(PM_X * PM_Y) k_cg_pm(Op op, PmGeom pg, const u
         if (MODE == 1 || first) return __ldg(va + q);
         return (R)(__ldg(va + q) + bf * __ldg(vb + q));
     };
-    R behind = ld(i0 - 1, j, k), cur = ld(i0, j, k);
+    // halo slots of this thread (an edge thread of the tile owns one or two)
+    const int hyj = ty == 0 ? j - 1 : (ty == PM_Y - 1 ? j + 1 : -1);
+    const int hxk = tx == 0 ? k - 1 : (tx == PM_X - 1 ? k + 1 : -1);
+    auto ldh = [&](int i, R& hy, R& hx) {
+        if (hyj != -1) hy = ld(i, hyj, k);
+        if (hxk != -1) hx = ld(i, j, hxk);
+    };
+    auto cell = [&](int i) { return (i * g.NY + j) * g.NZ + k; };
+    // software pipeline: everything plane i needs is loaded during plane i-1,
+    // the own column's value two planes ahead
+    R behind = ld(i0 - 1, j, k), cur = ld(i0, j, k), front = ld(i0 + 1, j, k);
+    R hy = 0, hx = 0;
+    ldh(i0, hy, hx);
+    uint32_t m = (inb && i0 < i1) ? nb8[cell(i0)] : 0u;
+    R xc = 0, rc = 0;
+    if (MODE == 1 && inb && i0 < i1) { xc = x[cell(i0)]; rc = r[cell(i0)]; }
     double acc = 0;
     for (int i = i0; i < i1; i++) {
-        R front = ld(i + 1, j, k);
+        const bool more = i + 1 < i1;
+        R front2 = ld(i + 2, j, k);
+        R hyn = 0, hxn = 0;
+        if (more) ldh(i + 1, hyn, hxn);
+        uint32_t mn = 0; R xn = 0, rn = 0;
+        if (inb && more) {
+            mn = nb8[cell(i + 1)];
+            if (MODE == 1) { xn = x[cell(i + 1)]; rn = r[cell(i + 1)]; }
+        }
         __syncthreads();
         tile[ty + 1][tx + 1] = cur;
-        if (ty == 0) tile[0][tx + 1] = ld(i, j - 1, k);
-        if (ty == PM_Y - 1) tile[PM_Y + 1][tx + 1] = ld(i, j + 1, k);
-        if (tx == 0) tile[ty + 1][0] = ld(i, j, k - 1);
-        if (tx == PM_X - 1) tile[ty + 1][PM_X + 1] = ld(i, j, k + 1);
+        if (hyj != -1) tile[ty == 0 ? 0 : PM_Y + 1][tx + 1] = hy;
+        if (hxk != -1) tile[ty + 1][tx == 0 ? 0 : PM_X + 1] = hx;
         __syncthreads();
         if (inb) {
-            const int c = (i * g.NY + j) * g.NZ + k;
-            const uint32_t m = nb8[c];
+            const int c = cell(i);
             if (MODE == 0) pout[c] = (m & 0x80) ? cur : (R)0;
             if (m & 0x80) {
                 R s = op.template start<R>(c, cur);
@@ -371,8 +399,8 @@ __global__ void __launch_bounds__(PM_X * PM_Y) k_cg_pm(Op op, PmGeom pg, const u
                 if (MODE == 0) {
                     acc += (double)z * (double)cur;
                 } else {
-                    R xv = x[c] + af * cur;
-                    R rv = r[c] + (-af) * z;
+                    R xv = xc + af * cur;
+                    R rv = rc + (-af) * z;
                     x[c] = xv; r[c] = rv;
                     acc += (double)rv * (double)rv;
                 }
@@ -380,7 +408,8 @@ __global__ void __launch_bounds__(PM_X * PM_Y) k_cg_pm(Op op, PmGeom pg, const u
                 x[c] = (R)0; r[c] = (R)0;
             }
         }
-        behind = cur; cur = front;
+        behind = cur; cur = front; front = front2;
+        hy = hyn; hx = hxn; m = mn; xc = xn; rc = rn;
     }
     if (MODE == 1 && skip_dot) return;
     double tot;
@@ -481,7 +510,7 @@ __global__ void k_heat_rhs(Grid g, const float* __restrict__ Tp, float* __restri
     MP_GRID_LOOP(idx, g.n) {
         float t = Tp[idx];
         save[idx] = t;
-        float al = op.alpha[mark[idx]];
+        float al = op.al_of(mark[idx]);
         if (fixedheat && fixedheat[idx] != MP_UNDEF_TEMPERATURE) t = fixedheat[idx];
         bo[idx] = t * g.h * g.h / al / op.dt;
     }

@@ -198,12 +198,8 @@ __global__ void k_mc_inc_fill(uint32_t nidx, const uint32_t* __restrict__ idx, c
 }
 __global__ void k_mc_inc_sort(uint32_t nv, const uint32_t* __restrict__ start, uint32_t* __restrict__ inc) {
     MP_GRID_LOOP(v, nv) {
-        uint32_t s0 = start[v], s1 = start[v + 1];
-        for (uint32_t s = s0 + 1; s < s1; s++) {
-            uint32_t x = inc[s], t = s;
-            while (t > s0 && inc[t - 1] > x) { inc[t] = inc[t - 1]; t--; }
-            inc[t] = x;
-        }
+        uint32_t s0 = start[v];
+        sort_distinct_run(inc, s0, start[v + 1] - s0, [](uint32_t) {});
     }
 }
 __global__ void k_mc_smooth(uint32_t nv, const uint32_t* __restrict__ start, const uint32_t* __restrict__ inc,

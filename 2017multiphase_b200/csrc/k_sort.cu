@@ -161,14 +161,19 @@ __device__ __forceinline__ uint32_t hash_key(float4 q, float gx0, float gy0, flo
 __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, float gy0, float gz0, float dx,
                              int w, int hh, int d, uint32_t* __restrict__ keys, uint32_t* __restrict__ cnt,
                              uint32_t* __restrict__ unsorted) {
+    __shared__ uint32_t blk_unsorted;
+    if (threadIdx.x == 0) blk_unsorted = 0;
+    __syncthreads();
     MP_GRID_LOOP(p, np) {
         uint32_t key = hash_key(pos[p], gx0, gy0, gz0, dx, w, hh, d);
-        if (p > 0 && hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d) > key) *unsorted = 1u;
+        if (p > 0 && hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d) > key) blk_unsorted = 1u;
         keys[p] = key;
         // one atomic per run of equal keys in the warp (particles arrive nearly sorted)
         unsigned peers = __match_any_sync(__activemask(), key);
         if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(cnt + key, (uint32_t)__popc(peers));
     }
+    __syncthreads();
+    if (threadIdx.x == 0 && blk_unsorted) *unsorted = 1u;   // one store per block
 }
 // place each particle index in its cell's range (order inside a cell fixed later);
 // counts run back to zero, ready for the next sort
@@ -191,15 +196,9 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, int np, const uint3
 __global__ void k_segsort(const uint32_t* __restrict__ off, int ncell, uint32_t* __restrict__ perm,
                           const float4* __restrict__ pos, uint8_t* __restrict__ tmask) {
     MP_GRID_LOOP(cc, ncell) {
-        uint32_t s0 = off[cc], s1 = off[cc + 1];
+        const uint32_t s0 = off[cc];
         uint32_t m = 0;
-        for (uint32_t s = s0 + 1; s < s1; s++) {
-            uint32_t v = perm[s];
-            uint32_t t = s;
-            while (t > s0 && perm[t - 1] > v) { perm[t] = perm[t - 1]; t--; }
-            perm[t] = v;
-        }
-        for (uint32_t s = s0; s < s1; s++) m |= 1u << (pflag(__ldg(pos + perm[s])) & 7);
+        sort_distinct_run(perm, s0, off[cc + 1] - s0, [&](uint32_t v) { m |= 1u << (pflag(__ldg(pos + v)) & 7); });
         tmask[cc] = (uint8_t)m;
     }
 }

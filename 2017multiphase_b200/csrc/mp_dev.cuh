@@ -153,4 +153,37 @@ MPD bool tile_ijk(const Tiles& T, int t, int& i, int& j, int& k) {
 // minus one grid stride; mp_create rejects grids that could exceed it)
 #define MP_GRID_LOOP(idx, N) for (int idx = (int)(blockIdx.x * blockDim.x + threadIdx.x); idx < (int)(N); idx += (int)(gridDim.x * blockDim.x))
 
+// Sorts the DISTINCT values a[s0 .. s0+cnt) ascending and calls each(v) once
+// per value. Up to RUN_REG values are loaded together into registers and each
+// is stored at its rank (the count of smaller values), so a short run costs
+// one round trip to memory instead of a chain of dependent ones; longer runs
+// use an insertion sort in place.
+constexpr int RUN_REG = 16;
+template <class F>
+__device__ __forceinline__ void sort_distinct_run(uint32_t* a, uint32_t s0, uint32_t cnt, F each) {
+    if (cnt <= (uint32_t)RUN_REG) {
+        uint32_t v[RUN_REG];
+        #pragma unroll
+        for (int q = 0; q < RUN_REG; q++) v[q] = (q < (int)cnt) ? a[s0 + q] : 0xffffffffu;
+        #pragma unroll
+        for (int q = 0; q < RUN_REG; q++) {
+            if (q < (int)cnt) {
+                uint32_t rk = 0;
+                #pragma unroll
+                for (int t = 0; t < RUN_REG; t++) rk += (v[t] < v[q]) ? 1u : 0u;
+                a[s0 + rk] = v[q];
+                each(v[q]);
+            }
+        }
+        return;
+    }
+    const uint32_t s1 = s0 + cnt;
+    for (uint32_t s = s0 + 1; s < s1; s++) {
+        uint32_t x = a[s], t = s;
+        while (t > s0 && a[t - 1] > x) { a[t] = a[t - 1]; t--; }
+        a[t] = x;
+    }
+    for (uint32_t s = s0; s < s1; s++) each(a[s]);
+}
+
 }  // namespace mpk

@@ -284,7 +284,8 @@ def main():
            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (CG dots, alpha/beta in f64)", "data": "synthetic",
            "config": {"workload": f"bubble column {p.nx}^3: liquid z<0.8, 200 air bubbles r~U[0.01,0.04], "
-                                  f"8 jittered particles/cell, dt=1/240, FLIP 0.95, CG rel 1e-6 (FP32 vectors, "
+                                  f"8 jittered particles/cell, dt=1/{1.0 / p.dt:.0f} (1/240 x (64/n)^2), FLIP 0.95, "
+                                  f"CG rel 1e-6 (FP32 vectors, "
                                   f"FP64 dots), marching cubes every step",
                       "grid": p.nx, "particles": int(st.par_num_now), "seed": args.seed,
                       "l2": "inputs larger than L2 (particle streams alone are ~5 GB)",

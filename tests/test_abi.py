@@ -89,7 +89,9 @@ def test_bad_arguments_are_rejected_without_a_gpu(mp):
 def test_scene_presets(mp):
     for cfg, n in [(1, 32), (2, 64), (3, 128), (4, 64), (5, 256)]:
         p = mp.scene_params(cfg, 0)
-        assert p.nx == n and abs(p.cellsize - 1.0 / n) < 1e-9 and abs(p.dt - 1 / 240) < 1e-9
+        # configuration 5 shrinks the step with h^2 below 64^3 cells per side
+        dt = 1 / 240 if cfg < 5 else (1 / 240) * (64 / n) ** 2
+        assert p.nx == n and abs(p.cellsize - 1.0 / n) < 1e-9 and abs(p.dt - dt) < 1e-9
     p = mp.scene_params(2, 0)
     assert p.b_gen_gas and p.b_heat_trans and p.b_fixed_heat and p.boiling_point == 1.0
     p = mp.scene_params(3, 0)
