@@ -17,6 +17,7 @@
 // Dot products are FP64 block sums finished by the last block in block order,
 // so they are deterministic. Vectors are FP32 (MP_PREC_MIXED) or FP64.
 #include "ctx.cuh"
+#include <type_traits>
 
 using namespace mpk;
 
@@ -428,6 +429,104 @@ __global__ void __launch_bounds__(PM_X * PM_Y) k_cg_pm(Op op, PmGeom pg, const u
     }
 }
 
+// ---- four cells along k per thread (FP32 vectors, NZ a multiple of 4) ---------
+// The same two passes as k_cg_pm without shared memory or barriers: a thread
+// owns one aligned float4 group of a k-row, loads the centre group, the four
+// +-i / +-j groups and the two k-edge scalars, and applies the row of each of
+// its four cells in the order of PressOp/HeatOp::apply. Groups without an
+// unknown are skipped entirely: x, r and both direction vectors are zero
+// there for the whole solve (x and the direction vectors are cleared at the
+// start, r by k_cg_init), and nothing writes them.
+template <class Op, int MODE>
+__global__ void __launch_bounds__(CG_T) k_cg_v4(Op op, const uint8_t* __restrict__ nb8,
+                                                const float* __restrict__ va, const float* __restrict__ vb,
+                                                float* __restrict__ pout, float* __restrict__ x, float* __restrict__ r,
+                                                Red Rd, int first, int it, int maxiter, int skip_dot) {
+    if (Rd.flag[F_DONE] != DONE_RUN) return;
+    const Grid& g = op.g;
+    const int NZ4 = g.NZ >> 2, sJ4 = NZ4, sI4 = g.NY * NZ4, ng = g.n >> 2;
+    const float bf = (MODE == 0 && !first) ? (float)Rd.scal[S_BETA] : 0.0f;
+    const float af = MODE == 1 ? (float)Rd.scal[S_ALPHA] : 0.0f;
+    const float4* __restrict__ a4 = reinterpret_cast<const float4*>(va);
+    const float4* __restrict__ b4 = reinterpret_cast<const float4*>(vb);
+    auto val4 = [&](int q) -> float4 {
+        float4 a = __ldg(a4 + q);
+        if (MODE == 1 || first) return a;
+        float4 b = __ldg(b4 + q);
+        return make_float4(a.x + bf * b.x, a.y + bf * b.y, a.z + bf * b.z, a.w + bf * b.w);
+    };
+    auto val1 = [&](int q) -> float {
+        if (MODE == 1 || first) return __ldg(va + q);
+        return __ldg(va + q) + bf * __ldg(vb + q);
+    };
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    double acc = 0;
+    MP_GRID_LOOP(q, ng) {
+        const uint32_t m4 = __ldg(reinterpret_cast<const uint32_t*>(nb8) + q);
+        if (!(m4 & 0x80808080u)) continue;
+        const int row = q / NZ4, kq = q - row * NZ4;
+        const int i = row / g.NY, j = row - i * g.NY;
+        const float4 c = val4(q);
+        const float4 xp = i + 1 < g.NX ? val4(q + sI4) : zero4;
+        const float4 xm = i > 0 ? val4(q - sI4) : zero4;
+        const float4 yp = j + 1 < g.NY ? val4(q + sJ4) : zero4;
+        const float4 ym = j > 0 ? val4(q - sJ4) : zero4;
+        const float zm = kq > 0 ? val1(4 * q - 1) : 0.0f;
+        const float zp = kq + 1 < NZ4 ? val1(4 * q + 4) : 0.0f;
+        float4 xo = zero4, ro = zero4;
+        if (MODE == 1) { xo = reinterpret_cast<const float4*>(x)[q]; ro = reinterpret_cast<const float4*>(r)[q]; }
+        const float cv[6] = {zm, c.x, c.y, c.z, c.w, zp};
+        const float xpv[4] = {xp.x, xp.y, xp.z, xp.w}, xmv[4] = {xm.x, xm.y, xm.z, xm.w};
+        const float ypv[4] = {yp.x, yp.y, yp.z, yp.w}, ymv[4] = {ym.x, ym.y, ym.z, ym.w};
+        float xov[4] = {xo.x, xo.y, xo.z, xo.w}, rov[4] = {ro.x, ro.y, ro.z, ro.w};
+        float po[4];
+        #pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const uint32_t m = (m4 >> (8 * e)) & 0xffu;
+            const float cur = cv[e + 1];
+            po[e] = (m & 0x80) ? cur : 0.0f;
+            if (m & 0x80) {
+                float s = op.template start<float>(4 * q + e, cur);
+                s = op.template comb<float>(s, (m & 1) ? cur : xpv[e]);
+                s = op.template comb<float>(s, (m & 2) ? cur : ypv[e]);
+                s = op.template comb<float>(s, (m & 4) ? cur : cv[e + 2]);
+                s = op.template comb<float>(s, (m & 8) ? cur : xmv[e]);
+                s = op.template comb<float>(s, (m & 16) ? cur : ymv[e]);
+                s = op.template comb<float>(s, (m & 32) ? cur : cv[e]);
+                const float z = op.template finish<float>(s);
+                if (MODE == 0) {
+                    acc += (double)z * (double)cur;
+                } else {
+                    xov[e] = xov[e] + af * cur;
+                    rov[e] = rov[e] + (-af) * z;
+                    acc += (double)rov[e] * (double)rov[e];
+                }
+            }
+        }
+        if (MODE == 0) {
+            reinterpret_cast<float4*>(pout)[q] = make_float4(po[0], po[1], po[2], po[3]);
+        } else {
+            reinterpret_cast<float4*>(x)[q] = make_float4(xov[0], xov[1], xov[2], xov[3]);
+            reinterpret_cast<float4*>(r)[q] = make_float4(rov[0], rov[1], rov[2], rov[3]);
+        }
+    }
+    if (MODE == 1 && skip_dot) return;
+    double tot;
+    if (finish_sum(Rd, acc, &tot)) {
+        if (MODE == 0) {
+            Rd.scal[S_ZP] = tot;
+            if (tot == 0) Rd.flag[F_DONE] = DONE_ZP0;
+            else Rd.scal[S_ALPHA] = Rd.scal[S_A] / tot;
+        } else {
+            Rd.scal[S_RR] = tot;
+            Rd.flag[F_ITERS] = it + 1;
+            if (tot < Rd.scal[S_EPS]) Rd.flag[F_DONE] = DONE_CONV;
+            else if (it + 1 >= maxiter) Rd.flag[F_DONE] = DONE_CAP;
+            else { Rd.scal[S_BETA] = tot / Rd.scal[S_A]; Rd.scal[S_A] = tot; }
+        }
+    }
+}
+
 // cptdivergence_bubble2 (spray_k.cu:3138-3263)
 template <class R>
 __global__ void k_divergence(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ ls,
@@ -565,6 +664,16 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     PmGeom pg{chunk};
     dim3 pmg((gg.NZ + PM_X - 1) / PM_X, (gg.NY + PM_Y - 1) / PM_Y, (gg.NX + chunk - 1) / chunk);
     if ((long long)pmg.x * pmg.y * pmg.z > 148LL * 32) { c->err = "cg: tiling exceeds partials buffer"; return MP_ERR_CAPACITY; }
+    // FP32 vectors on a grid whose k-rows split into float4 groups take the
+    // four-cells-per-thread kernels; they never write the direction vectors
+    // outside the unknowns, so both start cleared
+    constexpr bool kF32 = std::is_same<R, float>::value;
+    const bool v4 = kF32 && gg.NZ % 4 == 0;
+    const int nbv = (int)std::min<long long>(c->red_blocks, ((long long)(n / 4) + CG_T - 1) / CG_T);
+    if (v4) {
+        MP_CUDA(c, cudaMemsetAsync(p0, 0, sizeof(R) * n, s));
+        MP_CUDA(c, cudaMemsetAsync(p1, 0, sizeof(R) * n, s));
+    }
     unsigned int hflag[F_COUNT] = {0, 0};
     MP_CUDA(c, cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s));
     MP_CUDA(c, cudaStreamSynchronize(s));
@@ -574,15 +683,31 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
         int end = std::min(maxiter, it + batch);
         for (; it < end; it++) {
             bool tr = true_every > 0 && (it + 1) % true_every == 0;
-            {
-                KtScope kt(c, kt_stencil);
-                k_cg_pm<R, Op, 0><<<pmg, pmb, 0, s>>>(op, pg, nb8, r, pa, pb, nullptr, nullptr, Rd,
-                                                      it == 0 ? 1 : 0, it, maxiter, 0);
+            if constexpr (kF32) {
+                if (v4) {
+                    {
+                        KtScope kt(c, kt_stencil);
+                        k_cg_v4<Op, 0><<<nbv, CG_T, 0, s>>>(op, nb8, r, pa, pb, nullptr, nullptr, Rd,
+                                                            it == 0 ? 1 : 0, it, maxiter, 0);
+                    }
+                    {
+                        KtScope kt(c, MP_KT_CG_UPDATE);
+                        k_cg_v4<Op, 1><<<nbv, CG_T, 0, s>>>(op, nb8, pb, nullptr, nullptr, x, r, Rd, 0, it, maxiter,
+                                                            tr ? 1 : 0);
+                    }
+                }
             }
-            {
-                KtScope kt(c, MP_KT_CG_UPDATE);
-                k_cg_pm<R, Op, 1><<<pmg, pmb, 0, s>>>(op, pg, nb8, pb, nullptr, nullptr, x, r, Rd, 0, it, maxiter,
-                                                      tr ? 1 : 0);
+            if (!v4) {
+                {
+                    KtScope kt(c, kt_stencil);
+                    k_cg_pm<R, Op, 0><<<pmg, pmb, 0, s>>>(op, pg, nb8, r, pa, pb, nullptr, nullptr, Rd,
+                                                          it == 0 ? 1 : 0, it, maxiter, 0);
+                }
+                {
+                    KtScope kt(c, MP_KT_CG_UPDATE);
+                    k_cg_pm<R, Op, 1><<<pmg, pmb, 0, s>>>(op, pg, nb8, pb, nullptr, nullptr, x, r, Rd, 0, it, maxiter,
+                                                          tr ? 1 : 0);
+                }
             }
             if (tr) k_cg_true<R, Op><<<nb, CG_T, 0, s>>>(op, n, b, x, r, Rd, it, maxiter);
             c->launches += tr ? 3 : 2;
