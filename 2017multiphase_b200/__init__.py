@@ -133,6 +133,8 @@ def load_library() -> C.CDLL:
         "mp_sweep_u": ([vp, C.c_int], C.c_int),
         "mp_set_boundary_u": ([vp, C.c_int], C.c_int),
         "mp_project": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
+        "mp_pressure_cg_static": ([C.c_int, C.c_int, C.c_int, C.c_float, vp, vp, vp, C.c_int, C.c_int, C.c_float, vp,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
         "mp_mc": ([vp, C.c_int], C.c_int),
         "mp_mc_download": ([vp, C.c_int, vp, vp, vp, C.c_int, C.c_int], C.c_int),
         "mp_mc_download_field": ([vp, vp, vp], C.c_int),

@@ -262,6 +262,8 @@ static int check_params(const mp_params* p, std::string& err) {
 }
 
 static thread_local std::string g_create_err;
+// context-free calls report through the same slot (mp_last_error(NULL, ...))
+void mp_internal_set_global_error(const char* msg) { g_create_err = msg; }
 
 extern "C" int mp_create(const mp_params* p, void** ctx) {
     if (!ctx) return MP_ERR_ARG;

@@ -17,6 +17,9 @@
 // Dot products are FP64 block sums finished by the last block in block order,
 // so they are deterministic. Vectors are FP32 (MP_PREC_MIXED) or FP64.
 #include "ctx.cuh"
+#include <cstdint>
+#include <mutex>
+#include <string>
 #include <type_traits>
 
 using namespace mpk;
@@ -811,4 +814,145 @@ int k_heat(MpCtx* c) {
     MP_TRY(k_heat_g2p_launch(c));
     MP_TRY(k_latent_heat(c));
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Pressure CG without allocation (mp_pressure_cg_static)
+// ---------------------------------------------------------------------------
+// For callers that may not allocate device memory: the solve of mp_project on
+// caller-owned arrays, with every working vector in one fixed array that this
+// library holds on each GPU it is loaded on, for the life of the process.
+// Layout of the array (byte offsets, each part 256-byte aligned).
+namespace {
+constexpr int NA_MAX_CELLS = 64 * 64 * 64;                 // 262,144 cells
+constexpr int NA_MAX_BLOCKS = 148 * 32;                    // = the partial sums of mp_blocks()
+constexpr size_t na_up(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t NA_PART = 0;                                            // double[NA_MAX_BLOCKS]
+constexpr size_t NA_SCAL = na_up(NA_PART + sizeof(double) * NA_MAX_BLOCKS);   // double[8]
+constexpr size_t NA_COUNT = na_up(NA_SCAL + sizeof(double) * 8);         // uint32: counter, flags
+constexpr size_t NA_COUNT_BYTES = 64;
+constexpr size_t NA_NB8 = na_up(NA_COUNT + NA_COUNT_BYTES);             // uint8[cells]
+constexpr size_t NA_R = na_up(NA_NB8 + NA_MAX_CELLS);                   // float[cells] x 3
+constexpr size_t NA_P0 = na_up(NA_R + sizeof(float) * NA_MAX_CELLS);
+constexpr size_t NA_P1 = na_up(NA_P0 + sizeof(float) * NA_MAX_CELLS);
+constexpr size_t NA_BYTES = na_up(NA_P1 + sizeof(float) * NA_MAX_CELLS);   // about 3.3 MB
+}  // namespace
+
+// The scratch itself. In host code this name is only a stand-in for the
+// device symbol: its device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char mp_cg_static_scratch[NA_BYTES];
+
+void mp_internal_set_global_error(const char* msg);
+
+namespace {
+constexpr int NA_MAX_DEVICES = 256;
+std::mutex na_mu;
+void* na_addr[NA_MAX_DEVICES] = {};
+
+// Device address of the scratch on the current device, looked up once per
+// device (the first call on a device does this).
+cudaError_t na_scratch(unsigned char** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(na_mu);
+    if (!na_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, mp_cg_static_scratch);
+        if (e != cudaSuccess) return e;
+        na_addr[dev] = p;
+    }
+    *out = static_cast<unsigned char*>(na_addr[dev]);
+    return cudaSuccess;
+}
+}  // namespace
+
+extern "C" int mp_pressure_cg_static(int nx, int ny, int nz, float cellsize, const int8_t* mark,
+                                     const float* divergence, float* pressure, int max_iter, int tol_mode, float tol,
+                                     void* stream, int* iters, double* residual) {
+    auto fail = [](int rc, const std::string& msg) { mp_internal_set_global_error(msg.c_str()); return rc; };
+    auto cuda_fail = [&](cudaError_t e, const char* what) {
+        return fail(MP_ERR_CUDA, std::string("mp_pressure_cg_static: ") + what + ": " + cudaGetErrorString(e));
+    };
+    if (nx < 3 || ny < 3 || nz < 3 || !(cellsize > 0) || !mark || !divergence || !pressure || max_iter < 0 ||
+        (tol_mode != MP_TOL_REF_ABS && tol_mode != MP_TOL_REL))
+        return fail(MP_ERR_ARG, "mp_pressure_cg_static: bad grid, pointer, iteration cap or tolerance mode");
+    const long long nll = (long long)nx * ny * nz;
+    if (nll > NA_MAX_CELLS)
+        return fail(MP_ERR_CAPACITY, "mp_pressure_cg_static: " + std::to_string(nll) + " cells exceed the " +
+                                         std::to_string(NA_MAX_CELLS) + "-cell limit of its fixed scratch");
+    const int n = (int)nll;
+    unsigned char* base = nullptr;
+    cudaError_t e = na_scratch(&base);
+    if (e != cudaSuccess) return cuda_fail(e, "scratch address");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    Grid g{};
+    g.NX = nx; g.NY = ny; g.NZ = nz; g.n = n;
+    g.nfx = (nx + 1) * ny * nz; g.nfy = nx * (ny + 1) * nz; g.nfz = nx * ny * (nz + 1);
+    g.h = cellsize;
+    PressOp op{g, mark};
+    Red Rd{reinterpret_cast<double*>(base + NA_PART), reinterpret_cast<unsigned int*>(base + NA_COUNT),
+           reinterpret_cast<double*>(base + NA_SCAL), reinterpret_cast<unsigned int*>(base + NA_COUNT) + 1};
+    uint8_t* nb8 = base + NA_NB8;
+    float* r = reinterpret_cast<float*>(base + NA_R);
+    float* pa = reinterpret_cast<float*>(base + NA_P0);
+    float* pb = reinterpret_cast<float*>(base + NA_P1);
+
+    // the scratch keeps the previous call's contents: clear the block counter,
+    // the stop flags, the direction vectors and the solution
+    if ((e = cudaMemsetAsync(base + NA_COUNT, 0, NA_COUNT_BYTES, s)) != cudaSuccess) return cuda_fail(e, "clear");
+    if ((e = cudaMemsetAsync(pa, 0, sizeof(float) * n, s)) != cudaSuccess) return cuda_fail(e, "clear");
+    if ((e = cudaMemsetAsync(pb, 0, sizeof(float) * n, s)) != cudaSuccess) return cuda_fail(e, "clear");
+    if ((e = cudaMemsetAsync(pressure, 0, sizeof(float) * n, s)) != cudaSuccess) return cuda_fail(e, "clear");
+
+    const int nb = mp_blocks(n, 256);
+    k_cg_init<float, PressOp><<<nb, CG_T, 0, s>>>(op, n, divergence, r, Rd, tol_mode, tol);
+    k_nb8<PressOp><<<mp_blocks(n, 256), 256, 0, s>>>(op, n, nb8);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "launch");
+    const bool v4 = nz % 4 == 0 && reinterpret_cast<uintptr_t>(divergence) % 16 == 0 &&
+                    reinterpret_cast<uintptr_t>(pressure) % 16 == 0;
+    const int nbv = (int)std::min<long long>(nb, ((long long)(n / 4) + CG_T - 1) / CG_T);
+    dim3 pmb(PM_X, PM_Y);
+    int tiles = ((nz + PM_X - 1) / PM_X) * ((ny + PM_Y - 1) / PM_Y);
+    int chunk = std::max(4, (int)((nx * (long long)tiles + 4095) / 4096));
+    PmGeom pg{chunk};
+    dim3 pmg((nz + PM_X - 1) / PM_X, (ny + PM_Y - 1) / PM_Y, (nx + chunk - 1) / chunk);
+
+    unsigned int hflag[F_COUNT] = {0, 0};
+    if ((e = cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_fail(e, "stop flag");
+    int it = 0, batch = 8;
+    while (hflag[F_DONE] == DONE_RUN && it < max_iter) {
+        int end = std::min(max_iter, it + batch);
+        for (; it < end; it++) {
+            if (v4) {
+                k_cg_v4<PressOp, 0><<<nbv, CG_T, 0, s>>>(op, nb8, r, pa, pb, nullptr, nullptr, Rd, it == 0 ? 1 : 0,
+                                                         it, max_iter, 0);
+                k_cg_v4<PressOp, 1><<<nbv, CG_T, 0, s>>>(op, nb8, pb, nullptr, nullptr, pressure, r, Rd, 0, it,
+                                                         max_iter, 0);
+            } else {
+                k_cg_pm<float, PressOp, 0><<<pmg, pmb, 0, s>>>(op, pg, nb8, r, pa, pb, nullptr, nullptr, Rd,
+                                                               it == 0 ? 1 : 0, it, max_iter, 0);
+                k_cg_pm<float, PressOp, 1><<<pmg, pmb, 0, s>>>(op, pg, nb8, pb, nullptr, nullptr, pressure, r, Rd, 0,
+                                                               it, max_iter, 0);
+            }
+            std::swap(pa, pb);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "launch");
+        if ((e = cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_fail(e, "stop flag");
+        if (batch < 64) batch *= 2;
+    }
+    double rr = 0;
+    if ((e = cudaMemcpyAsync(&rr, Rd.scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_fail(e, "result");
+    if (iters) *iters = (int)hflag[F_ITERS];
+    if (residual) *residual = rr;
+    return hflag[F_DONE] == DONE_CAP ? MP_ERR_NOCONVERGE : MP_OK;
 }

@@ -294,6 +294,30 @@ int mp_sweep_phi(void* ctx, int phase);      /* sweepPhi  (phase = MP_TYPEFLUID|
 int mp_sweep_u(void* ctx, int phase);        /* sweepU                spray.cu:585  */
 int mp_set_boundary_u(void* ctx, int phase); /* setWaterBoundaryU     spray.cu:605  */
 int mp_project(void* ctx, int* iters, double* residual); /* project_CG_bubble spray.cu:1590 */
+/* The pressure CG of mp_project as a standalone call that allocates nothing
+ * (no cudaMalloc, cudaFree or allocating library routine). No counterpart in
+ * the reference. It is for callers that cannot allocate device memory while
+ * they run: code embedded in a host application that owns a fixed device
+ * budget (its own memory pool, or the rest of the GPU already taken), and
+ * code inside a frame or stream loop where cudaFree, which synchronises the
+ * whole device, would stall everything else on the GPU.
+ * The caller passes device arrays of nx*ny*nz cells: mark (int8, MP_TYPE*),
+ * divergence (float, the right-hand side mp_project builds, field MP_F_DIV)
+ * and pressure (float, written). The stop rule is mp_project's (tol_mode,
+ * tol, max_iter); iters and residual as there. Runs on `stream` (NULL: the
+ * default stream) and returns after it has finished.
+ * All working storage (residual, two direction vectors, neighbour bytes,
+ * reduction partials) lives in one fixed array of about 3.3 MB that the
+ * library holds on every GPU it is loaded on, until the process exits; grids
+ * above 262,144 cells (64^3) are rejected with MP_ERR_CAPACITY. The first call
+ * on a device looks up that array's device address; make that first call
+ * before any stream capture. Every call reuses the same array (the parts that
+ * must start at zero are cleared at each call), so calls whose GPU work
+ * overlaps, from other streams or host threads on the same device, race and
+ * give wrong results. Errors are read with mp_last_error(NULL, ...). */
+int mp_pressure_cg_static(int nx, int ny, int nz, float cellsize, const int8_t* mark,
+                          const float* divergence, float* pressure, int max_iter, int tol_mode,
+                          float tol, void* stream, int* iters, double* residual);
 int mp_g2p(void* ctx);                       /* mapvelg2p_bubble      spray.cu:1689 */
 int mp_solid_motion(void* ctx);              /* solidmotion[_fixed]   spray.cu:2685 */
 int mp_solo_air_update(void* ctx);           /* updateSoloAirParticle spray.cu:2620 */
