@@ -134,7 +134,7 @@ static void free_all(MpCtx* c) {
                     c->cell_tmp, c->mark, c->mark_tmp, c->cg_r, c->cg_p, c->cg_z, c->cg64, c->red, c->scal, c->red_count,
                     c->pos, c->vel, c->heat, c->pos2, c->vel2, c->heat2, c->pdens, c->pprs, c->pscr, c->pscr2,
                     c->flag_snap, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->scan_tmp, c->u32_scratch,
-                    c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_cube, c->mc_vflag, c->mc_vscan,
+                    c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_dens2, c->mc_cube, c->mc_vflag, c->mc_vscan,
                     c->mc_compact, c->mc_vverts, c->mc_vvscan, c->mc_emark, c->mc_escan, c->mc_vstart, c->mc_inc,
                     c->mc_fill, c->mc_tmpv};
     for (void* p : ptrs) if (p) cudaFree(p);
@@ -218,7 +218,7 @@ static int create_impl(MpCtx* c, const mp_params* p) {
         size_t nnode = (size_t)(2 * g.NX + 1) * (2 * g.NY + 1) * (2 * g.NZ + 1);
         size_t nvox = 8 * n;
         c->mc_edges = 3 * nnode;
-        MP_TRY(dalloc_t(c, &c->mc_dens, nnode));
+        MP_TRY(dalloc_t(c, &c->mc_dens, nnode)); MP_TRY(dalloc_t(c, &c->mc_dens2, nnode));
         MP_TRY(dalloc_t(c, &c->mc_cube, nvox));
         MP_TRY(dalloc_t(c, &c->mc_vflag, nvox)); MP_TRY(dalloc_t(c, &c->mc_vscan, nvox + 1));
         MP_TRY(dalloc_t(c, &c->mc_compact, nvox));
@@ -671,7 +671,8 @@ extern "C" int mp_mc_download_field(void* ctx, float* dens, uint8_t* cube) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     if (!c->P.b_run_mc) return MP_ERR_STATE;
     size_t nnode = (size_t)(2 * c->G.NX + 1) * (2 * c->G.NY + 1) * (2 * c->G.NZ + 1), nvox = 8 * (size_t)c->G.n;
-    if (dens) MP_CUDA(c, cudaMemcpyAsync(dens, c->mc_dens, 4 * nnode, cudaMemcpyDeviceToHost, c->stream));
+    const float* src = c->mc_last_dens ? c->mc_last_dens : c->mc_dens;
+    if (dens) MP_CUDA(c, cudaMemcpyAsync(dens, src, 4 * nnode, cudaMemcpyDeviceToHost, c->stream));
     if (cube) MP_CUDA(c, cudaMemcpyAsync(cube, c->mc_cube, nvox, cudaMemcpyDeviceToHost, c->stream));
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
     return MP_OK;
@@ -720,7 +721,8 @@ extern "C" int mp_step(void* ctx) {
     if (P.b_freeze) MP_TRY(k_freeze(c));
     if (P.b_run_mc && P.mc_every > 0 && c->S.frame % P.mc_every == 0) {
         MP_TRY(k_mc_presort(c));
-        for (int s = 0; s < 3; s++) MP_TRY(k_mc(c, s));
+        MP_TRY(k_mc(c, MP_MC_SOLID));
+        MP_TRY(k_mc_fluid_gas(c));
     }
     c->S.frame++;
     MP_CUDA(c, cudaStreamSynchronize(c->stream));

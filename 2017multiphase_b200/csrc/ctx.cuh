@@ -67,6 +67,8 @@ struct MpCtx {
     int32_t *mc_numverts = 0, *mc_tri = 0;
     // marching cubes
     float *mc_dens = 0;
+    float *mc_dens2 = 0;              // gas field of the fused fluid+gas density pass
+    const float* mc_last_dens = 0;    // field of the last extraction
     uint8_t *mc_cube = 0;
     uint32_t *mc_vflag = 0, *mc_vscan = 0, *mc_compact = 0, *mc_vverts = 0, *mc_vvscan = 0;
     uint32_t *mc_emark = 0, *mc_escan = 0;
@@ -157,6 +159,7 @@ int k_delete(MpCtx* c);
 int k_melt(MpCtx* c);
 int k_freeze(MpCtx* c);
 int k_mc(MpCtx* c, int surface);
+int k_mc_fluid_gas(MpCtx* c);
 int k_init_particle_heat(MpCtx* c);
 int k_pack_particles(MpCtx* c, int n, const float* pos3, const float* vel3, const int8_t* flag,
                      const float* mass, const float* T, const float* L, const float* sol, const float* gas);

@@ -29,9 +29,14 @@ struct McGrid {
     Tiles T;                // 3-D tiling of the nodes for the density gather
 };
 
-template <int SURF>
+// GAS2 (with SURF == MP_MC_FLUID): the gas field is accumulated in the same
+// pass into dens2. Both surfaces use the same radius and weight, the gas
+// particles are a subset of the fluid ones, and each sum keeps its own
+// accumulators in the same visiting order, so both fields equal the separate
+// passes bit for bit.
+template <int SURF, bool GAS2 = false>
 __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const float4* __restrict__ pos, float* __restrict__ dens,
-                                                    int scene) {
+                                                    int scene, float* __restrict__ dens2 = nullptr) {
     const Tiles T = m.T;
     const float hm = m.hm;
     const uint32_t need = SURF == MP_MC_SOLID ? (1u << MP_TYPESOLID)
@@ -40,8 +45,8 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
     MP_GRID_LOOP(t, T.threads()) {
         int i, j, k; if (!tile_ijk(T, t, i, j, k)) continue;
         float3 p = mk3((float)i, (float)j, (float)k) * hm;
-        float3 center = mk3(0.0f);
-        float wsum = 0.0f;
+        float3 center = mk3(0.0f), center2 = mk3(0.0f);
+        float wsum = 0.0f, wsum2 = 0.0f;
         for (int di = -2; di <= 1; ++di) {
             int a = i + di; if (a < 0 || a > m.NXMC - 1) continue;
             for (int dj = -2; dj <= 1; ++dj) {
@@ -50,7 +55,7 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
                     int cc = k + dk; if (cc < 0 || cc > m.NZMC - 1) continue;
                     int c = a * m.NYMC * m.NZMC + b * m.NZMC + cc;
                     if (!(__ldg(cl.tmask + c) & need)) continue;
-                    float3 res = mk3(0.0f);
+                    float3 res = mk3(0.0f), res2 = mk3(0.0f);
                     for (uint32_t q = __ldg(cl.off + c); q < __ldg(cl.off + c + 1); ++q) {
                         float4 o = __ldg(pos + q);
                         int f = pflag(o);
@@ -80,10 +85,14 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
                                 float w = R * R - dis * dis;
                                 w = w * w * w;
                                 res += op * w; wsum += w;
+                                if (GAS2 && (f == MP_TYPEAIR || (f == MP_TYPEAIRSOLO && scene != MP_SCENE_INTERACTION))) {
+                                    res2 += op * w; wsum2 += w;
+                                }
                             }
                         }
                     }
                     center += res;
+                    if (GAS2) center2 += res2;
                 }
             }
         }
@@ -104,6 +113,14 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
             if (wsum > 0) { center /= wsum; phi = r - length(p - center); }
             else phi = -r;
             if (border) phi = -1000.0f;
+            if (GAS2) {
+                const float r2 = 0.8f * hm;
+                float phi2;
+                if (wsum2 > 0) { center2 /= wsum2; phi2 = r2 - length(p - center2); }
+                else phi2 = -r2;
+                if (border) phi2 = -1000.0f;
+                dens2[(i * m.H + j) * m.D + k] = phi2;
+            }
         }
         dens[(i * m.H + j) * m.D + k] = phi;
     }
@@ -242,28 +259,59 @@ static int readback(MpCtx* c, const uint32_t* dptr, uint32_t* h) {
     return MP_OK;
 }
 
-// one runMC_smooth surface (spray.cu:804-979)
-int k_mc(MpCtx* c, int surface) {
-    if (!c->mc_sorted) { c->err = "mc: particles are not sorted on the 2x grid (call mp_mc_presort)"; return MP_ERR_STATE; }
+static McGrid mc_grid(const MpCtx* c) {
     McGrid m;
     m.NXMC = 2 * c->G.NX; m.NYMC = 2 * c->G.NY; m.NZMC = 2 * c->G.NZ;
     m.W = m.NXMC + 1; m.H = m.NYMC + 1; m.D = m.NZMC + 1;
     m.hm = c->G.h / (float)(m.NXMC / c->G.NX);
     m.T = make_tiles(m.W, m.H, m.D);
+    return m;
+}
+static int mc_extract(MpCtx* c, const McGrid& m, int surface, const float* dens);
+
+// one runMC_smooth surface (spray.cu:804-979)
+int k_mc(MpCtx* c, int surface) {
+    if (!c->mc_sorted) { c->err = "mc: particles are not sorted on the 2x grid (call mp_mc_presort)"; return MP_ERR_STATE; }
+    const McGrid m = mc_grid(c);
     Cells cl{c->cell_off, c->tmask};
-    long long nnode = (long long)m.W * m.H * m.D;
-    long long nvox = (long long)m.NXMC * m.NYMC * m.NZMC;
     cudaStream_t s = c->stream;
-    McSurface& out = c->mc[surface];
-    out.nverts = out.nindices = out.active = 0;
     {
         KtScope kt(c, MP_KT_MC_DENS);
         if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
         else if (surface == MP_MC_FLUID) k_mc_density<MP_MC_FLUID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
         else k_mc_density<MP_MC_GAS><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
     }
-    k_mc_classify<<<mp_blocks(nvox, 256), 256, 0, s>>>(m, c->mc_dens, c->mc_numverts, c->mc_cube, c->mc_vverts, c->mc_vflag);
-    c->launches += 2;
+    c->launches++;
+    return mc_extract(c, m, surface, c->mc_dens);
+}
+
+// the fluid and gas surfaces of one step from a single density pass (the
+// same fields and meshes as k_mc(FLUID) followed by k_mc(GAS))
+int k_mc_fluid_gas(MpCtx* c) {
+    if (!c->mc_sorted) { c->err = "mc: particles are not sorted on the 2x grid (call mp_mc_presort)"; return MP_ERR_STATE; }
+    const McGrid m = mc_grid(c);
+    Cells cl{c->cell_off, c->tmask};
+    {
+        KtScope kt(c, MP_KT_MC_DENS);
+        k_mc_density<MP_MC_FLUID, true><<<mp_blocks(m.T.threads(), 256), 256, 0, c->stream>>>(m, cl, c->pos, c->mc_dens,
+                                                                                               c->P.scene, c->mc_dens2);
+    }
+    c->launches++;
+    MP_TRY(mc_extract(c, m, MP_MC_FLUID, c->mc_dens));
+    return mc_extract(c, m, MP_MC_GAS, c->mc_dens2);
+}
+
+// classification, compaction, vertices, indices, smoothing and normals of one
+// surface from its nodal field
+static int mc_extract(MpCtx* c, const McGrid& m, int surface, const float* dens) {
+    long long nnode = (long long)m.W * m.H * m.D;
+    long long nvox = (long long)m.NXMC * m.NYMC * m.NZMC;
+    cudaStream_t s = c->stream;
+    McSurface& out = c->mc[surface];
+    out.nverts = out.nindices = out.active = 0;
+    c->mc_last_dens = dens;
+    k_mc_classify<<<mp_blocks(nvox, 256), 256, 0, s>>>(m, dens, c->mc_numverts, c->mc_cube, c->mc_vverts, c->mc_vflag);
+    c->launches++;
     MP_CHECK_LAUNCH(c);
     MP_TRY(mp_scan_u32(c, c->mc_vflag, c->mc_vscan, (size_t)nvox));
     uint32_t nact = 0;
@@ -287,7 +335,7 @@ int k_mc(MpCtx* c, int surface) {
     uint32_t nv = 0;
     MP_TRY(readback(c, c->mc_escan + nedge, &nv));
     if ((long long)nv > c->P.mc_max_verts) { c->err = "mc: vertex cap exceeded"; return MP_ERR_CAPACITY; }
-    k_mc_vertices<<<mp_blocks(nedge, 256), 256, 0, s>>>(m, nedge, c->mc_emark, c->mc_escan, c->mc_dens, out.verts);
+    k_mc_vertices<<<mp_blocks(nedge, 256), 256, 0, s>>>(m, nedge, c->mc_emark, c->mc_escan, dens, out.verts);
     k_mc_indices<<<mp_blocks(nact, 256), 256, 0, s>>>(m, nact, c->mc_compact, c->mc_cube, c->mc_vvscan, c->mc_numverts,
                                                       c->mc_tri, c->mc_escan, out.indices);
     c->launches += 2;

@@ -305,10 +305,27 @@ __global__ void k_correct_pos(Grid g, Cells cl, int np, const float4* __restrict
         float3 ip = xyz(q);
         int i, j, k; ijkpos(g, ip, i, j, k);
         float3 spring = mk3(0.0f);
-        // the three cells of a (di,dj) column are contiguous: their four range
-        // bounds are read together, then each cell is summed on its own
-        const int k0 = max(k - 1, 0), k1 = min(k + 1, g.NZ - 1);
-        for (int di = -1; di <= 1; di++) for (int dj = -1; dj <= 1; dj++) {
+        // With re below half a cell, a neighbour cell on the far side of the
+        // particle's own half-cell holds only particles whose d2 exceeds
+        // re2_skip (its whole extent is more than 1.002 re away along that
+        // axis, with a margin for the rounding of the cell coordinates), so
+        // every pair in it would be skipped: the cell is not visited.
+        const float3 rel = (ip - g0) / mk3(h, h, h);
+        const float cut_lo = 1.002f * (re / h) + 2e-4f;
+        auto span = [&](float r, int n, int c, int& lo, int& hi) {
+            lo = -1; hi = 1;
+            if (r >= 0 && r < (float)n) {
+                float fr = r - (float)c;
+                if (fr > cut_lo) lo = 0;
+                if (1.0f - fr > cut_lo) hi = 0;
+            }
+        };
+        int ilo, ihi, jlo, jhi, klo, khi;
+        span(rel.x, g.NX, i, ilo, ihi); span(rel.y, g.NY, j, jlo, jhi); span(rel.z, g.NZ, k, klo, khi);
+        // the cells of a (di,dj) column are contiguous: their range bounds are
+        // read together, then each cell is summed on its own
+        const int k0 = max(k + klo, 0), k1 = min(k + khi, g.NZ - 1);
+        for (int di = ilo; di <= ihi; di++) for (int dj = jlo; dj <= jhi; dj++) {
             if (!vc(g, i + di, j + dj, k)) continue;
             const int cb = cid(g, i + di, j + dj, k0);
             uint32_t bnd[4];
