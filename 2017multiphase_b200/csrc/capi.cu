@@ -705,7 +705,7 @@ extern "C" int mp_step(void* ctx) {
     MP_TRY(k_g2p(c));
     MP_TRY(k_solid_motion(c));
     MP_TRY(k_solo_air_update(c));
-    MP_TRY(k_hash_sort(c)); MP_TRY(k_collide_advect(c));
+    MP_TRY(k_hash_sort(c)); MP_TRY(k_collide_advect(c, true));
     if (P.b_correct_position) {
         MP_TRY(k_hash_sort(c)); MP_TRY(k_correct_pos(c));
         MP_TRY(k_hash_sort(c)); MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c)); MP_TRY(k_correct_pos_bubble(c));

@@ -150,7 +150,7 @@ int k_project(MpCtx* c, int* iters, double* res);
 int k_g2p(MpCtx* c);
 int k_solid_motion(MpCtx* c);
 int k_solo_air_update(MpCtx* c);
-int k_collide_advect(MpCtx* c);
+int k_collide_advect(MpCtx* c, bool skip_empty_solid = false);
 int k_correct_pos(MpCtx* c);
 int k_correct_pos_bubble(MpCtx* c);
 int k_heat(MpCtx* c);

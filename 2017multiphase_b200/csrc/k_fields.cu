@@ -328,10 +328,13 @@ __global__ void k_surftension(Grid g, float* __restrict__ sf, const int8_t* __re
 }
 
 // initSolidPhi (spray_k.cu:724-744)
-__global__ void k_init_solid_phi(Grid g, Cells cl, float* __restrict__ phi) {
+// also raises *any when some cell holds a SOLID particle (one atomic per warp)
+__global__ void k_init_solid_phi(Grid g, Cells cl, float* __restrict__ phi, uint32_t* __restrict__ any) {
     MP_GRID_LOOP(idx, g.n) {
         bool f = (cl.tmask[idx] >> MP_TYPESOLID) & 1;
         phi[idx] = f ? -0.5f : (float)(3 * g.NX);
+        unsigned b = __ballot_sync(__activemask(), f);
+        if (b && (threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1)) atomicOr(any, 1u);
     }
 }
 
@@ -441,7 +444,8 @@ int k_surface_tension_grid(MpCtx* c) {
 }
 
 int k_solid_phi(MpCtx* c) {
-    k_init_solid_phi<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, cells_of(c), c->phisolid);
+    MP_CUDA(c, cudaMemsetAsync(c->u32_scratch + 2, 0, sizeof(uint32_t), c->stream));
+    k_init_solid_phi<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, cells_of(c), c->phisolid, c->u32_scratch + 2);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     for (int it = 0; it < 3; it++) MP_TRY(k_sweep_pass_swap(c, &c->phisolid, -1));

@@ -733,9 +733,19 @@ int k_solo_air_update(MpCtx* c) {
 }
 
 // CollisionSolid (spray.cu:2959-2983)
-int k_collide_advect(MpCtx* c) {
-    MP_TRY(k_solid_phi(c));
-    MP_TRY(k_p2g_faces(c, c->su, 0));
+// skip_empty_solid: leave the solid velocity faces as they are when no cell
+// holds a SOLID particle. The collision reads them only where the solid level
+// set is at most half a cell, and without solid cells it is 3 NX everywhere.
+int k_collide_advect(MpCtx* c, bool skip_empty_solid) {
+    MP_TRY(k_solid_phi(c));   // raises u32_scratch[2] when a cell holds a SOLID particle
+    bool need_su = true;
+    if (skip_empty_solid) {
+        uint32_t any = 1;
+        MP_CUDA(c, cudaMemcpyAsync(&any, c->u32_scratch + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        MP_CUDA(c, cudaStreamSynchronize(c->stream));
+        need_su = any != 0;
+    }
+    if (need_su) MP_TRY(k_p2g_faces(c, c->su, 0));
     int np = c->np();
     if (!np) return MP_OK;
     const mp_params& P = c->P;
