@@ -133,6 +133,9 @@ def load_library() -> C.CDLL:
         "mp_sweep_u": ([vp, C.c_int], C.c_int),
         "mp_set_boundary_u": ([vp, C.c_int], C.c_int),
         "mp_project": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
+        "mp_checkpoint_size": ([vp, C.POINTER(C.c_size_t)], C.c_int),
+        "mp_checkpoint_save": ([vp, vp, C.c_size_t], C.c_int),
+        "mp_checkpoint_load": ([vp, vp, C.c_size_t], C.c_int),
         "mp_pressure_cg_static": ([C.c_int, C.c_int, C.c_int, C.c_float, vp, vp, vp, C.c_int, C.c_int, C.c_float, vp,
                                    C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
         "mp_mc": ([vp, C.c_int], C.c_int),
@@ -323,6 +326,18 @@ class Sim:
         rf = np.ascontiguousarray(randfloat, np.float32)
         sd = np.ascontiguousarray(seeds, np.int32)
         _check(self.lib.mp_set_tables(self.ctx, _ptr(rf), rf.size, _ptr(sd), sd.size), self.ctx)
+
+    def checkpoint(self) -> bytes:
+        """mp_checkpoint_save: the state the next step starts from."""
+        nb = C.c_size_t()
+        _check(self.lib.mp_checkpoint_size(self.ctx, C.byref(nb)), self.ctx)
+        buf = C.create_string_buffer(nb.value)
+        _check(self.lib.mp_checkpoint_save(self.ctx, buf, nb.value), self.ctx)
+        return buf.raw
+
+    def restore(self, blob: bytes):
+        """mp_checkpoint_load of a checkpoint taken with the same parameters."""
+        _check(self.lib.mp_checkpoint_load(self.ctx, C.c_char_p(blob), len(blob)), self.ctx)
 
     def state(self) -> MPState:
         s = MPState()

@@ -528,6 +528,98 @@ extern "C" int mp_set_tables(void* ctx, const float* randfloat, int nrand, const
     return MP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// checkpoint / resume: everything a step starts from. The grid fields are all
+// rebuilt from the particles inside a step, except the heat grid (kept, as the
+// heat stage reads it before its particle splat overwrites the cells it
+// reaches) and the fixed-heat input.
+// ---------------------------------------------------------------------------
+namespace {
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, params_bytes, state_bytes, pad;
+    int64_t np, nrand, nseed, ncell;
+    mp_params params;
+    mp_state state;
+};
+constexpr char kCkptMagic[8] = {'M', 'P', 'C', 'K', 'P', 'T', '0', '1'};
+size_t ckpt_bytes(const MpCtx* c) {
+    return sizeof(CkptHeader) + 3 * sizeof(float4) * (size_t)c->np() + sizeof(float) * (size_t)c->nrand +
+           sizeof(int32_t) * (size_t)c->nseed + 2 * sizeof(float) * (size_t)c->G.n;
+}
+}  // namespace
+
+extern "C" int mp_checkpoint_size(void* ctx, size_t* bytes) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!bytes) return MP_ERR_ARG;
+    *bytes = ckpt_bytes(c);
+    return MP_OK;
+}
+
+extern "C" int mp_checkpoint_save(void* ctx, void* host_dst, size_t bytes) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!host_dst) return MP_ERR_ARG;
+    if (bytes < ckpt_bytes(c)) { c->err = "checkpoint_save: buffer smaller than mp_checkpoint_size"; return MP_ERR_CAPACITY; }
+    CkptHeader h;
+    memset(&h, 0, sizeof(h));
+    memcpy(h.magic, kCkptMagic, 8);
+    h.version = 1; h.params_bytes = sizeof(mp_params); h.state_bytes = sizeof(mp_state);
+    h.np = c->np(); h.nrand = c->nrand; h.nseed = c->nseed; h.ncell = c->G.n;
+    h.params = c->P; h.state = c->S;
+    char* o = static_cast<char*>(host_dst);
+    memcpy(o, &h, sizeof(h)); o += sizeof(h);
+    cudaStream_t s = c->stream;
+    const size_t pb = sizeof(float4) * (size_t)h.np;
+    if (pb) {
+        MP_CUDA(c, cudaMemcpyAsync(o, c->pos, pb, cudaMemcpyDeviceToHost, s)); o += pb;
+        MP_CUDA(c, cudaMemcpyAsync(o, c->vel, pb, cudaMemcpyDeviceToHost, s)); o += pb;
+        MP_CUDA(c, cudaMemcpyAsync(o, c->heat, pb, cudaMemcpyDeviceToHost, s)); o += pb;
+    }
+    if (h.nrand) { MP_CUDA(c, cudaMemcpyAsync(o, c->randf, sizeof(float) * h.nrand, cudaMemcpyDeviceToHost, s)); o += sizeof(float) * h.nrand; }
+    if (h.nseed) { MP_CUDA(c, cudaMemcpyAsync(o, c->seeds, sizeof(int32_t) * h.nseed, cudaMemcpyDeviceToHost, s)); o += sizeof(int32_t) * h.nseed; }
+    MP_CUDA(c, cudaMemcpyAsync(o, c->fixedheat, sizeof(float) * h.ncell, cudaMemcpyDeviceToHost, s)); o += sizeof(float) * h.ncell;
+    MP_CUDA(c, cudaMemcpyAsync(o, c->Tp, sizeof(float) * h.ncell, cudaMemcpyDeviceToHost, s));
+    MP_CUDA(c, cudaStreamSynchronize(s));
+    return MP_OK;
+}
+
+extern "C" int mp_checkpoint_load(void* ctx, const void* host_src, size_t bytes) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!host_src || bytes < sizeof(CkptHeader)) { c->err = "checkpoint_load: no or short buffer"; return MP_ERR_ARG; }
+    CkptHeader h;
+    memcpy(&h, host_src, sizeof(h));
+    if (memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1 || h.params_bytes != sizeof(mp_params) ||
+        h.state_bytes != sizeof(mp_state)) { c->err = "checkpoint_load: not a checkpoint of this format"; return MP_ERR_ARG; }
+    if (memcmp(&h.params, &c->P, sizeof(mp_params)) != 0) {
+        c->err = "checkpoint_load: the checkpoint was taken with other parameters";
+        return MP_ERR_STATE;
+    }
+    if (h.np < 0 || h.np > c->P.par_num_max || h.ncell != c->G.n || h.nrand <= 200 || h.nseed < 0) {
+        c->err = "checkpoint_load: sizes do not fit this context"; return MP_ERR_ARG;
+    }
+    const size_t need = sizeof(CkptHeader) + 3 * sizeof(float4) * (size_t)h.np + sizeof(float) * (size_t)h.nrand +
+                        sizeof(int32_t) * (size_t)h.nseed + 2 * sizeof(float) * (size_t)h.ncell;
+    if (bytes < need) { c->err = "checkpoint_load: buffer shorter than its header says"; return MP_ERR_ARG; }
+    const char* o = static_cast<const char*>(host_src) + sizeof(CkptHeader);
+    const float* rf = reinterpret_cast<const float*>(o + 3 * sizeof(float4) * (size_t)h.np);
+    const int32_t* sd = reinterpret_cast<const int32_t*>(rf + h.nrand);
+    MP_TRY(mp_set_tables(ctx, rf, (int)h.nrand, h.nseed ? sd : nullptr, (int)h.nseed));
+    cudaStream_t s = c->stream;
+    const size_t pb = sizeof(float4) * (size_t)h.np;
+    if (pb) {
+        MP_CUDA(c, cudaMemcpyAsync(c->pos, o, pb, cudaMemcpyHostToDevice, s)); o += pb;
+        MP_CUDA(c, cudaMemcpyAsync(c->vel, o, pb, cudaMemcpyHostToDevice, s)); o += pb;
+        MP_CUDA(c, cudaMemcpyAsync(c->heat, o, pb, cudaMemcpyHostToDevice, s)); o += pb;
+    }
+    o = reinterpret_cast<const char*>(sd + h.nseed);
+    MP_CUDA(c, cudaMemcpyAsync(c->fixedheat, o, sizeof(float) * h.ncell, cudaMemcpyHostToDevice, s)); o += sizeof(float) * h.ncell;
+    MP_CUDA(c, cudaMemcpyAsync(c->Tp, o, sizeof(float) * h.ncell, cudaMemcpyHostToDevice, s));
+    MP_CUDA(c, cudaStreamSynchronize(s));
+    c->S = h.state;
+    c->mc_sorted = 0;
+    return MP_OK;
+}
+
 extern "C" int mp_mc_tables(int32_t* num_verts, int32_t* tri, int32_t* edge) {
     mp_internal_mc_tables(num_verts, tri, edge);
     return MP_OK;

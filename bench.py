@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-n", type=int, default=64, help="grid of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", default="", choices=["", "cg", "step"],
+                    help="small-footprint cases for ncu captures instead of the bench line: "
+                         "cg = one pressure solve on an n^3 liquid slab (z < 0.8) with a seeded divergence; "
+                         "step = one warm-up and one bubblesim step of the configuration at n^3")
     return ap.parse_args()
 
 
@@ -160,8 +164,66 @@ def run_reference(args, rank):
     print(json.dumps(out), flush=True)
 
 
+def profile_case(args):
+    """Cases sized for ncu: the device holds a few GB at most. Prints the
+    kernel-class timings of the measured part (CUDA events)."""
+    import importlib
+    import numpy as np
+    import torch
+    mp = importlib.import_module("2017multiphase_b200")
+    n = args.n or 256
+    if args.profile_case == "cg":
+        p = mp.scene_params(args.config, n)
+        p.par_num_max = 16
+        p.b_run_mc = 0
+        sim = mp.Sim(p)
+        mark = np.zeros((n, n, n), np.int8)
+        mark[:, :, int(0.8 * n):] = mp.TYPEVACUUM
+        mark[0], mark[-1] = mp.TYPEBOUNDARY, mp.TYPEBOUNDARY
+        mark[:, 0], mark[:, -1] = mp.TYPEBOUNDARY, mp.TYPEBOUNDARY
+        mark[:, :, 0], mark[:, :, -1] = mp.TYPEBOUNDARY, mp.TYPEBOUNDARY
+        sim.set_field("mark", mark.ravel())
+        sim.set_field("lsmerge", np.full(n ** 3, -0.5 / n, np.float32))
+        rng = np.random.default_rng(args.seed)
+        for f, cnt in [("waterux", (n + 1) * n * n), ("wateruy", n * (n + 1) * n), ("wateruz", n * n * (n + 1))]:
+            sim.set_field(f, (0.01 * rng.standard_normal(cnt)).astype(np.float32))
+        classes = {mp.KT_CG_STENCIL: ("k_cg_dir", CG_DIR_BYTES_PER_CELL), mp.KT_CG_UPDATE: ("k_cg_upd", CG_UPD_BYTES_PER_CELL)}
+        for k in classes:
+            sim.kernel_timing(k, True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, res, rc = sim.project_CG_bubble()
+        torch.cuda.synchronize()
+        out = {"case": "cg", "n": n, "iterations": it, "rc": rc, "solve_ms": (time.perf_counter() - t0) * 1e3}
+        for k, (nm, bpc) in classes.items():
+            ms, nl = sim.kernel_timing_read(k)
+            per = ms / max(nl, 1)
+            out[nm] = {"launches": nl, "us_per_launch": per * 1e3, "algorithmic_GBps": bpc * n ** 3 / (per / 1e3) / 1e9}
+    else:
+        sim = mp.Sim.from_config(args.config, n, args.seed)
+        sim.bubblesim()
+        classes = {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g_faces",
+                   mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
+        for k in classes:
+            sim.kernel_timing(k, True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.bubblesim()
+        torch.cuda.synchronize()
+        out = {"case": "step", "n": n, "config": args.config, "step_ms": (time.perf_counter() - t0) * 1e3,
+               "particles": int(sim.state().par_num_now)}
+        for k, nm in classes.items():
+            ms, nl = sim.kernel_timing_read(k)
+            out[nm] = {"launches": nl, "ms": ms}
+    print(json.dumps(out), flush=True)
+    sim.close()
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -342,8 +342,21 @@ int mp_mc_download(void* ctx, int surface, float* verts, float* normals,
 int mp_mc_download_field(void* ctx, float* dens, uint8_t* cubeindex);
 
 /* The whole bubblesim step in the reference's order and cadence
- * (spray.cpp:979-1233). Synchronous at exit. */
+ * (spray.cpp:979-1233). Synchronous at exit. Its solid-velocity faces
+ * (MP_F_SOLIDU*) are left as they were when no cell holds a SOLID particle:
+ * the collision reads them only within half a cell of a solid. */
 int mp_step(void* ctx);
+
+/* Checkpoint / resume of the state a step starts from: particles, the random
+ * table, nucleation cells, the fixed-heat field, the heat grid and mp_state.
+ * A context created with identical parameters that loads a checkpoint and
+ * steps reproduces the saving context's steps bit for bit. The reference
+ * keeps this state only in its process (no counterpart). Host buffers;
+ * mp_checkpoint_size gives the bytes needed; load rejects a checkpoint taken
+ * with other parameters (MP_ERR_STATE) or of another format (MP_ERR_ARG). */
+int mp_checkpoint_size(void* ctx, size_t* bytes);
+int mp_checkpoint_save(void* ctx, void* host_dst, size_t bytes);
+int mp_checkpoint_load(void* ctx, const void* host_src, size_t bytes);
 
 /* ---- measurement -------------------------------------------------------- */
 
