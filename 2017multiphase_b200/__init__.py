@@ -133,6 +133,12 @@ def load_library() -> C.CDLL:
         "mp_sweep_u": ([vp, C.c_int], C.c_int),
         "mp_set_boundary_u": ([vp, C.c_int], C.c_int),
         "mp_project": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
+        "mp_adj_record": ([vp, C.c_int, C.c_int], C.c_int),
+        "mp_adj_set_targets": ([vp, vp, C.c_int], C.c_int),
+        "mp_adj_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "mp_adj_loss": ([vp, C.c_int, vp, C.POINTER(C.c_double)], C.c_int),
+        "mp_adj_gradient": ([vp, C.c_int, vp, vp, C.POINTER(C.c_double)], C.c_int),
+        "mp_adj_release": ([vp], C.c_int),
         "mp_checkpoint_size": ([vp, C.POINTER(C.c_size_t)], C.c_int),
         "mp_checkpoint_save": ([vp, vp, C.c_size_t], C.c_int),
         "mp_checkpoint_load": ([vp, vp, C.c_size_t], C.c_int),
@@ -407,6 +413,40 @@ class Sim:
         _check(self.lib.mp_mc_download_field(self.ctx, _ptr(dens), _ptr(cube)), self.ctx)
         return dens, cube
 
+    # ---- adjoint of the FLUID-only step (mp_adj_*) -------------------------
+    def adj_record(self, nsteps: int, checkpoint_every: int):
+        """Runs `nsteps` steps from the current particles, recording the discrete
+        state the derivative holds fixed (mp_adj_record)."""
+        _check(self.lib.mp_adj_record(self.ctx, nsteps, checkpoint_every), self.ctx)
+
+    def adj_set_targets(self, samples: np.ndarray):
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 3)
+        _check(self.lib.mp_adj_set_targets(self.ctx, _ptr(s), len(s)), self.ctx)
+
+    def adj_num_particles(self) -> int:
+        n = C.c_int(); k = C.c_int()
+        _check(self.lib.mp_adj_info(self.ctx, C.byref(n), C.byref(k)), self.ctx)
+        return n.value
+
+    def adj_loss(self, v0=None, precision: int = PREC_MIXED) -> float:
+        """Loss of the recorded program from initial velocities v0 (a CUDA
+        float64 tensor (np, 3) in recording order, or None for the recorded ones)."""
+        loss = C.c_double()
+        vp = None if v0 is None else C.c_void_p(v0.data_ptr())
+        _check(self.lib.mp_adj_loss(self.ctx, precision, vp, C.byref(loss)), self.ctx)
+        return loss.value
+
+    def adj_gradient(self, v0=None, precision: int = PREC_MIXED):
+        """(loss, dL/dv0) as a CUDA float64 tensor (np, 3)."""
+        import torch
+        n = self.adj_num_particles()
+        g = torch.empty((n, 3), dtype=torch.float64, device=f"cuda:{torch.cuda.current_device()}")
+        loss = C.c_double()
+        vp = None if v0 is None else C.c_void_p(v0.data_ptr())
+        torch.cuda.synchronize()
+        _check(self.lib.mp_adj_gradient(self.ctx, precision, vp, C.c_void_p(g.data_ptr()), C.byref(loss)), self.ctx)
+        return loss.value, g
+
     # ---- measurement ------------------------------------------------------
     def kernel_timing(self, cls: int, enable: bool = True):
         _check(self.lib.mp_kernel_timing(self.ctx, cls, int(enable)), self.ctx)
@@ -426,3 +466,39 @@ class Sim:
         s = C.c_void_p()
         _check(self.lib.mp_get_stream(self.ctx, C.byref(s)), self.ctx)
         return s.value or 0
+
+
+def dam_break_targets(nsamples: int, seed: int, height: float = 0.3, margin: float = 0.1) -> np.ndarray:
+    """Target points of configuration 4's loss: (x, y) uniform in the box
+    interior from `seed`, on the surface z = height."""
+    rng = np.random.default_rng(seed)
+    xy = rng.uniform(margin, 1.0 - margin, size=(nsamples, 2))
+    return np.concatenate([xy, np.full((nsamples, 1), height)], axis=1).astype(np.float32)
+
+
+def _dam_break_function():
+    import torch
+
+    class DamBreakLoss(torch.autograd.Function):
+        """Loss of the recorded FLUID-only program as a function of the initial
+        particle velocities; backward is the hand-written adjoint
+        (mp_adj_gradient). The discrete state is the one recorded by
+        Sim.adj_record, so v0 should stay near the recorded velocities."""
+
+        @staticmethod
+        def forward(ctx, v0, sim, precision):
+            loss, grad = sim.adj_gradient(v0.detach().to(torch.float64).contiguous(), precision)
+            ctx.save_for_backward(grad)
+            return torch.tensor(loss, dtype=torch.float64, device=v0.device)
+
+        @staticmethod
+        def backward(ctx, gout):
+            (grad,) = ctx.saved_tensors
+            return gout * grad, None, None
+
+    return DamBreakLoss
+
+
+def dam_break_loss(v0, sim, precision: int = PREC_MIXED):
+    """torch.autograd entry: loss(v0) with d loss / d v0 from the adjoint."""
+    return _dam_break_function().apply(v0, sim, precision)

@@ -137,6 +137,7 @@ static void free_all(MpCtx* c) {
                     c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_dens2, c->mc_cube, c->mc_vflag, c->mc_vscan,
                     c->mc_compact, c->mc_vverts, c->mc_vvscan, c->mc_emark, c->mc_escan, c->mc_vstart, c->mc_inc,
                     c->mc_fill, c->mc_tmpv};
+    k_adj_free(c);
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int a = 0; a < 3; a++) {
         for (float* p : {c->wu[a], c->wuo[a], c->au[a], c->auo[a], c->su[a], c->tmpu[a]}) if (p) cudaFree(p);
@@ -526,6 +527,32 @@ extern "C" int mp_set_tables(void* ctx, const float* randfloat, int nrand, const
     if (nseed) MP_CUDA(c, cudaMemcpyAsync(c->seeds, seeds, sizeof(int32_t) * nseed, cudaMemcpyHostToDevice, c->stream));
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
     return MP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the FLUID-only step (k_adjoint.cu)
+// ---------------------------------------------------------------------------
+extern "C" int mp_adj_record(void* ctx, int nsteps, int checkpoint_every) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_adj_record(c, nsteps, checkpoint_every);
+}
+extern "C" int mp_adj_set_targets(void* ctx, const float* samples3, int nsamples) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_adj_set_targets(c, samples3, nsamples);
+}
+extern "C" int mp_adj_info(void* ctx, int* np, int* nsteps) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_adj_np(c, np, nsteps);
+}
+extern "C" int mp_adj_loss(void* ctx, int precision, const double* v0, double* loss) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!loss || (precision != MP_PREC_MIXED && precision != MP_PREC_FP64)) return MP_ERR_ARG;
+    return k_adj_run(c, precision, v0, nullptr, loss);
+}
+extern "C" int mp_adj_gradient(void* ctx, int precision, const double* v0, double* grad_v0, double* loss) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!grad_v0 || (precision != MP_PREC_MIXED && precision != MP_PREC_FP64)) return MP_ERR_ARG;
+    return k_adj_run(c, precision, v0, grad_v0, loss);
+}
+extern "C" int mp_adj_release(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c); k_adj_free(c); return MP_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -87,6 +87,8 @@ struct MpCtx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pool;
     int64_t launches = 0;
 
+    struct AdjTape* adj = nullptr;   // the adjoint module's tape (k_adjoint.cu)
+
     int np() const { return S.par_num_now; }
 };
 
@@ -160,6 +162,15 @@ int k_melt(MpCtx* c);
 int k_freeze(MpCtx* c);
 int k_mc(MpCtx* c, int surface);
 int k_mc_fluid_gas(MpCtx* c);
+int k_cg_solve(MpCtx* c, const int8_t* mark, float* x, const float* b, int maxiter, int tolmode, float tol, int* iters,
+               double* res);
+int k_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, int maxiter, int tolmode, float tol,
+               int* iters, double* res);
+void k_adj_free(MpCtx* c);
+int k_adj_record(MpCtx* c, int nsteps, int every);
+int k_adj_set_targets(MpCtx* c, const float* samples3, int nsamples);
+int k_adj_run(MpCtx* c, int precision, const double* v0, double* grad, double* loss);
+int k_adj_np(MpCtx* c, int* np, int* nsteps);
 int k_init_particle_heat(MpCtx* c);
 int k_pack_particles(MpCtx* c, int n, const float* pos3, const float* vel3, const int8_t* flag,
                      const float* mass, const float* T, const float* L, const float* sol, const float* gas);

@@ -138,9 +138,10 @@ extern "C" int mp_scene_params(int config, int n, mp_params* p) {
         p->heatalpha_fluid = 0.01f; p->heatalpha_solid = 0.01f; p->heatalpha_air = 0.01f; p->heatalpha_vacuum = 0.0001f;
         p->mc_every = 2;
         break;
-    case 4:   // differentiable dam break
+    case 4:   // differentiable dam break: the FLUID-only program the adjoint covers
         p->scene = MP_SCENE_DAMBREAK;
         p->b_run_mc = 0;
+        p->b_correct_position = 0;
         break;
     case 5:   // bubble column at scale, marching cubes every step
         p->scene = MP_SCENE_MULTIBUBBLE;

@@ -1,0 +1,1036 @@
+// k_adjoint.cu — reverse-mode derivative of the water-only dam-break step.
+//
+// The reference has no differentiation. This module differentiates the
+// program the bubblesim step (spray.cpp:979-1233) runs for a scene of FLUID
+// particles only, with the position corrections off:
+//   gravity (addgravityforce_k, spray_k.cu:330)
+//   -> velocity splat to faces (mapvelp2g_k_fluidSolid, spray_k.cu:2809-2866)
+//   -> extrapolation, two Jacobi passes (sweepu_k_bubble, spray_k.cu:3779-3880)
+//   -> wall rules (setWaterBoundaryU_k, spray_k.cu:956-995)
+//   -> projection (cptdivergence_bubble2 + solver_cg_bubble + subGradPress)
+//   -> extrapolation + wall rules again
+//   -> FLIP/PIC gather (mapvelg2p_flip_bubble, spray_k.cu:3525-3540, blended
+//      with the new grid velocity by flip_alpha as spray_k.cu:3487-3490)
+//   -> advection with the wall clamp (CollisionWithSolid_k, spray_k.cu:5276)
+// and, after the last step, the loss sum_s phi(y_s)^2 of the fluid distance
+// field (genlevelset, spray_k.cu:2753-2806) at target points y_s.
+//
+// Discrete state is recorded by running the engine's own stages once
+// (mp_adj_record) and then held fixed: the particle order and cell ranges of
+// each step's splat, the cell marks, the extrapolation distance field and the
+// nearest particle of each cell at the end. The derivative is that of the
+// program with this state frozen (the program is piecewise smooth; the frozen
+// state is the piece the recorded run lies on). The replay of the continuous
+// part and its transpose are templated on the arithmetic type: FP32 (the
+// engine's) and FP64 (the reference gradient and finite differences).
+//
+// Every transpose is a gather (faces over the particles of nearby cells,
+// particles over nearby faces, cells over nearby samples), so gradients are
+// deterministic. The projection's transpose is a second CG solve on the
+// symmetric pressure matrix. States are checkpointed every `every` steps and
+// recomputed segment by segment during the reverse sweep.
+#include "ctx.cuh"
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+using namespace mpk;
+
+int k_hash_sort(MpCtx* c);
+
+struct AdjTape {
+    int np = 0, nsteps = 0, every = 0;
+    std::vector<uint32_t*> order, off;   // per step: sorted slot -> particle id; cell ranges
+    std::vector<int8_t*> mark;           // per step: cell marks
+    std::vector<float*> phi;             // per step: fluid extrapolation distance
+    float* x0 = nullptr;                 // initial positions (id order, xyz)
+    float* v0 = nullptr;                 // initial velocities (id order, xyz)
+    float* mass = nullptr;               // id order
+    uint32_t* ids = nullptr;             // engine slot -> particle id while recording
+    uint32_t* ids2 = nullptr;
+    uint32_t* nearest = nullptr;         // per cell: nearest FLUID particle id at the end, or ~0u
+    float* samples = nullptr;            // target points sorted by their base cell
+    int nsamples = 0;
+    uint32_t* s_off = nullptr;           // per base cell: range of its samples (n + 1)
+    // replay / adjoint work, sized for `wesz`-byte elements
+    size_t wesz = 0;
+    int wk_ns = 0;                       // samples the work was sized for
+    std::vector<void*> wk;
+};
+
+namespace {
+
+constexpr uint32_t NONE = 0xffffffffu;
+
+template <class T> struct Fc { T* x; T* y; T* z; };
+template <class T> Fc<T> faces_of(void* base, const Grid& g) {
+    T* b = static_cast<T*>(base);
+    return Fc<T>{b, b + g.nfx, b + g.nfx + g.nfy};
+}
+// flat face index t -> axis and (i,j,k) in that axis' face grid
+__device__ __forceinline__ int face_decode(const Grid& g, long long t, int& i, int& j, int& k, int& idx) {
+    if (t < g.nfx) { idx = (int)t; getijk3(idx, g.NY, g.NZ, i, j, k); return 0; }
+    if (t < (long long)g.nfx + g.nfy) { idx = (int)(t - g.nfx); getijk3(idx, g.NY + 1, g.NZ, i, j, k); return 1; }
+    idx = (int)(t - g.nfx - g.nfy); getijk3(idx, g.NY, g.NZ + 1, i, j, k); return 2;
+}
+__device__ __forceinline__ int face_index(const Grid& g, int ax, int i, int j, int k) {
+    return ax == 0 ? fxi(g, i, j, k) : (ax == 1 ? fyi(g, i, j, k) : fzi(g, i, j, k));
+}
+template <class T> __device__ __forceinline__ T* fsel(const Fc<T>& f, int ax) { return ax == 0 ? f.x : (ax == 1 ? f.y : f.z); }
+
+// ---- recording helpers --------------------------------------------------------
+__global__ void k_ad_iota(int n, uint32_t* a) { MP_GRID_LOOP(i, n) a[i] = (uint32_t)i; }
+__global__ void k_ad_permute_ids(int n, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ in,
+                                 uint32_t* __restrict__ out) {
+    MP_GRID_LOOP(s, n) out[s] = in[perm[s]];
+}
+__global__ void k_ad_snapshot(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ pos,
+                              const float4* __restrict__ vel, float* __restrict__ x, float* __restrict__ v,
+                              float* __restrict__ m) {
+    MP_GRID_LOOP(s, n) {
+        uint32_t id = ids[s];
+        float4 p = pos[s], q = vel[s];
+        x[3 * id] = p.x; x[3 * id + 1] = p.y; x[3 * id + 2] = p.z;
+        v[3 * id] = q.x; v[3 * id + 1] = q.y; v[3 * id + 2] = q.z;
+        m[id] = q.w;
+    }
+}
+__global__ void k_ad_count_nonfluid(int n, const float4* __restrict__ pos, uint32_t* cnt) {
+    MP_GRID_LOOP(s, n) if (pflag(pos[s]) != MP_TYPEFLUID) atomicAdd(cnt, 1u);
+}
+// nearest FLUID particle of each cell centre within the genlevelset window
+// (2.5 cells; the +-2 cell box in a fixed order, first minimum kept)
+__global__ void k_ad_nearest(Grid g, Cells cl, const float4* __restrict__ pos, const uint32_t* __restrict__ ids,
+                             uint32_t* __restrict__ nearest) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        float h = g.h;
+        float3 gp = (mk3((float)i, (float)j, (float)k) + mk3(0.5f, 0.5f, 0.5f)) * h;
+        float best = 6.25f * h * h;
+        uint32_t who = NONE;
+        for (int di = -2; di <= 2; di++) for (int dj = -2; dj <= 2; dj++) for (int dk = -2; dk <= 2; dk++) {
+            int a = i + di, b = j + dj, cc = k + dk;
+            if (a < 0 || a >= g.NX || b < 0 || b >= g.NY || cc < 0 || cc >= g.NZ) continue;
+            int c = cid(g, a, b, cc);
+            for (uint32_t s = cl.off[c]; s < cl.off[c + 1]; s++) {
+                float4 q = pos[s];
+                if (pflag(q) != MP_TYPEFLUID) continue;
+                float3 d = xyz(q) - gp;
+                float d2 = dot(d, d);
+                if (d2 < best) { best = d2; who = ids[s]; }
+            }
+        }
+        nearest[idx] = who;
+    }
+}
+
+// ---- replay of the continuous part ----------------------------------------------
+template <class T>
+__global__ void k_ad_gravity(int np, const T* __restrict__ v, T* __restrict__ va, T dtg) {
+    MP_GRID_LOOP(p, np) {
+        va[3 * p] = v[3 * p]; va[3 * p + 1] = v[3 * p + 1];
+        va[3 * p + 2] = v[3 * p + 2] + dtg;
+    }
+}
+template <class T> __device__ __forceinline__ T sharpk(T r2) {
+    const T c = (T)1.4f * (T)1.4f;
+    T rr = r2 > (T)0.0001f ? r2 : (T)0.0001f;
+    T w = c / rr - (T)1;
+    return w > (T)0 ? w : (T)0;
+}
+// d sharpk / d r2 (zero where the weight is clamped)
+template <class T> __device__ __forceinline__ T sharpk_d(T r2) {
+    const T c = (T)1.4f * (T)1.4f;
+    if (!(r2 > (T)0.0001f)) return (T)0;
+    if (!(c / r2 - (T)1 > (T)0)) return (T)0;
+    return -c / (r2 * r2);
+}
+// face position in cell units
+__device__ __forceinline__ void face_pos(int ax, int i, int j, int k, float& gx, float& gy, float& gz) {
+    gx = (float)i + (ax == 0 ? 0.0f : 0.5f);
+    gy = (float)j + (ax == 1 ? 0.0f : 0.5f);
+    gz = (float)k + (ax == 2 ? 0.0f : 0.5f);
+}
+// splat: per face, the mass-weighted sharp-kernel average of the particles of
+// the cells [i-1,i] along the face normal and [-1,1] across (the order of
+// mapvelp2g_k_fluidSolid's loops)
+template <class T>
+__global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
+                         const float* __restrict__ mass, const T* __restrict__ x, const T* __restrict__ va,
+                         Fc<T> u, Fc<T> W) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    const T scale = (T)1 / (T)g.h;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        float fx, fy, fz; face_pos(ax, i, j, k, fx, fy, fz);
+        T w = 0, s = 0;
+        const int a0 = ax == 0 ? i - 1 : i - 1, a1 = ax == 0 ? i : i + 1;
+        const int b0 = j - 1, b1 = ax == 1 ? j : j + 1;
+        const int c0 = k - 1, c1 = ax == 2 ? k : k + 1;
+        for (int a = a0; a <= a1; a++) {
+            if (a < 0 || a > g.NX - 1) continue;
+            for (int b = b0; b <= b1; b++) {
+                if (b < 0 || b > g.NY - 1) continue;
+                for (int cc = c0; cc <= c1; cc++) {
+                    if (cc < 0 || cc > g.NZ - 1) continue;
+                    int c = cid(g, a, b, cc);
+                    for (uint32_t q = off[c]; q < off[c + 1]; q++) {
+                        uint32_t p = order[q];
+                        T dx = x[3 * p] * scale - (T)fx, dy = x[3 * p + 1] * scale - (T)fy, dz = x[3 * p + 2] * scale - (T)fz;
+                        T r2 = dx * dx + dy * dy + dz * dz;
+                        T wp = (T)mass[p] * sharpk(r2);
+                        w += wp; s += wp * va[3 * p + ax];
+                    }
+                }
+            }
+        }
+        fsel(W, ax)[idx] = w;
+        fsel(u, ax)[idx] = w > (T)0 ? s / w : (T)0;
+    }
+}
+template <class T> __global__ void k_ad_copy(long long n, const T* __restrict__ a, T* __restrict__ b) {
+    MP_GRID_LOOP(t, n) b[t] = a[t];
+}
+template <class T> __global__ void k_ad_sub(long long n, const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ o) {
+    MP_GRID_LOOP(t, n) o[t] = a[t] - b[t];
+}
+template <class T> __global__ void k_ad_axpy(long long n, T s, const T* __restrict__ a, T* __restrict__ o) {
+    MP_GRID_LOOP(t, n) o[t] += s * a[t];
+}
+
+// The octant an extrapolation pass picks for a face and its three weights
+// (sweepu_k_bubble: the last octant of the loop whose weights are all
+// non-negative). Returns false when the face keeps its value.
+__device__ bool sweep_sel(const Grid& g, int ax, int i, int j, int k, const float* __restrict__ ls,
+                          const int8_t* __restrict__ mark, int fl, int& sdi, int& sdj, int& sdk, float& swx,
+                          float& swy, float& swz) {
+    int n_ax = ax == 0 ? g.NX : (ax == 1 ? g.NY : g.NZ);
+    int e = ax == 0 ? i : (ax == 1 ? j : k);
+    if (!(e > 1 && e < n_ax - 1)) return false;
+    int i1 = i - (ax == 0), j1 = j - (ax == 1), k1 = k - (ax == 2);
+    if (mark[cid(g, i, j, k)] == fl || mark[cid(g, i1, j1, k1)] == fl) return false;
+    float l0 = ls[cid(g, i, j, k)], l1 = ls[cid(g, i1, j1, k1)];
+    bool found = false;
+    for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
+        float wx, wy, wz;
+        if (ax == 0) {
+            if (j + dj < 0 || j + dj > g.NY - 1 || k + dk < 0 || k + dk > g.NZ - 1) continue;
+            wx = (float)(-di) * (l0 - l1);
+            if (wx < 0) continue;
+            wy = (l0 + l1 - ls[cid(g, i, j + dj, k)] - ls[cid(g, i - 1, j + dj, k)]) * 0.5f;
+            if (wy < 0) continue;
+            wz = (l0 + l1 - ls[cid(g, i, j, k + dk)] - ls[cid(g, i - 1, j, k + dk)]) * 0.5f;
+            if (wz < 0) continue;
+        } else if (ax == 1) {
+            if (i + di < 0 || i + di > g.NX - 1 || k + dk < 0 || k + dk > g.NZ - 1) continue;
+            wy = (float)(-dj) * (l0 - l1);
+            if (wy < 0) continue;
+            wx = (l0 + l1 - ls[cid(g, i + di, j, k)] - ls[cid(g, i + di, j - 1, k)]) * 0.5f;
+            if (wx < 0) continue;
+            wz = (l0 + l1 - ls[cid(g, i, j, k + dk)] - ls[cid(g, i, j - 1, k + dk)]) * 0.5f;
+            if (wz < 0) continue;
+        } else {
+            if (i + di < 0 || i + di > g.NX - 1 || j + dj < 0 || j + dj > g.NY - 1) continue;
+            wz = (float)(-dk) * (l0 - l1);
+            if (wz < 0) continue;
+            wy = (l0 + l1 - ls[cid(g, i, j + dj, k)] - ls[cid(g, i, j + dj, k - 1)]) * 0.5f;
+            if (wy < 0) continue;
+            wx = (l0 + l1 - ls[cid(g, i + di, j, k)] - ls[cid(g, i + di, j, k - 1)]) * 0.5f;
+            if (wx < 0) continue;
+        }
+        float ws = wx + wy + wz;
+        if (ws == 0) wx = wy = wz = 1.0f / 3;
+        else { wx /= ws; wy /= ws; wz /= ws; }
+        sdi = di; sdj = dj; sdk = dk; swx = wx; swy = wy; swz = wz;
+        found = true;
+    }
+    return found;
+}
+template <class T>
+__global__ void k_ad_sweepu(Grid g, Fc<T> in, Fc<T> out, const float* __restrict__ ls, const int8_t* __restrict__ mark,
+                            int fl) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        const T* f = fsel(in, ax);
+        T res = f[idx];
+        int di, dj, dk; float wx, wy, wz;
+        if (sweep_sel(g, ax, i, j, k, ls, mark, fl, di, dj, dk, wx, wy, wz))
+            res = (T)wx * f[face_index(g, ax, i + di, j, k)] + (T)wy * f[face_index(g, ax, i, j + dj, k)] +
+                  (T)wz * f[face_index(g, ax, i, j, k + dk)];
+        fsel(out, ax)[idx] = res;
+    }
+}
+// transpose of one extrapolation pass: an input face keeps its own adjoint
+// unless the pass overwrote it, and receives from the (up to six) faces whose
+// chosen octant reads it
+template <class T>
+__global__ void k_ad_sweepu_adj(Grid g, Fc<T> ob, Fc<T> ib, const float* __restrict__ ls,
+                                const int8_t* __restrict__ mark, int fl) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        const T* o = fsel(ob, ax);
+        int di, dj, dk; float wx, wy, wz;
+        T acc = sweep_sel(g, ax, i, j, k, ls, mark, fl, di, dj, dk, wx, wy, wz) ? (T)0 : o[idx];
+        const int W = ax == 0 ? g.NX + 1 : g.NX, H = ax == 1 ? g.NY + 1 : g.NY, D = ax == 2 ? g.NZ + 1 : g.NZ;
+        // the reader f sits at g - d*e_dir and chose d along dir
+        for (int dir = 0; dir < 3; dir++) for (int d = -1; d <= 1; d += 2) {
+            int fi = i - (dir == 0 ? d : 0), fj = j - (dir == 1 ? d : 0), fk = k - (dir == 2 ? d : 0);
+            if (fi < 0 || fi >= W || fj < 0 || fj >= H || fk < 0 || fk >= D) continue;
+            int ei, ej, ek; float ax_w, ay_w, az_w;
+            if (!sweep_sel(g, ax, fi, fj, fk, ls, mark, fl, ei, ej, ek, ax_w, ay_w, az_w)) continue;
+            int chosen = dir == 0 ? ei : (dir == 1 ? ej : ek);
+            if (chosen != d) continue;
+            float wsel = dir == 0 ? ax_w : (dir == 1 ? ay_w : az_w);
+            acc += (T)wsel * o[face_index(g, ax, fi, fj, fk)];
+        }
+        fsel(ib, ax)[idx] = acc;
+    }
+}
+// wall rules (setWaterBoundaryU_k), in place; `zceil` marks the top z faces
+// that took the face below
+__device__ __forceinline__ bool bmis(const Grid& g, const int8_t* mark, int i, int j, int k, int i1, int j1, int k1) {
+    return (mark[cid(g, i, j, k)] == MP_TYPEBOUNDARY) != (mark[cid(g, i1, j1, k1)] == MP_TYPEBOUNDARY);
+}
+// 0: keep, 1: zero, 2: z ceiling rule (takes min(below, 0) of the face below)
+__device__ __forceinline__ int bound_rule(const Grid& g, const int8_t* mark, int ax, int i, int j, int k) {
+    if (ax == 0) {
+        if (i <= 1 || i >= g.NX + 1 - 2) return 1;
+        if (i > 1 && i < g.NX - 1 && bmis(g, mark, i, j, k, i - 1, j, k)) return 1;
+    } else if (ax == 1) {
+        if (j <= 1 || j >= g.NY + 1 - 2) return 1;
+        if (j > 0 && j < g.NY && bmis(g, mark, i, j, k, i, j - 1, k)) return 1;
+    } else {
+        if (k <= 1 || k >= g.NZ + 1 - 1) return 1;
+        if (k == g.NZ + 1 - 2) return 2;
+        if (k > 0 && k < g.NZ && bmis(g, mark, i, j, k, i, j, k - 1)) return 1;
+    }
+    return 0;
+}
+// whether the face below a ceiling face passes its value to the rule
+__device__ __forceinline__ bool zrule_pass(const Grid& g, const int8_t* mark, int i, int j, int kb) {
+    if (kb <= 1) return false;
+    if (kb > 0 && kb < g.NZ && bmis(g, mark, i, j, kb, i, j, kb - 1)) return false;
+    return true;
+}
+template <class T>
+__global__ void k_ad_bound(Grid g, Fc<T> u, Fc<T> uo, const int8_t* __restrict__ mark) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        const int r = bound_rule(g, mark, ax, i, j, k);
+        T v = fsel(u, ax)[idx];
+        if (r == 1) v = (T)0;
+        else if (r == 2) {
+            T below = zrule_pass(g, mark, i, j, k - 1) ? u.z[fzi(g, i, j, k - 1)] : (T)0;
+            v = below < (T)0 ? below : (T)0;
+        }
+        fsel(uo, ax)[idx] = v;
+    }
+}
+// transpose; `u` is the rule's input field (its value decides the ceiling rule)
+template <class T>
+__global__ void k_ad_bound_adj(Grid g, Fc<T> ob, Fc<T> ib, Fc<T> u, const int8_t* __restrict__ mark) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        const int r = bound_rule(g, mark, ax, i, j, k);
+        T acc = r == 0 ? fsel(ob, ax)[idx] : (T)0;
+        if (ax == 2 && k + 1 == g.NZ + 1 - 2 && bound_rule(g, mark, 2, i, j, k + 1) == 2 &&
+            zrule_pass(g, mark, i, j, k) && u.z[idx] < (T)0)
+            acc += ob.z[fzi(g, i, j, k + 1)];
+        fsel(ib, ax)[idx] = acc;
+    }
+}
+__device__ __forceinline__ bool unknown(const Grid& g, const int8_t* mark, int idx, int i, int j, int k) {
+    int m = mark[idx];
+    return (m == MP_TYPEFLUID || m == MP_TYPEAIR) && i > 0 && i < g.NX - 1 && j > 0 && j < g.NY - 1 && k > 0 &&
+           k < g.NZ - 1;
+}
+template <class T>
+__global__ void k_ad_div(Grid g, const int8_t* __restrict__ mark, Fc<T> u, T* __restrict__ b) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        T out = 0;
+        if (unknown(g, mark, idx, i, j, k))
+            out = (u.x[fxi(g, i + 1, j, k)] - u.x[fxi(g, i, j, k)] + u.y[fyi(g, i, j + 1, k)] - u.y[fyi(g, i, j, k)] +
+                   u.z[fzi(g, i, j, k + 1)] - u.z[fzi(g, i, j, k)]) / (T)g.h;
+        b[idx] = out;
+    }
+}
+template <class T>
+__global__ void k_ad_subgrad(Grid g, const T* __restrict__ p, Fc<T> u, Fc<T> uo) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    const T hh = (T)g.h;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        T v = fsel(u, ax)[idx];
+        int e = ax == 0 ? i : (ax == 1 ? j : k), n = ax == 0 ? g.NX : (ax == 1 ? g.NY : g.NZ);
+        if (e > 0 && e < n) {
+            T d = (p[cid(g, i, j, k)] - p[cid(g, i - (ax == 0), j - (ax == 1), k - (ax == 2))]) / hh;
+            v = v - d;
+        }
+        fsel(uo, ax)[idx] = v;
+    }
+}
+// pbar = -G^T ubar on the unknown cells
+template <class T>
+__global__ void k_ad_pbar(Grid g, const int8_t* __restrict__ mark, Fc<T> ub, T* __restrict__ pb) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        T out = 0;
+        if (unknown(g, mark, idx, i, j, k))
+            out = (ub.x[fxi(g, i + 1, j, k)] - ub.x[fxi(g, i, j, k)] + ub.y[fyi(g, i, j + 1, k)] - ub.y[fyi(g, i, j, k)] +
+                   ub.z[fzi(g, i, j, k + 1)] - ub.z[fzi(g, i, j, k)]) / (T)g.h;
+        pb[idx] = out;
+    }
+}
+// ub_out = ub_in + D^T q (q is zero off the unknowns)
+template <class T>
+__global__ void k_ad_divT(Grid g, const T* __restrict__ q, Fc<T> ubi, Fc<T> ubo) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        int e = ax == 0 ? i : (ax == 1 ? j : k), n = ax == 0 ? g.NX : (ax == 1 ? g.NY : g.NZ);
+        T acc = fsel(ubi, ax)[idx];
+        T lo = e > 0 ? q[cid(g, i - (ax == 0), j - (ax == 1), k - (ax == 2))] : (T)0;
+        T hi = e < n ? q[cid(g, i, j, k)] : (T)0;
+        acc += (lo - hi) / (T)g.h;
+        fsel(ubo, ax)[idx] = acc;
+    }
+}
+// trilinear of the face/cell grids (the engine's trilinear) with its gradient
+// in grid units
+template <class T>
+__device__ __forceinline__ T tri(const T* u, T x, T y, T z, int w, int hh, int d, T* gx, T* gy, T* gz) {
+    x = x < (T)0 ? (T)0 : (x > (T)w ? (T)w : x);
+    y = y < (T)0 ? (T)0 : (y > (T)hh ? (T)hh : y);
+    z = z < (T)0 ? (T)0 : (z > (T)d ? (T)d : z);
+    int i = (int)(x < (T)(w - 2) ? x : (T)(w - 2));
+    int j = (int)(y < (T)(hh - 2) ? y : (T)(hh - 2));
+    int k = (int)(z < (T)(d - 2) ? z : (T)(d - 2));
+    int b = i * hh * d + j * d + k, sj = d, si = hh * d;
+    T u000 = u[b], u100 = u[b + si], u010 = u[b + sj], u110 = u[b + si + sj];
+    T u001 = u[b + 1], u101 = u[b + si + 1], u011 = u[b + sj + 1], u111 = u[b + si + sj + 1];
+    T fi1 = (T)(i + 1) - x, fi0 = x - (T)i, fj1 = (T)(j + 1) - y, fj0 = y - (T)j, fk1 = (T)(k + 1) - z, fk0 = z - (T)k;
+    T a0 = fj1 * (fi1 * u000 + fi0 * u100) + fj0 * (fi1 * u010 + fi0 * u110);
+    T a1 = fj1 * (fi1 * u001 + fi0 * u101) + fj0 * (fi1 * u011 + fi0 * u111);
+    if (gx) {
+        *gx = fk1 * (fj1 * (u100 - u000) + fj0 * (u110 - u010)) + fk0 * (fj1 * (u101 - u001) + fj0 * (u111 - u011));
+        *gy = fk1 * ((fi1 * u010 + fi0 * u110) - (fi1 * u000 + fi0 * u100)) +
+              fk0 * ((fi1 * u011 + fi0 * u111) - (fi1 * u001 + fi0 * u101));
+        *gz = a1 - a0;
+    }
+    return fk1 * a0 + fk0 * a1;
+}
+// the interpolation point of a particle for face axis `ax` (grid units)
+template <class T> __device__ __forceinline__ void ipos(int ax, T X, T Y, T Z, T& x, T& y, T& z) {
+    x = ax == 0 ? X : X - (T)0.5f; y = ax == 1 ? Y : Y - (T)0.5f; z = ax == 2 ? Z : Z - (T)0.5f;
+}
+template <class T>
+__global__ void k_ad_g2p(Grid g, int np, const T* __restrict__ x, const T* __restrict__ va, Fc<T> uf, Fc<T> du,
+                         T alpha, T* __restrict__ vg) {
+    MP_GRID_LOOP(p, np) {
+        T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
+        for (int ax = 0; ax < 3; ax++) {
+            const int w = ax == 0 ? g.NX + 1 : g.NX, hh = ax == 1 ? g.NY + 1 : g.NY, d = ax == 2 ? g.NZ + 1 : g.NZ;
+            T a, b, c; ipos(ax, X, Y, Z, a, b, c);
+            T gv = tri<T>(fsel(du, ax), a, b, c, w, hh, d, nullptr, nullptr, nullptr);
+            T iv = va[3 * p + ax];
+            if (alpha == (T)1) iv = iv + gv;
+            else {
+                T ug = tri<T>(fsel(uf, ax), a, b, c, w, hh, d, nullptr, nullptr, nullptr);
+                iv = ((T)1 - alpha) * ug + alpha * (iv + gv);
+            }
+            vg[3 * p + ax] = iv;
+        }
+    }
+}
+template <class T>
+__global__ void k_ad_advect(Grid g, int np, const T* __restrict__ x, const T* __restrict__ vg, T* __restrict__ xo,
+                            T* __restrict__ vo, T dt) {
+    const T h = (T)g.h;
+    MP_GRID_LOOP(p, np) {
+        for (int a = 0; a < 3; a++) {
+            const int n = a == 0 ? g.NX : (a == 1 ? g.NY : g.NZ);
+            const T lo = (T)0 + (h + (T)0.5f * h), hi = (T)n * h - (h + (T)0.5f * h);
+            T ip = x[3 * p + a] + vg[3 * p + a] * dt, iv = vg[3 * p + a];
+            if (ip <= lo) { ip = lo; iv = (T)0; }
+            if (ip >= hi) { ip = hi; iv = (T)0; }
+            xo[3 * p + a] = ip; vo[3 * p + a] = iv;
+        }
+    }
+}
+
+// ---- loss ------------------------------------------------------------------------
+template <class T>
+__global__ void k_ad_phi(Grid g, const T* __restrict__ x, const uint32_t* __restrict__ nearest, T* __restrict__ phi) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        const T h = (T)g.h, cap = (T)2.5f * h;
+        T d = cap;
+        uint32_t p = nearest[idx];
+        if (p != NONE) {
+            T dx = x[3 * p] - ((T)i + (T)0.5f) * h, dy = x[3 * p + 1] - ((T)j + (T)0.5f) * h, dz = x[3 * p + 2] - ((T)k + (T)0.5f) * h;
+            T dd = sqrt(dx * dx + dy * dy + dz * dz);
+            d = dd < cap ? dd : cap;
+        }
+        phi[idx] = d - (T)0.5f * h;
+    }
+}
+// loss = sum_s phi(y_s)^2 in FP64, one block in a fixed order; also keeps phi(y_s)
+template <class T>
+__global__ void k_ad_loss(Grid g, int ns, const float* __restrict__ sp, const T* __restrict__ phi, double* __restrict__ sv,
+                          double* __restrict__ loss) {
+    __shared__ double part[256];
+    double acc = 0;
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        T X = (T)sp[3 * s] / (T)g.h - (T)0.5f, Y = (T)sp[3 * s + 1] / (T)g.h - (T)0.5f, Z = (T)sp[3 * s + 2] / (T)g.h - (T)0.5f;
+        T v = tri<T>(phi, X, Y, Z, g.NX, g.NY, g.NZ, nullptr, nullptr, nullptr);
+        sv[s] = (double)v;
+        acc += (double)v * (double)v;
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int q = 0; q < (int)blockDim.x; q++) t += part[q];
+        *loss = t;
+    }
+}
+// the sample's base cell of the cell-centred trilinear
+__host__ __device__ inline void sample_base(float h, int NX, int NY, int NZ, float px, float py, float pz, int& i,
+                                            int& j, int& k) {
+    float x = px / h - 0.5f, y = py / h - 0.5f, z = pz / h - 0.5f;
+    x = x < 0 ? 0 : (x > NX ? NX : x); y = y < 0 ? 0 : (y > NY ? NY : y); z = z < 0 ? 0 : (z > NZ ? NZ : z);
+    i = (int)(x < NX - 2 ? x : NX - 2); j = (int)(y < NY - 2 ? y : NY - 2); k = (int)(z < NZ - 2 ? z : NZ - 2);
+}
+// phibar_c = sum over samples whose stencil holds c of 2 phi(y_s) w_sc
+template <class T>
+__global__ void k_ad_phibar(Grid g, const float* __restrict__ sp, const uint32_t* __restrict__ soff,
+                            const double* __restrict__ sv, T* __restrict__ pb) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        T acc = 0;
+        for (int a = 0; a <= 1; a++) for (int b = 0; b <= 1; b++) for (int c = 0; c <= 1; c++) {
+            int bi = i - a, bj = j - b, bk = k - c;
+            if (bi < 0 || bj < 0 || bk < 0) continue;
+            int base = cid(g, bi, bj, bk);
+            for (uint32_t s = soff[base]; s < soff[base + 1]; s++) {
+                T X = (T)sp[3 * s] / (T)g.h - (T)0.5f, Y = (T)sp[3 * s + 1] / (T)g.h - (T)0.5f, Z = (T)sp[3 * s + 2] / (T)g.h - (T)0.5f;
+                X = X < (T)0 ? (T)0 : (X > (T)g.NX ? (T)g.NX : X);
+                Y = Y < (T)0 ? (T)0 : (Y > (T)g.NY ? (T)g.NY : Y);
+                Z = Z < (T)0 ? (T)0 : (Z > (T)g.NZ ? (T)g.NZ : Z);
+                T fx = a ? X - (T)bi : (T)(bi + 1) - X, fy = b ? Y - (T)bj : (T)(bj + 1) - Y, fz = c ? Z - (T)bk : (T)(bk + 1) - Z;
+                acc += (T)2 * (T)sv[s] * fx * fy * fz;
+            }
+        }
+        pb[idx] = acc;
+    }
+}
+// xbar of each particle from the cells it is nearest to (+-3 cell box)
+template <class T>
+__global__ void k_ad_phi_x(Grid g, int np, const T* __restrict__ x, const uint32_t* __restrict__ nearest,
+                           const T* __restrict__ pb, T* __restrict__ xb) {
+    MP_GRID_LOOP(p, np) {
+        const T h = (T)g.h, cap = (T)2.5f * h;
+        int ci = (int)(x[3 * p] / h), cj = (int)(x[3 * p + 1] / h), ck = (int)(x[3 * p + 2] / h);
+        T gx = 0, gy = 0, gz = 0;
+        for (int di = -3; di <= 3; di++) for (int dj = -3; dj <= 3; dj++) for (int dk = -3; dk <= 3; dk++) {
+            int a = ci + di, b = cj + dj, c = ck + dk;
+            if (a < 0 || a >= g.NX || b < 0 || b >= g.NY || c < 0 || c >= g.NZ) continue;
+            int idx = cid(g, a, b, c);
+            if (nearest[idx] != (uint32_t)p) continue;
+            T dx = x[3 * p] - ((T)a + (T)0.5f) * h, dy = x[3 * p + 1] - ((T)b + (T)0.5f) * h, dz = x[3 * p + 2] - ((T)c + (T)0.5f) * h;
+            T dd = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dd < cap) || dd == (T)0) continue;
+            T s = pb[idx] / dd;
+            gx += s * dx; gy += s * dy; gz += s * dz;
+        }
+        xb[3 * p] = gx; xb[3 * p + 1] = gy; xb[3 * p + 2] = gz;
+    }
+}
+
+// ---- transposes of the particle stages -------------------------------------------
+// advection with the clamp: a clamped component passes nothing back
+template <class T>
+__global__ void k_ad_advect_adj(Grid g, int np, const T* __restrict__ x, const T* __restrict__ vg, T dt,
+                                T* __restrict__ xb, const T* __restrict__ vb, T* __restrict__ vgb) {
+    const T h = (T)g.h;
+    MP_GRID_LOOP(p, np) {
+        for (int a = 0; a < 3; a++) {
+            const int n = a == 0 ? g.NX : (a == 1 ? g.NY : g.NZ);
+            const T lo = (T)0 + (h + (T)0.5f * h), hi = (T)n * h - (h + (T)0.5f * h);
+            T ip = x[3 * p + a] + vg[3 * p + a] * dt;
+            bool clamped = false;
+            if (ip <= lo) { ip = lo; clamped = true; }
+            if (ip >= hi) { ip = hi; clamped = true; }
+            T xin = xb[3 * p + a];
+            if (clamped) { xb[3 * p + a] = (T)0; vgb[3 * p + a] = (T)0; }
+            else { vgb[3 * p + a] = vb[3 * p + a] + dt * xin; }
+        }
+    }
+}
+// gather part of the particle side of the G2P transpose: vabar and the
+// position derivative of the interpolation
+template <class T>
+__global__ void k_ad_g2p_adj_p(Grid g, int np, const T* __restrict__ x, Fc<T> uf, Fc<T> du, T alpha,
+                               const T* __restrict__ vgb, T* __restrict__ vab, T* __restrict__ xb) {
+    MP_GRID_LOOP(p, np) {
+        const T ih = (T)1 / (T)g.h;
+        T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
+        const T cdu = alpha == (T)1 ? (T)1 : alpha, cu = alpha == (T)1 ? (T)0 : (T)1 - alpha;
+        T gxs = 0, gys = 0, gzs = 0;
+        for (int ax = 0; ax < 3; ax++) {
+            const int w = ax == 0 ? g.NX + 1 : g.NX, hh = ax == 1 ? g.NY + 1 : g.NY, d = ax == 2 ? g.NZ + 1 : g.NZ;
+            T a, b, c; ipos(ax, X, Y, Z, a, b, c);
+            T vb = vgb[3 * p + ax];
+            T gx1, gy1, gz1, gx2 = 0, gy2 = 0, gz2 = 0;
+            tri<T>(fsel(du, ax), a, b, c, w, hh, d, &gx1, &gy1, &gz1);
+            if (cu != (T)0) tri<T>(fsel(uf, ax), a, b, c, w, hh, d, &gx2, &gy2, &gz2);
+            gxs += vb * (cdu * gx1 + cu * gx2); gys += vb * (cdu * gy1 + cu * gy2); gzs += vb * (cdu * gz1 + cu * gz2);
+            vab[3 * p + ax] = cdu * vb;
+        }
+        xb[3 * p] += gxs * ih; xb[3 * p + 1] += gys * ih; xb[3 * p + 2] += gzs * ih;
+    }
+}
+// face side of the G2P transpose: q_f = sum of w_pf vgbar_p over the particles
+// whose interpolation stencil holds f. Those lie in cells [i-1,i] along the
+// face normal and [-1,1] across; the candidates are taken one cell wider,
+// since the recorded cell lists come from the recorded positions, and
+// membership is decided from the replay's own positions.
+template <class T>
+__global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
+                               const T* __restrict__ x, const T* __restrict__ vgb, Fc<T> q) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        const int w = ax == 0 ? g.NX + 1 : g.NX, hh = ax == 1 ? g.NY + 1 : g.NY, d = ax == 2 ? g.NZ + 1 : g.NZ;
+        T acc = 0;
+        const int a0 = i - 2, a1 = ax == 0 ? i + 1 : i + 2, b0 = j - 2, b1 = ax == 1 ? j + 1 : j + 2;
+        const int c0 = k - 2, c1 = ax == 2 ? k + 1 : k + 2;
+        for (int a = a0; a <= a1; a++) {
+            if (a < 0 || a > g.NX - 1) continue;
+            for (int b = b0; b <= b1; b++) {
+                if (b < 0 || b > g.NY - 1) continue;
+                for (int cc = c0; cc <= c1; cc++) {
+                    if (cc < 0 || cc > g.NZ - 1) continue;
+                    int c = cid(g, a, b, cc);
+                    for (uint32_t s = off[c]; s < off[c + 1]; s++) {
+                        uint32_t p = order[s];
+                        T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
+                        T px, py, pz; ipos(ax, X, Y, Z, px, py, pz);
+                        px = px < (T)0 ? (T)0 : (px > (T)w ? (T)w : px);
+                        py = py < (T)0 ? (T)0 : (py > (T)hh ? (T)hh : py);
+                        pz = pz < (T)0 ? (T)0 : (pz > (T)d ? (T)d : pz);
+                        int bi = (int)(px < (T)(w - 2) ? px : (T)(w - 2));
+                        int bj = (int)(py < (T)(hh - 2) ? py : (T)(hh - 2));
+                        int bk = (int)(pz < (T)(d - 2) ? pz : (T)(d - 2));
+                        int ei = i - bi, ej = j - bj, ek = k - bk;
+                        if (ei < 0 || ei > 1 || ej < 0 || ej > 1 || ek < 0 || ek > 1) continue;
+                        T fx = ei ? px - (T)bi : (T)(bi + 1) - px, fy = ej ? py - (T)bj : (T)(bj + 1) - py;
+                        T fz = ek ? pz - (T)bk : (T)(bk + 1) - pz;
+                        acc += fx * fy * fz * vgb[3 * p + ax];
+                    }
+                }
+            }
+        }
+        fsel(q, ax)[idx] = acc;
+    }
+}
+// splat transpose per particle over the faces whose window holds its cell
+// (the particle's cell is the recorded one: window membership is frozen)
+template <class T>
+__global__ void k_ad_p2g_adj(Grid g, int np, const T* __restrict__ x, const T* __restrict__ va,
+                             const float* __restrict__ mass, const uint32_t* __restrict__ cellof, Fc<T> u, Fc<T> W,
+                             Fc<T> ub, T* __restrict__ vab, T* __restrict__ xb) {
+    const T scale = (T)1 / (T)g.h;
+    MP_GRID_LOOP(p, np) {
+        T X = x[3 * p] * scale, Y = x[3 * p + 1] * scale, Z = x[3 * p + 2] * scale;
+        int ca, cb, cc;
+        getijk3((int)cellof[p], g.NY, g.NZ, ca, cb, cc);
+        const T m = (T)mass[p];
+        T vb[3] = {0, 0, 0}, gxs = 0, gys = 0, gzs = 0;
+        for (int ax = 0; ax < 3; ax++) {
+            const int W_ = ax == 0 ? g.NX + 1 : g.NX, H_ = ax == 1 ? g.NY + 1 : g.NY, D_ = ax == 2 ? g.NZ + 1 : g.NZ;
+            const int i0 = ca, i1 = ax == 0 ? ca + 1 : ca + 1, j0 = cb - (ax == 1 ? 0 : 1), j1 = cb + 1;
+            const int k0 = cc - (ax == 2 ? 0 : 1), k1 = cc + 1;
+            // x-face window: cells [i-1,i] -> faces i in [a, a+1]; across: [-1,1] -> faces [b-1, b+1]
+            const int fi0 = ax == 0 ? i0 : ca - 1, fi1 = ax == 0 ? i1 : ca + 1;
+            const T pv = va[3 * p + ax];
+            for (int fi = fi0; fi <= fi1; fi++) {
+                if (fi < 0 || fi >= W_) continue;
+                for (int fj = j0; fj <= j1; fj++) {
+                    if (fj < 0 || fj >= H_) continue;
+                    for (int fk = k0; fk <= k1; fk++) {
+                        if (fk < 0 || fk >= D_) continue;
+                        int f = face_index(g, ax, fi, fj, fk);
+                        T Wf = fsel(W, ax)[f];
+                        if (!(Wf > (T)0)) continue;
+                        float gx, gy, gz; face_pos(ax, fi, fj, fk, gx, gy, gz);
+                        T dx = X - (T)gx, dy = Y - (T)gy, dz = Z - (T)gz;
+                        T r2 = dx * dx + dy * dy + dz * dz;
+                        T k_ = sharpk(r2);
+                        T kd = sharpk_d(r2);
+                        if (k_ == (T)0 && kd == (T)0) continue;
+                        T u_b = fsel(ub, ax)[f];
+                        vb[ax] += u_b * m * k_ / Wf;
+                        T s = u_b * (pv - fsel(u, ax)[f]) / Wf * m * kd * (T)2 * scale;
+                        gxs += s * dx; gys += s * dy; gzs += s * dz;
+                    }
+                }
+            }
+        }
+        vab[3 * p] += vb[0]; vab[3 * p + 1] += vb[1]; vab[3 * p + 2] += vb[2];
+        xb[3 * p] += gxs; xb[3 * p + 1] += gys; xb[3 * p + 2] += gzs;
+    }
+}
+// the cell each particle had in a step's recorded sort
+__global__ void k_ad_cellof(int ncell, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
+                            uint32_t* __restrict__ cellof) {
+    MP_GRID_LOOP(c, ncell) for (uint32_t s = off[c]; s < off[c + 1]; s++) cellof[order[s]] = (uint32_t)c;
+}
+template <class T> __global__ void k_ad_to_double(long long n, const T* __restrict__ a, double* __restrict__ o) {
+    MP_GRID_LOOP(t, n) o[t] = (double)a[t];
+}
+template <class T> __global__ void k_ad_from_float(long long n, const float* __restrict__ a, T* __restrict__ o) {
+    MP_GRID_LOOP(t, n) o[t] = (T)a[t];
+}
+template <class T> __global__ void k_ad_from_double(long long n, const double* __restrict__ a, T* __restrict__ o) {
+    MP_GRID_LOOP(t, n) o[t] = (T)a[t];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+void k_adj_free(MpCtx* c) {
+    AdjTape* t = c->adj;
+    if (!t) return;
+    for (auto* p : t->order) cudaFree(p);
+    for (auto* p : t->off) cudaFree(p);
+    for (auto* p : t->mark) cudaFree(p);
+    for (auto* p : t->phi) cudaFree(p);
+    for (void* p : {(void*)t->x0, (void*)t->v0, (void*)t->mass, (void*)t->ids, (void*)t->ids2, (void*)t->nearest,
+                    (void*)t->samples, (void*)t->s_off})
+        if (p) cudaFree(p);
+    for (void* p : t->wk) if (p) cudaFree(p);
+    delete t;
+    c->adj = nullptr;
+}
+
+template <class T> static int amalloc(MpCtx* c, T** p, size_t count) {
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1));
+    if (e != cudaSuccess) { c->err = std::string("adjoint: cudaMalloc: ") + cudaGetErrorString(e); return MP_ERR_CUDA; }
+    return MP_OK;
+}
+#define ADJ_LAUNCH(c) MP_CHECK_LAUNCH(c)
+
+static int sorted_ids(MpCtx* c, AdjTape* t) {
+    // after k_hash_sort: when the particles moved, slot s now holds the
+    // particle of old slot perm[s]
+    MP_TRY(k_hash_sort(c));
+    uint32_t moved = 0;
+    MP_CUDA(c, cudaMemcpyAsync(&moved, c->u32_scratch + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (moved) {
+        k_ad_permute_ids<<<mp_blocks(t->np, 256), 256, 0, c->stream>>>(t->np, c->perm, t->ids, t->ids2);
+        ADJ_LAUNCH(c);
+        std::swap(t->ids, t->ids2);
+    }
+    return MP_OK;
+}
+
+int k_adj_record(MpCtx* c, int nsteps, int every) {
+    const mp_params& P = c->P;
+    if (nsteps < 1 || every < 1) { c->err = "adj_record: nsteps and checkpoint interval must be positive"; return MP_ERR_ARG; }
+    if (P.b_correct_position || P.b_heat_trans || P.b_gen_gas || P.b_melt || P.b_freeze || P.b_solid) {
+        c->err = "adj_record: the adjoint covers the FLUID-only step without position correction, heat, gas, "
+                 "melting, freezing or solids";
+        return MP_ERR_STATE;
+    }
+    const int np = c->np();
+    if (np == 0) { c->err = "adj_record: no particles"; return MP_ERR_STATE; }
+    MP_CUDA(c, cudaMemsetAsync(c->u32_scratch + 3, 0, sizeof(uint32_t), c->stream));
+    k_ad_count_nonfluid<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, c->pos, c->u32_scratch + 3);
+    uint32_t nonfluid = 0;
+    MP_CUDA(c, cudaMemcpyAsync(&nonfluid, c->u32_scratch + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (nonfluid) { c->err = "adj_record: every particle must be FLUID"; return MP_ERR_STATE; }
+    k_adj_free(c);
+    AdjTape* t = new AdjTape();
+    c->adj = t;
+    t->np = np; t->nsteps = nsteps; t->every = every;
+    const Grid& g = c->G;
+    MP_TRY(amalloc(c, &t->ids, np)); MP_TRY(amalloc(c, &t->ids2, np));
+    MP_TRY(amalloc(c, &t->x0, 3 * (size_t)np)); MP_TRY(amalloc(c, &t->v0, 3 * (size_t)np));
+    MP_TRY(amalloc(c, &t->mass, np)); MP_TRY(amalloc(c, &t->nearest, g.n));
+    k_ad_iota<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids);
+    k_ad_snapshot<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->pos, c->vel, t->x0, t->v0, t->mass);
+    ADJ_LAUNCH(c);
+    for (int k = 0; k < nsteps; k++) {
+        MP_TRY(sorted_ids(c, t));
+        MP_TRY(k_external_force(c));
+        MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
+        uint32_t* ord; uint32_t* off; int8_t* mk; float* ph;
+        MP_TRY(amalloc(c, &ord, np)); t->order.push_back(ord);
+        MP_TRY(amalloc(c, &off, (size_t)g.n + 1)); t->off.push_back(off);
+        MP_TRY(amalloc(c, &mk, g.n)); t->mark.push_back(mk);
+        MP_TRY(amalloc(c, &ph, g.n)); t->phi.push_back(ph);
+        MP_CUDA(c, cudaMemcpyAsync(ord, t->ids, sizeof(uint32_t) * np, cudaMemcpyDeviceToDevice, c->stream));
+        MP_CUDA(c, cudaMemcpyAsync(off, c->cell_off, sizeof(uint32_t) * ((size_t)g.n + 1), cudaMemcpyDeviceToDevice, c->stream));
+        MP_CUDA(c, cudaMemcpyAsync(mk, c->mark, g.n, cudaMemcpyDeviceToDevice, c->stream));
+        MP_TRY(k_p2g(c));
+        MP_TRY(k_sweep_phi(c, MP_TYPEFLUID));
+        MP_CUDA(c, cudaMemcpyAsync(ph, c->phifluid, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, c->stream));
+        MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+        int st = k_project(c, nullptr, nullptr);
+        if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+        MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+        MP_TRY(k_g2p(c));
+        MP_TRY(sorted_ids(c, t));
+        MP_TRY(k_collide_advect(c, true));
+        MP_TRY(sorted_ids(c, t));
+        c->S.frame++;
+    }
+    // nearest particle of each cell at the end (cells from the last sort)
+    k_ad_nearest<<<mp_blocks(g.n, 256), 256, 0, c->stream>>>(g, Cells{c->cell_off, c->tmask}, c->pos, t->ids, t->nearest);
+    ADJ_LAUNCH(c);
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+
+int k_adj_set_targets(MpCtx* c, const float* sp, int ns) {
+    AdjTape* t = c->adj;
+    if (!t) { c->err = "adj_set_targets: record first"; return MP_ERR_STATE; }
+    if (ns < 1 || !sp) { c->err = "adj_set_targets: no samples"; return MP_ERR_ARG; }
+    const Grid& g = c->G;
+    std::vector<std::pair<int, int>> key(ns);
+    for (int s = 0; s < ns; s++) {
+        int i, j, k; sample_base(g.h, g.NX, g.NY, g.NZ, sp[3 * s], sp[3 * s + 1], sp[3 * s + 2], i, j, k);
+        key[s] = {(i * g.NY + j) * g.NZ + k, s};
+    }
+    std::stable_sort(key.begin(), key.end());
+    std::vector<float> sorted(3 * (size_t)ns);
+    std::vector<uint32_t> off((size_t)g.n + 1, 0);
+    for (int s = 0; s < ns; s++) {
+        for (int a = 0; a < 3; a++) sorted[3 * s + a] = sp[3 * key[s].second + a];
+        off[key[s].first + 1]++;
+    }
+    for (int q = 0; q < g.n; q++) off[q + 1] += off[q];
+    if (t->samples) cudaFree(t->samples);
+    if (t->s_off) cudaFree(t->s_off);
+    t->samples = nullptr; t->s_off = nullptr;
+    MP_TRY(amalloc(c, &t->samples, 3 * (size_t)ns)); MP_TRY(amalloc(c, &t->s_off, (size_t)g.n + 1));
+    MP_CUDA(c, cudaMemcpy(t->samples, sorted.data(), sizeof(float) * 3 * ns, cudaMemcpyHostToDevice));
+    MP_CUDA(c, cudaMemcpy(t->s_off, off.data(), sizeof(uint32_t) * (g.n + 1), cudaMemcpyHostToDevice));
+    t->nsamples = ns;
+    return MP_OK;
+}
+
+namespace {
+// work layout (element counts; each buffer allocated for `esz`-byte elements)
+enum {
+    W_XS, W_VS, W_VA, W_VG, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
+    W_UP, W_WT, W_UOLD, W_T0, W_UE, W_UPROJ, W_UF, W_DU, W_B0, W_B1, W_B2,
+    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_COUNT
+};
+}
+
+template <class T> struct Replay {
+    MpCtx* c; AdjTape* t; Grid g; long long nf; int np;
+    T* a(int w) const { return static_cast<T*>(t->wk[w]); }
+    Fc<T> f(int w) const { return faces_of<T>(t->wk[w], g); }
+    T* seg_x(int s) const { return a(W_XS) + (size_t)s * 3 * np; }
+    T* seg_v(int s) const { return a(W_VS) + (size_t)s * 3 * np; }
+};
+
+template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
+    if (t->wesz == sizeof(T) && (int)t->wk.size() == W_COUNT && t->wk_ns >= t->nsamples) return MP_OK;
+    for (void* p : t->wk) if (p) cudaFree(p);
+    t->wk.assign(W_COUNT, nullptr);
+    const Grid& g = c->G;
+    const size_t np3 = 3 * (size_t)t->np, nf = (size_t)g.nfx + g.nfy + g.nfz, n = g.n;
+    const int nseg = (t->nsteps + t->every - 1) / t->every;
+    size_t cnt[W_COUNT];
+    cnt[W_XS] = cnt[W_VS] = np3 * (size_t)(nseg + t->every);   // segment starts, then one segment's steps
+    for (int w : {W_VA, W_VG, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN}) cnt[w] = np3;
+    for (int w : {W_UP, W_WT, W_UOLD, W_T0, W_UE, W_UPROJ, W_UF, W_DU, W_B0, W_B1, W_B2}) cnt[w] = nf;
+    for (int w : {W_CB, W_CP, W_CQ, W_PHI}) cnt[w] = n;
+    cnt[W_SV] = (size_t)std::max(t->nsamples, 1) * 2;   // doubles
+    cnt[W_LOSS] = 2;
+    cnt[W_CELLOF] = (size_t)t->np;   // uint32
+    for (int w = 0; w < W_COUNT; w++) {
+        size_t es = (w == W_SV || w == W_LOSS) ? sizeof(double) : (w == W_CELLOF ? sizeof(uint32_t) : sizeof(T));
+        size_t bytes = es * std::max<size_t>(cnt[w], 1);
+        cudaError_t e = cudaMalloc(&t->wk[w], bytes);
+        if (e != cudaSuccess) { c->err = std::string("adjoint work: ") + cudaGetErrorString(e); return MP_ERR_CUDA; }
+    }
+    t->wesz = sizeof(T);
+    t->wk_ns = t->nsamples;
+    return MP_OK;
+}
+
+template <class T> static int cg_tol_of(const MpCtx* c, int& mode, float& tol, int& maxit) {
+    if (sizeof(T) == sizeof(double)) { mode = MP_TOL_REL; tol = 1e-13f; maxit = std::max(c->P.cg_max_iter, 6000); }
+    else { mode = c->P.cg_tol_mode; tol = c->P.cg_tol; maxit = c->P.cg_max_iter; }
+    return MP_OK;
+}
+
+// one step of the replay from (x, v) to (xo, vo); leaves the step's grid
+// intermediates in the work buffers
+template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, const T* v, T* xo, T* vo) {
+    MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
+    cudaStream_t s = c->stream;
+    const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
+    const mp_params& P = c->P;
+    k_ad_gravity<T><<<nbp, 256, 0, s>>>(R.np, v, R.a(W_VA), (T)P.dt * (T)P.gravity_z);
+    k_ad_p2g<T><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], t->mass, x, R.a(W_VA), R.f(W_UP), R.f(W_WT));
+    k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, R.a(W_UP), R.a(W_UOLD));
+    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_UP), R.f(W_T0), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B0), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), R.f(W_UE), t->mark[k]);
+    k_ad_div<T><<<nbc, 256, 0, s>>>(g, t->mark[k], R.f(W_UE), R.a(W_CB));
+    MP_CHECK_LAUNCH(c);
+    int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
+    int it = 0; double res = 0;
+    int st = k_cg_solve(c, t->mark[k], R.a(W_CP), R.a(W_CB), maxit, mode, tol, &it, &res);
+    if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+    k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, R.a(W_CP), R.f(W_UE), R.f(W_UPROJ));
+    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_UPROJ), R.f(W_B1), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_UF), t->mark[k]);
+    k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, R.a(W_UF), R.a(W_UOLD), R.a(W_DU));
+    k_ad_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VA), R.f(W_UF), R.f(W_DU), (T)P.flip_alpha, R.a(W_VG));
+    k_ad_advect<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VG), xo, vo, (T)P.dt);
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+// reverse of fwd_step (run right after it, on its intermediates): (xb, vb)
+// hold the adjoint of the step's outputs on entry and of its inputs on exit
+template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, T* xb, T* vb) {
+    MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
+    cudaStream_t s = c->stream;
+    const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
+    const mp_params& P = c->P;
+    const T alpha = (T)P.flip_alpha;
+    k_ad_advect_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VG), (T)P.dt, xb, vb, R.a(W_VGB));
+    k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.f(W_UF), R.f(W_DU), alpha, R.a(W_VGB), R.a(W_VAB), xb);
+    // q = I^T vgbar on B0; ufbar = q, uoldbar = -cdu q
+    k_ad_g2p_adj_f<T><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], x, R.a(W_VGB), R.f(W_B0));
+    const T cdu = alpha == (T)1 ? (T)1 : alpha;
+    // wall rules then the two passes, transposed (B0 -> B1 -> B2 -> B1)
+    k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), R.f(W_B1), R.f(W_B2), t->mark[k]);
+    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_T0), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B1), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    // projection: ubar_e = ubar_proj + D^T L^-1 (-G^T ubar_proj)
+    k_ad_pbar<T><<<nbc, 256, 0, s>>>(g, t->mark[k], R.f(W_B1), R.a(W_CB));
+    MP_CHECK_LAUNCH(c);
+    int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
+    int it = 0; double res = 0;
+    int st = k_cg_solve(c, t->mark[k], R.a(W_CQ), R.a(W_CB), maxit, mode, tol, &it, &res);
+    if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+    k_ad_divT<T><<<nbf, 256, 0, s>>>(g, R.a(W_CQ), R.f(W_B1), R.f(W_B2));
+    // wall rules and passes before the projection (input of the rule: B0 of the forward = W_T0's successor)
+    k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), R.f(W_UE), t->mark[k]);
+    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    // upbar = that + uoldbar
+    k_ad_axpy<T><<<nbf, 256, 0, s>>>(R.nf, -cdu, R.a(W_B0), R.a(W_B1));
+    // splat transpose (vabar += ..., xbar += ...)
+    uint32_t* cellof = static_cast<uint32_t*>(t->wk[W_CELLOF]);
+    k_ad_cellof<<<nbc, 256, 0, s>>>(g.n, t->order[k], t->off[k], cellof);
+    k_ad_p2g_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VA), t->mass, cellof, R.f(W_UP), R.f(W_WT), R.f(W_B1),
+                                        R.a(W_VAB), xb);
+    // gravity: vbar = vabar
+    k_ad_copy<T><<<nbp, 256, 0, s>>>(3LL * R.np, R.a(W_VAB), vb);
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+template <class T> static int adj_loss_fwd(const Replay<T>& R, const T* x, double* loss_host) {
+    MpCtx* c = R.c; AdjTape* t = R.t;
+    k_ad_phi<T><<<mp_blocks(R.g.n, 256), 256, 0, c->stream>>>(R.g, x, t->nearest, R.a(W_PHI));
+    double* sv = static_cast<double*>(t->wk[W_SV]);
+    double* dl = static_cast<double*>(t->wk[W_LOSS]);
+    k_ad_loss<T><<<1, 256, 0, c->stream>>>(R.g, t->nsamples, t->samples, R.a(W_PHI), sv, dl);
+    MP_CHECK_LAUNCH(c);
+    MP_CUDA(c, cudaMemcpyAsync(loss_host, dl, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+
+template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, double* loss) {
+    AdjTape* t = c->adj;
+    if (!t) { c->err = "adjoint: record first (mp_adj_record)"; return MP_ERR_STATE; }
+    if (!t->nsamples) { c->err = "adjoint: no target samples (mp_adj_set_targets)"; return MP_ERR_STATE; }
+    MP_TRY(adj_work<T>(c, t));
+    Replay<T> R{c, t, c->G, (long long)c->G.nfx + c->G.nfy + c->G.nfz, t->np};
+    cudaStream_t s = c->stream;
+    const long long np3 = 3LL * t->np;
+    const int nb3 = mp_blocks(np3, 256);
+    // forward over all steps, keeping the segment starts
+    T* x = R.a(W_X); T* v = R.a(W_V); T* xn = R.a(W_XN); T* vn = R.a(W_VN);
+    k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->x0, x);
+    if (v0) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, v0, v);
+    else k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->v0, v);
+    MP_CHECK_LAUNCH(c);
+    const int E = t->every, nseg = (t->nsteps + E - 1) / E;
+    std::vector<T*> ckx(nseg), ckv(nseg);
+    // segment starts live in a second set of slots after the per-step states
+    // when the work is large enough; otherwise the replay recomputes from 0
+    for (int k = 0; k < t->nsteps; k++) {
+        if (k % E == 0) {
+            int sgi = k / E;
+            ckx[sgi] = R.seg_x(sgi); ckv[sgi] = R.seg_v(sgi);
+            MP_CUDA(c, cudaMemcpyAsync(ckx[sgi], x, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
+            MP_CUDA(c, cudaMemcpyAsync(ckv[sgi], v, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
+        }
+        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn));
+        std::swap(x, xn); std::swap(v, vn);
+    }
+    double L = 0;
+    MP_TRY(adj_loss_fwd<T>(R, x, &L));
+    if (loss) *loss = L;
+    if (!grad) return MP_OK;
+    // loss transpose
+    T* xb = R.a(W_XB); T* vb = R.a(W_VB);
+    k_ad_phibar<T><<<mp_blocks(c->G.n, 256), 256, 0, s>>>(c->G, t->samples, t->s_off,
+                                                          static_cast<double*>(t->wk[W_SV]), R.a(W_CQ));
+    k_ad_phi_x<T><<<mp_blocks(t->np, 256), 256, 0, s>>>(c->G, t->np, x, t->nearest, R.a(W_CQ), xb);
+    MP_CUDA(c, cudaMemsetAsync(vb, 0, sizeof(T) * np3, s));
+    MP_CHECK_LAUNCH(c);
+    // reverse sweep, segment by segment: the segment's states are recomputed
+    // from its start into the per-step slots, then the steps are reversed,
+    // each after recomputing its own grid intermediates
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+        const int k0 = sg * E, len = std::min(t->nsteps, k0 + E) - k0;
+        MP_CUDA(c, cudaMemcpyAsync(R.seg_x(nseg), ckx[sg], sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
+        MP_CUDA(c, cudaMemcpyAsync(R.seg_v(nseg), ckv[sg], sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
+        for (int j = 0; j + 1 < len; j++)
+            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), R.seg_x(nseg + j + 1),
+                               R.seg_v(nseg + j + 1)));
+        for (int j = len - 1; j >= 0; j--) {
+            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), R.a(W_XN), R.a(W_VN)));
+            MP_TRY(adj_step<T>(R, k0 + j, R.seg_x(nseg + j), xb, vb));
+        }
+    }
+    k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, vb, grad);
+    MP_CHECK_LAUNCH(c);
+    MP_CUDA(c, cudaStreamSynchronize(s));
+    return MP_OK;
+}
+
+int k_adj_run(MpCtx* c, int precision, const double* v0, double* grad, double* loss) {
+    if (precision == MP_PREC_FP64) return adj_run<double>(c, v0, grad, loss);
+    return adj_run<float>(c, v0, grad, loss);
+}
+int k_adj_np(MpCtx* c, int* np, int* nsteps) {
+    if (!c->adj) { c->err = "adjoint: record first"; return MP_ERR_STATE; }
+    if (np) *np = c->adj->np;
+    if (nsteps) *nsteps = c->adj->nsteps;
+    return MP_OK;
+}

@@ -730,6 +730,23 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     return hflag[F_DONE] == DONE_CAP ? MP_ERR_NOCONVERGE : MP_OK;
 }
 
+// The pressure matrix of project_CG_bubble for a given mark field, solved on
+// the context's CG scratch (FP32 vectors: cg_r/cg_p/cg_z; FP64: the last
+// three fifths of cg64). x is cleared first. Used by the adjoint module.
+int k_cg_solve(MpCtx* c, const int8_t* mark, float* x, const float* b, int maxiter, int tolmode, float tol, int* iters,
+               double* res) {
+    PressOp op{c->G, mark};
+    return run_cg<float>(c, op, x, b, c->cg_r, c->cg_p, c->cg_z, maxiter, tolmode, tol, 0, iters, res,
+                         MP_KT_CG_STENCIL);
+}
+int k_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, int maxiter, int tolmode, float tol,
+               int* iters, double* res) {
+    PressOp op{c->G, mark};
+    const size_t n = (size_t)c->G.n;
+    return run_cg<double>(c, op, x, b, c->cg64 + 2 * n, c->cg64 + 3 * n, c->cg64 + 4 * n, maxiter, tolmode, tol, 0,
+                          iters, res, MP_KT_CG_STENCIL);
+}
+
 // project_CG_bubble (spray.cu:1590-1611)
 int k_project(MpCtx* c, int* iters, double* res) {
     const Grid& g = c->G;

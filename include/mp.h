@@ -347,6 +347,30 @@ int mp_mc_download_field(void* ctx, float* dens, uint8_t* cubeindex);
  * the collision reads them only within half a cell of a solid. */
 int mp_step(void* ctx);
 
+/* ---- adjoint (no counterpart in the reference) -------------------------------
+ * Reverse-mode derivative of the step for a scene of FLUID particles only,
+ * with position correction, heat, gas, melting, freezing and solids off
+ * (configuration 4, the dam break). mp_adj_record runs `nsteps` engine steps
+ * from the current particles (advancing the context) and records the
+ * discrete state of each step (splat order and cell ranges, cell marks, the
+ * extrapolation distance field, and at the end each cell's nearest particle);
+ * the derivative is that of the program with this state held fixed.
+ * mp_adj_set_targets takes the target points y_s (host float xyz) of the
+ * loss L = sum_s phi(y_s)^2, phi the fluid distance field of genlevelset
+ * after the last step. mp_adj_loss replays the program from the recorded
+ * initial particles with initial velocities v0 (device, double xyz per
+ * particle in the order the particles had at mp_adj_record; NULL: the
+ * recorded ones) and returns L; mp_adj_gradient also writes dL/dv0 (device,
+ * double xyz). precision: MP_PREC_MIXED replays in FP32 (CG dots in FP64),
+ * MP_PREC_FP64 in FP64 with a 1e-13 relative CG stop. States are kept every
+ * `checkpoint_every` steps and recomputed segment by segment backwards. */
+int mp_adj_record(void* ctx, int nsteps, int checkpoint_every);
+int mp_adj_set_targets(void* ctx, const float* samples3, int nsamples);
+int mp_adj_info(void* ctx, int* np, int* nsteps);
+int mp_adj_loss(void* ctx, int precision, const double* v0, double* loss);
+int mp_adj_gradient(void* ctx, int precision, const double* v0, double* grad_v0, double* loss);
+int mp_adj_release(void* ctx);
+
 /* Checkpoint / resume of the state a step starts from: particles, the random
  * table, nucleation cells, the fixed-heat field, the heat grid and mp_state.
  * A context created with identical parameters that loads a checkpoint and
