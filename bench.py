@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-n", type=int, default=64, help="grid of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adj-steps", type=int, default=8, help="steps of the forward+adjoint measurement (0: skip)")
+    ap.add_argument("--adj-every", type=int, default=4, help="checkpoint interval of the adjoint")
     ap.add_argument("--profile-case", default="", choices=["", "cg", "step"],
                     help="small-footprint cases for ncu captures instead of the bench line: "
                          "cg = one pressure solve on an n^3 liquid slab (z < 0.8) with a seeded divergence; "
@@ -219,6 +221,46 @@ def profile_case(args):
     sim.close()
 
 
+def fwd_adjoint(args, n, local, dist):
+    """Forward + adjoint throughput on the FLUID-only program the adjoint covers
+    (configuration 4, the dam break, at the bench's grid): the recorded engine
+    steps plus the gradient of the loss with respect to the initial particle
+    velocities (FP32 replay and transpose, checkpoints every --adj-every steps),
+    timed with CUDA events on the context's stream, max over ranks."""
+    import importlib
+    import torch
+    mp = importlib.import_module("2017multiphase_b200")
+    sim = mp.Sim.from_config(4, n, replica_seed(2017004, int(os.environ.get("RANK", "0"))))
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    targets = mp.dam_break_targets(4096, 2017004, height=0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    sim.adj_record(args.adj_steps, args.adj_every)
+    e1.record(stream)
+    sim.adj_set_targets(targets)
+    loss, grad = sim.adj_gradient(None, mp.PREC_MIXED)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms, adj_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    tot = fwd_ms + adj_ms
+    if dist:
+        t = torch.tensor([tot], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot = float(t.item())
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    res = {"value": world * args.adj_steps / (tot / 1e3), "unit": "steps/s", "steps": args.adj_steps,
+           "checkpoint_every": args.adj_every, "fwd_ms_per_step": fwd_ms / args.adj_steps,
+           "adjoint_ms_per_step": adj_ms / args.adj_steps, "particles": sim.adj_num_particles(),
+           "loss": loss, "grad_norm": float(grad.norm()),
+           "workload": f"dam break {n}^3 (liquid x<0.4, z<0.6, FLUID only, no position correction), "
+                       f"loss = sum phi^2 on 4096 target points at z=0.3, dL/dv0 in FP32"}
+    sim.close()
+    return res
+
+
 def main():
     args = parse()
     if args.profile_case:
@@ -357,6 +399,10 @@ def main():
            "mesh": {"verts": [int(v) for v in st.mc_verts], "triangles": [int(v) // 3 for v in st.mc_indices]},
            "kernel_ms": {names[k]: {"ms": kt[k][0], "launches": kt[k][1]} for k in classes},
            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
+    nx = p.nx
+    sim.close()
+    if args.adj_steps > 0:
+        out["fwd_adjoint"] = fwd_adjoint(args, nx, local, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             times, threads, npart = cpu_sample(args.config, args.cpu_n, args.seed)
@@ -371,7 +417,6 @@ def main():
                                    "sample": f"failed: {e}"}
     if rank == 0:
         print(json.dumps(out), flush=True)
-    sim.close()
     if dist:
         dist.destroy_process_group()
 
