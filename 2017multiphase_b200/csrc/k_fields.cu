@@ -163,6 +163,69 @@ __global__ void k_initphi(int n, int NX, float* __restrict__ phi, const int8_t* 
 }
 
 // sweepu_k_bubble (spray_k.cu:3779-3880): one pass over all three face sets
+// One extrapolation pass for a face of axis AX (sweepu_k_bubble): a face
+// between two cells that are not of type fl takes the weighted average of
+// its three upwind neighbour faces of the last octant (in the reference's
+// loop order) whose three weights are all non-negative, else keeps its value.
+// The eight level-set values the octants read are loaded once, and only the
+// chosen octant's average is formed (the reference overwrites the result
+// for every valid octant, so the last one is what remains).
+template <int AX>
+__device__ __forceinline__ float sweepu_face(const Grid& g, const float* __restrict__ in, const float* __restrict__ ls,
+                                             const int8_t* __restrict__ mark, int fl, int i, int j, int k, int idx) {
+    const int sI = g.NY * g.NZ, sJ = g.NZ;
+    const int c0 = cid(g, i, j, k), c1 = c0 - (AX == 0 ? sI : (AX == 1 ? sJ : 1));
+    float res = in[idx];
+    const int e = AX == 0 ? i : (AX == 1 ? j : k), n = AX == 0 ? g.NX : (AX == 1 ? g.NY : g.NZ);
+    if (!(e > 1 && e < n - 1 && mark[c0] != fl && mark[c1] != fl)) return res;
+    const float l0 = ls[c0], l1 = ls[c1];
+    // the two cross axes (p, q) of this face axis, in the order the weights are named
+    const int sP = AX == 0 ? sJ : sI, sQ = AX == 2 ? sJ : 1;
+    const int ep = AX == 0 ? j : i, np_ = AX == 0 ? g.NY : g.NX;
+    const int eq = AX == 2 ? j : k, nq = AX == 2 ? g.NY : g.NZ;
+    // the cross neighbours' values, kept apart so the sums keep the reference's
+    // order ((l0 + l1 - l(c0 + s)) - l(c1 + s))
+    float p0[2] = {0, 0}, p1[2] = {0, 0}, q0[2] = {0, 0}, q1[2] = {0, 0};
+    bool okp[2], okq[2];
+    for (int t = 0; t < 2; t++) {
+        int d = t == 0 ? -1 : 1;
+        okp[t] = ep + d >= 0 && ep + d <= np_ - 1;
+        okq[t] = eq + d >= 0 && eq + d <= nq - 1;
+        if (okp[t]) { p0[t] = ls[c0 + d * sP]; p1[t] = ls[c1 + d * sP]; }
+        if (okq[t]) { q0[t] = ls[c0 + d * sQ]; q1[t] = ls[c1 + d * sQ]; }
+    }
+    int sd = 0, sp = 0, sq = 0; float w0 = 0, wp = 0, wq = 0; bool found = false;
+    // loop order of the reference: di, dj, dk each -1 then +1
+    for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
+        const int dn = AX == 0 ? di : (AX == 1 ? dj : dk);          // along the face normal
+        const int dpp = AX == 0 ? dj : di, dqq = AX == 2 ? dj : dk;  // across
+        const int tp = dpp > 0, tq = dqq > 0;
+        if (!okp[tp] || !okq[tq]) continue;
+        float wn = (float)(-dn) * (l0 - l1);
+        if (wn < 0) continue;
+        float a = (l0 + l1 - p0[tp] - p1[tp]) * 0.5f;
+        if (a < 0) continue;
+        float b = (l0 + l1 - q0[tq] - q1[tq]) * 0.5f;
+        if (b < 0) continue;
+        sd = dn; sp = dpp; sq = dqq; w0 = wn; wp = a; wq = b; found = true;
+    }
+    if (!found) return res;
+    // name the weights by axis as the reference does (wx, wy, wz)
+    float wx, wy, wz;
+    if (AX == 0) { wx = w0; wy = wp; wz = wq; }
+    else if (AX == 1) { wy = w0; wx = wp; wz = wq; }
+    else { wz = w0; wx = wp; wy = wq; }
+    float ws = wx + wy + wz;
+    if (ws == 0) wx = wy = wz = 1.0f / 3;
+    else { wx /= ws; wy /= ws; wz /= ws; }
+    int di, dj, dk;
+    if (AX == 0) { di = sd; dj = sp; dk = sq; }
+    else if (AX == 1) { dj = sd; di = sp; dk = sq; }
+    else { dk = sd; di = sp; dj = sq; }
+    if (AX == 0) return wx * in[fxi(g, i + di, j, k)] + wy * in[fxi(g, i, j + dj, k)] + wz * in[fxi(g, i, j, k + dk)];
+    if (AX == 1) return wx * in[fyi(g, i + di, j, k)] + wy * in[fyi(g, i, j + dj, k)] + wz * in[fyi(g, i, j, k + dk)];
+    return wx * in[fzi(g, i + di, j, k)] + wy * in[fzi(g, i, j + dj, k)] + wz * in[fzi(g, i, j, k + dk)];
+}
 __global__ void k_sweepu(Grid g, const float* __restrict__ ix, const float* __restrict__ iy, const float* __restrict__ iz,
                          float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
                          const float* __restrict__ ls, const int8_t* __restrict__ mark, int fl) {
@@ -171,74 +234,19 @@ __global__ void k_sweepu(Grid g, const float* __restrict__ ix, const float* __re
         int i, j, k;
         if (t < g.nfx) {
             int idx = (int)t;
-            float res = ix[idx];
             getijk3(idx, g.NY, g.NZ, i, j, k);
-            if (i > 1 && i < g.NX - 1 && mark[cid(g, i, j, k)] != fl && mark[cid(g, i - 1, j, k)] != fl) {
-                float l0 = ls[cid(g, i, j, k)], l1 = ls[cid(g, i - 1, j, k)];
-                for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
-                    if (j + dj < 0 || j + dj > g.NY - 1 || k + dk < 0 || k + dk > g.NZ - 1) continue;
-                    float wx = (float)(-di) * (l0 - l1);
-                    if (wx < 0) continue;
-                    float wy = (l0 + l1 - ls[cid(g, i, j + dj, k)] - ls[cid(g, i - 1, j + dj, k)]) * 0.5f;
-                    if (wy < 0) continue;
-                    float wz = (l0 + l1 - ls[cid(g, i, j, k + dk)] - ls[cid(g, i - 1, j, k + dk)]) * 0.5f;
-                    if (wz < 0) continue;
-                    float ws = wx + wy + wz;
-                    if (ws == 0) wx = wy = wz = 1.0f / 3;
-                    else { wx /= ws; wy /= ws; wz /= ws; }
-                    res = wx * ix[fxi(g, i + di, j, k)] + wy * ix[fxi(g, i, j + dj, k)] + wz * ix[fxi(g, i, j, k + dk)];
-                }
-            }
-            ox[idx] = res;
+            ox[idx] = sweepu_face<0>(g, ix, ls, mark, fl, i, j, k, idx);
         } else if (t < (long long)g.nfx + g.nfy) {
             int idx = (int)(t - g.nfx);
-            float res = iy[idx];
             getijk3(idx, g.NY + 1, g.NZ, i, j, k);
-            if (j > 1 && j < g.NY - 1 && mark[cid(g, i, j, k)] != fl && mark[cid(g, i, j - 1, k)] != fl) {
-                float l0 = ls[cid(g, i, j, k)], l1 = ls[cid(g, i, j - 1, k)];
-                for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
-                    if (i + di < 0 || i + di > g.NX - 1 || k + dk < 0 || k + dk > g.NZ - 1) continue;
-                    float wy = (float)(-dj) * (l0 - l1);
-                    if (wy < 0) continue;
-                    float wx = (l0 + l1 - ls[cid(g, i + di, j, k)] - ls[cid(g, i + di, j - 1, k)]) * 0.5f;
-                    if (wx < 0) continue;
-                    float wz = (l0 + l1 - ls[cid(g, i, j, k + dk)] - ls[cid(g, i, j - 1, k + dk)]) * 0.5f;
-                    if (wz < 0) continue;
-                    float ws = wx + wy + wz;
-                    if (ws == 0) wx = wy = wz = 1.0f / 3;
-                    else { wx /= ws; wy /= ws; wz /= ws; }
-                    res = wx * iy[fyi(g, i + di, j, k)] + wy * iy[fyi(g, i, j + dj, k)] + wz * iy[fyi(g, i, j, k + dk)];
-                }
-            }
-            oy[idx] = res;
+            oy[idx] = sweepu_face<1>(g, iy, ls, mark, fl, i, j, k, idx);
         } else {
             int idx = (int)(t - g.nfx - g.nfy);
-            float res = iz[idx];
             getijk3(idx, g.NY, g.NZ + 1, i, j, k);
-            if (k > 1 && k < g.NZ - 1 && mark[cid(g, i, j, k)] != fl && mark[cid(g, i, j, k - 1)] != fl) {
-                float l0 = ls[cid(g, i, j, k)], l1 = ls[cid(g, i, j, k - 1)];
-                for (int di = -1; di <= 1; di += 2) for (int dj = -1; dj <= 1; dj += 2) for (int dk = -1; dk <= 1; dk += 2) {
-                    if (i + di < 0 || i + di > g.NX - 1 || j + dj < 0 || j + dj > g.NY - 1) continue;
-                    float wz = (float)(-dk) * (l0 - l1);
-                    if (wz < 0) continue;
-                    float wy = (l0 + l1 - ls[cid(g, i, j + dj, k)] - ls[cid(g, i, j + dj, k - 1)]) * 0.5f;
-                    if (wy < 0) continue;
-                    float wx = (l0 + l1 - ls[cid(g, i + di, j, k)] - ls[cid(g, i + di, j, k - 1)]) * 0.5f;
-                    if (wx < 0) continue;
-                    float ws = wx + wy + wz;
-                    if (ws == 0) wx = wy = wz = 1.0f / 3;
-                    else { wx /= ws; wy /= ws; wz /= ws; }
-                    res = wx * iz[fzi(g, i + di, j, k)] + wy * iz[fzi(g, i, j + dj, k)] + wz * iz[fzi(g, i, j, k + dk)];
-                }
-            }
-            oz[idx] = res;
+            oz[idx] = sweepu_face<2>(g, iz, ls, mark, fl, i, j, k, idx);
         }
     }
 }
-
-// setWaterBoundaryU_k (spray_k.cu:956-995). Faces below the ceiling are only
-// ever zeroed, so the ceiling rule's read of the face below sees either the
-// old value (then re-applies that face's rule) or the zero it was set to.
 __device__ __forceinline__ float zrule(const Grid& g, const int8_t* mark, int i, int j, int k, float v) {
     if (k <= 1) return 0.0f;
     if (k > 0 && k < g.NZ && ((mark[cid(g, i, j, k)] == MP_TYPEBOUNDARY) != (mark[cid(g, i, j, k - 1)] == MP_TYPEBOUNDARY)))

@@ -126,6 +126,26 @@ __global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const fl
     }
 }
 
+// raises *flag when some cell's type mask has `bits`
+__global__ void k_mc_any_type(long long n, const uint8_t* __restrict__ tmask, uint32_t bits, uint32_t* flag) {
+    MP_GRID_LOOP(c, n) {
+        bool hit = (tmask[c] & bits) != 0;
+        if (__any_sync(__activemask(), hit) && (threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1))
+            atomicOr(flag, 1u);
+    }
+}
+// the solid field when no cell holds a SOLID particle: every node has wsum = 0,
+// so the density pass writes -r, and -10 on the border (its min with -r)
+__global__ void k_mc_solid_empty(McGrid m, float* __restrict__ dens) {
+    const long long tot = (long long)m.W * m.H * m.D;
+    const float r = 0.75f * m.hm;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k; getijk3((int)t, m.H, m.D, i, j, k);
+        bool border = (i * j * k == 0 || i == m.NXMC || j == m.NYMC || k == m.NZMC);
+        dens[t] = border ? fminf(-r, -10.0f) : -r;
+    }
+}
+
 __device__ __forceinline__ float node(const McGrid& m, const float* d, int i, int j, int k) {
     return d[(size_t)i * m.H * m.D + (size_t)j * m.D + k];
 }
@@ -275,9 +295,21 @@ int k_mc(MpCtx* c, int surface) {
     const McGrid m = mc_grid(c);
     Cells cl{c->cell_off, c->tmask};
     cudaStream_t s = c->stream;
+    bool solid_empty = false;
+    if (surface == MP_MC_SOLID) {
+        const long long nvox = (long long)m.NXMC * m.NYMC * m.NZMC;
+        MP_CUDA(c, cudaMemsetAsync(c->u32_scratch + 4, 0, sizeof(uint32_t), s));
+        k_mc_any_type<<<mp_blocks(nvox, 256), 256, 0, s>>>(nvox, c->tmask, 1u << MP_TYPESOLID, c->u32_scratch + 4);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        uint32_t any = 1;
+        MP_TRY(readback(c, c->u32_scratch + 4, &any));
+        solid_empty = any == 0;
+    }
     {
         KtScope kt(c, MP_KT_MC_DENS);
-        if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
+        if (solid_empty) k_mc_solid_empty<<<mp_blocks((long long)m.W * m.H * m.D, 256), 256, 0, s>>>(m, c->mc_dens);
+        else if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
         else if (surface == MP_MC_FLUID) k_mc_density<MP_MC_FLUID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
         else k_mc_density<MP_MC_GAS><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
     }

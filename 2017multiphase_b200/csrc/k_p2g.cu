@@ -60,33 +60,26 @@ __global__ void __launch_bounds__(256) k_p2g_faces(Grid g, Cells cl, const float
                         bool ok = WHICH == 0 ? (f == MP_TYPEFLUID || f == MP_TYPESOLID) : (f == MP_TYPEAIR);
                         if (!ok) continue;
                         // sharp_kernel(r2, 1.4) is exactly zero once r2 exceeds 1.4^2, and a
-                        // zero weight adds +-0 to both sums: such pairs are skipped
+                        // zero weight adds +-0 to both sums: such pairs are skipped, and the
+                        // velocity is read only when some face takes the particle
                         const float cut = (1.4f * 1.4f) * 1.0001f;
-                        float4 v = __ldg(vel + p);
                         float3 ps = mk3(q.x, q.y, q.z) * scale;
-                        if (ax) {
-                            float3 d = ps - gpx;
-                            float r2 = dot(d, d);
-                            if (r2 <= cut) {
-                                float w = v.w * sharp_kernel(r2, 1.4f);
-                                wx += w; sx += w * v.x;
-                            }
+                        float3 dx = ps - gpx, dy = ps - gpy, dz = ps - gpz;
+                        float r2x = dot(dx, dx), r2y = dot(dy, dy), r2z = dot(dz, dz);
+                        bool tx = ax && r2x <= cut, ty = ay && r2y <= cut, tz = az && r2z <= cut;
+                        if (!(tx || ty || tz)) continue;
+                        float4 v = __ldg(vel + p);
+                        if (tx) {
+                            float w = v.w * sharp_kernel(r2x, 1.4f);
+                            wx += w; sx += w * v.x;
                         }
-                        if (ay) {
-                            float3 d = ps - gpy;
-                            float r2 = dot(d, d);
-                            if (r2 <= cut) {
-                                float w = v.w * sharp_kernel(r2, 1.4f);
-                                wy += w; sy += w * v.y;
-                            }
+                        if (ty) {
+                            float w = v.w * sharp_kernel(r2y, 1.4f);
+                            wy += w; sy += w * v.y;
                         }
-                        if (az) {
-                            float3 d = ps - gpz;
-                            float r2 = dot(d, d);
-                            if (r2 <= cut) {
-                                float w = v.w * sharp_kernel(r2, 1.4f);
-                                wz += w; sz += w * v.z;
-                            }
+                        if (tz) {
+                            float w = v.w * sharp_kernel(r2z, 1.4f);
+                            wz += w; sz += w * v.z;
                         }
                     }
                 }
