@@ -306,10 +306,11 @@ int k_mc(MpCtx* c, int surface) {
         MP_TRY(readback(c, c->u32_scratch + 4, &any));
         solid_empty = any == 0;
     }
-    {
+    if (solid_empty) {
+        k_mc_solid_empty<<<mp_blocks((long long)m.W * m.H * m.D, 256), 256, 0, s>>>(m, c->mc_dens);
+    } else {
         KtScope kt(c, MP_KT_MC_DENS);
-        if (solid_empty) k_mc_solid_empty<<<mp_blocks((long long)m.W * m.H * m.D, 256), 256, 0, s>>>(m, c->mc_dens);
-        else if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
+        if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
         else if (surface == MP_MC_FLUID) k_mc_density<MP_MC_FLUID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
         else k_mc_density<MP_MC_GAS><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
     }

@@ -34,6 +34,24 @@ CG_DIR_TRAFFIC_PER_CELL = None
 CG_UPD_TRAFFIC_PER_CELL = None
 
 
+def names_kt(mp):
+    return {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g_faces",
+            mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
+
+
+# DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum),
+# as functions of (cells, particles): the capture's bytes scaled by the units a
+# launch processes (profiles/ gives each capture and its command)
+TRAFFIC_PER_LAUNCH = {
+    # profiles/cg_v4_liquid_slab_256.md: 175.4 MB and 258.9 MB per launch at 256^3
+    "k_cg_dir": lambda n, np_: 175.37e6 * n / 256 ** 3,
+    "k_cg_upd": lambda n, np_: 258.86e6 * n / 256 ** 3,
+    # profiles/mc_density_correctpos_bubble_column_128.md: 711.9 MB per launch at
+    # 128^3 (12.9M particles); nodes and particles both grow with the cells
+    "k_mc_density": lambda n, np_: 711.91e6 * n / 128 ** 3,
+}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -365,23 +383,39 @@ def main():
     e2e = {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h / max(args.e2e_steps, 1))}
 
-    # roofline of the dominant kernel class (by device time in the timed region)
+    # roofline of the dominant kernel class (by device time in the timed
+    # region); algorithmic bytes per launch from the compulsory-traffic model
+    # (each byte a launch must move, counted once; N_p particles, n cells)
     peak, peak_kind = peaks()
-    dom = max([mp.KT_CG_STENCIL, mp.KT_CG_UPDATE], key=lambda k: kt[k][0])
-    bpc = CG_DIR_BYTES_PER_CELL if dom == mp.KT_CG_STENCIL else CG_UPD_BYTES_PER_CELL
-    tpc = CG_DIR_TRAFFIC_PER_CELL if dom == mp.KT_CG_STENCIL else CG_UPD_TRAFFIC_PER_CELL
+    npart = int(sim.state().par_num_now)
+    model = {mp.KT_CG_STENCIL: ("k_cg_v4<PressOp,0> (direction + A p)", CG_DIR_BYTES_PER_CELL * n),
+             mp.KT_CG_UPDATE: ("k_cg_v4<PressOp,1> (x, r update)", CG_UPD_BYTES_PER_CELL * n),
+             mp.KT_P2G: ("k_p2g_faces (water + air launches)", 29 * npart + 56 * n),
+             mp.KT_G2P: ("k_g2p", 37 * npart + 72 * n),
+             mp.KT_SORT: ("hash sort (count, scan, scatter, segment sort, gather)", 102 * npart + 8 * n),
+             mp.KT_LEVELSET: ("k_genlevelset", 13 * npart + 9 * n),
+             mp.KT_MC_DENS: ("k_mc_density (fused fluid + gas fields at 2x)", 13 * npart + 64 * n)}
+    dom = max(model, key=lambda k: kt[k][0])
     ms_k, nl = kt[dom]
     per_launch_s = ms_k / 1e3 / max(nl, 1)
-    achieved = bpc * n / per_launch_s / 1e9
+    alg = model[dom][1]
+    achieved = alg / per_launch_s / 1e9
+    traffic = TRAFFIC_PER_LAUNCH.get(names_kt(mp)[dom])
     cg_ms = kt[mp.KT_CG_STENCIL][0] + kt[mp.KT_CG_UPDATE][0]
     cg_launch_pairs = max(kt[mp.KT_CG_STENCIL][1], 1)
     pcg_gbs = (CG_DIR_BYTES_PER_CELL + CG_UPD_BYTES_PER_CELL) * n * cg_launch_pairs / (cg_ms / 1e3) / 1e9
-    names = {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g_faces",
-             mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
-    roof = {"kernel": names[dom], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-            "traffic": (tpc * n if tpc else None), "algorithmic_bytes_per_launch": bpc * n,
+    names = names_kt(mp)
+    psrc = f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback"
+    roof = {"kernel": model[dom][0], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": psrc,
+            "traffic": (traffic(n, npart) if traffic else None), "algorithmic_bytes_per_launch": alg,
             "avg_launch_ms": per_launch_s * 1e3}
+    cls_table = {}
+    for k, (nm, b) in model.items():
+        ms_c, nl_c = kt[k]
+        if nl_c:
+            a = b / (ms_c / 1e3 / nl_c) / 1e9
+            cls_table[names[k]] = {"ms": ms_c, "launches": nl_c, "algorithmic_GBps": a, "frac": a / peak}
 
     st = sim.state()
     out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
@@ -395,9 +429,11 @@ def main():
                       "l2": "inputs larger than L2 (particle streams alone are ~5 GB)",
                       "parallelism": f"replicas x{world}"},
            "roofline": roof, "pcg_hbm_gbs": pcg_gbs,
+           "pcg_roofline": {"achieved": pcg_gbs, "peak": peak, "unit": "GB/s", "frac": pcg_gbs / peak,
+                            "note": "both CG passes, 34 B/cell/iteration algorithmic"},
            "cg_iters_per_step": cg_iters / max(args.steps, 1),
            "mesh": {"verts": [int(v) for v in st.mc_verts], "triangles": [int(v) // 3 for v in st.mc_indices]},
-           "kernel_ms": {names[k]: {"ms": kt[k][0], "launches": kt[k][1]} for k in classes},
+           "kernel_classes": cls_table,
            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
     nx = p.nx
     sim.close()
