@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(PM_X * PM_Y) k_cg_pm(Op op, PmGeom pg, const u
 // there for the whole solve (x and the direction vectors are cleared at the
 // start, r by k_cg_init), and nothing writes them.
 template <class Op, int MODE>
-__global__ void __launch_bounds__(CG_T) k_cg_v4(Op op, const uint8_t* __restrict__ nb8,
+__global__ void __launch_bounds__(CG_T, 6) k_cg_v4(Op op, const uint8_t* __restrict__ nb8,
                                                 const float* __restrict__ va, const float* __restrict__ vb,
                                                 float* __restrict__ pout, float* __restrict__ x, float* __restrict__ r,
                                                 Red Rd, int first, int it, int maxiter, int skip_dot) {

@@ -35,7 +35,7 @@ struct McGrid {
 // accumulators in the same visiting order, so both fields equal the separate
 // passes bit for bit.
 template <int SURF, bool GAS2 = false>
-__global__ void __launch_bounds__(256) k_mc_density(McGrid m, Cells cl, const float4* __restrict__ pos, float* __restrict__ dens,
+__global__ void __launch_bounds__(256, 6) k_mc_density(McGrid m, Cells cl, const float4* __restrict__ pos, float* __restrict__ dens,
                                                     int scene, float* __restrict__ dens2 = nullptr) {
     const Tiles T = m.T;
     const float hm = m.hm;

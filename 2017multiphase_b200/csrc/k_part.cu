@@ -290,7 +290,7 @@ __global__ void k_collide_freezing(Grid g, Cells cl, int np, const float4* __res
 }
 
 // correctparticlepos: reads pos, writes out (out of place)
-__global__ void k_correct_pos(Grid g, Cells cl, int np, const float4* __restrict__ pos, const float4* __restrict__ vel,
+__global__ void __launch_bounds__(256, 6) k_correct_pos(Grid g, Cells cl, int np, const float4* __restrict__ pos, const float4* __restrict__ vel,
                               float4* __restrict__ out, float re, float spring_k, float samplespace, float dt) {
     const float h = g.h;
     const float3 g0 = mk3(g.gx0, g.gy0, g.gz0);
