@@ -246,46 +246,80 @@ __device__ bool sweep_sel(const Grid& g, int ax, int i, int j, int k, const floa
     }
     return found;
 }
+// each face's extrapolation choice for one step, computed once and shared by
+// the forward passes and their transposes: bit 7 set when the pass overwrites
+// the face, bits 0-2 the chosen octant's signs (di, dj, dk > 0), and the three
+// normalised weights
+__global__ void k_ad_sweep_sel(Grid g, const float* __restrict__ ls, const int8_t* __restrict__ mark, int fl,
+                               uint8_t* __restrict__ sel, float* __restrict__ sw) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        int di, dj, dk; float wx = 0, wy = 0, wz = 0;
+        uint8_t code = 0;
+        if (sweep_sel(g, ax, i, j, k, ls, mark, fl, di, dj, dk, wx, wy, wz))
+            code = (uint8_t)(0x80 | (di > 0 ? 1 : 0) | (dj > 0 ? 2 : 0) | (dk > 0 ? 4 : 0));
+        sel[t] = code;
+        sw[3 * t] = wx; sw[3 * t + 1] = wy; sw[3 * t + 2] = wz;
+    }
+}
+__device__ __forceinline__ long long face_flat(const Grid& g, int ax, int i, int j, int k) {
+    return ax == 0 ? (long long)fxi(g, i, j, k)
+                   : (ax == 1 ? (long long)g.nfx + fyi(g, i, j, k) : (long long)g.nfx + g.nfy + fzi(g, i, j, k));
+}
+// one extrapolation pass (sweepu_k_bubble's arithmetic) from the stored choices
 template <class T>
-__global__ void k_ad_sweepu(Grid g, Fc<T> in, Fc<T> out, const float* __restrict__ ls, const int8_t* __restrict__ mark,
-                            int fl) {
+__global__ void k_ad_sweepu_s(Grid g, Fc<T> in, Fc<T> out, const uint8_t* __restrict__ sel, const float* __restrict__ sw) {
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
     MP_GRID_LOOP(t, tot) {
         int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
         const T* f = fsel(in, ax);
         T res = f[idx];
-        int di, dj, dk; float wx, wy, wz;
-        if (sweep_sel(g, ax, i, j, k, ls, mark, fl, di, dj, dk, wx, wy, wz))
-            res = (T)wx * f[face_index(g, ax, i + di, j, k)] + (T)wy * f[face_index(g, ax, i, j + dj, k)] +
-                  (T)wz * f[face_index(g, ax, i, j, k + dk)];
+        const uint8_t code = sel[t];
+        if (code & 0x80) {
+            const int di = code & 1 ? 1 : -1, dj = code & 2 ? 1 : -1, dk = code & 4 ? 1 : -1;
+            res = (T)sw[3 * t] * f[face_index(g, ax, i + di, j, k)] + (T)sw[3 * t + 1] * f[face_index(g, ax, i, j + dj, k)] +
+                  (T)sw[3 * t + 2] * f[face_index(g, ax, i, j, k + dk)];
+        }
         fsel(out, ax)[idx] = res;
     }
 }
-// transpose of one extrapolation pass: an input face keeps its own adjoint
-// unless the pass overwrote it, and receives from the (up to six) faces whose
-// chosen octant reads it
+// its transpose: an input face keeps its own adjoint unless the pass
+// overwrote it, and receives from the (up to six) faces whose chosen octant
+// reads it
 template <class T>
-__global__ void k_ad_sweepu_adj(Grid g, Fc<T> ob, Fc<T> ib, const float* __restrict__ ls,
-                                const int8_t* __restrict__ mark, int fl) {
+__global__ void k_ad_sweepu_adj_s(Grid g, Fc<T> ob, Fc<T> ib, const uint8_t* __restrict__ sel,
+                                  const float* __restrict__ sw) {
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
     MP_GRID_LOOP(t, tot) {
         int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
         const T* o = fsel(ob, ax);
-        int di, dj, dk; float wx, wy, wz;
-        T acc = sweep_sel(g, ax, i, j, k, ls, mark, fl, di, dj, dk, wx, wy, wz) ? (T)0 : o[idx];
+        T acc = (sel[t] & 0x80) ? (T)0 : o[idx];
         const int W = ax == 0 ? g.NX + 1 : g.NX, H = ax == 1 ? g.NY + 1 : g.NY, D = ax == 2 ? g.NZ + 1 : g.NZ;
-        // the reader f sits at g - d*e_dir and chose d along dir
         for (int dir = 0; dir < 3; dir++) for (int d = -1; d <= 1; d += 2) {
             int fi = i - (dir == 0 ? d : 0), fj = j - (dir == 1 ? d : 0), fk = k - (dir == 2 ? d : 0);
             if (fi < 0 || fi >= W || fj < 0 || fj >= H || fk < 0 || fk >= D) continue;
-            int ei, ej, ek; float ax_w, ay_w, az_w;
-            if (!sweep_sel(g, ax, fi, fj, fk, ls, mark, fl, ei, ej, ek, ax_w, ay_w, az_w)) continue;
-            int chosen = dir == 0 ? ei : (dir == 1 ? ej : ek);
+            const long long ft = face_flat(g, ax, fi, fj, fk);
+            const uint8_t code = sel[ft];
+            if (!(code & 0x80)) continue;
+            const int chosen = (code >> dir) & 1 ? 1 : -1;
             if (chosen != d) continue;
-            float wsel = dir == 0 ? ax_w : (dir == 1 ? ay_w : az_w);
-            acc += (T)wsel * o[face_index(g, ax, fi, fj, fk)];
+            acc += (T)sw[3 * ft + dir] * o[face_index(g, ax, fi, fj, fk)];
         }
         fsel(ib, ax)[idx] = acc;
+    }
+}
+// raises *flag when some particle's cell from its replay position differs from
+// its recorded cell (the G2P transpose then searches the wider window)
+template <class T>
+__global__ void k_ad_cell_mismatch(Grid g, int np, const T* __restrict__ x, const uint32_t* __restrict__ cellof,
+                                   uint32_t* flag) {
+    MP_GRID_LOOP(p, np) {
+        int a, b, c; getijk3((int)cellof[p], g.NY, g.NZ, a, b, c);
+        const T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
+        bool bad = !(X >= (T)0 && Y >= (T)0 && Z >= (T)0) || (int)X != a || (int)Y != b || (int)Z != c;
+        if (__any_sync(__activemask(), bad) && (threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1))
+            atomicOr(flag, 1u);
     }
 }
 // wall rules (setWaterBoundaryU_k), in place; `zceil` marks the top z faces
@@ -597,10 +631,11 @@ __global__ void k_ad_g2p_adj_p(Grid g, int np, const T* __restrict__ x, Fc<T> uf
 }
 // face side of the G2P transpose: q_f = sum of w_pf vgbar_p over the particles
 // whose interpolation stencil holds f. Those lie in cells [i-1,i] along the
-// face normal and [-1,1] across; the candidates are taken one cell wider,
-// since the recorded cell lists come from the recorded positions, and
-// membership is decided from the replay's own positions.
-template <class T>
+// face normal and [-1,1] across of their replay positions; the candidates come
+// from the recorded cell lists, so when some particle's replay cell differs
+// from its recorded one (WIDE) they are taken one cell wider. Membership is
+// decided from the replay's own positions either way.
+template <class T, bool WIDE>
 __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
                                const T* __restrict__ x, const T* __restrict__ vgb, Fc<T> q) {
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
@@ -608,8 +643,9 @@ __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ order, const
         int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
         const int w = ax == 0 ? g.NX + 1 : g.NX, hh = ax == 1 ? g.NY + 1 : g.NY, d = ax == 2 ? g.NZ + 1 : g.NZ;
         T acc = 0;
-        const int a0 = i - 2, a1 = ax == 0 ? i + 1 : i + 2, b0 = j - 2, b1 = ax == 1 ? j + 1 : j + 2;
-        const int c0 = k - 2, c1 = ax == 2 ? k + 1 : k + 2;
+        const int wd = WIDE ? 1 : 0;
+        const int a0 = i - 1 - wd, a1 = (ax == 0 ? i : i + 1) + wd, b0 = j - 1 - wd, b1 = (ax == 1 ? j : j + 1) + wd;
+        const int c0 = k - 1 - wd, c1 = (ax == 2 ? k : k + 1) + wd;
         for (int a = a0; a <= a1; a++) {
             if (a < 0 || a > g.NX - 1) continue;
             for (int b = b0; b <= b1; b++) {
@@ -831,13 +867,21 @@ int k_adj_set_targets(MpCtx* c, const float* sp, int ns) {
 }
 
 namespace {
-// work layout (element counts; each buffer allocated for `esz`-byte elements)
+// work layout: element counts per buffer; W_I* hold one step's intermediates
+// per slot (`every` slots: a segment's steps are replayed into them and then
+// reversed without recomputation)
 enum {
-    W_XS, W_VS, W_VA, W_VG, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
-    W_UP, W_WT, W_UOLD, W_T0, W_UE, W_UPROJ, W_UF, W_DU, W_B0, W_B1, W_B2,
-    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_COUNT
+    W_XS, W_VS, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
+    W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2,
+    W_IVA, W_IVG, W_IUP, W_IWT, W_IUE, W_IUF, W_IDU, W_ISEL, W_ISW,
+    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_COUNT
 };
 }
+
+// one step's intermediates (what its transpose reads)
+template <class T> struct Inter {
+    T* va; T* vg; Fc<T> up, wt, ue, uf, du; uint8_t* sel; float* sw;
+};
 
 template <class T> struct Replay {
     MpCtx* c; AdjTape* t; Grid g; long long nf; int np;
@@ -845,6 +889,17 @@ template <class T> struct Replay {
     Fc<T> f(int w) const { return faces_of<T>(t->wk[w], g); }
     T* seg_x(int s) const { return a(W_XS) + (size_t)s * 3 * np; }
     T* seg_v(int s) const { return a(W_VS) + (size_t)s * 3 * np; }
+    Inter<T> inter(int j) const {
+        const size_t np3 = 3 * (size_t)np, nfs = (size_t)nf;
+        Inter<T> I;
+        I.va = a(W_IVA) + j * np3; I.vg = a(W_IVG) + j * np3;
+        I.up = faces_of<T>(a(W_IUP) + j * nfs, g); I.wt = faces_of<T>(a(W_IWT) + j * nfs, g);
+        I.ue = faces_of<T>(a(W_IUE) + j * nfs, g); I.uf = faces_of<T>(a(W_IUF) + j * nfs, g);
+        I.du = faces_of<T>(a(W_IDU) + j * nfs, g);
+        I.sel = static_cast<uint8_t*>(t->wk[W_ISEL]) + j * nfs;
+        I.sw = static_cast<float*>(t->wk[W_ISW]) + 3 * j * nfs;
+        return I;
+    }
 };
 
 template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
@@ -854,17 +909,23 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     const Grid& g = c->G;
     const size_t np3 = 3 * (size_t)t->np, nf = (size_t)g.nfx + g.nfy + g.nfz, n = g.n;
     const int nseg = (t->nsteps + t->every - 1) / t->every;
-    size_t cnt[W_COUNT];
+    const size_t E = (size_t)t->every;
+    size_t cnt[W_COUNT], es[W_COUNT];
+    for (int w = 0; w < W_COUNT; w++) es[w] = sizeof(T);
     cnt[W_XS] = cnt[W_VS] = np3 * (size_t)(nseg + t->every);   // segment starts, then one segment's steps
-    for (int w : {W_VA, W_VG, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN}) cnt[w] = np3;
-    for (int w : {W_UP, W_WT, W_UOLD, W_T0, W_UE, W_UPROJ, W_UF, W_DU, W_B0, W_B1, W_B2}) cnt[w] = nf;
+    for (int w : {W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN}) cnt[w] = np3;
+    for (int w : {W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2}) cnt[w] = nf;
+    cnt[W_IVA] = cnt[W_IVG] = np3 * E;
+    for (int w : {W_IUP, W_IWT, W_IUE, W_IUF, W_IDU}) cnt[w] = nf * E;
+    cnt[W_ISEL] = nf * E; es[W_ISEL] = 1;
+    cnt[W_ISW] = 3 * nf * E; es[W_ISW] = sizeof(float);
     for (int w : {W_CB, W_CP, W_CQ, W_PHI}) cnt[w] = n;
-    cnt[W_SV] = (size_t)std::max(t->nsamples, 1) * 2;   // doubles
-    cnt[W_LOSS] = 2;
-    cnt[W_CELLOF] = (size_t)t->np;   // uint32
+    cnt[W_SV] = (size_t)std::max(t->nsamples, 1) * 2; es[W_SV] = sizeof(double);
+    cnt[W_LOSS] = 2; es[W_LOSS] = sizeof(double);
+    cnt[W_CELLOF] = (size_t)t->np; es[W_CELLOF] = sizeof(uint32_t);
+    cnt[W_FLAG] = 4; es[W_FLAG] = sizeof(uint32_t);
     for (int w = 0; w < W_COUNT; w++) {
-        size_t es = (w == W_SV || w == W_LOSS) ? sizeof(double) : (w == W_CELLOF ? sizeof(uint32_t) : sizeof(T));
-        size_t bytes = es * std::max<size_t>(cnt[w], 1);
+        size_t bytes = es[w] * std::max<size_t>(cnt[w], 1);
         cudaError_t e = cudaMalloc(&t->wk[w], bytes);
         if (e != cudaSuccess) { c->err = std::string("adjoint work: ") + cudaGetErrorString(e); return MP_ERR_CUDA; }
     }
@@ -879,53 +940,67 @@ template <class T> static int cg_tol_of(const MpCtx* c, int& mode, float& tol, i
     return MP_OK;
 }
 
-// one step of the replay from (x, v) to (xo, vo); leaves the step's grid
-// intermediates in the work buffers
-template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, const T* v, T* xo, T* vo) {
+// one step of the replay from (x, v) to (xo, vo), keeping what its transpose
+// needs in I
+template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, const T* v, T* xo, T* vo,
+                                       const Inter<T>& I) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
     cudaStream_t s = c->stream;
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
     const mp_params& P = c->P;
-    k_ad_gravity<T><<<nbp, 256, 0, s>>>(R.np, v, R.a(W_VA), (T)P.dt * (T)P.gravity_z);
-    k_ad_p2g<T><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], t->mass, x, R.a(W_VA), R.f(W_UP), R.f(W_WT));
-    k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, R.a(W_UP), R.a(W_UOLD));
-    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_UP), R.f(W_T0), t->phi[k], t->mark[k], MP_TYPEFLUID);
-    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B0), t->phi[k], t->mark[k], MP_TYPEFLUID);
-    k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), R.f(W_UE), t->mark[k]);
-    k_ad_div<T><<<nbc, 256, 0, s>>>(g, t->mark[k], R.f(W_UE), R.a(W_CB));
+    k_ad_sweep_sel<<<nbf, 256, 0, s>>>(g, t->phi[k], t->mark[k], MP_TYPEFLUID, I.sel, I.sw);
+    k_ad_gravity<T><<<nbp, 256, 0, s>>>(R.np, v, I.va, (T)P.dt * (T)P.gravity_z);
+    k_ad_p2g<T><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], t->mass, x, I.va, I.up, I.wt);
+    k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, I.up.x, R.a(W_UOLD));
+    k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, I.up, R.f(W_T0), I.sel, I.sw);
+    k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B0), I.sel, I.sw);
+    k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), I.ue, t->mark[k]);
+    k_ad_div<T><<<nbc, 256, 0, s>>>(g, t->mark[k], I.ue, R.a(W_CB));
     MP_CHECK_LAUNCH(c);
     int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
     int it = 0; double res = 0;
     int st = k_cg_solve(c, t->mark[k], R.a(W_CP), R.a(W_CB), maxit, mode, tol, &it, &res);
     if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
-    k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, R.a(W_CP), R.f(W_UE), R.f(W_UPROJ));
-    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_UPROJ), R.f(W_B1), t->phi[k], t->mark[k], MP_TYPEFLUID);
-    k_ad_sweepu<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), t->phi[k], t->mark[k], MP_TYPEFLUID);
-    k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_UF), t->mark[k]);
-    k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, R.a(W_UF), R.a(W_UOLD), R.a(W_DU));
-    k_ad_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VA), R.f(W_UF), R.f(W_DU), (T)P.flip_alpha, R.a(W_VG));
-    k_ad_advect<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VG), xo, vo, (T)P.dt);
+    k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, R.a(W_CP), I.ue, R.f(W_UPROJ));
+    k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_UPROJ), R.f(W_B1), I.sel, I.sw);
+    k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), I.sel, I.sw);
+    k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), I.uf, t->mark[k]);
+    k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, I.uf.x, R.a(W_UOLD), I.du.x);
+    k_ad_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.va, I.uf, I.du, (T)P.flip_alpha, I.vg);
+    k_ad_advect<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, xo, vo, (T)P.dt);
     MP_CHECK_LAUNCH(c);
     return MP_OK;
 }
 
-// reverse of fwd_step (run right after it, on its intermediates): (xb, vb)
-// hold the adjoint of the step's outputs on entry and of its inputs on exit
-template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, T* xb, T* vb) {
+// transpose of a step from its intermediates: (xb, vb) hold the adjoint of the
+// step's outputs on entry and of its inputs on exit
+template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, const Inter<T>& I, T* xb, T* vb) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
     cudaStream_t s = c->stream;
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
     const mp_params& P = c->P;
     const T alpha = (T)P.flip_alpha;
-    k_ad_advect_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VG), (T)P.dt, xb, vb, R.a(W_VGB));
-    k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.f(W_UF), R.f(W_DU), alpha, R.a(W_VGB), R.a(W_VAB), xb);
+    uint32_t* cellof = static_cast<uint32_t*>(t->wk[W_CELLOF]);
+    uint32_t* flag = static_cast<uint32_t*>(t->wk[W_FLAG]);
+    k_ad_cellof<<<nbc, 256, 0, s>>>(g.n, t->order[k], t->off[k], cellof);
+    MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
+    k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x, cellof, flag);
+    k_ad_advect_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, (T)P.dt, xb, vb, R.a(W_VGB));
+    k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.uf, I.du, alpha, R.a(W_VGB), R.a(W_VAB), xb);
+    MP_CHECK_LAUNCH(c);
+    uint32_t wide = 1;
+    MP_CUDA(c, cudaMemcpyAsync(&wide, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(c, cudaStreamSynchronize(s));
     // q = I^T vgbar on B0; ufbar = q, uoldbar = -cdu q
-    k_ad_g2p_adj_f<T><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], x, R.a(W_VGB), R.f(W_B0));
+    if (wide) k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], x, R.a(W_VGB), R.f(W_B0));
+    else k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], x, R.a(W_VGB), R.f(W_B0));
     const T cdu = alpha == (T)1 ? (T)1 : alpha;
-    // wall rules then the two passes, transposed (B0 -> B1 -> B2 -> B1)
-    k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), R.f(W_B1), R.f(W_B2), t->mark[k]);
-    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_T0), t->phi[k], t->mark[k], MP_TYPEFLUID);
-    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B1), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    // wall rules then the two passes, transposed (B0 -> B1 -> T0 -> B1); the
+    // ceiling rule's decision reads the rule's output, equal to its input
+    // wherever the decision matters
+    k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), R.f(W_B1), I.uf, t->mark[k]);
+    k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_T0), I.sel, I.sw);
+    k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B1), I.sel, I.sw);
     // projection: ubar_e = ubar_proj + D^T L^-1 (-G^T ubar_proj)
     k_ad_pbar<T><<<nbc, 256, 0, s>>>(g, t->mark[k], R.f(W_B1), R.a(W_CB));
     MP_CHECK_LAUNCH(c);
@@ -934,17 +1009,13 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, T*
     int st = k_cg_solve(c, t->mark[k], R.a(W_CQ), R.a(W_CB), maxit, mode, tol, &it, &res);
     if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
     k_ad_divT<T><<<nbf, 256, 0, s>>>(g, R.a(W_CQ), R.f(W_B1), R.f(W_B2));
-    // wall rules and passes before the projection (input of the rule: B0 of the forward = W_T0's successor)
-    k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), R.f(W_UE), t->mark[k]);
-    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), t->phi[k], t->mark[k], MP_TYPEFLUID);
-    k_ad_sweepu_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), t->phi[k], t->mark[k], MP_TYPEFLUID);
+    k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), I.ue, t->mark[k]);
+    k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), I.sel, I.sw);
+    k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), I.sel, I.sw);
     // upbar = that + uoldbar
     k_ad_axpy<T><<<nbf, 256, 0, s>>>(R.nf, -cdu, R.a(W_B0), R.a(W_B1));
     // splat transpose (vabar += ..., xbar += ...)
-    uint32_t* cellof = static_cast<uint32_t*>(t->wk[W_CELLOF]);
-    k_ad_cellof<<<nbc, 256, 0, s>>>(g.n, t->order[k], t->off[k], cellof);
-    k_ad_p2g_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, R.a(W_VA), t->mass, cellof, R.f(W_UP), R.f(W_WT), R.f(W_B1),
-                                        R.a(W_VAB), xb);
+    k_ad_p2g_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.va, t->mass, cellof, I.up, I.wt, R.f(W_B1), R.a(W_VAB), xb);
     // gravity: vbar = vabar
     k_ad_copy<T><<<nbp, 256, 0, s>>>(3LL * R.np, R.a(W_VAB), vb);
     MP_CHECK_LAUNCH(c);
@@ -972,7 +1043,8 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
     cudaStream_t s = c->stream;
     const long long np3 = 3LL * t->np;
     const int nb3 = mp_blocks(np3, 256);
-    // forward over all steps, keeping the segment starts
+    // forward over all steps, keeping the segment starts (slot 0 holds each
+    // step's intermediates in passing)
     T* x = R.a(W_X); T* v = R.a(W_V); T* xn = R.a(W_XN); T* vn = R.a(W_VN);
     k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->x0, x);
     if (v0) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, v0, v);
@@ -980,8 +1052,7 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
     MP_CHECK_LAUNCH(c);
     const int E = t->every, nseg = (t->nsteps + E - 1) / E;
     std::vector<T*> ckx(nseg), ckv(nseg);
-    // segment starts live in a second set of slots after the per-step states
-    // when the work is large enough; otherwise the replay recomputes from 0
+    const Inter<T> scratch = R.inter(0);
     for (int k = 0; k < t->nsteps; k++) {
         if (k % E == 0) {
             int sgi = k / E;
@@ -989,7 +1060,7 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
             MP_CUDA(c, cudaMemcpyAsync(ckx[sgi], x, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
             MP_CUDA(c, cudaMemcpyAsync(ckv[sgi], v, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
         }
-        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn));
+        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, scratch));
         std::swap(x, xn); std::swap(v, vn);
     }
     double L = 0;
@@ -1003,20 +1074,19 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
     k_ad_phi_x<T><<<mp_blocks(t->np, 256), 256, 0, s>>>(c->G, t->np, x, t->nearest, R.a(W_CQ), xb);
     MP_CUDA(c, cudaMemsetAsync(vb, 0, sizeof(T) * np3, s));
     MP_CHECK_LAUNCH(c);
-    // reverse sweep, segment by segment: the segment's states are recomputed
-    // from its start into the per-step slots, then the steps are reversed,
-    // each after recomputing its own grid intermediates
+    // reverse sweep, segment by segment: the segment is replayed from its
+    // start, each step's state and intermediates kept in its slot, then the
+    // steps are reversed
     for (int sg = nseg - 1; sg >= 0; sg--) {
         const int k0 = sg * E, len = std::min(t->nsteps, k0 + E) - k0;
         MP_CUDA(c, cudaMemcpyAsync(R.seg_x(nseg), ckx[sg], sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
         MP_CUDA(c, cudaMemcpyAsync(R.seg_v(nseg), ckv[sg], sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
-        for (int j = 0; j + 1 < len; j++)
-            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), R.seg_x(nseg + j + 1),
-                               R.seg_v(nseg + j + 1)));
-        for (int j = len - 1; j >= 0; j--) {
-            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), R.a(W_XN), R.a(W_VN)));
-            MP_TRY(adj_step<T>(R, k0 + j, R.seg_x(nseg + j), xb, vb));
+        for (int j = 0; j < len; j++) {
+            T* xo = j + 1 < len ? R.seg_x(nseg + j + 1) : R.a(W_XN);
+            T* vo = j + 1 < len ? R.seg_v(nseg + j + 1) : R.a(W_VN);
+            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), xo, vo, R.inter(j)));
         }
+        for (int j = len - 1; j >= 0; j--) MP_TRY(adj_step<T>(R, k0 + j, R.seg_x(nseg + j), R.inter(j), xb, vb));
     }
     k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, vb, grad);
     MP_CHECK_LAUNCH(c);
