@@ -155,8 +155,7 @@ __device__ __forceinline__ void face_pos(int ax, int i, int j, int k, float& gx,
 // the cells [i-1,i] along the face normal and [-1,1] across (the order of
 // mapvelp2g_k_fluidSolid's loops)
 template <class T>
-__global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
-                         const float* __restrict__ mass, const T* __restrict__ x, const T* __restrict__ va,
+__global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4, const T* __restrict__ vs4,
                          Fc<T> u, Fc<T> W) {
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
     const T scale = (T)1 / (T)g.h;
@@ -175,17 +174,31 @@ __global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ order, const uint3
                     if (cc < 0 || cc > g.NZ - 1) continue;
                     int c = cid(g, a, b, cc);
                     for (uint32_t q = off[c]; q < off[c + 1]; q++) {
-                        uint32_t p = order[q];
-                        T dx = x[3 * p] * scale - (T)fx, dy = x[3 * p + 1] * scale - (T)fy, dz = x[3 * p + 2] * scale - (T)fz;
+                        const T* r = xs4 + 4 * (size_t)q;
+                        T dx = r[0] * scale - (T)fx, dy = r[1] * scale - (T)fy, dz = r[2] * scale - (T)fz;
                         T r2 = dx * dx + dy * dy + dz * dz;
-                        T wp = (T)mass[p] * sharpk(r2);
-                        w += wp; s += wp * va[3 * p + ax];
+                        T wp = r[3] * sharpk(r2);
+                        w += wp; s += wp * vs4[4 * (size_t)q + ax];
                     }
                 }
             }
         }
         fsel(W, ax)[idx] = w;
         fsel(u, ax)[idx] = w > (T)0 ? s / w : (T)0;
+    }
+}
+// particle records in a step's recorded sorted order: (a xyz, mass or 0) and
+// (b xyz, 0), so the face gathers read contiguous records within a cell
+template <class T>
+__global__ void k_ad_slot_gather(int np, const uint32_t* __restrict__ order, const T* __restrict__ a,
+                                 const T* __restrict__ b, const float* __restrict__ mass, T* __restrict__ oa,
+                                 T* __restrict__ ob) {
+    MP_GRID_LOOP(s, np) {
+        const uint32_t p = order[s];
+        oa[4 * (size_t)s] = a[3 * p]; oa[4 * (size_t)s + 1] = a[3 * p + 1]; oa[4 * (size_t)s + 2] = a[3 * p + 2];
+        oa[4 * (size_t)s + 3] = mass ? (T)mass[p] : (T)0;
+        ob[4 * (size_t)s] = b[3 * p]; ob[4 * (size_t)s + 1] = b[3 * p + 1]; ob[4 * (size_t)s + 2] = b[3 * p + 2];
+        ob[4 * (size_t)s + 3] = (T)0;
     }
 }
 template <class T> __global__ void k_ad_copy(long long n, const T* __restrict__ a, T* __restrict__ b) {
@@ -609,9 +622,11 @@ __global__ void k_ad_advect_adj(Grid g, int np, const T* __restrict__ x, const T
 // gather part of the particle side of the G2P transpose: vabar and the
 // position derivative of the interpolation
 template <class T>
-__global__ void k_ad_g2p_adj_p(Grid g, int np, const T* __restrict__ x, Fc<T> uf, Fc<T> du, T alpha,
-                               const T* __restrict__ vgb, T* __restrict__ vab, T* __restrict__ xb) {
-    MP_GRID_LOOP(p, np) {
+__global__ void k_ad_g2p_adj_p(Grid g, int np, const uint32_t* __restrict__ order, const T* __restrict__ x, Fc<T> uf,
+                               Fc<T> du, T alpha, const T* __restrict__ vgb, T* __restrict__ vab, T* __restrict__ xb) {
+    // particles in sorted order, so neighbouring threads read neighbouring faces
+    MP_GRID_LOOP(sl, np) {
+        const uint32_t p = order[sl];
         const T ih = (T)1 / (T)g.h;
         T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
         const T cdu = alpha == (T)1 ? (T)1 : alpha, cu = alpha == (T)1 ? (T)0 : (T)1 - alpha;
@@ -636,8 +651,8 @@ __global__ void k_ad_g2p_adj_p(Grid g, int np, const T* __restrict__ x, Fc<T> uf
 // from its recorded one (WIDE) they are taken one cell wider. Membership is
 // decided from the replay's own positions either way.
 template <class T, bool WIDE>
-__global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
-                               const T* __restrict__ x, const T* __restrict__ vgb, Fc<T> q) {
+__global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4,
+                               const T* __restrict__ vgs4, Fc<T> q) {
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
     MP_GRID_LOOP(t, tot) {
         int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
@@ -654,8 +669,8 @@ __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ order, const
                     if (cc < 0 || cc > g.NZ - 1) continue;
                     int c = cid(g, a, b, cc);
                     for (uint32_t s = off[c]; s < off[c + 1]; s++) {
-                        uint32_t p = order[s];
-                        T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
+                        const T* r = xs4 + 4 * (size_t)s;
+                        T X = r[0] / (T)g.h, Y = r[1] / (T)g.h, Z = r[2] / (T)g.h;
                         T px, py, pz; ipos(ax, X, Y, Z, px, py, pz);
                         px = px < (T)0 ? (T)0 : (px > (T)w ? (T)w : px);
                         py = py < (T)0 ? (T)0 : (py > (T)hh ? (T)hh : py);
@@ -667,7 +682,7 @@ __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ order, const
                         if (ei < 0 || ei > 1 || ej < 0 || ej > 1 || ek < 0 || ek > 1) continue;
                         T fx = ei ? px - (T)bi : (T)(bi + 1) - px, fy = ej ? py - (T)bj : (T)(bj + 1) - py;
                         T fz = ek ? pz - (T)bk : (T)(bk + 1) - pz;
-                        acc += fx * fy * fz * vgb[3 * p + ax];
+                        acc += fx * fy * fz * vgs4[4 * (size_t)s + ax];
                     }
                 }
             }
@@ -678,11 +693,14 @@ __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ order, const
 // splat transpose per particle over the faces whose window holds its cell
 // (the particle's cell is the recorded one: window membership is frozen)
 template <class T>
-__global__ void k_ad_p2g_adj(Grid g, int np, const T* __restrict__ x, const T* __restrict__ va,
-                             const float* __restrict__ mass, const uint32_t* __restrict__ cellof, Fc<T> u, Fc<T> W,
-                             Fc<T> ub, T* __restrict__ vab, T* __restrict__ xb) {
+__global__ void k_ad_p2g_adj(Grid g, int np, const uint32_t* __restrict__ order, const T* __restrict__ x,
+                             const T* __restrict__ va, const float* __restrict__ mass,
+                             const uint32_t* __restrict__ cellof, Fc<T> u, Fc<T> W, Fc<T> ub, T* __restrict__ vab,
+                             T* __restrict__ xb) {
     const T scale = (T)1 / (T)g.h;
-    MP_GRID_LOOP(p, np) {
+    // particles in sorted order, so neighbouring threads read neighbouring faces
+    MP_GRID_LOOP(sl, np) {
+        const uint32_t p = order[sl];
         T X = x[3 * p] * scale, Y = x[3 * p + 1] * scale, Z = x[3 * p + 2] * scale;
         int ca, cb, cc;
         getijk3((int)cellof[p], g.NY, g.NZ, ca, cb, cc);
@@ -874,7 +892,7 @@ enum {
     W_XS, W_VS, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
     W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2,
     W_IVA, W_IVG, W_IUP, W_IWT, W_IUE, W_IUF, W_IDU, W_ISEL, W_ISW,
-    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_COUNT
+    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_S4A, W_S4B, W_COUNT
 };
 }
 
@@ -924,6 +942,7 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     cnt[W_LOSS] = 2; es[W_LOSS] = sizeof(double);
     cnt[W_CELLOF] = (size_t)t->np; es[W_CELLOF] = sizeof(uint32_t);
     cnt[W_FLAG] = 4; es[W_FLAG] = sizeof(uint32_t);
+    cnt[W_S4A] = cnt[W_S4B] = 4 * (size_t)t->np;
     for (int w = 0; w < W_COUNT; w++) {
         size_t bytes = es[w] * std::max<size_t>(cnt[w], 1);
         cudaError_t e = cudaMalloc(&t->wk[w], bytes);
@@ -950,7 +969,8 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     const mp_params& P = c->P;
     k_ad_sweep_sel<<<nbf, 256, 0, s>>>(g, t->phi[k], t->mark[k], MP_TYPEFLUID, I.sel, I.sw);
     k_ad_gravity<T><<<nbp, 256, 0, s>>>(R.np, v, I.va, (T)P.dt * (T)P.gravity_z);
-    k_ad_p2g<T><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], t->mass, x, I.va, I.up, I.wt);
+    k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, t->mass, R.a(W_S4A), R.a(W_S4B));
+    k_ad_p2g<T><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), I.up, I.wt);
     k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, I.up.x, R.a(W_UOLD));
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, I.up, R.f(W_T0), I.sel, I.sw);
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B0), I.sel, I.sw);
@@ -986,14 +1006,15 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
     MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
     k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x, cellof, flag);
     k_ad_advect_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, (T)P.dt, xb, vb, R.a(W_VGB));
-    k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.uf, I.du, alpha, R.a(W_VGB), R.a(W_VAB), xb);
+    k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.uf, I.du, alpha, R.a(W_VGB), R.a(W_VAB), xb);
+    k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, R.a(W_VGB), nullptr, R.a(W_S4A), R.a(W_S4B));
     MP_CHECK_LAUNCH(c);
     uint32_t wide = 1;
     MP_CUDA(c, cudaMemcpyAsync(&wide, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     MP_CUDA(c, cudaStreamSynchronize(s));
     // q = I^T vgbar on B0; ufbar = q, uoldbar = -cdu q
-    if (wide) k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], x, R.a(W_VGB), R.f(W_B0));
-    else k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->order[k], t->off[k], x, R.a(W_VGB), R.f(W_B0));
+    if (wide) k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0));
+    else k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0));
     const T cdu = alpha == (T)1 ? (T)1 : alpha;
     // wall rules then the two passes, transposed (B0 -> B1 -> T0 -> B1); the
     // ceiling rule's decision reads the rule's output, equal to its input
@@ -1015,7 +1036,8 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
     // upbar = that + uoldbar
     k_ad_axpy<T><<<nbf, 256, 0, s>>>(R.nf, -cdu, R.a(W_B0), R.a(W_B1));
     // splat transpose (vabar += ..., xbar += ...)
-    k_ad_p2g_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.va, t->mass, cellof, I.up, I.wt, R.f(W_B1), R.a(W_VAB), xb);
+    k_ad_p2g_adj<T><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.va, t->mass, cellof, I.up, I.wt, R.f(W_B1),
+                                        R.a(W_VAB), xb);
     // gravity: vbar = vabar
     k_ad_copy<T><<<nbp, 256, 0, s>>>(3LL * R.np, R.a(W_VAB), vb);
     MP_CHECK_LAUNCH(c);
