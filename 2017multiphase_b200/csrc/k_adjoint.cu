@@ -892,7 +892,7 @@ enum {
     W_XS, W_VS, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
     W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2,
     W_IVA, W_IVG, W_IUP, W_IWT, W_IUE, W_IUF, W_IDU, W_ISEL, W_ISW,
-    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_S4A, W_S4B, W_COUNT
+    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_S4A, W_S4B, W_PST, W_COUNT
 };
 }
 
@@ -943,6 +943,7 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     cnt[W_CELLOF] = (size_t)t->np; es[W_CELLOF] = sizeof(uint32_t);
     cnt[W_FLAG] = 4; es[W_FLAG] = sizeof(uint32_t);
     cnt[W_S4A] = cnt[W_S4B] = 4 * (size_t)t->np;
+    cnt[W_PST] = n * (size_t)t->nsteps;   // each step's pressure from the first replay
     for (int w = 0; w < W_COUNT; w++) {
         size_t bytes = es[w] * std::max<size_t>(cnt[w], 1);
         cudaError_t e = cudaMalloc(&t->wk[w], bytes);
@@ -961,8 +962,10 @@ template <class T> static int cg_tol_of(const MpCtx* c, int& mode, float& tol, i
 
 // one step of the replay from (x, v) to (xo, vo), keeping what its transpose
 // needs in I
+// The pressure solve's result is stored in pst (first replay) or copied from
+// it (segment replays): the inputs are the same bit for bit, so is the result.
 template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, const T* v, T* xo, T* vo,
-                                       const Inter<T>& I) {
+                                       const Inter<T>& I, bool solve) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
     cudaStream_t s = c->stream;
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
@@ -977,11 +980,14 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), I.ue, t->mark[k]);
     k_ad_div<T><<<nbc, 256, 0, s>>>(g, t->mark[k], I.ue, R.a(W_CB));
     MP_CHECK_LAUNCH(c);
-    int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
-    int it = 0; double res = 0;
-    int st = k_cg_solve(c, t->mark[k], R.a(W_CP), R.a(W_CB), maxit, mode, tol, &it, &res);
-    if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
-    k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, R.a(W_CP), I.ue, R.f(W_UPROJ));
+    T* pk = R.a(W_PST) + (size_t)k * g.n;
+    if (solve) {
+        int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
+        int it = 0; double res = 0;
+        int st = k_cg_solve(c, t->mark[k], pk, R.a(W_CB), maxit, mode, tol, &it, &res);
+        if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+    }
+    k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, pk, I.ue, R.f(W_UPROJ));
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_UPROJ), R.f(W_B1), I.sel, I.sw);
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), I.sel, I.sw);
     k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), I.uf, t->mark[k]);
@@ -1082,7 +1088,7 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
             MP_CUDA(c, cudaMemcpyAsync(ckx[sgi], x, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
             MP_CUDA(c, cudaMemcpyAsync(ckv[sgi], v, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
         }
-        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, scratch));
+        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, scratch, true));
         std::swap(x, xn); std::swap(v, vn);
     }
     double L = 0;
@@ -1106,7 +1112,7 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
         for (int j = 0; j < len; j++) {
             T* xo = j + 1 < len ? R.seg_x(nseg + j + 1) : R.a(W_XN);
             T* vo = j + 1 < len ? R.seg_v(nseg + j + 1) : R.a(W_VN);
-            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), xo, vo, R.inter(j)));
+            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), xo, vo, R.inter(j), false));
         }
         for (int j = len - 1; j >= 0; j--) MP_TRY(adj_step<T>(R, k0 + j, R.seg_x(nseg + j), R.inter(j), xb, vb));
     }
