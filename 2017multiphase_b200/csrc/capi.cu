@@ -134,7 +134,7 @@ static void free_all(MpCtx* c) {
                     c->cell_tmp, c->mark, c->mark_tmp, c->cg_r, c->cg_p, c->cg_z, c->cg64, c->red, c->scal, c->red_count,
                     c->pos, c->vel, c->heat, c->pos2, c->vel2, c->heat2, c->pdens, c->pprs, c->pscr, c->pscr2,
                     c->flag_snap, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->scan_tmp, c->u32_scratch,
-                    c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_dens2, c->mc_cube, c->mc_vflag, c->mc_vscan,
+                    c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_dens2, c->gfm_beta, c->gfm_s, c->mc_cube, c->mc_vflag, c->mc_vscan,
                     c->mc_compact, c->mc_vverts, c->mc_vvscan, c->mc_emark, c->mc_escan, c->mc_vstart, c->mc_inc,
                     c->mc_fill, c->mc_tmpv};
     k_adj_free(c);
@@ -257,7 +257,11 @@ static int check_params(const mp_params* p, std::string& err) {
     if (p->scene < 0 || p->scene > MP_SCENE_ALL) { err = "bad scene"; return MP_ERR_ARG; }
     if (p->precision != MP_PREC_MIXED && p->precision != MP_PREC_FP64) { err = "bad precision"; return MP_ERR_ARG; }
     if (p->cg_tol_mode != MP_TOL_REF_ABS && p->cg_tol_mode != MP_TOL_REL) { err = "bad cg_tol_mode"; return MP_ERR_ARG; }
-    if (p->coef_mode != MP_COEF_REF) { err = "only MP_COEF_REF is implemented"; return MP_ERR_ARG; }
+    if (p->coef_mode != MP_COEF_REF && p->coef_mode != MP_COEF_GFM) { err = "unknown coef_mode"; return MP_ERR_ARG; }
+    if (p->coef_mode == MP_COEF_GFM && p->precision != MP_PREC_MIXED) {
+        err = "MP_COEF_GFM runs with MP_PREC_MIXED vectors"; return MP_ERR_ARG;
+    }
+    if (p->coef_mode == MP_COEF_GFM && !(p->density_ratio > 0)) { err = "density_ratio must be positive"; return MP_ERR_ARG; }
     if (p->mc_max_verts < 1 || p->mc_max_tris < 1) { err = "marching-cubes caps must be positive"; return MP_ERR_ARG; }
     return MP_OK;
 }

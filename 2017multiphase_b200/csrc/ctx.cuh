@@ -47,6 +47,8 @@ struct MpCtx {
     double *scal = 0;            // device scalars (see k_cg.cu)
     unsigned int *red_count = 0; // last-block counters
     int red_blocks = 0;
+    float *gfm_beta = 0;         // ghost-fluid face weights (x, y, z faces), allocated on first use
+    float *gfm_s = 0;            // its Jacobi scaling per cell
     // particles
     float4 *pos = 0, *vel = 0, *heat = 0;
     float4 *pos2 = 0, *vel2 = 0, *heat2 = 0;

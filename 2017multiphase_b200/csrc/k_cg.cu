@@ -159,6 +159,48 @@ struct HeatOp {
     template <class R> __device__ __forceinline__ R finish(R s) const { return s; }
 };
 
+// Ghost-fluid variable-density operator (the density-ratio extension; the
+// reference's projection is constant-coefficient). Face weights beta = 1/rho
+// of the face (kernel k_gfm_beta); rows over FLUID and AIR interior cells:
+//   (A p)_c = sum over neighbours that are not walls of beta_f (p_nb - p_c) / h^2
+// with p = 0 off the unknowns (beta = 1 everywhere gives computeAx_bubble).
+// It is applied Jacobi-scaled, S A S with S = diag^-1/2 (zero off the
+// unknowns), so plain CG on it is Jacobi-preconditioned CG on A.
+struct GfmOp {
+    Grid g;
+    const int8_t* __restrict__ mark;
+    const float* __restrict__ bx;
+    const float* __restrict__ by;
+    const float* __restrict__ bz;
+    const float* __restrict__ S;
+    __device__ __forceinline__ bool mask(int idx, int i, int j, int k) const {
+        int m = mark[idx];
+        return (m == MP_TYPEFLUID || m == MP_TYPEAIR) && inner(g, i, j, k);
+    }
+    __device__ __forceinline__ bool fixed(int q) const { return mark[q] == MP_TYPEBOUNDARY; }
+    template <class R, class F>
+    __device__ __forceinline__ R apply(int idx, F val) const {
+        const int sI = g.NY * g.NZ, sJ = g.NZ;
+        int i, j, k; getijk(g, idx, i, j, k);
+        const R sc = (R)S[idx], c = val(idx);
+        R s = 0;
+        auto term = [&](int q, float beta) {
+            if (mark[q] != MP_TYPEBOUNDARY) s += (R)beta * ((R)S[q] * val(q) - sc * c);
+        };
+        term(idx + sI, bx[fxi(g, i + 1, j, k)]);
+        term(idx + sJ, by[fyi(g, i, j + 1, k)]);
+        term(idx + 1, bz[fzi(g, i, j, k + 1)]);
+        term(idx - sI, bx[fxi(g, i, j, k)]);
+        term(idx - sJ, by[fyi(g, i, j, k)]);
+        term(idx - 1, bz[fzi(g, i, j, k)]);
+        return sc * s / ((R)g.h * (R)g.h);
+    }
+};
+// operators whose rows are not the unit 7-point stencil take the general
+// (one cell per thread) CG passes
+template <class Op> struct op_general : std::false_type {};
+template <> struct op_general<GfmOp> : std::true_type {};
+
 #define CG_CELL_LOOP(idx, n, i, j, k)                                                  \
     MP_GRID_LOOP(idx, n)                                                               \
         for (int row_ = idx / op.g.NZ, k = idx - row_ * op.g.NZ,                        \
@@ -596,6 +638,100 @@ __global__ void k_subgrad(Grid g, const R* __restrict__ p, float* wx, float* wy,
     }
 }
 
+// ---- ghost-fluid coefficients ---------------------------------------------------
+// Face weights beta = 1/rho_face, densities rho_liquid = 1 and rho_air =
+// 1/ratio. A face between two unknowns of one type takes that type's density;
+// between a FLUID and an AIR cell, rho_face = theta rho_liquid + (1 - theta)
+// rho_air with theta the liquid fraction of the segment between the centres
+// (theta = -ls_L / (ls_G - ls_L) from the merged level set, the fraction the
+// two-phase divergence uses, clamped to [0, 1]); a face with one unknown side
+// takes that side's density; others 0.
+__device__ __forceinline__ bool gfm_unknown(int m) { return m == MP_TYPEFLUID || m == MP_TYPEAIR; }
+__global__ void k_gfm_beta(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ ls, float rho_air,
+                           float* __restrict__ bx, float* __restrict__ by, float* __restrict__ bz) {
+    long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx, ax;
+        if (t < g.nfx) { idx = (int)t; getijk3(idx, g.NY, g.NZ, i, j, k); ax = 0; }
+        else if (t < (long long)g.nfx + g.nfy) { idx = (int)(t - g.nfx); getijk3(idx, g.NY + 1, g.NZ, i, j, k); ax = 1; }
+        else { idx = (int)(t - g.nfx - g.nfy); getijk3(idx, g.NY, g.NZ + 1, i, j, k); ax = 2; }
+        const int e = ax == 0 ? i : (ax == 1 ? j : k), n = ax == 0 ? g.NX : (ax == 1 ? g.NY : g.NZ);
+        float beta = 0.0f;
+        if (e > 0 && e < n) {
+            const int cb = cid(g, i, j, k), ca = cid(g, i - (ax == 0), j - (ax == 1), k - (ax == 2));
+            const int ma = mark[ca], mb = mark[cb];
+            const bool ua = gfm_unknown(ma), ub = gfm_unknown(mb);
+            auto rho = [&](int m) { return m == MP_TYPEAIR ? rho_air : 1.0f; };
+            if (ua && ub) {
+                if (ma == mb) beta = 1.0f / rho(ma);
+                else {
+                    const int cl = ma == MP_TYPEFLUID ? ca : cb, cg = ma == MP_TYPEFLUID ? cb : ca;
+                    const float ll = ls[cl], lg = ls[cg];
+                    float th = (lg == ll) ? 0.5f : (0.0f - ll) / (lg - ll);
+                    th = fminf(1.0f, fmaxf(0.0f, th));
+                    beta = 1.0f / (th * 1.0f + (1.0f - th) * rho_air);
+                }
+            } else if (ua) beta = 1.0f / rho(ma);
+            else if (ub) beta = 1.0f / rho(mb);
+        }
+        (ax == 0 ? bx : (ax == 1 ? by : bz))[idx] = beta;
+    }
+}
+// S = diag^-1/2 on the unknowns (0 elsewhere) and bs = S b
+__global__ void k_gfm_scale(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ bx,
+                            const float* __restrict__ by, const float* __restrict__ bz, const float* __restrict__ b,
+                            float* __restrict__ S, float* __restrict__ bs) {
+    const int sI = g.NY * g.NZ, sJ = g.NZ;
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk(g, idx, i, j, k);
+        float sc = 0.0f;
+        if (gfm_unknown(mark[idx]) && inner(g, i, j, k)) {
+            float d = 0.0f;
+            if (mark[idx + sI] != MP_TYPEBOUNDARY) d += bx[fxi(g, i + 1, j, k)];
+            if (mark[idx + sJ] != MP_TYPEBOUNDARY) d += by[fyi(g, i, j + 1, k)];
+            if (mark[idx + 1] != MP_TYPEBOUNDARY) d += bz[fzi(g, i, j, k + 1)];
+            if (mark[idx - sI] != MP_TYPEBOUNDARY) d += bx[fxi(g, i, j, k)];
+            if (mark[idx - sJ] != MP_TYPEBOUNDARY) d += by[fyi(g, i, j, k)];
+            if (mark[idx - 1] != MP_TYPEBOUNDARY) d += bz[fzi(g, i, j, k)];
+            d /= g.h * g.h;
+            sc = d > 0.0f ? 1.0f / sqrtf(d) : 0.0f;
+        }
+        S[idx] = sc;
+        bs[idx] = sc * b[idx];
+    }
+}
+__global__ void k_gfm_unscale(int n, const float* __restrict__ S, float* __restrict__ x) {
+    MP_GRID_LOOP(idx, n) x[idx] = S[idx] * x[idx];
+}
+// u -= beta grad p on the interior faces of both velocity fields
+__global__ void k_subgrad_gfm(Grid g, const float* __restrict__ p, const float* __restrict__ bx,
+                              const float* __restrict__ by, const float* __restrict__ bz, float* wx, float* wy,
+                              float* wz, float* ax, float* ay, float* az) {
+    long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k;
+        if (t < g.nfx) {
+            int idx = (int)t; getijk3(idx, g.NY, g.NZ, i, j, k);
+            if (i > 0 && i < g.NX) {
+                float d = bx[idx] * (p[cid(g, i, j, k)] - p[cid(g, i - 1, j, k)]) / g.h;
+                wx[idx] -= d; ax[idx] -= d;
+            }
+        } else if (t < (long long)g.nfx + g.nfy) {
+            int idx = (int)(t - g.nfx); getijk3(idx, g.NY + 1, g.NZ, i, j, k);
+            if (j > 0 && j < g.NY) {
+                float d = by[idx] * (p[cid(g, i, j, k)] - p[cid(g, i, j - 1, k)]) / g.h;
+                wy[idx] -= d; ay[idx] -= d;
+            }
+        } else {
+            int idx = (int)(t - g.nfx - g.nfy); getijk3(idx, g.NY, g.NZ + 1, i, j, k);
+            if (k > 0 && k < g.NZ) {
+                float d = bz[idx] * (p[cid(g, i, j, k)] - p[cid(g, i, j, k - 1)]) / g.h;
+                wz[idx] -= d; az[idx] -= d;
+            }
+        }
+    }
+}
+
 // ---- heat grid ----------------------------------------------------------------
 __global__ void k_heat_bottom(Grid g, float* __restrict__ Tp, float inc, float clampv) {
     MP_GRID_LOOP(idx, g.n) {
@@ -656,10 +792,13 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     k_cg_init<R, Op><<<nb, CG_T, 0, s>>>(op, n, b, r, Rd, tolmode, tol);
     c->launches++;
     MP_CHECK_LAUNCH(c);
+    constexpr bool kGeneral = op_general<Op>::value;
     // neighbour bytes for the plane-marching kernels (mark_tmp is free scratch here)
     uint8_t* nb8 = reinterpret_cast<uint8_t*>(c->mark_tmp);
-    k_nb8<Op><<<mp_blocks(n, 256), 256, 0, s>>>(op, n, nb8);
-    c->launches++;
+    if constexpr (!kGeneral) {
+        k_nb8<Op><<<mp_blocks(n, 256), 256, 0, s>>>(op, n, nb8);
+        c->launches++;
+    }
     const Grid& gg = c->G;
     dim3 pmb(PM_X, PM_Y);
     int tiles = ((gg.NZ + PM_X - 1) / PM_X) * ((gg.NY + PM_Y - 1) / PM_Y);
@@ -686,6 +825,16 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
         int end = std::min(maxiter, it + batch);
         for (; it < end; it++) {
             bool tr = true_every > 0 && (it + 1) % true_every == 0;
+            if constexpr (kGeneral) {
+                {
+                    KtScope kt(c, kt_stencil);
+                    k_cg_dir<R, Op><<<nb, CG_T, 0, s>>>(op, n, r, pa, pb, Rd, it == 0 ? 1 : 0);
+                }
+                {
+                    KtScope kt(c, MP_KT_CG_UPDATE);
+                    k_cg_upd<R, Op><<<nb, CG_T, 0, s>>>(op, n, pb, x, r, Rd, it, maxiter, tr ? 1 : 0);
+                }
+            } else {
             if constexpr (kF32) {
                 if (v4) {
                     {
@@ -711,6 +860,7 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
                     k_cg_pm<R, Op, 1><<<pmg, pmb, 0, s>>>(op, pg, nb8, pb, nullptr, nullptr, x, r, Rd, 0, it, maxiter,
                                                           tr ? 1 : 0);
                 }
+            }
             }
             if (tr) k_cg_true<R, Op><<<nb, CG_T, 0, s>>>(op, n, b, x, r, Rd, it, maxiter);
             c->launches += tr ? 3 : 2;
@@ -755,7 +905,31 @@ int k_project(MpCtx* c, int* iters, double* res) {
     long long ftot = (long long)g.nfx + g.nfy + g.nfz;
     long long gtot = std::max(ftot, (long long)g.n);
     int it = 0; double rr = 0; int rc;
-    if (c->P.precision == MP_PREC_FP64) {
+    if (c->P.coef_mode == MP_COEF_GFM) {
+        // ghost-fluid variable density (FP32 vectors, FP64 dots); the scaled
+        // right-hand side lives in cell_tmp, free during the projection
+        if (!c->gfm_beta) {
+            MP_CUDA(c, cudaMalloc((void**)&c->gfm_beta, sizeof(float) * (size_t)ftot));
+            MP_CUDA(c, cudaMalloc((void**)&c->gfm_s, sizeof(float) * (size_t)g.n));
+        }
+        float* bx = c->gfm_beta; float* by = bx + g.nfx; float* bz = by + g.nfy;
+        float* x = c->press;
+        k_divergence<float><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
+                                                        c->au[0], c->au[1], c->au[2], c->divg, nullptr);
+        k_gfm_beta<<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, c->mark, c->lsmerge, 1.0f / c->P.density_ratio,
+                                                                bx, by, bz);
+        k_gfm_scale<<<nbk, 256, 0, c->stream>>>(g, c->mark, bx, by, bz, c->divg, c->gfm_s, c->cell_tmp);
+        c->launches += 3;
+        MP_CHECK_LAUNCH(c);
+        GfmOp gop{g, c->mark, bx, by, bz, c->gfm_s};
+        rc = run_cg<float>(c, gop, x, c->cell_tmp, c->cg_r, c->cg_p, c->cg_z, c->P.cg_max_iter, c->P.cg_tol_mode,
+                           c->P.cg_tol, 0, &it, &rr, MP_KT_CG_STENCIL);
+        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+        k_gfm_unscale<<<nbk, 256, 0, c->stream>>>(g.n, c->gfm_s, x);
+        k_subgrad_gfm<<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, x, bx, by, bz, c->wu[0], c->wu[1], c->wu[2],
+                                                                   c->au[0], c->au[1], c->au[2]);
+        c->launches += 2;
+    } else if (c->P.precision == MP_PREC_FP64) {
         double* x = c->cg64;
         double* b = x + g.n; double* r = b + g.n; double* p0 = r + g.n; double* p1 = p0 + g.n;
         k_divergence<double><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],

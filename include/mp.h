@@ -76,7 +76,7 @@ extern "C" {
 #define MP_PREC_MIXED    0   /* FP32 vectors, FP64 dots/alpha/beta            */
 #define MP_PREC_FP64     1   /* divergence, CG and gradient in FP64           */
 #define MP_COEF_REF      0   /* constant-coefficient Laplacian (reference)    */
-#define MP_COEF_GFM      1   /* variable density, ghost-fluid face weights    */
+#define MP_COEF_GFM      1   /* variable density, ghost-fluid face weights (extension; MP_PREC_MIXED only) */
 
 #define MP_PARAMS_VERSION 3
 

@@ -833,7 +833,114 @@ struct Oracle {
         if (residual) *residual = res;
         return capped ? MP_ERR_NOCONVERGE : MP_OK;
     }
+    // Ghost-fluid variable density (MP_COEF_GFM, an extension; the reference's
+    // projection is constant-coefficient): face weights beta = 1/rho_face with
+    // rho_liquid = 1, rho_air = 1/ratio, theta-blended across liquid-air faces
+    // (theta = -ls_L / (ls_G - ls_L), clamped to [0, 1]); the system
+    //   sum over non-wall neighbours of beta_f (p_nb - p_c) / h^2 = div
+    // solved in FP64 to a 1e-12 relative residual (Jacobi-scaled CG), then
+    // u -= beta grad p on both velocity fields. The reference solution the GPU
+    // form is checked against.
+    int project_gfm(int* iters, double* residual) {
+        std::vector<double> b;
+        divergence<double>(b);
+        for (int i = 0; i < n; i++) divg[i] = (float)b[i];
+        const float rho_air = 1.0f / P.density_ratio;
+        std::vector<float> beta[3] = {std::vector<float>(nfx, 0.f), std::vector<float>(nfy, 0.f),
+                                      std::vector<float>(nfz, 0.f)};
+        auto unknown = [&](int m) { return m == TF || m == TA; };
+        auto rho = [&](int m) { return m == TA ? rho_air : 1.0f; };
+        for (int ax = 0; ax < 3; ax++) {
+            int nf = ax == 0 ? nfx : (ax == 1 ? nfy : nfz);
+            #pragma omp parallel for
+            for (int idx = 0; idx < nf; idx++) {
+                int i, j, k;
+                if (ax == 0) getijk3(idx, NX + 1, NY, NZ, i, j, k);
+                else if (ax == 1) getijk3(idx, NX, NY + 1, NZ, i, j, k);
+                else getijk3(idx, NX, NY, NZ + 1, i, j, k);
+                int e = ax == 0 ? i : (ax == 1 ? j : k), nn = ax == 0 ? NX : (ax == 1 ? NY : NZ);
+                float bt = 0.f;
+                if (e > 0 && e < nn) {
+                    int cb = cid(i, j, k), ca = cid(i - (ax == 0), j - (ax == 1), k - (ax == 2));
+                    int ma = mark[ca], mb = mark[cb];
+                    if (unknown(ma) && unknown(mb)) {
+                        if (ma == mb) bt = 1.0f / rho(ma);
+                        else {
+                            int cl = ma == TF ? ca : cb, cg = ma == TF ? cb : ca;
+                            float ll = lsmerge[cl], lg = lsmerge[cg];
+                            float th = (lg == ll) ? 0.5f : (0.0f - ll) / (lg - ll);
+                            th = std::min(1.0f, std::max(0.0f, th));
+                            bt = 1.0f / (th * 1.0f + (1.0f - th) * rho_air);
+                        }
+                    } else if (unknown(ma)) bt = 1.0f / rho(ma);
+                    else if (unknown(mb)) bt = 1.0f / rho(mb);
+                }
+                beta[ax][idx] = bt;
+            }
+        }
+        auto inner = [&](int i, int j, int k) { return i > 0 && i < NX - 1 && j > 0 && j < NY - 1 && k > 0 && k < NZ - 1; };
+        auto mask = [&](int c) { int i, j, k; getijk(c, i, j, k); return unknown(mark[c]) && inner(i, j, k); };
+        // the six (neighbour, face weight) pairs of a cell
+        auto nbrs = [&](int c, int* q, double* w) {
+            int i, j, k; getijk(c, i, j, k);
+            q[0] = cid(i + 1, j, k); w[0] = beta[0][fx(i + 1, j, k)];
+            q[1] = cid(i, j + 1, k); w[1] = beta[1][fy(i, j + 1, k)];
+            q[2] = cid(i, j, k + 1); w[2] = beta[2][fz(i, j, k + 1)];
+            q[3] = cid(i - 1, j, k); w[3] = beta[0][fx(i, j, k)];
+            q[4] = cid(i, j - 1, k); w[4] = beta[1][fy(i, j, k)];
+            q[5] = cid(i, j, k - 1); w[5] = beta[2][fz(i, j, k)];
+        };
+        const double h2 = (double)h * (double)h;
+        std::vector<double> S(n, 0.0), bs(n, 0.0), y(n, 0.0);
+        #pragma omp parallel for
+        for (int c = 0; c < n; c++) {
+            if (!mask(c)) continue;
+            int q[6]; double w[6]; nbrs(c, q, w);
+            double d = 0;
+            for (int t = 0; t < 6; t++) if (mark[q[t]] != TB) d += w[t];
+            d /= h2;
+            S[c] = d > 0 ? 1.0 / std::sqrt(d) : 0.0;
+            bs[c] = S[c] * b[c];
+        }
+        auto A = [&](std::vector<double>& o, const std::vector<double>& v) {
+            #pragma omp parallel for
+            for (int c = 0; c < n; c++) {
+                if (!mask(c)) { o[c] = 0; continue; }
+                int q[6]; double w[6]; nbrs(c, q, w);
+                double s = 0;
+                for (int t = 0; t < 6; t++)
+                    if (mark[q[t]] != TB) s += w[t] * (S[q[t]] * v[q[t]] - S[c] * v[c]);
+                o[c] = S[c] * s / h2;
+            }
+        };
+        bool capped = false;
+        double res = 0;
+        int it = cg<double>(y, bs, mask, A, std::max(P.cg_max_iter, 20000), MP_TOL_REL, 1e-12f, 0, res, capped);
+        std::vector<double> p(n);
+        for (int c = 0; c < n; c++) { p[c] = S[c] * y[c]; press[c] = (float)p[c]; }
+        for (int ax = 0; ax < 3; ax++) {
+            int nf = ax == 0 ? nfx : (ax == 1 ? nfy : nfz);
+            #pragma omp parallel for
+            for (int idx = 0; idx < nf; idx++) {
+                int i, j, k;
+                if (ax == 0) getijk3(idx, NX + 1, NY, NZ, i, j, k);
+                else if (ax == 1) getijk3(idx, NX, NY + 1, NZ, i, j, k);
+                else getijk3(idx, NX, NY, NZ + 1, i, j, k);
+                int e = ax == 0 ? i : (ax == 1 ? j : k), nn = ax == 0 ? NX : (ax == 1 ? NY : NZ);
+                if (!(e > 0 && e < nn)) continue;
+                double d = (double)beta[ax][idx] *
+                           (p[cid(i, j, k)] - p[cid(i - (ax == 0), j - (ax == 1), k - (ax == 2))]) / (double)h;
+                wu[ax][idx] = (float)((double)wu[ax][idx] - d);
+                au[ax][idx] = (float)((double)au[ax][idx] - d);
+            }
+        }
+        last_iters = it; last_res = res;
+        if (iters) *iters = it;
+        if (residual) *residual = res;
+        return capped ? MP_ERR_NOCONVERGE : MP_OK;
+    }
     int project(int* iters, double* residual) {
+        if (P.coef_mode == MP_COEF_GFM) return project_gfm(iters, residual);
         if (P.precision == MP_PREC_FP64) return project_t<double>(iters, residual);
         return project_t<float>(iters, residual);
     }

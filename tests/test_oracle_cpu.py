@@ -103,6 +103,63 @@ def test_projection_solves_the_reference_laplacian(mp, oracle_mod, config):
     assert (x[~unk] == 0).all()
 
 
+def _to_projection(o):
+    o.hashAndSortParticles(); o.addexternalforce(); o.computeLevelset(0.0); o.sweepLSAndMardGrid()
+    o.markSoloAirParticle(); o.computesurfacetension()
+    o.mapvelp2g_bubble(); o.enforceDragForce()
+    for ph in (1, 0):
+        o.sweepPhi(ph); o.sweepU(ph)
+    o.setWaterBoundaryU(1); o.setWaterBoundaryU(0)
+
+
+def test_gfm_at_unit_density_ratio_is_the_reference_projection(mp, oracle_mod):
+    """With rho_liquid = rho_air every face weight is 1 and the ghost-fluid
+    projection is the reference's constant-coefficient one."""
+    out = []
+    for over in ({"precision": mp.PREC_FP64, "cg_tol": 1e-13, "cg_max_iter": 20000},
+                 {"coef_mode": 1, "density_ratio": 1.0}):
+        o, p, _ = _oracle(mp, oracle_mod, 1, 32, **over)
+        _to_projection(o)
+        it, res, rc = o.project_CG_bubble()
+        assert rc == 0
+        out.append({f: o.get_field(f).astype(np.float64) for f in ("press", "waterux", "airuz")})
+    for f in out[0]:
+        a, b = out[0][f], out[1][f]
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(a).max(), f
+
+
+def test_gfm_projection_leaves_single_phase_interiors_divergence_free(mp, oracle_mod):
+    """At a 1000:1 density ratio the projected faces satisfy D u = 0 wherever
+    the divergence reads one phase only (cells whose six neighbours are of
+    their own type), i.e. D beta G is the matrix that was solved."""
+    o, p, _ = _oracle(mp, oracle_mod, 1, 32, coef_mode=1, density_ratio=1000.0)
+    _to_projection(o)
+    b = None
+    it, res, rc = o.project_CG_bubble()
+    assert rc == 0 and it > 0
+    b = o.get_field("div").astype(np.float64)
+    n, h = p.nx, p.cellsize
+    mark = o.get_field("mark").reshape(n, n, n)
+    w = [o.get_field(f).astype(np.float64) for f in ("waterux", "wateruy", "wateruz")]
+    a = [o.get_field(f).astype(np.float64) for f in ("airux", "airuy", "airuz")]
+    w = [w[0].reshape(n + 1, n, n), w[1].reshape(n, n + 1, n), w[2].reshape(n, n, n + 1)]
+    a = [a[0].reshape(n + 1, n, n), a[1].reshape(n, n + 1, n), a[2].reshape(n, n, n + 1)]
+    checked = 0
+    worst = 0.0
+    for t, u in ((mp.TYPEFLUID, w), (mp.TYPEAIR, a)):
+        c = mark[1:-1, 1:-1, 1:-1] == t
+        for d in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+            c &= np.roll(mark, (-d[0], -d[1], -d[2]), axis=(0, 1, 2))[1:-1, 1:-1, 1:-1] == t
+        div = ((u[0][2:-1, 1:-1, 1:-1] - u[0][1:-2, 1:-1, 1:-1]) + (u[1][1:-1, 2:-1, 1:-1] - u[1][1:-1, 1:-2, 1:-1]) +
+               (u[2][1:-1, 1:-1, 2:-1] - u[2][1:-1, 1:-1, 1:-2])) / h
+        checked += int(c.sum())
+        if c.any():
+            worst = max(worst, float(np.abs(div[c]).max()))
+    assert checked > 1000
+    # face velocities are stored in FP32 after the FP64 solve
+    assert worst <= 1e-5 * float(np.abs(b).max())
+
+
 def test_oracle_is_thread_count_independent(mp, oracle_mod):
     a, _, _ = _oracle(mp, oracle_mod, 2, 16, seed=5)
     oracle_mod.load().or_set_threads(1)
