@@ -324,30 +324,53 @@ __global__ void __launch_bounds__(256, 6) k_correct_pos(Grid g, Cells cl, int np
         span(rel.x, g.NX, i, ilo, ihi); span(rel.y, g.NY, j, jlo, jhi); span(rel.z, g.NZ, k, klo, khi);
         // the cells of a (di,dj) column are contiguous: their range bounds are
         // read together, then each cell is summed on its own
+        // Two phases keep the warp's lanes together: the scan collects the
+        // pairs within re (a few of the ~64 candidates) in visiting order,
+        // with the ordinal of their cell; the spring terms of the collected
+        // pairs are then formed in that order, each cell's sum added to the
+        // total when the next cell starts (a cell without pairs adds +0, a
+        // no-op). A full buffer is drained in the middle of the scan.
+        constexpr int CP_BUF = 16;
+        uint32_t ent[CP_BUF];
+        uint8_t eo[CP_BUF];
+        int ne = 0, cur = -1;
+        float3 s = mk3(0.0f);
+        auto drain = [&]() {
+            for (int e = 0; e < ne; e++) {
+                if ((int)eo[e] != cur) { spring += s; s = mk3(0.0f); cur = eo[e]; }
+                const uint32_t t = ent[e];
+                float3 o = xyz(__ldg(pos + t));
+                float3 dd = o - ip;
+                float m = __ldg(&vel[t].w);
+                float dist = length(dd);
+                float w = m * smooth_kernel(dist * dist, re);
+                if (dist > 0.1f * re) s += w * (ip - o) / dist;
+            }
+            ne = 0;
+        };
         const int k0 = max(k + klo, 0), k1 = min(k + khi, g.NZ - 1);
+        int ord = 0;
         for (int di = ilo; di <= ihi; di++) for (int dj = jlo; dj <= jhi; dj++) {
             if (!vc(g, i + di, j + dj, k)) continue;
             const int cb = cid(g, i + di, j + dj, k0);
             uint32_t bnd[4];
             #pragma unroll
             for (int q = 0; q < 4; q++) bnd[q] = (q <= k1 - k0 + 1) ? __ldg(cl.off + cb + q) : 0u;
-            for (int cc = 0; cc <= k1 - k0; cc++) {
-            float3 s = mk3(0.0f);
-            for (uint32_t t = bnd[cc]; t < bnd[cc + 1]; ++t) {
-                float3 o = xyz(__ldg(pos + t));
-                float3 dd = o - ip;
-                // beyond re the kernel weight is exactly zero and the pair adds a
-                // signed zero, which leaves the sum unchanged: skip it (exact test
-                // with margin: dist*dist >= re*re whenever d2 > 1.001 re*re)
-                if (dot(dd, dd) > re2_skip) continue;
-                float m = __ldg(&vel[t].w);
-                float dist = length(dd);
-                float w = m * smooth_kernel(dist * dist, re);
-                if (dist > 0.1f * re) s += w * (ip - o) / dist;
-            }
-            spring += s;
+            for (int cc = 0; cc <= k1 - k0; cc++, ord++) {
+                for (uint32_t t = bnd[cc]; t < bnd[cc + 1]; ++t) {
+                    float3 o = xyz(__ldg(pos + t));
+                    float3 dd = o - ip;
+                    // beyond re the kernel weight is exactly zero and the pair adds a
+                    // signed zero, which leaves the sum unchanged: skip it (exact test
+                    // with margin: dist*dist >= re*re whenever d2 > 1.001 re*re)
+                    if (dot(dd, dd) > re2_skip) continue;
+                    if (ne == CP_BUF) drain();
+                    ent[ne] = t; eo[ne] = (uint8_t)ord; ne++;
+                }
             }
         }
+        drain();
+        spring += s;
         spring *= spring_k * re;
         if (length(dt * spring) > 0.3f * h) ip += h * 0.3f * spring / length(spring);
         else ip += dt * spring;
