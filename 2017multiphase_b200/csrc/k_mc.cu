@@ -26,103 +26,162 @@ struct McGrid {
     int NXMC, NYMC, NZMC;   // voxels
     int W, H, D;            // nodes
     float hm;               // node spacing
-    Tiles T;                // 3-D tiling of the nodes for the density gather
 };
 
+// One thread computes NJ x NK nodes, (i, j0 + nj, k0 + nk). Neighbouring
+// nodes share most of their 4 x 4 x 4 cell windows, so the thread walks the
+// union window once, (a, b, c) ascending, and each node takes only the cells
+// of its own window: every node sees its cells, and the particles in them, in
+// the reference's (di, dj, dk, particle) order, and keeps its own per-cell
+// partial sum (res) and running sums, so each field value is bit-identical to
+// the one-node-per-thread gather. A cell's header (type mask, range) and its
+// particles are loaded once for all the nodes that need them.
 // GAS2 (with SURF == MP_MC_FLUID): the gas field is accumulated in the same
 // pass into dens2. Both surfaces use the same radius and weight, the gas
 // particles are a subset of the fluid ones, and each sum keeps its own
 // accumulators in the same visiting order, so both fields equal the separate
 // passes bit for bit.
-template <int SURF, bool GAS2 = false>
-__global__ void __launch_bounds__(256, 6) k_mc_density(McGrid m, Cells cl, const float4* __restrict__ pos, float* __restrict__ dens,
-                                                    int scene, float* __restrict__ dens2 = nullptr) {
-    const Tiles T = m.T;
+template <int SURF, bool GAS2, int NJ, int NK, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mc_density(McGrid m, Tiles T, Cells cl, const float4* __restrict__ pos,
+                                                          float* __restrict__ dens, int scene, float* __restrict__ dens2) {
     const float hm = m.hm;
     const uint32_t need = SURF == MP_MC_SOLID ? (1u << MP_TYPESOLID)
                         : SURF == MP_MC_FLUID ? ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO) | (1u << MP_TYPEFLUID))
                                               : ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO));
+    const float R = SURF == MP_MC_SOLID ? hm : hm * 2;
+    const float cut = SURF == MP_MC_SOLID ? hm * hm * 1.001f : R * R * 1.001f;
     MP_GRID_LOOP(t, T.threads()) {
-        int i, j, k; if (!tile_ijk(T, t, i, j, k)) continue;
-        float3 p = mk3((float)i, (float)j, (float)k) * hm;
-        float3 center = mk3(0.0f), center2 = mk3(0.0f);
-        float wsum = 0.0f, wsum2 = 0.0f;
+        int i, jt, kt; if (!tile_ijk(T, t, i, jt, kt)) continue;
+        const int j0 = jt * NJ, k0 = kt * NK;
+        const float px = (float)i * hm;
+        float py[NJ], pz[NK];
+        #pragma unroll
+        for (int n = 0; n < NJ; n++) py[n] = (float)(j0 + n) * hm;
+        #pragma unroll
+        for (int n = 0; n < NK; n++) pz[n] = (float)(k0 + n) * hm;
+        float cx[NJ][NK], cy[NJ][NK], cz[NJ][NK], ws[NJ][NK];
+        float gx[NJ][NK], gy[NJ][NK], gz[NJ][NK], gw[NJ][NK];
+        #pragma unroll
+        for (int u = 0; u < NJ; u++)
+            #pragma unroll
+            for (int v = 0; v < NK; v++) {
+                cx[u][v] = cy[u][v] = cz[u][v] = ws[u][v] = 0.0f;
+                gx[u][v] = gy[u][v] = gz[u][v] = gw[u][v] = 0.0f;
+            }
+        // the cell loops stay rolled: unrolled, they multiply the particle loop's
+        // code until the instruction cache misses dominate
+        #pragma unroll 1
         for (int di = -2; di <= 1; ++di) {
             int a = i + di; if (a < 0 || a > m.NXMC - 1) continue;
-            for (int dj = -2; dj <= 1; ++dj) {
-                int b = j + dj; if (b < 0 || b > m.NYMC - 1) continue;
-                for (int dk = -2; dk <= 1; ++dk) {
-                    int cc = k + dk; if (cc < 0 || cc > m.NZMC - 1) continue;
-                    int c = a * m.NYMC * m.NZMC + b * m.NZMC + cc;
+            #pragma unroll 1
+            for (int b = j0 - 2; b <= j0 + NJ; ++b) {
+                if (b < 0 || b > m.NYMC - 1) continue;
+                const int cb = a * m.NYMC * m.NZMC + b * m.NZMC;
+                #pragma unroll 1
+                for (int cc = k0 - 2; cc <= k0 + NK; ++cc) {
+                    if (cc < 0 || cc > m.NZMC - 1) continue;
+                    int c = cb + cc;
                     if (!(__ldg(cl.tmask + c) & need)) continue;
-                    float3 res = mk3(0.0f), res2 = mk3(0.0f);
-                    for (uint32_t q = __ldg(cl.off + c); q < __ldg(cl.off + c + 1); ++q) {
+                    float rx[NJ][NK], ry[NJ][NK], rz[NJ][NK];
+                    float sx[NJ][NK], sy[NJ][NK], sz[NJ][NK];
+                    #pragma unroll
+                    for (int u = 0; u < NJ; u++)
+                        #pragma unroll
+                        for (int v = 0; v < NK; v++) rx[u][v] = ry[u][v] = rz[u][v] = sx[u][v] = sy[u][v] = sz[u][v] = 0.0f;
+                    const uint32_t q1 = __ldg(cl.off + c + 1);
+                    #pragma unroll 1
+                    for (uint32_t q = __ldg(cl.off + c); q < q1; ++q) {
                         float4 o = __ldg(pos + q);
                         int f = pflag(o);
-                        float3 op = xyz(o);
-                        // beyond the kernel radius the weight is exactly zero and the pair
-                        // adds nothing: skip it before the sqrt (exact test with margin)
-                        float3 dd = op - p;
-                        float d2 = dot(dd, dd);
-                        if (SURF == MP_MC_SOLID) {
-                            if (f != MP_TYPESOLID) continue;
-                            if (d2 > hm * hm * 1.001f) continue;
-                            float dis = length(op - p);
-                            if (dis < hm) {
-                                float w = dis / (4 * hm);
-                                w = 1 - w * w;
-                                w = (float)fmax((double)(w * w * w), 0.0);
-                                res += op * w; wsum += w;
-                            }
-                        } else {
-                            bool ok = SURF == MP_MC_FLUID ? (f == MP_TYPEAIR || f == MP_TYPEAIRSOLO || f == MP_TYPEFLUID)
-                                                          : (f == MP_TYPEAIR || (f == MP_TYPEAIRSOLO && scene != MP_SCENE_INTERACTION));
-                            if (!ok) continue;
-                            float R = hm * 2;
-                            if (d2 > R * R * 1.001f) continue;
-                            float dis = length(op - p);
-                            if (dis < R) {
-                                float w = R * R - dis * dis;
-                                w = w * w * w;
-                                res += op * w; wsum += w;
-                                if (GAS2 && (f == MP_TYPEAIR || (f == MP_TYPEAIRSOLO && scene != MP_SCENE_INTERACTION))) {
-                                    res2 += op * w; wsum2 += w;
+                        bool ok = SURF == MP_MC_SOLID ? (f == MP_TYPESOLID)
+                                : SURF == MP_MC_FLUID ? (f == MP_TYPEAIR || f == MP_TYPEAIRSOLO || f == MP_TYPEFLUID)
+                                                      : (f == MP_TYPEAIR || (f == MP_TYPEAIRSOLO && scene != MP_SCENE_INTERACTION));
+                        if (!ok) continue;
+                        const bool gas = GAS2 && (f == MP_TYPEAIR || (f == MP_TYPEAIRSOLO && scene != MP_SCENE_INTERACTION));
+                        const float dx = o.x - px;
+                        #pragma unroll
+                        for (int u = 0; u < NJ; u++) {
+                            // node j0 + u takes cells j0 + u - 2 .. j0 + u + 1
+                            if (b - j0 - u < -2 || b - j0 - u > 1) continue;
+                            const float dy = o.y - py[u];
+                            const float dxy = dx * dx + dy * dy;
+                            #pragma unroll
+                            for (int v = 0; v < NK; v++) {
+                                if (cc - k0 - v < -2 || cc - k0 - v > 1) continue;
+                                const float dz = o.z - pz[v];
+                                // dot(d, d) evaluates (x*x + y*y) + z*z; beyond the kernel
+                                // radius the weight is exactly zero and the pair adds nothing:
+                                // skip it before the sqrt (exact test with margin)
+                                const float d2 = dxy + dz * dz;
+                                if (d2 > cut) continue;
+                                const float dis = sqrtf(d2);
+                                if (!(dis < R)) continue;
+                                float w;
+                                if (SURF == MP_MC_SOLID) {
+                                    w = dis / (4 * hm);
+                                    w = 1 - w * w;
+                                    w = (float)fmax((double)(w * w * w), 0.0);
+                                } else {
+                                    w = R * R - dis * dis;
+                                    w = w * w * w;
                                 }
+                                rx[u][v] += o.x * w; ry[u][v] += o.y * w; rz[u][v] += o.z * w; ws[u][v] += w;
+                                if (gas) { sx[u][v] += o.x * w; sy[u][v] += o.y * w; sz[u][v] += o.z * w; gw[u][v] += w; }
                             }
                         }
                     }
-                    center += res;
-                    if (GAS2) center2 += res2;
+                    // a node outside this cell's window kept res = +0, and center + (+0)
+                    // is center (center is never -0: it starts at +0 and sums of finite
+                    // values round to +0)
+                    #pragma unroll
+                    for (int u = 0; u < NJ; u++)
+                        #pragma unroll
+                        for (int v = 0; v < NK; v++) {
+                            cx[u][v] += rx[u][v]; cy[u][v] += ry[u][v]; cz[u][v] += rz[u][v];
+                            if (GAS2) { gx[u][v] += sx[u][v]; gy[u][v] += sy[u][v]; gz[u][v] += sz[u][v]; }
+                        }
                 }
             }
         }
-        bool border = (i * j * k == 0 || i == m.NXMC || j == m.NYMC || k == m.NZMC);
-        float phi;
-        if (SURF == MP_MC_SOLID) {
-            float r = 0.75f * hm, thigh = 0.51f, tlow = 0.49f;
-            if (wsum > 0) {
-                center /= wsum;
-                float Ev = fmaxf(center.x, fmaxf(center.y, center.z)) / (4 * hm);
-                float gamma = (thigh - Ev) / (thigh - tlow);
-                float f = (Ev < tlow) ? 1 : gamma * gamma * gamma - 3 * gamma * gamma + 3 * gamma;
-                phi = (length(p - center) - r * f);
-            } else phi = -r;
-            if (border) phi = fminf(phi, -10.0f);
-        } else {
-            float r = SURF == MP_MC_FLUID ? 0.5f * hm : 0.8f * hm;
-            if (wsum > 0) { center /= wsum; phi = r - length(p - center); }
-            else phi = -r;
-            if (border) phi = -1000.0f;
-            if (GAS2) {
-                const float r2 = 0.8f * hm;
-                float phi2;
-                if (wsum2 > 0) { center2 /= wsum2; phi2 = r2 - length(p - center2); }
-                else phi2 = -r2;
-                if (border) phi2 = -1000.0f;
-                dens2[(i * m.H + j) * m.D + k] = phi2;
+        #pragma unroll
+        for (int u = 0; u < NJ; u++)
+            #pragma unroll
+            for (int v = 0; v < NK; v++) {
+                const int j = j0 + u, k = k0 + v;
+                if (j >= m.H || k >= m.D) continue;
+                const float3 p = mk3(px, py[u], pz[v]);
+                float3 center = mk3(cx[u][v], cy[u][v], cz[u][v]);
+                const float wsum = ws[u][v];
+                bool border = (i * j * k == 0 || i == m.NXMC || j == m.NYMC || k == m.NZMC);
+                float phi;
+                if (SURF == MP_MC_SOLID) {
+                    float r = 0.75f * hm, thigh = 0.51f, tlow = 0.49f;
+                    if (wsum > 0) {
+                        center /= wsum;
+                        float Ev = fmaxf(center.x, fmaxf(center.y, center.z)) / (4 * hm);
+                        float gamma = (thigh - Ev) / (thigh - tlow);
+                        float f = (Ev < tlow) ? 1 : gamma * gamma * gamma - 3 * gamma * gamma + 3 * gamma;
+                        phi = (length(p - center) - r * f);
+                    } else phi = -r;
+                    if (border) phi = fminf(phi, -10.0f);
+                } else {
+                    float r = SURF == MP_MC_FLUID ? 0.5f * hm : 0.8f * hm;
+                    if (wsum > 0) { center /= wsum; phi = r - length(p - center); }
+                    else phi = -r;
+                    if (border) phi = -1000.0f;
+                    if (GAS2) {
+                        const float r2 = 0.8f * hm;
+                        float3 center2 = mk3(gx[u][v], gy[u][v], gz[u][v]);
+                        const float wsum2 = gw[u][v];
+                        float phi2;
+                        if (wsum2 > 0) { center2 /= wsum2; phi2 = r2 - length(p - center2); }
+                        else phi2 = -r2;
+                        if (border) phi2 = -1000.0f;
+                        dens2[(i * m.H + j) * m.D + k] = phi2;
+                    }
+                }
+                dens[(i * m.H + j) * m.D + k] = phi;
             }
-        }
-        dens[(i * m.H + j) * m.D + k] = phi;
     }
 }
 
@@ -284,8 +343,36 @@ static McGrid mc_grid(const MpCtx* c) {
     m.NXMC = 2 * c->G.NX; m.NYMC = 2 * c->G.NY; m.NZMC = 2 * c->G.NZ;
     m.W = m.NXMC + 1; m.H = m.NYMC + 1; m.D = m.NZMC + 1;
     m.hm = c->G.h / (float)(m.NXMC / c->G.NX);
-    m.T = make_tiles(m.W, m.H, m.D);
     return m;
+}
+
+// nodes per thread of the density gather (along j, along k) and its
+// resident-blocks hint, for the single-field and the fused fluid + gas passes
+#ifndef MC_DENS_NJ
+#define MC_DENS_NJ 2
+#endif
+#ifndef MC_DENS_NK
+#define MC_DENS_NK 1
+#endif
+#ifndef MC_DENS_MINB
+#define MC_DENS_MINB 4
+#endif
+#ifndef MC_GAS2_NJ
+#define MC_GAS2_NJ 2
+#endif
+#ifndef MC_GAS2_NK
+#define MC_GAS2_NK 1
+#endif
+#ifndef MC_GAS2_MINB
+#define MC_GAS2_MINB 4
+#endif
+template <int SURF, bool GAS2>
+static void launch_density(const McGrid& m, Cells cl, const float4* pos, float* dens, int scene, float* dens2,
+                           cudaStream_t s) {
+    constexpr int NJ = GAS2 ? MC_GAS2_NJ : MC_DENS_NJ, NK = GAS2 ? MC_GAS2_NK : MC_DENS_NK;
+    constexpr int MINB = GAS2 ? MC_GAS2_MINB : MC_DENS_MINB;
+    const Tiles T = make_tiles(m.W, (m.H + NJ - 1) / NJ, (m.D + NK - 1) / NK);
+    k_mc_density<SURF, GAS2, NJ, NK, MINB><<<mp_blocks(T.threads(), 256), 256, 0, s>>>(m, T, cl, pos, dens, scene, dens2);
 }
 static int mc_extract(MpCtx* c, const McGrid& m, int surface, const float* dens);
 
@@ -310,9 +397,9 @@ int k_mc(MpCtx* c, int surface) {
         k_mc_solid_empty<<<mp_blocks((long long)m.W * m.H * m.D, 256), 256, 0, s>>>(m, c->mc_dens);
     } else {
         KtScope kt(c, MP_KT_MC_DENS);
-        if (surface == MP_MC_SOLID) k_mc_density<MP_MC_SOLID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
-        else if (surface == MP_MC_FLUID) k_mc_density<MP_MC_FLUID><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
-        else k_mc_density<MP_MC_GAS><<<mp_blocks(m.T.threads(), 256), 256, 0, s>>>(m, cl, c->pos, c->mc_dens, c->P.scene);
+        if (surface == MP_MC_SOLID) launch_density<MP_MC_SOLID, false>(m, cl, c->pos, c->mc_dens, c->P.scene, nullptr, s);
+        else if (surface == MP_MC_FLUID) launch_density<MP_MC_FLUID, false>(m, cl, c->pos, c->mc_dens, c->P.scene, nullptr, s);
+        else launch_density<MP_MC_GAS, false>(m, cl, c->pos, c->mc_dens, c->P.scene, nullptr, s);
     }
     c->launches++;
     return mc_extract(c, m, surface, c->mc_dens);
@@ -326,8 +413,7 @@ int k_mc_fluid_gas(MpCtx* c) {
     Cells cl{c->cell_off, c->tmask};
     {
         KtScope kt(c, MP_KT_MC_DENS);
-        k_mc_density<MP_MC_FLUID, true><<<mp_blocks(m.T.threads(), 256), 256, 0, c->stream>>>(m, cl, c->pos, c->mc_dens,
-                                                                                               c->P.scene, c->mc_dens2);
+        launch_density<MP_MC_FLUID, true>(m, cl, c->pos, c->mc_dens, c->P.scene, c->mc_dens2, c->stream);
     }
     c->launches++;
     MP_TRY(mc_extract(c, m, MP_MC_FLUID, c->mc_dens));
