@@ -27,9 +27,12 @@ LIB_PATH = os.path.join(_HERE, "libmp.so")
 INCLUDE_H = os.path.join(os.path.dirname(_HERE), "include", "mp.h")
 
 # status codes (mp.h)
-MP_OK, MP_ERR_CUDA, MP_ERR_CAPACITY, MP_ERR_NOCONVERGE, MP_ERR_TIMEOUT, MP_ERR_ARG, MP_ERR_STATE = range(7)
+MP_OK, MP_ERR_CUDA, MP_ERR_CAPACITY, MP_ERR_NOCONVERGE, MP_ERR_TIMEOUT, MP_ERR_ARG, MP_ERR_STATE, MP_ERR_IO = range(8)
 _ERR_NAMES = {1: "MP_ERR_CUDA", 2: "MP_ERR_CAPACITY", 3: "MP_ERR_NOCONVERGE", 4: "MP_ERR_TIMEOUT",
-              5: "MP_ERR_ARG", 6: "MP_ERR_STATE"}
+              5: "MP_ERR_ARG", 6: "MP_ERR_STATE", 7: "MP_ERR_IO"}
+# per-frame file formats and particle kinds (mp.h, cspray::output*)
+OUT_POV_MESH, OUT_OBJ_MESH, OUT_BOBJ_GZ = range(3)
+OUT_PARTICLES_COLORED, OUT_PARTICLES_SOLO, OUT_PARTICLES_AIR = range(3)
 
 # particle and cell types (utility.h:13-19)
 TYPEFLUID, TYPEAIR, TYPEBOUNDARY, TYPEVACUUM, TYPEAIRSOLO, TYPESOLID = range(6)
@@ -64,6 +67,11 @@ class MPState(C.Structure):
                 ("last_heat_cg_iters", C.c_int32), ("last_heat_cg_residual", C.c_double),
                 ("mc_verts", C.c_int32 * 3), ("mc_indices", C.c_int32 * 3), ("mc_active_voxels", C.c_int32 * 3),
                 ("reserved", C.c_int32 * 6)]
+
+
+class MPOutput(C.Structure):
+    _fields_ = [("dir", C.c_char_p), ("pov", C.c_int32), ("obj", C.c_int32), ("colored_particles", C.c_int32),
+                ("t_render_min", C.c_float), ("t_render_max", C.c_float)]
 
 
 _lib = None
@@ -155,6 +163,11 @@ def load_library() -> C.CDLL:
         "mp_scene_particles": ([P, C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_int), vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "mp_scene_tables": ([P, C.c_int, C.c_uint64, vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "mp_scene_fixed_heat": ([P, C.c_int, vp], C.c_int),
+        "mp_write_mesh": ([C.c_int, C.c_char_p, C.c_char_p, vp, vp, C.c_int, vp, C.c_int], C.c_int),
+        "mp_write_particles": ([C.c_int, C.c_char_p, vp, vp, vp, C.c_int, C.c_float, C.c_float], C.c_int),
+        "mp_export_mesh": ([vp, C.c_int, C.c_int, C.c_char_p], C.c_int),
+        "mp_export_particles": ([vp, C.c_int, C.c_char_p, C.c_float, C.c_float], C.c_int),
+        "mp_set_output": ([vp, C.POINTER(MPOutput)], C.c_int),
     }
     for nm, (args, res) in sig.items():
         f = getattr(lib, nm)
@@ -241,6 +254,29 @@ def scene_fixed_heat(p, config: int) -> np.ndarray:
     fh = np.zeros(p.nx * p.ny * p.nz, np.float32)
     _check(lib.mp_scene_fixed_heat(C.byref(p), config, _ptr(fh)), None)
     return fh
+
+
+def write_mesh(fmt: int, path: str, verts: np.ndarray, normals: np.ndarray, indices: np.ndarray,
+               object_name: str = "water"):
+    """One mesh from host arrays in the reference's POV-Ray / OBJ / BOBJ.gz
+    format (mp_write_mesh)."""
+    lib = load_library()
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    nr = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+    ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    _check(lib.mp_write_mesh(fmt, os.fsencode(path), object_name.encode(), _ptr(v), _ptr(nr), len(v), _ptr(ix),
+                             len(ix)), None)
+
+
+def write_particles(kind: int, path: str, pos: np.ndarray, flag: Optional[np.ndarray] = None,
+                    temperature: Optional[np.ndarray] = None, t_min: float = 273.0, t_max: float = 373.0):
+    """POV-Ray particle spheres from host arrays (mp_write_particles)."""
+    lib = load_library()
+    p3 = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    fl = None if flag is None else np.ascontiguousarray(flag, np.int8)
+    T = None if temperature is None else np.ascontiguousarray(temperature, np.float32)
+    _check(lib.mp_write_particles(kind, os.fsencode(path), _ptr(p3), _ptr(fl), _ptr(T), len(p3), t_min, t_max),
+           None)
 
 
 def mc_tables():
@@ -405,6 +441,27 @@ class Sim:
         v = np.zeros((nv, 3), np.float32); nr = np.zeros((nv, 3), np.float32); ix = np.zeros(ni, np.uint32)
         _check(self.lib.mp_mc_download(self.ctx, surface, _ptr(v), _ptr(nr), _ptr(ix), nv, ni), self.ctx)
         return v, nr, ix
+
+    # ---- per-frame files (cspray::output*) ----------------------------------
+    def export_mesh(self, surface: int, fmt: int, path: str):
+        """The last extraction of `surface` as a file (mp_export_mesh)."""
+        _check(self.lib.mp_export_mesh(self.ctx, surface, fmt, os.fsencode(path)), self.ctx)
+
+    def export_particles(self, kind: int, path: str, t_min: float = 273.0, t_max: float = 373.0):
+        _check(self.lib.mp_export_particles(self.ctx, kind, os.fsencode(path), t_min, t_max), self.ctx)
+
+    def set_output(self, out_dir: Optional[str], pov: bool = False, obj: bool = True, colored_particles: bool = True,
+                   t_render_min: float = 273.0, t_render_max: float = 373.0):
+        """Per-frame files written by each step that extracts meshes (mp_set_output);
+        defaults are cspray::initparam's (spray.cpp:30-33, 61). None turns it off.
+        `out_dir` is a prefix used as written, so it ends with a separator."""
+        if out_dir is None:
+            self._out = None
+            _check(self.lib.mp_set_output(self.ctx, None), self.ctx)
+            return
+        self._out = MPOutput(os.fsencode(out_dir), int(pov), int(obj), int(colored_particles), t_render_min,
+                             t_render_max)
+        _check(self.lib.mp_set_output(self.ctx, C.byref(self._out)), self.ctx)
 
     def mc_field(self):
         p = self.params

@@ -801,6 +801,104 @@ extern "C" int mp_mc_download_field(void* ctx, float* dens, uint8_t* cube) {
     return MP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// per-frame files: the writers of host/export.cpp on the context's data
+// ---------------------------------------------------------------------------
+// runMC_solid / runMC_fluid / runMC_gas pass these object names (spray.cu:767-784)
+static const char* mc_object_name(int surface) {
+    return surface == MP_MC_SOLID ? "solid" : (surface == MP_MC_FLUID ? "water" : "gas");
+}
+static int io_error(MpCtx* c, int rc, const std::string& path) {
+    if (rc == MP_ERR_IO) c->err = "cannot open or write " + path;
+    else if (rc != MP_OK) c->err = "export: bad arguments for " + path;
+    return rc;
+}
+static int export_mesh(MpCtx* c, int surface, int format, const std::string& path) {
+    const McSurface& m = c->mc[surface];
+    std::vector<float> v(3 * (size_t)m.nverts), nrm(3 * (size_t)m.nverts);
+    std::vector<uint32_t> idx((size_t)m.nindices);
+    if (m.nverts) {
+        MP_CUDA(c, cudaMemcpyAsync(v.data(), m.verts, 12 * (size_t)m.nverts, cudaMemcpyDeviceToHost, c->stream));
+        MP_CUDA(c, cudaMemcpyAsync(nrm.data(), m.normals, 12 * (size_t)m.nverts, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (m.nindices)
+        MP_CUDA(c, cudaMemcpyAsync(idx.data(), m.indices, 4 * (size_t)m.nindices, cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return io_error(c, mp_write_mesh(format, path.c_str(), mc_object_name(surface), v.data(), nrm.data(), m.nverts,
+                                     idx.data(), m.nindices), path);
+}
+static int export_particles(MpCtx* c, int kind, const std::string& path, float tmin, float tmax) {
+    const int np = c->np();
+    std::vector<float> pos(3 * (size_t)np), T((size_t)np);
+    std::vector<int8_t> flag((size_t)np);
+    MP_TRY(k_unpack_particles(c, np, pos.data(), nullptr, flag.data(), nullptr, T.data(), nullptr, nullptr, nullptr));
+    return io_error(c, mp_write_particles(kind, path.c_str(), pos.data(), flag.data(), T.data(), np, tmin, tmax), path);
+}
+static std::string fmt_path(const char* f, const std::string& dir, const char* name, int frame) {
+    char buf[64];
+    if (name) std::snprintf(buf, sizeof(buf), f, name, frame);
+    else std::snprintf(buf, sizeof(buf), f, frame);
+    return dir + buf;
+}
+
+extern "C" int mp_export_mesh(void* ctx, int surface, int format, const char* path) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!path || surface < 0 || surface > 2 || format < MP_OUT_POV_MESH || format > MP_OUT_BOBJ_GZ) {
+        c->err = "export_mesh: bad arguments"; return MP_ERR_ARG;
+    }
+    if (!c->P.b_run_mc) { c->err = "export_mesh: marching cubes is off (b_run_mc)"; return MP_ERR_STATE; }
+    return export_mesh(c, surface, format, path);
+}
+extern "C" int mp_export_particles(void* ctx, int kind, const char* path, float t_min, float t_max) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!path || kind < MP_OUT_PARTICLES_COLORED || kind > MP_OUT_PARTICLES_AIR) {
+        c->err = "export_particles: bad arguments"; return MP_ERR_ARG;
+    }
+    return export_particles(c, kind, path, t_min, t_max);
+}
+extern "C" int mp_set_output(void* ctx, const mp_output* o) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!o) { c->out_on = false; return MP_OK; }
+    if (!o->dir) { c->err = "set_output: dir is null"; return MP_ERR_ARG; }
+    c->out_on = true;
+    c->out_dir = o->dir;
+    c->out_pov = o->pov; c->out_obj = o->obj; c->out_colored = o->colored_particles;
+    c->out_tmin = o->t_render_min; c->out_tmax = o->t_render_max;
+    return MP_OK;
+}
+
+// the meshes just extracted, as runMC_smooth writes them (spray.cu:858-863,
+// 954-958): POV-Ray mesh2 when pov; BOBJ when obj, or an empty OBJ for an
+// empty surface; in extraction order solid, water, gas
+static int step_output_meshes(MpCtx* c, int F) {
+    for (int s : {MP_MC_SOLID, MP_MC_FLUID, MP_MC_GAS}) {
+        const char* nm = mc_object_name(s);
+        const bool empty = c->mc[s].nverts == 0;
+        if (c->out_pov) MP_TRY(export_mesh(c, s, MP_OUT_POV_MESH, fmt_path("waterdata/%s%05d.pov", c->out_dir, nm, F)));
+        if (c->out_obj) {
+            if (empty) MP_TRY(export_mesh(c, s, MP_OUT_OBJ_MESH, fmt_path("waterOBJdata/%s%05d.obj", c->out_dir, nm, F)));
+            else MP_TRY(export_mesh(c, s, MP_OUT_BOBJ_GZ,
+                                    c->out_dir + nm + fmt_path("BOBJdata/fluidsurface_final_%04d.bobj.gz", "", nullptr, F - 1)));
+        }
+    }
+    return MP_OK;
+}
+// the particle files at the end of bubblesim (spray.cpp:1208-1216)
+static int step_output_particles(MpCtx* c, int F) {
+    if (!c->out_pov) return MP_OK;
+    const int sc = c->P.scene;
+    if (sc == MP_SCENE_INTERACTION)
+        MP_TRY(export_particles(c, MP_OUT_PARTICLES_SOLO, fmt_path("waterdata/solobubble%05d.pov", c->out_dir, nullptr, F),
+                                c->out_tmin, c->out_tmax));
+    if (c->out_colored)
+        MP_TRY(export_particles(c, MP_OUT_PARTICLES_COLORED,
+                                fmt_path("waterdata/allparticles%05d.pov", c->out_dir, nullptr, F), c->out_tmin, c->out_tmax));
+    if (sc == MP_SCENE_BOILING)
+        MP_TRY(export_particles(c, MP_OUT_PARTICLES_AIR, fmt_path("waterdata/solobubble%05d.pov", c->out_dir, nullptr, F),
+                                c->out_tmin, c->out_tmax));
+    return MP_OK;
+}
+
 // bubblesim (spray.cpp:979-1233): the stage order and cadence of the reference.
 // Scene-scripted flag toggles of SCENE_ALL / MELTANDBOIL / INTERACTION frames
 // (spray.cpp:1007-1047), pouring (spray.cpp:999-1002) and seed re-draws with
@@ -842,13 +940,22 @@ extern "C" int mp_step(void* ctx) {
     MP_TRY(k_hash_sort(c));
     if (P.b_melt) MP_TRY(k_melt(c));
     if (P.b_freeze) MP_TRY(k_freeze(c));
+    const bool out_frame = c->out_on && P.mc_every > 0 && c->S.frame % P.mc_every == 0;
     if (P.b_run_mc && P.mc_every > 0 && c->S.frame % P.mc_every == 0) {
         MP_TRY(k_mc_presort(c));
         MP_TRY(k_mc(c, MP_MC_SOLID));
         MP_TRY(k_mc_fluid_gas(c));
     }
+    // a file that cannot be written ends the step's output, not the step
+    // (the reference printed and paused); the frame still advances
+    int out_rc = MP_OK;
+    if (out_frame) {
+        const int F = c->S.frame / P.mc_every;
+        if (P.b_run_mc) out_rc = step_output_meshes(c, F);
+        if (out_rc == MP_OK) out_rc = step_output_particles(c, F);
+    }
     c->S.frame++;
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
     MP_CHECK_LAUNCH(c);
-    return warn;
+    return out_rc != MP_OK ? out_rc : warn;
 }

@@ -30,6 +30,12 @@ struct MpCtx {
     mpk::Grid G{};
     std::string err;
 
+    // per-frame files written by mp_step (mp_set_output)
+    bool out_on = false;
+    std::string out_dir;
+    int out_pov = 0, out_obj = 0, out_colored = 0;
+    float out_tmin = 0.0f, out_tmax = 1.0f;
+
     // cell fields
     float *press = 0, *divg = 0, *lsfluid = 0, *lsair = 0, *lsmerge = 0;
     float *phifluid = 0, *phiair = 0, *phisolid = 0;

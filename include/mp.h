@@ -42,6 +42,7 @@ extern "C" {
 #define MP_ERR_TIMEOUT     4   /* a bounded device-side wait gave up         */
 #define MP_ERR_ARG         5   /* bad argument (null, size, id)              */
 #define MP_ERR_STATE       6   /* call not valid in the current state        */
+#define MP_ERR_IO          7   /* an output file could not be opened/written */
 
 /* ---- particle / cell types (utility.h:13-19) ------------------------- */
 #define MP_TYPEFLUID    0
@@ -346,6 +347,59 @@ int mp_mc_download_field(void* ctx, float* dens, uint8_t* cubeindex);
  * (MP_F_SOLIDU*) are left as they were when no cell holds a SOLID particle:
  * the collision reads them only within half a cell of a solid. */
 int mp_step(void* ctx);
+
+/* ---- per-frame files (cspray::output*, spray.cu:2250-2526) --------------
+ * The reference's writers, byte for byte with its printf formats: an empty
+ * mesh gives an empty file, a vertex or normal with a NaN component is
+ * written as (0,0,0) (verifyfloat3, spray.cu:999), OBJ indices are 1-based,
+ * and the BOBJ face block is preceded by the number of indices (not of
+ * triangles). BOBJ is gzip at level 1 ("wb1"). A file that cannot be opened
+ * or written gives MP_ERR_IO (the reference printed and paused). */
+#define MP_OUT_POV_MESH  0   /* outputPovRaywater: POV-Ray mesh2   (spray.cu:2250) */
+#define MP_OUT_OBJ_MESH  1   /* outputOBJwater: Wavefront OBJ      (spray.cu:2308) */
+#define MP_OUT_BOBJ_GZ   2   /* outputBOBJwater: Blender .bobj.gz  (spray.cu:2373) */
+#define MP_OUT_PARTICLES_COLORED 0  /* outputColoredParticle: all particles,
+                                       coloured by temperature  (spray.cu:2440) */
+#define MP_OUT_PARTICLES_SOLO    1  /* outputSoloBubblePovRay: AIRSOLO (spray.cu:2468) */
+#define MP_OUT_PARTICLES_AIR     2  /* outputAirParticlePovRay: AIR    (spray.cu:2498) */
+
+/* One mesh from host arrays: float3 vertices and normals, uint32 indices
+ * (3 per triangle, each below nverts). object_name names the POV-Ray
+ * material (`<name>_material`). */
+int mp_write_mesh(int format, const char* path, const char* object_name, const float* verts,
+                  const float* normals, int nverts, const uint32_t* indices, int nindices);
+/* POV-Ray spheres from host arrays: float3 positions, int8 flags (SOLO/AIR
+ * kinds), temperatures (COLORED: colour of (T - t_min)/(t_max - t_min)*6
+ * on mapColorBlue2Red_h, spray.cpp:1299). */
+int mp_write_particles(int kind, const char* path, const float* pos, const int8_t* flag,
+                       const float* temperature, int n, float t_min, float t_max);
+/* The same writers on the context's data: the last extraction of `surface`
+ * (MP_MC_*), named "solid" / "water" / "gas" as runMC_solid / runMC_fluid /
+ * runMC_gas name it (spray.cu:767-784), and the current particles. */
+int mp_export_mesh(void* ctx, int surface, int format, const char* path);
+int mp_export_particles(void* ctx, int kind, const char* path, float t_min, float t_max);
+
+/* Per-frame output of bubblesim. With it set, every mp_step that extracts
+ * the meshes (frame % mc_every == 0, mc_every = outputframeDelta) writes, as
+ * runMC_smooth (spray.cu:954-958, 858-863) and bubblesim (spray.cpp:1208-1216) do,
+ * with F = frame / mc_every:
+ *   pov: <dir>waterdata/<name>%05d.pov per surface; the particle files
+ *        <dir>waterdata/allparticles%05d.pov (colored_particles),
+ *        <dir>waterdata/solobubble%05d.pov (AIRSOLO spheres in
+ *        MP_SCENE_INTERACTION, AIR spheres in MP_SCENE_BOILING);
+ *   obj: <dir><name>BOBJdata/fluidsurface_final_%04d.bobj.gz with F - 1,
+ *        or, for an empty surface, an empty <dir>waterOBJdata/<name>%05d.obj.
+ * `dir` is a prefix used as written (end it with '/'); the directories must
+ * exist, as in the reference. NULL turns the output off (the default). */
+typedef struct mp_output {
+    const char* dir;           /* outputdir                                */
+    int32_t pov;               /* boutputpovray                            */
+    int32_t obj;               /* boutputobj                               */
+    int32_t colored_particles; /* bOutputColoredParticle                   */
+    float   t_render_min;      /* temperatureMin_render                    */
+    float   t_render_max;      /* temperatureMax_render                    */
+} mp_output;
+int mp_set_output(void* ctx, const mp_output* out);
 
 /* ---- adjoint (no counterpart in the reference) -------------------------------
  * Reverse-mode derivative of the step for a scene of FLUID particles only,
