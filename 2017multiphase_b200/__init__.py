@@ -33,9 +33,16 @@ _ERR_NAMES = {1: "MP_ERR_CUDA", 2: "MP_ERR_CAPACITY", 3: "MP_ERR_NOCONVERGE", 4:
 # per-frame file formats and particle kinds (mp.h, cspray::output*)
 OUT_POV_MESH, OUT_OBJ_MESH, OUT_BOBJ_GZ = range(3)
 OUT_PARTICLES_COLORED, OUT_PARTICLES_SOLO, OUT_PARTICLES_AIR = range(3)
+# pouring emitter layouts (mp_scene_pour)
+POUR_FREEZING, POUR_INTERACTION, POUR_INTERACTION2 = range(3)
 
 # particle and cell types (utility.h:13-19)
 TYPEFLUID, TYPEAIR, TYPEBOUNDARY, TYPEVACUUM, TYPEAIRSOLO, TYPESOLID = range(6)
+# scenes (utility.h:114-131)
+(SCENE_FLUIDSPHERE, SCENE_SMOKE, SCENE_BOILING, SCENE_BOILING_HIGHRES, SCENE_MULTIBUBBLE, SCENE_DAMBREAK,
+ SCENE_MELTING, SCENE_MELTINGPOUR, SCENE_FREEZING, SCENE_INTERACTION, SCENE_INTERACTION_HIGHRES, SCENE_MELTANDBOIL,
+ SCENE_MELTANDBOIL_HIGHRES, SCENE_HEATTRANSFER) = range(14)
+SCENE_ALL = 15
 MC_SOLID, MC_FLUID, MC_GAS = 0, 1, 2
 PREC_MIXED, PREC_FP64 = 0, 1
 TOL_REF_ABS, TOL_REL = 0, 1
@@ -168,6 +175,8 @@ def load_library() -> C.CDLL:
         "mp_export_mesh": ([vp, C.c_int, C.c_int, C.c_char_p], C.c_int),
         "mp_export_particles": ([vp, C.c_int, C.c_char_p, C.c_float, C.c_float], C.c_int),
         "mp_set_output": ([vp, C.POINTER(MPOutput)], C.c_int),
+        "mp_scene_pour": ([C.c_int, C.c_float, C.c_float, vp, vp, vp, C.c_int, vp, vp, C.POINTER(C.c_int)], C.c_int),
+        "mp_set_pour": ([vp, vp, vp, C.c_int], C.c_int),
     }
     for nm, (args, res) in sig.items():
         f = getattr(lib, nm)
@@ -176,7 +185,7 @@ def load_library() -> C.CDLL:
     for nm in ["mp_hash_sort", "mp_external_force", "mp_sweep_ls_mark", "mp_mark_solo_air", "mp_surface_tension",
                "mp_markgrid_bubble", "mp_p2g", "mp_drag", "mp_g2p", "mp_solid_motion", "mp_solo_air_update",
                "mp_collide_advect", "mp_correct_pos", "mp_correct_pos_bubble", "mp_heat", "mp_gen_gas", "mp_delete",
-               "mp_melt", "mp_freeze", "mp_mc_presort", "mp_step"]:
+               "mp_melt", "mp_freeze", "mp_mc_presort", "mp_step", "mp_pour"]:
         f = getattr(lib, nm)
         f.argtypes = [vp]
         f.restype = C.c_int
@@ -277,6 +286,21 @@ def write_particles(kind: int, path: str, pos: np.ndarray, flag: Optional[np.nda
     T = None if temperature is None else np.ascontiguousarray(temperature, np.float32)
     _check(lib.mp_write_particles(kind, os.fsencode(path), _ptr(p3), _ptr(fl), _ptr(T), len(p3), t_min, t_max),
            None)
+
+
+def scene_pour(variant: int, samplespace: float, radius: float, center, vel, center2=None):
+    """The emitter points of CompPouringParam_* (mp_scene_pour): (pos, vel) float32 (n, 3)."""
+    lib = load_library()
+    c1 = np.ascontiguousarray(center, np.float32)
+    c2 = None if center2 is None else np.ascontiguousarray(center2, np.float32)
+    v = np.ascontiguousarray(vel, np.float32)
+    n = C.c_int()
+    _check(lib.mp_scene_pour(variant, samplespace, radius, _ptr(c1), _ptr(c2), _ptr(v), 0, None, None, C.byref(n)),
+           None)
+    pos = np.zeros((n.value, 3), np.float32); vel3 = np.zeros((n.value, 3), np.float32)
+    _check(lib.mp_scene_pour(variant, samplespace, radius, _ptr(c1), _ptr(c2), _ptr(v), n.value, _ptr(pos),
+                             _ptr(vel3), C.byref(n)), None)
+    return pos, vel3
 
 
 def mc_tables():
@@ -389,6 +413,11 @@ class Sim:
     def set_state(self, s: MPState):
         _check(self.lib.mp_set_state(self.ctx, C.byref(s)), self.ctx)
 
+    def get_params(self):
+        p = Params()
+        _check(self.lib.mp_get_params(self.ctx, C.byref(p)), self.ctx)
+        return p
+
     def set_params(self, p):
         _check(self.lib.mp_set_params(self.ctx, C.byref(p)), self.ctx)
         self.params = p
@@ -432,7 +461,11 @@ class Sim:
     def Freezing(self): return self._stage("mp_freeze")
     def preMC(self): return self._stage("mp_mc_presort")
     def runMC(self, surface): return self._stage("mp_mc", surface)
-    def bubblesim(self): return self._stage("mp_step", allow_noconverge=True)
+    def bubblesim(self):
+        rc = self._stage("mp_step", allow_noconverge=True)
+        # the frame-scripted switches of some scenes change the parameters
+        self.params = self.get_params()
+        return rc
     simstep = bubblesim
 
     def mc_mesh(self, surface: int):
@@ -441,6 +474,15 @@ class Sim:
         v = np.zeros((nv, 3), np.float32); nr = np.zeros((nv, 3), np.float32); ix = np.zeros(ni, np.uint32)
         _check(self.lib.mp_mc_download(self.ctx, surface, _ptr(v), _ptr(nr), _ptr(ix), nv, ni), self.ctx)
         return v, nr, ix
+
+    # ---- pouring (cspray::pouring / pouringgas) ------------------------------
+    def set_pour(self, pos: np.ndarray, vel: np.ndarray):
+        """The emitter (dpourpos / dpourvel) the step pours from (mp_set_pour)."""
+        p3 = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        v3 = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        _check(self.lib.mp_set_pour(self.ctx, _ptr(p3), _ptr(v3), len(p3)), self.ctx)
+
+    def pouring(self): return self._stage("mp_pour")
 
     # ---- per-frame files (cspray::output*) ----------------------------------
     def export_mesh(self, surface: int, fmt: int, path: str):

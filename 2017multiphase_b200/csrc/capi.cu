@@ -40,7 +40,8 @@ static const ParamField kParamFields[] = {
     PF_F(solubility_coef), PF_F(solid_bounce_param), PF_F(flip_alpha), PF_I(cg_tol_mode), PF_F(cg_tol),
     PF_I(cg_max_iter), PF_I(heat_cg_max_iter), PF_I(cg_true_residual_every), PF_I(precision),
     PF_I(coef_mode), PF_F(density_ratio), PF_I(mc_max_verts), PF_I(mc_max_tris), PF_I(seed_redraw),
-    PF_I(update_seed_frame_delta), PF_I(b_fixed_heat),
+    PF_I(update_seed_frame_delta), PF_I(b_fixed_heat), PF_F(pos_rand_param), PF_F(vel_rand_param),
+    PF_I(begin_frame), PF_I(b_run_mc_solid),
 };
 
 extern "C" int mp_params_size(void) { return (int)sizeof(mp_params); }
@@ -110,6 +111,9 @@ extern "C" int mp_params_default(mp_params* p, int nx, int ny, int nz, int par_n
     p->mc_max_verts = (int)mv; p->mc_max_tris = (int)std::min(2 * mv, 128000000LL);
     p->seed_redraw = 0; p->update_seed_frame_delta = 15;
     p->b_fixed_heat = 0;
+    p->pos_rand_param = 0.1f; p->vel_rand_param = 0.0f;   // spray.cpp:55
+    p->begin_frame = 0;                                   // spray.cpp:73
+    p->b_run_mc_solid = 1;                                // spray.cpp:63
     return mp_params_derive(p);
 }
 
@@ -136,7 +140,7 @@ static void free_all(MpCtx* c) {
                     c->flag_snap, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->scan_tmp, c->u32_scratch,
                     c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_dens2, c->gfm_beta, c->gfm_s, c->mc_cube, c->mc_vflag, c->mc_vscan,
                     c->mc_compact, c->mc_vverts, c->mc_vvscan, c->mc_emark, c->mc_escan, c->mc_vstart, c->mc_inc,
-                    c->mc_fill, c->mc_tmpv};
+                    c->mc_fill, c->mc_tmpv, c->pour_pos, c->pour_vel};
     k_adj_free(c);
     for (void* p : ptrs) if (p) cudaFree(p);
     for (int a = 0; a < 3; a++) {
@@ -802,6 +806,54 @@ extern "C" int mp_mc_download_field(void* ctx, float* dens, uint8_t* cube) {
 }
 
 // ---------------------------------------------------------------------------
+// pouring emitters (dpourpos / dpourvel, spray.cpp:1416-1545; spray.cu:3012-3043)
+// ---------------------------------------------------------------------------
+extern "C" int mp_set_pour(void* ctx, const float* pos3, const float* vel3, int n) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (n < 0 || (n > 0 && (!pos3 || !vel3))) { c->err = "set_pour: bad arguments"; return MP_ERR_ARG; }
+    if (n > c->pour_n) {
+        if (c->pour_pos) cudaFree(c->pour_pos);
+        if (c->pour_vel) cudaFree(c->pour_vel);
+        c->pour_pos = c->pour_vel = nullptr; c->pour_n = 0;
+        MP_TRY(dalloc_t(c, &c->pour_pos, 3 * (size_t)n));
+        MP_TRY(dalloc_t(c, &c->pour_vel, 3 * (size_t)n));
+    }
+    if (n > 0) {
+        MP_CUDA(c, cudaMemcpyAsync(c->pour_pos, pos3, 12 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        MP_CUDA(c, cudaMemcpyAsync(c->pour_vel, vel3, 12 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    c->pour_n = n;
+    return MP_OK;
+}
+extern "C" int mp_pour(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    return k_pour(c);
+}
+
+// the frame-scripted switches of bubblesim (spray.cpp:1007-1047), applied to
+// the context's parameters at the start of the step
+static void scene_toggles(MpCtx* c) {
+    mp_params& P = c->P;
+    const int sc = P.scene, f = c->S.frame;
+    if (sc == MP_SCENE_ALL && f == 0) {
+        P.b_fix_solid = 0; P.b_add_heat_bottom = 0; P.b_gen_gas = 0; P.b_melt = 0;
+        P.b_freeze = 1;
+    }
+    if (sc == MP_SCENE_ALL && f == 500) P.b_freeze = 0;
+    if (sc == MP_SCENE_ALL && f == 520) { P.b_add_heat_bottom = 1; P.b_melt = 1; }
+    if (sc == MP_SCENE_ALL && f == 1250) P.b_gen_gas = 1;
+    if ((sc == MP_SCENE_MELTANDBOIL || sc == MP_SCENE_MELTANDBOIL_HIGHRES) && f == 300) P.b_fix_solid = 0;
+    if (sc == MP_SCENE_MELTANDBOIL_HIGHRES && f == 400) P.b_add_heat_bottom = 0;
+    if (sc == MP_SCENE_MELTANDBOIL_HIGHRES && f == 700) P.b_add_heat_bottom = 1;
+    if (sc == MP_SCENE_MELTANDBOIL && f == 400) P.b_gen_gas = !P.b_gen_gas;
+    if (sc == MP_SCENE_MELTANDBOIL && f == 700) {
+        P.b_gen_gas = !P.b_gen_gas; P.drag_param_grid = 0.03f; P.vapor_gen_rate = 0.005f;
+    }
+    if ((sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES) && f == P.begin_frame) P.b_fix_solid = 0;
+}
+
+// ---------------------------------------------------------------------------
 // per-frame files: the writers of host/export.cpp on the context's data
 // ---------------------------------------------------------------------------
 // runMC_solid / runMC_fluid / runMC_gas pass these object names (spray.cu:767-784)
@@ -899,15 +951,17 @@ static int step_output_particles(MpCtx* c, int F) {
     return MP_OK;
 }
 
-// bubblesim (spray.cpp:979-1233): the stage order and cadence of the reference.
-// Scene-scripted flag toggles of SCENE_ALL / MELTANDBOIL / INTERACTION frames
-// (spray.cpp:1007-1047), pouring (spray.cpp:999-1002) and seed re-draws with
-// the host rand() are not part of this step.
+// bubblesim (spray.cpp:979-1233): the stage order and cadence of the reference,
+// starting with pouring (spray.cpp:998-1001) and the frame-scripted switches
+// (spray.cpp:1007-1047). Seed re-draws with the host rand() are not part of
+// this step.
 extern "C" int mp_step(void* ctx) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     const mp_params& P = c->P;
     int sc = P.scene;
     int warn = MP_OK, st;
+    MP_TRY(k_pour(c));
+    scene_toggles(c);
     MP_TRY(k_hash_sort(c));
     MP_TRY(k_external_force(c));
     MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
@@ -943,7 +997,13 @@ extern "C" int mp_step(void* ctx) {
     const bool out_frame = c->out_on && P.mc_every > 0 && c->S.frame % P.mc_every == 0;
     if (P.b_run_mc && P.mc_every > 0 && c->S.frame % P.mc_every == 0) {
         MP_TRY(k_mc_presort(c));
-        MP_TRY(k_mc(c, MP_MC_SOLID));
+        // runMC_interaction (spray.cu:788-802): with bRunMCSolid off the solid
+        // surface of frame 0 is kept, moved by the solid motion, and only its
+        // normals are recomputed
+        const bool inter = sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES ||
+                           sc == MP_SCENE_MELTANDBOIL || sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL;
+        if (inter && c->S.frame > 0 && !P.b_run_mc_solid) MP_TRY(k_mc_renormal(c, MP_MC_SOLID));
+        else MP_TRY(k_mc(c, MP_MC_SOLID));
         MP_TRY(k_mc_fluid_gas(c));
     }
     // a file that cannot be written ends the step's output, not the step

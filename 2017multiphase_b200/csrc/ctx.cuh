@@ -71,6 +71,7 @@ struct MpCtx {
     uint32_t *u32_scratch = 0;   // small device counters
     // tables
     float *randf = 0; int nrand = 0;
+    float *pour_pos = 0, *pour_vel = 0; int pour_n = 0;   // emitter (dpourpos / dpourvel), float3 each
     int32_t *seeds = 0; int nseed = 0;
     int32_t *mc_numverts = 0, *mc_tri = 0;
     // marching cubes
@@ -159,6 +160,8 @@ int k_set_boundary_u(MpCtx* c, int phase);
 int k_project(MpCtx* c, int* iters, double* res);
 int k_g2p(MpCtx* c);
 int k_solid_motion(MpCtx* c);
+int k_pour(MpCtx* c);
+int k_mc_renormal(MpCtx* c, int surface);
 int k_solo_air_update(MpCtx* c);
 int k_collide_advect(MpCtx* c, bool skip_empty_solid = false);
 int k_correct_pos(MpCtx* c);

@@ -270,3 +270,34 @@ extern "C" int mp_scene_fixed_heat(const mp_params* p, int config, float* fh) {
             }
     return MP_OK;
 }
+
+// CompPouringParam_Freezing / _Ineraction / _Ineraction2 (spray.cpp:1416-1545):
+// the emitter disc(s) as a square lattice in the xy plane, points farther
+// than `radius` from the centre dropped; float arithmetic as the reference's
+// host code (ipos = centre + (x*ss, y*ss, 0), length(ipos - centre))
+extern "C" int mp_scene_pour(int variant, float samplespace, float radius, const float* center, const float* center2,
+                             const float* vel, int cap, float* pos3, float* vel3, int* n) {
+    if (!center || !vel || !n || cap < 0 || samplespace <= 0 || radius < 0) return MP_ERR_ARG;
+    if (variant == MP_POUR_INTERACTION2 && !center2) return MP_ERR_ARG;
+    if (variant < MP_POUR_FREEZING || variant > MP_POUR_INTERACTION2) return MP_ERR_ARG;
+    const float ss = variant == MP_POUR_FREEZING ? samplespace : samplespace * 2.0f;
+    const int num = variant == MP_POUR_FREEZING ? (int)(radius / samplespace) * 3 : (int)(radius / ss);
+    int cnt = 0;
+    auto disc = [&](const float* c) {
+        for (int x = -num; x <= num; x++)
+            for (int y = -num; y <= num; y++) {
+                float px = c[0] + (float)x * ss, py = c[1] + (float)y * ss, pz = c[2] + 0.0f;
+                float dx = px - c[0], dy = py - c[1], dz = pz - c[2];
+                if (sqrtf(dx * dx + dy * dy + dz * dz) > radius) continue;
+                if (cnt < cap) {
+                    if (pos3) { pos3[3 * cnt] = px; pos3[3 * cnt + 1] = py; pos3[3 * cnt + 2] = pz; }
+                    if (vel3) { vel3[3 * cnt] = vel[0]; vel3[3 * cnt + 1] = vel[1]; vel3[3 * cnt + 2] = vel[2]; }
+                }
+                cnt++;
+            }
+    };
+    disc(center);
+    if (variant == MP_POUR_INTERACTION2) disc(center2);
+    *n = cnt;
+    return MP_OK;
+}

@@ -420,6 +420,35 @@ int k_mc_fluid_gas(MpCtx* c) {
     return mc_extract(c, m, MP_MC_GAS, c->mc_dens2);
 }
 
+// incidence lists of a surface's vertices (vstart: nv+1, inc: nidx), each
+// list ascending
+static int mc_incidence(MpCtx* c, const McSurface& out, uint32_t nv, uint32_t nidx) {
+    cudaStream_t s = c->stream;
+    MP_CUDA(c, cudaMemsetAsync(c->mc_fill, 0, sizeof(uint32_t) * (nv + 1), s));
+    k_mc_inc_count<<<mp_blocks(nidx, 256), 256, 0, s>>>(nidx, out.indices, c->mc_fill);
+    c->launches++;
+    MP_TRY(mp_scan_u32(c, c->mc_fill, c->mc_vstart, nv));
+    k_mc_inc_fill<<<mp_blocks(nidx, 256), 256, 0, s>>>(nidx, out.indices, c->mc_vstart, c->mc_fill, c->mc_inc);
+    k_mc_inc_sort<<<mp_blocks(nv, 256), 256, 0, s>>>(nv, c->mc_vstart, c->mc_inc);
+    c->launches += 2;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+// runMC_interaction's stored-surface branch (spray.cu:788-794): calNormals
+// on the surface as it stands (moved by the solid motion), no re-extraction
+int k_mc_renormal(MpCtx* c, int surface) {
+    McSurface& out = c->mc[surface];
+    const uint32_t nv = (uint32_t)out.nverts, nidx = (uint32_t)out.nindices;
+    if (nv == 0) return MP_OK;
+    MP_TRY(mc_incidence(c, out, nv, nidx));
+    k_mc_normals<<<mp_blocks(nv, 256), 256, 0, c->stream>>>(nv, c->mc_vstart, c->mc_inc, out.indices, out.verts,
+                                                              out.normals);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
 // classification, compaction, vertices, indices, smoothing and normals of one
 // surface from its nodal field
 static int mc_extract(MpCtx* c, const McGrid& m, int surface, const float* dens) {
@@ -459,15 +488,7 @@ static int mc_extract(MpCtx* c, const McGrid& m, int surface, const float* dens)
                                                       c->mc_tri, c->mc_escan, out.indices);
     c->launches += 2;
     MP_CHECK_LAUNCH(c);
-    // incidence lists (vstart: nv+1, inc: nidx)
-    MP_CUDA(c, cudaMemsetAsync(c->mc_fill, 0, sizeof(uint32_t) * (nv + 1), s));
-    k_mc_inc_count<<<mp_blocks(nidx, 256), 256, 0, s>>>(nidx, out.indices, c->mc_fill);
-    c->launches++;
-    MP_TRY(mp_scan_u32(c, c->mc_fill, c->mc_vstart, nv));
-    k_mc_inc_fill<<<mp_blocks(nidx, 256), 256, 0, s>>>(nidx, out.indices, c->mc_vstart, c->mc_fill, c->mc_inc);
-    k_mc_inc_sort<<<mp_blocks(nv, 256), 256, 0, s>>>(nv, c->mc_vstart, c->mc_inc);
-    c->launches += 2;
-    MP_CHECK_LAUNCH(c);
+    MP_TRY(mc_incidence(c, out, nv, nidx));
     if (c->P.b_smooth_mc) {
         for (int it = 0; it < c->P.smooth_iters; it++) {
             k_mc_smooth<<<mp_blocks(nv, 256), 256, 0, s>>>(nv, c->mc_vstart, c->mc_inc, out.indices, out.verts, c->mc_tmpv);

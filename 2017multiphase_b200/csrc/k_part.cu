@@ -504,6 +504,39 @@ __global__ void k_solid_move(int np, float4* __restrict__ pos, float4* __restric
     }
 }
 
+// computeSolidVertex_k (spray_k.cu:5254-5263): the stored solid surface moves
+// with the rigid motion of the solid particles (transposeParticle as above)
+__global__ void k_solid_vertex(int nv, float3* __restrict__ vtx, float3 rg0, float3 rg, Mat3 rm) {
+    MP_GRID_LOOP(v, nv) {
+        float3 t = vtx[v] - rg0;
+        const float* m = rm.m;
+        float3 r2 = mk3(t.x * m[0] + t.y * m[3] + t.z * m[6], t.x * m[1] + t.y * m[4] + t.z * m[7],
+                        t.x * m[2] + t.y * m[5] + t.z * m[8]);
+        vtx[v] = r2 + rg;
+    }
+}
+
+// pouringwater (spray_k.cu:5575-5596): emitter point idx appends particle
+// np + idx with jitter from the random table. The callers pass frame 0, so
+// the table offset is idx % (nrand - 6). The reference leaves the slot's
+// solubility as it was; here it is 0 (updatesolubility sets it before use).
+__global__ void k_pour_particles(int n, int np, const float* __restrict__ ppos, const float* __restrict__ pvel,
+                                 const float* __restrict__ rf, int nrand, float4* __restrict__ pos,
+                                 float4* __restrict__ vel, float4* __restrict__ heat, int flag, float posrand,
+                                 float velrand, float samplespace, float m0, float T, float L) {
+    MP_GRID_LOOP(idx, n) {
+        int rb = (0 + idx) % (nrand - 6);
+        float3 rv = mk3(rf[rb] * 2.0f - 1.0f, rf[rb + 1] * 2.0f - 1.0f, rf[rb + 2] * 2.0f - 1.0f);
+        rb += 3;
+        float3 rp = mk3(rf[rb] * 2.0f - 1.0f, rf[rb + 1] * 2.0f - 1.0f, rf[rb + 2] * 2.0f - 1.0f);
+        float3 p = mk3(ppos[3 * idx], ppos[3 * idx + 1], ppos[3 * idx + 2]) + rp * posrand * samplespace;
+        float3 v = mk3(pvel[3 * idx], pvel[3 * idx + 1], pvel[3 * idx + 2]) + rv * velrand;
+        pos[np + idx] = make_float4(p.x, p.y, p.z, flagbits(flag));
+        vel[np + idx] = make_float4(v.x, v.y, v.z, m0);
+        heat[np + idx] = make_float4(T, L, 0.0f, 0.0f);
+    }
+}
+
 // ---- heat / phase change -----------------------------------------------------
 __global__ void k_latent(int np, const float4* __restrict__ pos, float4* __restrict__ heat, float mp, float bp, float lth) {
     MP_GRID_LOOP(p, np) {
@@ -869,6 +902,37 @@ int k_solid_motion(MpCtx* c) {
     k_solid_move<<<PB(np)>>>(np, c->pos, c->vel, rg0, rg, R, T, rm);
     c->launches++;
     MP_CHECK_LAUNCH(c);
+    // the solid surface extracted once (bRunMCSolid off) follows the same motion
+    const int sc = P.scene;
+    const McSurface& sm = c->mc[MP_MC_SOLID];
+    if ((sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES || sc == MP_SCENE_MELTANDBOIL ||
+         sc == MP_SCENE_MELTANDBOIL_HIGHRES) && c->S.frame > 0 && !P.b_run_mc_solid && P.b_run_mc && sm.nverts > 0) {
+        k_solid_vertex<<<mp_blocks(sm.nverts, 256), 256, 0, c->stream>>>(sm.nverts, sm.verts, rg0, rg, rm);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+    }
+    return MP_OK;
+}
+
+// pouring / pouringgas (spray.cu:3012-3043): water every 4th frame; in the
+// interaction scenes from begin_frame on, AIRSOLO gas every 6th frame; only
+// when the emitter's points fit under par_num_max
+int k_pour(MpCtx* c) {
+    const mp_params& P = c->P;
+    const int sc = P.scene, frame = c->S.frame;
+    const bool gas = (sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES) && frame >= P.begin_frame;
+    const int every = gas ? 6 : 4;
+    const int n = c->pour_n, np = c->np();
+    if (frame % every != 0 || n == 0 || (long long)n + np > P.par_num_max) return MP_OK;
+    if (c->nrand <= 6) { c->err = "pour: random table not set"; return MP_ERR_STATE; }
+    k_pour_particles<<<mp_blocks(n, 256), 256, 0, c->stream>>>(
+        n, np, c->pour_pos, c->pour_vel, c->randf, c->nrand, c->pos, c->vel, c->heat,
+        gas ? MP_TYPEAIRSOLO : MP_TYPEFLUID, P.pos_rand_param, P.vel_rand_param, P.samplespace, P.m0,
+        P.default_liquid_T, P.liquid_heat_th);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    c->S.par_num_now = np + n;
+    c->mc_sorted = 0;
     return MP_OK;
 }
 

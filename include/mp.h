@@ -79,7 +79,7 @@ extern "C" {
 #define MP_COEF_REF      0   /* constant-coefficient Laplacian (reference)    */
 #define MP_COEF_GFM      1   /* variable density, ghost-fluid face weights (extension; MP_PREC_MIXED only) */
 
-#define MP_PARAMS_VERSION 3
+#define MP_PARAMS_VERSION 4
 
 /*
  * Runtime parameters: the reference's FlipConstant (utility.h:26-46), the
@@ -137,7 +137,13 @@ typedef struct mp_params {
      * at it, the reference's dormant Dirichlet path (compb_heat,
      * spray_k.cu:4515-4519, updateFixedHeat spray_k.cu:4478) */
     int32_t b_fixed_heat;
-    int32_t reserved[7];
+    /* pouring emitters and the interaction scenes (spray.h:94, 138, 357) */
+    float   pos_rand_param;          /* posrandparam: emitter position jitter, samplespace units */
+    float   vel_rand_param;          /* velrandparam: emitter velocity jitter                   */
+    int32_t begin_frame;             /* m_beginFrame: first gas-pouring / solid-release frame   */
+    int32_t b_run_mc_solid;          /* bRunMCSolid: 0 = extract the solid surface once, then
+                                        move it with the rigid solid motion                     */
+    int32_t reserved[3];
 } mp_params;
 
 #define MP_UNDEF_TEMPERATURE (-10000.0f)   /* utility.h:24 */
@@ -342,8 +348,38 @@ int mp_mc_download(void* ctx, int surface, float* verts, float* normals,
  * (uint8[8n]) of the last extraction. */
 int mp_mc_download_field(void* ctx, float* dens, uint8_t* cubeindex);
 
+/* ---- pouring emitters (spray.cpp:1416-1545, spray.cu:3012-3043) ---------
+ * The emitter is a set of points with a velocity each (dpourpos /
+ * dpourvel). mp_scene_pour lays one out as the scene set-up does:
+ * MP_POUR_FREEZING = CompPouringParam_Freezing (disc of radius `radius` at
+ * `center`, samplespace spacing); MP_POUR_INTERACTION = CompPouringParam_
+ * Ineraction (2 x samplespace spacing); MP_POUR_INTERACTION2 = _Ineraction2
+ * (two such discs, at `center` and `center2`). All points get `vel`. It writes
+ * at most `cap` points (pos3/vel3 may be NULL to count) and sets *n to the
+ * number of points of the emitter; host code only. */
+#define MP_POUR_FREEZING      0
+#define MP_POUR_INTERACTION   1
+#define MP_POUR_INTERACTION2  2
+int mp_scene_pour(int variant, float samplespace, float radius, const float* center, const float* center2,
+                  const float* vel, int cap, float* pos3, float* vel3, int* n);
+/* Sets the context's emitter (copied); n = 0 removes it. */
+int mp_set_pour(void* ctx, const float* pos3, const float* vel3, int n);
+/* pouring / pouringgas: appends the emitter's n particles (pouringwater,
+ * spray_k.cu:5575-5596: position jitter pos_rand_param * samplespace, velocity
+ * jitter vel_rand_param, both from the random table) as FLUID every 4th frame
+ * or, in MP_SCENE_INTERACTION(_HIGHRES) from begin_frame on, as AIRSOLO every
+ * 6th frame; nothing when they would exceed par_num_max. mp_step calls it
+ * first. */
+int mp_pour(void* ctx);
+
 /* The whole bubblesim step in the reference's order and cadence
- * (spray.cpp:979-1233). Synchronous at exit. Its solid-velocity faces
+ * (spray.cpp:979-1233): pouring, the frame-scripted parameter switches of
+ * MP_SCENE_ALL / MELTANDBOIL(_HIGHRES) / INTERACTION(_HIGHRES)
+ * (spray.cpp:1007-1047; they change the context's parameters, as
+ * mp_get_params shows), then the stages. In those scenes with
+ * b_run_mc_solid = 0 the solid surface is extracted at frame 0 only, moved
+ * with the rigid solid motion (computeSolidVertex_k) and re-normalled
+ * (runMC_interaction). Synchronous at exit. Its solid-velocity faces
  * (MP_F_SOLIDU*) are left as they were when no cell holds a SOLID particle:
  * the collision reads them only within half a cell of a solid. */
 int mp_step(void* ctx);

@@ -68,7 +68,7 @@ def test_state_struct_size(mp):
 
 def test_params_default_and_derive(mp):
     p = mp.default_params(64, 64, 64, 1000)
-    assert p.version == 3 and p.nx == 64 and abs(p.cellsize - 1 / 64) < 1e-9
+    assert p.version == 4 and p.nx == 64 and abs(p.cellsize - 1 / 64) < 1e-9
     # spray.cpp:573-588: m0 = waterrho / (1/samplespace)^3, airm0 = m0
     assert abs(p.m0 - 1000.0 * (0.5 / 64) ** 3) < 1e-9 and p.airm0 == p.m0
     assert p.cg_max_iter == 800 and p.heat_cg_max_iter == 3800 and p.heat_clamp == 378.0
