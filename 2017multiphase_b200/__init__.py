@@ -185,7 +185,8 @@ def load_library() -> C.CDLL:
     for nm in ["mp_hash_sort", "mp_external_force", "mp_sweep_ls_mark", "mp_mark_solo_air", "mp_surface_tension",
                "mp_markgrid_bubble", "mp_p2g", "mp_drag", "mp_g2p", "mp_solid_motion", "mp_solo_air_update",
                "mp_collide_advect", "mp_correct_pos", "mp_correct_pos_bubble", "mp_heat", "mp_gen_gas", "mp_delete",
-               "mp_melt", "mp_freeze", "mp_mc_presort", "mp_step", "mp_pour"]:
+               "mp_melt", "mp_freeze", "mp_mc_presort", "mp_step", "mp_pour", "mp_heatsim",
+               "mp_init_heat_grid"]:
         f = getattr(lib, nm)
         f.argtypes = [vp]
         f.restype = C.c_int
@@ -483,6 +484,10 @@ class Sim:
         _check(self.lib.mp_set_pour(self.ctx, _ptr(p3), _ptr(v3), len(p3)), self.ctx)
 
     def pouring(self): return self._stage("mp_pour")
+
+    # ---- heat-only mode (SIMULATION_HEATONLY) --------------------------------
+    def initheat_grid(self): return self._stage("mp_init_heat_grid")
+    def heatsim(self): return self._stage("mp_heatsim", allow_noconverge=True)
 
     # ---- per-frame files (cspray::output*) ----------------------------------
     def export_mesh(self, surface: int, fmt: int, path: str):

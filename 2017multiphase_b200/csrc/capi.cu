@@ -826,6 +826,14 @@ extern "C" int mp_set_pour(void* ctx, const float* pos3, const float* vel3, int 
     c->pour_n = n;
     return MP_OK;
 }
+extern "C" int mp_heatsim(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    return k_heatsim(c);
+}
+extern "C" int mp_init_heat_grid(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    return k_init_heat_grid_launch(c);
+}
 extern "C" int mp_pour(void* ctx) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     return k_pour(c);

@@ -161,6 +161,8 @@ int k_project(MpCtx* c, int* iters, double* res);
 int k_g2p(MpCtx* c);
 int k_solid_motion(MpCtx* c);
 int k_pour(MpCtx* c);
+int k_heatsim(MpCtx* c);
+int k_init_heat_grid_launch(MpCtx* c);
 int k_mc_renormal(MpCtx* c, int surface);
 int k_solo_air_update(MpCtx* c);
 int k_collide_advect(MpCtx* c, bool skip_empty_solid = false);

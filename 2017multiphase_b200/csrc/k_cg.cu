@@ -967,15 +967,12 @@ int k_heat_g2p_launch(MpCtx* c);
 int k_latent_heat(MpCtx* c);
 
 // updateTemperature (spray.cu:1889-1947)
-int k_heat(MpCtx* c) {
+// compb_heat, solver_cg_heat and setBoundaryHeat (spray.cu:1780-1852): the
+// implicit diffusion of Tp, Tp_save keeping the field before it
+static int heat_solve(MpCtx* c) {
     const Grid& g = c->G;
     const mp_params& P = c->P;
     int nb = mp_blocks(g.n, 256);
-    MP_TRY(k_heat_p2g_launch(c));
-    if (P.b_add_heat_bottom) {
-        k_heat_bottom<<<nb, 256, 0, c->stream>>>(g, c->Tp, P.heat_increase_bottom, P.heat_clamp);
-        c->launches++;
-    }
     HeatOp op;
     op.g = g; op.mark = c->mark; op.dt = P.dt;
     op.alpha[MP_TYPEFLUID] = P.heatalpha_fluid; op.alpha[MP_TYPEAIR] = P.heatalpha_air;
@@ -999,12 +996,64 @@ int k_heat(MpCtx* c) {
         c->launches++;
         std::swap(c->Tp, c->cell_tmp);
     }
+    MP_CHECK_LAUNCH(c);
+    return rc;
+}
+
+int k_heat(MpCtx* c) {
+    const Grid& g = c->G;
+    const mp_params& P = c->P;
+    int nb = mp_blocks(g.n, 256);
+    MP_TRY(k_heat_p2g_launch(c));
+    if (P.b_add_heat_bottom) {
+        k_heat_bottom<<<nb, 256, 0, c->stream>>>(g, c->Tp, P.heat_increase_bottom, P.heat_clamp);
+        c->launches++;
+    }
+    const int rc = heat_solve(c);
+    if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
     k_tp_change<<<nb, 256, 0, c->stream>>>(g.n, c->Tp, c->Tp_save, c->mark);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     MP_TRY(k_heat_g2p_launch(c));
     MP_TRY(k_latent_heat(c));
     return rc;
+}
+
+// heatsim (spray.cu:1959-1987): the grid-only heat step of SIMULATION_HEATONLY
+int k_heatsim(MpCtx* c) {
+    const int rc = heat_solve(c);
+    if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+    c->S.frame++;
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+namespace {
+// initheat_grid_k (spray_k.cu:5603-5621) then markBoundaryCell: in each
+// xz-section, a hot SOLID disc (100) and a cold FLUID disc (0) of radius
+// 0.15 NX, VACUUM (20) below NZ/2 and AIR (80) above
+__global__ void k_init_heat_grid(Grid g, float* __restrict__ tp, int8_t* __restrict__ mark) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        float x = (float)i, z = (float)k;
+        const float r = (float)(g.NX * 0.15);
+        float a = x - (float)(g.NX / 4), b = z - (float)(g.NZ / 4);
+        float a2 = x - (float)(g.NX / 4 * 3), b2 = z - (float)(g.NZ / 4 * 3);
+        if (sqrtf(a * a + b * b) <= r) { tp[idx] = 100; mark[idx] = MP_TYPESOLID; }
+        else if (sqrtf(a2 * a2 + b2 * b2) <= r) { tp[idx] = 0; mark[idx] = MP_TYPEFLUID; }
+        else if (z < (float)(g.NZ / 2)) { tp[idx] = 20; mark[idx] = MP_TYPEVACUUM; }
+        else { tp[idx] = 80; mark[idx] = MP_TYPEAIR; }
+        if (i == 0 || i == g.NX - 1 || j == 0 || j == g.NY - 1 || k == 0 || k == g.NZ - 1) mark[idx] = MP_TYPEBOUNDARY;
+    }
+}
+}  // namespace
+
+int k_init_heat_grid_launch(MpCtx* c) {
+    k_init_heat_grid<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, c->Tp, c->mark);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -372,6 +372,19 @@ int mp_set_pour(void* ctx, const float* pos3, const float* vel3, int n);
  * first. */
 int mp_pour(void* ctx);
 
+/* ---- heat-only mode (SIMULATION_HEATONLY, MP_SCENE_HEATTRANSFER) --------
+ * mp_init_heat_grid: initheat_grid (spray.cu:1949-1955): in every xz-section
+ * a SOLID disc at 100 and a FLUID disc at 0 (radius 0.15 nx, centres at
+ * (nx/4, nz/4) and (3nx/4, 3nz/4)), VACUUM at 20 below nz/2, AIR at 80
+ * above, and the outer shell BOUNDARY; it sets MP_F_TP and MP_F_MARK.
+ * mp_heatsim: heatsim (spray.cu:1959-1987): one implicit diffusion step of
+ * the cell temperatures (compb_heat, the heat CG, setBoundaryHeat when
+ * b_extend_heat_to_boundary), with the cell marks as they are and no
+ * particles; advances the frame. The reference's scene uses heatalpha
+ * fluid 0.0001, air 0.005, solid 0.015, vacuum 0.05 (spray.cpp:531-546). */
+int mp_init_heat_grid(void* ctx);
+int mp_heatsim(void* ctx);
+
 /* The whole bubblesim step in the reference's order and cadence
  * (spray.cpp:979-1233): pouring, the frame-scripted parameter switches of
  * MP_SCENE_ALL / MELTANDBOIL(_HIGHRES) / INTERACTION(_HIGHRES)

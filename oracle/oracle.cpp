@@ -1344,6 +1344,34 @@ struct Oracle {
                 Tp[idx] = fminf(P.heat_clamp, Tp[idx]);
             }
         }
+        bool capped = heat_solve();
+        #pragma omp parallel for
+        for (int idx = 0; idx < n; idx++)     // compTpChange (spray_k.cu:4607-4617)
+            Tp_save[idx] = (mark[idx] != TB) ? Tp[idx] - Tp_save[idx] : 0;
+        bool mab = P.scene == MP_SCENE_MELTANDBOIL || P.scene == MP_SCENE_MELTANDBOIL_HIGHRES || P.scene == MP_SCENE_ALL;
+        float a = P.alpha_temp_trans;
+        #pragma omp parallel for
+        for (int p = 0; p < np; p++) {   // mapHeatg2p[_MeltAndBoil] (spray_k.cu:4655-4679)
+            F3 ip = pos[p];
+            float nt = a * (T[p] + scaleFromGrid(ip, Tp_save)) + (1 - a) * scaleFromGrid(ip, Tp);
+            if (mab && flag[p] == TSOL) T[p] = 0.95f * (T[p]) + 0.05f * nt;
+            else T[p] = nt;
+        }
+        float mp_ = P.melting_point, bp = P.boiling_point, lth = P.liquid_heat_th;
+        #pragma omp parallel for
+        for (int p = 0; p < np; p++) {   // updateLatentHeat_k (spray_k.cu:5546-5573)
+            if (flag[p] == TSOL && T[p] > mp_) { L[p] += T[p] - mp_; T[p] = mp_; }
+            if (flag[p] == TF) {
+                if (T[p] < mp_) { L[p] -= mp_ - T[p]; T[p] = mp_; }
+                else if (T[p] > bp) { L[p] += T[p] - bp; T[p] = bp; }
+                else L[p] = lth;
+            }
+        }
+        return capped ? MP_ERR_NOCONVERGE : MP_OK;
+    }
+    // compb_heat, solver_cg_heat, setBoundaryHeat (spray.cu:1780-1852); true
+    // when the CG stopped at its cap
+    bool heat_solve() {
         Tp_save = Tp;
         float at[MP_TYPECNT]; alpha_table(at);
         #pragma omp parallel for
@@ -1374,29 +1402,28 @@ struct Oracle {
                 else if (k == 0) Tp[idx] = in[cid(i, j, k + 1)];
             }
         }
-        #pragma omp parallel for
-        for (int idx = 0; idx < n; idx++)     // compTpChange (spray_k.cu:4607-4617)
-            Tp_save[idx] = (mark[idx] != TB) ? Tp[idx] - Tp_save[idx] : 0;
-        bool mab = P.scene == MP_SCENE_MELTANDBOIL || P.scene == MP_SCENE_MELTANDBOIL_HIGHRES || P.scene == MP_SCENE_ALL;
-        float a = P.alpha_temp_trans;
-        #pragma omp parallel for
-        for (int p = 0; p < np; p++) {   // mapHeatg2p[_MeltAndBoil] (spray_k.cu:4655-4679)
-            F3 ip = pos[p];
-            float nt = a * (T[p] + scaleFromGrid(ip, Tp_save)) + (1 - a) * scaleFromGrid(ip, Tp);
-            if (mab && flag[p] == TSOL) T[p] = 0.95f * (T[p]) + 0.05f * nt;
-            else T[p] = nt;
-        }
-        float mp_ = P.melting_point, bp = P.boiling_point, lth = P.liquid_heat_th;
-        #pragma omp parallel for
-        for (int p = 0; p < np; p++) {   // updateLatentHeat_k (spray_k.cu:5546-5573)
-            if (flag[p] == TSOL && T[p] > mp_) { L[p] += T[p] - mp_; T[p] = mp_; }
-            if (flag[p] == TF) {
-                if (T[p] < mp_) { L[p] -= mp_ - T[p]; T[p] = mp_; }
-                else if (T[p] > bp) { L[p] += T[p] - bp; T[p] = bp; }
-                else L[p] = lth;
-            }
-        }
+        return capped;
+    }
+    // heatsim (spray.cu:1959-1987)
+    int heatsim() {
+        bool capped = heat_solve();
+        frame++;
         return capped ? MP_ERR_NOCONVERGE : MP_OK;
+    }
+    // initheat_grid_k + markBoundaryCell (spray_k.cu:5603-5621, 535-545)
+    void init_heat_grid() {
+        for (int idx = 0; idx < n; idx++) {
+            int i, j, k; getijk(idx, i, j, k);
+            float x = (float)i, z = (float)k;
+            float r = (float)(NX * 0.15);
+            float a = x - (float)(NX / 4), b = z - (float)(NZ / 4);
+            float a2 = x - (float)(NX / 4 * 3), b2 = z - (float)(NZ / 4 * 3);
+            if (sqrtf(a * a + b * b) <= r) { Tp[idx] = 100; mark[idx] = TSOL; }
+            else if (sqrtf(a2 * a2 + b2 * b2) <= r) { Tp[idx] = 0; mark[idx] = TF; }
+            else if (z < (float)(NZ / 2)) { Tp[idx] = 20; mark[idx] = MP_TYPEVACUUM; }
+            else { Tp[idx] = 80; mark[idx] = MP_TYPEAIR; }
+            if (i == 0 || i == NX - 1 || j == 0 || j == NY - 1 || k == 0 || k == NZ - 1) mark[idx] = TB;
+        }
     }
 
     // GenerateGasParticle (spray.cu:2653-2683): updatesolubility (spray_k.cu:4719-4727),
@@ -1964,6 +1991,8 @@ int or_collide_advect(void* v) { ((Oracle*)v)->collide_advect(); return MP_OK; }
 int or_correct_pos(void* v) { ((Oracle*)v)->correct_pos(); return MP_OK; }
 int or_correct_pos_bubble(void* v) { ((Oracle*)v)->correct_pos_bubble(); return MP_OK; }
 int or_heat(void* v) { return ((Oracle*)v)->heat(); }
+int or_heatsim(void* v) { return ((Oracle*)v)->heatsim(); }
+int or_init_heat_grid(void* v) { ((Oracle*)v)->init_heat_grid(); return MP_OK; }
 int or_gen_gas(void* v) { return ((Oracle*)v)->gen_gas(); }
 int or_delete(void* v) { ((Oracle*)v)->del(); return MP_OK; }
 int or_melt(void* v) { ((Oracle*)v)->melt(); return MP_OK; }

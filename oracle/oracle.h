@@ -63,6 +63,8 @@ int or_collide_advect(void* o);
 int or_correct_pos(void* o);
 int or_correct_pos_bubble(void* o);
 int or_heat(void* o);
+int or_heatsim(void* o);          /* heatsim (spray.cu:1959-1987)            */
+int or_init_heat_grid(void* o);   /* initheat_grid (spray.cu:1949-1955)      */
 int or_gen_gas(void* o);
 int or_delete(void* o);
 int or_melt(void* o);

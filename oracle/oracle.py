@@ -39,7 +39,8 @@ def load():
     for nm in ["or_hash_sort", "or_external_force", "or_sweep_ls_mark", "or_mark_solo_air", "or_surface_tension",
                "or_markgrid_bubble", "or_p2g", "or_drag", "or_g2p", "or_solid_motion", "or_solo_air_update",
                "or_collide_advect", "or_correct_pos", "or_correct_pos_bubble", "or_heat", "or_gen_gas", "or_delete",
-               "or_melt", "or_freeze", "or_mc_presort", "or_step", "or_init_particle_heat"]:
+               "or_melt", "or_freeze", "or_mc_presort", "or_step", "or_init_particle_heat", "or_heatsim",
+               "or_init_heat_grid"]:
         f = getattr(lib, nm)
         f.argtypes = [vp]
         f.restype = C.c_int
@@ -176,6 +177,8 @@ class Oracle:
     def correctpos(self): return self._rc(self.lib.or_correct_pos(self.h))
     def correctpos_bubble(self): return self._rc(self.lib.or_correct_pos_bubble(self.h))
     def updateTemperature(self): return self._rc(self.lib.or_heat(self.h), ok=(0, 3))
+    def heatsim(self): return self._rc(self.lib.or_heatsim(self.h), ok=(0, 3))
+    def initheat_grid(self): return self._rc(self.lib.or_init_heat_grid(self.h))
     def GenerateGasParticle(self): return self._rc(self.lib.or_gen_gas(self.h))
     def deleteAirFluidParticle(self): return self._rc(self.lib.or_delete(self.h))
     def MeltSolid(self): return self._rc(self.lib.or_melt(self.h))
