@@ -177,6 +177,7 @@ def load_library() -> C.CDLL:
         "mp_set_output": ([vp, C.POINTER(MPOutput)], C.c_int),
         "mp_scene_pour": ([C.c_int, C.c_float, C.c_float, vp, vp, vp, C.c_int, vp, vp, C.POINTER(C.c_int)], C.c_int),
         "mp_set_pour": ([vp, vp, vp, C.c_int], C.c_int),
+        "mp_project_water": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     }
     for nm, (args, res) in sig.items():
         f = getattr(lib, nm)
@@ -186,7 +187,8 @@ def load_library() -> C.CDLL:
                "mp_markgrid_bubble", "mp_p2g", "mp_drag", "mp_g2p", "mp_solid_motion", "mp_solo_air_update",
                "mp_collide_advect", "mp_correct_pos", "mp_correct_pos_bubble", "mp_heat", "mp_gen_gas", "mp_delete",
                "mp_melt", "mp_freeze", "mp_mc_presort", "mp_step", "mp_pour", "mp_heatsim",
-               "mp_init_heat_grid"]:
+               "mp_init_heat_grid", "mp_flip_mark", "mp_water_p2g", "mp_water_g2p", "mp_water_advect",
+               "mp_watersim"]:
         f = getattr(lib, nm)
         f.argtypes = [vp]
         f.restype = C.c_int
@@ -484,6 +486,19 @@ class Sim:
         _check(self.lib.mp_set_pour(self.ctx, _ptr(p3), _ptr(v3), len(p3)), self.ctx)
 
     def pouring(self): return self._stage("mp_pour")
+
+    # ---- water-only mode (SIMULATION_WATER) ----------------------------------
+    def flipMark_sphere(self): return self._stage("mp_flip_mark")
+    def mapvelp2g(self): return self._stage("mp_water_p2g")
+    def mapvelg2p(self): return self._stage("mp_water_g2p")
+    def wateradvect(self): return self._stage("mp_water_advect")
+
+    def project_CG(self):
+        it = C.c_int(); res = C.c_double()
+        rc = _check(self.lib.mp_project_water(self.ctx, C.byref(it), C.byref(res)), self.ctx, allow_noconverge=True)
+        return it.value, res.value, rc
+
+    def watersim(self): return self._stage("mp_watersim", allow_noconverge=True)
 
     # ---- heat-only mode (SIMULATION_HEATONLY) --------------------------------
     def initheat_grid(self): return self._stage("mp_init_heat_grid")

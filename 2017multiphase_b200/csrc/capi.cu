@@ -834,6 +834,51 @@ extern "C" int mp_init_heat_grid(void* ctx) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     return k_init_heat_grid_launch(c);
 }
+// ---- the water mode (SIMULATION_WATER) ------------------------------------
+extern "C" int mp_flip_mark(void* ctx) { MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_flip_mark(c); }
+extern "C" int mp_water_p2g(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    MP_TRY(need_cells(c));
+    return k_water_p2g(c);
+}
+extern "C" int mp_project_water(void* ctx, int* iters, double* res) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    return k_project_water(c, iters, res);
+}
+extern "C" int mp_water_g2p(void* ctx) { MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_water_g2p(c); }
+extern "C" int mp_water_advect(void* ctx) { MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_water_advect(c); }
+
+// watersim (spray.cpp:741-797). Where the reference extracts the fluid surface
+// from the cell ranges of the last (simulation-grid) sort, this step re-sorts
+// on the 2x grid first, as the density pass requires (preMC).
+extern "C" int mp_watersim(void* ctx) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    const mp_params& P = c->P;
+    int warn = MP_OK, st;
+    MP_TRY(k_hash_sort(c));
+    MP_TRY(k_sweep_phi(c, MP_TYPEFLUID));
+    MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
+    MP_TRY(k_flip_mark(c));
+    MP_TRY(k_surface_tension(c));
+    MP_TRY(k_water_p2g(c));
+    MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+    st = k_project_water(c, nullptr, nullptr);
+    if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st);
+    MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+    MP_TRY(k_water_g2p(c));
+    MP_TRY(k_water_advect(c));
+    MP_TRY(k_hash_sort(c));
+    MP_TRY(k_correct_pos(c));
+    if (P.b_run_mc) {
+        MP_TRY(k_mc_presort(c));
+        MP_TRY(k_mc(c, MP_MC_FLUID));
+    }
+    c->S.frame++;
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    MP_CHECK_LAUNCH(c);
+    return warn;
+}
+
 extern "C" int mp_pour(void* ctx) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     return k_pour(c);

@@ -162,6 +162,11 @@ int k_g2p(MpCtx* c);
 int k_solid_motion(MpCtx* c);
 int k_pour(MpCtx* c);
 int k_heatsim(MpCtx* c);
+int k_flip_mark(MpCtx* c);
+int k_water_p2g(MpCtx* c);
+int k_project_water(MpCtx* c, int* iters, double* res);
+int k_water_g2p(MpCtx* c);
+int k_water_advect(MpCtx* c);
 int k_init_heat_grid_launch(MpCtx* c);
 int k_mc_renormal(MpCtx* c, int surface);
 int k_solo_air_update(MpCtx* c);

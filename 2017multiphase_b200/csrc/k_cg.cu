@@ -82,13 +82,16 @@ __device__ __forceinline__ bool finish_sum(const Red& R, double mine, double* to
 __device__ __forceinline__ bool inner(const Grid& g, int i, int j, int k) {
     return i > 0 && i < g.NX - 1 && j > 0 && j < g.NY - 1 && k > 0 && k < g.NZ - 1;
 }
-// computeAx_bubble (spray_k.cu:3423-3447): rows over FLUID and AIR cells
+// computeAx_bubble (spray_k.cu:3423-3447): rows over FLUID and AIR cells;
+// with air = false, computeAx (spray_k.cu:2300-2322) of the single-phase
+// solve: rows over FLUID cells only, AIR cells a zero-pressure region
 struct PressOp {
     Grid g;
     const int8_t* __restrict__ mark;
+    bool air = true;
     __device__ __forceinline__ bool mask(int idx, int i, int j, int k) const {
         int m = mark[idx];
-        return (m == MP_TYPEFLUID || m == MP_TYPEAIR) && inner(g, i, j, k);
+        return (m == MP_TYPEFLUID || (air && m == MP_TYPEAIR)) && inner(g, i, j, k);
     }
     template <class R, class F>
     __device__ __forceinline__ R apply(int idx, F val) const {
@@ -607,7 +610,21 @@ __global__ void k_divergence(Grid g, const int8_t* __restrict__ mark, const floa
     }
 }
 
-// subGradPress on the water and the air face fields
+// cptdivergence (spray_k.cu:86-100): the single-phase divergence of the water
+// faces over FLUID cells, zero elsewhere, in the reference's summation order
+__global__ void k_divergence_water(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ ux,
+                                   const float* __restrict__ uy, const float* __restrict__ uz, float* __restrict__ div) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk(g, (int)idx, i, j, k);
+        float d = 0.0f;
+        if (mark[idx] == MP_TYPEFLUID)
+            d = (ux[fxi(g, i + 1, j, k)] - ux[fxi(g, i, j, k)] + uy[fyi(g, i, j + 1, k)] - uy[fyi(g, i, j, k)] +
+                 uz[fzi(g, i, j, k + 1)] - uz[fzi(g, i, j, k)]) / g.h;
+        div[idx] = d;
+    }
+}
+
+// subGradPress on the water and the air face fields (air skipped when null)
 template <class R>
 __global__ void k_subgrad(Grid g, const R* __restrict__ p, float* wx, float* wy, float* wz, float* ax, float* ay, float* az,
                           float* __restrict__ pf) {
@@ -619,19 +636,19 @@ __global__ void k_subgrad(Grid g, const R* __restrict__ p, float* wx, float* wy,
             int idx = (int)t; getijk3(idx, g.NY, g.NZ, i, j, k);
             if (i > 0 && i < g.NX) {
                 R d = (p[cid(g, i, j, k)] - p[cid(g, i - 1, j, k)]) / hh;
-                wx[idx] = (float)((R)wx[idx] - d); ax[idx] = (float)((R)ax[idx] - d);
+                wx[idx] = (float)((R)wx[idx] - d); if (ax) ax[idx] = (float)((R)ax[idx] - d);
             }
         } else if (t < (long long)g.nfx + g.nfy) {
             int idx = (int)(t - g.nfx); getijk3(idx, g.NY + 1, g.NZ, i, j, k);
             if (j > 0 && j < g.NY) {
                 R d = (p[cid(g, i, j, k)] - p[cid(g, i, j - 1, k)]) / hh;
-                wy[idx] = (float)((R)wy[idx] - d); ay[idx] = (float)((R)ay[idx] - d);
+                wy[idx] = (float)((R)wy[idx] - d); if (ay) ay[idx] = (float)((R)ay[idx] - d);
             }
         } else if (t < (long long)g.nfx + g.nfy + g.nfz) {
             int idx = (int)(t - g.nfx - g.nfy); getijk3(idx, g.NY, g.NZ + 1, i, j, k);
             if (k > 0 && k < g.NZ) {
                 R d = (p[cid(g, i, j, k)] - p[cid(g, i, j, k - 1)]) / hh;
-                wz[idx] = (float)((R)wz[idx] - d); az[idx] = (float)((R)az[idx] - d);
+                wz[idx] = (float)((R)wz[idx] - d); if (az) az[idx] = (float)((R)az[idx] - d);
             }
         }
         if (pf && t < g.n) pf[t] = (float)p[t];
@@ -953,6 +970,34 @@ int k_project(MpCtx* c, int* iters, double* res) {
         k_subgrad<float><<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, x, c->wu[0], c->wu[1], c->wu[2], c->au[0],
                                                                       c->au[1], c->au[2], nullptr);
     }
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    c->S.last_cg_iters = it;
+    c->S.last_cg_residual = rr;
+    if (iters) *iters = it;
+    if (res) *res = rr;
+    return rc;
+}
+
+// project_CG (spray.cu:241-271): the single-phase projection of the water
+// mode (FP32 vectors, FP64 dots, as the reference projection's mixed form)
+int k_project_water(MpCtx* c, int* iters, double* res) {
+    const Grid& g = c->G;
+    if (c->P.precision != MP_PREC_MIXED || c->P.coef_mode != MP_COEF_REF) {
+        c->err = "project_water: the single-phase solve is MP_PREC_MIXED, MP_COEF_REF only";
+        return MP_ERR_STATE;
+    }
+    PressOp op{g, c->mark, false};
+    long long ftot = (long long)g.nfx + g.nfy + g.nfz;
+    k_divergence_water<<<mp_blocks(g.n, 256), 256, 0, c->stream>>>(g, c->mark, c->wu[0], c->wu[1], c->wu[2], c->divg);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    int it = 0; double rr = 0;
+    int rc = run_cg<float>(c, op, c->press, c->divg, c->cg_r, c->cg_p, c->cg_z, c->P.cg_max_iter, c->P.cg_tol_mode,
+                           c->P.cg_tol, c->P.cg_true_residual_every, &it, &rr, MP_KT_CG_STENCIL);
+    if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+    k_subgrad<float><<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, c->press, c->wu[0], c->wu[1], c->wu[2], nullptr,
+                                                                  nullptr, nullptr, nullptr);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     c->S.last_cg_iters = it;

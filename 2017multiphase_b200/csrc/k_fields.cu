@@ -346,6 +346,12 @@ __global__ void k_init_solid_phi(Grid g, Cells cl, float* __restrict__ phi, uint
     }
 }
 
+// flipAirVacuum (spray_k.cu:461-469): VACUUM cells become AIR (the water
+// mode's free surface, a zero-pressure region for the single-phase solve)
+__global__ void k_flip_air_vacuum(int n, int8_t* __restrict__ mark) {
+    MP_GRID_LOOP(idx, n) if (mark[idx] == MP_TYPEVACUUM) mark[idx] = MP_TYPEAIR;
+}
+
 }  // namespace
 
 static Cells cells_of(MpCtx* c) { return Cells{c->cell_off, c->tmask}; }
@@ -387,6 +393,14 @@ static int sweep_ls_one(MpCtx* c, float** ls) {
     MP_CHECK_LAUNCH(c);
     return MP_OK;
 }
+// flipMark_sphere (spray.cu:515-520)
+int k_flip_mark(MpCtx* c) {
+    k_flip_air_vacuum<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G.n, c->mark);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
 int k_sweep_ls_mark(MpCtx* c) {
     MP_TRY(sweep_ls_one(c, &c->lsfluid));
     MP_TRY(sweep_ls_one(c, &c->lsair));

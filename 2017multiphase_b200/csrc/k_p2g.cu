@@ -379,6 +379,27 @@ __global__ void k_heat_g2p(Grid g, int np, const float4* __restrict__ pos, float
     }
 }
 
+// computeDeltaU on the water faces only (the water mode, spray.cu:362-376)
+__global__ void k_delta_u_water(long long n0, long long n1, long long n2, const float* w0, const float* w1,
+                                const float* w2, float* o0, float* o1, float* o2) {
+    long long tot = n0 + n1 + n2;
+    MP_GRID_LOOP(t, tot) {
+        if (t < n0) o0[t] = w0[t] - o0[t];
+        else if (t < n0 + n1) { long long s = t - n0; o1[s] = w1[s] - o1[s]; }
+        else { long long s = t - n0 - n1; o2[s] = w2[s] - o2[s]; }
+    }
+}
+// mapvelg2p_flip (spray_k.cu:242-253): every particle takes the interpolated
+// water velocity change, whatever its type
+__global__ void k_g2p_flip_all(Grid g, int np, const float4* __restrict__ pos, float4* __restrict__ vel, FaceSet d) {
+    MP_GRID_LOOP(p, np) {
+        float3 ip = xyz(pos[p]);
+        float4 v = vel[p];
+        float3 iv = xyz(v) + velFromGrid(g, ip, d.x, d.y, d.z);
+        vel[p] = make_float4(iv.x, iv.y, iv.z, v.w);
+    }
+}
+
 }  // namespace
 
 static Cells cells_of(MpCtx* c) { return Cells{c->cell_off, c->tmask}; }
@@ -410,6 +431,41 @@ int k_p2g(MpCtx* c) {
     k_copy3<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g.nfx, g.nfy, g.nfz, c->wu[0], c->wu[1], c->wu[2], c->wuo[0], c->wuo[1], c->wuo[2]);
     k_copy3<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g.nfx, g.nfy, g.nfz, c->au[0], c->au[1], c->au[2], c->auo[0], c->auo[1], c->auo[2]);
     c->launches += 2;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+// mapvelp2g of the water mode (spray.cu:340-353): the water faces, then
+// their copy for the FLIP update (velmode FLIP)
+int k_water_p2g(MpCtx* c) {
+    {
+        KtScope kt(c, MP_KT_P2G);
+        MP_TRY(k_p2g_faces(c, c->wu, 0));
+    }
+    const Grid& g = c->G;
+    long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    k_copy3<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g.nfx, g.nfy, g.nfz, c->wu[0], c->wu[1], c->wu[2], c->wuo[0],
+                                                        c->wuo[1], c->wuo[2]);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+// mapvelg2p of the water mode (spray.cu:362-376): computeDeltaU on the water
+// faces, then mapvelg2p_flip
+int k_water_g2p(MpCtx* c) {
+    const Grid& g = c->G;
+    long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    k_delta_u_water<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g.nfx, g.nfy, g.nfz, c->wu[0], c->wu[1], c->wu[2],
+                                                                c->wuo[0], c->wuo[1], c->wuo[2]);
+    c->launches++;
+    int np = c->np();
+    if (np > 0) {
+        KtScope kt(c, MP_KT_G2P);
+        k_g2p_flip_all<<<mp_blocks(np, 256), 256, 0, c->stream>>>(g, np, c->pos, c->vel,
+                                                                  FaceSet{c->wuo[0], c->wuo[1], c->wuo[2]});
+        c->launches++;
+    }
     MP_CHECK_LAUNCH(c);
     return MP_OK;
 }

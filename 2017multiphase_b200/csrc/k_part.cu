@@ -537,6 +537,41 @@ __global__ void k_pour_particles(int n, int np, const float* __restrict__ ppos, 
     }
 }
 
+// advectparticle_RK2 (spray_k.cu:409-458) with velmode FLIP: the particle
+// velocity blends the grid velocity with FLIP_ALPHA = 0.95 (utility.h:9), the
+// position takes a midpoint step through the grid velocity, and both are
+// clamped one cell and half a sample spacing inside the walls. SOLID
+// particles keep their position.
+__global__ void k_advect_rk2(Grid g, int np, float4* __restrict__ pos, float4* __restrict__ vel,
+                             const float* __restrict__ ux, const float* __restrict__ uy, const float* __restrict__ uz,
+                             float dt, float samplespace) {
+    const float h = g.h;
+    const float3 g0 = mk3(g.gx0, g.gy0, g.gz0);
+    const float3 g1 = g0 + mk3((float)g.NX, (float)g.NY, (float)g.NZ) * h;
+    const float flip = 0.95f;
+    MP_GRID_LOOP(p, np) {
+        float4 q = pos[p], v4 = vel[p];
+        float3 ip = xyz(q), iv = xyz(v4);
+        float3 tmin = g0 + (mk3(h, h, h) + mk3(0.5f * samplespace));
+        float3 tmax = g1 - (mk3(h, h, h) + mk3(0.5f * samplespace));
+        float3 gv = velFromGrid(g, ip, ux, uy, uz);
+        iv = (1 - flip) * gv + flip * iv;
+        float3 mid = ip + gv * dt * 0.5f;
+        float3 gvm = velFromGrid(g, mid, ux, uy, uz);
+        ip += gvm * dt;
+        if (ip.x <= tmin.x) { ip.x = tmin.x; iv.x = 0.0f; }
+        if (ip.y <= tmin.y) { ip.y = tmin.y; iv.y = 0.0f; }
+        if (ip.z <= tmin.z) { ip.z = tmin.z; iv.z = 0.0f; }
+        if (ip.x >= tmax.x) { ip.x = tmax.x; iv.x = 0.0f; }
+        if (ip.y >= tmax.y) { ip.y = tmax.y; iv.y = 0.0f; }
+        if (ip.z >= tmax.z) { ip.z = tmax.z; iv.z = 0.0f; }
+        if (pflag(q) != MP_TYPESOLID) {
+            vel[p] = with_xyz(v4, iv);
+            pos[p] = with_xyz(q, ip);
+        } else vel[p] = with_xyz(v4, iv);
+    }
+}
+
 // ---- heat / phase change -----------------------------------------------------
 __global__ void k_latent(int np, const float4* __restrict__ pos, float4* __restrict__ heat, float mp, float bp, float lth) {
     MP_GRID_LOOP(p, np) {
@@ -911,6 +946,17 @@ int k_solid_motion(MpCtx* c) {
         c->launches++;
         MP_CHECK_LAUNCH(c);
     }
+    return MP_OK;
+}
+
+// wateradvect (spray.cu:293-305)
+int k_water_advect(MpCtx* c) {
+    int np = c->np();
+    if (!np) return MP_OK;
+    k_advect_rk2<<<PB(np)>>>(c->G, np, c->pos, c->vel, c->wu[0], c->wu[1], c->wu[2], c->P.dt, c->P.samplespace);
+    c->launches++;
+    MP_CHECK_LAUNCH(c);
+    c->mc_sorted = 0;
     return MP_OK;
 }
 

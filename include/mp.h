@@ -385,6 +385,26 @@ int mp_pour(void* ctx);
 int mp_init_heat_grid(void* ctx);
 int mp_heatsim(void* ctx);
 
+/* ---- water-only mode (SIMULATION_WATER, cspray::watersim) ----------------
+ * Stages of the single-phase FLIP step, under the reference's names:
+ * flipMark_sphere (spray.cu:515: VACUUM cells become AIR), mapvelp2g
+ * (spray.cu:340: water faces from FLUID and SOLID particles, copied for the
+ * FLIP update), project_CG (spray.cu:241: cptdivergence over FLUID cells, CG
+ * with FLUID unknowns and AIR at zero pressure, subGradPress on the water
+ * faces; MP_PREC_MIXED and MP_COEF_REF only), mapvelg2p (spray.cu:362:
+ * computeDeltaU on the water faces, every particle takes the change) and
+ * wateradvect (spray.cu:293: advectparticle_RK2, velocity blended with the
+ * grid as FLIP_ALPHA = 0.95, midpoint position step, wall clamp). mp_watersim
+ * runs the step of spray.cpp:741-797 and extracts the FLUID surface when
+ * b_run_mc is set; it re-sorts on the 2x grid before the extraction, which
+ * the reference omits. */
+int mp_flip_mark(void* ctx);
+int mp_water_p2g(void* ctx);
+int mp_project_water(void* ctx, int* iters, double* res);
+int mp_water_g2p(void* ctx);
+int mp_water_advect(void* ctx);
+int mp_watersim(void* ctx);
+
 /* The whole bubblesim step in the reference's order and cadence
  * (spray.cpp:979-1233): pouring, the frame-scripted parameter switches of
  * MP_SCENE_ALL / MELTANDBOIL(_HIGHRES) / INTERACTION(_HIGHRES)

@@ -973,6 +973,101 @@ struct Oracle {
         }
     }
 
+    // ---- the water mode (watersim, spray.cpp:741-797) -------------------------
+    void flip_mark() {   // flipAirVacuum (spray_k.cu:461-469)
+        for (int idx = 0; idx < n; idx++) if (mark[idx] == TV) mark[idx] = TA;
+    }
+    void water_p2g() {   // mapvelp2g (spray.cu:340-353)
+        p2g_into(wu, 0);
+        for (int a = 0; a < 3; a++) wuo[a] = wu[a];
+    }
+    // project_CG (spray.cu:241-271): cptdivergence (spray_k.cu:86-100) over
+    // FLUID cells, CG with FLUID unknowns (computeAx, spray_k.cu:2300-2322),
+    // subGradPress on the water faces
+    int project_water(int* iters, double* residual) {
+        std::vector<float> b(n, 0.0f), x(n, 0.0f);
+        for (int idx = 0; idx < n; idx++) {
+            int i, j, k; getijk(idx, i, j, k);
+            if (mark[idx] == TF)
+                b[idx] = (wu[0][fx(i + 1, j, k)] - wu[0][fx(i, j, k)] + wu[1][fy(i, j + 1, k)] - wu[1][fy(i, j, k)] +
+                          wu[2][fz(i, j, k + 1)] - wu[2][fz(i, j, k)]) / h;
+        }
+        divg = b;
+        auto mask = [&](int i) { return mark[i] == TF; };
+        auto A = [&](std::vector<float>& o, const std::vector<float>& v) {
+            float h2 = h * h;
+            #pragma omp parallel for
+            for (int idx = 0; idx < n; idx++) {
+                if (mark[idx] != TF) { o[idx] = 0; continue; }
+                int i, j, k; getijk(idx, i, j, k);
+                float c = v[idx];
+                float s = -6.0f * c;
+                auto nb = [&](int a, int bb, int cc) { int q = cid(a, bb, cc); return (mark[q] == TB) ? c : v[q]; };
+                s += nb(i + 1, j, k); s += nb(i, j + 1, k); s += nb(i, j, k + 1);
+                s += nb(i - 1, j, k); s += nb(i, j - 1, k); s += nb(i, j, k - 1);
+                o[idx] = s / h2;
+            }
+        };
+        bool capped = false;
+        double res = 0;
+        int it = cg<float>(x, b, mask, A, P.cg_max_iter, P.cg_tol_mode, P.cg_tol, P.cg_true_residual_every, res, capped);
+        press = x;
+        subgrad<float>(wu, x);
+        last_iters = it; last_res = res;
+        if (iters) *iters = it;
+        if (residual) *residual = res;
+        return capped ? MP_ERR_NOCONVERGE : MP_OK;
+    }
+    void water_g2p() {   // mapvelg2p (spray.cu:362-376): computeDeltaU, mapvelg2p_flip
+        for (int a = 0; a < 3; a++)
+            for (size_t i = 0; i < wu[a].size(); i++) wuo[a][i] = wu[a][i] - wuo[a][i];
+        #pragma omp parallel for
+        for (int p = 0; p < np; p++) vel[p] += velFromGrid(pos[p], wuo);
+    }
+    void water_advect() {   // advectparticle_RK2 (spray_k.cu:409-458), velmode FLIP
+        F3 g0 = mk(P.gmin_x, P.gmin_y, P.gmin_z);
+        F3 g1 = g0 + mk((float)NX, (float)NY, (float)NZ) * h;
+        const float flip = 0.95f;   // FLIP_ALPHA (utility.h:9)
+        #pragma omp parallel for
+        for (int p = 0; p < np; p++) {
+            F3 ip = pos[p], iv = vel[p];
+            F3 tmin = g0 + (mk(h, h, h) + mk(0.5f * P.samplespace));
+            F3 tmax = g1 - (mk(h, h, h) + mk(0.5f * P.samplespace));
+            F3 gv = velFromGrid(ip, wu);
+            iv = (1 - flip) * gv + flip * iv;
+            F3 mid = ip + gv * P.dt * 0.5f;
+            F3 gvm = velFromGrid(mid, wu);
+            ip += gvm * P.dt;
+            if (ip.x <= tmin.x) { ip.x = tmin.x; iv.x = 0.0f; }
+            if (ip.y <= tmin.y) { ip.y = tmin.y; iv.y = 0.0f; }
+            if (ip.z <= tmin.z) { ip.z = tmin.z; iv.z = 0.0f; }
+            if (ip.x >= tmax.x) { ip.x = tmax.x; iv.x = 0.0f; }
+            if (ip.y >= tmax.y) { ip.y = tmax.y; iv.y = 0.0f; }
+            if (ip.z >= tmax.z) { ip.z = tmax.z; iv.z = 0.0f; }
+            vel[p] = iv;
+            if (flag[p] != TSOL) pos[p] = ip;
+        }
+    }
+    int watersim() {
+        int rc = MP_OK, st;
+        hash_sort();
+        sweep_phi(TF);
+        levelset(0); sweep_ls_mark();
+        flip_mark();
+        surface_tension();
+        water_p2g();
+        sweep_u(TF); set_boundary_u(TF);
+        st = project_water(nullptr, nullptr); if (st) rc = st;
+        sweep_u(TF); set_boundary_u(TF);
+        water_g2p();
+        water_advect();
+        hash_sort();
+        correct_pos();
+        if (P.b_run_mc) { mc_presort(); st = mc(MP_MC_FLUID); if (st) return st; }
+        frame++;
+        return rc;
+    }
+
     // FP64 sum of a float3 array over SOLID-masked entries (accumulate_GPU_f3)
     static void dsum3(const std::vector<F3>& a, int nn, double out[3]) {
         out[0] = out[1] = out[2] = 0;
@@ -1992,6 +2087,12 @@ int or_correct_pos(void* v) { ((Oracle*)v)->correct_pos(); return MP_OK; }
 int or_correct_pos_bubble(void* v) { ((Oracle*)v)->correct_pos_bubble(); return MP_OK; }
 int or_heat(void* v) { return ((Oracle*)v)->heat(); }
 int or_heatsim(void* v) { return ((Oracle*)v)->heatsim(); }
+int or_flip_mark(void* v) { ((Oracle*)v)->flip_mark(); return MP_OK; }
+int or_water_p2g(void* v) { ((Oracle*)v)->water_p2g(); return MP_OK; }
+int or_project_water(void* v, int* it, double* res) { return ((Oracle*)v)->project_water(it, res); }
+int or_water_g2p(void* v) { ((Oracle*)v)->water_g2p(); return MP_OK; }
+int or_water_advect(void* v) { ((Oracle*)v)->water_advect(); return MP_OK; }
+int or_watersim(void* v) { return ((Oracle*)v)->watersim(); }
 int or_init_heat_grid(void* v) { ((Oracle*)v)->init_heat_grid(); return MP_OK; }
 int or_gen_gas(void* v) { return ((Oracle*)v)->gen_gas(); }
 int or_delete(void* v) { ((Oracle*)v)->del(); return MP_OK; }

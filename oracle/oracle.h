@@ -64,6 +64,13 @@ int or_correct_pos(void* o);
 int or_correct_pos_bubble(void* o);
 int or_heat(void* o);
 int or_heatsim(void* o);          /* heatsim (spray.cu:1959-1987)            */
+/* the water mode (watersim, spray.cpp:741-797) and its stages */
+int or_flip_mark(void* o);
+int or_water_p2g(void* o);
+int or_project_water(void* o, int* iters, double* res);
+int or_water_g2p(void* o);
+int or_water_advect(void* o);
+int or_watersim(void* o);
 int or_init_heat_grid(void* o);   /* initheat_grid (spray.cu:1949-1955)      */
 int or_gen_gas(void* o);
 int or_delete(void* o);

@@ -40,7 +40,7 @@ def load():
                "or_markgrid_bubble", "or_p2g", "or_drag", "or_g2p", "or_solid_motion", "or_solo_air_update",
                "or_collide_advect", "or_correct_pos", "or_correct_pos_bubble", "or_heat", "or_gen_gas", "or_delete",
                "or_melt", "or_freeze", "or_mc_presort", "or_step", "or_init_particle_heat", "or_heatsim",
-               "or_init_heat_grid"]:
+               "or_init_heat_grid", "or_flip_mark", "or_water_p2g", "or_water_g2p", "or_water_advect", "or_watersim"]:
         f = getattr(lib, nm)
         f.argtypes = [vp]
         f.restype = C.c_int
@@ -61,6 +61,7 @@ def load():
     lib.or_sweep_u.argtypes = [vp, C.c_int]
     lib.or_set_boundary_u.argtypes = [vp, C.c_int]
     lib.or_project.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    lib.or_project_water.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.or_mc.argtypes = [vp, C.c_int]
     lib.or_mc_get.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, C.c_int]
     lib.or_mc_get_field.argtypes = [vp, vp, vp]
@@ -178,6 +179,16 @@ class Oracle:
     def correctpos_bubble(self): return self._rc(self.lib.or_correct_pos_bubble(self.h))
     def updateTemperature(self): return self._rc(self.lib.or_heat(self.h), ok=(0, 3))
     def heatsim(self): return self._rc(self.lib.or_heatsim(self.h), ok=(0, 3))
+    def flipMark_sphere(self): return self._rc(self.lib.or_flip_mark(self.h))
+    def mapvelp2g(self): return self._rc(self.lib.or_water_p2g(self.h))
+    def mapvelg2p(self): return self._rc(self.lib.or_water_g2p(self.h))
+    def wateradvect(self): return self._rc(self.lib.or_water_advect(self.h))
+    def watersim(self): return self._rc(self.lib.or_watersim(self.h), ok=(0, 3))
+
+    def project_CG(self):
+        it = C.c_int(); res = C.c_double()
+        rc = self._rc(self.lib.or_project_water(self.h, C.byref(it), C.byref(res)), ok=(0, 3))
+        return it.value, res.value, rc
     def initheat_grid(self): return self._rc(self.lib.or_init_heat_grid(self.h))
     def GenerateGasParticle(self): return self._rc(self.lib.or_gen_gas(self.h))
     def deleteAirFluidParticle(self): return self._rc(self.lib.or_delete(self.h))
