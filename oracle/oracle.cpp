@@ -1151,6 +1151,18 @@ struct Oracle {
                        t.x * m02 + t.y * m12 + t.z * m22);
             pos[p] = r2 + rg;
         }
+        // computeSolidVertex_k (spray_k.cu:5254-5263) on the solid surface kept
+        // from frame 0 when bRunMCSolid is off (spray.cu:2771-2772)
+        const int sc = P.scene;
+        if ((sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES || sc == MP_SCENE_MELTANDBOIL ||
+             sc == MP_SCENE_MELTANDBOIL_HIGHRES) && frame > 0 && !P.b_run_mc_solid && P.b_run_mc) {
+            for (F3& v : mc_out[MP_MC_SOLID].verts) {
+                F3 t = v - rg0;
+                F3 r2 = mk(t.x * m00 + t.y * m10 + t.z * m20, t.x * m01 + t.y * m11 + t.z * m21,
+                           t.x * m02 + t.y * m12 + t.z * m22);
+                v = r2 + rg;
+            }
+        }
     }
 
     // updateSoloAirParticle (spray.cu:2620-2651)
@@ -1845,7 +1857,13 @@ struct Oracle {
                 // the mu = -0.53 pass sees zeroed weights in the reference and changes nothing
             }
         }
-        out.normals.assign(nv, mk(0.0f));   // calNormals (spray.cu:924-940; spray_k.cu:2223-2260)
+        normals_of(out, vstart, inc);
+        return MP_OK;
+    }
+    // calNormals (spray.cu:924-940; spray_k.cu:2223-2260)
+    static void normals_of(MCOut& out, const std::vector<uint32_t>& vstart, const std::vector<uint32_t>& inc) {
+        const int nv = (int)out.verts.size();
+        out.normals.assign(nv, mk(0.0f));
         for (int q = 0; q < nv; q++) {
             F3 nrm = mk(0.0f);
             for (uint32_t s = vstart[q]; s < vstart[q + 1]; s++) {
@@ -1856,7 +1874,18 @@ struct Oracle {
             if (length(nrm) > 0) nrm = normalize(nrm);
             out.normals[q] = nrm;
         }
-        return MP_OK;
+    }
+    // runMC_interaction's stored-surface branch (spray.cu:788-794)
+    void renormal(int surface) {
+        MCOut& out = mc_out[surface];
+        const int nv = (int)out.verts.size(), ntri = (int)out.indices.size() / 3;
+        std::vector<uint32_t> vstart(nv + 1, 0);
+        for (uint32_t x : out.indices) vstart[x + 1]++;
+        for (int q = 0; q < nv; q++) vstart[q + 1] += vstart[q];
+        std::vector<uint32_t> inc(out.indices.size()), fillp(vstart.begin(), vstart.end() - 1);
+        for (int t = 0; t < ntri; t++)
+            for (int c = 0; c < 3; c++) inc[fillp[out.indices[3 * t + c]]++] = 3 * t + c;
+        normals_of(out, vstart, inc);
     }
 
     // ---- initTemperature / initSolubility (spray.cu:1989-1999) -------------
@@ -1876,8 +1905,51 @@ struct Oracle {
     }
 
     // ---- bubblesim (spray.cpp:979-1233) ----------------------------------
+    // ---- pouring and the frame-scripted switches (spray.cpp:998-1047) ----------
+    std::vector<F3> pour_pos, pour_vel;
+    void pour() {   // pouring / pouringgas (spray.cu:3012-3043), pouringwater (spray_k.cu:5575-5596)
+        const int sc = P.scene;
+        const bool is_gas = (sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES) && frame >= P.begin_frame;
+        const int every = is_gas ? 6 : 4, npour = (int)pour_pos.size();
+        if (frame % every != 0 || npour == 0 || (long long)npour + np > P.par_num_max) return;
+        const int nr = (int)randf.size();
+        if ((int)pos.size() < np + npour) return;
+        for (int idx = 0; idx < npour; idx++) {
+            int rb = (0 + idx) % (nr - 6);
+            F3 rv = mk(randf[rb] * 2.0f - 1.0f, randf[rb + 1] * 2.0f - 1.0f, randf[rb + 2] * 2.0f - 1.0f);
+            rb += 3;
+            F3 rp = mk(randf[rb] * 2.0f - 1.0f, randf[rb + 1] * 2.0f - 1.0f, randf[rb + 2] * 2.0f - 1.0f);
+            const int q = np + idx;
+            pos[q] = pour_pos[idx] + rp * P.pos_rand_param * P.samplespace;
+            vel[q] = pour_vel[idx] + rv * P.vel_rand_param;
+            mass[q] = P.m0;
+            flag[q] = (int8_t)(is_gas ? TS : TF);
+            T[q] = P.default_liquid_T; L[q] = P.liquid_heat_th;
+            sol[q] = 0.0f; gas[q] = 0.0f;
+        }
+        np += npour;
+    }
+    void scene_toggles() {
+        const int sc = P.scene, f = frame;
+        if (sc == MP_SCENE_ALL && f == 0) {
+            P.b_fix_solid = 0; P.b_add_heat_bottom = 0; P.b_gen_gas = 0; P.b_melt = 0;
+            P.b_freeze = 1;
+        }
+        if (sc == MP_SCENE_ALL && f == 500) P.b_freeze = 0;
+        if (sc == MP_SCENE_ALL && f == 520) { P.b_add_heat_bottom = 1; P.b_melt = 1; }
+        if (sc == MP_SCENE_ALL && f == 1250) P.b_gen_gas = 1;
+        if ((sc == MP_SCENE_MELTANDBOIL || sc == MP_SCENE_MELTANDBOIL_HIGHRES) && f == 300) P.b_fix_solid = 0;
+        if (sc == MP_SCENE_MELTANDBOIL_HIGHRES && f == 400) P.b_add_heat_bottom = 0;
+        if (sc == MP_SCENE_MELTANDBOIL_HIGHRES && f == 700) P.b_add_heat_bottom = 1;
+        if (sc == MP_SCENE_MELTANDBOIL && f == 400) P.b_gen_gas = !P.b_gen_gas;
+        if (sc == MP_SCENE_MELTANDBOIL && f == 700) { P.b_gen_gas = !P.b_gen_gas; P.drag_param_grid = 0.03f; P.vapor_gen_rate = 0.005f; }
+        if ((sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES) && f == P.begin_frame) P.b_fix_solid = 0;
+    }
+
     int step() {
         int rc = MP_OK, st;
+        pour();
+        scene_toggles();
         int sc = P.scene;
         hash_sort();
         external_force();
@@ -1911,7 +1983,12 @@ struct Oracle {
         if (P.b_freeze) freeze();
         if (P.b_run_mc && P.mc_every > 0 && frame % P.mc_every == 0) {
             mc_presort();
-            for (int s = 0; s < 3; s++) { st = mc(s); if (st) return st; }
+            const bool inter = sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES ||
+                               sc == MP_SCENE_MELTANDBOIL || sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL;
+            for (int s = 0; s < 3; s++) {
+                if (s == MP_MC_SOLID && inter && frame > 0 && !P.b_run_mc_solid) { renormal(s); continue; }
+                st = mc(s); if (st) return st;
+            }
         }
         frame++;
         return rc;
@@ -2087,6 +2164,16 @@ int or_correct_pos(void* v) { ((Oracle*)v)->correct_pos(); return MP_OK; }
 int or_correct_pos_bubble(void* v) { ((Oracle*)v)->correct_pos_bubble(); return MP_OK; }
 int or_heat(void* v) { return ((Oracle*)v)->heat(); }
 int or_heatsim(void* v) { return ((Oracle*)v)->heatsim(); }
+int or_set_pour(void* v, const float* pos3, const float* vel3, int n) {
+    Oracle* o = (Oracle*)v;
+    o->pour_pos.resize(n); o->pour_vel.resize(n);
+    for (int i = 0; i < n; i++) {
+        o->pour_pos[i] = mk(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2]);
+        o->pour_vel[i] = mk(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2]);
+    }
+    return MP_OK;
+}
+int or_get_params(void* v, mp_params* p) { *p = ((Oracle*)v)->P; return MP_OK; }
 int or_flip_mark(void* v) { ((Oracle*)v)->flip_mark(); return MP_OK; }
 int or_water_p2g(void* v) { ((Oracle*)v)->water_p2g(); return MP_OK; }
 int or_project_water(void* v, int* it, double* res) { return ((Oracle*)v)->project_water(it, res); }

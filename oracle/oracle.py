@@ -62,6 +62,8 @@ def load():
     lib.or_set_boundary_u.argtypes = [vp, C.c_int]
     lib.or_project.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.or_project_water.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    lib.or_set_pour.argtypes = [vp, vp, vp, C.c_int]
+    lib.or_get_params.argtypes = [vp, vp]
     lib.or_mc.argtypes = [vp, C.c_int]
     lib.or_mc_get.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, C.c_int]
     lib.or_mc_get_field.argtypes = [vp, vp, vp]
@@ -179,6 +181,15 @@ class Oracle:
     def correctpos_bubble(self): return self._rc(self.lib.or_correct_pos_bubble(self.h))
     def updateTemperature(self): return self._rc(self.lib.or_heat(self.h), ok=(0, 3))
     def heatsim(self): return self._rc(self.lib.or_heatsim(self.h), ok=(0, 3))
+    def set_pour(self, pos, vel):
+        p3 = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        v3 = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        return self._rc(self.lib.or_set_pour(self.h, _ptr(p3), _ptr(v3), len(p3)))
+
+    def get_params(self, p):
+        """Fills the ctypes mp_params `p` with the oracle's current parameters."""
+        return self._rc(self.lib.or_get_params(self.h, C.byref(p)))
+
     def flipMark_sphere(self): return self._rc(self.lib.or_flip_mark(self.h))
     def mapvelp2g(self): return self._rc(self.lib.or_water_p2g(self.h))
     def mapvelg2p(self): return self._rc(self.lib.or_water_g2p(self.h))

@@ -170,3 +170,38 @@ def test_interaction_solid_surface_follows_the_solid(mp, run_mc_solid):
         err = np.abs(n2 - _normals(v2.astype(np.float64), i2)).max(axis=1)
         assert (err > 1e-4).mean() < 1e-3, err.max()
     sim.close()
+
+
+def test_step_with_pouring_switches_and_kept_solid_surface_matches_oracle(mp, oracle_mod):
+    """Whole steps of a melt-and-boil scene with an emitter and bRunMCSolid off,
+    GPU against the oracle: the same particles poured, the same switches, the
+    solid surface of frame 0 moved and re-normalled, fields within the bounds
+    of the bubblesim step test."""
+    from parity_util import make_pair, rel_err, snapshot
+    sim, orc = make_pair(mp, oracle_mod, 3, 32, 7406, scene=mp.SCENE_MELTANDBOIL, b_run_mc_solid=0, b_fix_solid=0,
+                         b_melt=0, b_freeze=0, mc_every=2)
+    p = sim.params
+    ppos, pvel = mp.scene_pour(mp.POUR_FREEZING, p.samplespace, 0.035, (0.6, 0.45, 0.75), (0.0, 0.0, -0.5))
+    sim.set_pour(ppos, pvel); orc.set_pour(ppos, pvel)
+    i0 = None
+    for step in range(3):
+        sim.bubblesim(); orc.bubblesim()
+        gs, rs = sim.state(), orc.state()
+        assert gs.frame == rs.frame == step + 1 and gs.par_num_now == rs.par_num_now
+        g, r = snapshot(sim), snapshot(orc)
+        for f in ["press", "lsmerge", "waterux", "wateruy", "wateruz", "pos", "vel"]:
+            e = rel_err(g[f], r[f])
+            assert e <= 1e-5 * (step + 1), f"step {step} {f}: rel err {e:.3e}"
+        gv, gn, gi = sim.mc_mesh(mp.MC_SOLID)
+        rv, rn, ri = orc.mc_mesh(mp.MC_SOLID)
+        assert len(gv) > 0 and len(rv) > 0
+        # the frame-0 extraction sees fields 1e-5 apart, so its case indices can
+        # flip at a threshold; where the surfaces agree, so do their motions
+        if np.array_equal(gi, ri):
+            assert rel_err(gv, rv) <= 1e-5 * (step + 1)
+        if i0 is None:
+            i0, r0 = gi, ri
+        assert np.array_equal(gi, i0) and np.array_equal(ri, r0)   # the frame-0 surfaces, never re-extracted
+    # the emitter poured at frame 0
+    assert sim.state().par_num_now >= len(ppos)
+    sim.close()
