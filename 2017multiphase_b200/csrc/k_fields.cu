@@ -94,13 +94,31 @@ __global__ void k_sweep(Grid g, const float* __restrict__ in, float* __restrict_
             const float nx[2] = {vx[0] ? __ldg(in + idx - sI) : 0.f, vx[1] ? __ldg(in + idx + sI) : 0.f};
             const float ny[2] = {vy[0] ? __ldg(in + idx - sJ) : 0.f, vy[1] ? __ldg(in + idx + sJ) : 0.f};
             const float nz[2] = {vz[0] ? __ldg(in + idx - 1) : 0.f, vz[1] ? __ldg(in + idx + 1) : 0.f};
+            // An octant with m = min(a,b,c) >= res cannot lower res, and skips the
+            // sqrt and the division. Its result is m + 1 rounded (>= m) when that
+            // is not above the maximum; otherwise ((a+b)+c + sqrt(...)) / 3
+            // rounded, which by monotone rounding is at least fl(fl(3m) / 3) (or
+            // NaN): that is m itself when 3m is exact (fl(3m) - 2m == m, the
+            // subtraction being exact), and at least m - ulp(m) otherwise, so
+            // then m two ulps down must still be >= res. The field is unchanged
+            // bit for bit.
             #pragma unroll
             for (int a = 0; a < 2; a++)
             #pragma unroll
             for (int b = 0; b < 2; b++)
             #pragma unroll
-            for (int e = 0; e < 2; e++)
-                if (vx[a] && vy[b] && vz[e]) solvedistance(nx[a], ny[b], nz[e], res);
+            for (int e = 0; e < 2; e++) {
+                if (!(vx[a] && vy[b] && vz[e])) continue;
+                const float m = fminf(nx[a], fminf(ny[b], nz[e]));
+                if (m >= res) {
+                    const float mx = fmaxf(nx[a], fmaxf(ny[b], nz[e]));
+                    if (!(m + 1 > mx)) continue;
+                    const float t = 3.0f * m;
+                    if (t - 2.0f * m == m) continue;
+                    if (m > 1e-30f && __int_as_float(__float_as_int(m) - 2) >= res) continue;
+                }
+                solvedistance(nx[a], ny[b], nz[e], res);
+            }
         }
         out[idx] = res;
     }

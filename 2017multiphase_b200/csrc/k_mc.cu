@@ -349,13 +349,13 @@ static McGrid mc_grid(const MpCtx* c) {
 // nodes per thread of the density gather (along j, along k) and its
 // resident-blocks hint, for the single-field and the fused fluid + gas passes
 #ifndef MC_DENS_NJ
-#define MC_DENS_NJ 2
+#define MC_DENS_NJ 1
 #endif
 #ifndef MC_DENS_NK
 #define MC_DENS_NK 1
 #endif
 #ifndef MC_DENS_MINB
-#define MC_DENS_MINB 4
+#define MC_DENS_MINB 6
 #endif
 #ifndef MC_GAS2_NJ
 #define MC_GAS2_NJ 2
