@@ -19,72 +19,23 @@ using namespace mpk;
 
 namespace {
 
-// particle positions in flight per thread, and the resident-blocks hint
-#ifndef P2G_BATCH
-#define P2G_BATCH 1
-#endif
-#ifndef P2G_MINB
-#define P2G_MINB 4
-#endif
-
-// The particles p0 <= p < p1 of consecutive cells, taken in ascending order by
-// the x- and y-faces when ax / ay, and by the z-face below pz (the end of the
-// cells inside the z-face's window). Positions are loaded B at a time, so B
-// loads are in flight, and a velocity only for a particle that some face
-// takes; each face still adds its particles one by one in ascending order.
+// The air P2G (mapvelp2g_k_air, spray_k.cu:2894-2937): AIR particles, window
+// -2..1 along the face normal and -2..2 across (100 cells). One thread owns the
+// x-, y- and z-face with the same (i,j,k) and walks the union of their windows
+// once; each face accumulates only the cells of its own window, in the
+// reference's (di,dj,dk,particle) order. Bubbles are sparse, so each cell's type
+// mask is tested first and only cells with an AIR particle are walked.
 // sharp_kernel(r2, 1.4) is exactly zero once r2 exceeds 1.4^2, and a zero
-// weight adds +-0 to both sums, so such pairs are skipped.
-template <int WHICH, int B>
-__device__ __forceinline__ void p2g_range(uint32_t p0, uint32_t p1, uint32_t pz, bool ax, bool ay,
-                                          const float4* __restrict__ pos, const float4* __restrict__ vel, float scale,
-                                          float3 gpx, float3 gpy, float3 gpz, float& wx, float& sx, float& wy,
-                                          float& sy, float& wz, float& sz) {
-    const float cut = (1.4f * 1.4f) * 1.0001f;
-    for (uint32_t p = p0; p < p1; p += B) {
-        float4 q[B];
-        #pragma unroll
-        for (int u = 0; u < B; u++) q[u] = (p + u < p1) ? __ldg(pos + p + u) : make_float4(0.f, 0.f, 0.f, flagbits(-1));
-        float r2x[B], r2y[B], r2z[B];
-        bool tx[B], ty[B], tz[B];
-        #pragma unroll
-        for (int u = 0; u < B; u++) {
-            int f = pflag(q[u]);
-            bool ok = WHICH == 0 ? (f == MP_TYPEFLUID || f == MP_TYPESOLID) : (f == MP_TYPEAIR);
-            float3 ps = mk3(q[u].x, q[u].y, q[u].z) * scale;
-            float3 dx = ps - gpx, dy = ps - gpy, dz = ps - gpz;
-            r2x[u] = dot(dx, dx); r2y[u] = dot(dy, dy); r2z[u] = dot(dz, dz);
-            tx[u] = ok && ax && r2x[u] <= cut;
-            ty[u] = ok && ay && r2y[u] <= cut;
-            tz[u] = ok && p + u < pz && r2z[u] <= cut;
-        }
-        float4 v[B];
-        #pragma unroll
-        for (int u = 0; u < B; u++)
-            v[u] = (tx[u] || ty[u] || tz[u]) ? __ldg(vel + p + u) : make_float4(0.f, 0.f, 0.f, 0.f);
-        #pragma unroll
-        for (int u = 0; u < B; u++) {
-            if (tx[u]) { float w = v[u].w * sharp_kernel(r2x[u], 1.4f); wx += w; sx += w * v[u].x; }
-            if (ty[u]) { float w = v[u].w * sharp_kernel(r2y[u], 1.4f); wy += w; sy += w * v[u].y; }
-            if (tz[u]) { float w = v[u].w * sharp_kernel(r2z[u], 1.4f); wz += w; sz += w * v[u].z; }
-        }
-    }
-}
-
-// which = 0: FLUID and SOLID particles, window -1..0 along the face normal and
-// -1..1 across (18 cells); which = 1: AIR particles, -2..1 and -2..2 (100 cells).
-// Water: the cells (a, b, k-1..k+1) are consecutive in the sorted order, so
-// the thread walks each such column as one particle range; cells without a
-// water particle hold only particles the type test rejects. Air: bubbles are
-// sparse, so each cell's type mask is tested first and only cells with an AIR
-// particle are walked.
-template <int WHICH>
-__global__ void __launch_bounds__(256, P2G_MINB) k_p2g_faces(Grid g, Cells cl, const float4* __restrict__ pos,
-                                                   const float4* __restrict__ vel, float* __restrict__ ux,
-                                                   float* __restrict__ uy, float* __restrict__ uz) {
-    constexpr int R = WHICH == 0 ? 1 : 2;      // union window -R..R
-    constexpr int HI = WHICH == 0 ? 0 : 1;     // upper bound along the face normal
+// weight adds +-0 to both sums, so such pairs are skipped, and the velocity is
+// read only when some face takes the particle.
+__global__ void __launch_bounds__(256, 4) k_p2g_air(Grid g, Cells cl, const float4* __restrict__ pos,
+                                                    const float4* __restrict__ vel, float* __restrict__ ux,
+                                                    float* __restrict__ uy, float* __restrict__ uz) {
+    constexpr int R = 2;       // union window -R..R
+    constexpr int HI = 1;      // upper bound along the face normal
     const Tiles T = make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1);
     const float scale = 1.0f / g.h;
+    const float cut = (1.4f * 1.4f) * 1.0001f;
     MP_GRID_LOOP(t, T.threads()) {
         int i, j, k; if (!tile_ijk(T, t, i, j, k)) continue;
         bool hx = (j < g.NY && k < g.NZ), hy = (i < g.NX && k < g.NZ), hz = (i < g.NX && j < g.NY);
@@ -95,27 +46,31 @@ __global__ void __launch_bounds__(256, P2G_MINB) k_p2g_faces(Grid g, Cells cl, c
         const int klo = max(k - R, 0), khi = min(k + R, g.NZ - 1);
         for (int di = -R; di <= R; di++) {
             int a = i + di; if (a < 0 || a > g.NX - 1) continue;
-            bool inx = hx && di <= HI;
+            const bool ax = hx && di <= HI;
             for (int dj = -R; dj <= R; dj++) {
                 int b = j + dj; if (b < 0 || b > g.NY - 1) continue;
-                bool iny = hy && dj <= HI;
-                bool ax = inx, ay = iny;
+                const bool ay = hy && dj <= HI;
                 if (!(ax || ay || hz)) continue;
                 const int cb = cid(g, a, b, 0);
-                if (WHICH == 0) {
-                    // the z-face takes the cells up to k + HI
-                    const uint32_t s0 = __ldg(cl.off + cb + klo), s1 = __ldg(cl.off + cb + khi + 1);
-                    const uint32_t sz0 = hz ? __ldg(cl.off + cb + min(k + HI, khi) + 1) : s0;
-                    p2g_range<WHICH, P2G_BATCH>(s0, s1, sz0, ax, ay, pos, vel, scale, gpx, gpy, gpz, wx, sx, wy, sy, wz, sz);
-                } else {
-                    for (int cc = klo; cc <= khi; cc++) {
-                        bool az = hz && cc - k <= HI;
-                        if (!(ax || ay || az)) continue;
-                        // the type mask is built at sort time; AIR <-> AIRSOLO flips since then
-                        // (markSoloAirParticle) keep the union bit valid
-                        if (!(__ldg(cl.tmask + cb + cc) & ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO)))) continue;
-                        const uint32_t s0 = __ldg(cl.off + cb + cc), s1 = __ldg(cl.off + cb + cc + 1);
-                        p2g_range<WHICH, P2G_BATCH>(s0, s1, az ? s1 : s0, ax, ay, pos, vel, scale, gpx, gpy, gpz, wx, sx, wy, sy, wz, sz);
+                for (int cc = klo; cc <= khi; cc++) {
+                    const bool az = hz && cc - k <= HI;
+                    if (!(ax || ay || az)) continue;
+                    // the type mask is built at sort time; AIR <-> AIRSOLO flips since then
+                    // (markSoloAirParticle) keep the union bit valid
+                    if (!(__ldg(cl.tmask + cb + cc) & ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO)))) continue;
+                    const uint32_t s1 = __ldg(cl.off + cb + cc + 1);
+                    for (uint32_t p = __ldg(cl.off + cb + cc); p < s1; ++p) {
+                        const float4 q = __ldg(pos + p);
+                        if (pflag(q) != MP_TYPEAIR) continue;
+                        const float3 ps = mk3(q.x, q.y, q.z) * scale;
+                        const float3 dx = ps - gpx, dy = ps - gpy, dz = ps - gpz;
+                        const float r2x = dot(dx, dx), r2y = dot(dy, dy), r2z = dot(dz, dz);
+                        const bool tx = ax && r2x <= cut, ty = ay && r2y <= cut, tz = az && r2z <= cut;
+                        if (!(tx || ty || tz)) continue;
+                        const float4 v = __ldg(vel + p);
+                        if (tx) { float w = v.w * sharp_kernel(r2x, 1.4f); wx += w; sx += w * v.x; }
+                        if (ty) { float w = v.w * sharp_kernel(r2y, 1.4f); wy += w; sy += w * v.y; }
+                        if (tz) { float w = v.w * sharp_kernel(r2z, 1.4f); wz += w; sz += w * v.z; }
                     }
                 }
             }
@@ -137,7 +92,9 @@ __global__ void __launch_bounds__(256, P2G_MINB) k_p2g_faces(Grid g, Cells cl, c
 __device__ __forceinline__ uint32_t p2g_slot(uint32_t t) { return t + (t >> 3); }
 __host__ __device__ constexpr int p2g_slots(int cap) { return cap + cap / 8; }
 
-// The water P2G of k_p2g_faces<0> with each warp's particle loads coalesced.
+// The water P2G (mapvelp2g_k_fluidSolid, spray_k.cu:2829-2892): FLUID and
+// SOLID particles, window -1..0 along the face normal and -1..1 across (18
+// cells), with each warp's particle loads coalesced.
 // A warp holds the nodes (i, j, k0 .. k0+31); for one (di, dj) its lanes'
 // windows are overlapping ranges of the cells (a, b, k0-1 .. k0+32), which are
 // consecutive in the sorted order. The warp copies that particle range, CAP at
@@ -146,7 +103,7 @@ __host__ __device__ constexpr int p2g_slots(int cap) { return cap + cap / 8; }
 // ascending order. Per-lane loads from global memory hit ~32 separate lines per
 // warp instruction and saturate L1; the staged reads do not. Every face adds
 // the same particles in the same order with the same arithmetic as
-// k_p2g_faces<0>, so the fields are bit-identical.
+// the one-thread-per-face-triple gather, so the fields are bit-identical.
 template <int CAP>
 __global__ void __launch_bounds__(256, P2G_SMINB) k_p2g_water(Grid g, Cells cl, const float4* __restrict__ pos,
                                                               const float4* __restrict__ vel, float* __restrict__ ux,
@@ -413,7 +370,7 @@ int k_p2g_faces(MpCtx* c, float** out, int which) {
         k_p2g_water<P2G_CAP><<<mp_blocks(tot, 256), 256, smem, c->stream>>>(g, cells_of(c), c->pos, c->vel, out[0], out[1], out[2]);
     }
     else
-        k_p2g_faces<1><<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g, cells_of(c), c->pos, c->vel, out[0], out[1], out[2]);
+        k_p2g_air<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g, cells_of(c), c->pos, c->vel, out[0], out[1], out[2]);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     return MP_OK;

@@ -35,7 +35,7 @@ CG_UPD_TRAFFIC_PER_CELL = None
 
 
 def names_kt(mp):
-    return {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g_faces",
+    return {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g",
             mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
 
 
@@ -222,7 +222,7 @@ def profile_case(args):
     else:
         sim = mp.Sim.from_config(args.config, n, args.seed)
         sim.bubblesim()
-        classes = {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g_faces",
+        classes = {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g",
                    mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
         for k in classes:
             sim.kernel_timing(k, True)
@@ -390,7 +390,7 @@ def main():
     npart = int(sim.state().par_num_now)
     model = {mp.KT_CG_STENCIL: ("k_cg_v4<PressOp,0> (direction + A p)", CG_DIR_BYTES_PER_CELL * n),
              mp.KT_CG_UPDATE: ("k_cg_v4<PressOp,1> (x, r update)", CG_UPD_BYTES_PER_CELL * n),
-             mp.KT_P2G: ("k_p2g_faces (water + air launches)", 29 * npart + 56 * n),
+             mp.KT_P2G: ("k_p2g_water + k_p2g_air (water + air launches)", 29 * npart + 56 * n),
              mp.KT_G2P: ("k_g2p", 37 * npart + 72 * n),
              mp.KT_SORT: ("hash sort (count, scan, scatter, segment sort, gather)", 102 * npart + 8 * n),
              mp.KT_LEVELSET: ("k_genlevelset", 13 * npart + 9 * n),
