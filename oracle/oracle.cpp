@@ -2174,6 +2174,7 @@ int or_set_pour(void* v, const float* pos3, const float* vel3, int n) {
     return MP_OK;
 }
 int or_get_params(void* v, mp_params* p) { *p = ((Oracle*)v)->P; return MP_OK; }
+int or_pour(void* v) { ((Oracle*)v)->pour(); return MP_OK; }
 int or_flip_mark(void* v) { ((Oracle*)v)->flip_mark(); return MP_OK; }
 int or_water_p2g(void* v) { ((Oracle*)v)->water_p2g(); return MP_OK; }
 int or_project_water(void* v, int* it, double* res) { return ((Oracle*)v)->project_water(it, res); }

@@ -40,7 +40,8 @@ def load():
                "or_markgrid_bubble", "or_p2g", "or_drag", "or_g2p", "or_solid_motion", "or_solo_air_update",
                "or_collide_advect", "or_correct_pos", "or_correct_pos_bubble", "or_heat", "or_gen_gas", "or_delete",
                "or_melt", "or_freeze", "or_mc_presort", "or_step", "or_init_particle_heat", "or_heatsim",
-               "or_init_heat_grid", "or_flip_mark", "or_water_p2g", "or_water_g2p", "or_water_advect", "or_watersim"]:
+               "or_init_heat_grid", "or_flip_mark", "or_water_p2g", "or_water_g2p", "or_water_advect", "or_watersim",
+               "or_pour"]:
         f = getattr(lib, nm)
         f.argtypes = [vp]
         f.restype = C.c_int
@@ -190,6 +191,7 @@ class Oracle:
         """Fills the ctypes mp_params `p` with the oracle's current parameters."""
         return self._rc(self.lib.or_get_params(self.h, C.byref(p)))
 
+    def pouring(self): return self._rc(self.lib.or_pour(self.h))
     def flipMark_sphere(self): return self._rc(self.lib.or_flip_mark(self.h))
     def mapvelp2g(self): return self._rc(self.lib.or_water_p2g(self.h))
     def mapvelg2p(self): return self._rc(self.lib.or_water_g2p(self.h))

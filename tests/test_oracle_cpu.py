@@ -60,10 +60,11 @@ def test_hash_out_of_range_axis_maps_to_zero(mp, oracle_mod):
     assert set(nz.tolist()) == expect
 
 
-def _laplacian(mark, nx, ny, nz, h):
-    """computeAx_bubble (spray_k.cu:3423-3447) as a sparse matrix over FLUID/AIR cells."""
+def _laplacian(mark, nx, ny, nz, h, types=(0, 1)):
+    """computeAx_bubble (spray_k.cu:3423-3447) as a sparse matrix over FLUID/AIR
+    cells; with types=(0,) computeAx (spray_k.cu:2300-2322) over FLUID cells."""
     idx = lambda i, j, k: (i * ny + j) * nz + k
-    unk = np.isin(mark, (0, 1))
+    unk = np.isin(mark, types)
     rows, cols, vals = [], [], []
     for c in np.nonzero(unk)[0]:
         i, j, k = c // (ny * nz), (c // nz) % ny, c % nz
@@ -170,6 +171,73 @@ def test_oracle_is_thread_count_independent(mp, oracle_mod):
     b.bubblesim()
     for f, v in r1.items():
         assert np.array_equal(v, b.get_field(f), equal_nan=True), f
+
+
+def _water_to_projection(o):
+    o.hashAndSortParticles(); o.sweepPhi(0); o.computeLevelset(0.0); o.sweepLSAndMardGrid()
+    o.flipMark_sphere(); o.computesurfacetension(); o.mapvelp2g()
+    o.sweepU(0); o.setWaterBoundaryU(0)
+
+
+def test_water_projection_solves_the_single_phase_laplacian(mp, oracle_mod):
+    """project_CG of the water mode: FLUID unknowns, AIR cells (the flipped
+    vacuum) at zero pressure, BOUNDARY neighbours Neumann; the FP32 CG reaches
+    the direct solve to the accuracy its vectors allow, and the divergence is
+    cptdivergence's over FLUID cells."""
+    o, p, _ = _oracle(mp, oracle_mod, 4, 16, cg_tol_mode=mp.TOL_REL, cg_tol=1e-7, cg_max_iter=10000)
+    _water_to_projection(o)
+    mark = o.get_field("mark")
+    assert not (mark == 3).any() and (mark == 1).any()          # no VACUUM left, AIR present
+    ux, uy, uz = (o.get_field(f).astype(np.float64) for f in ("waterux", "wateruy", "wateruz"))
+    it, res, rc = o.project_CG()
+    assert rc == 0 and it > 0
+    n = p.nx
+    ux = ux.reshape(n + 1, n, n); uy = uy.reshape(n, n + 1, n); uz = uz.reshape(n, n, n + 1)
+    div = ((ux[1:] - ux[:-1]) + (uy[:, 1:] - uy[:, :-1]) + (uz[:, :, 1:] - uz[:, :, :-1])).reshape(-1) / p.cellsize
+    b = o.get_field("div").astype(np.float64)
+    fl = mark == 0
+    assert np.allclose(b[fl], div[fl], rtol=1e-5, atol=1e-3) and (b[~fl] == 0).all()
+    x = o.get_field("press").astype(np.float64)
+    A, unk = _laplacian(mark, n, n, n, p.cellsize, types=(0,))
+    sub = np.nonzero(unk)[0]
+    xd = spla.spsolve(A[sub][:, sub].tocsc(), b[sub])
+    assert np.linalg.norm(x[sub] - xd) / np.linalg.norm(xd) < 1e-4
+    assert (x[~unk] == 0).all()
+
+
+def test_oracle_modes_are_thread_count_independent(mp, oracle_mod):
+    runs = []
+    for th in (1, 4):
+        oracle_mod.load().or_set_threads(th)
+        o, _, _ = _oracle(mp, oracle_mod, 4, 16, seed=6)
+        o.watersim(); o.watersim()
+        h, ph, _ = _oracle(mp, oracle_mod, 1, 16, seed=6)
+        h.initheat_grid(); h.heatsim(); h.heatsim()
+        runs.append({"pos": o.get_field("pos"), "press": o.get_field("press"), "tp": h.get_field("tp")})
+    for f in runs[0]:
+        assert np.array_equal(runs[0][f], runs[1][f]), f
+
+
+def test_oracle_pouring_matches_the_numpy_restatement(mp, oracle_mod):
+    """The oracle's pouring stage appends exactly what oracle/pour_ref.py's
+    restatement of pouringwater gives, with the reference's per-type values."""
+    from oracle import pour_ref
+    o, p, parts = _oracle(mp, oracle_mod, 1, 16, seed=8)
+    rf, _ = mp.scene_tables(p, 1, 8)
+    ppos, pvel = pour_ref.emitter(0, p.samplespace, 0.05, (0.5, 0.5, 0.5), (0.0, 0.0, -0.5))
+    o.set_pour(ppos, pvel)
+    np0 = o.state().par_num_now
+    o.pouring()                                       # frame 0: 0 % 4 == 0
+    d = o.download_particles()
+    assert len(d["pos"]) == np0 + len(ppos)
+    rpos, rvel = pour_ref.pour(ppos, pvel, rf, p.pos_rand_param, p.vel_rand_param, p.samplespace)
+    t = slice(np0, None)
+    assert np.array_equal(d["pos"][t].view(np.uint32), rpos.view(np.uint32))
+    assert np.array_equal(d["vel"][t].view(np.uint32), rvel.view(np.uint32))
+    assert (d["flag"][t] == mp.TYPEFLUID).all() and (d["mass"][t] == np.float32(p.m0)).all()
+    st = o.state(); st.frame = 1; o.set_state(st)
+    o.pouring()                                       # not a pouring frame
+    assert o.state().par_num_now == np0 + len(ppos)
 
 
 def test_scene_configurations(mp):
