@@ -267,6 +267,11 @@ static int check_params(const mp_params* p, std::string& err) {
     }
     if (p->coef_mode == MP_COEF_GFM && !(p->density_ratio > 0)) { err = "density_ratio must be positive"; return MP_ERR_ARG; }
     if (p->mc_max_verts < 1 || p->mc_max_tris < 1) { err = "marching-cubes caps must be positive"; return MP_ERR_ARG; }
+    if (p->seed_redraw != 0) {
+        // updateSeedCell draws with the host's rand(): not part of this step;
+        // the nucleation cells stay those of mp_set_tables
+        err = "seed_redraw is not supported: set the nucleation cells with mp_set_tables"; return MP_ERR_ARG;
+    }
     return MP_OK;
 }
 

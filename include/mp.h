@@ -131,7 +131,9 @@ typedef struct mp_params {
     int32_t coef_mode;               /* MP_COEF_*                             */
     float   density_ratio;           /* rho_liquid / rho_air for MP_COEF_GFM  */
     int32_t mc_max_verts, mc_max_tris;
-    int32_t seed_redraw;             /* 1: updateSeedCell cadence is on       */
+    int32_t seed_redraw;             /* must be 0: updateSeedCell's re-draw with
+                                        the host rand() is not supported; the
+                                        nucleation cells are mp_set_tables'   */
     int32_t update_seed_frame_delta;
     /* 1: cells whose MP_F_FIXEDHEAT value is not MP_UNDEF_TEMPERATURE are held
      * at it, the reference's dormant Dirichlet path (compb_heat,

@@ -98,3 +98,17 @@ def test_scene_presets(mp):
     assert p.b_melt and p.b_freeze and p.melting_point == 1.0
     with pytest.raises(mp.MPError):
         mp.scene_params(9, 0)
+
+
+def test_unsupported_seed_redraw_is_rejected(mp):
+    """updateSeedCell's host-rand() re-draw is not part of the step, so asking
+    for it fails at mp_create with a message instead of being ignored."""
+    import ctypes as C
+    lib = mp.load_library()
+    p = mp.default_params(16, 16, 16, 100)
+    p.seed_redraw = 1
+    ctx = C.c_void_p()
+    assert lib.mp_create(C.byref(p), C.byref(ctx)) == mp.MP_ERR_ARG
+    buf = C.create_string_buffer(256)
+    lib.mp_last_error(None, buf, 256)
+    assert b"seed_redraw" in buf.value
