@@ -97,7 +97,10 @@ typedef struct mp_params {
     float   gravity_x, gravity_y, gravity_z;
     float   gmin_x, gmin_y, gmin_z;  /* domain origin (hparam.gmin)           */
     float   samplespace;             /* hparam.samplespace                    */
-    float   m0, airm0, waterrho, solidrho, pradius;
+    float   m0, airm0, waterrho, solidrho, pradius;   /* solidrho (buoyancyForSolid,
+                                        launch commented out) and pradius (triangle
+                                        hashing for rendering) are kept for
+                                        FlipConstant parity; the step reads neither */
     float   poly6kern, spikykern, lapkern;
     /* scene switches (spray.h:344-358) */
     int32_t b_solid, b_melt, b_freeze, b_fix_solid, b_gen_gas, b_heat_trans;
@@ -112,11 +115,14 @@ typedef struct mp_params {
     float   drag_param_solo, drag_param_grid, viscosity_sph;
     float   default_solid_T, default_liquid_T, liquid_heat_th, alpha_temp_trans;
     float   bounce_vel_param, bounce_pos_param, heat_increase_bottom;
-    float   bubble_max_vel, max_vel_for_bubble;
+    float   bubble_max_vel, max_vel_for_bubble;   /* the second clamps nothing: its
+                                        use in enforceForceSoloAirP is commented out
+                                        (spray_k.cu:4366-4367) */
     float   buoyance_rate_air, buoyance_rate_solo;
     float   vapor_gen_rate, init_dissolve_gas_rate, init_gas_rate;
     float   correction_spring, correction_radius;
-    float   mc_density;              /* fMCDensity                            */
+    float   mc_density;              /* fMCDensity: passed to the step's density
+                                        kernels, which do not read it          */
     float   heat_clamp;              /* 378.0 in addHeatAtBottom (spray_k.cu:4502) */
     float   solubility_coef;         /* 1018.9 in updatesolubility (spray_k.cu:4725) */
     float   solid_bounce_param;      /* SolidbounceParam                      */
