@@ -979,14 +979,16 @@ extern "C" int mp_set_output(void* ctx, const mp_output* o) {
 
 // the meshes just extracted, as runMC_smooth writes them (spray.cu:858-863,
 // 954-958): POV-Ray mesh2 when pov; BOBJ when obj, or an empty OBJ for an
-// empty surface; in extraction order solid, water, gas
-static int step_output_meshes(MpCtx* c, int F) {
+// empty surface; in extraction order solid, water, gas. A solid surface kept
+// from frame 0 (runMC_interaction, spray.cu:790-799) goes to a text OBJ.
+static int step_output_meshes(MpCtx* c, int F, bool kept_solid) {
     for (int s : {MP_MC_SOLID, MP_MC_FLUID, MP_MC_GAS}) {
         const char* nm = mc_object_name(s);
         const bool empty = c->mc[s].nverts == 0;
+        const bool text_obj = empty || (kept_solid && s == MP_MC_SOLID);
         if (c->out_pov) MP_TRY(export_mesh(c, s, MP_OUT_POV_MESH, fmt_path("waterdata/%s%05d.pov", c->out_dir, nm, F)));
         if (c->out_obj) {
-            if (empty) MP_TRY(export_mesh(c, s, MP_OUT_OBJ_MESH, fmt_path("waterOBJdata/%s%05d.obj", c->out_dir, nm, F)));
+            if (text_obj) MP_TRY(export_mesh(c, s, MP_OUT_OBJ_MESH, fmt_path("waterOBJdata/%s%05d.obj", c->out_dir, nm, F)));
             else MP_TRY(export_mesh(c, s, MP_OUT_BOBJ_GZ,
                                     c->out_dir + nm + fmt_path("BOBJdata/fluidsurface_final_%04d.bobj.gz", "", nullptr, F - 1)));
         }
@@ -1053,14 +1055,15 @@ extern "C" int mp_step(void* ctx) {
     if (P.b_melt) MP_TRY(k_melt(c));
     if (P.b_freeze) MP_TRY(k_freeze(c));
     const bool out_frame = c->out_on && P.mc_every > 0 && c->S.frame % P.mc_every == 0;
+    // runMC_interaction (spray.cu:788-802): with bRunMCSolid off the solid
+    // surface of frame 0 is kept, moved by the solid motion, and only its
+    // normals are recomputed
+    const bool inter = sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES ||
+                       sc == MP_SCENE_MELTANDBOIL || sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL;
+    const bool kept_solid = inter && c->S.frame > 0 && !P.b_run_mc_solid;
     if (P.b_run_mc && P.mc_every > 0 && c->S.frame % P.mc_every == 0) {
         MP_TRY(k_mc_presort(c));
-        // runMC_interaction (spray.cu:788-802): with bRunMCSolid off the solid
-        // surface of frame 0 is kept, moved by the solid motion, and only its
-        // normals are recomputed
-        const bool inter = sc == MP_SCENE_INTERACTION || sc == MP_SCENE_INTERACTION_HIGHRES ||
-                           sc == MP_SCENE_MELTANDBOIL || sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL;
-        if (inter && c->S.frame > 0 && !P.b_run_mc_solid) MP_TRY(k_mc_renormal(c, MP_MC_SOLID));
+        if (kept_solid) MP_TRY(k_mc_renormal(c, MP_MC_SOLID));
         else MP_TRY(k_mc(c, MP_MC_SOLID));
         MP_TRY(k_mc_fluid_gas(c));
     }
@@ -1069,7 +1072,7 @@ extern "C" int mp_step(void* ctx) {
     int out_rc = MP_OK;
     if (out_frame) {
         const int F = c->S.frame / P.mc_every;
-        if (P.b_run_mc) out_rc = step_output_meshes(c, F);
+        if (P.b_run_mc) out_rc = step_output_meshes(c, F, kept_solid);
         if (out_rc == MP_OK) out_rc = step_output_particles(c, F);
     }
     c->S.frame++;

@@ -465,7 +465,9 @@ int mp_export_particles(void* ctx, int kind, const char* path, float t_min, floa
  *        <dir>waterdata/solobubble%05d.pov (AIRSOLO spheres in
  *        MP_SCENE_INTERACTION, AIR spheres in MP_SCENE_BOILING);
  *   obj: <dir><name>BOBJdata/fluidsurface_final_%04d.bobj.gz with F - 1,
- *        or, for an empty surface, an empty <dir>waterOBJdata/<name>%05d.obj.
+ *        or, for an empty surface, an empty <dir>waterOBJdata/<name>%05d.obj;
+ *        a solid surface kept from frame 0 (b_run_mc_solid = 0 in the
+ *        interaction scenes) goes to <dir>waterOBJdata/solid%05d.obj.
  * `dir` is a prefix used as written (end it with '/'); the directories must
  * exist, as in the reference. NULL turns the output off (the default). */
 typedef struct mp_output {

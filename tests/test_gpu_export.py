@@ -89,3 +89,21 @@ def test_context_exporters_and_missing_directory(mp, tmp_path):
     sim.set_output(None)
     sim.bubblesim()
     sim.close()
+
+
+def test_kept_solid_surface_is_written_as_text_obj(mp, tmp_path):
+    """runMC_interaction's kept-surface branch writes the solid mesh with
+    outputOBJwater (a text OBJ), not as BOBJ."""
+    sim = mp.Sim.from_config(3, 32, 7320, scene=mp.SCENE_MELTANDBOIL, b_run_mc_solid=0, b_fix_solid=0, b_melt=0,
+                             b_freeze=0, mc_every=2)
+    root = str(tmp_path) + "/"
+    _dirs(root)
+    sim.set_output(root, pov=False, obj=True, colored_particles=False)
+    for _ in range(3):                    # frames 0, 1, 2: extraction at 0, kept surface at 2
+        sim.bubblesim()
+    v, n, ix = sim.mc_mesh(mp.MC_SOLID)
+    assert len(v) > 0
+    assert _read(f"{root}waterOBJdata/solid00001.obj") == export_ref.obj_mesh(v, n, ix)
+    assert os.path.exists(f"{root}solidBOBJdata/fluidsurface_final_-001.bobj.gz")   # frame 0: extracted
+    assert not os.path.exists(f"{root}solidBOBJdata/fluidsurface_final_0000.bobj.gz")
+    sim.close()
