@@ -853,6 +853,8 @@ extern "C" int mp_project_water(void* ctx, int* iters, double* res) {
 extern "C" int mp_water_g2p(void* ctx) { MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_water_g2p(c); }
 extern "C" int mp_water_advect(void* ctx) { MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_water_advect(c); }
 
+static int step_output_meshes(MpCtx* c, int F, bool kept_solid, bool fluid_only);
+
 // watersim (spray.cpp:741-797). Where the reference extracts the fluid surface
 // from the cell ranges of the last (simulation-grid) sort, this step re-sorts
 // on the 2x grid first, as the density pass requires (preMC).
@@ -874,14 +876,18 @@ extern "C" int mp_watersim(void* ctx) {
     MP_TRY(k_water_advect(c));
     MP_TRY(k_hash_sort(c));
     MP_TRY(k_correct_pos(c));
+    int out_rc = MP_OK;
     if (P.b_run_mc) {
         MP_TRY(k_mc_presort(c));
         MP_TRY(k_mc(c, MP_MC_FLUID));
+        // runMC_fluid's files (spray.cu:954-958, 858-863) on output frames
+        if (c->out_on && P.mc_every > 0 && c->S.frame % P.mc_every == 0)
+            out_rc = step_output_meshes(c, c->S.frame / P.mc_every, false, true);
     }
     c->S.frame++;
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
     MP_CHECK_LAUNCH(c);
-    return warn;
+    return out_rc != MP_OK ? out_rc : warn;
 }
 
 extern "C" int mp_pour(void* ctx) {
@@ -981,8 +987,9 @@ extern "C" int mp_set_output(void* ctx, const mp_output* o) {
 // 954-958): POV-Ray mesh2 when pov; BOBJ when obj, or an empty OBJ for an
 // empty surface; in extraction order solid, water, gas. A solid surface kept
 // from frame 0 (runMC_interaction, spray.cu:790-799) goes to a text OBJ.
-static int step_output_meshes(MpCtx* c, int F, bool kept_solid) {
+static int step_output_meshes(MpCtx* c, int F, bool kept_solid, bool fluid_only) {
     for (int s : {MP_MC_SOLID, MP_MC_FLUID, MP_MC_GAS}) {
+        if (fluid_only && s != MP_MC_FLUID) continue;
         const char* nm = mc_object_name(s);
         const bool empty = c->mc[s].nverts == 0;
         const bool text_obj = empty || (kept_solid && s == MP_MC_SOLID);
@@ -1072,7 +1079,7 @@ extern "C" int mp_step(void* ctx) {
     int out_rc = MP_OK;
     if (out_frame) {
         const int F = c->S.frame / P.mc_every;
-        if (P.b_run_mc) out_rc = step_output_meshes(c, F, kept_solid);
+        if (P.b_run_mc) out_rc = step_output_meshes(c, F, kept_solid, false);
         if (out_rc == MP_OK) out_rc = step_output_particles(c, F);
     }
     c->S.frame++;

@@ -405,7 +405,8 @@ int mp_heatsim(void* ctx);
  * grid as FLIP_ALPHA = 0.95, midpoint position step, wall clamp). mp_watersim
  * runs the step of spray.cpp:741-797 and extracts the FLUID surface when
  * b_run_mc is set; it re-sorts on the 2x grid before the extraction, which
- * the reference omits. */
+ * the reference omits. With mp_set_output it writes the FLUID surface's files
+ * as mp_step does. */
 int mp_flip_mark(void* ctx);
 int mp_water_p2g(void* ctx);
 int mp_project_water(void* ctx, int* iters, double* res);

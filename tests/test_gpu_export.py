@@ -107,3 +107,20 @@ def test_kept_solid_surface_is_written_as_text_obj(mp, tmp_path):
     assert os.path.exists(f"{root}solidBOBJdata/fluidsurface_final_-001.bobj.gz")   # frame 0: extracted
     assert not os.path.exists(f"{root}solidBOBJdata/fluidsurface_final_0000.bobj.gz")
     sim.close()
+
+
+def test_water_mode_writes_the_fluid_surface(mp, tmp_path):
+    """watersim reaches runMC_fluid's writers too: the water surface only."""
+    sim = mp.Sim.from_config(4, 32, 7330, b_run_mc=1, b_correct_position=1)
+    root = str(tmp_path) + "/"
+    _dirs(root)
+    sim.set_output(root, pov=True, obj=True, colored_particles=True)
+    sim.watersim()                        # frame 0
+    v, n, ix = sim.mc_mesh(mp.MC_FLUID)
+    assert len(v) > 0
+    assert _read(f"{root}waterdata/water00000.pov") == export_ref.pov_mesh(v, n, ix, "water")
+    assert gzip.decompress(_read(f"{root}waterBOBJdata/fluidsurface_final_-001.bobj.gz")) == \
+        export_ref.bobj_payload(v, n, ix)
+    files = {f for _, _, fs in os.walk(root) for f in fs}
+    assert files == {"water00000.pov", "fluidsurface_final_-001.bobj.gz"}
+    sim.close()
