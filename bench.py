@@ -141,13 +141,14 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(config, n_cpu, seed, steps=1, warm=1):
-    """The CPU oracle (the reference step restated, OpenMP over all host cores) on a
-    bounded sample of the workload: the same configuration on an n_cpu^3 grid."""
+def cpu_sample(config, n_cpu, seed, steps=1, warm=1, threads=None):
+    """The CPU oracle (the reference step restated, OpenMP over all host cores, or
+    `threads` of them) on a bounded sample of the workload: the same
+    configuration on an n_cpu^3 grid."""
     import importlib
     mp = importlib.import_module("2017multiphase_b200")
     from oracle import oracle as oracle_mod
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     p = mp.scene_params(config, n_cpu)
     orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables(), threads=threads)
     parts = mp.scene_particles(p, config, seed)
@@ -448,6 +449,14 @@ def main():
                                    "sample": f"one oracle step of the same configuration on a {args.cpu_n}^3 grid "
                                              f"({npart} particles, {times[0]:.2f} s), scaled by the cell ratio "
                                              f"{scale:.0f}x to {p.nx}^3"}
+            # the same restatement on one host thread (the reference's host code is serial)
+            n1 = max(16, args.cpu_n // 2)
+            t1, _, np1 = cpu_sample(args.config, n1, args.seed, threads=1)
+            s1 = (p.nx / n1) ** 3
+            out["cpu_baseline"]["single_thread"] = {
+                "value": 1.0 / (t1[0] * s1), "unit": "steps/s", "cores": 1,
+                "sample": f"one oracle step on a {n1}^3 grid ({np1} particles, {t1[0]:.2f} s), "
+                          f"scaled by {s1:.0f}x to {p.nx}^3"}
         except Exception as e:   # the baseline is reported, not required
             out["cpu_baseline"] = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
                                    "sample": f"failed: {e}"}
