@@ -76,6 +76,15 @@ class MPState(C.Structure):
                 ("reserved", C.c_int32 * 6)]
 
 
+class MPSceneInfo(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("sim_mode", C.c_int32),
+                ("init_fluid_particles", C.c_int32), ("split_num", C.c_int32), ("par_num_extra", C.c_int32),
+                ("seed_num", C.c_int32), ("pour_variant", C.c_int32), ("pour_radius", C.c_float),
+                ("pour_pos", C.c_float * 3), ("pour_pos2", C.c_float * 3), ("pour_vel", C.c_float * 3),
+                ("solid_init_pos", C.c_float * 3), ("t_render_min", C.c_float), ("t_render_max", C.c_float),
+                ("frame_max", C.c_int32), ("output_colored_particles", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
 class MPOutput(C.Structure):
     _fields_ = [("dir", C.c_char_p), ("pov", C.c_int32), ("obj", C.c_int32), ("colored_particles", C.c_int32),
                 ("t_render_min", C.c_float), ("t_render_max", C.c_float)]
@@ -177,6 +186,7 @@ def load_library() -> C.CDLL:
         "mp_set_output": ([vp, C.POINTER(MPOutput)], C.c_int),
         "mp_scene_pour": ([C.c_int, C.c_float, C.c_float, vp, vp, vp, C.c_int, vp, vp, C.POINTER(C.c_int)], C.c_int),
         "mp_set_pour": ([vp, vp, vp, C.c_int], C.c_int),
+        "mp_reference_scene": ([C.c_int, P, C.POINTER(MPSceneInfo)], C.c_int),
         "mp_project_water": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     }
     for nm, (args, res) in sig.items():
@@ -289,6 +299,25 @@ def write_particles(kind: int, path: str, pos: np.ndarray, flag: Optional[np.nda
     T = None if temperature is None else np.ascontiguousarray(temperature, np.float32)
     _check(lib.mp_write_particles(kind, os.fsencode(path), _ptr(p3), _ptr(fl), _ptr(T), len(p3), t_min, t_max),
            None)
+
+
+SIM_WATER, SIM_SOLIDCOUPLING, SIM_SMOKE, SIM_BUBBLE, SIM_HEATONLY = range(5)
+
+
+def reference_scene(scene: int):
+    """cspray::initparam's parameters for the reference's named scene (mp_reference_scene):
+    (params, info) with info a dict of the branch's other settings."""
+    lib = load_library()
+    p = Params()
+    info = MPSceneInfo()
+    _check(lib.mp_reference_scene(scene, C.byref(p), C.byref(info)), None)
+    d = {}
+    for nm, typ in MPSceneInfo._fields_:
+        if nm == "reserved":
+            continue
+        v = getattr(info, nm)
+        d[nm] = list(v) if hasattr(v, "__len__") else v
+    return p, d
 
 
 def scene_pour(variant: int, samplespace: float, radius: float, center, vel, center2=None):

@@ -301,3 +301,243 @@ extern "C" int mp_scene_pour(int variant, float samplespace, float radius, const
     *n = cnt;
     return MP_OK;
 }
+
+// ---------------------------------------------------------------------------
+// cspray::initparam (spray.cpp:23-626) for the reference's named scenes
+// ---------------------------------------------------------------------------
+#define MP_TRY_HOST(x)                        \
+    do {                                      \
+        int rc_ = (x);                        \
+        if (rc_ != MP_OK) return rc_;         \
+    } while (0)
+
+namespace {
+void set3(float* d, float x, float y, float z) { d[0] = x; d[1] = y; d[2] = z; }
+// the grid each branch insists on (initparam exits on any other)
+bool scene_grid(int scene, int& nx, int& ny, int& nz) {
+    switch (scene) {
+    case MP_SCENE_DAMBREAK: nx = 32; ny = 32; nz = 32; return true;
+    case MP_SCENE_FLUIDSPHERE: nx = 24; ny = 24; nz = 96; return true;
+    case MP_SCENE_BOILING: nx = 64; ny = 64; nz = 64; return true;
+    case MP_SCENE_BOILING_HIGHRES: nx = 128; ny = 128; nz = 96; return true;
+    case MP_SCENE_MULTIBUBBLE: nx = 32; ny = 32; nz = 64; return true;
+    case MP_SCENE_MELTING: case MP_SCENE_MELTINGPOUR: case MP_SCENE_FREEZING: nx = 64; ny = 64; nz = 64; return true;
+    case MP_SCENE_INTERACTION: case MP_SCENE_MELTANDBOIL: nx = 64; ny = 48; nz = 64; return true;
+    case MP_SCENE_INTERACTION_HIGHRES: nx = 96; ny = 64; nz = 96; return true;
+    case MP_SCENE_MELTANDBOIL_HIGHRES: nx = 96; ny = 96; nz = 96; return true;
+    case MP_SCENE_ALL: nx = 96; ny = 128; nz = 128; return true;
+    case MP_SCENE_HEATTRANSFER: nx = 256; ny = 256; nz = 256; return true;
+    default: return false;   // SMOKE has no initparam branch
+    }
+}
+}  // namespace
+
+extern "C" int mp_reference_scene(int scene, mp_params* p, mp_scene_info* info) {
+    int nx, ny, nz;
+    if (!p || !scene_grid(scene, nx, ny, nz)) return MP_ERR_ARG;
+    mp_scene_info I;
+    memset(&I, 0, sizeof(I));
+    I.nx = nx; I.ny = ny; I.nz = nz;
+    I.pour_variant = -1;
+    MP_TRY_HOST(mp_params_default(p, nx, ny, nz, 0));
+    p->scene = scene;
+    // common defaults (spray.cpp:29-78)
+    p->mc_every = 2;                                     // outputframeDelta
+    p->surfacetension_sigma = 1.0f;
+    p->heatalpha_fluid = 0.02f; p->heatalpha_air = 0.008f;
+    p->heatalpha_solid = 0.2f; p->heatalpha_vacuum = 0.0001f;
+    p->default_temperature = 293.15f; p->temperature0 = 273.15f;
+    p->melting_point = 273.15f; p->boiling_point = 373.15f;
+    p->drag_param_solo = 10; p->drag_param_grid = 0.05f;
+    p->viscosity_sph = 1.8f;
+    p->b_solid = 0; p->b_melt = 0; p->b_freeze = 0; p->b_fix_solid = 0;
+    p->b_gen_gas = 1; p->b_heat_trans = 1; p->b_add_heat_bottom = 1;
+    p->b_extend_heat_to_boundary = 0; p->b_correct_position = 1;
+    p->solid_bounce_param = 0.5f;
+    p->default_solid_T = 263.15f; p->default_liquid_T = 293.15f; p->liquid_heat_th = 10;
+    p->pos_rand_param = 0.1f; p->vel_rand_param = 0.0f;
+    p->alpha_temp_trans = 0.0f;
+    p->bounce_vel_param = 1.0f; p->bounce_pos_param = 0;
+    I.seed_num = 4;
+    p->init_dissolve_gas_rate = 1.0f; p->init_gas_rate = 0.7f;
+    p->vapor_gen_rate = 0.01f;
+    I.t_render_max = 373; I.t_render_min = 273.0f;
+    p->b_smooth_mc = 1;
+    p->b_run_mc_solid = 1;
+    I.frame_max = 1500;
+    p->bubble_max_vel = 6.5f;
+    p->update_seed_frame_delta = 15;
+    p->buoyance_rate_air = 1.25f; p->buoyance_rate_solo = 1.05f;
+    p->begin_frame = 0;
+    I.output_colored_particles = 1;
+    p->gravity_x = 0; p->gravity_y = 0; p->gravity_z = -9.8f;
+    p->cellsize = 1.0f / 64;
+    p->samplespace = 0.5f * p->cellsize;
+    // heatIncreaseBottom is set only by the scenes below; elsewhere 0 here
+    p->heat_increase_bottom = 0.0f;
+    I.split_num = 1;
+    I.sim_mode = MP_SIM_BUBBLE;
+    // the scene's branch (spray.cpp:83-547)
+    switch (scene) {
+    case MP_SCENE_DAMBREAK:
+        I.split_num = 1; I.init_fluid_particles = 81920; I.par_num_extra = 0;
+        I.sim_mode = MP_SIM_SOLIDCOUPLING;
+        set3(I.solid_init_pos, 0.25f, 0.25f, 0.2f);
+        p->b_solid = 1;
+        break;
+    case MP_SCENE_FLUIDSPHERE:
+        I.split_num = 2; I.init_fluid_particles = 200000;
+        I.sim_mode = MP_SIM_WATER;
+        break;
+    case MP_SCENE_BOILING:
+    case MP_SCENE_BOILING_HIGHRES: {
+        const bool hi = scene == MP_SCENE_BOILING_HIGHRES;
+        p->b_solid = 0; p->b_melt = 0; p->b_freeze = 0; p->b_gen_gas = 1; p->b_heat_trans = 1;
+        p->b_add_heat_bottom = 1; p->b_extend_heat_to_boundary = 1;
+        if (hi) { I.split_num = 1; I.init_fluid_particles = 3000000; I.par_num_extra = 1000000; }
+        else { I.split_num = 2; I.init_fluid_particles = 800000; }
+        set3(I.solid_init_pos, 0.20f, 0.20f, 0.7f);
+        p->default_temperature = 293.0f;
+        p->vapor_gen_rate = 0.01f;
+        p->default_liquid_T = 293.0f;
+        p->init_dissolve_gas_rate = 0.95f; p->init_gas_rate = 0.88f;
+        p->heat_increase_bottom = hi ? 3.0f : 1.5f;
+        p->heatalpha_fluid = 0.18f; p->heatalpha_air = 0.08f;
+        I.seed_num = hi ? 3 : 2;
+        p->drag_param_solo = 5; p->drag_param_grid = hi ? 0.15f : 0.12f;
+        I.t_render_max = 373; I.t_render_min = 273.0f;
+        I.frame_max = hi ? 2000 : 1000;
+        break;
+    }
+    case MP_SCENE_MULTIBUBBLE:
+        p->b_solid = 0; p->b_melt = 0; p->b_freeze = 0; p->b_fix_solid = 0; p->b_gen_gas = 0; p->b_heat_trans = 0;
+        p->b_add_heat_bottom = 0; p->b_extend_heat_to_boundary = 0; p->b_correct_position = 1;
+        I.split_num = 2; I.init_fluid_particles = 250000;
+        set3(I.solid_init_pos, 0.5f, 0.5f, 0.2f);
+        p->surfacetension_sigma = 0;
+        break;
+    case MP_SCENE_MELTING:
+        p->b_melt = 1; p->b_solid = 1; p->b_add_heat_bottom = 0;
+        I.split_num = 1; I.init_fluid_particles = 350000;
+        set3(I.solid_init_pos, 0.5f, 0.5f, 0.15f);
+        p->default_temperature = 293.15f;
+        p->heatalpha_fluid = 0.020000f;
+        p->heatalpha_air = 0.00008f;
+        break;
+    case MP_SCENE_MELTINGPOUR:
+        p->b_melt = 1; p->b_solid = 1; p->b_fix_solid = 1; p->b_freeze = 0; p->b_gen_gas = 0;
+        p->b_add_heat_bottom = 0; p->b_extend_heat_to_boundary = 1;
+        I.output_colored_particles = 1;
+        I.split_num = 1; I.init_fluid_particles = 0; I.par_num_extra = 100000;
+        I.pour_variant = MP_POUR_FREEZING; I.pour_radius = 0.035f;
+        set3(I.pour_pos, 0.6f, 0.45f, 0.75f); set3(I.pour_vel, 0.0f, 0.0f, -0.50f);
+        set3(I.solid_init_pos, 0.55f, 0.45f, -0.33f);
+        p->default_temperature = 273.15f;
+        p->melting_point = 265.15f;
+        p->default_solid_T = 263.15f; p->default_liquid_T = 293.15f;
+        p->heatalpha_fluid = 0.01f; p->heatalpha_air = 05.15f;
+        p->bounce_vel_param = 1.3f; p->bounce_pos_param = 1.0f;
+        I.t_render_max = 283; I.t_render_min = 263;
+        p->alpha_temp_trans = 0.95f;
+        break;
+    case MP_SCENE_FREEZING:
+        p->b_melt = 0; p->b_solid = 1; p->b_fix_solid = 1; p->b_freeze = 1; p->b_correct_position = 1;
+        p->b_add_heat_bottom = 1;
+        I.output_colored_particles = 1;
+        I.split_num = 2; I.init_fluid_particles = 0; I.par_num_extra = 100000;
+        I.pour_variant = MP_POUR_FREEZING; I.pour_radius = 0.035f;
+        set3(I.pour_pos, 0.60f, 0.48f, 0.75f); set3(I.pour_vel, 0.0f, 0.0f, -0.5f);
+        set3(I.solid_init_pos, 0.55f, 0.45f, -0.330f);
+        p->default_temperature = 265.15f;
+        p->heatalpha_fluid = 0.00001f; p->heatalpha_air = 0.00008f;
+        p->default_solid_T = 263.15f; p->default_liquid_T = 280.15f; p->liquid_heat_th = 10;
+        p->bounce_vel_param = 1.0f; p->bounce_pos_param = 0.5f;
+        p->alpha_temp_trans = 0.98f;
+        p->viscosity_sph = 1.2f;
+        I.t_render_max = 276; I.t_render_min = 264;
+        break;
+    case MP_SCENE_INTERACTION:
+    case MP_SCENE_INTERACTION_HIGHRES: {
+        const bool hi = scene == MP_SCENE_INTERACTION_HIGHRES;
+        p->b_melt = 0; p->b_freeze = 0; p->b_fix_solid = hi ? 0 : 1; p->b_solid = 1; p->b_gen_gas = 0;
+        p->b_heat_trans = 0; p->b_add_heat_bottom = 0;
+        p->b_run_mc_solid = 0;
+        I.split_num = 1;
+        I.init_fluid_particles = hi ? 1500000 : 280000; I.par_num_extra = hi ? 200000 : 100000;
+        if (hi) {
+            I.pour_variant = MP_POUR_INTERACTION; I.pour_radius = 0.060f;
+            set3(I.pour_pos, 0.25f, 0.25f, 0.05f); set3(I.pour_vel, 0.0f, 0.0f, 1.5f);
+            set3(I.solid_init_pos, 0.750f, 0.58f, 0.8f);
+        } else {
+            I.pour_variant = MP_POUR_INTERACTION2; I.pour_radius = 0.05f;
+            set3(I.pour_pos, 0.27f, 0.25f, 0.05f); set3(I.pour_pos2, 0.45f, 0.25f, 0.05f);
+            set3(I.pour_vel, 0.0f, 0.0f, 1.1f);
+            set3(I.solid_init_pos, 0.41f, 0.28f, 0.2f);
+        }
+        p->default_temperature = 293.15f;
+        p->heatalpha_fluid = 0.0008f; p->heatalpha_air = 0.0008f;
+        p->bounce_vel_param = 1.3f; p->bounce_pos_param = 1.0f;
+        p->drag_param_solo = 5;
+        if (!hi) {
+            p->drag_param_grid = 0.08f;
+            p->surfacetension_sigma = 0.6f;
+            p->begin_frame = 20;
+        }
+        break;
+    }
+    case MP_SCENE_MELTANDBOIL:
+    case MP_SCENE_MELTANDBOIL_HIGHRES:
+    case MP_SCENE_ALL: {
+        const bool hi = scene == MP_SCENE_MELTANDBOIL_HIGHRES, all = scene == MP_SCENE_ALL;
+        p->b_melt = 1; p->b_freeze = 0; p->b_fix_solid = 1; p->b_solid = 1; p->b_gen_gas = 1; p->b_heat_trans = 1;
+        p->b_add_heat_bottom = 1; p->b_extend_heat_to_boundary = 1;
+        p->b_run_mc_solid = 1;
+        I.split_num = 1;
+        I.init_fluid_particles = all ? 3100000 : (hi ? 2400000 : 400000);
+        I.par_num_extra = all ? 500000 : (hi ? 600000 : 100000);
+        if (all) set3(I.solid_init_pos, 0.8f, 01.30f, 0.2f);
+        else if (hi) set3(I.solid_init_pos, 0.850f, 0.68f, 0.65f);
+        else set3(I.solid_init_pos, 0.50f, 0.38f, 0.2f);
+        p->default_temperature = 293.0f;
+        p->boiling_point = 373.15f;
+        if (all) { p->heatalpha_fluid = 0.0001f; p->heatalpha_air = 00.0008f; }
+        else if (hi) { p->heatalpha_fluid = 0.12f; p->heatalpha_air = 0.08f; }
+        else { p->heatalpha_fluid = 0.1f; p->heatalpha_air = 0.08f; }
+        p->init_dissolve_gas_rate = 0.95f; p->init_gas_rate = 0.95f;
+        if (all) { p->default_solid_T = 223.15f; p->default_liquid_T = 280.15f; p->liquid_heat_th = 10; }
+        else if (hi) { p->default_solid_T = 243.15f; p->default_liquid_T = 350.15f; p->liquid_heat_th = 20; }
+        else { p->default_solid_T = 233.15f; p->default_liquid_T = 350.15f; p->liquid_heat_th = 20; }
+        p->vapor_gen_rate = hi ? 0.017f : 0.015f;
+        p->heat_increase_bottom = all ? 50.0f : 1.5f;
+        I.seed_num = hi ? 8 : 2;
+        I.t_render_max = 373; I.t_render_min = 353;
+        p->drag_param_solo = 5; p->drag_param_grid = hi ? 0.08f : 0.03f;
+        p->bubble_max_vel = 9.5f;
+        p->update_seed_frame_delta = 12;
+        p->buoyance_rate_air = 1.45f; p->buoyance_rate_solo = 1.05f;
+        I.frame_max = 2000;
+        break;
+    }
+    case MP_SCENE_HEATTRANSFER:
+        I.sim_mode = MP_SIM_HEATONLY;
+        p->b_extend_heat_to_boundary = 1;
+        I.split_num = 0; I.init_fluid_particles = 0; I.par_num_extra = 1;
+        I.t_render_max = 100.5f; I.t_render_min = -0.5f;
+        p->heatalpha_fluid = 0.0001f; p->heatalpha_air = 0.005f;
+        p->heatalpha_solid = 0.015f; p->heatalpha_vacuum = 0.05f;
+        break;
+    default: return MP_ERR_ARG;
+    }
+    // after the branches (spray.cpp:570-626)
+    p->dt = 0.003f;
+    p->gmin_x = p->gmin_y = p->gmin_z = 0.0f;
+    p->waterrho = 1000.0f; p->solidrho = 800.0f;
+    p->mc_density = 0.5f;
+    p->smooth_iters = 5;
+    p->correction_spring = 500000.0f;
+    p->correction_radius = 0.5f;
+    p->par_num_max = I.par_num_extra + I.init_fluid_particles * I.split_num;
+    MP_TRY_HOST(mp_params_derive(p));
+    if (info) *info = I;
+    return MP_OK;
+}

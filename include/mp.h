@@ -356,6 +356,35 @@ int mp_mc_download(void* ctx, int surface, float* verts, float* normals,
  * (uint8[8n]) of the last extraction. */
 int mp_mc_download_field(void* ctx, float* dens, uint8_t* cubeindex);
 
+/* ---- the reference's scenes (cspray::initparam, spray.cpp:23-626) -------
+ * mp_reference_scene fills `p` with the parameters initparam gives scene
+ * `scene` (MP_SCENE_*): its common defaults (spray.cpp:29-78), the scene's
+ * branch (83-547) and the derived constants (573-626), in the reference's
+ * units (Kelvin temperatures); fields this library adds keep
+ * mp_params_default's values. `info` (may be NULL) gets the rest of the
+ * branch. Host code only. */
+#define MP_SIM_WATER          0   /* SIMULATIONMODE (utility.h:105-111)     */
+#define MP_SIM_SOLIDCOUPLING  1   /* SPH solid coupling: not in this library */
+#define MP_SIM_SMOKE          2   /* not in this library                    */
+#define MP_SIM_BUBBLE         3   /* mp_step                                */
+#define MP_SIM_HEATONLY       4   /* mp_heatsim                             */
+typedef struct mp_scene_info {
+    int32_t nx, ny, nz;             /* the grid initparam requires (it exits otherwise) */
+    int32_t sim_mode;               /* MP_SIM_*                                */
+    int32_t init_fluid_particles;   /* initfluidparticle                       */
+    int32_t split_num;              /* par_num_max = par_num_extra +           */
+    int32_t par_num_extra;          /*   (fluid + solid points) * split_num    */
+    int32_t seed_num;               /* seednum: nucleation cells               */
+    int32_t pour_variant;           /* MP_POUR_* of CompPouringParam_*, or -1  */
+    float   pour_radius, pour_pos[3], pour_pos2[3], pour_vel[3];
+    float   solid_init_pos[3];      /* solidInitPos                            */
+    float   t_render_min, t_render_max;
+    int32_t frame_max;
+    int32_t output_colored_particles;   /* bOutputColoredParticle          */
+    int32_t reserved[8];
+} mp_scene_info;
+int mp_reference_scene(int scene, mp_params* p, mp_scene_info* info);
+
 /* ---- pouring emitters (spray.cpp:1416-1545, spray.cu:3012-3043) ---------
  * The emitter is a set of points with a velocity each (dpourpos /
  * dpourvel). mp_scene_pour lays one out as the scene set-up does:
