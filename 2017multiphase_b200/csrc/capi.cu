@@ -860,26 +860,30 @@ static int step_output_meshes(MpCtx* c, int F, bool kept_solid, bool fluid_only)
 // on the 2x grid first, as the density pass requires (preMC).
 extern "C" int mp_watersim(void* ctx) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    NvtxRange step_range("watersim");
     const mp_params& P = c->P;
     int warn = MP_OK, st;
-    MP_TRY(k_hash_sort(c));
-    MP_TRY(k_sweep_phi(c, MP_TYPEFLUID));
-    MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
-    MP_TRY(k_flip_mark(c));
-    MP_TRY(k_surface_tension(c));
-    MP_TRY(k_water_p2g(c));
-    MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
-    st = k_project_water(c, nullptr, nullptr);
+    MP_STAGE("hashAndSortParticles", k_hash_sort(c));
+    MP_STAGE("sweepPhi", k_sweep_phi(c, MP_TYPEFLUID));
+    MP_STAGE("computeLevelset", k_levelset(c)); MP_STAGE("sweepLSAndMardGrid", k_sweep_ls_mark(c));
+    MP_STAGE("flipMark_sphere", k_flip_mark(c));
+    MP_STAGE("computesurfacetension", k_surface_tension(c));
+    MP_STAGE("mapvelp2g", k_water_p2g(c));
+    MP_STAGE("sweepU", k_sweep_u(c, MP_TYPEFLUID)); MP_STAGE("setWaterBoundaryU", k_set_boundary_u(c, MP_TYPEFLUID));
+    {
+        NvtxRange r_("project_CG");
+        st = k_project_water(c, nullptr, nullptr);
+    }
     if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st);
-    MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
-    MP_TRY(k_water_g2p(c));
-    MP_TRY(k_water_advect(c));
-    MP_TRY(k_hash_sort(c));
-    MP_TRY(k_correct_pos(c));
+    MP_STAGE("sweepU", k_sweep_u(c, MP_TYPEFLUID)); MP_STAGE("setWaterBoundaryU", k_set_boundary_u(c, MP_TYPEFLUID));
+    MP_STAGE("mapvelg2p", k_water_g2p(c));
+    MP_STAGE("wateradvect", k_water_advect(c));
+    MP_STAGE("hashAndSortParticles", k_hash_sort(c));
+    MP_STAGE("correctpos", k_correct_pos(c));
     int out_rc = MP_OK;
     if (P.b_run_mc) {
-        MP_TRY(k_mc_presort(c));
-        MP_TRY(k_mc(c, MP_MC_FLUID));
+        MP_STAGE("preMC", k_mc_presort(c));
+        MP_STAGE("runMC_smooth", k_mc(c, MP_MC_FLUID));
         // runMC_fluid's files (spray.cu:954-958, 858-863) on output frames
         if (c->out_on && P.mc_every > 0 && c->S.frame % P.mc_every == 0)
             out_rc = step_output_meshes(c, c->S.frame / P.mc_every, false, true);
@@ -1024,43 +1028,53 @@ static int step_output_particles(MpCtx* c, int F) {
 // this step.
 extern "C" int mp_step(void* ctx) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    NvtxRange step_range("bubblesim");
     const mp_params& P = c->P;
     int sc = P.scene;
     int warn = MP_OK, st;
-    MP_TRY(k_pour(c));
+    MP_STAGE("pouring", k_pour(c));
     scene_toggles(c);
-    MP_TRY(k_hash_sort(c));
-    MP_TRY(k_external_force(c));
-    MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
-    MP_TRY(k_mark_solo_air(c));
-    MP_TRY(k_surface_tension(c));
-    if (sc == MP_SCENE_MELTING || sc == MP_SCENE_FREEZING) MP_TRY(k_markgrid_bubble(c));
-    MP_TRY(k_p2g(c));
-    MP_TRY(k_drag(c));
-    MP_TRY(k_sweep_phi(c, MP_TYPEAIR)); MP_TRY(k_sweep_u(c, MP_TYPEAIR));
-    MP_TRY(k_sweep_phi(c, MP_TYPEFLUID)); MP_TRY(k_sweep_u(c, MP_TYPEFLUID));
-    MP_TRY(k_set_boundary_u(c, MP_TYPEAIR)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
-    st = k_project(c, nullptr, nullptr);
-    if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st);
-    MP_TRY(k_sweep_u(c, MP_TYPEAIR)); MP_TRY(k_sweep_u(c, MP_TYPEFLUID));
-    MP_TRY(k_set_boundary_u(c, MP_TYPEAIR)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
-    MP_TRY(k_g2p(c));
-    MP_TRY(k_solid_motion(c));
-    MP_TRY(k_solo_air_update(c));
-    MP_TRY(k_hash_sort(c)); MP_TRY(k_collide_advect(c, true));
-    if (P.b_correct_position) {
-        MP_TRY(k_hash_sort(c)); MP_TRY(k_correct_pos(c));
-        MP_TRY(k_hash_sort(c)); MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c)); MP_TRY(k_correct_pos_bubble(c));
-    } else {
-        MP_TRY(k_hash_sort(c)); MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
+    MP_STAGE("hashAndSortParticles", k_hash_sort(c));
+    MP_STAGE("addexternalforce", k_external_force(c));
+    MP_STAGE("computeLevelset", k_levelset(c)); MP_STAGE("sweepLSAndMardGrid", k_sweep_ls_mark(c));
+    MP_STAGE("markSoloAirParticle", k_mark_solo_air(c));
+    MP_STAGE("computesurfacetension", k_surface_tension(c));
+    if (sc == MP_SCENE_MELTING || sc == MP_SCENE_FREEZING) MP_STAGE("markgrid_bubble", k_markgrid_bubble(c));
+    MP_STAGE("mapvelp2g_bubble", k_p2g(c));
+    MP_STAGE("enforceDragForce", k_drag(c));
+    MP_STAGE("sweepPhi", k_sweep_phi(c, MP_TYPEAIR)); MP_STAGE("sweepU", k_sweep_u(c, MP_TYPEAIR));
+    MP_STAGE("sweepPhi", k_sweep_phi(c, MP_TYPEFLUID)); MP_STAGE("sweepU", k_sweep_u(c, MP_TYPEFLUID));
+    MP_STAGE("setWaterBoundaryU", k_set_boundary_u(c, MP_TYPEAIR)); MP_STAGE("setWaterBoundaryU", k_set_boundary_u(c, MP_TYPEFLUID));
+    {
+        NvtxRange r_("project_CG_bubble");
+        st = k_project(c, nullptr, nullptr);
     }
-    MP_TRY(k_hash_sort(c));
-    if (P.b_heat_trans) { st = k_heat(c); if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st); }
-    if (P.b_gen_gas && c->S.frame % 2 == 0) MP_TRY(k_gen_gas(c));
-    MP_TRY(k_hash_sort(c)); MP_TRY(k_delete(c));
-    MP_TRY(k_hash_sort(c));
-    if (P.b_melt) MP_TRY(k_melt(c));
-    if (P.b_freeze) MP_TRY(k_freeze(c));
+    if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st);
+    MP_STAGE("sweepU", k_sweep_u(c, MP_TYPEAIR)); MP_STAGE("sweepU", k_sweep_u(c, MP_TYPEFLUID));
+    MP_STAGE("setWaterBoundaryU", k_set_boundary_u(c, MP_TYPEAIR)); MP_STAGE("setWaterBoundaryU", k_set_boundary_u(c, MP_TYPEFLUID));
+    MP_STAGE("mapvelg2p_bubble", k_g2p(c));
+    MP_STAGE("solidmotion", k_solid_motion(c));
+    MP_STAGE("updateSoloAirParticle", k_solo_air_update(c));
+    MP_STAGE("hashAndSortParticles", k_hash_sort(c)); MP_STAGE("CollisionSolid", k_collide_advect(c, true));
+    if (P.b_correct_position) {
+        MP_STAGE("hashAndSortParticles", k_hash_sort(c)); MP_STAGE("correctpos", k_correct_pos(c));
+        MP_STAGE("hashAndSortParticles", k_hash_sort(c)); MP_STAGE("computeLevelset", k_levelset(c)); MP_STAGE("sweepLSAndMardGrid", k_sweep_ls_mark(c)); MP_STAGE("correctpos_bubble", k_correct_pos_bubble(c));
+    } else {
+        MP_STAGE("hashAndSortParticles", k_hash_sort(c)); MP_STAGE("computeLevelset", k_levelset(c)); MP_STAGE("sweepLSAndMardGrid", k_sweep_ls_mark(c));
+    }
+    MP_STAGE("hashAndSortParticles", k_hash_sort(c));
+    if (P.b_heat_trans) {
+        {
+            NvtxRange r_("updateTemperature");
+            st = k_heat(c);
+        }
+        if (st == MP_ERR_NOCONVERGE) warn = st; else MP_TRY(st);
+    }
+    if (P.b_gen_gas && c->S.frame % 2 == 0) MP_STAGE("GenerateGasParticle", k_gen_gas(c));
+    MP_STAGE("hashAndSortParticles", k_hash_sort(c)); MP_STAGE("deleteAirFluidParticle", k_delete(c));
+    MP_STAGE("hashAndSortParticles", k_hash_sort(c));
+    if (P.b_melt) MP_STAGE("MeltSolid", k_melt(c));
+    if (P.b_freeze) MP_STAGE("Freezing", k_freeze(c));
     const bool out_frame = c->out_on && P.mc_every > 0 && c->S.frame % P.mc_every == 0;
     // runMC_interaction (spray.cu:788-802): with bRunMCSolid off the solid
     // surface of frame 0 is kept, moved by the solid motion, and only its
@@ -1069,10 +1083,10 @@ extern "C" int mp_step(void* ctx) {
                        sc == MP_SCENE_MELTANDBOIL || sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL;
     const bool kept_solid = inter && c->S.frame > 0 && !P.b_run_mc_solid;
     if (P.b_run_mc && P.mc_every > 0 && c->S.frame % P.mc_every == 0) {
-        MP_TRY(k_mc_presort(c));
-        if (kept_solid) MP_TRY(k_mc_renormal(c, MP_MC_SOLID));
-        else MP_TRY(k_mc(c, MP_MC_SOLID));
-        MP_TRY(k_mc_fluid_gas(c));
+        MP_STAGE("preMC", k_mc_presort(c));
+        if (kept_solid) MP_STAGE("runMC_interaction", k_mc_renormal(c, MP_MC_SOLID));
+        else MP_STAGE("runMC_smooth", k_mc(c, MP_MC_SOLID));
+        MP_STAGE("runMC_fluid_gas", k_mc_fluid_gas(c));
     }
     // a file that cannot be written ends the step's output, not the step
     // (the reference printed and paused); the frame still advances

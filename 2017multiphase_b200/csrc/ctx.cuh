@@ -10,6 +10,7 @@
 //   cell ranges as CSR offsets off[n+1] (off[c]..off[c+1] is cell c).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <string>
 #include <vector>
 #include "mp_dev.cuh"
@@ -132,6 +133,21 @@ inline int mp_blocks(long long n, int threads) {
     if (b < 1) b = 1;
     return (int)b;
 }
+
+// a named range on the host timeline for nsys / ncu --nvtx; without a tool
+// attached the calls do nothing
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+// one stage of a step, under the reference method's name
+#define MP_STAGE(name, call)   \
+    do {                       \
+        NvtxRange r_(name);    \
+        MP_TRY(call);          \
+    } while (0)
 
 // kernel-class timing (events around launches on the context stream)
 void kt_begin(MpCtx* c, int cls, cudaEvent_t* ev_end);
