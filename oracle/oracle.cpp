@@ -1757,6 +1757,26 @@ struct Oracle {
     }
     int mc(int surface) {
         mc_density(surface);
+        return mc_extract(surface);
+    }
+    // genSphereDensfield (spray_k.cu:1827-1846): the analytic sphere field the
+    // reference used to test its extraction, then the extraction itself
+    int mc_sphere(int surface, F3 center, float radius) {
+        NXMC = 2 * NX; NYMC = 2 * NY; NZMC = 2 * NZ;
+        const int W = NXMC + 1, H = NYMC + 1, D = NZMC + 1;
+        mc_dens.assign((size_t)W * H * D, 0.0f);
+        for (int i = 0; i < W; i++) for (int j = 0; j < H; j++) for (int k = 0; k < D; k++) {
+            float phi;
+            if (i * j * k == 0 || i == NXMC || j == NYMC || k == NZMC) phi = -0.1f;
+            else {
+                F3 pp = mk((float)i, (float)j, (float)k) * h / (float)(NXMC / NX);
+                phi = radius - length(pp - center);
+            }
+            mc_dens[((size_t)i * H + j) * D + k] = phi;
+        }
+        return mc_extract(surface);
+    }
+    int mc_extract(int surface) {
         int W = NXMC + 1, H = NYMC + 1, D = NZMC + 1;
         int nvox = NXMC * NYMC * NZMC;
         mc_cube.assign(nvox, 0);
@@ -2175,6 +2195,11 @@ int or_set_pour(void* v, const float* pos3, const float* vel3, int n) {
 }
 int or_get_params(void* v, mp_params* p) { *p = ((Oracle*)v)->P; return MP_OK; }
 int or_pour(void* v) { ((Oracle*)v)->pour(); return MP_OK; }
+int or_mc_sphere(void* v, int s, float cx, float cy, float cz, float r) {
+    Oracle* o = (Oracle*)v;
+    if (s < 0 || s > 2 || o->mc_numverts.empty()) return MP_ERR_STATE;
+    return o->mc_sphere(s, mk(cx, cy, cz), r);
+}
 int or_flip_mark(void* v) { ((Oracle*)v)->flip_mark(); return MP_OK; }
 int or_water_p2g(void* v) { ((Oracle*)v)->water_p2g(); return MP_OK; }
 int or_project_water(void* v, int* it, double* res) { return ((Oracle*)v)->project_water(it, res); }

@@ -67,6 +67,8 @@ int or_heatsim(void* o);          /* heatsim (spray.cu:1959-1987)            */
 int or_set_pour(void* o, const float* pos3, const float* vel3, int n);   /* dpourpos / dpourvel */
 int or_get_params(void* o, mp_params* p);   /* the parameters as the scene switches left them */
 int or_pour(void* o);             /* pouring / pouringgas (spray.cu:3012-3043) */
+/* the extraction of `surface` from genSphereDensfield's sphere (spray_k.cu:1827) */
+int or_mc_sphere(void* o, int surface, float cx, float cy, float cz, float radius);
 /* the water mode (watersim, spray.cpp:741-797) and its stages */
 int or_flip_mark(void* o);
 int or_water_p2g(void* o);

@@ -65,6 +65,7 @@ def load():
     lib.or_project_water.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.or_set_pour.argtypes = [vp, vp, vp, C.c_int]
     lib.or_get_params.argtypes = [vp, vp]
+    lib.or_mc_sphere.argtypes = [vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float]
     lib.or_mc.argtypes = [vp, C.c_int]
     lib.or_mc_get.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, C.c_int]
     lib.or_mc_get_field.argtypes = [vp, vp, vp]
@@ -192,6 +193,8 @@ class Oracle:
         return self._rc(self.lib.or_get_params(self.h, C.byref(p)))
 
     def pouring(self): return self._rc(self.lib.or_pour(self.h))
+    def runMC_sphere(self, s, center, radius):
+        return self._rc(self.lib.or_mc_sphere(self.h, s, *[float(c) for c in center], float(radius)))
     def flipMark_sphere(self): return self._rc(self.lib.or_flip_mark(self.h))
     def mapvelp2g(self): return self._rc(self.lib.or_water_p2g(self.h))
     def mapvelg2p(self): return self._rc(self.lib.or_water_g2p(self.h))

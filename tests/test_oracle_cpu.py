@@ -264,3 +264,33 @@ def test_scene_configurations(mp):
     rf, seeds = mp.scene_tables(p2, 2, 9)
     assert rf.size == 10000 and 0 <= rf.min() and rf.max() < 1 and len(set(seeds.tolist())) == 16
     assert ((seeds % 32) == 2).all()
+
+
+@pytest.mark.parametrize("smooth", [0, 1])
+def test_marching_cubes_on_the_reference_sphere_field(mp, oracle_mod, smooth):
+    """The extraction on genSphereDensfield's analytic sphere (spray_k.cu:1827):
+    a closed, consistently oriented surface whose vertices lie on the sphere
+    (to the linear interpolation's error; Taubin's lambda step pulls them in by
+    less than a fifth of a 2x cell) with normals along the radius."""
+    p = mp.scene_params(1, 16)
+    p.b_smooth_mc = smooth
+    o = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    c, r = np.array([0.5, 0.48, 0.52]), 0.3
+    assert o.runMC_sphere(1, c, r) == 0
+    v, n, ix = o.mc_mesh(1)
+    assert len(v) > 100 and len(ix) % 3 == 0
+    hm = p.cellsize / 2
+    d = np.linalg.norm(v.astype(np.float64) - c, axis=1)
+    tol = 0.2 * hm if smooth else 0.02 * hm
+    assert np.abs(d - r).max() < tol, np.abs(d - r).max() / hm
+    radial = (v.astype(np.float64) - c) / d[:, None]
+    cosang = np.sum(radial * n, axis=1)
+    assert (np.abs(np.linalg.norm(n, axis=1) - 1) < 1e-5).all()
+    assert (np.abs(cosang) > 0.9).all() and (np.sign(cosang) == np.sign(cosang[0])).all()
+    tri = ix.reshape(-1, 3)
+    edges = {}
+    for t in tri:
+        for a, b in ((t[0], t[1]), (t[1], t[2]), (t[2], t[0])):
+            edges[(a, b)] = edges.get((a, b), 0) + 1
+    # closed and consistently wound: every directed edge once, its reverse once
+    assert all(cnt == 1 and edges.get((b, a), 0) == 1 for (a, b), cnt in edges.items())
