@@ -28,10 +28,10 @@ DEFAULT_SRC = "/root/reference/Multiphase/Multiphase"
 OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "librefhost.so")
 
-# Kernels launched by refhost/stages.inc (spray_k.cu names).  Kernels that use
-# shared memory with __syncthreads (reorderDataAndFindCellStartD, the scan and
-# reduction kernels) are not emulated: their results are defined by their
-# semantics (stable sort, exclusive scan, sum).
+# Kernels launched by refhost/stages.inc (spray_k.cu names).  Thrust's sort
+# and scan (spray_thrust.cu) and the float reductions (product(),
+# accumulate_GPU_f3) are not the reference's kernels: the sort and the scan are
+# restated by their definitions (stable ascending sort, exclusive sum).
 KERNELS = [
     "addgravityforce_k", "addbuoyancyforce_vel", "genlevelset", "markLS_bigpositive",
     "setLSback_bigpositive", "preparels", "setLSback", "mergeLSAndMarkGrid", "computePhigra",
@@ -52,6 +52,8 @@ KERNELS = [
     "set_nonsolid_2_zero", "setVelZeroSolid_k", "solidCollisionWithBound", "compute_cI_k",
     "cptdivergence", "computeAx", "pcg_op", "mapvelg2p_flip",
     "advectparticle_RK2", "flipAirVacuum", "markfluid", "markair",
+    "reorderDataAndFindCellStartD", "compactVoxels", "markActiveEdge_MC", "generateTriangles_indices",
+    "smooth_computedisplacement", "smooth_addDisplacement", "calnormal_k", "normalizeTriangleNor_k",
 ]
 # __device__ helpers that need what the shim does not give (triangle hashing,
 # rendering); nothing in KERNELS calls them.

@@ -30,6 +30,12 @@ class RHState(C.Structure):
                 ("capped", C.c_int32)]
 
 
+class RHMesh(C.Structure):
+    _fields_ = [("dens", C.c_void_p), ("voxel_verts", C.c_void_p), ("verts", C.c_void_p), ("normals", C.c_void_p),
+                ("indices", C.c_void_p), ("maxv", C.c_int32), ("maxi", C.c_int32), ("nverts", C.c_int32),
+                ("nindices", C.c_int32), ("active", C.c_int32)]
+
+
 def load(src_dir=None):
     """Loads the library, building it from the reference source first when it
     is missing (raises FileNotFoundError without the reference tree)."""
@@ -44,6 +50,10 @@ def load(src_dir=None):
     lib.rh_stage.restype = C.c_int
     lib.rh_last_error.restype = C.c_char_p
     lib.rh_verify_own_writes.argtypes = [C.c_int]
+    lib.rh_mc.argtypes = [C.POINTER(RHState), C.c_void_p, C.c_int, C.POINTER(RHMesh)]
+    lib.rh_mc.restype = C.c_int
+    lib.rh_smooth_normals.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int]
+    lib.rh_smooth_normals.restype = None
     _lib = lib
     return lib
 
@@ -74,6 +84,9 @@ class RefHost:
         self.iters, self.residual, self.capped = 0, 0.0, 0
         self.rf = np.zeros(1, np.float32)
         self.seeds = np.zeros(1, np.int32)
+        self.mesh = {}
+        self.dens = np.zeros((2 * nx + 1) * (2 * ny + 1) * (2 * nz + 1), np.float32)
+        self.voxel_verts = np.zeros(8 * n, np.uint32)
 
     # ---- state, in the Oracle's interface --------------------------------------
     def get_field(self, name):
@@ -118,19 +131,55 @@ class RefHost:
         return s
 
     # ---- stages ------------------------------------------------------------------
-    def run(self, name, arg=0.0):
+    def _state(self):
         st = RHState()
         for fname, fid in self.FIELD_ID.items():
             st.f[fid] = self.a[fname].ctypes.data
         st.np, st.cap, st.frame, st.n_real_solid = self.np, self.params.par_num_max, self.frame, self.n_real_solid
         st.randfloat, st.nrand = self.rf.ctypes.data, self.rf.size
         st.seeds, st.nseed = self.seeds.ctypes.data, self.seeds.size
+        return st
+
+    def run(self, name, arg=0.0):
+        st = self._state()
         rc = self.lib.rh_stage(name.encode(), C.byref(st), C.addressof(self.params), C.c_float(arg))
         if rc:
             raise RuntimeError(f"reference stage {name}: {self.lib.rh_last_error().decode()}")
         self.np, self.n_real_solid = st.np, st.n_real_solid
         self.iters, self.residual, self.capped = st.iters, st.residual, st.capped
         return rc
+
+    def runMC(self, surface, maxv=2_000_000, maxi=6_000_000):
+        """runMC_smooth for one surface (MP_MC_*); preMC must have run."""
+        st = self._state()
+        v = np.zeros((maxv, 3), np.float32)
+        nr = np.zeros((maxv, 3), np.float32)
+        ix = np.zeros(maxi, np.uint32)
+        m = RHMesh(self.dens.ctypes.data, self.voxel_verts.ctypes.data, v.ctypes.data, nr.ctypes.data,
+                   ix.ctypes.data, maxv, maxi, 0, 0, 0)
+        rc = self.lib.rh_mc(C.byref(st), C.addressof(self.params), surface, C.byref(m))
+        if rc:
+            raise RuntimeError(f"reference runMC: {self.lib.rh_last_error().decode()}")
+        self.mesh[surface] = (v[: m.nverts].copy(), nr[: m.nverts].copy(), ix[: m.nindices].copy(), m.active)
+        return rc
+
+    def smooth_and_normals(self, verts, indices, smooth, iters):
+        """smoothMesh (when smooth) and calNormals on a given mesh; returns
+        the smoothed vertices and the normals."""
+        v = np.ascontiguousarray(verts, np.float32).copy()
+        ix = np.ascontiguousarray(indices, np.uint32)
+        nr = np.zeros_like(v)
+        self.lib.rh_smooth_normals(v.ctypes.data, nr.ctypes.data, len(v), ix.ctypes.data, ix.size, int(smooth),
+                                   int(iters))
+        return v, nr
+
+    def mc_mesh(self, surface):
+        v, nr, ix, _ = self.mesh[surface]
+        return v, nr, ix
+
+    def mc_field(self):
+        """The last density field and classifyVoxel's per-voxel vertex counts."""
+        return self.dens.copy(), self.voxel_verts.copy()
 
     def __getattr__(self, name):
         if name.startswith("_") or name in ("a", "lib"):

@@ -5,7 +5,9 @@
 // emulated thread after another (oracle/make_refhost.py, refhost/stages.inc).
 //
 //   * __global__/__device__/__constant__ are plain C++; threadIdx, blockIdx,
-//     blockDim and gridDim are globals that host_launch() sets per thread;
+//     blockDim and gridDim are thread-local globals that host_launch() sets
+//     per emulated thread (host_launch_sync() runs a block's threads
+//     concurrently, for the kernels that call __syncthreads);
 //   * helper_math.h's float3 arithmetic (a CUDA samples header the reference
 //     includes, not present here) is restated with the same operation order
 //     (componentwise, one rounding per operation);
@@ -22,7 +24,7 @@
 #define __device__
 #define __global__
 #define __constant__
-#define __shared__ static
+#define __shared__
 #define __forceinline__ inline
 #include <vector_types.h>
 #include <vector_functions.h>
@@ -33,9 +35,11 @@
 #include <cstdint>
 #include <algorithm>
 #include <vector>
+#include <thread>
+#include <pthread.h>
 
-static uint3 threadIdx, blockIdx;
-static dim3 blockDim, gridDim;
+static thread_local uint3 threadIdx, blockIdx;
+static thread_local dim3 blockDim, gridDim;
 
 // Runs f once per thread of a <<<grid, block>>> launch, blocks and threads in
 // ascending order.
@@ -53,6 +57,36 @@ static void host_launch(dim3 grid, dim3 block, F&& f) {
                             threadIdx = make_uint3(tx, ty, tz);
                             f();
                         }
+}
+
+// A launch of a kernel that synchronises its block (__syncthreads over
+// shared memory): one host thread per CUDA thread of a one-dimensional block,
+// the blocks one after another, a barrier for __syncthreads and between
+// blocks.  Shared arrays declared `extern __shared__` are host globals
+// (globals.inc); a `__shared__` array inside a kernel becomes a local array of
+// each thread, which is what kernels that only use their own slots need.
+static pthread_barrier_t* rh_bar = nullptr;
+template <class F>
+static void host_launch_sync(unsigned grid, unsigned block, F&& f) {
+    pthread_barrier_t bar;
+    pthread_barrier_init(&bar, nullptr, block);
+    rh_bar = &bar;
+    std::vector<std::thread> ts;
+    ts.reserve(block);
+    for (unsigned t = 0; t < block; t++)
+        ts.emplace_back([&, t] {
+            gridDim = dim3(grid);
+            blockDim = dim3(block);
+            threadIdx = make_uint3(t, 0, 0);
+            for (unsigned b = 0; b < grid; b++) {
+                blockIdx = make_uint3(b, 0, 0);
+                f();
+                pthread_barrier_wait(&bar);
+            }
+        });
+    for (auto& th : ts) th.join();
+    rh_bar = nullptr;
+    pthread_barrier_destroy(&bar);
 }
 
 static inline int __mul24(int a, int b) { return a * b; }
@@ -102,7 +136,7 @@ static inline int atomicMax(int* a, int v) { int o = *a; if (v > o) *a = v; retu
 static inline int atomicMin(int* a, int v) { int o = *a; if (v < o) *a = v; return o; }
 static inline int __float_as_int(float f) { int i; memcpy(&i, &f, 4); return i; }
 static inline float __int_as_float(int i) { float f; memcpy(&f, &i, 4); return f; }
-static inline void __syncthreads() {}
+static inline void __syncthreads() { if (rh_bar) pthread_barrier_wait(rh_bar); }
 
 struct HostTex { const unsigned* p = nullptr; };
 template <class T> static inline T tex1Dfetch(const HostTex& t, int i) { return (T)t.p[i]; }
