@@ -27,7 +27,7 @@ class RHState(C.Structure):
     _fields_ = [("f", C.c_void_p * 45), ("np", C.c_int32), ("cap", C.c_int32), ("frame", C.c_int32),
                 ("n_real_solid", C.c_int32), ("randfloat", C.c_void_p), ("nrand", C.c_int32),
                 ("seeds", C.c_void_p), ("nseed", C.c_int32), ("iters", C.c_int32), ("residual", C.c_double),
-                ("capped", C.c_int32)]
+                ("capped", C.c_int32), ("pour_pos", C.c_void_p), ("pour_vel", C.c_void_p), ("npour", C.c_int32)]
 
 
 class RHMesh(C.Structure):
@@ -85,6 +85,8 @@ class RefHost:
         self.rf = np.zeros(1, np.float32)
         self.seeds = np.zeros(1, np.int32)
         self.mesh = {}
+        self.pour_pos = np.zeros((0, 3), np.float32)
+        self.pour_vel = np.zeros((0, 3), np.float32)
         self.dens = np.zeros((2 * nx + 1) * (2 * ny + 1) * (2 * nz + 1), np.float32)
         self.voxel_verts = np.zeros(8 * n, np.uint32)
 
@@ -102,12 +104,12 @@ class RefHost:
     def upload_particles(self, pos, flag, mass, vel=None, temp=None, lheat=None, solubility=None, gascontain=None):
         pos = np.asarray(pos, np.float32).reshape(-1, 3)
         self.np = pos.shape[0]
+        for k in PARTICLES:     # unused slots read as a fresh, zeroed buffer
+            self.a[k][:] = 0
         vals = dict(pos=pos, vel=vel, flag=flag, mass=mass, temp=temp, lheat=lheat, solubility=solubility,
                     gascontain=gascontain)
         for k, v in vals.items():
-            if v is None:
-                self.a[k][:] = 0
-            else:
+            if v is not None:
                 self.set_field(k, v)
 
     def download_particles(self):
@@ -119,6 +121,10 @@ class RefHost:
     def set_tables(self, randfloat, seeds):
         self.rf = np.ascontiguousarray(randfloat, np.float32)
         self.seeds = np.ascontiguousarray(seeds, np.int32)
+
+    def set_pour(self, pos, vel):
+        self.pour_pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        self.pour_vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
 
     def set_state(self, s):
         self.frame = s.frame
@@ -138,6 +144,7 @@ class RefHost:
         st.np, st.cap, st.frame, st.n_real_solid = self.np, self.params.par_num_max, self.frame, self.n_real_solid
         st.randfloat, st.nrand = self.rf.ctypes.data, self.rf.size
         st.seeds, st.nseed = self.seeds.ctypes.data, self.seeds.size
+        st.pour_pos, st.pour_vel, st.npour = self.pour_pos.ctypes.data, self.pour_vel.ctypes.data, len(self.pour_pos)
         return st
 
     def run(self, name, arg=0.0):
