@@ -9,7 +9,8 @@ CUDA 12) and mixes its kernels with host launch code.  Most of its kernels,
 though, are plain per-thread functions.  This recipe reads spray_k.cu where it
 lies, takes the text of every `__device__` helper and of the kernels named in
 KERNELS (unchanged, in file order), and compiles them with g++ under
-oracle/refhost/shim.h, which gives the CUDA execution model (threadIdx,
+oracle/refhost/shim.h (and the per-frame file writers of class cspray under
+oracle/refhost/cspray_io.h), which gives the CUDA execution model (threadIdx,
 blockIdx, ...), helper_math's float3 arithmetic and the few intrinsics the
 kernels use a host meaning.  oracle/refhost/stages.inc then launches them the
 way spray.cu does, one emulated thread after another.  The extracted source
@@ -130,6 +131,52 @@ def extract(src_dir):
     return "".join(parts)
 
 
+# The per-frame file writers (host code of class cspray) and the helpers they
+# call, compiled under refhost/cspray_io.h.
+HOST_FUNCTIONS = [
+    ("spray.cu", "verifyfloat3"), ("spray.cpp", "cspray::mapColorBlue2Red_h"),
+    ("spray.cu", "cspray::outputPovRaywater"), ("spray.cu", "cspray::outputOBJwater"),
+    ("spray.cu", "cspray::outputBOBJwater"), ("spray.cu", "cspray::outputColoredParticle"),
+    ("spray.cu", "cspray::outputSoloBubblePovRay"), ("spray.cu", "cspray::outputAirParticlePovRay"),
+]
+
+
+def _host_function(text, name, fname):
+    """The text of one top-level host function definition, found by name."""
+    m = re.search(r"^[A-Za-z_][\w \t\*&]*\b" + re.escape(name) + r"\s*\([^)]*\)\s*\{", text, re.M)
+    if not m:
+        raise SystemExit(f"{name} not found in {fname}")
+    depth, i = 0, m.end() - 1
+    while True:
+        c = text[i]
+        if c in "\"'":                       # skip string and character literals
+            j = i + 1
+            while text[j] != c:
+                j += 2 if text[j] == "\\" else 1
+            i = j
+        elif text.startswith("//", i):
+            i = text.index("\n", i)
+        elif text.startswith("/*", i):
+            i = text.index("*/", i) + 1
+        elif c == "{":
+            depth += 1
+        elif c == "}":
+            depth -= 1
+            if depth == 0:
+                break
+        i += 1
+    line = text.count("\n", 0, m.start()) + 1
+    return f'#line {line} "{fname}"\n' + text[m.start():i + 1] + "\n"
+
+
+def extract_io(src_dir):
+    parts = []
+    for fname, name in HOST_FUNCTIONS:
+        with open(os.path.join(src_dir, fname), encoding="latin-1") as f:
+            parts.append(_host_function(f.read(), name, fname))
+    return "".join(parts)
+
+
 def build(src_dir=DEFAULT_SRC, quiet=False, keep_source=False):
     if not os.path.exists(os.path.join(src_dir, "spray_k.cu")):
         raise FileNotFoundError(f"reference source not found under {src_dir}")
@@ -142,15 +189,22 @@ def build(src_dir=DEFAULT_SRC, quiet=False, keep_source=False):
         f.write('#include "tables.h"\n' if os.path.exists(os.path.join(src_dir, "tables.h")) else "")
         f.write(body)
         f.write('#include "stages.inc"\n')
+    io = os.path.join(OUT_DIR, "spray_io_host.cpp")
+    with open(io, "w") as f:
+        f.write('// generated by oracle/make_refhost.py from the reference spray.cu / spray.cpp; not committed\n')
+        f.write('#include "cspray_io.h"\n')
+        f.write(extract_io(src_dir))
+        f.write('#include "io.inc"\n')
     inc = os.path.join(HERE, "refhost")
     cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-w",
            "-I", inc, "-I", src_dir, "-I", os.path.join(HERE, "..", "include"), "-I", "/usr/local/cuda/include",
-           cpp, "-o", LIB]
+           cpp, io, "-o", LIB, "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("refhost build failed:\n" + r.stderr[-6000:])
     if not keep_source:
         os.remove(cpp)
+        os.remove(io)
     if not quiet:
         print(LIB)
     return LIB
