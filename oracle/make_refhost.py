@@ -131,13 +131,15 @@ def extract(src_dir):
     return "".join(parts)
 
 
-# The per-frame file writers (host code of class cspray) and the helpers they
-# call, compiled under refhost/cspray_io.h.
+# The per-frame file writers and the pouring emitters (host code of class
+# cspray) and the helpers they call, compiled under refhost/cspray_io.h.
 HOST_FUNCTIONS = [
     ("spray.cu", "verifyfloat3"), ("spray.cpp", "cspray::mapColorBlue2Red_h"),
     ("spray.cu", "cspray::outputPovRaywater"), ("spray.cu", "cspray::outputOBJwater"),
     ("spray.cu", "cspray::outputBOBJwater"), ("spray.cu", "cspray::outputColoredParticle"),
     ("spray.cu", "cspray::outputSoloBubblePovRay"), ("spray.cu", "cspray::outputAirParticlePovRay"),
+    ("spray.cpp", "cspray::CompPouringParam_Freezing"), ("spray.cpp", "cspray::CompPouringParam_Ineraction"),
+    ("spray.cpp", "cspray::CompPouringParam_Ineraction2"),
 ]
 
 

@@ -92,3 +92,27 @@ def test_particle_files_equal_the_reference_writers(mp, refhost, shortdir, kind)
     mp.write_particles(kinds[kind], ours, pos, flag, temp, 263.0, 383.0)
     ref = _read(os.path.join(shortdir, fn))
     assert len(ref) > 0 and _read(ours) == ref
+
+
+@pytest.mark.parametrize("variant, radius, c2", [(0, 0.035, None), (1, 0.05, None), (2, 0.04, (0.3, 0.7, 0.8)),
+                                                 (0, 0.0, None)])
+def test_pouring_emitters_equal_the_reference(mp, refhost, variant, radius, c2):
+    """mp_scene_pour against CompPouringParam_Freezing / _Ineraction /
+    _Ineraction2 (spray.cpp:1416-1545), points and velocities bit for bit."""
+    lib = refhost.load()
+    vp = C.c_void_p
+    lib.rh_pour_lattice.argtypes = [C.c_int, C.c_float, C.c_float, vp, vp, vp, vp, vp, C.c_int]
+    lib.rh_pour_lattice.restype = C.c_int
+    ss = np.float32(1.0 / 64 * 0.5)
+    c1 = np.array([0.5, 0.45, 0.9], np.float32)
+    vel = np.array([0.0, 0.1, -0.5], np.float32)
+    cc2 = None if c2 is None else np.array(c2, np.float32)
+    cap = 100000
+    rp = np.zeros((cap, 3), np.float32)
+    rv = np.zeros((cap, 3), np.float32)
+    n = lib.rh_pour_lattice(variant, ss, radius, c1.ctypes.data, None if cc2 is None else cc2.ctypes.data,
+                            vel.ctypes.data, rp.ctypes.data, rv.ctypes.data, cap)
+    pos, pvel = mp.scene_pour(variant, float(ss), radius, c1, vel, center2=cc2)
+    assert len(pos) == n
+    assert np.array_equal(pos.view(np.uint32), rp[:n].view(np.uint32))
+    assert np.array_equal(pvel.view(np.uint32), rv[:n].view(np.uint32))
