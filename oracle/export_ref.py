@@ -8,9 +8,11 @@ outputBOBJwater (2373-2438), outputColoredParticle (2440-2466),
 outputSoloBubblePovRay (2468-2496), outputAirParticlePovRay (2498-2526), with
 verifyfloat3 (spray.cu:999-1008) and mapColorBlue2Red_h (spray.cpp:1299-1360).
 C's "%f" and Python's "%f" both print the correctly rounded 6-decimal value of
-the same double, so the texts agree byte for byte. Parity unpinned: the
-reference ships no output files or tests for these writers; this restatement
-is checked only against the reference's source text.
+the same double, so the texts agree byte for byte. The reference ships no
+output files or tests for these writers; the writers themselves, compiled for
+the host by oracle/make_refhost.py, pin the product's files in
+tests/test_refhost_io.py, and this restatement stays as the checker that
+travels without the reference tree.
 """
 from __future__ import annotations
 

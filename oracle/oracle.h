@@ -7,14 +7,20 @@
  * path: only tests/, __graft_entry__.smoke() and bench.py's CPU baseline
  * may load it. Nothing in the product links or calls it.
  *
- * Parity status: the reference cannot be compiled or run here (Windows,
- * GL, CUDA texture references removed in CUDA 12, missing CUDA-samples
- * headers), and it ships no tests, golden vectors or fixtures. The only
- * known-answer data it contains is the marching-cubes edge table, which
- * the tests check against. Everything else in this file is "parity
- * unpinned": it restates the reference's arithmetic, operation by
- * operation, with the deterministic semantics listed in DESIGN.md where
- * the reference races (in-place sweeps, float atomics, atomic appends).
+ * Parity status: pinned to the reference's own kernels.  The reference
+ * does not build here as a program (Windows, GL, CUDA texture references
+ * removed in CUDA 12, missing CUDA-samples headers) and ships no tests or
+ * golden vectors, but its kernels compile for the host: oracle/
+ * make_refhost.py takes their text from spray_k.cu unchanged, and
+ * oracle/refhost/stages.inc launches them as spray.cu does.  The tests
+ * tests/test_refhost_*.py run every stage of this file against them on the
+ * same inputs and require bit-equal results.  Where the reference's
+ * outcome depends on thread scheduling (in-place sweeps, float atomics,
+ * atomic appends, float reductions) this file states the definition it
+ * uses, and the kernel launches there follow the same definition.  The
+ * marching-cubes triangle lists follow the generated case table
+ * (csrc/mc_tables.cpp), which triangulates some cases differently from
+ * tables.h.
  *
  * Build: g++ -O2 -fopenmp -ffp-contract=off (see oracle/Makefile).
  */

@@ -3,8 +3,9 @@
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load this;
 the product never does. The oracle restates the reference's multiphase FLIP
 step (gaoyangVR/2017Multiphase, Multiphase/Multiphase/spray.cpp:979-1233 and the
-spray_k.cu kernels it launches) on the CPU. Parity status: unpinned except for
-the marching-cubes tables (see oracle.h).
+spray_k.cu kernels it launches) on the CPU. Parity status: pinned to the
+reference's own kernels compiled for the host (oracle/make_refhost.py,
+tests/test_refhost_*.py; see oracle.h).
 """
 from __future__ import annotations
 

@@ -8,7 +8,11 @@ CompPouringParam_Freezing / _Ineraction / _Ineraction2
 pouringwater (Multiphase/Multiphase/spray_k.cu:5575-5596) as called by
 pouring / pouringgas (spray.cu:3012-3043, frame argument 0) for the particles
 it appends. All arithmetic in float32, one rounding per operation, in the
-reference's order. Parity unpinned: the reference ships no emitter data.
+reference's order. The reference ships no emitter data; its own
+CompPouringParam_* and pouringwater, compiled for the host by
+oracle/make_refhost.py, pin the product's emitters in tests/test_refhost_io.py
+and tests/test_refhost_modes.py, and this restatement stays as the checker
+that travels without the reference tree.
 """
 from __future__ import annotations
 
