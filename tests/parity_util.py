@@ -112,3 +112,45 @@ def compare(gpu, ref, exact=True, rtol=1e-5, skip=()):
             if e > rtol:
                 bad.append((k, f"rel err {e:.3e} > {rtol}"))
     return bad
+
+
+def state_digest(obj):
+    """SHA-256 over the whole state: every field and particle attribute, the
+    cell starts, and the cell ends of the occupied cells (the reference leaves
+    the others stale)."""
+    import hashlib
+    h = hashlib.sha256()
+    snap = snapshot(obj)
+    for k in sorted(snap):
+        h.update(k.encode())
+        h.update(np.ascontiguousarray(snap[k]).tobytes())
+    cs, ce = obj.get_field("cellstart"), obj.get_field("cellend")
+    h.update(cs.tobytes())
+    h.update(np.where(cs != 0xFFFFFFFF, ce, 0).astype(np.uint32).tobytes())
+    return h.hexdigest()
+
+
+def staged_digests(obj, p, frames, mc=True):
+    """Runs `frames` bubblesim frames stage by stage on obj (the oracle or the
+    reference's kernels), and the three surfaces' extraction after the last;
+    returns [(frame, stage, digest)] after every stage, then the surfaces'
+    density digests and counts."""
+    import hashlib
+    out = []
+    for frame in range(frames):
+        st = obj.state()
+        st.frame = frame
+        obj.set_state(st)
+        for stage in bubblesim_stages(p, frame):
+            getattr(obj, stage[0])(*stage[1:])
+            out.append([frame, " ".join(str(x) for x in stage), state_digest(obj)])
+    if mc:
+        obj.preMC()
+        out.append([frames, "preMC", state_digest(obj)])
+        for surf in (0, 1, 2):
+            obj.runMC(surf)
+            dens = obj.mc_field()[0]
+            verts, _, idx = obj.mc_mesh(surf)
+            out.append([frames, f"runMC {surf}", hashlib.sha256(dens.tobytes()).hexdigest(),
+                        int(len(verts)), int(len(idx))])
+    return out
