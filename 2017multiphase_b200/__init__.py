@@ -151,6 +151,7 @@ def load_library() -> C.CDLL:
         "mp_set_field": ([vp, C.c_int, vp, C.c_size_t], C.c_int),
         "mp_set_tables": ([vp, vp, C.c_int, vp, C.c_int], C.c_int),
         "mp_mc_tables": ([vp, vp, vp], C.c_int),
+        "mp_set_mc_tables": ([vp, vp, vp], C.c_int),
         "mp_init_particle_heat": ([vp], C.c_int),
         "mp_levelset": ([vp, C.c_float], C.c_int),
         "mp_sweep_phi": ([vp, C.c_int], C.c_int),
@@ -508,6 +509,12 @@ class Sim:
         return v, nr, ix
 
     # ---- pouring (cspray::pouring / pouringgas) ------------------------------
+    def set_mc_tables(self, num_verts: np.ndarray, tri: np.ndarray):
+        """Replaces the marching-cubes case tables of this context (mp_set_mc_tables)."""
+        nv = np.ascontiguousarray(num_verts, np.int32).reshape(256)
+        tr = np.ascontiguousarray(tri, np.int32).reshape(256 * 16)
+        _check(self.lib.mp_set_mc_tables(self.ctx, _ptr(nv), _ptr(tr)), self.ctx)
+
     def set_pour(self, pos: np.ndarray, vel: np.ndarray):
         """The emitter (dpourpos / dpourvel) the step pours from (mp_set_pour)."""
         p3 = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)

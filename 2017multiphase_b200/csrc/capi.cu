@@ -665,6 +665,29 @@ extern "C" int mp_mc_tables(int32_t* num_verts, int32_t* tri, int32_t* edge) {
     return MP_OK;
 }
 
+extern "C" int mp_set_mc_tables(void* ctx, const int32_t* num_verts, const int32_t* tri) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!num_verts || !tri) { c->err = "set_mc_tables: null table"; return MP_ERR_ARG; }
+    // the cube's edges as corner pairs, corner v being bit v of the case index
+    static const int kEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                     {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+    for (int cs = 0; cs < 256; cs++) {
+        int nv = num_verts[cs];
+        if (nv < 0 || nv > 15 || nv % 3) { c->err = "set_mc_tables: a vertex count is not 0..15 in steps of 3"; return MP_ERR_ARG; }
+        for (int t = 0; t < nv; t++) {
+            int e = tri[cs * 16 + t];
+            if (e < 0 || e > 11 || ((cs >> kEdge[e][0]) & 1) == ((cs >> kEdge[e][1]) & 1)) {
+                c->err = "set_mc_tables: a triangle uses an edge its case does not cross";
+                return MP_ERR_ARG;
+            }
+        }
+    }
+    MP_CUDA(c, cudaMemcpyAsync(c->mc_numverts, num_verts, sizeof(int32_t) * 256, cudaMemcpyHostToDevice, c->stream));
+    MP_CUDA(c, cudaMemcpyAsync(c->mc_tri, tri, sizeof(int32_t) * 256 * 16, cudaMemcpyHostToDevice, c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
+}
+
 // ---------------------------------------------------------------------------
 // kernel timing
 // ---------------------------------------------------------------------------

@@ -266,6 +266,13 @@ int mp_set_tables(void* ctx, const float* randfloat, int nrand,
 /* Marching-cubes case tables this build uses (numVerts[256], tri[256*16],
  * edge[256]); generated, not copied (see mc_tables.cpp). */
 int mp_mc_tables(int32_t* num_verts, int32_t* tri, int32_t* edge);
+/* Replaces the context's marching-cubes case tables (numVerts[256],
+ * tri[256*16]) for its later extractions, e.g. with the reference's own
+ * tables.h (spray_k.cu reads them through edgeTex/triTex/numVertsTex,
+ * spray_k.cu:2262-2277) to reproduce its triangulation.  Every count must be
+ * 0..15 in steps of 3 and every listed edge one that the case crosses
+ * (MP_ERR_ARG otherwise). */
+int mp_set_mc_tables(void* ctx, const int32_t* num_verts, const int32_t* tri);
 
 /* ---- scene set-up (cspray::init, spray.cpp:628-670) -------------------- */
 

@@ -65,9 +65,11 @@ def reference_mode(mp, config, n, seed):
 
 
 def copy_state(src, dst):
-    for f in CELL_FIELDS + FACE_FIELDS + ["cellstart", "cellend"]:
+    for f in CELL_FIELDS + FACE_FIELDS:
         dst.set_field(f, src.get_field(f))
     dst.upload_particles(**src.download_particles())
+    for f in ("cellstart", "cellend"):          # after the particles: the ranges index them
+        dst.set_field(f, src.get_field(f))
     dst.set_state(src.state())
 
 
@@ -200,3 +202,40 @@ def test_marching_cubes_equals_the_reference_kernels(mp, oracle_mod, refhost, co
                 sv, sn = ref.smooth_and_normals(*unsmoothed[surf], 1, p.smooth_iters)
                 assert np.array_equal(sv, ov) and np.array_equal(sn, on), f"smoothing surface {surf}"
     assert any(len(m[0]) for m in unsmoothed.values())
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_marching_cubes_with_the_reference_tables(mp, oracle_mod, refhost, config):
+    """With the reference's own case tables (tables.h, read here as data and
+    given to the oracle, as mp_set_mc_tables gives them to the library) the
+    extraction reproduces the reference's meshes: the same index lists, bit
+    for bit, and the vertices within the 2e-6 voxel of the shared-edge race;
+    normals follow to rounding."""
+    from test_mc_tables import _parse_reference
+    _, ref_tri, ref_nv = _parse_reference()
+    p, parts, rf, seeds = reference_mode(mp, config, N, 2017_770 + config)
+    p.b_smooth_mc = 0
+    _, bad, orc0 = run_pair(mp, oracle_mod, refhost, config, N, 2017_770 + config, frames=1)
+    assert not bad
+    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=(ref_nv.astype(np.int32),
+                                                                   ref_tri.reshape(-1).astype(np.int32)))
+    copy_state(orc0, orc)
+    ref = refhost.RefHost(p, mp.FIELD_ID, mp.MPState)
+    copy_state(orc, ref)
+    ref.run("preMC")
+    orc.preMC()
+    vs = p.cellsize / 2
+    meshes = 0
+    for surf in (mp.MC_SOLID, mp.MC_FLUID, mp.MC_GAS):
+        ref.runMC(surf)
+        orc.runMC(surf)
+        rv, rn, ri = ref.mc_mesh(surf)
+        ov, on, oi = orc.mc_mesh(surf)
+        assert np.array_equal(ri, oi), f"indices surface {surf}"
+        if len(ov):
+            meshes += 1
+            assert np.abs(rv.astype(np.float64) - ov).max() <= 2e-6 * vs
+            _, n0 = ref.smooth_and_normals(ov, oi, 0, 0)
+            assert np.array_equal(n0, on)
+            assert np.abs(rn - on).max() < 1e-3
+    assert meshes >= 1
