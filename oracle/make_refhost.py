@@ -52,7 +52,7 @@ KERNELS = [
     "pouringwater", "computeSolidVertex_k", "computePosSolid_k", "computeVelSolid_k",
     "set_nonsolid_2_zero", "setVelZeroSolid_k", "solidCollisionWithBound", "compute_cI_k",
     "cptdivergence", "computeAx", "pcg_op", "mapvelg2p_flip",
-    "advectparticle_RK2", "flipAirVacuum", "markfluid", "markair",
+    "advectparticle_RK2", "flipAirVacuum", "markfluid", "markair", "initHeatParticle", "initsolubility_k",
     "reorderDataAndFindCellStartD", "compactVoxels", "markActiveEdge_MC", "generateTriangles_indices",
     "smooth_computedisplacement", "smooth_addDisplacement", "calnormal_k", "normalizeTriangleNor_k",
 ]

@@ -101,3 +101,13 @@ def test_pouring(mp, oracle_mod, refhost, scene, frames):
         poured = orc.state().par_num_now - n0
         every = 6 if (scene == "INTERACTION" and f >= 2) else 4
         assert poured == (len(ppos) if f % every == 0 else 0)
+
+
+@pytest.mark.parametrize("config", [2, 3])
+def test_particle_heat_initialisation(mp, oracle_mod, refhost, config):
+    """initTemperature + initSolubility (spray.cu:1989-1999): initHeatParticle
+    and initsolubility_k, and the SOLID count the step starts from."""
+    p, orc, ref, _ = _pair(mp, oracle_mod, refhost, config, 2017_790 + config)
+    assert not _stage(orc, ref, ("initHeatAndSolubility",))
+    assert ref.n_real_solid == orc.state().n_real_solpoint
+    assert (orc.download_particles()["solubility"] > 0).any()
