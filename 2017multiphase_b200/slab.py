@@ -77,12 +77,56 @@ def owner_of_planes(i: np.ndarray, bounds: Sequence[Tuple[int, int]]) -> np.ndar
     return np.searchsorted(starts, np.asarray(i), side="right") - 1
 
 
+def hash_cells(pos: np.ndarray, cellsize: float, gmin: Sequence[float], dims: Sequence[int]) -> np.ndarray:
+    """calcHashD's cell index of each particle (getijkfrompos, spray_k.cu:51-57,
+    and getidx): (pos - gmin) / cellsize per axis in float32, truncated, an
+    axis outside the grid giving 0."""
+    p = np.asarray(pos, np.float32).reshape(-1, 3)
+    ijk = []
+    for a in range(3):
+        u = (p[:, a] - np.float32(gmin[a])) / np.float32(cellsize)
+        ijk.append(np.where((u >= 0) & (u < dims[a]), u.astype(np.int64), 0))
+    return (ijk[0] * dims[1] + ijk[1]) * dims[2] + ijk[2]
+
+
 def route_particles(pos: np.ndarray, cellsize: float, gmin_x: float, nx: int,
                     bounds: Sequence[Tuple[int, int]]) -> np.ndarray:
     """The owning rank of each particle (float32 positions, (n, 3))."""
     x = (np.asarray(pos, np.float32)[:, 0] - np.float32(gmin_x)) / np.float32(cellsize)
     i = np.where((x >= 0) & (x < nx), x.astype(np.int64), 0)
     return owner_of_planes(i, bounds)
+
+
+def migrate(arrays: dict, owner: np.ndarray, world: int) -> dict:
+    """Moves particles to the ranks `owner` names, over torch.distributed
+    all-to-all.  Every rank receives the particles sent to it in source-rank
+    order, each source's in its own order.  A rank's slice of the previous
+    (cell-sorted) particle array is in global order, and slabs follow in rank
+    order, so the received particles are in the global previous order.  A
+    local stable sort by cell then gives the slab exactly its part of the
+    single-domain stable sort."""
+    import torch
+    import torch.distributed as dist
+    owner = np.asarray(owner, np.int64)
+    order = np.argsort(owner, kind="stable")
+    send_counts = torch.from_numpy(np.bincount(owner, minlength=world).astype(np.int64))
+    recv_counts = torch.empty(world, dtype=torch.int64)
+    dist.all_to_all_single(recv_counts, send_counts)
+    sc, rc = send_counts.tolist(), recv_counts.tolist()
+    out = {}
+    for name, a in arrays.items():
+        a = np.ascontiguousarray(np.asarray(a)[order])
+        w = a.dtype.itemsize * int(np.prod(a.shape[1:], dtype=np.int64))     # bytes per particle
+        b = a.view(np.uint8).reshape(len(a), w)
+        pad = (-w) % 4                                                      # sent as int32 words
+        if pad:
+            b = np.concatenate([b, np.zeros((len(b), pad), np.uint8)], axis=1)
+        send = torch.from_numpy(np.ascontiguousarray(b).view(np.int32))
+        recv = torch.empty((sum(rc), send.shape[1]), dtype=torch.int32)
+        dist.all_to_all_single(recv, send, rc, sc)
+        rb = np.ascontiguousarray(recv.numpy().view(np.uint8)[:, :w])
+        out[name] = rb.view(a.dtype).reshape((sum(rc),) + a.shape[1:])
+    return out
 
 
 def block_range(x0: int, x1: int, ny: int, nz: int, block: int = BLOCK) -> Tuple[int, int]:

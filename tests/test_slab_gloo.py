@@ -201,3 +201,91 @@ def test_slab_cg_equals_the_single_domain_solve(mp, oracle_mod, tmp_path, world)
     assert iters == {it} and it > 0
     ref = o.get_field("press").reshape(shape)
     assert np.array_equal(press, ref), f"max |d| {np.abs(press - ref).max()}"
+
+
+# ---- particle migration -----------------------------------------------------------
+
+PARTS = ["pos", "vel", "flag", "mass", "temp", "lheat", "solubility", "gascontain"]
+
+
+def _migrate_worker(rank, world, port, inp, outdir):
+    import sys
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import importlib
+    sl = importlib.import_module("2017multiphase_b200.slab")
+    d = np.load(inp)
+    dims = tuple(int(x) for x in d["dims"])
+    nx, ny, nz = dims
+    x0, x1 = sl.partition(nx, ny, nz, world)[rank]
+    g0, g1 = x0 * ny * nz, x1 * ny * nz
+    mine = (d["old_cell"] >= g0) & (d["old_cell"] < g1)          # this rank's particles before the move
+    arrays = {k: d[k][mine] for k in PARTS}
+    owner = sl.route_particles(arrays["pos"], float(d["h"]), float(d["gmin"][0]), nx, sl.partition(nx, ny, nz, world))
+    got = sl.migrate(arrays, owner, world)
+    cell = sl.hash_cells(got["pos"], float(d["h"]), d["gmin"], dims)
+    assert ((cell >= g0) & (cell < g1)).all()
+    order = np.argsort(cell, kind="stable")                       # sortParticles, on the slab
+    out = {k: v[order] for k, v in got.items()}
+    cs = cell[order]
+    start = np.full(g1 - g0, 0xFFFFFFFF, np.uint32)
+    end = np.zeros(g1 - g0, np.uint32)
+    for q in range(len(cs)):                                      # reorderDataAndFindCellStartD, by definition
+        if q == 0 or cs[q] != cs[q - 1]:
+            start[cs[q] - g0] = q
+            if q > 0:
+                end[cs[q - 1] - g0] = q
+        if q == len(cs) - 1:
+            end[cs[q] - g0] = q + 1
+    np.savez(os.path.join(outdir, f"m{rank}.npz"), start=start, end=end, g0=g0, g1=g1, n=len(cs), **out)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_migration_and_local_sort_equal_the_global_sort(mp, oracle_mod, tmp_path, world):
+    """After collision and advection moved the particles, each rank sends its
+    particles to the slab of their new cell and sorts what it holds: the
+    result is, slab by slab, the single-domain hashAndSortParticles (particle
+    order, every attribute, cell ranges)."""
+    from parity_util import bubblesim_stages
+    p = mp.scene_params(1, 32)
+    o = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    o.upload_particles(**mp.scene_particles(p, 1, 2017_920))
+    rf, seeds = mp.scene_tables(p, 1, 2017_920)
+    o.set_tables(rf, seeds)
+    for st in bubblesim_stages(p, 0):
+        getattr(o, st[0])(*st[1:])
+        if st[0] == "CollisionSolid":
+            break
+    before = o.download_particles()
+    cs, ce = o.get_field("cellstart"), o.get_field("cellend")     # the sort before the move
+    old_cell = np.zeros(len(before["pos"]), np.int64)
+    for c in np.nonzero(cs != 0xFFFFFFFF)[0]:
+        old_cell[cs[c]:ce[c]] = c
+    inp = tmp_path / "in.npz"
+    np.savez(inp, dims=np.array([p.nx, p.ny, p.nz]), h=p.cellsize, gmin=np.array([p.gmin_x, p.gmin_y, p.gmin_z]),
+             old_cell=old_cell, **before)
+    tmp.spawn(_migrate_worker, args=(world, _free_port(), str(inp), str(tmp_path)), nprocs=world, join=True)
+    o.hashAndSortParticles()
+    after = o.download_particles()
+    gcs, gce = o.get_field("cellstart"), o.get_field("cellend")
+    off = 0
+    for r in range(world):
+        d = np.load(tmp_path / f"m{r}.npz")
+        n, g0, g1 = int(d["n"]), int(d["g0"]), int(d["g1"])
+        for k in PARTS:
+            assert np.array_equal(d[k], after[k][off:off + n]), (r, k)
+        occ = gcs[g0:g1] != 0xFFFFFFFF
+        assert np.array_equal(d["start"] != 0xFFFFFFFF, occ)
+        assert np.array_equal(d["start"][occ].astype(np.int64) + off, gcs[g0:g1][occ])
+        assert np.array_equal(d["end"][occ].astype(np.int64) + off, gce[g0:g1][occ])
+        off += n
+    assert off == len(after["pos"])
+    sl = _slab()
+    bounds = sl.partition(p.nx, p.ny, p.nz, world)
+    old_rank = sl.owner_of_planes(old_cell // (p.ny * p.nz), bounds)
+    new_rank = sl.route_particles(before["pos"], p.cellsize, p.gmin_x, p.nx, bounds)
+    assert (old_rank != new_rank).sum() > 0            # particles did cross slab boundaries
