@@ -127,6 +127,14 @@ def test_every_stage_equals_the_reference_kernels(mp, oracle_mod, refhost, confi
         assert {"markgrid_bubble", "MeltSolid", "Freezing"} <= names
 
 
+def test_every_stage_equals_the_reference_kernels_at_32(mp, oracle_mod, refhost):
+    """The bubble column at 32^3 (the benchmark's configuration at a size the
+    emulated kernels finish in seconds), one frame."""
+    checked, bad, _ = run_pair(mp, oracle_mod, refhost, 5, 32, 2017_705, frames=1)
+    assert not bad, bad
+    assert len(checked) >= 25
+
+
 def test_in_place_kernels_write_only_their_own_element(mp, oracle_mod, refhost):
     """The Jacobi launches assume that each thread writes only its own element;
     checked thread by thread on the kernels that use them."""
