@@ -33,3 +33,14 @@ def has_gpu():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+@pytest.fixture(scope="session")
+def refhost():
+    """The reference's own kernels compiled for the host (oracle/make_refhost.py),
+    built once per session from the reference tree; tests that use it skip
+    themselves when the tree is absent."""
+    from oracle import make_refhost
+    make_refhost.build(quiet=True)
+    from oracle import refhost as rh
+    return rh

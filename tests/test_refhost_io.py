@@ -14,7 +14,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from test_refhost_stages import SRC, refhost  # noqa: F401  (fixture)
+from test_refhost_stages import SRC
 
 pytestmark = pytest.mark.skipif(not os.path.exists(SRC + "/spray_k.cu"), reason="reference source tree not present")
 

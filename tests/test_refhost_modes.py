@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from parity_util import bubblesim_stages, compare, snapshot
-from test_refhost_stages import SRC, copy_state, reference_mode, refhost  # noqa: F401  (fixture)
+from test_refhost_stages import SRC, copy_state, reference_mode
 
 pytestmark = pytest.mark.skipif(not __import__("os").path.exists(SRC + "/spray_k.cu"),
                                 reason="reference source tree not present")

@@ -35,14 +35,6 @@ TEMPERATURES = ["default_temperature", "temperature0", "melting_point", "boiling
 N = 16
 
 
-@pytest.fixture(scope="module")
-def refhost():
-    from oracle import make_refhost
-    make_refhost.build(SRC, quiet=True)
-    from oracle import refhost as rh
-    return rh
-
-
 def reference_mode(mp, config, n, seed):
     """Parameters, particles and tables of a configuration in the reference's modes."""
     p = mp.scene_params(config, n)
