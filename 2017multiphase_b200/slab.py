@@ -161,6 +161,25 @@ def combine_blocks(total_blocks: int, b0: int, partials: np.ndarray, all_reduce=
     return s
 
 
+def combine_blocks_many(total_blocks: int, b0: int, partials: Sequence[np.ndarray], all_reduce=None) -> List[float]:
+    """Several dot products from one all-reduce: the block vectors of each are
+    stacked, reduced together and each added in block order (a CG that needs
+    two dot products per iteration pays one reduction's latency for both)."""
+    v = np.zeros((len(partials), total_blocks))
+    for q, part in enumerate(partials):
+        v[q, b0:b0 + len(part)] = part
+    flat = v.reshape(-1)
+    if all_reduce is not None:
+        all_reduce(flat)
+    out = []
+    for q in range(len(partials)):
+        s = 0.0
+        for x in flat[q * total_blocks:(q + 1) * total_blocks]:
+            s += x
+        out.append(s)
+    return out
+
+
 def exchange_ghosts(ext, rank: int, world: int, width: int = 1) -> None:
     """Fills the `width` ghost planes on each side of `ext` (a tensor of shape
     (owned planes + 2*width, ny, nz)) with the neighbouring ranks' edge planes,

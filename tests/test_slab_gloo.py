@@ -99,7 +99,7 @@ def _apply_A(x_ext, m_ext, h2):
     return np.where((m == TF) | (m == TA), out, np.float32(0)).astype(np.float32)
 
 
-def _worker(rank, world, port, inp, outdir):
+def _worker(rank, world, port, inp, outdir, pipelined=False):
     import sys
     import torch
     import torch.distributed as dist
@@ -130,8 +130,14 @@ def _worker(rank, world, port, inp, outdir):
         sl.exchange_ghosts(ext, rank, world)
         return _apply_A(e, m_ext, h2)
 
+    n_reduce = [0]
+
+    def count(v):
+        n_reduce[0] += 1
+        sl.torch_all_reduce(v)
+
     def dot(u, v):
-        return sl.combine_blocks(nblk, b0, sl.block_partials(u, v), sl.torch_all_reduce)
+        return sl.combine_blocks(nblk, b0, sl.block_partials(u, v), count)
 
     x = np.zeros((nl, ny, nz), np.float32)
     z = A(x)
@@ -139,7 +145,33 @@ def _worker(rank, world, port, inp, outdir):
     rr = dot(r, r)
     eps = float(np.float32(d["tol"]) * np.float32(mark.size))
     k = 0
-    if not rr < eps:
+    if pipelined and not rr < eps:
+        # Chronopoulos-Gear: one all-reduce per iteration for both dot products
+        def dots2(u, v, w, t):
+            return sl.combine_blocks_many(nblk, b0, [sl.block_partials(u, v), sl.block_partials(w, t)], count)
+        u = r.copy()
+        w = A(u)
+        gamma, delta = dots2(r, u, w, u)
+        p, s = u.copy(), w.copy()
+        alpha = gamma / delta
+        while True:
+            af = np.float32(alpha)
+            x = np.where(mask, x + af * p, np.float32(0)).astype(np.float32)
+            r = np.where(mask, r + (-af) * s, np.float32(0)).astype(np.float32)
+            k += 1
+            u = r
+            w = A(u)
+            gamma_new, delta = dots2(r, u, w, u)
+            if gamma_new < eps or k >= int(d["maxiter"]):
+                rr = gamma_new
+                break
+            beta = gamma_new / gamma
+            alpha = gamma_new / (delta - beta * gamma_new / alpha)
+            gamma = gamma_new
+            bf = np.float32(beta)
+            p = np.where(mask, u + bf * p, np.float32(0)).astype(np.float32)
+            s = np.where(mask, w + bf * s, np.float32(0)).astype(np.float32)
+    elif not rr < eps:
         p = r.copy()
         a = rr
         while True:
@@ -160,7 +192,7 @@ def _worker(rank, world, port, inp, outdir):
             p = np.where(mask, r + bf * p, np.float32(0)).astype(np.float32)
             a = rr
             k += 1
-    np.savez(os.path.join(outdir, f"x{rank}.npz"), x=x, x0=x0, x1=x1, iters=k, rr=rr)
+    np.savez(os.path.join(outdir, f"x{rank}.npz"), x=x, x0=x0, x1=x1, iters=k, rr=rr, reductions=n_reduce[0])
     dist.barrier()
     dist.destroy_process_group()
 
@@ -173,8 +205,9 @@ def _free_port():
     return port
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_slab_cg_equals_the_single_domain_solve(mp, oracle_mod, tmp_path, world):
+def _projection_system(mp, oracle_mod, tmp_path):
+    """The pressure system of configuration 1 at 32^3 before its projection, and
+    the oracle's single-domain solve of it."""
     from parity_util import bubblesim_stages
     p = mp.scene_params(1, 32)
     p.cg_tol_mode, p.cg_tol, p.cg_max_iter = mp.TOL_REF_ABS, 0.01, 800
@@ -191,16 +224,43 @@ def test_slab_cg_equals_the_single_domain_solve(mp, oracle_mod, tmp_path, world)
     inp = tmp_path / "in.npz"
     np.savez(inp, mark=o.get_field("mark").reshape(shape), div=o.get_field("div").reshape(shape), h=p.cellsize,
              tol=p.cg_tol, maxiter=p.cg_max_iter)
-    tmp.spawn(_worker, args=(world, _free_port(), str(inp), str(tmp_path)), nprocs=world, join=True)
+    return inp, shape, it, o.get_field("press").reshape(shape)
+
+
+def _gather(tmp_path, world, shape):
     press = np.zeros(shape, np.float32)
-    iters = set()
+    iters, reductions = set(), set()
     for r in range(world):
         d = np.load(tmp_path / f"x{r}.npz")
         press[int(d["x0"]):int(d["x1"])] = d["x"]
         iters.add(int(d["iters"]))
-    assert iters == {it} and it > 0
-    ref = o.get_field("press").reshape(shape)
+        reductions.add(int(d["reductions"]))
+    assert len(iters) == 1 and len(reductions) == 1
+    return press, iters.pop(), reductions.pop()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_slab_cg_equals_the_single_domain_solve(mp, oracle_mod, tmp_path, world):
+    inp, shape, it, ref = _projection_system(mp, oracle_mod, tmp_path)
+    tmp.spawn(_worker, args=(world, _free_port(), str(inp), str(tmp_path)), nprocs=world, join=True)
+    press, iters, reductions = _gather(tmp_path, world, shape)
+    assert iters == it and it > 0
+    assert reductions == 2 * it + 1                  # r.r at the start, z.p and r.r per iteration
     assert np.array_equal(press, ref), f"max |d| {np.abs(press - ref).max()}"
+
+
+def test_single_reduction_cg_on_slabs(mp, oracle_mod, tmp_path):
+    """The Chronopoulos-Gear form of the CG, which computes both dot products
+    of an iteration in one all-reduce: half the reductions (the latency that
+    bounds a decomposed solve), the same iteration count within two, and the
+    pressure within 1e-5 of the single-domain solve."""
+    inp, shape, it, ref = _projection_system(mp, oracle_mod, tmp_path)
+    tmp.spawn(_worker, args=(2, _free_port(), str(inp), str(tmp_path), True), nprocs=2, join=True)
+    press, iters, reductions = _gather(tmp_path, 2, shape)
+    assert abs(iters - it) <= 2
+    assert reductions == iters + 2                   # r.r and the first pair at the start, one per iteration
+    scale = np.abs(ref).max()
+    assert np.abs(press.astype(np.float64) - ref).max() <= 1e-5 * scale
 
 
 # ---- particle migration -----------------------------------------------------------
