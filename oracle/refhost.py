@@ -27,7 +27,8 @@ class RHState(C.Structure):
     _fields_ = [("f", C.c_void_p * 45), ("np", C.c_int32), ("cap", C.c_int32), ("frame", C.c_int32),
                 ("n_real_solid", C.c_int32), ("randfloat", C.c_void_p), ("nrand", C.c_int32),
                 ("seeds", C.c_void_p), ("nseed", C.c_int32), ("iters", C.c_int32), ("residual", C.c_double),
-                ("capped", C.c_int32), ("pour_pos", C.c_void_p), ("pour_vel", C.c_void_p), ("npour", C.c_int32)]
+                ("capped", C.c_int32), ("pour_pos", C.c_void_p), ("pour_vel", C.c_void_p), ("npour", C.c_int32),
+                ("solid_verts", C.c_void_p), ("nsolid_verts", C.c_int32), ("run_mc_solid", C.c_int32)]
 
 
 class RHMesh(C.Structure):
@@ -87,6 +88,7 @@ class RefHost:
         self.mesh = {}
         self.pour_pos = np.zeros((0, 3), np.float32)
         self.pour_vel = np.zeros((0, 3), np.float32)
+        self.solid_verts = np.zeros((0, 3), np.float32)   # the kept solid surface solidmotion moves
         self.dens = np.zeros((2 * nx + 1) * (2 * ny + 1) * (2 * nz + 1), np.float32)
         self.voxel_verts = np.zeros(8 * n, np.uint32)
 
@@ -145,6 +147,8 @@ class RefHost:
         st.randfloat, st.nrand = self.rf.ctypes.data, self.rf.size
         st.seeds, st.nseed = self.seeds.ctypes.data, self.seeds.size
         st.pour_pos, st.pour_vel, st.npour = self.pour_pos.ctypes.data, self.pour_vel.ctypes.data, len(self.pour_pos)
+        st.solid_verts, st.nsolid_verts = self.solid_verts.ctypes.data, len(self.solid_verts)
+        st.run_mc_solid = self.params.b_run_mc_solid
         return st
 
     def run(self, name, arg=0.0):

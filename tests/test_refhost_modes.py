@@ -111,3 +111,30 @@ def test_particle_heat_initialisation(mp, oracle_mod, refhost, config):
     assert not _stage(orc, ref, ("initHeatAndSolubility",))
     assert ref.n_real_solid == orc.state().n_real_solpoint
     assert (orc.download_particles()["solubility"] > 0).any()
+
+
+def test_kept_solid_surface_moves_with_the_solid(mp, oracle_mod, refhost):
+    """runMC_interaction keeps the solid surface extracted at frame 0 when
+    bRunMCSolid is off, and solidmotion moves it with computeSolidVertex_k
+    (spray.cu:2770-2772, spray_k.cu:5254-5263): the moved vertices equal the
+    reference's, bit for bit, with the particles."""
+    p, orc, ref, _ = _pair(mp, oracle_mod, refhost, 3, 2017_795, scene=mp.SCENE_MELTANDBOIL, b_fix_solid=0,
+                           b_run_mc_solid=0, b_run_mc=1)
+    for st in bubblesim_stages(p, 0):
+        getattr(orc, st[0])(*st[1:])
+    orc.preMC()
+    orc.runMC(mp.MC_SOLID)                         # the surface kept from frame 0
+    kept = orc.mc_mesh(mp.MC_SOLID)[0]
+    assert len(kept) > 0
+    s = orc.state()
+    s.frame = 1
+    orc.set_state(s)
+    for st in bubblesim_stages(p, 1):
+        if st[0] == "solidmotion":
+            ref.solid_verts = kept.copy()
+            assert not _stage(orc, ref, st)
+            moved = orc.mc_mesh(mp.MC_SOLID)[0]
+            assert np.array_equal(ref.solid_verts, moved)
+            assert np.abs(moved - kept).max() > 0
+            break
+        getattr(orc, st[0])(*st[1:])
