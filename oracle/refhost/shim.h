@@ -6,8 +6,8 @@
 //
 //   * __global__/__device__/__constant__ are plain C++; threadIdx, blockIdx,
 //     blockDim and gridDim are thread-local globals that host_launch() sets
-//     per emulated thread (host_launch_sync() runs a block's threads
-//     concurrently, for the kernels that call __syncthreads);
+//     per emulated thread (host_launch_sync() runs a block's threads as
+//     cooperative fibers, for the kernels that call __syncthreads);
 //   * helper_math.h's float3 arithmetic (a CUDA samples header the reference
 //     includes, not present here) is restated with the same operation order
 //     (componentwise, one rounding per operation);
@@ -35,8 +35,8 @@
 #include <cstdint>
 #include <algorithm>
 #include <vector>
-#include <thread>
-#include <pthread.h>
+#include <functional>
+#include <ucontext.h>
 
 static thread_local uint3 threadIdx, blockIdx;
 static thread_local dim3 blockDim, gridDim;
@@ -60,33 +60,60 @@ static void host_launch(dim3 grid, dim3 block, F&& f) {
 }
 
 // A launch of a kernel that synchronises its block (__syncthreads over
-// shared memory): one host thread per CUDA thread of a one-dimensional block,
-// the blocks one after another, a barrier for __syncthreads and between
-// blocks.  Shared arrays declared `extern __shared__` are host globals
+// shared memory): each CUDA thread of the one-dimensional block is a
+// cooperative fiber (ucontext) on this host thread; the fibers run in thread
+// order up to their next __syncthreads, one round after another, so every
+// thread reaches a barrier before any passes it.  The blocks run one after
+// another.  Shared arrays declared `extern __shared__` are host globals
 // (globals.inc); a `__shared__` array inside a kernel becomes a local array of
 // each thread, which is what kernels that only use their own slots need.
-static pthread_barrier_t* rh_bar = nullptr;
+static bool rh_in_fiber = false;
+static ucontext_t rh_sched;
+static std::vector<ucontext_t> rh_fiber;
+static std::vector<char> rh_fiber_done;
+static unsigned rh_cur = 0;
+static std::function<void()> rh_fiber_fn;
+static void rh_fiber_entry() {
+    unsigned t = rh_cur;
+    rh_fiber_fn();
+    rh_fiber_done[t] = 1;          // returns to rh_sched through uc_link
+}
+static inline void __syncthreads() {
+    if (rh_in_fiber) swapcontext(&rh_fiber[rh_cur], &rh_sched);
+}
 template <class F>
 static void host_launch_sync(unsigned grid, unsigned block, F&& f) {
-    pthread_barrier_t bar;
-    pthread_barrier_init(&bar, nullptr, block);
-    rh_bar = &bar;
-    std::vector<std::thread> ts;
-    ts.reserve(block);
-    for (unsigned t = 0; t < block; t++)
-        ts.emplace_back([&, t] {
-            gridDim = dim3(grid);
-            blockDim = dim3(block);
-            threadIdx = make_uint3(t, 0, 0);
-            for (unsigned b = 0; b < grid; b++) {
-                blockIdx = make_uint3(b, 0, 0);
-                f();
-                pthread_barrier_wait(&bar);
+    static std::vector<std::vector<char>> stacks;
+    const size_t stack_bytes = 64 * 1024;
+    if (stacks.size() < block) stacks.resize(block);
+    for (auto& st : stacks) if (st.size() < stack_bytes) st.assign(stack_bytes, 0);
+    rh_fiber.assign(block, ucontext_t());
+    rh_fiber_fn = f;
+    gridDim = dim3(grid);
+    blockDim = dim3(block);
+    for (unsigned b = 0; b < grid; b++) {
+        blockIdx = make_uint3(b, 0, 0);
+        rh_fiber_done.assign(block, 0);
+        for (unsigned t = 0; t < block; t++) {
+            getcontext(&rh_fiber[t]);
+            rh_fiber[t].uc_stack.ss_sp = stacks[t].data();
+            rh_fiber[t].uc_stack.ss_size = stack_bytes;
+            rh_fiber[t].uc_link = &rh_sched;
+            makecontext(&rh_fiber[t], rh_fiber_entry, 0);
+        }
+        rh_in_fiber = true;
+        for (bool all_done = false; !all_done;) {
+            all_done = true;
+            for (unsigned t = 0; t < block; t++) {
+                if (rh_fiber_done[t]) continue;
+                rh_cur = t;
+                threadIdx = make_uint3(t, 0, 0);
+                swapcontext(&rh_sched, &rh_fiber[t]);
+                all_done = all_done && rh_fiber_done[t];
             }
-        });
-    for (auto& th : ts) th.join();
-    rh_bar = nullptr;
-    pthread_barrier_destroy(&bar);
+        }
+        rh_in_fiber = false;
+    }
 }
 
 static inline int __mul24(int a, int b) { return a * b; }
@@ -136,7 +163,6 @@ static inline int atomicMax(int* a, int v) { int o = *a; if (v > o) *a = v; retu
 static inline int atomicMin(int* a, int v) { int o = *a; if (v < o) *a = v; return o; }
 static inline int __float_as_int(float f) { int i; memcpy(&i, &f, 4); return i; }
 static inline float __int_as_float(int i) { float f; memcpy(&f, &i, 4); return f; }
-static inline void __syncthreads() { if (rh_bar) pthread_barrier_wait(rh_bar); }
 
 struct HostTex { const unsigned* p = nullptr; };
 template <class T> static inline T tex1Dfetch(const HostTex& t, int i) { return (T)t.p[i]; }
