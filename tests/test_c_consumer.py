@@ -34,6 +34,9 @@ int main(int argc, char** argv) {
     uint32_t idx[3] = {0, 1, 2};
     if (mp_write_mesh(MP_OUT_OBJ_MESH, argv[1], "water", verts, nrm, 3, idx, 3) != MP_OK) return 6;
     if (mp_write_mesh(MP_OUT_OBJ_MESH, "/nonexistent-dir/x.obj", "water", verts, nrm, 3, idx, 3) != MP_ERR_IO) return 7;
+    int32_t nvt[256], tri[256 * 16], edge[256];
+    if (mp_mc_tables(nvt, tri, edge) != MP_OK || nvt[1] != 3) return 8;
+    if (mp_set_mc_tables(NULL, nvt, tri) != MP_ERR_ARG) return 9;      /* no context: refused, no GPU needed */
     printf("%d %.9g %.9g %.9g\n", n, pos[0], pos[1], pos[2]);
     return 0;
 }
