@@ -269,3 +269,33 @@ def test_fp64_cg_scalars_against_the_reference_float_reductions(mp, oracle_mod, 
             return
         getattr(orc, st[0])(*st[1:])
     pytest.fail("no projection in the step")
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_the_reference_sweeps_depend_on_thread_order(mp, oracle_mod, refhost, config):
+    """Why the oracle defines the in-place sweeps as Jacobi passes: the
+    reference's sweepphibytype (spray_k.cu:771-788) reads neighbours that other
+    threads of the same launch overwrite, so its result depends on the order in
+    which threads run.  Run in place with the threads in ascending order (one
+    order a GPU may take), sweepLSAndMardGrid's level set differs from the
+    Jacobi result by up to a few cells (measured at 32^3: 2.1 cells in
+    configuration 1, 2.8 and 60 flipped cell marks out of 32768 in
+    configuration 5).  Both are results the reference can give; the oracle
+    and the GPU take the one that does not depend on scheduling."""
+    p, parts, rf, seeds = reference_mode(mp, config, 32, 55)
+    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    orc.upload_particles(**parts)
+    orc.set_tables(rf, seeds)
+    ref = refhost.RefHost(p, mp.FIELD_ID, mp.MPState)
+    ref.set_tables(rf, seeds)
+    for st in bubblesim_stages(p, 0):
+        if st[0] == "sweepLSAndMardGrid":
+            copy_state(orc, ref)
+            ref.run("sweepLSAndMardGrid_inplace")
+            orc.sweepLSAndMardGrid()
+            a, b = snapshot(ref), snapshot(orc)
+            d = np.abs(a["lsmerge"].astype(np.float64) - b["lsmerge"]) / p.cellsize
+            assert 0 < d.max() < 5          # differs, within the five passes' reach
+            assert (a["mark"] != b["mark"]).mean() < 0.01
+            return
+        getattr(orc, st[0])(*st[1:])
