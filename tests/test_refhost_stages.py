@@ -326,3 +326,21 @@ def test_the_reference_drag_depends_on_thread_order(mp, oracle_mod, refhost):
             assert max(rel_err(a[f], b[f]) for f in ("waterux", "wateruy", "wateruz")) < 1e-6
             return
         getattr(orc, st[0])(*st[1:])
+
+
+def test_sphere_field_equals_the_reference_kernel(mp, oracle_mod, refhost):
+    """genSphereDensfield (spray_k.cu:1828-1848): the oracle's analytic sphere
+    density equals the reference kernel's, node for node."""
+    import ctypes as C
+    p = mp.scene_params(1, 16)
+    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    center, radius = (0.5 * 16 * p.cellsize, 0.48 * 16 * p.cellsize, 0.52 * 16 * p.cellsize), 0.3 * 16 * p.cellsize
+    orc.runMC_sphere(mp.MC_FLUID, center, radius)
+    dens = orc.mc_field()[0]
+    ref = np.zeros_like(dens)
+    lib = refhost.load()
+    lib.rh_sphere_dens.argtypes = [C.c_void_p, C.c_void_p] + [C.c_float] * 4
+    lib.rh_sphere_dens.restype = None
+    lib.rh_sphere_dens(C.addressof(p), ref.ctypes.data, *[C.c_float(x) for x in center], C.c_float(radius))
+    assert np.array_equal(ref, dens)
+    assert (dens > 0).any() and (dens < 0).any()
