@@ -35,9 +35,13 @@ TEMPERATURES = ["default_temperature", "temperature0", "melting_point", "boiling
 N = 16
 
 
-def reference_mode(mp, config, n, seed):
-    """Parameters, particles and tables of a configuration in the reference's modes."""
+def reference_mode(mp, config, n, seed, dims=None):
+    """Parameters, particles and tables of a configuration in the reference's
+    modes (on an nx x ny x nz grid of the same cell size when dims is given)."""
     p = mp.scene_params(config, n)
+    if dims is not None:
+        p.nx, p.ny, p.nz = dims
+        p.par_num_max = 16 * dims[0] * dims[1] * dims[2]
     p.flip_alpha = 1.0
     p.cg_tol_mode = mp.TOL_REF_ABS
     p.cg_tol = 0.01
@@ -65,8 +69,8 @@ def copy_state(src, dst):
     dst.set_state(src.state())
 
 
-def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2):
-    p, parts, rf, seeds = reference_mode(mp, config, n, seed)
+def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2, dims=None):
+    p, parts, rf, seeds = reference_mode(mp, config, n, seed, dims)
     orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
     orc.upload_particles(**parts)
     orc.set_tables(rf, seeds)
@@ -125,6 +129,15 @@ def test_every_stage_equals_the_reference_kernels_at_32(mp, oracle_mod, refhost)
     checked, bad, _ = run_pair(mp, oracle_mod, refhost, 5, 32, 2017_705, frames=1)
     assert not bad, bad
     assert len(checked) >= 25
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_every_stage_on_a_non_cubic_grid(mp, oracle_mod, refhost, config):
+    """16 x 24 x 20 cells: the x-slowest indexing (getidx, spray_k.cu:66-69)
+    with three different extents, which a cubic grid cannot tell apart."""
+    checked, bad, _ = run_pair(mp, oracle_mod, refhost, config, 16, 2017_706 + config, dims=(16, 24, 20))
+    assert not bad, bad
+    assert len(checked) >= 60
 
 
 def test_in_place_kernels_write_only_their_own_element(mp, oracle_mod, refhost):
