@@ -357,3 +357,59 @@ def test_sphere_field_equals_the_reference_kernel(mp, oracle_mod, refhost):
     lib.rh_sphere_dens(C.addressof(p), ref.ctypes.data, *[C.c_float(x) for x in center], C.c_float(radius))
     assert np.array_equal(ref, dens)
     assert (dens > 0).any() and (dens < 0).any()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_projection_stencils_on_slabs(mp, oracle_mod, refhost, world):
+    """The x-slab plan (2017multiphase_b200/slab.py) with the reference's own
+    kernels: cptdivergence_bubble2 and subGradPress (spray_k.cu:3138-3263,
+    198-224) run on each slab with one ghost plane per side (the grid's ends
+    padded with BOUNDARY cells) give the owned cells' divergence and the owned
+    faces' corrected velocities of the single-domain projection, bit for bit."""
+    import importlib
+    sl = importlib.import_module("2017multiphase_b200.slab")
+    p, parts, rf, seeds = reference_mode(mp, 1, 32, 2017_760)
+    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    orc.upload_particles(**parts)
+    orc.set_tables(rf, seeds)
+    for st in bubblesim_stages(p, 0):
+        if st[0] == "project_CG_bubble":
+            break
+        getattr(orc, st[0])(*st[1:])
+    before = snapshot(orc)
+    orc.project_CG_bubble()
+    after = snapshot(orc)
+    nx, ny, nz = p.nx, p.ny, p.nz
+    cells = ["mark", "lsmerge", "div", "press"]
+    xfaces = ["waterux", "airux"]
+    yzfaces = ["wateruy", "wateruz", "airuy", "airuz"]
+
+    def planes(a, n_planes, lo, hi, pad):
+        a = a.reshape(n_planes, -1)
+        out = np.full((hi - lo, a.shape[1]), pad, a.dtype)
+        s0, s1 = max(lo, 0), min(hi, n_planes)
+        out[s0 - lo:s1 - lo] = a[s0:s1]
+        return out.ravel()
+
+    for x0, x1 in sl.partition(nx, ny, nz, world):
+        nl = x1 - x0
+        q = type(p).from_buffer_copy(p)
+        q.nx = nl + 2
+        ref = refhost.RefHost(q, mp.FIELD_ID, mp.MPState)
+        for f in cells:
+            src = after["press"] if f == "press" else before[f]
+            ref.set_field(f, planes(src, nx, x0 - 1, x1 + 1, mp.TYPEBOUNDARY if f == "mark" else 0))
+        for f in xfaces:
+            ref.set_field(f, planes(before[f], nx + 1, x0 - 1, x1 + 2, 0))
+        for f in yzfaces:
+            ref.set_field(f, planes(before[f], nx, x0 - 1, x1 + 1, 0))
+        ref.run("divergence_bubble")
+        div = ref.get_field("div").reshape(nl + 2, -1)[1:-1]
+        assert np.array_equal(div, after["div"].reshape(nx, -1)[x0:x1]), (x0, x1)
+        ref.run("subgrad_bubble")
+        for f in xfaces:
+            got = ref.get_field(f).reshape(nl + 3, -1)[1:-1]
+            assert np.array_equal(got, after[f].reshape(nx + 1, -1)[x0:x1 + 1]), (f, x0, x1)
+        for f in yzfaces:
+            got = ref.get_field(f).reshape(nl + 2, -1)[1:-1]
+            assert np.array_equal(got, after[f].reshape(nx, -1)[x0:x1]), (f, x0, x1)
