@@ -413,3 +413,29 @@ def test_projection_stencils_on_slabs(mp, oracle_mod, refhost, world):
         for f in yzfaces:
             got = ref.get_field(f).reshape(nl + 2, -1)[1:-1]
             assert np.array_equal(got, after[f].reshape(nx, -1)[x0:x1]), (f, x0, x1)
+
+
+def test_the_reference_solo_air_forces_depend_on_thread_order(mp, oracle_mod, refhost):
+    """enforceForceSoloAirP (spray_k.cu:4335-4373) reads the neighbours'
+    velocities it is overwriting.  The oracle reads the velocities from before
+    the launch; with the threads in ascending order some air particles see
+    neighbours already updated, and their velocities move (measured on the
+    bubble column at 16^3: 179 of the 297 air particles)."""
+    p, parts, rf, seeds = reference_mode(mp, 5, N, 2017_705)
+    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
+    orc.upload_particles(**parts)
+    orc.set_tables(rf, seeds)
+    ref = refhost.RefHost(p, mp.FIELD_ID, mp.MPState)
+    ref.set_tables(rf, seeds)
+    for st in bubblesim_stages(p, 0):
+        if st[0] == "updateSoloAirParticle":
+            assert (orc.download_particles()["flag"] == mp.TYPEAIRSOLO).sum() > 0
+            copy_state(orc, ref)
+            ref.run("updateSoloAirParticle_inplace")
+            orc.updateSoloAirParticle()
+            a, b = ref.download_particles(), orc.download_particles()
+            moved = np.any(a["vel"] != b["vel"], axis=1)
+            assert moved.any()
+            assert np.isin(b["flag"][moved], [mp.TYPEAIR, mp.TYPEAIRSOLO]).all()   # only the air the SPH moves
+            return
+        getattr(orc, st[0])(*st[1:])
