@@ -25,7 +25,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/Multiphase/Multiphase"
+# the reference's source directory; MP_REFERENCE_SRC points at another checkout
+DEFAULT_SRC = os.environ.get("MP_REFERENCE_SRC", "/root/reference/Multiphase/Multiphase")
 OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "librefhost.so")
 

@@ -41,6 +41,6 @@ def refhost():
     built once per session from the reference tree; tests that use it skip
     themselves when the tree is absent."""
     from oracle import make_refhost
-    make_refhost.build(quiet=True)
+    make_refhost.build(make_refhost.DEFAULT_SRC, quiet=True)
     from oracle import refhost as rh
     return rh

@@ -25,7 +25,7 @@ import pytest
 
 from parity_util import CELL_FIELDS, FACE_FIELDS, bubblesim_stages, compare, snapshot
 
-SRC = "/root/reference/Multiphase/Multiphase"
+from oracle.make_refhost import DEFAULT_SRC as SRC
 pytestmark = pytest.mark.skipif(not os.path.exists(os.path.join(SRC, "spray_k.cu")),
                                 reason="reference source tree not present")
 
