@@ -18,7 +18,6 @@
 // so they are deterministic. Vectors are FP32 (MP_PREC_MIXED) or FP64.
 #include "ctx.cuh"
 #include <cstdint>
-#include <mutex>
 #include <string>
 #include <type_traits>
 
@@ -1130,25 +1129,15 @@ static __device__ __align__(256) unsigned char mp_cg_static_scratch[NA_BYTES];
 void mp_internal_set_global_error(const char* msg);
 
 namespace {
-constexpr int NA_MAX_DEVICES = 256;
-std::mutex na_mu;
-void* na_addr[NA_MAX_DEVICES] = {};
-
-// Device address of the scratch on the current device, looked up once per
-// device (the first call on a device does this).
+// Device address of the scratch in the current device's context. It is looked
+// up on every call: cudaGetSymbolAddress allocates nothing, and an address
+// kept from an earlier call would belong to a context that cudaDeviceReset or
+// a caller's own driver-API context may have replaced since.
 cudaError_t na_scratch(unsigned char** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, mp_cg_static_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(na_mu);
-    if (!na_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, mp_cg_static_scratch);
-        if (e != cudaSuccess) return e;
-        na_addr[dev] = p;
-    }
-    *out = static_cast<unsigned char*>(na_addr[dev]);
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 }  // namespace
@@ -1168,6 +1157,18 @@ extern "C" int mp_pressure_cg_static(int nx, int ny, int nz, float cellsize, con
         return fail(MP_ERR_CAPACITY, "mp_pressure_cg_static: " + std::to_string(nll) + " cells exceed the " +
                                          std::to_string(NA_MAX_CELLS) + "-cell limit of its fixed scratch");
     const int n = (int)nll;
+    const int nb = mp_blocks(n, 256);
+    const bool v4 = nz % 4 == 0 && reinterpret_cast<uintptr_t>(divergence) % 16 == 0 &&
+                    reinterpret_cast<uintptr_t>(pressure) % 16 == 0;
+    const int nbv = (int)std::min<long long>(nb, ((long long)(n / 4) + CG_T - 1) / CG_T);
+    dim3 pmb(PM_X, PM_Y);
+    int tiles = ((nz + PM_X - 1) / PM_X) * ((ny + PM_Y - 1) / PM_Y);
+    int chunk = std::max(4, (int)((nx * (long long)tiles + 4095) / 4096));
+    PmGeom pg{chunk};
+    dim3 pmg((nz + PM_X - 1) / PM_X, (ny + PM_Y - 1) / PM_Y, (nx + chunk - 1) / chunk);
+    if ((long long)pmg.x * pmg.y * pmg.z > NA_MAX_BLOCKS || nb > NA_MAX_BLOCKS)
+        return fail(MP_ERR_CAPACITY, "mp_pressure_cg_static: launch tiling exceeds the fixed partial-sum slots");
+
     unsigned char* base = nullptr;
     cudaError_t e = na_scratch(&base);
     if (e != cudaSuccess) return cuda_fail(e, "scratch address");
@@ -1192,19 +1193,9 @@ extern "C" int mp_pressure_cg_static(int nx, int ny, int nz, float cellsize, con
     if ((e = cudaMemsetAsync(pb, 0, sizeof(float) * n, s)) != cudaSuccess) return cuda_fail(e, "clear");
     if ((e = cudaMemsetAsync(pressure, 0, sizeof(float) * n, s)) != cudaSuccess) return cuda_fail(e, "clear");
 
-    const int nb = mp_blocks(n, 256);
     k_cg_init<float, PressOp><<<nb, CG_T, 0, s>>>(op, n, divergence, r, Rd, tol_mode, tol);
     k_nb8<PressOp><<<mp_blocks(n, 256), 256, 0, s>>>(op, n, nb8);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "launch");
-    const bool v4 = nz % 4 == 0 && reinterpret_cast<uintptr_t>(divergence) % 16 == 0 &&
-                    reinterpret_cast<uintptr_t>(pressure) % 16 == 0;
-    const int nbv = (int)std::min<long long>(nb, ((long long)(n / 4) + CG_T - 1) / CG_T);
-    dim3 pmb(PM_X, PM_Y);
-    int tiles = ((nz + PM_X - 1) / PM_X) * ((ny + PM_Y - 1) / PM_Y);
-    int chunk = std::max(4, (int)((nx * (long long)tiles + 4095) / 4096));
-    PmGeom pg{chunk};
-    dim3 pmg((nz + PM_X - 1) / PM_X, (ny + PM_Y - 1) / PM_Y, (nx + chunk - 1) / chunk);
-
     unsigned int hflag[F_COUNT] = {0, 0};
     if ((e = cudaMemcpyAsync(hflag, Rd.flag, sizeof(hflag), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)

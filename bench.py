@@ -28,10 +28,6 @@ FALLBACK_HBM_GBS = 6650.0
 # p, x, r, mark and writes x, r.
 CG_DIR_BYTES_PER_CELL = 13
 CG_UPD_BYTES_PER_CELL = 21
-# DRAM bytes per cell per launch measured by ncu on the same kernels
-# (profiles/cg_kernels_bubble_column.md); None until captured.
-CG_DIR_TRAFFIC_PER_CELL = None
-CG_UPD_TRAFFIC_PER_CELL = None
 
 
 def names_kt(mp):
@@ -41,13 +37,13 @@ def names_kt(mp):
 
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum),
 # as functions of (cells, particles): the capture's bytes scaled by the units a
-# launch processes (profiles/ gives each capture and its command)
+# launch processes
 TRAFFIC_PER_LAUNCH = {
-    # profiles/cg_v4_liquid_slab_256.md: 175.4 MB and 258.9 MB per launch at 256^3
+    # the CG passes captured at 256^3: 175.4 MB and 258.9 MB per launch
     "k_cg_dir": lambda n, np_: 175.37e6 * n / 256 ** 3,
     "k_cg_upd": lambda n, np_: 258.86e6 * n / 256 ** 3,
-    # profiles/mc_density_correctpos_bubble_column_128.md: 711.9 MB per launch at
-    # 128^3 (12.9M particles); nodes and particles both grow with the cells
+    # the MC density pass captured at 128^3 (12.9M particles): 711.9 MB per
+    # launch; nodes and particles both grow with the cells
     "k_mc_density": lambda n, np_: 711.91e6 * n / 128 ** 3,
 }
 
@@ -66,6 +62,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=8, help="steps of the forward+adjoint measurement (0: skip)")
     ap.add_argument("--adj-every", type=int, default=4, help="checkpoint interval of the adjoint")
+    ap.add_argument("--precision-steps", type=int, default=3,
+                    help="steps of the all-FP64 form timed after the main region (0: skip the precision report)")
     ap.add_argument("--profile-case", default="", choices=["", "cg", "step"],
                     help="small-footprint cases for ncu captures instead of the bench line: "
                          "cg = one pressure solve on an n^3 liquid slab (z < 0.8) with a seeded divergence; "
@@ -238,6 +236,90 @@ def profile_case(args):
             out[nm] = {"launches": nl, "ms": ms}
     print(json.dumps(out), flush=True)
     sim.close()
+
+
+# the stages of bubblesim before the projection (spray.cpp:979-1233), bubble scenes
+PRE_PROJECTION = [("hashAndSortParticles",), ("addexternalforce",), ("computeLevelset", 0.0),
+                  ("sweepLSAndMardGrid",), ("markSoloAirParticle",), ("computesurfacetension",),
+                  ("mapvelp2g_bubble",), ("enforceDragForce",), ("sweepPhi", 1), ("sweepU", 1), ("sweepPhi", 0),
+                  ("sweepU", 0), ("setWaterBoundaryU", 1), ("setWaterBoundaryU", 0)]
+STEP_FIELDS = ["press", "waterux", "wateruy", "wateruz", "airux", "airuy", "airuz", "lsmerge", "tp"]
+
+
+def rel_l2(a, b):
+    import numpy as np
+    a = np.asarray(a, np.float64).ravel(); b = np.asarray(b, np.float64).ravel()
+    den = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a))
+
+
+def precision_report(sim, mp, stream, fp64_steps):
+    """The mixed FP32/FP64 form against the all-FP64 form on the bench's own
+    state: (1) one projection from the same faces solved three ways -- FP64 to
+    a relative residual of 1e-12 (the exact pressure to FP64 precision), the
+    FP64 form and the mixed form at the configuration's stop rule -- with each
+    form's relative L2 pressure error against the first and its solve time;
+    (2) one whole step from the same checkpoint in each form, with the
+    relative L2 difference of every output field; (3) the FP64 form's
+    steps/s over `fp64_steps` steps (CUDA events on the context stream)."""
+    import torch
+    p0 = sim.get_params()
+    for st in PRE_PROJECTION:
+        getattr(sim, st[0])(*st[1:])
+    faces = {f: sim.get_field(f) for f in ["waterux", "wateruy", "wateruz", "airux", "airuy", "airuz"]}
+
+    def solve(prec, tol, maxit):
+        p = sim.get_params()
+        p.precision, p.cg_tol, p.cg_max_iter = prec, tol, maxit
+        sim.set_params(p)
+        for f, a in faces.items():
+            sim.set_field(f, a)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        it, _, rc = sim.project_CG_bubble()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return sim.get_field("press"), it, rc, e0.elapsed_time(e1)
+
+    pref, it_ref, rc_ref, _ = solve(mp.PREC_FP64, 1e-12, 20000)
+    p64, it64, rc64, ms64 = solve(mp.PREC_FP64, p0.cg_tol, p0.cg_max_iter)
+    p32, it32, rc32, ms32 = solve(mp.PREC_MIXED, p0.cg_tol, p0.cg_max_iter)
+    out = {"projection": {
+        "reference": f"FP64 CG to relative residual 1e-12 ({it_ref} iterations, rc {rc_ref})",
+        "mixed": {"pressure_rel_err": rel_l2(p32, pref), "iterations": it32, "solve_ms": ms32, "rc": rc32},
+        "fp64": {"pressure_rel_err": rel_l2(p64, pref), "iterations": it64, "solve_ms": ms64, "rc": rc64}}}
+    sim.set_params(p0)
+    # one whole step from the same state in each form
+    blob = sim.checkpoint()
+    snaps = {}
+    for name, prec in (("fp64", mp.PREC_FP64), ("mixed", mp.PREC_MIXED)):
+        sim.restore(blob)
+        p = sim.get_params(); p.precision = prec; sim.set_params(p)
+        sim.bubblesim()
+        snaps[name] = {f: sim.get_field(f) for f in STEP_FIELDS}
+        parts = sim.download_particles()
+        snaps[name]["pos"], snaps[name]["vel"] = parts["pos"], parts["vel"]
+    out["step_fields_rel_l2"] = {f: rel_l2(snaps["mixed"][f], snaps["fp64"][f]) for f in snaps["mixed"]
+                                 if snaps["mixed"][f].shape == snaps["fp64"][f].shape}
+    # the FP64 form's throughput
+    sim.restore(blob)
+    p = sim.get_params(); p.precision = mp.PREC_FP64; sim.set_params(p)
+    sim.bubblesim()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(fp64_steps):
+        sim.bubblesim()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["fp64_form"] = {"value": fp64_steps / (ms / 1e3), "unit": "steps/s", "steps": fp64_steps,
+                        "ms_per_step": ms / fp64_steps,
+                        "what": "the same step with the projection (divergence, CG vectors and scalars, "
+                                "gradient) in FP64"}
+    sim.set_params(p0)
+    return out
 
 
 def fwd_adjoint(args, n, local, dist):
@@ -437,6 +519,9 @@ def main():
            "kernel_classes": cls_table,
            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
     nx = p.nx
+    if args.precision_steps > 0:
+        out["precision"] = precision_report(sim, mp, stream, args.precision_steps)
+        out["pressure_rel_err"] = out["precision"]["projection"]["mixed"]["pressure_rel_err"]
     sim.close()
     if args.adj_steps > 0:
         out["fwd_adjoint"] = fwd_adjoint(args, nx, local, dist)

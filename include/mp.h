@@ -325,18 +325,26 @@ int mp_project(void* ctx, int* iters, double* residual); /* project_CG_bubble sp
  * whole device, would stall everything else on the GPU.
  * The caller passes device arrays of nx*ny*nz cells: mark (int8, MP_TYPE*),
  * divergence (float, the right-hand side mp_project builds, field MP_F_DIV)
- * and pressure (float, written). The stop rule is mp_project's (tol_mode,
- * tol, max_iter); iters and residual as there. Runs on `stream` (NULL: the
- * default stream) and returns after it has finished.
+ * and pressure (float, written). It solves mp_project's system with
+ * mp_project's stop rule (tol_mode, tol, max_iter) and returns the same
+ * pressure, iteration count and residual as mp_project does for
+ * MP_PREC_MIXED, MP_COEF_REF, the bubble mode (FLUID and AIR cells are
+ * unknowns) and cg_true_residual_every = 0; it has no FP64, ghost-fluid,
+ * single-phase or true-residual variant. Runs on `stream` (NULL: the default
+ * stream), synchronises it (the stop flag is read back between iteration
+ * batches) and returns after it has finished, so it must not be called on a
+ * stream that is being captured.
  * All working storage (residual, two direction vectors, neighbour bytes,
  * reduction partials) lives in one fixed array of about 3.3 MB that the
  * library holds on every GPU it is loaded on, until the process exits; grids
- * above 262,144 cells (64^3) are rejected with MP_ERR_CAPACITY. The first call
- * on a device looks up that array's device address; make that first call
- * before any stream capture. Every call reuses the same array (the parts that
- * must start at zero are cleared at each call), so calls whose GPU work
- * overlaps, from other streams or host threads on the same device, race and
- * give wrong results. Errors are read with mp_last_error(NULL, ...). */
+ * above 262,144 cells (64^3) are rejected with MP_ERR_CAPACITY before any GPU
+ * work. Each call looks up that array's address in the current context
+ * (cudaGetSymbolAddress, which allocates nothing), so it stays valid across
+ * cudaDeviceReset and in a caller's own context. Every call reuses the same
+ * array (the parts that must start at zero are cleared at each call), so
+ * calls whose GPU work overlaps, from other streams or host threads on the
+ * same device, race and give wrong results. Errors are read with
+ * mp_last_error(NULL, ...). */
 int mp_pressure_cg_static(int nx, int ny, int nz, float cellsize, const int8_t* mark,
                           const float* divergence, float* pressure, int max_iter, int tol_mode,
                           float tol, void* stream, int* iters, double* residual);

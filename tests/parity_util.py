@@ -40,9 +40,19 @@ def bubblesim_stages(p, frame):
     return s
 
 
-def make_pair(mp, oracle_mod, config, n, seed, **overrides):
+def grid_params(mp, config, nx, ny=None, nz=None):
+    """The parameters of configuration `config` at cell size 1/nx on an
+    nx x ny x nz grid (the configuration's shapes clipped to that box); a
+    non-cubic grid keeps the cubic grid's cell size and particle capacity."""
+    p = mp.scene_params(config, nx)
+    p.ny = ny or nx
+    p.nz = nz or nx
+    return p
+
+
+def make_pair(mp, oracle_mod, config, n, seed, params=None, **overrides):
     """A GPU Sim and an oracle with identical parameters, particles and tables."""
-    p = mp.scene_params(config, n)
+    p = params if params is not None else mp.scene_params(config, n)
     for k, v in overrides.items():
         setattr(p, k, v)
     sim = mp.Sim.from_config(config, n, seed, params=p)
@@ -86,6 +96,53 @@ def rel_err(a, b):
         return np.inf
     scale = max(np.abs(b[fin]).max() if fin.any() else 0.0, 1e-30)
     return float(np.abs(a[fin] - b[fin]).max() / scale) if fin.any() else 0.0
+
+
+def rel_l2(a, b):
+    """||a - b||_2 / ||b||_2 over the entries finite on both sides (0 when b is 0)."""
+    a = np.asarray(a, np.float64).ravel(); b = np.asarray(b, np.float64).ravel()
+    if a.shape != b.shape:
+        return np.inf
+    fin = np.isfinite(a) & np.isfinite(b)
+    den = np.linalg.norm(b[fin])
+    return float(np.linalg.norm(a[fin] - b[fin]) / den) if den > 0 else float(np.linalg.norm(a[fin]))
+
+
+DRIFT_GRID = ["press", "lsmerge", "tp", "waterux", "wateruy", "wateruz", "airux", "airuy", "airuz"]
+
+
+def drift(gpu, ref):
+    """Drift of the GPU run from the oracle's after many steps: relative L2 error
+    of the grid fields, the fraction of cells whose mark differs, the relative
+    difference of the particle counts, and, while the counts agree, the relative
+    L2 error of the particle positions, velocities and temperatures."""
+    out = {f: rel_l2(gpu[f], ref[f]) for f in DRIFT_GRID}
+    out["mark"] = float((gpu["mark"] != ref["mark"]).mean())
+    ng, nr = len(gpu["flag"]), len(ref["flag"])
+    out["count"] = abs(ng - nr) / max(nr, 1)
+    for f in ("pos", "vel", "temp"):
+        out[f] = rel_l2(gpu[f], ref[f]) if ng == nr else np.inf
+    return out
+
+
+def check_one_step(sim, orc, config, rtol=1e-5):
+    """One whole bubblesim step on both sides from identical inputs: frame and
+    particle count equal, marks and flags equal except for a handful of
+    threshold flips, float fields within rtol (max-norm relative, per field)."""
+    sim.bubblesim()
+    orc.bubblesim()
+    gs, rs = sim.state(), orc.state()
+    assert gs.frame == rs.frame == 1
+    assert gs.par_num_now == rs.par_num_now
+    g, r = snapshot(sim), snapshot(orc)
+    mism = (g["mark"] != r["mark"]).mean()
+    assert mism <= 1e-3, f"marks differ in {mism:.2e} of cells"
+    assert (g["flag"] != r["flag"]).mean() <= 1e-3
+    for f in ["press", "lsmerge", "lsfluid", "lsair", "tp", "waterux", "wateruy", "wateruz", "airux", "airuy", "airuz",
+              "pos", "vel", "temp"]:
+        e = rel_err(g[f], r[f])
+        assert e <= rtol, f"config {config} {f}: rel err {e:.3e}"
+    return gs, rs
 
 
 def compare(gpu, ref, exact=True, rtol=1e-5, skip=()):

@@ -14,7 +14,8 @@ import pytest
 
 from conftest import ROOT
 
-SPRAY_CPP = "/root/reference/Multiphase/Multiphase/spray.cpp"
+# the reference's source directory (MP_REFERENCE_SRC, as oracle/make_refhost.py reads it)
+SPRAY_CPP = os.path.join(os.environ.get("MP_REFERENCE_SRC", "/root/reference/Multiphase/Multiphase"), "spray.cpp")
 
 # reference member -> mp_params field (p) or mp_scene_info field (i)
 PARAM = {
