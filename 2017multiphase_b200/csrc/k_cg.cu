@@ -31,7 +31,7 @@ constexpr int CG_T = 256;
 enum { S_A = 0, S_RR = 1, S_ALPHA = 2, S_BETA = 3, S_EPS = 4, S_ZP = 5 };
 // flag slots (unsigned int): done state and iteration count
 enum { F_DONE = 0, F_ITERS = 1, F_COUNT = 2 };
-enum { DONE_RUN = 0, DONE_CONV = 1, DONE_CAP = 2, DONE_ZP0 = 3 };
+enum { DONE_RUN = 0, DONE_CONV = 1, DONE_CAP = 2, DONE_ZP0 = 3, DONE_TIMEOUT = 4 };
 
 struct Red {
     double* part;           // gridDim.x partials
@@ -574,6 +574,10 @@ __global__ void __launch_bounds__(CG_T, 6) k_cg_v4(Op op, const uint8_t* __restr
     }
 }
 
+}  // namespace
+#include "cg_tma.cuh"
+namespace {
+
 // cptdivergence_bubble2 (spray_k.cu:3138-3263)
 template <class R>
 __global__ void k_divergence(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ ls,
@@ -826,6 +830,40 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     // four-cells-per-thread kernels; they never write the direction vectors
     // outside the unknowns, so both start cleared
     constexpr bool kF32 = std::is_same<R, float>::value;
+    auto al16 = [](const void* q) { return reinterpret_cast<uintptr_t>(q) % 16 == 0; };
+    // TMA plane marching: FP32 vectors, NZ a multiple of 16 (the neighbour
+    // bytes' row stride), 16-byte aligned vectors
+    bool tma = kF32 && !kGeneral && c->cg_use_tma && gg.NZ % 16 == 0 && al16(x) && al16(r) && al16(p0) &&
+               al16(p1) && tt_encoder() != nullptr;
+    TtMaps tmaps[4];   // direction with p_old = p0 / p1, update with p = p1 / p0
+    dim3 tgrid;
+    int tchunk = 0;
+    if constexpr (kF32 && !kGeneral) {
+        if (tma) {
+            tma = tt_encode(&tmaps[0].a, r, gg, 4, TT_HK, TT_HJ) && tt_encode(&tmaps[0].b, p0, gg, 4, TT_HK, TT_HJ) &&
+                  tt_encode(&tmaps[0].nb, nb8, gg, 1, TT_K, TT_J);
+            tmaps[1] = tmaps[0];
+            tma = tma && tt_encode(&tmaps[1].b, p1, gg, 4, TT_HK, TT_HJ);
+            tma = tma && tt_encode(&tmaps[2].a, p1, gg, 4, TT_HK, TT_HJ) && tt_encode(&tmaps[2].b, x, gg, 4, TT_K, TT_J) &&
+                  tt_encode(&tmaps[2].c, r, gg, 4, TT_K, TT_J) && tt_encode(&tmaps[2].nb, nb8, gg, 1, TT_K, TT_J);
+            tmaps[3] = tmaps[2];
+            tma = tma && tt_encode(&tmaps[3].a, p0, gg, 4, TT_HK, TT_HJ);
+        }
+        if (tma) {
+            const int tk = (gg.NZ + TT_K - 1) / TT_K, tj = (gg.NY + TT_J - 1) / TT_J;
+            // planes per CTA: one wave of 3 CTAs per SM, at least 4 planes
+            int nch = std::max(1, (148 * 3) / (tk * tj));
+            tchunk = c->cg_tma_chunk > 0 ? c->cg_tma_chunk : std::max(4, (gg.NX + nch - 1) / nch);
+            tgrid = dim3(tk, tj, (gg.NX + tchunk - 1) / tchunk);
+            if ((long long)tgrid.x * tgrid.y * tgrid.z > 148LL * 32) tma = false;
+        }
+        if (tma) {
+            MP_CUDA(c, cudaFuncSetAttribute(k_cg_tma<Op, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)tt_smem_bytes<0>()));
+            MP_CUDA(c, cudaFuncSetAttribute(k_cg_tma<Op, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)tt_smem_bytes<1>()));
+        }
+    }
     const bool v4 = kF32 && gg.NZ % 4 == 0;
     const int nbv = (int)std::min<long long>(c->red_blocks, ((long long)(n / 4) + CG_T - 1) / CG_T);
     if (v4) {
@@ -852,7 +890,19 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
                 }
             } else {
             if constexpr (kF32) {
-                if (v4) {
+                if (tma) {
+                    const int d = (pa == p0) ? 0 : 1;   // p_old
+                    {
+                        KtScope kt(c, kt_stencil);
+                        k_cg_tma<Op, 0><<<tgrid, TT_THREADS, tt_smem_bytes<0>(), s>>>(
+                            op, tmaps[d], pb, nullptr, nullptr, Rd, tchunk, it == 0 ? 1 : 0, it, maxiter, 0);
+                    }
+                    {
+                        KtScope kt(c, MP_KT_CG_UPDATE);
+                        k_cg_tma<Op, 1><<<tgrid, TT_THREADS, tt_smem_bytes<1>(), s>>>(
+                            op, tmaps[2 + d], nullptr, x, r, Rd, tchunk, 0, it, maxiter, tr ? 1 : 0);
+                    }
+                } else if (v4) {
                     {
                         KtScope kt(c, kt_stencil);
                         k_cg_v4<Op, 0><<<nbv, CG_T, 0, s>>>(op, nb8, r, pa, pb, nullptr, nullptr, Rd,
@@ -865,7 +915,7 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
                     }
                 }
             }
-            if (!v4) {
+            if (!v4 && !tma) {
                 {
                     KtScope kt(c, kt_stencil);
                     k_cg_pm<R, Op, 0><<<pmg, pmb, 0, s>>>(op, pg, nb8, r, pa, pb, nullptr, nullptr, Rd,
@@ -893,6 +943,11 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     MP_CUDA(c, cudaStreamSynchronize(s));
     *iters_out = (int)hflag[F_ITERS];
     *res_out = rr;
+    if (hflag[F_DONE] == DONE_TIMEOUT) {
+        MP_CUDA(c, cudaMemsetAsync(Rd.count, 0, sizeof(unsigned int), s));
+        c->err = "cg: a TMA tile wait ran out of time";
+        return MP_ERR_TIMEOUT;
+    }
     return hflag[F_DONE] == DONE_CAP ? MP_ERR_NOCONVERGE : MP_OK;
 }
 

@@ -294,6 +294,7 @@ def precision_report(sim, mp, stream, fp64_steps):
     blob = sim.checkpoint()
     snaps = {}
     for name, prec in (("fp64", mp.PREC_FP64), ("mixed", mp.PREC_MIXED)):
+        sim.set_params(p0)
         sim.restore(blob)
         p = sim.get_params(); p.precision = prec; sim.set_params(p)
         sim.bubblesim()
@@ -303,6 +304,7 @@ def precision_report(sim, mp, stream, fp64_steps):
     out["step_fields_rel_l2"] = {f: rel_l2(snaps["mixed"][f], snaps["fp64"][f]) for f in snaps["mixed"]
                                  if snaps["mixed"][f].shape == snaps["fp64"][f].shape}
     # the FP64 form's throughput
+    sim.set_params(p0)
     sim.restore(blob)
     p = sim.get_params(); p.precision = mp.PREC_FP64; sim.set_params(p)
     sim.bubblesim()

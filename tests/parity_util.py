@@ -122,7 +122,27 @@ def drift(gpu, ref):
     out["count"] = abs(ng - nr) / max(nr, 1)
     for f in ("pos", "vel", "temp"):
         out[f] = rel_l2(gpu[f], ref[f]) if ng == nr else np.inf
+    ag, ar = aggregates(gpu), aggregates(ref)
+    for k in ar:
+        out["agg_" + k] = abs(ag[k] - ar[k]) / max(abs(ar[k]), 1e-30)
     return out
+
+
+def aggregates(snap):
+    """Whole-domain quantities of a state: particle kinetic energy, the mean
+    particle temperature, the centroid height of the gas particles (AIR and
+    AIRSOLO) and of the liquid, and the cell counts of liquid and gas."""
+    f = snap["flag"]
+    v = snap["vel"].astype(np.float64); m = snap["mass"].astype(np.float64)
+    z = snap["pos"][:, 2].astype(np.float64)
+    gas = (f == 1) | (f == 4)
+    liq = f == 0
+    return {"kinetic": float((m * (v * v).sum(1)).sum()) + 1e-30,
+            "temp": float(snap["temp"].astype(np.float64).mean()) if len(f) else 0.0,
+            "gas_z": float(z[gas].mean()) if gas.any() else 0.0,
+            "liquid_z": float(z[liq].mean()) if liq.any() else 0.0,
+            "fluid_cells": float((snap["mark"] == 0).sum()),
+            "gas_cells": float((snap["mark"] == 1).sum())}
 
 
 def check_one_step(sim, orc, config, rtol=1e-5):

@@ -70,3 +70,30 @@ def test_cg_matches_oracle_iterations(mp, oracle_mod):
     assert abs(ig - io) <= 1, (ig, io)
     assert rel_err(sim.get_field("press"), orc.get_field("press")) <= 1e-5
     sim.close()
+
+
+@pytest.mark.parametrize("config,shape", [(5, (64, 64, 64)), (1, (40, 24, 48))], ids=["64^3", "40x24x48"])
+def test_cg_tma_matches_float4_passes(mp, oracle_mod, monkeypatch, config, shape):
+    """The TMA plane-marching CG passes write the same vectors as the float4
+    passes (their FP64 dot products add in another order): same iteration
+    count within one, pressure within 1e-5, on a cube and on a grid whose
+    tiles are partial in j and k."""
+    from parity_util import grid_params
+    out = {}
+    for kernel in ("v4", "tma"):
+        monkeypatch.setenv("MP_CG_KERNEL", kernel)
+        p = grid_params(mp, config, *shape)
+        sim = mp.Sim.from_config(config, shape[0], 77 + config, params=p)
+        for st in ["hashAndSortParticles", "addexternalforce"]:
+            getattr(sim, st)()
+        sim.computeLevelset(0.0); sim.sweepLSAndMardGrid(); sim.mapvelp2g_bubble()
+        for ph in (1, 0):
+            sim.sweepPhi(ph); sim.sweepU(ph)
+        sim.setWaterBoundaryU(1); sim.setWaterBoundaryU(0)
+        it, res, rc = sim.project_CG_bubble()
+        assert rc == 0
+        out[kernel] = (it, sim.get_field("press"), sim.get_field("waterux"))
+        sim.close()
+    assert abs(out["v4"][0] - out["tma"][0]) <= 1, (out["v4"][0], out["tma"][0])
+    assert rel_err(out["tma"][1], out["v4"][1]) <= 1e-5
+    assert rel_err(out["tma"][2], out["v4"][2]) <= 1e-5
