@@ -85,6 +85,11 @@ class MPSceneInfo(C.Structure):
                 ("frame_max", C.c_int32), ("output_colored_particles", C.c_int32), ("reserved", C.c_int32 * 8)]
 
 
+class MPGrad(C.Structure):
+    """mp_grad: device arrays of doubles, xyz per particle (NULL members allowed)."""
+    _fields_ = [("pos", C.c_void_p), ("vel", C.c_void_p)]
+
+
 class MPOutput(C.Structure):
     _fields_ = [("dir", C.c_char_p), ("pov", C.c_int32), ("obj", C.c_int32), ("colored_particles", C.c_int32),
                 ("t_render_min", C.c_float), ("t_render_max", C.c_float)]
@@ -164,6 +169,9 @@ def load_library() -> C.CDLL:
         "mp_adj_loss": ([vp, C.c_int, vp, C.POINTER(C.c_double)], C.c_int),
         "mp_adj_gradient": ([vp, C.c_int, vp, vp, C.POINTER(C.c_double)], C.c_int),
         "mp_adj_release": ([vp], C.c_int),
+        "mp_adj_forward": ([vp, C.c_int, C.POINTER(MPGrad), C.POINTER(MPGrad)], C.c_int),
+        "mp_step_adjoint": ([vp, C.c_int, C.POINTER(MPGrad), C.POINTER(MPGrad), C.POINTER(MPGrad)], C.c_int),
+        "mp_adj_level_set_loss": ([vp, C.c_int, vp, C.POINTER(C.c_double), vp], C.c_int),
         "mp_checkpoint_size": ([vp, C.POINTER(C.c_size_t)], C.c_int),
         "mp_checkpoint_save": ([vp, vp, C.c_size_t], C.c_int),
         "mp_checkpoint_load": ([vp, vp, C.c_size_t], C.c_int),
@@ -602,6 +610,46 @@ class Sim:
         _check(self.lib.mp_adj_gradient(self.ctx, precision, vp, C.c_void_p(g.data_ptr()), C.byref(loss)), self.ctx)
         return loss.value, g
 
+    @staticmethod
+    def _grad(pos=None, vel=None):
+        return MPGrad(None if pos is None else pos.data_ptr(), None if vel is None else vel.data_ptr())
+
+    def _empty3(self):
+        import torch
+        return torch.empty((self.adj_num_particles(), 3), dtype=torch.float64,
+                           device=f"cuda:{torch.cuda.current_device()}")
+
+    def adj_forward(self, x0=None, v0=None, precision: int = PREC_MIXED):
+        """The recorded program from initial positions/velocities (CUDA float64
+        (np, 3) tensors in recording order, None: the recorded ones) to the
+        final (xT, vT) (mp_adj_forward)."""
+        import torch
+        xT, vT = self._empty3(), self._empty3()
+        inp, out = self._grad(x0, v0), self._grad(xT, vT)
+        torch.cuda.synchronize()
+        _check(self.lib.mp_adj_forward(self.ctx, precision, C.byref(inp), C.byref(out)), self.ctx)
+        return xT, vT
+
+    def step_adjoint(self, x0=None, v0=None, xT_bar=None, vT_bar=None, precision: int = PREC_MIXED):
+        """The vector-Jacobian product of the recorded program at (x0, v0):
+        (x0_bar, v0_bar) = J^T (xT_bar, vT_bar) (mp_step_adjoint)."""
+        import torch
+        x0b, v0b = self._empty3(), self._empty3()
+        inp, dout, din = self._grad(x0, v0), self._grad(xT_bar, vT_bar), self._grad(x0b, v0b)
+        torch.cuda.synchronize()
+        _check(self.lib.mp_step_adjoint(self.ctx, precision, C.byref(inp), C.byref(dout), C.byref(din)), self.ctx)
+        return x0b, v0b
+
+    def adj_level_set_loss(self, xT, precision: int = PREC_MIXED, grad: bool = True):
+        """(L, dL/dxT) of the target-point loss at final positions xT."""
+        import torch
+        loss = C.c_double()
+        g = self._empty3() if grad else None
+        torch.cuda.synchronize()
+        _check(self.lib.mp_adj_level_set_loss(self.ctx, precision, C.c_void_p(xT.data_ptr()), C.byref(loss),
+                                              None if g is None else C.c_void_p(g.data_ptr())), self.ctx)
+        return loss.value, g
+
     # ---- measurement ------------------------------------------------------
     def kernel_timing(self, cls: int, enable: bool = True):
         _check(self.lib.mp_kernel_timing(self.ctx, cls, int(enable)), self.ctx)
@@ -631,29 +679,98 @@ def dam_break_targets(nsamples: int, seed: int, height: float = 0.3, margin: flo
     return np.concatenate([xy, np.full((nsamples, 1), height)], axis=1).astype(np.float32)
 
 
-def _dam_break_function():
+def _functions():
     import torch
 
-    class DamBreakLoss(torch.autograd.Function):
-        """Loss of the recorded FLUID-only program as a function of the initial
-        particle velocities; backward is the hand-written adjoint
-        (mp_adj_gradient). The discrete state is the one recorded by
-        Sim.adj_record, so v0 should stay near the recorded velocities."""
+    class MPStep(torch.autograd.Function):
+        """The recorded steps (Sim.adj_record) as a function of the particles'
+        initial positions and velocities, (x0, v0) -> (xT, vT), CUDA float64
+        (np, 3) tensors in recording order. backward is the hand-written
+        adjoint (mp_step_adjoint), run only when a gradient is asked for. The
+        discrete state (splat order, cell marks, extrapolation choices) is the
+        recorded one, so the inputs should stay near the recorded state."""
 
         @staticmethod
-        def forward(ctx, v0, sim, precision):
-            loss, grad = sim.adj_gradient(v0.detach().to(torch.float64).contiguous(), precision)
-            ctx.save_for_backward(grad)
-            return torch.tensor(loss, dtype=torch.float64, device=v0.device)
+        def forward(ctx, x0, v0, sim, precision):
+            x0 = x0.detach().to(torch.float64).contiguous()
+            v0 = v0.detach().to(torch.float64).contiguous()
+            ctx.save_for_backward(x0, v0)
+            ctx.sim, ctx.precision = sim, precision
+            return sim.adj_forward(x0, v0, precision)
+
+        @staticmethod
+        def backward(ctx, gx, gv):
+            if not (ctx.needs_input_grad[0] or ctx.needs_input_grad[1]):
+                return None, None, None, None
+            x0, v0 = ctx.saved_tensors
+            gx = None if gx is None else gx.to(torch.float64).contiguous()
+            gv = None if gv is None else gv.to(torch.float64).contiguous()
+            x0b, v0b = ctx.sim.step_adjoint(x0, v0, gx, gv, ctx.precision)
+            return (x0b if ctx.needs_input_grad[0] else None), (v0b if ctx.needs_input_grad[1] else None), None, None
+
+    class LevelSetLoss(torch.autograd.Function):
+        """sum_s phi(y_s)^2 of the final fluid distance field at the target
+        points (mp_adj_set_targets) as a function of the final positions."""
+
+        @staticmethod
+        def forward(ctx, xT, sim, precision):
+            xT = xT.detach().to(torch.float64).contiguous()
+            ctx.save_for_backward(xT)
+            ctx.sim, ctx.precision = sim, precision
+            loss, _ = sim.adj_level_set_loss(xT, precision, grad=False)
+            return torch.tensor(loss, dtype=torch.float64, device=xT.device)
 
         @staticmethod
         def backward(ctx, gout):
-            (grad,) = ctx.saved_tensors
+            if not ctx.needs_input_grad[0]:
+                return None, None, None
+            (xT,) = ctx.saved_tensors
+            _, g = ctx.sim.adj_level_set_loss(xT, ctx.precision, grad=True)
+            return gout * g, None, None
+
+    class DamBreakLoss(torch.autograd.Function):
+        """Loss of the recorded FLUID-only program as a function of the initial
+        particle velocities; forward evaluates the loss only, backward runs the
+        adjoint (mp_adj_gradient)."""
+
+        @staticmethod
+        def forward(ctx, v0, sim, precision):
+            v0 = v0.detach().to(torch.float64).contiguous()
+            ctx.save_for_backward(v0)
+            ctx.sim, ctx.precision = sim, precision
+            return torch.tensor(sim.adj_loss(v0, precision), dtype=torch.float64, device=v0.device)
+
+        @staticmethod
+        def backward(ctx, gout):
+            if not ctx.needs_input_grad[0]:
+                return None, None, None
+            (v0,) = ctx.saved_tensors
+            _, grad = ctx.sim.adj_gradient(v0, ctx.precision)
             return gout * grad, None, None
 
-    return DamBreakLoss
+    return MPStep, LevelSetLoss, DamBreakLoss
+
+
+_FUNCS = None
+
+
+def _fn(i):
+    global _FUNCS
+    if _FUNCS is None:
+        _FUNCS = _functions()
+    return _FUNCS[i]
+
+
+def mp_step(x0, v0, sim, precision: int = PREC_MIXED):
+    """torch.autograd entry: (xT, vT) of the recorded steps from (x0, v0)."""
+    return _fn(0).apply(x0, v0, sim, precision)
+
+
+def level_set_loss(xT, sim, precision: int = PREC_MIXED):
+    """torch.autograd entry: the target-point level-set loss of final positions."""
+    return _fn(1).apply(xT, sim, precision)
 
 
 def dam_break_loss(v0, sim, precision: int = PREC_MIXED):
     """torch.autograd entry: loss(v0) with d loss / d v0 from the adjoint."""
-    return _dam_break_function().apply(v0, sim, precision)
+    return _fn(2).apply(v0, sim, precision)

@@ -199,14 +199,15 @@ __global__ void __launch_bounds__(TT_THREADS, 3)
     for (; t < nplanes; t++) {
         const int q = q0 + t;
         unsigned char* st = sm + (t % TT_NS) * SB;
-        if (!tt_bar_wait(bar + (t % TT_NS), (uint32_t)((t / TT_NS) & 1))) atomicExch(&tt_fail, 1);
-        __syncthreads();
-        if (tt_fail) break;
+        // every thread waits for the stage itself; a wait that runs out is
+        // seen by all threads after the barrier below
+        const bool ok = tt_bar_wait(bar + (t % TT_NS), (uint32_t)((t / TT_NS) & 1));
+        if (!ok) atomicExch(&tt_fail, 1);
         // the window plane of q from the stage
         float4* w = reinterpret_cast<float4*>(win + (t % TT_NW) * (TT_HK * TT_HJ));
         const float4* sa = reinterpret_cast<const float4*>(st);
         const float4* sb = reinterpret_cast<const float4*>(st + TT_HALO_PAD);
-        for (int e = tid; e < TT_HK * TT_HJ / 4; e += TT_THREADS) {
+        for (int e = tid; ok && e < TT_HK * TT_HJ / 4; e += TT_THREADS) {
             float4 a = sa[e];
             if (MODE == 0 && !first) {
                 const float4 b = sb[e];
@@ -228,6 +229,7 @@ __global__ void __launch_bounds__(TT_THREADS, 3)
         // writes that refill it, and publish the window plane
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        if (tt_fail) break;
         if (tid == 0 && t + TT_NS < nplanes) issue(t + TT_NS);
         // the row of plane q-1 from window planes q-2, q-1, q
         const int ic = q - 1;

@@ -210,6 +210,10 @@ int k_adj_record(MpCtx* c, int nsteps, int every);
 int k_adj_set_targets(MpCtx* c, const float* samples3, int nsamples);
 int k_adj_run(MpCtx* c, int precision, const double* v0, double* grad, double* loss);
 int k_adj_np(MpCtx* c, int* np, int* nsteps);
+int k_adj_forward(MpCtx* c, int precision, const double* x0, const double* v0, double* xT, double* vT);
+int k_adj_vjp(MpCtx* c, int precision, const double* x0, const double* v0, const double* xTb, const double* vTb,
+              double* x0b, double* v0b);
+int k_adj_ls_loss(MpCtx* c, int precision, const double* xT, double* loss, double* xTb);
 int k_init_particle_heat(MpCtx* c);
 int k_pack_particles(MpCtx* c, int n, const float* pos3, const float* vel3, const int8_t* flag,
                      const float* mass, const float* T, const float* L, const float* sol, const float* gas);

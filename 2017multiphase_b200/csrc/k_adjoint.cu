@@ -1062,10 +1062,26 @@ template <class T> static int adj_loss_fwd(const Replay<T>& R, const T* x, doubl
     return MP_OK;
 }
 
-template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, double* loss) {
+// What one replay computes. Primal inputs and outputs and all cotangents are
+// device arrays of doubles, xyz per particle in recording order.
+struct AdjIO {
+    const double* x0 = nullptr;   // initial positions (NULL: the recorded ones)
+    const double* v0 = nullptr;   // initial velocities (NULL: the recorded ones)
+    double* xT = nullptr;         // final positions (NULL: not wanted)
+    double* vT = nullptr;         // final velocities
+    bool loss = false;            // evaluate the level-set loss; with `reverse`, seed the sweep with its cotangent
+    double* loss_out = nullptr;
+    const double* xTb = nullptr;  // otherwise the seed: cotangents of the final positions / velocities (NULL: 0)
+    const double* vTb = nullptr;
+    bool reverse = false;         // run the reverse sweep
+    double* x0b = nullptr;        // cotangents of the initial positions / velocities (NULL: not wanted)
+    double* v0b = nullptr;
+};
+
+template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
     AdjTape* t = c->adj;
     if (!t) { c->err = "adjoint: record first (mp_adj_record)"; return MP_ERR_STATE; }
-    if (!t->nsamples) { c->err = "adjoint: no target samples (mp_adj_set_targets)"; return MP_ERR_STATE; }
+    if (io.loss && !t->nsamples) { c->err = "adjoint: no target samples (mp_adj_set_targets)"; return MP_ERR_STATE; }
     MP_TRY(adj_work<T>(c, t));
     Replay<T> R{c, t, c->G, (long long)c->G.nfx + c->G.nfy + c->G.nfz, t->np};
     cudaStream_t s = c->stream;
@@ -1074,8 +1090,9 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
     // forward over all steps, keeping the segment starts (slot 0 holds each
     // step's intermediates in passing)
     T* x = R.a(W_X); T* v = R.a(W_V); T* xn = R.a(W_XN); T* vn = R.a(W_VN);
-    k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->x0, x);
-    if (v0) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, v0, v);
+    if (io.x0) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, io.x0, x);
+    else k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->x0, x);
+    if (io.v0) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, io.v0, v);
     else k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->v0, v);
     MP_CHECK_LAUNCH(c);
     const int E = t->every, nseg = (t->nsteps + E - 1) / E;
@@ -1091,16 +1108,31 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
         MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, scratch, true));
         std::swap(x, xn); std::swap(v, vn);
     }
-    double L = 0;
-    MP_TRY(adj_loss_fwd<T>(R, x, &L));
-    if (loss) *loss = L;
-    if (!grad) return MP_OK;
-    // loss transpose
+    if (io.xT) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, x, io.xT);
+    if (io.vT) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, v, io.vT);
+    MP_CHECK_LAUNCH(c);
+    if (io.loss) {
+        double L = 0;
+        MP_TRY(adj_loss_fwd<T>(R, x, &L));
+        if (io.loss_out) *io.loss_out = L;
+    }
+    if (!io.reverse) {
+        MP_CUDA(c, cudaStreamSynchronize(s));
+        return MP_OK;
+    }
+    // the seed of the reverse sweep
     T* xb = R.a(W_XB); T* vb = R.a(W_VB);
-    k_ad_phibar<T><<<mp_blocks(c->G.n, 256), 256, 0, s>>>(c->G, t->samples, t->s_off,
-                                                          static_cast<double*>(t->wk[W_SV]), R.a(W_CQ));
-    k_ad_phi_x<T><<<mp_blocks(t->np, 256), 256, 0, s>>>(c->G, t->np, x, t->nearest, R.a(W_CQ), xb);
-    MP_CUDA(c, cudaMemsetAsync(vb, 0, sizeof(T) * np3, s));
+    if (io.loss) {
+        k_ad_phibar<T><<<mp_blocks(c->G.n, 256), 256, 0, s>>>(c->G, t->samples, t->s_off,
+                                                              static_cast<double*>(t->wk[W_SV]), R.a(W_CQ));
+        k_ad_phi_x<T><<<mp_blocks(t->np, 256), 256, 0, s>>>(c->G, t->np, x, t->nearest, R.a(W_CQ), xb);
+        MP_CUDA(c, cudaMemsetAsync(vb, 0, sizeof(T) * np3, s));
+    } else {
+        if (io.xTb) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, io.xTb, xb);
+        else MP_CUDA(c, cudaMemsetAsync(xb, 0, sizeof(T) * np3, s));
+        if (io.vTb) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, io.vTb, vb);
+        else MP_CUDA(c, cudaMemsetAsync(vb, 0, sizeof(T) * np3, s));
+    }
     MP_CHECK_LAUNCH(c);
     // reverse sweep, segment by segment: the segment is replayed from its
     // start, each step's state and intermediates kept in its slot, then the
@@ -1116,15 +1148,63 @@ template <class T> static int adj_run(MpCtx* c, const double* v0, double* grad, 
         }
         for (int j = len - 1; j >= 0; j--) MP_TRY(adj_step<T>(R, k0 + j, R.seg_x(nseg + j), R.inter(j), xb, vb));
     }
-    k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, vb, grad);
+    if (io.v0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, vb, io.v0b);
+    if (io.x0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, xb, io.x0b);
     MP_CHECK_LAUNCH(c);
     MP_CUDA(c, cudaStreamSynchronize(s));
     return MP_OK;
 }
 
+// the level-set loss of given final positions and its cotangent
+template <class T> static int adj_ls_loss(MpCtx* c, const double* xT, double* loss, double* xTb) {
+    AdjTape* t = c->adj;
+    if (!t) { c->err = "adjoint: record first (mp_adj_record)"; return MP_ERR_STATE; }
+    if (!t->nsamples) { c->err = "adjoint: no target samples (mp_adj_set_targets)"; return MP_ERR_STATE; }
+    MP_TRY(adj_work<T>(c, t));
+    Replay<T> R{c, t, c->G, (long long)c->G.nfx + c->G.nfy + c->G.nfz, t->np};
+    cudaStream_t s = c->stream;
+    const long long np3 = 3LL * t->np;
+    const int nb3 = mp_blocks(np3, 256);
+    T* x = R.a(W_X);
+    k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, xT, x);
+    MP_CHECK_LAUNCH(c);
+    double L = 0;
+    MP_TRY(adj_loss_fwd<T>(R, x, &L));
+    if (loss) *loss = L;
+    if (xTb) {
+        T* xb = R.a(W_XB);
+        k_ad_phibar<T><<<mp_blocks(c->G.n, 256), 256, 0, s>>>(c->G, t->samples, t->s_off,
+                                                              static_cast<double*>(t->wk[W_SV]), R.a(W_CQ));
+        k_ad_phi_x<T><<<mp_blocks(t->np, 256), 256, 0, s>>>(c->G, t->np, x, t->nearest, R.a(W_CQ), xb);
+        k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, xb, xTb);
+        MP_CHECK_LAUNCH(c);
+        MP_CUDA(c, cudaStreamSynchronize(s));
+    }
+    return MP_OK;
+}
+
 int k_adj_run(MpCtx* c, int precision, const double* v0, double* grad, double* loss) {
-    if (precision == MP_PREC_FP64) return adj_run<double>(c, v0, grad, loss);
-    return adj_run<float>(c, v0, grad, loss);
+    AdjIO io;
+    io.v0 = v0; io.loss = true; io.loss_out = loss; io.reverse = grad != nullptr; io.v0b = grad;
+    if (precision == MP_PREC_FP64) return adj_run<double>(c, io);
+    return adj_run<float>(c, io);
+}
+int k_adj_forward(MpCtx* c, int precision, const double* x0, const double* v0, double* xT, double* vT) {
+    AdjIO io;
+    io.x0 = x0; io.v0 = v0; io.xT = xT; io.vT = vT;
+    if (precision == MP_PREC_FP64) return adj_run<double>(c, io);
+    return adj_run<float>(c, io);
+}
+int k_adj_vjp(MpCtx* c, int precision, const double* x0, const double* v0, const double* xTb, const double* vTb,
+              double* x0b, double* v0b) {
+    AdjIO io;
+    io.x0 = x0; io.v0 = v0; io.xTb = xTb; io.vTb = vTb; io.reverse = true; io.x0b = x0b; io.v0b = v0b;
+    if (precision == MP_PREC_FP64) return adj_run<double>(c, io);
+    return adj_run<float>(c, io);
+}
+int k_adj_ls_loss(MpCtx* c, int precision, const double* xT, double* loss, double* xTb) {
+    if (precision == MP_PREC_FP64) return adj_ls_loss<double>(c, xT, loss, xTb);
+    return adj_ls_loss<float>(c, xT, loss, xTb);
 }
 int k_adj_np(MpCtx* c, int* np, int* nsteps) {
     if (!c->adj) { c->err = "adjoint: record first"; return MP_ERR_STATE; }

@@ -141,7 +141,7 @@ struct HeatOp {
         float al = al_of(mark[idx]);
         float h = g.h;
         R c = val(idx);
-        R s = (R)(h * h / al / dt + 6.0f) * c;
+        R s = ((R)h * (R)h / (R)al / (R)dt + (R)6.0f) * c;
         int q;
         q = idx + sI; s -= fix(q) ? c : val(q);
         q = idx + sJ; s -= fix(q) ? c : val(q);
@@ -155,7 +155,7 @@ struct HeatOp {
     template <class R> __device__ __forceinline__ R start(int idx, R c) const {
         float al = al_of(mark[idx]);
         float h = g.h;
-        return (R)(h * h / al / dt + 6.0f) * c;
+        return ((R)h * (R)h / (R)al / (R)dt + (R)6.0f) * c;
     }
     template <class R> __device__ __forceinline__ R comb(R s, R v) const { return s - v; }
     template <class R> __device__ __forceinline__ R finish(R s) const { return s; }
@@ -773,6 +773,23 @@ __global__ void k_heat_rhs(Grid g, const float* __restrict__ Tp, float* __restri
         bo[idx] = t * g.h * g.h / al / op.dt;
     }
 }
+// the same right-hand side in FP64 (the all-FP64 form)
+__global__ void k_heat_rhs64(Grid g, const float* __restrict__ Tp, float* __restrict__ save, double* __restrict__ bo,
+                             float* __restrict__ bof, const int8_t* __restrict__ mark,
+                             const float* __restrict__ fixedheat, HeatOp op) {
+    MP_GRID_LOOP(idx, g.n) {
+        float t = Tp[idx];
+        save[idx] = t;
+        double al = op.al_of(mark[idx]);
+        if (fixedheat && fixedheat[idx] != MP_UNDEF_TEMPERATURE) t = fixedheat[idx];
+        const double b = (double)t * (double)g.h * (double)g.h / al / (double)op.dt;
+        bo[idx] = b;
+        bof[idx] = (float)b;
+    }
+}
+__global__ void k_d2f(int n, const double* __restrict__ a, float* __restrict__ b) {
+    MP_GRID_LOOP(idx, n) b[idx] = (float)a[idx];
+}
 __global__ void k_heat_bound(Grid g, const float* __restrict__ in, float* __restrict__ out) {
     MP_GRID_LOOP(idx, g.n) {
         int i, j, k; getijk(g, (int)idx, i, j, k);
@@ -1080,14 +1097,30 @@ static int heat_solve(MpCtx* c) {
     int sc = P.scene;
     op.boil = (sc == MP_SCENE_BOILING || sc == MP_SCENE_BOILING_HIGHRES || sc == MP_SCENE_MELTANDBOIL ||
                sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL) ? 1 : 0;
-    k_heat_rhs<<<nb, 256, 0, c->stream>>>(g, c->Tp, c->Tp_save, c->Tp_old, c->mark,
-                                          P.b_fixed_heat ? c->fixedheat : nullptr, op);
-    c->launches++;
-    MP_CHECK_LAUNCH(c);
     int it = 0; double rr = 0;
-    int rc = run_cg<float>(c, op, c->Tp, c->Tp_old, c->cg_r, c->cg_p, c->cg_z, P.heat_cg_max_iter, MP_TOL_REF_ABS,
+    int rc;
+    if (P.precision == MP_PREC_FP64) {
+        // the all-FP64 form: right-hand side, vectors and scalars in FP64
+        double* xd = c->cg64; double* bd = xd + g.n;
+        double* rd = bd + g.n; double* p0 = rd + g.n; double* p1 = p0 + g.n;
+        k_heat_rhs64<<<nb, 256, 0, c->stream>>>(g, c->Tp, c->Tp_save, bd, c->Tp_old, c->mark,
+                                                P.b_fixed_heat ? c->fixedheat : nullptr, op);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        rc = run_cg<double>(c, op, xd, bd, rd, p0, p1, P.heat_cg_max_iter, MP_TOL_REF_ABS, 0.01f, 0, &it, &rr,
+                            MP_KT_CG_STENCIL);
+        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+        k_d2f<<<nb, 256, 0, c->stream>>>(g.n, xd, c->Tp);
+        c->launches++;
+    } else {
+        k_heat_rhs<<<nb, 256, 0, c->stream>>>(g, c->Tp, c->Tp_save, c->Tp_old, c->mark,
+                                              P.b_fixed_heat ? c->fixedheat : nullptr, op);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        rc = run_cg<float>(c, op, c->Tp, c->Tp_old, c->cg_r, c->cg_p, c->cg_z, P.heat_cg_max_iter, MP_TOL_REF_ABS,
                            0.01f, 0, &it, &rr, MP_KT_CG_STENCIL);
-    if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+    }
     c->S.last_heat_cg_iters = it;
     c->S.last_heat_cg_residual = rr;
     if (P.b_extend_heat_to_boundary) {

@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="grid size (0: the configuration's own, 256)")
     ap.add_argument("--seed", type=int, default=2017005)
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-n", type=int, default=64, help="grid of the bounded CPU sample")
+    ap.add_argument("--ref-steps", type=int, default=2, help="reference arm: at most this many timed oracle steps")
+    ap.add_argument("--ref-warmup", type=int, default=0, help="reference arm: at most this many warm-up steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=8, help="steps of the forward+adjoint measurement (0: skip)")
     ap.add_argument("--adj-every", type=int, default=4, help="checkpoint interval of the adjoint")
@@ -139,21 +140,25 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(config, n_cpu, seed, steps=1, warm=1, threads=None):
-    """The CPU oracle (the reference step restated, OpenMP over all host cores, or
-    `threads` of them) on a bounded sample of the workload: the same
-    configuration on an n_cpu^3 grid."""
-    import importlib
-    mp = importlib.import_module("2017multiphase_b200")
-    from oracle import oracle as oracle_mod
+def workload_config(p, npart0, seed, world):
+    """The `config` object of both arms' JSON lines (the same workload)."""
+    return {"workload": f"bubble column {p.nx}^3: liquid z<0.8, 200 air bubbles r~U[0.01,0.04], "
+                        f"8 jittered particles/cell, dt=1/{1.0 / p.dt:.0f} (1/240 x (64/n)^2), FLIP 0.95, "
+                        f"constant-coefficient projection (the reference's; coef_mode ref), "
+                        f"CG rel 1e-6, marching cubes every step",
+            "grid": p.nx, "particles": int(npart0), "seed": seed,
+            "l2": "inputs larger than L2 (particle streams alone are ~5 GB)",
+            "parallelism": f"replicas x{world}"}
+
+
+def oracle_steps(config, n, seed, steps, warm, threads=None):
+    """The CPU oracle (the reference step restated in C++, OpenMP over the
+    host cores) on configuration `config` at n^3, built from the oracle's own
+    scene inputs (oracle/scene.py: nothing of the product is loaded). Returns
+    (per-step seconds, threads, initial particles, params)."""
+    from oracle import scene
     threads = threads or os.cpu_count() or 1
-    p = mp.scene_params(config, n_cpu)
-    orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables(), threads=threads)
-    parts = mp.scene_particles(p, config, seed)
-    orc.upload_particles(**parts)
-    rf, seeds = mp.scene_tables(p, config, seed)
-    orc.set_tables(rf, seeds)
-    orc.set_field("fixedheat", mp.scene_fixed_heat(p, config))
+    orc, p, npart = scene.make_oracle(config, n, seed, threads=threads)
     for _ in range(warm):
         orc.bubblesim()
     times = []
@@ -161,23 +166,29 @@ def cpu_sample(config, n_cpu, seed, steps=1, warm=1, threads=None):
         t = time.perf_counter()
         orc.bubblesim()
         times.append(time.perf_counter() - t)
-    return times, threads, len(parts["flag"])
+    return times, threads, npart, p
 
 
 def run_reference(args, rank):
-    n_full = args.n or 256
+    """The reference arm: whole oracle steps of the same configuration at the
+    same grid on the host cores. A step at 256^3 takes minutes on the CPU, so
+    it times min(steps, --ref-steps) steps after min(warmup, --ref-warmup)."""
     if rank != 0:
         return
-    times, threads, npart = cpu_sample(args.config, args.cpu_n, args.seed, steps=args.steps, warm=args.warmup)
-    scale = (n_full / args.cpu_n) ** 3
-    per_step = sum(times) / len(times) * scale
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    n = args.n or 256
+    steps = max(1, min(args.steps, args.ref_steps))
+    warm = min(args.warmup, args.ref_warmup)
+    t0 = time.perf_counter()
+    times, threads, npart, p = oracle_steps(args.config, n, replica_seed(args.seed, rank), steps, warm)
+    per_step = sum(times) / len(times)
     value = 1.0 / per_step
-    sample = (f"oracle step of the same configuration on a {args.cpu_n}^3 grid ({npart} particles), "
-              f"time scaled by the cell ratio ({scale:.0f}x) to {n_full}^3")
+    sample = (f"{steps} whole oracle step(s) of the same configuration at {n}^3 ({npart} particles) after "
+              f"{warm} warm-up step(s), {threads} host threads; {time.perf_counter() - t0:.0f} s including set-up")
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": f"bubble column {n_full}^3 (CPU oracle sample)", "grid": n_full},
+           "steps": steps, "steps_requested": args.steps, "warmup": warm, "ms_per_step": per_step * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (CG dots in f64)",
+           "data": "synthetic", "config": workload_config(p, npart, args.seed, world),
            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -243,7 +254,7 @@ PRE_PROJECTION = [("hashAndSortParticles",), ("addexternalforce",), ("computeLev
                   ("sweepLSAndMardGrid",), ("markSoloAirParticle",), ("computesurfacetension",),
                   ("mapvelp2g_bubble",), ("enforceDragForce",), ("sweepPhi", 1), ("sweepU", 1), ("sweepPhi", 0),
                   ("sweepU", 0), ("setWaterBoundaryU", 1), ("setWaterBoundaryU", 0)]
-STEP_FIELDS = ["press", "waterux", "wateruy", "wateruz", "airux", "airuy", "airuz", "lsmerge", "tp"]
+STEP_FIELDS = ["press", "waterux", "wateruy", "wateruz", "airux", "airuy", "airuz", "lsmerge"]
 
 
 def rel_l2(a, b):
@@ -262,6 +273,7 @@ def precision_report(sim, mp, stream, fp64_steps):
     (2) one whole step from the same checkpoint in each form, with the
     relative L2 difference of every output field; (3) the FP64 form's
     steps/s over `fp64_steps` steps (CUDA events on the context stream)."""
+    import numpy as np
     import torch
     p0 = sim.get_params()
     for st in PRE_PROJECTION:
@@ -300,9 +312,17 @@ def precision_report(sim, mp, stream, fp64_steps):
         sim.bubblesim()
         snaps[name] = {f: sim.get_field(f) for f in STEP_FIELDS}
         parts = sim.download_particles()
-        snaps[name]["pos"], snaps[name]["vel"] = parts["pos"], parts["vel"]
-    out["step_fields_rel_l2"] = {f: rel_l2(snaps["mixed"][f], snaps["fp64"][f]) for f in snaps["mixed"]
+        v = parts["vel"].astype(np.float64)
+        gas = (parts["flag"] == mp.TYPEAIR) | (parts["flag"] == mp.TYPEAIRSOLO)
+        snaps[name]["particle_kinetic_energy"] = float((parts["mass"] * (v * v).sum(1)).sum())
+        snaps[name]["gas_particle_mean_z"] = float(parts["pos"][gas, 2].astype(np.float64).mean())
+        snaps[name]["particles"] = len(parts["flag"])
+    # per cell / face: relative L2 difference; particles (whose order after the
+    # step's re-sorts is not comparable index by index): whole-domain sums
+    out["step_fields_rel_l2"] = {f: rel_l2(snaps["mixed"][f], snaps["fp64"][f]) for f in STEP_FIELDS
                                  if snaps["mixed"][f].shape == snaps["fp64"][f].shape}
+    out["step_particles_rel"] = {q: abs(snaps["mixed"][q] - snaps["fp64"][q]) / max(abs(snaps["fp64"][q]), 1e-30)
+                                 for q in ("particle_kinetic_energy", "gas_particle_mean_z", "particles")}
     # the FP64 form's throughput
     sim.set_params(p0)
     sim.restore(blob)
@@ -319,7 +339,7 @@ def precision_report(sim, mp, stream, fp64_steps):
     out["fp64_form"] = {"value": fp64_steps / (ms / 1e3), "unit": "steps/s", "steps": fp64_steps,
                         "ms_per_step": ms / fp64_steps,
                         "what": "the same step with the projection (divergence, CG vectors and scalars, "
-                                "gradient) in FP64"}
+                                "gradient) and the heat solve in FP64"}
     sim.set_params(p0)
     return out
 
@@ -390,6 +410,7 @@ def main():
     sim = mp.Sim.from_config(args.config, args.n, replica_seed(args.seed, rank))
     p = sim.params
     n = p.nx * p.ny * p.nz
+    npart0 = int(sim.state().par_num_now)
     stream = torch.cuda.ExternalStream(sim.stream_handle())
     for _ in range(args.warmup):
         sim.bubblesim()
@@ -506,13 +527,7 @@ def main():
     out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (CG dots, alpha/beta in f64)", "data": "synthetic",
-           "config": {"workload": f"bubble column {p.nx}^3: liquid z<0.8, 200 air bubbles r~U[0.01,0.04], "
-                                  f"8 jittered particles/cell, dt=1/{1.0 / p.dt:.0f} (1/240 x (64/n)^2), FLIP 0.95, "
-                                  f"CG rel 1e-6 (FP32 vectors, "
-                                  f"FP64 dots), marching cubes every step",
-                      "grid": p.nx, "particles": int(st.par_num_now), "seed": args.seed,
-                      "l2": "inputs larger than L2 (particle streams alone are ~5 GB)",
-                      "parallelism": f"replicas x{world}"},
+           "config": workload_config(p, npart0, args.seed, world),
            "roofline": roof, "pcg_hbm_gbs": pcg_gbs,
            "pcg_roofline": {"achieved": pcg_gbs, "peak": peak, "unit": "GB/s", "frac": pcg_gbs / peak,
                             "note": "both CG passes, 34 B/cell/iteration algorithmic"},
@@ -529,24 +544,12 @@ def main():
         out["fwd_adjoint"] = fwd_adjoint(args, nx, local, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            times, threads, npart = cpu_sample(args.config, args.cpu_n, args.seed)
-            scale = (p.nx / args.cpu_n) ** 3
-            out["cpu_baseline"] = {"value": 1.0 / (times[0] * scale), "unit": "steps/s", "cores": threads,
-                                   "kind": "port",
-                                   "sample": f"one oracle step of the same configuration on a {args.cpu_n}^3 grid "
-                                             f"({npart} particles, {times[0]:.2f} s), scaled by the cell ratio "
-                                             f"{scale:.0f}x to {p.nx}^3"}
-            # the same restatement on one host thread (the reference's host code is serial)
-            try:
-                n1 = max(16, args.cpu_n // 2)
-                t1, _, np1 = cpu_sample(args.config, n1, args.seed, threads=1)
-                s1 = (p.nx / n1) ** 3
-                out["cpu_baseline"]["single_thread"] = {
-                    "value": 1.0 / (t1[0] * s1), "unit": "steps/s", "cores": 1,
-                    "sample": f"one oracle step on a {n1}^3 grid ({np1} particles, {t1[0]:.2f} s), "
-                              f"scaled by {s1:.0f}x to {p.nx}^3"}
-            except Exception as e:
-                out["cpu_baseline"]["single_thread"] = {"value": None, "sample": f"failed: {e}"}
+            t0 = time.perf_counter()
+            times, threads, npart, _ = oracle_steps(args.config, nx, args.seed, 1, 0)
+            out["cpu_baseline"] = {"value": 1.0 / times[0], "unit": "steps/s", "cores": threads, "kind": "port",
+                                   "sample": f"one whole oracle step of the same configuration at {nx}^3 "
+                                             f"({npart} particles, {times[0]:.1f} s; "
+                                             f"{time.perf_counter() - t0:.0f} s with set-up), no warm-up"}
         except Exception as e:   # the baseline is reported, not required
             out["cpu_baseline"] = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
                                    "sample": f"failed: {e}"}

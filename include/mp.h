@@ -75,7 +75,7 @@ extern "C" {
 #define MP_TOL_REF_ABS   0   /* stop when r.r < cg_tol*n  (spray.cu:1619,1666) */
 #define MP_TOL_REL       1   /* stop when |r| <= cg_tol*|b|                    */
 #define MP_PREC_MIXED    0   /* FP32 vectors, FP64 dots/alpha/beta            */
-#define MP_PREC_FP64     1   /* divergence, CG and gradient in FP64           */
+#define MP_PREC_FP64     1   /* divergence, pressure CG, gradient and the heat CG in FP64 */
 #define MP_COEF_REF      0   /* constant-coefficient Laplacian (reference)    */
 #define MP_COEF_GFM      1   /* variable density, ghost-fluid face weights (extension; MP_PREC_MIXED only) */
 
@@ -543,6 +543,29 @@ int mp_set_output(void* ctx, const mp_output* out);
  * MP_PREC_FP64 in FP64 with a 1e-13 relative CG stop. States are kept every
  * `checkpoint_every` steps and recomputed segment by segment backwards. */
 int mp_adj_record(void* ctx, int nsteps, int checkpoint_every);
+/* The recorded program as a differentiable map of the particles' initial
+ * state to their final state, (x0, v0) -> (xT, vT), with the general
+ * vector-Jacobian product of it (no counterpart in the reference).
+ * Every array is a device array of doubles, xyz per particle in the order the
+ * particles had at mp_adj_record; a NULL member of `in` means the recorded
+ * values, a NULL member of `dout` a zero cotangent, a NULL member of `out` or
+ * `din` that the result is not wanted.
+ * mp_adj_forward replays the program from `in` and writes `out`.
+ * mp_step_adjoint replays it from `in` and writes the cotangents of the
+ * initial state, din = J^T dout, by the reverse sweep (the transposed splat,
+ * extrapolation, wall rules, projection as a second CG solve on the pressure
+ * matrix, FLIP/PIC gather and advection), recomputing each segment of
+ * `checkpoint_every` steps from its checkpoint.
+ * mp_adj_level_set_loss evaluates the loss of mp_adj_set_targets at final
+ * positions `pos` and writes dloss/dpos (NULL: not wanted), so the loss can
+ * be composed with the map. */
+typedef struct mp_grad {
+    double* pos;   /* xyz per particle */
+    double* vel;   /* xyz per particle */
+} mp_grad;
+int mp_adj_forward(void* ctx, int precision, const mp_grad* in, mp_grad* out);
+int mp_step_adjoint(void* ctx, int precision, const mp_grad* in, const mp_grad* dout, mp_grad* din);
+int mp_adj_level_set_loss(void* ctx, int precision, const double* pos, double* loss, double* dloss_dpos);
 int mp_adj_set_targets(void* ctx, const float* samples3, int nsamples);
 int mp_adj_info(void* ctx, int* np, int* nsteps);
 int mp_adj_loss(void* ctx, int precision, const double* v0, double* loss);

@@ -15,7 +15,9 @@ pytestmark = pytest.mark.gpu
 def _setup(mp, n, steps, every, seed=2017004, nsamples=1024):
     import torch
     sim = mp.Sim.from_config(4, n, seed)
-    v0 = torch.from_numpy(sim.download_particles()["vel"].astype(np.float64)).cuda()
+    parts = sim.download_particles()
+    v0 = torch.from_numpy(parts["vel"].astype(np.float64)).cuda()
+    sim._x0_recorded = torch.from_numpy(parts["pos"].astype(np.float64)).cuda()
     sim.adj_record(steps, every)
     sim.adj_set_targets(mp.dam_break_targets(nsamples, seed, height=0.3))
     return sim, v0
@@ -106,4 +108,55 @@ def test_record_rejects_programs_outside_the_adjoint(mp):
     sim = mp.Sim.from_config(1, 32, 2017001)   # air bubble: not FLUID-only
     with pytest.raises(mp.MPError):
         sim.adj_record(2, 1)
+    sim.close()
+
+
+def test_vector_jacobian_product_matches_central_differences(mp):
+    """mp_step_adjoint with arbitrary cotangents w on the final positions and
+    velocities: <J^T w, d> equals the central difference of <w, f(x0, v0)>
+    along seeded directions d of the initial velocities and of the initial
+    positions (FP64 replays of the recorded program)."""
+    import torch
+    sim, v0 = _setup(mp, 32, 6, 3)
+    x0 = sim._x0_recorded
+    xT, vT = sim.adj_forward(x0, v0, mp.PREC_FP64)
+    gen = torch.Generator(device="cpu").manual_seed(21)
+    wx = torch.randn(xT.shape, generator=gen, dtype=torch.float64).cuda()
+    wv = torch.randn(vT.shape, generator=gen, dtype=torch.float64).cuda()
+    x0b, v0b = sim.step_adjoint(x0, v0, wx, wv, mp.PREC_FP64)
+    assert torch.isfinite(x0b).all() and torch.isfinite(v0b).all()
+
+    def f(x, v):
+        a, b = sim.adj_forward(x, v, mp.PREC_FP64)
+        return float((a * wx).sum() + (b * wv).sum())
+
+    for i, d in enumerate(_directions(v0, 3, 23)):
+        eps = 1e-6
+        fd = (f(x0, v0 + eps * d) - f(x0, v0 - eps * d)) / (2 * eps)
+        ad = float((v0b * d).sum())
+        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), f"v direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
+    for i, d in enumerate(_directions(v0, 3, 29)):
+        eps = 1e-8
+        fd = (f(x0 + eps * d, v0) - f(x0 - eps * d, v0)) / (2 * eps)
+        ad = float((x0b * d).sum())
+        assert abs(fd - ad) <= 1e-4 * max(abs(fd), abs(ad)), f"x direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
+    sim.close()
+
+
+def test_autograd_composition_equals_the_loss_gradient(mp):
+    """The loss composed through autograd, level_set_loss(mp_step(x0, v0)[0]),
+    gives the gradient mp_adj_gradient computes for the same program; backward
+    runs only for the inputs that ask for it."""
+    import torch
+    sim, v0 = _setup(mp, 32, 4, 2)
+    L64, g64 = sim.adj_gradient(v0, mp.PREC_FP64)
+    x = sim._x0_recorded.clone()
+    v = v0.clone().requires_grad_(True)
+    xT, vT = mp.mp_step(x, v, sim, mp.PREC_FP64)
+    loss = mp.level_set_loss(xT, sim, mp.PREC_FP64)
+    loss.backward()
+    assert abs(float(loss.detach()) - L64) <= 1e-12 * abs(L64)
+    assert x.grad is None
+    rel = float((v.grad - g64).norm() / g64.norm())
+    assert rel <= 1e-10, f"composed gradient differs by {rel:.3e}"
     sim.close()

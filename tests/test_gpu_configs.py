@@ -67,23 +67,47 @@ def test_one_step_non_cubic(mp, oracle_mod, config):
     sim.close()
 
 
-# configuration: (grid, steps, {quantity: bound}); None = not bounded
+# The stated drift. The GPU and the oracle agree bit for bit until the first
+# FP32 rounding of a CG scalar or of an SPH force sum falls the other way
+# (step 2 of the rising bubble, step ~75 of pool boiling, never in 200 steps
+# of melting/freezing at 32^3); from there the difference grows at the flow's
+# own rate -- about x10 per step in the rising bubble, whose solo-air SPH
+# particles make it chaotic -- so per-particle and per-cell fields
+# decorrelate within ~10 steps while whole-domain quantities stay close.
+# configuration: grid, steps, and per checked step {quantity: bound}
+# (quantities of parity_util.drift; agg_* are relative differences of
+# parity_util.aggregates). The bounds are 3-10x the measured drift.
 DRIFT_CASES = {
-    1: (32, 20, None),
-    2: (32, 100, None),
-    3: (32, 200, None),
+    1: (32, 20, {
+        4: {"press": 1e-5, "lsmerge": 1e-5, "waterux": 1e-4, "wateruy": 1e-4, "wateruz": 1e-4, "airux": 1e-4,
+            "airuy": 1e-4, "airuz": 1e-4, "mark": 0.0, "count": 0.0, "pos": 1e-3, "vel": 1e-2},
+        20: {"agg_kinetic": 2e-2, "agg_gas_z": 5e-3, "agg_liquid_z": 2e-4, "agg_fluid_cells": 2e-2,
+             "agg_gas_cells": 5e-2, "count": 0.0, "mark": 0.05},
+    }),
+    2: (32, 100, {
+        60: "exact",
+        100: {"agg_kinetic": 0.5, "agg_temp": 1e-2, "agg_gas_z": 0.2, "agg_liquid_z": 2e-3,
+              "agg_fluid_cells": 2e-2, "count": 1e-2, "mark": 0.1},
+    }),
+    3: (32, 200, {200: "exact"}),
 }
 
 
 @pytest.mark.parametrize("config", sorted(DRIFT_CASES))
 def test_drift_over_steps(mp, oracle_mod, config):
-    n, steps, bounds = DRIFT_CASES[config]
+    n, steps, checks = DRIFT_CASES[config]
     sim, orc = make_pair(mp, oracle_mod, config, n, 2017_300 + config)
-    for _ in range(steps):
+    for s in range(1, steps + 1):
         sim.bubblesim()
         orc.bubblesim()
-    d = drift(snapshot(sim), snapshot(orc))
-    print(f"config {config}, {steps} steps:", {k: f"{v:.2e}" for k, v in d.items()})
-    for q, b in (bounds or {}).items():
-        assert d[q] <= b, f"config {config} after {steps} steps: {q} drift {d[q]:.3e} > {b:.1e}"
+        if s not in checks:
+            continue
+        g, r = snapshot(sim), snapshot(orc)
+        if checks[s] == "exact":
+            bad = compare(g, r, exact=True)
+            assert not bad, f"config {config} step {s}: not bit-identical: {bad[:3]}"
+            continue
+        d = drift(g, r)
+        for q, b in checks[s].items():
+            assert d[q] <= b, f"config {config} after {s} steps: {q} drift {d[q]:.3e} > {b:.1e}"
     sim.close()
