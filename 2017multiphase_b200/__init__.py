@@ -86,8 +86,9 @@ class MPSceneInfo(C.Structure):
 
 
 class MPGrad(C.Structure):
-    """mp_grad: device arrays of doubles, xyz per particle (NULL members allowed)."""
-    _fields_ = [("pos", C.c_void_p), ("vel", C.c_void_p)]
+    """mp_grad: device arrays of doubles, xyz (or one temperature) per particle
+    (NULL members allowed)."""
+    _fields_ = [("pos", C.c_void_p), ("vel", C.c_void_p), ("temp", C.c_void_p)]
 
 
 class MPOutput(C.Structure):
@@ -184,6 +185,7 @@ def load_library() -> C.CDLL:
         "mp_kernel_timing_read": ([vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)], C.c_int),
         "mp_kernel_timing_reset": ([vp], C.c_int),
         "mp_launch_count": ([vp], C.c_int64),
+        "mp_work_counts": ([vp, C.POINTER(C.c_int64), C.c_int], C.c_int),
         "mp_scene_params": ([C.c_int, C.c_int, P], C.c_int),
         "mp_scene_particles": ([P, C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_int), vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "mp_scene_tables": ([P, C.c_int, C.c_uint64, vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
@@ -581,6 +583,7 @@ class Sim:
         """Runs `nsteps` steps from the current particles, recording the discrete
         state the derivative holds fixed (mp_adj_record)."""
         _check(self.lib.mp_adj_record(self.ctx, nsteps, checkpoint_every), self.ctx)
+        self._adj_heat = bool(self.params.b_heat_trans)
 
     def adj_set_targets(self, samples: np.ndarray):
         s = np.ascontiguousarray(samples, np.float32).reshape(-1, 3)
@@ -611,34 +614,43 @@ class Sim:
         return loss.value, g
 
     @staticmethod
-    def _grad(pos=None, vel=None):
-        return MPGrad(None if pos is None else pos.data_ptr(), None if vel is None else vel.data_ptr())
+    def _grad(pos=None, vel=None, temp=None):
+        return MPGrad(None if pos is None else pos.data_ptr(), None if vel is None else vel.data_ptr(),
+                      None if temp is None else temp.data_ptr())
 
-    def _empty3(self):
+    def _empty3(self, cols=3):
         import torch
-        return torch.empty((self.adj_num_particles(), 3), dtype=torch.float64,
-                           device=f"cuda:{torch.cuda.current_device()}")
+        shape = (self.adj_num_particles(), cols) if cols > 1 else (self.adj_num_particles(),)
+        return torch.empty(shape, dtype=torch.float64, device=f"cuda:{torch.cuda.current_device()}")
 
-    def adj_forward(self, x0=None, v0=None, precision: int = PREC_MIXED):
+    def adj_forward(self, x0=None, v0=None, precision: int = PREC_MIXED, T0=None):
         """The recorded program from initial positions/velocities (CUDA float64
-        (np, 3) tensors in recording order, None: the recorded ones) to the
-        final (xT, vT) (mp_adj_forward)."""
+        (np, 3) tensors in recording order, None: the recorded ones) and, when
+        the recording ran the heat stage, initial temperatures (np,), to the
+        final (xT, vT) or (xT, vT, TT) (mp_adj_forward)."""
         import torch
+        heat = getattr(self, "_adj_heat", False)
         xT, vT = self._empty3(), self._empty3()
-        inp, out = self._grad(x0, v0), self._grad(xT, vT)
+        TT = self._empty3(1) if heat else None
+        inp, out = self._grad(x0, v0, T0 if heat else None), self._grad(xT, vT, TT)
         torch.cuda.synchronize()
         _check(self.lib.mp_adj_forward(self.ctx, precision, C.byref(inp), C.byref(out)), self.ctx)
-        return xT, vT
+        return (xT, vT, TT) if heat else (xT, vT)
 
-    def step_adjoint(self, x0=None, v0=None, xT_bar=None, vT_bar=None, precision: int = PREC_MIXED):
-        """The vector-Jacobian product of the recorded program at (x0, v0):
-        (x0_bar, v0_bar) = J^T (xT_bar, vT_bar) (mp_step_adjoint)."""
+    def step_adjoint(self, x0=None, v0=None, xT_bar=None, vT_bar=None, precision: int = PREC_MIXED, T0=None,
+                     TT_bar=None):
+        """The vector-Jacobian product of the recorded program at (x0, v0[, T0]):
+        (x0_bar, v0_bar[, T0_bar]) = J^T (xT_bar, vT_bar[, TT_bar]) (mp_step_adjoint)."""
         import torch
+        heat = getattr(self, "_adj_heat", False)
         x0b, v0b = self._empty3(), self._empty3()
-        inp, dout, din = self._grad(x0, v0), self._grad(xT_bar, vT_bar), self._grad(x0b, v0b)
+        T0b = self._empty3(1) if heat else None
+        inp = self._grad(x0, v0, T0 if heat else None)
+        dout = self._grad(xT_bar, vT_bar, TT_bar if heat else None)
+        din = self._grad(x0b, v0b, T0b)
         torch.cuda.synchronize()
         _check(self.lib.mp_step_adjoint(self.ctx, precision, C.byref(inp), C.byref(dout), C.byref(din)), self.ctx)
-        return x0b, v0b
+        return (x0b, v0b, T0b) if heat else (x0b, v0b)
 
     def adj_level_set_loss(self, xT, precision: int = PREC_MIXED, grad: bool = True):
         """(L, dL/dxT) of the target-point loss at final positions xT."""
@@ -665,6 +677,12 @@ class Sim:
     def launch_count(self) -> int:
         return int(self.lib.mp_launch_count(self.ctx))
 
+    def work_counts(self) -> Dict[str, int]:
+        """mp_work_counts: sorts that reordered / found the order, CG iterations."""
+        a = (C.c_int64 * 3)()
+        _check(self.lib.mp_work_counts(self.ctx, a, 3), self.ctx)
+        return {"sort_full": int(a[0]), "sort_fast": int(a[1]), "cg_iters": int(a[2])}
+
     def stream_handle(self) -> int:
         s = C.c_void_p()
         _check(self.lib.mp_get_stream(self.ctx, C.byref(s)), self.ctx)
@@ -684,29 +702,35 @@ def _functions():
 
     class MPStep(torch.autograd.Function):
         """The recorded steps (Sim.adj_record) as a function of the particles'
-        initial positions and velocities, (x0, v0) -> (xT, vT), CUDA float64
-        (np, 3) tensors in recording order. backward is the hand-written
+        initial positions and velocities, and of their temperatures when the
+        recording ran the heat stage: (x0, v0[, T0]) -> (xT, vT[, TT]), CUDA
+        float64 tensors in recording order. backward is the hand-written
         adjoint (mp_step_adjoint), run only when a gradient is asked for. The
         discrete state (splat order, cell marks, extrapolation choices) is the
         recorded one, so the inputs should stay near the recorded state."""
 
         @staticmethod
-        def forward(ctx, x0, v0, sim, precision):
+        def forward(ctx, x0, v0, T0, sim, precision):
             x0 = x0.detach().to(torch.float64).contiguous()
             v0 = v0.detach().to(torch.float64).contiguous()
-            ctx.save_for_backward(x0, v0)
+            T0 = None if T0 is None else T0.detach().to(torch.float64).contiguous()
+            ctx.heat = T0 is not None
+            ctx.save_for_backward(x0, v0, T0)
             ctx.sim, ctx.precision = sim, precision
-            return sim.adj_forward(x0, v0, precision)
+            return sim.adj_forward(x0, v0, precision, T0=T0)
 
         @staticmethod
-        def backward(ctx, gx, gv):
-            if not (ctx.needs_input_grad[0] or ctx.needs_input_grad[1]):
-                return None, None, None, None
-            x0, v0 = ctx.saved_tensors
-            gx = None if gx is None else gx.to(torch.float64).contiguous()
-            gv = None if gv is None else gv.to(torch.float64).contiguous()
-            x0b, v0b = ctx.sim.step_adjoint(x0, v0, gx, gv, ctx.precision)
-            return (x0b if ctx.needs_input_grad[0] else None), (v0b if ctx.needs_input_grad[1] else None), None, None
+        def backward(ctx, *grads):
+            if not any(ctx.needs_input_grad[:3]):
+                return None, None, None, None, None
+            x0, v0, T0 = ctx.saved_tensors
+            g = [None if q is None else q.to(torch.float64).contiguous() for q in grads]
+            out = ctx.sim.step_adjoint(x0, v0, g[0], g[1], ctx.precision, T0=T0,
+                                       TT_bar=g[2] if ctx.heat else None)
+            x0b, v0b = out[0], out[1]
+            T0b = out[2] if ctx.heat else None
+            need = ctx.needs_input_grad
+            return (x0b if need[0] else None), (v0b if need[1] else None), (T0b if need[2] else None), None, None
 
     class LevelSetLoss(torch.autograd.Function):
         """sum_s phi(y_s)^2 of the final fluid distance field at the target
@@ -761,9 +785,10 @@ def _fn(i):
     return _FUNCS[i]
 
 
-def mp_step(x0, v0, sim, precision: int = PREC_MIXED):
-    """torch.autograd entry: (xT, vT) of the recorded steps from (x0, v0)."""
-    return _fn(0).apply(x0, v0, sim, precision)
+def mp_step(x0, v0, sim, precision: int = PREC_MIXED, T0=None):
+    """torch.autograd entry: (xT, vT) of the recorded steps from (x0, v0), or
+    (xT, vT, TT) from (x0, v0, T0) when the recording ran the heat stage."""
+    return _fn(0).apply(x0, v0, T0, sim, precision)
 
 
 def level_set_loss(xT, sim, precision: int = PREC_MIXED):

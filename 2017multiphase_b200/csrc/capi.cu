@@ -468,13 +468,12 @@ extern "C" int mp_adj_gradient(void* ctx, int precision, const double* v0, doubl
 extern "C" int mp_adj_forward(void* ctx, int precision, const mp_grad* in, mp_grad* out) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     if (!out || (precision != MP_PREC_MIXED && precision != MP_PREC_FP64)) return MP_ERR_ARG;
-    return k_adj_forward(c, precision, in ? in->pos : nullptr, in ? in->vel : nullptr, out->pos, out->vel);
+    return k_adj_forward(c, precision, in, out);
 }
 extern "C" int mp_step_adjoint(void* ctx, int precision, const mp_grad* in, const mp_grad* dout, mp_grad* din) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     if (!dout || !din || (precision != MP_PREC_MIXED && precision != MP_PREC_FP64)) return MP_ERR_ARG;
-    return k_adj_vjp(c, precision, in ? in->pos : nullptr, in ? in->vel : nullptr, dout->pos, dout->vel, din->pos,
-                     din->vel);
+    return k_adj_vjp(c, precision, in, dout, din);
 }
 extern "C" int mp_adj_level_set_loss(void* ctx, int precision, const double* pos, double* loss, double* dloss_dpos) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
@@ -657,6 +656,13 @@ extern "C" int mp_kernel_timing_reset(void* ctx) {
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
     for (int k = 0; k < MP_KT_COUNT; k++) { kt_harvest(c, k); c->kt_ms[k] = 0; c->kt_launch[k] = 0; }
     c->launches = 0;
+    for (int k = 0; k < MP_WC_COUNT; k++) c->work[k] = 0;
+    return MP_OK;
+}
+extern "C" int mp_work_counts(void* ctx, int64_t* counts, int n) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!counts || n < 0) return MP_ERR_ARG;
+    for (int k = 0; k < n && k < MP_WC_COUNT; k++) counts[k] = c->work[k];
     return MP_OK;
 }
 extern "C" int64_t mp_launch_count(void* ctx) {

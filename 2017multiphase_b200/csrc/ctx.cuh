@@ -101,6 +101,7 @@ struct MpCtx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pending[MP_KT_COUNT];
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt_pool;
     int64_t launches = 0;
+    int64_t work[MP_WC_COUNT] = {};   // mp_work_counts
 
     struct AdjTape* adj = nullptr;   // the adjoint module's tape (k_adjoint.cu)
 
@@ -210,9 +211,12 @@ int k_adj_record(MpCtx* c, int nsteps, int every);
 int k_adj_set_targets(MpCtx* c, const float* samples3, int nsamples);
 int k_adj_run(MpCtx* c, int precision, const double* v0, double* grad, double* loss);
 int k_adj_np(MpCtx* c, int* np, int* nsteps);
-int k_adj_forward(MpCtx* c, int precision, const double* x0, const double* v0, double* xT, double* vT);
-int k_adj_vjp(MpCtx* c, int precision, const double* x0, const double* v0, const double* xTb, const double* vTb,
-              double* x0b, double* v0b);
+int k_heat_cg_solve(MpCtx* c, const int8_t* mark, float* x, const float* b, int maxiter, int tolmode, float tol,
+                    int* iters, double* res);
+int k_heat_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, int maxiter, int tolmode, float tol,
+                    int* iters, double* res);
+int k_adj_forward(MpCtx* c, int precision, const mp_grad* in, mp_grad* out);
+int k_adj_vjp(MpCtx* c, int precision, const mp_grad* in, const mp_grad* dout, mp_grad* din);
 int k_adj_ls_loss(MpCtx* c, int precision, const double* xT, double* loss, double* xTb);
 int k_init_particle_heat(MpCtx* c);
 int k_pack_particles(MpCtx* c, int n, const float* pos3, const float* vel3, const int8_t* flag,

@@ -52,6 +52,12 @@ struct AdjTape {
     float* samples = nullptr;            // target points sorted by their base cell
     int nsamples = 0;
     uint32_t* s_off = nullptr;           // per base cell: range of its samples (n + 1)
+    // the heat stage (b_heat_trans): per step, the sort and the cell marks it ran on
+    bool heat = false;
+    std::vector<uint32_t*> order_h, off_h;
+    std::vector<int8_t*> mark_h;
+    float* T0 = nullptr;                 // initial temperatures (id order)
+    float* fixedheat = nullptr;          // the fixed-heat field (b_fixed_heat), or null
     // replay / adjoint work, sized for `wesz`-byte elements
     size_t wesz = 0;
     int wk_ns = 0;                       // samples the work was sized for
@@ -94,6 +100,10 @@ __global__ void k_ad_snapshot(int n, const uint32_t* __restrict__ ids, const flo
         v[3 * id] = q.x; v[3 * id + 1] = q.y; v[3 * id + 2] = q.z;
         m[id] = q.w;
     }
+}
+__global__ void k_ad_snapshot_T(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ heat,
+                                float* __restrict__ T) {
+    MP_GRID_LOOP(s, n) T[ids[s]] = heat[s].x;
 }
 __global__ void k_ad_count_nonfluid(int n, const float4* __restrict__ pos, uint32_t* cnt) {
     MP_GRID_LOOP(s, n) if (pflag(pos[s]) != MP_TYPEFLUID) atomicAdd(cnt, 1u);
@@ -740,6 +750,237 @@ __global__ void k_ad_p2g_adj(Grid g, int np, const uint32_t* __restrict__ order,
         xb[3 * p] += gxs; xb[3 * p + 1] += gys; xb[3 * p + 2] += gzs;
     }
 }
+// ---- heat (updateTemperature for FLUID particles, spray.cu:1889-1947) --------------
+// The heat stage after advection: mapHeatp2g_hash (cell temperature = sharp-
+// kernel mean of the particle temperatures over the 27 cells, spray_k.cu:
+// 4619-4653), the implicit diffusion solve (compb_heat, solver_cg_heat,
+// setBoundaryHeat), the change per cell (compTpChange) and mapHeatg2p
+// (T_p <- a (T_p + I dT) + (1 - a) I T_new, spray_k.cu:4655-4679), then
+// updateLatentHeat_k's clamp of FLUID temperatures to [melting, boiling].
+struct HeatCoef {
+    float alpha[MP_TYPECNT];
+    float dt;
+    __device__ __forceinline__ float al(int m) const {
+        float a = alpha[0];
+        #pragma unroll
+        for (int t = 1; t < MP_TYPECNT; t++) a = (m == t) ? alpha[t] : a;
+        return a;
+    }
+};
+// sorted-slot records (x, y, z, s) of the positions and one scalar per particle
+template <class T>
+__global__ void k_ad_slot_gather1(int np, const uint32_t* __restrict__ order, const T* __restrict__ x,
+                                  const T* __restrict__ sc, T* __restrict__ o4) {
+    MP_GRID_LOOP(s, np) {
+        const uint32_t p = order[s];
+        o4[4 * (size_t)s] = x[3 * p]; o4[4 * (size_t)s + 1] = x[3 * p + 1]; o4[4 * (size_t)s + 2] = x[3 * p + 2];
+        o4[4 * (size_t)s + 3] = sc[p];
+    }
+}
+template <class T>
+__global__ void k_ad_heat_p2g(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4, T dflt,
+                              T* __restrict__ Tc, T* __restrict__ Wc) {
+    const T scale = (T)1 / (T)g.h;
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        const T gx = (T)i + (T)0.5f, gy = (T)j + (T)0.5f, gz = (T)k + (T)0.5f;
+        T ws = 0, hs = 0;
+        for (int a = i - 1; a <= i + 1; a++) {
+            if (a < 0 || a > g.NX - 1) continue;
+            for (int b = j - 1; b <= j + 1; b++) {
+                if (b < 0 || b > g.NY - 1) continue;
+                const int k0 = max(k - 1, 0), k1 = min(k + 1, g.NZ - 1);
+                for (uint32_t q = off[cid(g, a, b, k0)]; q < off[cid(g, a, b, k1) + 1]; q++) {
+                    const T* r = xs4 + 4 * (size_t)q;
+                    const T dx = r[0] * scale - gx, dy = r[1] * scale - gy, dz = r[2] * scale - gz;
+                    const T w = sharpk(dx * dx + dy * dy + dz * dz);
+                    ws += w; hs += w * r[3];
+                }
+            }
+        }
+        Tc[idx] = ws > (T)0 ? hs / ws : dflt;
+        Wc[idx] = ws;
+    }
+}
+// right-hand side of the implicit solve: T h^2 / (alpha dt), with the fixed
+// temperature where one is set
+template <class T>
+__global__ void k_ad_heat_rhs(Grid g, const T* __restrict__ Tc, const int8_t* __restrict__ mark,
+                              const float* __restrict__ fixedheat, HeatCoef hc, T* __restrict__ b) {
+    MP_GRID_LOOP(idx, g.n) {
+        T t = Tc[idx];
+        if (fixedheat && fixedheat[idx] != MP_UNDEF_TEMPERATURE) t = (T)fixedheat[idx];
+        b[idx] = t * (T)g.h * (T)g.h / (T)hc.al(mark[idx]) / (T)hc.dt;
+    }
+}
+// setBoundaryHeat: a shell cell takes its inner neighbour's value (x, then y,
+// then z walls first)
+__device__ __forceinline__ int heat_src(const Grid& g, int i, int j, int k) {
+    if (i == g.NX - 1) return cid(g, i - 1, j, k);
+    if (i == 0) return cid(g, i + 1, j, k);
+    if (j == g.NY - 1) return cid(g, i, j - 1, k);
+    if (j == 0) return cid(g, i, j + 1, k);
+    if (k == g.NZ - 1) return cid(g, i, j, k - 1);
+    if (k == 0) return cid(g, i, j, k + 1);
+    return cid(g, i, j, k);
+}
+template <class T>
+__global__ void k_ad_heat_ext(Grid g, const T* __restrict__ in, T* __restrict__ out) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        out[idx] = in[heat_src(g, i, j, k)];
+    }
+}
+// its transpose as a gather: a cell collects its own cotangent (if it is not
+// a shell cell) and those of the shell neighbours that copy from it
+template <class T>
+__global__ void k_ad_heat_ext_adj(Grid g, const T* __restrict__ ob, T* __restrict__ ib) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        T acc = heat_src(g, i, j, k) == idx ? ob[idx] : (T)0;
+        const int nb[6][3] = {{i + 1, j, k}, {i - 1, j, k}, {i, j + 1, k}, {i, j - 1, k}, {i, j, k + 1}, {i, j, k - 1}};
+        for (int q = 0; q < 6; q++) {
+            const int a = nb[q][0], b = nb[q][1], c = nb[q][2];
+            if (a < 0 || a > g.NX - 1 || b < 0 || b > g.NY - 1 || c < 0 || c > g.NZ - 1) continue;
+            const int s = cid(g, a, b, c);
+            if (s != idx && heat_src(g, a, b, c) == idx) acc += ob[s];
+        }
+        ib[idx] = acc;
+    }
+}
+template <class T>
+__global__ void k_ad_heat_dT(int n, const T* __restrict__ Te, const T* __restrict__ Tc, const int8_t* __restrict__ mark,
+                             T* __restrict__ dT) {
+    MP_GRID_LOOP(idx, n) dT[idx] = mark[idx] != MP_TYPEBOUNDARY ? Te[idx] - Tc[idx] : (T)0;
+}
+// mapHeatg2p, then the latent-heat clamp of FLUID temperatures
+template <class T>
+__global__ void k_ad_heat_g2p(Grid g, int np, const T* __restrict__ x, const T* __restrict__ Tp,
+                              const T* __restrict__ dT, const T* __restrict__ Te, T a, T mp, T bp,
+                              T* __restrict__ T1, T* __restrict__ T2) {
+    MP_GRID_LOOP(p, np) {
+        const T X = x[3 * p] / (T)g.h - (T)0.5f, Y = x[3 * p + 1] / (T)g.h - (T)0.5f, Z = x[3 * p + 2] / (T)g.h - (T)0.5f;
+        const T id = tri<T>(dT, X, Y, Z, g.NX, g.NY, g.NZ, nullptr, nullptr, nullptr);
+        const T it = tri<T>(Te, X, Y, Z, g.NX, g.NY, g.NZ, nullptr, nullptr, nullptr);
+        const T t1 = a * (Tp[p] + id) + ((T)1 - a) * it;
+        T1[p] = t1;
+        T2[p] = t1 < mp ? mp : (t1 > bp ? bp : t1);
+    }
+}
+// particle side of the G2P transpose: the clamp passes nothing back where it
+// clamped; Tpb = a T1bar; xbar += T1bar (a grad I dT + (1 - a) grad I Te) / h.
+// T1bar is kept in q1 for the cell side.
+template <class T>
+__global__ void k_ad_heat_g2p_adj_p(Grid g, int np, const T* __restrict__ x, const T* __restrict__ T1,
+                                    const T* __restrict__ dT, const T* __restrict__ Te, T a, T mp, T bp,
+                                    T* __restrict__ Tb, T* __restrict__ q1, T* __restrict__ xb) {
+    MP_GRID_LOOP(p, np) {
+        const T t1 = T1[p];
+        const T b1 = (t1 < mp || t1 > bp) ? (T)0 : Tb[p];
+        q1[p] = b1;
+        Tb[p] = a * b1;
+        const T X = x[3 * p] / (T)g.h - (T)0.5f, Y = x[3 * p + 1] / (T)g.h - (T)0.5f, Z = x[3 * p + 2] / (T)g.h - (T)0.5f;
+        T gx1, gy1, gz1, gx2, gy2, gz2;
+        tri<T>(dT, X, Y, Z, g.NX, g.NY, g.NZ, &gx1, &gy1, &gz1);
+        tri<T>(Te, X, Y, Z, g.NX, g.NY, g.NZ, &gx2, &gy2, &gz2);
+        const T ih = (T)1 / (T)g.h;
+        xb[3 * p] += b1 * (a * gx1 + ((T)1 - a) * gx2) * ih;
+        xb[3 * p + 1] += b1 * (a * gy1 + ((T)1 - a) * gy2) * ih;
+        xb[3 * p + 2] += b1 * (a * gz1 + ((T)1 - a) * gz2) * ih;
+    }
+}
+// cell side: q_c = sum over the particles whose trilinear stencil holds c of
+// w_pc T1bar_p (candidates from the recorded cells, one cell wider when some
+// replay position left its recorded cell)
+template <class T, bool WIDE>
+__global__ void k_ad_heat_g2p_adj_c(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4,
+                                    T* __restrict__ q) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        const int wd = WIDE ? 2 : 1;
+        T acc = 0;
+        for (int a = i - wd; a <= i + wd; a++) {
+            if (a < 0 || a > g.NX - 1) continue;
+            for (int b = j - wd; b <= j + wd; b++) {
+                if (b < 0 || b > g.NY - 1) continue;
+                const int k0 = max(k - wd, 0), k1 = min(k + wd, g.NZ - 1);
+                for (uint32_t s = off[cid(g, a, b, k0)]; s < off[cid(g, a, b, k1) + 1]; s++) {
+                    const T* r = xs4 + 4 * (size_t)s;
+                    T px = r[0] / (T)g.h - (T)0.5f, py = r[1] / (T)g.h - (T)0.5f, pz = r[2] / (T)g.h - (T)0.5f;
+                    px = px < (T)0 ? (T)0 : (px > (T)g.NX ? (T)g.NX : px);
+                    py = py < (T)0 ? (T)0 : (py > (T)g.NY ? (T)g.NY : py);
+                    pz = pz < (T)0 ? (T)0 : (pz > (T)g.NZ ? (T)g.NZ : pz);
+                    const int bi = (int)(px < (T)(g.NX - 2) ? px : (T)(g.NX - 2));
+                    const int bj = (int)(py < (T)(g.NY - 2) ? py : (T)(g.NY - 2));
+                    const int bk = (int)(pz < (T)(g.NZ - 2) ? pz : (T)(g.NZ - 2));
+                    const int ei = i - bi, ej = j - bj, ek = k - bk;
+                    if (ei < 0 || ei > 1 || ej < 0 || ej > 1 || ek < 0 || ek > 1) continue;
+                    const T fx = ei ? px - (T)bi : (T)(bi + 1) - px, fy = ej ? py - (T)bj : (T)(bj + 1) - py;
+                    const T fz = ek ? pz - (T)bk : (T)(bk + 1) - pz;
+                    acc += fx * fy * fz * r[3];
+                }
+            }
+        }
+        q[idx] = acc;
+    }
+}
+// dT = Te - Tc off the walls: Tebar = (1 - a) q + dTbar, Tcbar = -dTbar
+template <class T>
+__global__ void k_ad_heat_mix(int n, const int8_t* __restrict__ mark, const T* __restrict__ q, T a, T* __restrict__ Teb,
+                              T* __restrict__ Tcb) {
+    MP_GRID_LOOP(idx, n) {
+        const T dtb = mark[idx] != MP_TYPEBOUNDARY ? a * q[idx] : (T)0;
+        Teb[idx] = ((T)1 - a) * q[idx] + dtb;
+        Tcb[idx] = -dtb;
+    }
+}
+// Tcbar += bbar h^2 / (alpha dt) where the right-hand side took the cell's
+// own temperature (bbar is zero off the solve's unknowns)
+template <class T>
+__global__ void k_ad_heat_rhs_adj(Grid g, const T* __restrict__ bb, const int8_t* __restrict__ mark,
+                                  const float* __restrict__ fixedheat, HeatCoef hc, T* __restrict__ Tcb) {
+    MP_GRID_LOOP(idx, g.n) {
+        if (fixedheat && fixedheat[idx] != MP_UNDEF_TEMPERATURE) continue;
+        Tcb[idx] += bb[idx] * (T)g.h * (T)g.h / (T)hc.al(mark[idx]) / (T)hc.dt;
+    }
+}
+// mapHeatp2g transpose per particle over the cells whose window holds its
+// recorded cell: Tpbar += Tcbar w / W, xbar += Tcbar (T_p - Tc) / W dw/dx
+template <class T>
+__global__ void k_ad_heat_p2g_adj(Grid g, int np, const T* __restrict__ x, const T* __restrict__ Tp,
+                                  const uint32_t* __restrict__ cellof, const T* __restrict__ Tc,
+                                  const T* __restrict__ Wc, const T* __restrict__ Tcb, T* __restrict__ Tb,
+                                  T* __restrict__ xb) {
+    const T scale = (T)1 / (T)g.h;
+    MP_GRID_LOOP(p, np) {
+        int ca, cb, cc; getijk3((int)cellof[p], g.NY, g.NZ, ca, cb, cc);
+        const T X = x[3 * p] * scale, Y = x[3 * p + 1] * scale, Z = x[3 * p + 2] * scale;
+        const T tp = Tp[p];
+        T tb = 0, gxs = 0, gys = 0, gzs = 0;
+        for (int a = ca - 1; a <= ca + 1; a++) {
+            if (a < 0 || a > g.NX - 1) continue;
+            for (int b = cb - 1; b <= cb + 1; b++) {
+                if (b < 0 || b > g.NY - 1) continue;
+                for (int c = cc - 1; c <= cc + 1; c++) {
+                    if (c < 0 || c > g.NZ - 1) continue;
+                    const int idx = cid(g, a, b, c);
+                    const T W = Wc[idx];
+                    if (!(W > (T)0)) continue;
+                    const T dx = X - ((T)a + (T)0.5f), dy = Y - ((T)b + (T)0.5f), dz = Z - ((T)c + (T)0.5f);
+                    const T r2 = dx * dx + dy * dy + dz * dz;
+                    const T w = sharpk(r2), kd = sharpk_d(r2);
+                    const T cb_ = Tcb[idx];
+                    tb += cb_ * w / W;
+                    const T sgr = cb_ * (tp - Tc[idx]) / W * kd * (T)2 * scale;
+                    gxs += sgr * dx; gys += sgr * dy; gzs += sgr * dz;
+                }
+            }
+        }
+        Tb[p] += tb;
+        xb[3 * p] += gxs; xb[3 * p + 1] += gys; xb[3 * p + 2] += gzs;
+    }
+}
+
 // the cell each particle had in a step's recorded sort
 __global__ void k_ad_cellof(int ncell, const uint32_t* __restrict__ order, const uint32_t* __restrict__ off,
                             uint32_t* __restrict__ cellof) {
@@ -767,8 +1008,11 @@ void k_adj_free(MpCtx* c) {
     for (auto* p : t->off) cudaFree(p);
     for (auto* p : t->mark) cudaFree(p);
     for (auto* p : t->phi) cudaFree(p);
+    for (auto* p : t->order_h) cudaFree(p);
+    for (auto* p : t->off_h) cudaFree(p);
+    for (auto* p : t->mark_h) cudaFree(p);
     for (void* p : {(void*)t->x0, (void*)t->v0, (void*)t->mass, (void*)t->ids, (void*)t->ids2, (void*)t->nearest,
-                    (void*)t->samples, (void*)t->s_off})
+                    (void*)t->samples, (void*)t->s_off, (void*)t->T0, (void*)t->fixedheat})
         if (p) cudaFree(p);
     for (void* p : t->wk) if (p) cudaFree(p);
     delete t;
@@ -800,9 +1044,17 @@ static int sorted_ids(MpCtx* c, AdjTape* t) {
 int k_adj_record(MpCtx* c, int nsteps, int every) {
     const mp_params& P = c->P;
     if (nsteps < 1 || every < 1) { c->err = "adj_record: nsteps and checkpoint interval must be positive"; return MP_ERR_ARG; }
-    if (P.b_correct_position || P.b_heat_trans || P.b_gen_gas || P.b_melt || P.b_freeze || P.b_solid) {
-        c->err = "adj_record: the adjoint covers the FLUID-only step without position correction, heat, gas, "
+    if (P.b_correct_position || P.b_gen_gas || P.b_melt || P.b_freeze || P.b_solid) {
+        c->err = "adj_record: the adjoint covers the FLUID-only step without position correction, gas, "
                  "melting, freezing or solids";
+        return MP_ERR_STATE;
+    }
+    const int sc = P.scene;
+    const bool boil = sc == MP_SCENE_BOILING || sc == MP_SCENE_BOILING_HIGHRES || sc == MP_SCENE_MELTANDBOIL ||
+                      sc == MP_SCENE_MELTANDBOIL_HIGHRES || sc == MP_SCENE_ALL;
+    if (P.b_heat_trans && (P.b_add_heat_bottom || boil)) {
+        c->err = "adj_record: the heat stage is differentiated without the bottom heat increment and outside "
+                 "the boiling scenes (whose heat matrix is not symmetric)";
         return MP_ERR_STATE;
     }
     const int np = c->np();
@@ -824,6 +1076,17 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     k_ad_iota<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids);
     k_ad_snapshot<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->pos, c->vel, t->x0, t->v0, t->mass);
     ADJ_LAUNCH(c);
+    t->heat = P.b_heat_trans != 0;
+    if (t->heat) {
+        MP_TRY(amalloc(c, &t->T0, np));
+        k_ad_snapshot_T<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->heat, t->T0);
+        ADJ_LAUNCH(c);
+        if (P.b_fixed_heat) {
+            MP_TRY(amalloc(c, &t->fixedheat, g.n));
+            MP_CUDA(c, cudaMemcpyAsync(t->fixedheat, c->fixedheat, sizeof(float) * g.n, cudaMemcpyDeviceToDevice,
+                                       c->stream));
+        }
+    }
     for (int k = 0; k < nsteps; k++) {
         MP_TRY(sorted_ids(c, t));
         MP_TRY(k_external_force(c));
@@ -847,6 +1110,22 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
         MP_TRY(sorted_ids(c, t));
         MP_TRY(k_collide_advect(c, true));
         MP_TRY(sorted_ids(c, t));
+        if (t->heat) {
+            // bubblesim without position correction: level set and marks of
+            // the advected particles, a sort, then updateTemperature
+            MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
+            MP_TRY(sorted_ids(c, t));
+            uint32_t* oh; uint32_t* fh; int8_t* mh;
+            MP_TRY(amalloc(c, &oh, np)); t->order_h.push_back(oh);
+            MP_TRY(amalloc(c, &fh, (size_t)g.n + 1)); t->off_h.push_back(fh);
+            MP_TRY(amalloc(c, &mh, g.n)); t->mark_h.push_back(mh);
+            MP_CUDA(c, cudaMemcpyAsync(oh, t->ids, sizeof(uint32_t) * np, cudaMemcpyDeviceToDevice, c->stream));
+            MP_CUDA(c, cudaMemcpyAsync(fh, c->cell_off, sizeof(uint32_t) * ((size_t)g.n + 1), cudaMemcpyDeviceToDevice,
+                                       c->stream));
+            MP_CUDA(c, cudaMemcpyAsync(mh, c->mark, g.n, cudaMemcpyDeviceToDevice, c->stream));
+            int st = k_heat(c);
+            if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+        }
         c->S.frame++;
     }
     // nearest particle of each cell at the end (cells from the last sort)
@@ -892,13 +1171,19 @@ enum {
     W_XS, W_VS, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
     W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2,
     W_IVA, W_IVG, W_IUP, W_IWT, W_IUE, W_IUF, W_IDU, W_ISEL, W_ISW,
-    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_S4A, W_S4B, W_PST, W_COUNT
+    W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_S4A, W_S4B, W_PST,
+    // heat: temperatures (current, next, segment states, cotangent), per-slot
+    // intermediates (cell temperature and weight, extended solution, change;
+    // particle temperature before the clamp), scratch, cached solves
+    W_T, W_TN, W_TS, W_TB, W_HT1, W_HTC, W_HWC, W_HTE, W_HDT, W_HB, W_HBB, W_HQ, W_HQ1, W_HTEB, W_HTCB, W_HST,
+    W_HS4, W_HCELLOF, W_COUNT
 };
 }
 
 // one step's intermediates (what its transpose reads)
 template <class T> struct Inter {
     T* va; T* vg; Fc<T> up, wt, ue, uf, du; uint8_t* sel; float* sw;
+    T* Tc; T* Wc; T* Te; T* dT; T* T1;   // heat stage (when recorded)
 };
 
 template <class T> struct Replay {
@@ -916,8 +1201,12 @@ template <class T> struct Replay {
         I.du = faces_of<T>(a(W_IDU) + j * nfs, g);
         I.sel = static_cast<uint8_t*>(t->wk[W_ISEL]) + j * nfs;
         I.sw = static_cast<float*>(t->wk[W_ISW]) + 3 * j * nfs;
+        const size_t n = t->heat ? (size_t)g.n : 0, npp = t->heat ? (size_t)np : 0;
+        I.Tc = a(W_HTC) + j * n; I.Wc = a(W_HWC) + j * n; I.Te = a(W_HTE) + j * n; I.dT = a(W_HDT) + j * n;
+        I.T1 = a(W_HT1) + j * npp;
         return I;
     }
+    T* seg_T(int s) const { return a(W_TS) + (size_t)s * np; }
 };
 
 template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
@@ -944,6 +1233,15 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     cnt[W_FLAG] = 4; es[W_FLAG] = sizeof(uint32_t);
     cnt[W_S4A] = cnt[W_S4B] = 4 * (size_t)t->np;
     cnt[W_PST] = n * (size_t)t->nsteps;   // each step's pressure from the first replay
+    const size_t hn = t->heat ? n : 0, hp = t->heat ? (size_t)t->np : 0;
+    for (int w : {W_T, W_TN, W_TB, W_HQ1}) cnt[w] = hp;
+    cnt[W_TS] = hp * (size_t)(nseg + t->every);
+    cnt[W_HT1] = hp * E;
+    for (int w : {W_HTC, W_HWC, W_HTE, W_HDT}) cnt[w] = hn * E;
+    for (int w : {W_HB, W_HBB, W_HQ, W_HTEB, W_HTCB}) cnt[w] = hn;
+    cnt[W_HST] = hn * (size_t)t->nsteps;
+    cnt[W_HS4] = 4 * hp;
+    cnt[W_HCELLOF] = hp; es[W_HCELLOF] = sizeof(uint32_t);
     for (int w = 0; w < W_COUNT; w++) {
         size_t bytes = es[w] * std::max<size_t>(cnt[w], 1);
         cudaError_t e = cudaMalloc(&t->wk[w], bytes);
@@ -960,12 +1258,94 @@ template <class T> static int cg_tol_of(const MpCtx* c, int& mode, float& tol, i
     return MP_OK;
 }
 
+static HeatCoef heat_coef(const mp_params& P) {
+    HeatCoef hc;
+    hc.alpha[MP_TYPEFLUID] = P.heatalpha_fluid; hc.alpha[MP_TYPEAIR] = P.heatalpha_air;
+    hc.alpha[MP_TYPEVACUUM] = P.heatalpha_vacuum; hc.alpha[MP_TYPESOLID] = P.heatalpha_solid;
+    hc.alpha[MP_TYPEAIRSOLO] = P.heatalpha_air; hc.alpha[MP_TYPEBOUNDARY] = 0;
+    hc.dt = P.dt;
+    return hc;
+}
+
+// the heat stage of step k on the advected positions x1: temperatures Tin ->
+// Tout, keeping its intermediates in I (its solve cached per step in W_HST)
+template <class T> static int heat_fwd(const Replay<T>& R, int k, const T* x1, const T* Tin, T* Tout,
+                                       const Inter<T>& I, bool solve) {
+    MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
+    cudaStream_t s = c->stream;
+    const mp_params& P = c->P;
+    const int nbp = mp_blocks(R.np, 256), nbc = mp_blocks(g.n, 256);
+    k_ad_slot_gather1<T><<<nbp, 256, 0, s>>>(R.np, t->order_h[k], x1, Tin, R.a(W_HS4));
+    k_ad_heat_p2g<T><<<nbc, 256, 0, s>>>(g, t->off_h[k], R.a(W_HS4), (T)P.default_temperature, I.Tc, I.Wc);
+    k_ad_heat_rhs<T><<<nbc, 256, 0, s>>>(g, I.Tc, t->mark_h[k], t->fixedheat, heat_coef(P), R.a(W_HB));
+    MP_CHECK_LAUNCH(c);
+    T* tn = R.a(W_HST) + (size_t)k * g.n;
+    if (solve) {
+        // the engine's stop rule in FP32 (absolute, as updateTemperature); FP64: relative 1e-13
+        const bool f64 = sizeof(T) == sizeof(double);
+        int it = 0; double res = 0;
+        int st = k_heat_cg_solve(c, t->mark_h[k], tn, R.a(W_HB), f64 ? std::max(P.heat_cg_max_iter, 6000) : P.heat_cg_max_iter,
+                                 f64 ? MP_TOL_REL : MP_TOL_REF_ABS, f64 ? 1e-13f : 0.01f, &it, &res);
+        if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+    }
+    if (P.b_extend_heat_to_boundary) k_ad_heat_ext<T><<<nbc, 256, 0, s>>>(g, tn, I.Te);
+    else k_ad_copy<T><<<nbc, 256, 0, s>>>(g.n, tn, I.Te);
+    k_ad_heat_dT<T><<<nbc, 256, 0, s>>>(g.n, I.Te, I.Tc, t->mark_h[k], I.dT);
+    k_ad_heat_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x1, Tin, I.dT, I.Te, (T)P.alpha_temp_trans, (T)P.melting_point,
+                                         (T)P.boiling_point, I.T1, Tout);
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
+// transpose of the heat stage: Tb holds the cotangent of Tout on entry and of
+// Tin on exit; the cotangent of x1 is added to xb
+template <class T> static int heat_adj(const Replay<T>& R, int k, const T* x1, const T* Tin, const Inter<T>& I, T* Tb,
+                                       T* xb) {
+    MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
+    cudaStream_t s = c->stream;
+    const mp_params& P = c->P;
+    const int nbp = mp_blocks(R.np, 256), nbc = mp_blocks(g.n, 256);
+    const T a = (T)P.alpha_temp_trans;
+    uint32_t* cellof = static_cast<uint32_t*>(t->wk[W_HCELLOF]);
+    uint32_t* flag = static_cast<uint32_t*>(t->wk[W_FLAG]);
+    k_ad_cellof<<<nbc, 256, 0, s>>>(g.n, t->order_h[k], t->off_h[k], cellof);
+    MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
+    k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x1, cellof, flag);
+    k_ad_heat_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, x1, I.T1, I.dT, I.Te, a, (T)P.melting_point,
+                                               (T)P.boiling_point, Tb, R.a(W_HQ1), xb);
+    k_ad_slot_gather1<T><<<nbp, 256, 0, s>>>(R.np, t->order_h[k], x1, R.a(W_HQ1), R.a(W_HS4));
+    MP_CHECK_LAUNCH(c);
+    uint32_t wide = 1;
+    MP_CUDA(c, cudaMemcpyAsync(&wide, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(c, cudaStreamSynchronize(s));
+    if (wide) k_ad_heat_g2p_adj_c<T, true><<<nbc, 256, 0, s>>>(g, t->off_h[k], R.a(W_HS4), R.a(W_HQ));
+    else k_ad_heat_g2p_adj_c<T, false><<<nbc, 256, 0, s>>>(g, t->off_h[k], R.a(W_HS4), R.a(W_HQ));
+    k_ad_heat_mix<T><<<nbc, 256, 0, s>>>(g.n, t->mark_h[k], R.a(W_HQ), a, R.a(W_HTEB), R.a(W_HTCB));
+    if (P.b_extend_heat_to_boundary) k_ad_heat_ext_adj<T><<<nbc, 256, 0, s>>>(g, R.a(W_HTEB), R.a(W_HBB));
+    else k_ad_copy<T><<<nbc, 256, 0, s>>>(g.n, R.a(W_HTEB), R.a(W_HBB));
+    MP_CHECK_LAUNCH(c);
+    // the transposed solve (the heat matrix is symmetric): relative stop, the
+    // cotangent's scale being arbitrary
+    {
+        const bool f64 = sizeof(T) == sizeof(double);
+        int it = 0; double res = 0;
+        int st = k_heat_cg_solve(c, t->mark_h[k], R.a(W_HB), R.a(W_HBB),
+                                 f64 ? std::max(P.heat_cg_max_iter, 6000) : P.heat_cg_max_iter, MP_TOL_REL,
+                                 f64 ? 1e-13f : 1e-6f, &it, &res);
+        if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+    }
+    k_ad_heat_rhs_adj<T><<<nbc, 256, 0, s>>>(g, R.a(W_HB), t->mark_h[k], t->fixedheat, heat_coef(P), R.a(W_HTCB));
+    k_ad_heat_p2g_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x1, Tin, cellof, I.Tc, I.Wc, R.a(W_HTCB), Tb, xb);
+    MP_CHECK_LAUNCH(c);
+    return MP_OK;
+}
+
 // one step of the replay from (x, v) to (xo, vo), keeping what its transpose
 // needs in I
 // The pressure solve's result is stored in pst (first replay) or copied from
 // it (segment replays): the inputs are the same bit for bit, so is the result.
 template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, const T* v, T* xo, T* vo,
-                                       const Inter<T>& I, bool solve) {
+                                       const T* Tin, T* Tout, const Inter<T>& I, bool solve) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
     cudaStream_t s = c->stream;
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
@@ -995,13 +1375,17 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     k_ad_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.va, I.uf, I.du, (T)P.flip_alpha, I.vg);
     k_ad_advect<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, xo, vo, (T)P.dt);
     MP_CHECK_LAUNCH(c);
+    if (t->heat) MP_TRY(heat_fwd<T>(R, k, xo, Tin, Tout, I, solve));
     return MP_OK;
 }
 
 // transpose of a step from its intermediates: (xb, vb) hold the adjoint of the
 // step's outputs on entry and of its inputs on exit
-template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, const Inter<T>& I, T* xb, T* vb) {
+template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, const T* x1, const T* Tin,
+                                       const Inter<T>& I, T* xb, T* vb, T* Tb) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
+    // the heat stage ran last, on the advected positions x1
+    if (t->heat) MP_TRY(heat_adj<T>(R, k, x1, Tin, I, Tb, xb));
     cudaStream_t s = c->stream;
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
     const mp_params& P = c->P;
@@ -1067,15 +1451,19 @@ template <class T> static int adj_loss_fwd(const Replay<T>& R, const T* x, doubl
 struct AdjIO {
     const double* x0 = nullptr;   // initial positions (NULL: the recorded ones)
     const double* v0 = nullptr;   // initial velocities (NULL: the recorded ones)
+    const double* T0 = nullptr;   // initial temperatures, one per particle (heat recorded; NULL: the recorded ones)
     double* xT = nullptr;         // final positions (NULL: not wanted)
     double* vT = nullptr;         // final velocities
+    double* TT = nullptr;         // final temperatures
     bool loss = false;            // evaluate the level-set loss; with `reverse`, seed the sweep with its cotangent
     double* loss_out = nullptr;
-    const double* xTb = nullptr;  // otherwise the seed: cotangents of the final positions / velocities (NULL: 0)
-    const double* vTb = nullptr;
+    const double* xTb = nullptr;  // otherwise the seed: cotangents of the final positions / velocities /
+    const double* vTb = nullptr;  // temperatures (NULL: 0)
+    const double* TTb = nullptr;
     bool reverse = false;         // run the reverse sweep
-    double* x0b = nullptr;        // cotangents of the initial positions / velocities (NULL: not wanted)
-    double* v0b = nullptr;
+    double* x0b = nullptr;        // cotangents of the initial positions / velocities / temperatures
+    double* v0b = nullptr;        // (NULL: not wanted)
+    double* T0b = nullptr;
 };
 
 template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
@@ -1094,9 +1482,15 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
     else k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->x0, x);
     if (io.v0) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, io.v0, v);
     else k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->v0, v);
+    const int nb1 = mp_blocks(t->np, 256);
+    T* Tc = t->heat ? R.a(W_T) : nullptr; T* Tn = t->heat ? R.a(W_TN) : nullptr;
+    if (t->heat) {
+        if (io.T0) k_ad_from_double<T><<<nb1, 256, 0, s>>>(t->np, io.T0, Tc);
+        else k_ad_from_float<T><<<nb1, 256, 0, s>>>(t->np, t->T0, Tc);
+    }
     MP_CHECK_LAUNCH(c);
     const int E = t->every, nseg = (t->nsteps + E - 1) / E;
-    std::vector<T*> ckx(nseg), ckv(nseg);
+    std::vector<T*> ckx(nseg), ckv(nseg), ckT(nseg, nullptr);
     const Inter<T> scratch = R.inter(0);
     for (int k = 0; k < t->nsteps; k++) {
         if (k % E == 0) {
@@ -1104,12 +1498,17 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
             ckx[sgi] = R.seg_x(sgi); ckv[sgi] = R.seg_v(sgi);
             MP_CUDA(c, cudaMemcpyAsync(ckx[sgi], x, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
             MP_CUDA(c, cudaMemcpyAsync(ckv[sgi], v, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
+            if (t->heat) {
+                ckT[sgi] = R.seg_T(sgi);
+                MP_CUDA(c, cudaMemcpyAsync(ckT[sgi], Tc, sizeof(T) * t->np, cudaMemcpyDeviceToDevice, s));
+            }
         }
-        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, scratch, true));
-        std::swap(x, xn); std::swap(v, vn);
+        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, Tc, Tn, scratch, true));
+        std::swap(x, xn); std::swap(v, vn); std::swap(Tc, Tn);
     }
     if (io.xT) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, x, io.xT);
     if (io.vT) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, v, io.vT);
+    if (io.TT && t->heat) k_ad_to_double<T><<<nb1, 256, 0, s>>>(t->np, Tc, io.TT);
     MP_CHECK_LAUNCH(c);
     if (io.loss) {
         double L = 0;
@@ -1133,6 +1532,11 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
         if (io.vTb) k_ad_from_double<T><<<nb3, 256, 0, s>>>(np3, io.vTb, vb);
         else MP_CUDA(c, cudaMemsetAsync(vb, 0, sizeof(T) * np3, s));
     }
+    T* Tb = t->heat ? R.a(W_TB) : nullptr;
+    if (t->heat) {
+        if (!io.loss && io.TTb) k_ad_from_double<T><<<nb1, 256, 0, s>>>(t->np, io.TTb, Tb);
+        else MP_CUDA(c, cudaMemsetAsync(Tb, 0, sizeof(T) * t->np, s));
+    }
     MP_CHECK_LAUNCH(c);
     // reverse sweep, segment by segment: the segment is replayed from its
     // start, each step's state and intermediates kept in its slot, then the
@@ -1141,15 +1545,19 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
         const int k0 = sg * E, len = std::min(t->nsteps, k0 + E) - k0;
         MP_CUDA(c, cudaMemcpyAsync(R.seg_x(nseg), ckx[sg], sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
         MP_CUDA(c, cudaMemcpyAsync(R.seg_v(nseg), ckv[sg], sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
-        for (int j = 0; j < len; j++) {
-            T* xo = j + 1 < len ? R.seg_x(nseg + j + 1) : R.a(W_XN);
-            T* vo = j + 1 < len ? R.seg_v(nseg + j + 1) : R.a(W_VN);
-            MP_TRY(fwd_step<T>(R, k0 + j, R.seg_x(nseg + j), R.seg_v(nseg + j), xo, vo, R.inter(j), false));
-        }
-        for (int j = len - 1; j >= 0; j--) MP_TRY(adj_step<T>(R, k0 + j, R.seg_x(nseg + j), R.inter(j), xb, vb));
+        if (t->heat)
+            MP_CUDA(c, cudaMemcpyAsync(R.seg_T(nseg), ckT[sg], sizeof(T) * t->np, cudaMemcpyDeviceToDevice, s));
+        auto xs = [&](int j) { return j < len ? R.seg_x(nseg + j) : R.a(W_XN); };
+        auto vs = [&](int j) { return j < len ? R.seg_v(nseg + j) : R.a(W_VN); };
+        auto Ts = [&](int j) -> T* { return !t->heat ? nullptr : (j < len ? R.seg_T(nseg + j) : R.a(W_TN)); };
+        for (int j = 0; j < len; j++)
+            MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), R.inter(j), false));
+        for (int j = len - 1; j >= 0; j--)
+            MP_TRY(adj_step<T>(R, k0 + j, xs(j), xs(j + 1), Ts(j), R.inter(j), xb, vb, Tb));
     }
     if (io.v0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, vb, io.v0b);
     if (io.x0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, xb, io.x0b);
+    if (io.T0b && t->heat) k_ad_to_double<T><<<nb1, 256, 0, s>>>(t->np, Tb, io.T0b);
     MP_CHECK_LAUNCH(c);
     MP_CUDA(c, cudaStreamSynchronize(s));
     return MP_OK;
@@ -1189,16 +1597,19 @@ int k_adj_run(MpCtx* c, int precision, const double* v0, double* grad, double* l
     if (precision == MP_PREC_FP64) return adj_run<double>(c, io);
     return adj_run<float>(c, io);
 }
-int k_adj_forward(MpCtx* c, int precision, const double* x0, const double* v0, double* xT, double* vT) {
+int k_adj_forward(MpCtx* c, int precision, const mp_grad* in, mp_grad* out) {
     AdjIO io;
-    io.x0 = x0; io.v0 = v0; io.xT = xT; io.vT = vT;
+    if (in) { io.x0 = in->pos; io.v0 = in->vel; io.T0 = in->temp; }
+    io.xT = out->pos; io.vT = out->vel; io.TT = out->temp;
     if (precision == MP_PREC_FP64) return adj_run<double>(c, io);
     return adj_run<float>(c, io);
 }
-int k_adj_vjp(MpCtx* c, int precision, const double* x0, const double* v0, const double* xTb, const double* vTb,
-              double* x0b, double* v0b) {
+int k_adj_vjp(MpCtx* c, int precision, const mp_grad* in, const mp_grad* dout, mp_grad* din) {
     AdjIO io;
-    io.x0 = x0; io.v0 = v0; io.xTb = xTb; io.vTb = vTb; io.reverse = true; io.x0b = x0b; io.v0b = v0b;
+    if (in) { io.x0 = in->pos; io.v0 = in->vel; io.T0 = in->temp; }
+    io.xTb = dout->pos; io.vTb = dout->vel; io.TTb = dout->temp;
+    io.reverse = true;
+    io.x0b = din->pos; io.v0b = din->vel; io.T0b = din->temp;
     if (precision == MP_PREC_FP64) return adj_run<double>(c, io);
     return adj_run<float>(c, io);
 }

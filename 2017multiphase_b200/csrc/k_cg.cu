@@ -698,9 +698,10 @@ __global__ void k_gfm_beta(Grid g, const int8_t* __restrict__ mark, const float*
     }
 }
 // S = diag^-1/2 on the unknowns (0 elsewhere) and bs = S b
+template <class R>
 __global__ void k_gfm_scale(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ bx,
-                            const float* __restrict__ by, const float* __restrict__ bz, const float* __restrict__ b,
-                            float* __restrict__ S, float* __restrict__ bs) {
+                            const float* __restrict__ by, const float* __restrict__ bz, const R* __restrict__ b,
+                            float* __restrict__ S, R* __restrict__ bs) {
     const int sI = g.NY * g.NZ, sJ = g.NZ;
     MP_GRID_LOOP(idx, g.n) {
         int i, j, k; getijk(g, idx, i, j, k);
@@ -717,14 +718,16 @@ __global__ void k_gfm_scale(Grid g, const int8_t* __restrict__ mark, const float
             sc = d > 0.0f ? 1.0f / sqrtf(d) : 0.0f;
         }
         S[idx] = sc;
-        bs[idx] = sc * b[idx];
+        bs[idx] = (R)sc * b[idx];
     }
 }
-__global__ void k_gfm_unscale(int n, const float* __restrict__ S, float* __restrict__ x) {
-    MP_GRID_LOOP(idx, n) x[idx] = S[idx] * x[idx];
+template <class R>
+__global__ void k_gfm_unscale(int n, const float* __restrict__ S, R* __restrict__ x) {
+    MP_GRID_LOOP(idx, n) x[idx] = (R)S[idx] * x[idx];
 }
 // u -= beta grad p on the interior faces of both velocity fields
-__global__ void k_subgrad_gfm(Grid g, const float* __restrict__ p, const float* __restrict__ bx,
+template <class R>
+__global__ void k_subgrad_gfm(Grid g, const R* __restrict__ p, const float* __restrict__ bx,
                               const float* __restrict__ by, const float* __restrict__ bz, float* wx, float* wy,
                               float* wz, float* ax, float* ay, float* az) {
     long long tot = (long long)g.nfx + g.nfy + g.nfz;
@@ -733,20 +736,20 @@ __global__ void k_subgrad_gfm(Grid g, const float* __restrict__ p, const float* 
         if (t < g.nfx) {
             int idx = (int)t; getijk3(idx, g.NY, g.NZ, i, j, k);
             if (i > 0 && i < g.NX) {
-                float d = bx[idx] * (p[cid(g, i, j, k)] - p[cid(g, i - 1, j, k)]) / g.h;
-                wx[idx] -= d; ax[idx] -= d;
+                const R d = (R)bx[idx] * (p[cid(g, i, j, k)] - p[cid(g, i - 1, j, k)]) / (R)g.h;
+                wx[idx] = (float)((R)wx[idx] - d); ax[idx] = (float)((R)ax[idx] - d);
             }
         } else if (t < (long long)g.nfx + g.nfy) {
             int idx = (int)(t - g.nfx); getijk3(idx, g.NY + 1, g.NZ, i, j, k);
             if (j > 0 && j < g.NY) {
-                float d = by[idx] * (p[cid(g, i, j, k)] - p[cid(g, i, j - 1, k)]) / g.h;
-                wy[idx] -= d; ay[idx] -= d;
+                const R d = (R)by[idx] * (p[cid(g, i, j, k)] - p[cid(g, i, j - 1, k)]) / (R)g.h;
+                wy[idx] = (float)((R)wy[idx] - d); ay[idx] = (float)((R)ay[idx] - d);
             }
         } else {
             int idx = (int)(t - g.nfx - g.nfy); getijk3(idx, g.NY, g.NZ + 1, i, j, k);
             if (k > 0 && k < g.NZ) {
-                float d = bz[idx] * (p[cid(g, i, j, k)] - p[cid(g, i, j, k - 1)]) / g.h;
-                wz[idx] -= d; az[idx] -= d;
+                const R d = (R)bz[idx] * (p[cid(g, i, j, k)] - p[cid(g, i, j, k - 1)]) / (R)g.h;
+                wz[idx] = (float)((R)wz[idx] - d); az[idx] = (float)((R)az[idx] - d);
             }
         }
     }
@@ -960,6 +963,7 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     MP_CUDA(c, cudaStreamSynchronize(s));
     *iters_out = (int)hflag[F_ITERS];
     *res_out = rr;
+    c->work[MP_WC_CG_ITERS] += hflag[F_ITERS];
     if (hflag[F_DONE] == DONE_TIMEOUT) {
         MP_CUDA(c, cudaMemsetAsync(Rd.count, 0, sizeof(unsigned int), s));
         c->err = "cg: a TMA tile wait ran out of time";
@@ -985,6 +989,31 @@ int k_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, int max
                           iters, res, MP_KT_CG_STENCIL);
 }
 
+// The heat matrix of updateTemperature for a given mark field (the adjoint's
+// replay and transposed solve; boiling scenes, whose VACUUM cells make the
+// matrix unsymmetric, are not differentiated), on the context's CG scratch.
+static HeatOp heat_op(MpCtx* c, const int8_t* mark) {
+    const mp_params& P = c->P;
+    HeatOp op;
+    op.g = c->G; op.mark = mark; op.dt = P.dt;
+    op.alpha[MP_TYPEFLUID] = P.heatalpha_fluid; op.alpha[MP_TYPEAIR] = P.heatalpha_air;
+    op.alpha[MP_TYPEVACUUM] = P.heatalpha_vacuum; op.alpha[MP_TYPESOLID] = P.heatalpha_solid;
+    op.alpha[MP_TYPEAIRSOLO] = P.heatalpha_air; op.alpha[MP_TYPEBOUNDARY] = 0;
+    op.boil = 0;
+    return op;
+}
+int k_heat_cg_solve(MpCtx* c, const int8_t* mark, float* x, const float* b, int maxiter, int tolmode, float tol,
+                    int* iters, double* res) {
+    return run_cg<float>(c, heat_op(c, mark), x, b, c->cg_r, c->cg_p, c->cg_z, maxiter, tolmode, tol, 0, iters, res,
+                         MP_KT_CG_STENCIL);
+}
+int k_heat_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, int maxiter, int tolmode, float tol,
+                    int* iters, double* res) {
+    const size_t n = (size_t)c->G.n;
+    return run_cg<double>(c, heat_op(c, mark), x, b, c->cg64 + 2 * n, c->cg64 + 3 * n, c->cg64 + 4 * n, maxiter,
+                          tolmode, tol, 0, iters, res, MP_KT_CG_STENCIL);
+}
+
 // project_CG_bubble (spray.cu:1590-1611)
 int k_project(MpCtx* c, int* iters, double* res) {
     const Grid& g = c->G;
@@ -1002,21 +1031,41 @@ int k_project(MpCtx* c, int* iters, double* res) {
         }
         float* bx = c->gfm_beta; float* by = bx + g.nfx; float* bz = by + g.nfy;
         float* x = c->press;
-        k_divergence<float><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
-                                                        c->au[0], c->au[1], c->au[2], c->divg, nullptr);
+        if (c->P.precision != MP_PREC_FP64)
+            k_divergence<float><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
+                                                            c->au[0], c->au[1], c->au[2], c->divg, nullptr);
         k_gfm_beta<<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, c->mark, c->lsmerge, 1.0f / c->P.density_ratio,
                                                                 bx, by, bz);
-        k_gfm_scale<<<nbk, 256, 0, c->stream>>>(g, c->mark, bx, by, bz, c->divg, c->gfm_s, c->cell_tmp);
-        c->launches += 3;
-        MP_CHECK_LAUNCH(c);
         GfmOp gop{g, c->mark, bx, by, bz, c->gfm_s};
-        rc = run_cg<float>(c, gop, x, c->cell_tmp, c->cg_r, c->cg_p, c->cg_z, c->P.cg_max_iter, c->P.cg_tol_mode,
-                           c->P.cg_tol, 0, &it, &rr, MP_KT_CG_STENCIL);
-        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
-        k_gfm_unscale<<<nbk, 256, 0, c->stream>>>(g.n, c->gfm_s, x);
-        k_subgrad_gfm<<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, x, bx, by, bz, c->wu[0], c->wu[1], c->wu[2],
-                                                                   c->au[0], c->au[1], c->au[2]);
-        c->launches += 2;
+        if (c->P.precision == MP_PREC_FP64) {
+            // the all-FP64 form: right-hand side, vectors and scalars in FP64
+            double* xd = c->cg64; double* bd = xd + g.n; double* rd = bd + g.n;
+            double* p0 = rd + g.n; double* p1 = p0 + g.n;
+            k_divergence<double><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
+                                                             c->au[0], c->au[1], c->au[2], bd, c->divg);
+            k_gfm_scale<double><<<nbk, 256, 0, c->stream>>>(g, c->mark, bx, by, bz, bd, c->gfm_s, bd);
+            c->launches += 3;
+            MP_CHECK_LAUNCH(c);
+            rc = run_cg<double>(c, gop, xd, bd, rd, p0, p1, c->P.cg_max_iter, c->P.cg_tol_mode, c->P.cg_tol, 0, &it,
+                                &rr, MP_KT_CG_STENCIL);
+            if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+            k_gfm_unscale<double><<<nbk, 256, 0, c->stream>>>(g.n, c->gfm_s, xd);
+            k_d2f<<<nbk, 256, 0, c->stream>>>(g.n, xd, x);
+            k_subgrad_gfm<double><<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, xd, bx, by, bz, c->wu[0], c->wu[1],
+                                                                               c->wu[2], c->au[0], c->au[1], c->au[2]);
+            c->launches += 3;
+        } else {
+            k_gfm_scale<float><<<nbk, 256, 0, c->stream>>>(g, c->mark, bx, by, bz, c->divg, c->gfm_s, c->cell_tmp);
+            c->launches += 3;
+            MP_CHECK_LAUNCH(c);
+            rc = run_cg<float>(c, gop, x, c->cell_tmp, c->cg_r, c->cg_p, c->cg_z, c->P.cg_max_iter, c->P.cg_tol_mode,
+                               c->P.cg_tol, 0, &it, &rr, MP_KT_CG_STENCIL);
+            if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+            k_gfm_unscale<float><<<nbk, 256, 0, c->stream>>>(g.n, c->gfm_s, x);
+            k_subgrad_gfm<float><<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, x, bx, by, bz, c->wu[0], c->wu[1],
+                                                                              c->wu[2], c->au[0], c->au[1], c->au[2]);
+            c->launches += 2;
+        }
     } else if (c->P.precision == MP_PREC_FP64) {
         double* x = c->cg64;
         double* b = x + g.n; double* r = b + g.n; double* p0 = r + g.n; double* p1 = p0 + g.n;

@@ -238,6 +238,7 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     uint32_t h_unsorted = 1;
     MP_CUDA(c, cudaMemcpyAsync(&h_unsorted, unsorted, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->work[h_unsorted ? MP_WC_SORT_FULL : MP_WC_SORT_FAST]++;
     if (!h_unsorted) {
         // already in cell order: the stable sort is the identity permutation;
         // the counts still have to run back to zero for the next sort

@@ -439,6 +439,7 @@ def main():
     ms = e0.elapsed_time(e1)
     launches = sim.launch_count()
     kt = {k: sim.kernel_timing_read(k) for k in classes}
+    work_counts = sim.work_counts()
     for k in classes:
         sim.kernel_timing(k, False)
     t_max = ms
@@ -490,38 +491,51 @@ def main():
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h / max(args.e2e_steps, 1))}
 
     # roofline of the dominant kernel class (by device time in the timed
-    # region); algorithmic bytes per launch from the compulsory-traffic model
-    # (each byte a launch must move, counted once; N_p particles, n cells)
+    # region); algorithmic bytes from the compulsory-traffic model (each byte
+    # a launch must move, counted once; N_p particles, n cells), per unit of
+    # work: a CG iteration for the CG passes (launches of an iteration batch
+    # after the stop test are not counted), a call otherwise; a sort that
+    # found the particles in cell order moves only positions and ranges
     peak, peak_kind = peaks()
     npart = int(sim.state().par_num_now)
-    model = {mp.KT_CG_STENCIL: ("k_cg_v4<PressOp,0> (direction + A p)", CG_DIR_BYTES_PER_CELL * n),
-             mp.KT_CG_UPDATE: ("k_cg_v4<PressOp,1> (x, r update)", CG_UPD_BYTES_PER_CELL * n),
-             mp.KT_P2G: ("k_p2g_water + k_p2g_air (water + air launches)", 29 * npart + 56 * n),
-             mp.KT_G2P: ("k_g2p", 37 * npart + 72 * n),
-             mp.KT_SORT: ("hash sort (count, scan, scatter, segment sort, gather)", 102 * npart + 8 * n),
-             mp.KT_LEVELSET: ("k_genlevelset", 13 * npart + 9 * n),
-             mp.KT_MC_DENS: ("k_mc_density (fused fluid + gas fields at 2x)", 13 * npart + 64 * n)}
+    wc = work_counts
+    model = {mp.KT_CG_STENCIL: ("k_cg_tma<PressOp,0> (direction p = r + beta p, A p, p.Ap)",
+                                CG_DIR_BYTES_PER_CELL * n * wc["cg_iters"], wc["cg_iters"]),
+             mp.KT_CG_UPDATE: ("k_cg_tma<PressOp,1> (A p, x and r update, r.r)",
+                               CG_UPD_BYTES_PER_CELL * n * wc["cg_iters"], wc["cg_iters"]),
+             mp.KT_P2G: ("k_p2g_water + k_p2g_air (water + air launches)", (29 * npart + 56 * n) * kt[mp.KT_P2G][1],
+                         kt[mp.KT_P2G][1]),
+             mp.KT_G2P: ("k_g2p", (37 * npart + 72 * n) * kt[mp.KT_G2P][1], kt[mp.KT_G2P][1]),
+             mp.KT_SORT: ("hash sort (count, scan, scatter, segment sort, gather)",
+                          (102 * npart + 8 * n) * wc["sort_full"] + (12 * npart + 8 * n) * wc["sort_fast"],
+                          wc["sort_full"] + wc["sort_fast"]),
+             mp.KT_LEVELSET: ("k_genlevelset", (13 * npart + 9 * n) * kt[mp.KT_LEVELSET][1], kt[mp.KT_LEVELSET][1]),
+             mp.KT_MC_DENS: ("k_mc_density (fused fluid + gas fields at 2x)", (13 * npart + 64 * n) * kt[mp.KT_MC_DENS][1],
+                             kt[mp.KT_MC_DENS][1])}
     dom = max(model, key=lambda k: kt[k][0])
-    ms_k, nl = kt[dom]
-    per_launch_s = ms_k / 1e3 / max(nl, 1)
-    alg = model[dom][1]
-    achieved = alg / per_launch_s / 1e9
+    ms_k = kt[dom][0]
+    units = max(model[dom][2], 1)
+    per_unit_s = ms_k / 1e3 / units
+    alg = model[dom][1] / units
+    achieved = alg / per_unit_s / 1e9
     traffic = TRAFFIC_PER_LAUNCH.get(names_kt(mp)[dom])
     cg_ms = kt[mp.KT_CG_STENCIL][0] + kt[mp.KT_CG_UPDATE][0]
-    cg_launch_pairs = max(kt[mp.KT_CG_STENCIL][1], 1)
-    pcg_gbs = (CG_DIR_BYTES_PER_CELL + CG_UPD_BYTES_PER_CELL) * n * cg_launch_pairs / (cg_ms / 1e3) / 1e9
+    pcg_gbs = (CG_DIR_BYTES_PER_CELL + CG_UPD_BYTES_PER_CELL) * n * max(wc["cg_iters"], 1) / (cg_ms / 1e3) / 1e9
     names = names_kt(mp)
     psrc = f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback"
     roof = {"kernel": model[dom][0], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": psrc,
             "traffic": (traffic(n, npart) if traffic else None), "algorithmic_bytes_per_launch": alg,
-            "avg_launch_ms": per_launch_s * 1e3}
+            "avg_launch_ms": per_unit_s * 1e3}
     cls_table = {}
-    for k, (nm, b) in model.items():
+    for k, (nm, b, u) in model.items():
         ms_c, nl_c = kt[k]
-        if nl_c:
-            a = b / (ms_c / 1e3 / nl_c) / 1e9
-            cls_table[names[k]] = {"ms": ms_c, "launches": nl_c, "algorithmic_GBps": a, "frac": a / peak}
+        if nl_c and ms_c > 0:
+            a = b / (ms_c / 1e3) / 1e9
+            cls_table[names[k]] = {"ms": ms_c, "launches": nl_c, "work_units": u, "algorithmic_GBps": a,
+                                   "frac": a / peak}
+    cls_table["sort"]["calls_reordering"] = wc["sort_full"]
+    cls_table["sort"]["calls_in_order"] = wc["sort_fast"]
 
     st = sim.state()
     out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
@@ -530,7 +544,7 @@ def main():
            "config": workload_config(p, npart0, args.seed, world),
            "roofline": roof, "pcg_hbm_gbs": pcg_gbs,
            "pcg_roofline": {"achieved": pcg_gbs, "peak": peak, "unit": "GB/s", "frac": pcg_gbs / peak,
-                            "note": "both CG passes, 34 B/cell/iteration algorithmic"},
+                            "note": "both CG passes, 34 B/cell/iteration algorithmic, per CG iteration"},
            "cg_iters_per_step": cg_iters / max(args.steps, 1),
            "mesh": {"verts": [int(v) for v in st.mc_verts], "triangles": [int(v) // 3 for v in st.mc_indices]},
            "kernel_classes": cls_table,

@@ -562,6 +562,7 @@ int mp_adj_record(void* ctx, int nsteps, int checkpoint_every);
 typedef struct mp_grad {
     double* pos;   /* xyz per particle */
     double* vel;   /* xyz per particle */
+    double* temp;  /* one per particle; used when the recording ran the heat stage */
 } mp_grad;
 int mp_adj_forward(void* ctx, int precision, const mp_grad* in, mp_grad* out);
 int mp_step_adjoint(void* ctx, int precision, const mp_grad* in, const mp_grad* dout, mp_grad* din);
@@ -592,6 +593,16 @@ int mp_kernel_timing_read(void* ctx, int kernel_class, double* ms, int64_t* laun
 int mp_kernel_timing_reset(void* ctx);
 /* Number of this library's kernel launches since the last reset. */
 int64_t mp_launch_count(void* ctx);
+/* Work counters since the last mp_kernel_timing_reset, for the byte models
+ * of the measurement: particle sorts that reordered the particles, sorts
+ * that found them already in cell order (keys and ranges only), and CG
+ * iterations performed (pressure and heat solves; the launches of an
+ * iteration batch after the stop test are not iterations). */
+#define MP_WC_SORT_FULL  0
+#define MP_WC_SORT_FAST  1
+#define MP_WC_CG_ITERS   2
+#define MP_WC_COUNT      3
+int mp_work_counts(void* ctx, int64_t* counts, int n);
 
 #ifdef __cplusplus
 }

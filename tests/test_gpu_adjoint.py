@@ -160,3 +160,88 @@ def test_autograd_composition_equals_the_loss_gradient(mp):
     rel = float((v.grad - g64).norm() / g64.norm())
     assert rel <= 1e-10, f"composed gradient differs by {rel:.3e}"
     sim.close()
+
+
+def _setup_heat(mp, n, steps, every, seed=2017006):
+    """The dam break with the heat stage on: a hot bottom plate held at 1.25,
+    initial temperatures 0.95 + 0.05 N(0, 1), FLIP/PIC temperature transfer
+    0.3, melting and boiling points outside the range reached (no clamp)."""
+    import torch
+    p = mp.scene_params(4, n)
+    p.b_heat_trans = 1; p.b_fixed_heat = 1; p.b_extend_heat_to_boundary = 1
+    p.heatalpha_fluid = 0.05; p.heatalpha_vacuum = 0.0001
+    p.default_temperature = 1.0; p.melting_point = 0.2; p.boiling_point = 5.0
+    p.alpha_temp_trans = 0.3
+    sim = mp.Sim.from_config(4, n, seed, params=p)
+    parts = sim.download_particles()
+    rng = np.random.default_rng(seed)
+    parts["temp"] = (0.95 + 0.05 * rng.standard_normal(len(parts["temp"]))).astype(np.float32)
+    sim.upload_particles(**parts)
+    fh = np.full(n ** 3, -1000.0, np.float32).reshape(n, n, n)
+    fh[1:-1, 1:-1, :4] = 1.25
+    sim.set_field("fixedheat", fh.ravel())
+    x0 = torch.from_numpy(parts["pos"].astype(np.float64)).cuda()
+    v0 = torch.from_numpy(parts["vel"].astype(np.float64)).cuda()
+    T0 = torch.from_numpy(parts["temp"].astype(np.float64)).cuda()
+    sim.adj_record(steps, every)
+    return sim, x0, v0, T0
+
+
+def test_heat_adjoint_matches_central_differences(mp):
+    """The heat stage's transpose (the splat of particle temperatures, the
+    implicit diffusion as a second solve on the symmetric heat matrix, the
+    boundary copy, the FLIP/PIC transfer back): <J^T w, d> against central
+    differences of the FP64 replay, along seeded directions of the initial
+    temperatures, velocities and positions, for random cotangents w on the
+    final positions, velocities and temperatures."""
+    import torch
+    sim, x0, v0, T0 = _setup_heat(mp, 32, 4, 2)
+    xT, vT, TT = sim.adj_forward(x0, v0, mp.PREC_FP64, T0=T0)
+    assert torch.isfinite(TT).all() and float((TT - T0).abs().max()) > 1e-4   # the heat stage did something
+    gen = torch.Generator(device="cpu").manual_seed(31)
+    wx = torch.randn(xT.shape, generator=gen, dtype=torch.float64).cuda()
+    wv = torch.randn(vT.shape, generator=gen, dtype=torch.float64).cuda()
+    wT = torch.randn(TT.shape, generator=gen, dtype=torch.float64).cuda()
+    x0b, v0b, T0b = sim.step_adjoint(x0, v0, wx, wv, mp.PREC_FP64, T0=T0, TT_bar=wT)
+
+    def f(x, v, T):
+        a, b, c = sim.adj_forward(x, v, mp.PREC_FP64, T0=T)
+        return float((a * wx).sum() + (b * wv).sum() + (c * wT).sum())
+
+    gd = torch.Generator(device="cpu").manual_seed(37)
+    for i in range(3):
+        d = torch.randn(T0.shape, generator=gd, dtype=torch.float64).cuda()
+        eps = 1e-6
+        fd = (f(x0, v0, T0 + eps * d) - f(x0, v0, T0 - eps * d)) / (2 * eps)
+        ad = float((T0b * d).sum())
+        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), f"T direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
+    for i, d in enumerate(_directions(v0, 2, 41)):
+        eps = 1e-6
+        fd = (f(x0, v0 + eps * d, T0) - f(x0, v0 - eps * d, T0)) / (2 * eps)
+        ad = float((v0b * d).sum())
+        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), f"v direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
+    for i, d in enumerate(_directions(v0, 2, 43)):
+        eps = 1e-8
+        fd = (f(x0 + eps * d, v0, T0) - f(x0 - eps * d, v0, T0)) / (2 * eps)
+        ad = float((x0b * d).sum())
+        assert abs(fd - ad) <= 1e-4 * max(abs(fd), abs(ad)), f"x direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
+    sim.close()
+
+
+def test_heat_autograd_and_fp32_against_fp64(mp):
+    """torch.autograd through the heat-recorded program: the gradient of
+    sum(TT^2) with respect to T0 from mp_step equals the FP64 VJP, and the
+    FP32 replay's gradient is within 1e-3 of the FP64 one."""
+    import torch
+    sim, x0, v0, T0 = _setup_heat(mp, 32, 4, 2)
+    T = T0.clone().requires_grad_(True)
+    xT, vT, TT = mp.mp_step(x0, v0, sim, mp.PREC_FP64, T0=T)
+    (TT * TT).sum().backward()
+    _, _, TT64 = sim.adj_forward(x0, v0, mp.PREC_FP64, T0=T0)
+    _, _, g64 = sim.step_adjoint(x0, v0, None, None, mp.PREC_FP64, T0=T0, TT_bar=2 * TT64)
+    assert float((T.grad - g64).norm() / g64.norm()) <= 1e-12
+    _, _, TT32 = sim.adj_forward(x0, v0, mp.PREC_MIXED, T0=T0)
+    _, _, g32 = sim.step_adjoint(x0, v0, None, None, mp.PREC_MIXED, T0=T0, TT_bar=2 * TT32)
+    rel = float((g32 - g64).norm() / g64.norm())
+    assert rel <= 1e-3, f"FP32 heat gradient rel err {rel:.3e}"
+    sim.close()
