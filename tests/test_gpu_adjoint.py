@@ -177,7 +177,7 @@ def _setup_heat(mp, n, steps, every, seed=2017006):
     rng = np.random.default_rng(seed)
     parts["temp"] = (0.95 + 0.05 * rng.standard_normal(len(parts["temp"]))).astype(np.float32)
     sim.upload_particles(**parts)
-    fh = np.full(n ** 3, -1000.0, np.float32).reshape(n, n, n)
+    fh = np.full(n ** 3, -10000.0, np.float32).reshape(n, n, n)   # MP_UNDEF_TEMPERATURE: not held
     fh[1:-1, 1:-1, :4] = 1.25
     sim.set_field("fixedheat", fh.ravel())
     x0 = torch.from_numpy(parts["pos"].astype(np.float64)).cuda()
