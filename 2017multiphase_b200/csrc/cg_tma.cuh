@@ -75,12 +75,18 @@ __device__ __forceinline__ bool tt_bar_test(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 // waits for the barrier's phase `parity` to complete; false after TT_WAIT_NS
+// (the clock is read once every 256 polls: a poll already suspends the warp
+// for a while, and reading the clock on every poll costs issue slots)
 __device__ __forceinline__ bool tt_bar_wait(uint64_t* bar, uint32_t parity) {
-    if (tt_bar_test(bar, parity)) return true;
-    const unsigned long long t0 = tt_clock_ns();
-    while (!tt_bar_test(bar, parity))
-        if (tt_clock_ns() - t0 > TT_WAIT_NS) return false;
-    return true;
+    unsigned long long t0 = 0;
+    for (uint32_t i = 1;; ++i) {
+        if (tt_bar_test(bar, parity)) return true;
+        if ((i & 255u) == 0) {
+            const unsigned long long t = tt_clock_ns();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > TT_WAIT_NS) return false;
+        }
+    }
 }
 __device__ __forceinline__ void tt_load(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
     asm volatile(

@@ -940,7 +940,8 @@ template <class T>
 __global__ void k_ad_heat_rhs_adj(Grid g, const T* __restrict__ bb, const int8_t* __restrict__ mark,
                                   const float* __restrict__ fixedheat, HeatCoef hc, T* __restrict__ Tcb) {
     MP_GRID_LOOP(idx, g.n) {
-        if (fixedheat && fixedheat[idx] != MP_UNDEF_TEMPERATURE) continue;
+        // walls (alpha 0, outside the solve) and held cells pass nothing back
+        if (mark[idx] == MP_TYPEBOUNDARY || (fixedheat && fixedheat[idx] != MP_UNDEF_TEMPERATURE)) continue;
         Tcb[idx] += bb[idx] * (T)g.h * (T)g.h / (T)hc.al(mark[idx]) / (T)hc.dt;
     }
 }

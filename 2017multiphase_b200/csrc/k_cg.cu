@@ -17,6 +17,7 @@
 // Dot products are FP64 block sums finished by the last block in block order,
 // so they are deterministic. Vectors are FP32 (MP_PREC_MIXED) or FP64.
 #include "ctx.cuh"
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <type_traits>
@@ -88,6 +89,9 @@ struct PressOp {
     Grid g;
     const int8_t* __restrict__ mark;
     bool air = true;
+    // 1/h^2 when h^2 is a power of two (then s * inv_h2 equals s / h^2 bit for
+    // bit and saves the division), else 0
+    float inv_h2 = 0.0f;
     __device__ __forceinline__ bool mask(int idx, int i, int j, int k) const {
         int m = mark[idx];
         return (m == MP_TYPEFLUID || (air && m == MP_TYPEAIR)) && inner(g, i, j, k);
@@ -111,8 +115,20 @@ struct PressOp {
     __device__ __forceinline__ bool fixed(int q) const { return mark[q] == MP_TYPEBOUNDARY; }
     template <class R> __device__ __forceinline__ R start(int, R c) const { return (R)(-6.0f) * c; }
     template <class R> __device__ __forceinline__ R comb(R s, R v) const { return s + v; }
-    template <class R> __device__ __forceinline__ R finish(R s) const { return s / ((R)g.h * (R)g.h); }
+    template <class R> __device__ __forceinline__ R finish(R s) const {
+        if (inv_h2 != 0.0f) return s * (R)inv_h2;
+        return s / ((R)g.h * (R)g.h);
+    }
 };
+// PressOp with inv_h2 set when h^2 (rounded to float, as the stencil forms it)
+// is an exact power of two
+inline PressOp press_op(const Grid& g, const int8_t* mark, bool air = true) {
+    PressOp op{g, mark, air};
+    const float h2 = g.h * g.h;
+    int e = 0;
+    if (h2 > 0.0f && std::frexp(h2, &e) == 0.5f) op.inv_h2 = 1.0f / h2;
+    return op;
+}
 // computeAx_heat (spray_k.cu:4526-4568): rows over non-BOUNDARY cells
 struct HeatOp {
     Grid g;
@@ -977,13 +993,13 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
 // three fifths of cg64). x is cleared first. Used by the adjoint module.
 int k_cg_solve(MpCtx* c, const int8_t* mark, float* x, const float* b, int maxiter, int tolmode, float tol, int* iters,
                double* res) {
-    PressOp op{c->G, mark};
+    PressOp op = press_op(c->G, mark);
     return run_cg<float>(c, op, x, b, c->cg_r, c->cg_p, c->cg_z, maxiter, tolmode, tol, 0, iters, res,
                          MP_KT_CG_STENCIL);
 }
 int k_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, int maxiter, int tolmode, float tol,
                int* iters, double* res) {
-    PressOp op{c->G, mark};
+    PressOp op = press_op(c->G, mark);
     const size_t n = (size_t)c->G.n;
     return run_cg<double>(c, op, x, b, c->cg64 + 2 * n, c->cg64 + 3 * n, c->cg64 + 4 * n, maxiter, tolmode, tol, 0,
                           iters, res, MP_KT_CG_STENCIL);
@@ -1017,7 +1033,7 @@ int k_heat_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, in
 // project_CG_bubble (spray.cu:1590-1611)
 int k_project(MpCtx* c, int* iters, double* res) {
     const Grid& g = c->G;
-    PressOp op{g, c->mark};
+    PressOp op = press_op(g, c->mark);
     int nbk = mp_blocks(g.n, 256);
     long long ftot = (long long)g.nfx + g.nfy + g.nfz;
     long long gtot = std::max(ftot, (long long)g.n);
@@ -1107,7 +1123,7 @@ int k_project_water(MpCtx* c, int* iters, double* res) {
         c->err = "project_water: the single-phase solve is MP_PREC_MIXED, MP_COEF_REF only";
         return MP_ERR_STATE;
     }
-    PressOp op{g, c->mark, false};
+    PressOp op = press_op(g, c->mark, false);
     long long ftot = (long long)g.nfx + g.nfy + g.nfz;
     k_divergence_water<<<mp_blocks(g.n, 256), 256, 0, c->stream>>>(g, c->mark, c->wu[0], c->wu[1], c->wu[2], c->divg);
     c->launches++;
@@ -1315,7 +1331,7 @@ extern "C" int mp_pressure_cg_static(int nx, int ny, int nz, float cellsize, con
     g.NX = nx; g.NY = ny; g.NZ = nz; g.n = n;
     g.nfx = (nx + 1) * ny * nz; g.nfy = nx * (ny + 1) * nz; g.nfz = nx * ny * (nz + 1);
     g.h = cellsize;
-    PressOp op{g, mark};
+    PressOp op = press_op(g, mark);
     Red Rd{reinterpret_cast<double*>(base + NA_PART), reinterpret_cast<unsigned int*>(base + NA_COUNT),
            reinterpret_cast<double*>(base + NA_SCAL), reinterpret_cast<unsigned int*>(base + NA_COUNT) + 1};
     uint8_t* nb8 = base + NA_NB8;
