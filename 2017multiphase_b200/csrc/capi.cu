@@ -163,9 +163,7 @@ static int check_params(const mp_params* p, std::string& err) {
     if (p->precision != MP_PREC_MIXED && p->precision != MP_PREC_FP64) { err = "bad precision"; return MP_ERR_ARG; }
     if (p->cg_tol_mode != MP_TOL_REF_ABS && p->cg_tol_mode != MP_TOL_REL) { err = "bad cg_tol_mode"; return MP_ERR_ARG; }
     if (p->coef_mode != MP_COEF_REF && p->coef_mode != MP_COEF_GFM) { err = "unknown coef_mode"; return MP_ERR_ARG; }
-    if (p->coef_mode == MP_COEF_GFM && p->precision != MP_PREC_MIXED) {
-        err = "MP_COEF_GFM runs with MP_PREC_MIXED vectors"; return MP_ERR_ARG;
-    }
+    if (!(p->cg_refine_tol >= 0.0f && p->cg_refine_tol < 1.0f)) { err = "cg_refine_tol must be in [0, 1)"; return MP_ERR_ARG; }
     if (p->coef_mode == MP_COEF_GFM && !(p->density_ratio > 0)) { err = "density_ratio must be positive"; return MP_ERR_ARG; }
     if (p->mc_max_verts < 1 || p->mc_max_tris < 1) { err = "marching-cubes caps must be positive"; return MP_ERR_ARG; }
     if (p->seed_redraw != 0) {

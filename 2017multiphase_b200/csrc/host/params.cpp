@@ -32,7 +32,7 @@ static const ParamField kParamFields[] = {
     PF_I(cg_max_iter), PF_I(heat_cg_max_iter), PF_I(cg_true_residual_every), PF_I(precision),
     PF_I(coef_mode), PF_F(density_ratio), PF_I(mc_max_verts), PF_I(mc_max_tris), PF_I(seed_redraw),
     PF_I(update_seed_frame_delta), PF_I(b_fixed_heat), PF_F(pos_rand_param), PF_F(vel_rand_param),
-    PF_I(begin_frame), PF_I(b_run_mc_solid),
+    PF_I(begin_frame), PF_I(b_run_mc_solid), PF_F(cg_refine_tol),
 };
 
 extern "C" int mp_params_size(void) { return (int)sizeof(mp_params); }

@@ -29,7 +29,7 @@ namespace {
 constexpr int CG_T = 256;
 
 // device scalar slots
-enum { S_A = 0, S_RR = 1, S_ALPHA = 2, S_BETA = 3, S_EPS = 4, S_ZP = 5 };
+enum { S_A = 0, S_RR = 1, S_ALPHA = 2, S_BETA = 3, S_EPS = 4, S_ZP = 5, S_TRUE = 6 };
 // flag slots (unsigned int): done state and iteration count
 enum { F_DONE = 0, F_ITERS = 1, F_COUNT = 2 };
 enum { DONE_RUN = 0, DONE_CONV = 1, DONE_CAP = 2, DONE_ZP0 = 3, DONE_TIMEOUT = 4 };
@@ -323,6 +323,30 @@ __global__ void __launch_bounds__(CG_T) k_cg_true(Op op, int n, const R* __restr
         else if (it + 1 >= maxiter) Rd.flag[F_DONE] = DONE_CAP;
         else { Rd.scal[S_BETA] = tot / Rd.scal[S_A]; Rd.scal[S_A] = tot; }
     }
+}
+
+// mixed-precision refinement: the true residual in FP64, r = mask ? b - A x :
+// 0 with the row applied in FP64, its FP32 copy (the next correction's
+// right-hand side) and |r|^2 into scal[slot]
+template <class Op>
+__global__ void __launch_bounds__(CG_T) k_cg_resid64(Op op, int n, const double* __restrict__ b,
+                                                     const double* __restrict__ x, double* __restrict__ r,
+                                                     float* __restrict__ r32, Red Rd, int slot) {
+    auto xv = [&](int q) -> double { return __ldg(x + q); };
+    double acc = 0;
+    CG_CELL_LOOP(idx, n, i, j, k) {
+        int id = (int)idx;
+        double v = 0;
+        if (op.mask(id, i, j, k)) v = b[idx] - op.template apply<double>(id, xv);
+        r[idx] = v;
+        r32[idx] = (float)v;
+        acc += v * v;
+    }
+    double tot;
+    if (finish_sum(Rd, acc, &tot)) Rd.scal[slot] = tot;
+}
+__global__ void k_add_f2d(int n, const float* __restrict__ e, double* __restrict__ x) {
+    MP_GRID_LOOP(idx, n) x[idx] += (double)e[idx];
 }
 
 // ---- plane-marching stencil kernels -------------------------------------------
@@ -988,6 +1012,49 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     return hflag[F_DONE] == DONE_CAP ? MP_ERR_NOCONVERGE : MP_OK;
 }
 
+// Mixed-precision iterative refinement of A x = b: x and the true residual
+// r = b - A x live in FP64 (x64, r64) and the residual is recomputed in FP64
+// after every correction; each correction e solves A e = r with FP32 vectors
+// (run_cg, relative tolerance inner_tol) and is added to x in FP64. The stop
+// rule (tolmode, tol) is tested on the FP64 true residual, so the solution's
+// accuracy is not bounded by FP32 storage of x. r32 and e32 are FP32 scratch.
+template <class Op>
+static int run_cg_refined(MpCtx* c, const Op& op, double* x64, const double* b64, double* r64, float* r32,
+                          float* e32, int maxiter, int tolmode, float tol, float inner_tol, int* iters_out,
+                          double* res_out) {
+    const int n = c->G.n;
+    cudaStream_t s = c->stream;
+    Red Rd = red_of(c);
+    MP_CUDA(c, cudaMemsetAsync(x64, 0, sizeof(double) * n, s));
+    auto resid = [&](double* rr) -> int {
+        k_cg_resid64<Op><<<c->red_blocks, CG_T, 0, s>>>(op, n, b64, x64, r64, r32, Rd, S_TRUE);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        MP_CUDA(c, cudaMemcpyAsync(rr, Rd.scal + S_TRUE, sizeof(double), cudaMemcpyDeviceToHost, s));
+        MP_CUDA(c, cudaStreamSynchronize(s));
+        return MP_OK;
+    };
+    double rr0 = 0, rr = 0;
+    MP_TRY(resid(&rr0));
+    rr = rr0;
+    const double eps = tolmode == MP_TOL_REF_ABS ? (double)(tol * (float)n) : (double)tol * (double)tol * rr0;
+    int total = 0;
+    while (!(rr < eps) && total < maxiter && rr0 > 0) {
+        int it = 0; double ri = 0;
+        int rc = run_cg<float>(c, op, e32, r32, c->cg_r, c->cg_p, c->cg_z, maxiter - total, MP_TOL_REL, inner_tol, 0,
+                               &it, &ri, MP_KT_CG_STENCIL);
+        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+        total += it;
+        if (it == 0) break;
+        k_add_f2d<<<mp_blocks(n, 256), 256, 0, s>>>(n, e32, x64);
+        c->launches++;
+        MP_TRY(resid(&rr));
+    }
+    *iters_out = total;
+    *res_out = rr;
+    return (rr < eps || rr0 == 0) ? MP_OK : MP_ERR_NOCONVERGE;
+}
+
 // The pressure matrix of project_CG_bubble for a given mark field, solved on
 // the context's CG scratch (FP32 vectors: cg_r/cg_p/cg_z; FP64: the last
 // three fifths of cg64). x is cleared first. Used by the adjoint module.
@@ -1047,13 +1114,29 @@ int k_project(MpCtx* c, int* iters, double* res) {
         }
         float* bx = c->gfm_beta; float* by = bx + g.nfx; float* bz = by + g.nfy;
         float* x = c->press;
-        if (c->P.precision != MP_PREC_FP64)
+        if (c->P.precision != MP_PREC_FP64 && !(c->P.cg_refine_tol > 0))
             k_divergence<float><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
                                                             c->au[0], c->au[1], c->au[2], c->divg, nullptr);
         k_gfm_beta<<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, c->mark, c->lsmerge, 1.0f / c->P.density_ratio,
                                                                 bx, by, bz);
         GfmOp gop{g, c->mark, bx, by, bz, c->gfm_s};
-        if (c->P.precision == MP_PREC_FP64) {
+        if (c->P.precision == MP_PREC_MIXED && c->P.cg_refine_tol > 0) {
+            // mixed-precision refinement of the scaled system
+            double* x64 = c->cg64; double* b64 = x64 + g.n; double* r64 = b64 + g.n;
+            k_divergence<double><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
+                                                             c->au[0], c->au[1], c->au[2], b64, c->divg);
+            k_gfm_scale<double><<<nbk, 256, 0, c->stream>>>(g, c->mark, bx, by, bz, b64, c->gfm_s, b64);
+            c->launches += 3;
+            MP_CHECK_LAUNCH(c);
+            rc = run_cg_refined(c, gop, x64, b64, r64, c->cell_tmp, x, c->P.cg_max_iter, c->P.cg_tol_mode,
+                                c->P.cg_tol, c->P.cg_refine_tol, &it, &rr);
+            if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+            k_gfm_unscale<double><<<nbk, 256, 0, c->stream>>>(g.n, c->gfm_s, x64);
+            k_d2f<<<nbk, 256, 0, c->stream>>>(g.n, x64, x);
+            k_subgrad_gfm<double><<<mp_blocks(ftot, 256), 256, 0, c->stream>>>(g, x64, bx, by, bz, c->wu[0], c->wu[1],
+                                                                               c->wu[2], c->au[0], c->au[1], c->au[2]);
+            c->launches += 3;
+        } else if (c->P.precision == MP_PREC_FP64) {
             // the all-FP64 form: right-hand side, vectors and scalars in FP64
             double* xd = c->cg64; double* bd = xd + g.n; double* rd = bd + g.n;
             double* p0 = rd + g.n; double* p1 = p0 + g.n;
@@ -1093,6 +1176,19 @@ int k_project(MpCtx* c, int* iters, double* res) {
                             c->P.cg_true_residual_every, &it, &rr, MP_KT_CG_STENCIL);
         if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
         k_subgrad<double><<<mp_blocks(gtot, 256), 256, 0, c->stream>>>(g, x, c->wu[0], c->wu[1], c->wu[2], c->au[0],
+                                                                       c->au[1], c->au[2], c->press);
+    } else if (c->P.cg_refine_tol > 0) {
+        // mixed-precision refinement: FP64 right-hand side, solution and true
+        // residual; FP32-vector corrections
+        double* x64 = c->cg64; double* b64 = x64 + g.n; double* r64 = b64 + g.n;
+        k_divergence<double><<<nbk, 256, 0, c->stream>>>(g, c->mark, c->lsmerge, c->wu[0], c->wu[1], c->wu[2],
+                                                         c->au[0], c->au[1], c->au[2], b64, c->divg);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        rc = run_cg_refined(c, op, x64, b64, r64, c->cell_tmp, c->press, c->P.cg_max_iter, c->P.cg_tol_mode,
+                            c->P.cg_tol, c->P.cg_refine_tol, &it, &rr);
+        if (rc != MP_OK && rc != MP_ERR_NOCONVERGE) return rc;
+        k_subgrad<double><<<mp_blocks(gtot, 256), 256, 0, c->stream>>>(g, x64, c->wu[0], c->wu[1], c->wu[2], c->au[0],
                                                                        c->au[1], c->au[2], c->press);
     } else {
         float* x = c->press;

@@ -77,7 +77,7 @@ extern "C" {
 #define MP_PREC_MIXED    0   /* FP32 vectors, FP64 dots/alpha/beta            */
 #define MP_PREC_FP64     1   /* divergence, pressure CG, gradient and the heat CG in FP64 */
 #define MP_COEF_REF      0   /* constant-coefficient Laplacian (reference)    */
-#define MP_COEF_GFM      1   /* variable density, ghost-fluid face weights (extension; MP_PREC_MIXED only) */
+#define MP_COEF_GFM      1   /* variable density, ghost-fluid face weights (extension)                 */
 
 #define MP_PARAMS_VERSION 4
 
@@ -151,7 +151,14 @@ typedef struct mp_params {
     int32_t begin_frame;             /* m_beginFrame: first gas-pouring / solid-release frame   */
     int32_t b_run_mc_solid;          /* bRunMCSolid: 0 = extract the solid surface once, then
                                         move it with the rigid solid motion                     */
-    int32_t reserved[3];
+    /* > 0: the MP_PREC_MIXED pressure solve runs as mixed-precision iterative
+     * refinement: x and the true residual r = b - A x are kept and recomputed
+     * in FP64 (right-hand side from the FP64 divergence), each correction is
+     * an FP32-vector CG on r to this relative tolerance, and the stop rule
+     * (cg_tol_mode, cg_tol) is tested on the FP64 true residual. 0: one CG
+     * pass (the reference's recurrence). */
+    float   cg_refine_tol;
+    int32_t reserved[2];
 } mp_params;
 
 #define MP_UNDEF_TEMPERATURE (-10000.0f)   /* utility.h:24 */

@@ -93,3 +93,23 @@ def test_gfm_fp64_form_matches_fp64_oracle_at_1e5(mp, oracle_mod, config):
         e = rel_err(sim.get_field(f), orc.get_field(f))
         assert e <= 1e-5, f"{f}: rel err {e:.3e}"
     sim.close()
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_gfm_mixed_refined_matches_fp64_oracle_at_1e5(mp, oracle_mod, config):
+    """The mixed form at 1000:1 with iterative refinement (FP32-vector CG
+    corrections to 1e-3, solution and true residual in FP64, stop at a 1e-10
+    relative true residual): pressure and every face velocity within 1e-5
+    relative of the oracle's FP64 solve, which plain FP32-vector CG misses
+    (see test_gfm_projection_matches_fp64_oracle)."""
+    sim, orc = make_pair(mp, oracle_mod, config, 32, 9300 + config, coef_mode=1, density_ratio=1000.0,
+                         cg_max_iter=20000, cg_tol=1e-10, cg_refine_tol=1e-3)
+    _before_projection(sim)
+    transplant(sim, orc)
+    it, res, rc = sim.project_CG_bubble()
+    assert rc == 0 and it > 0
+    orc.project_CG_bubble()
+    for f in ["press", "waterux", "wateruy", "wateruz", "airux", "airuy", "airuz"]:
+        e = rel_err(sim.get_field(f), orc.get_field(f))
+        assert e <= 1e-5, f"{f}: rel err {e:.3e}"
+    sim.close()

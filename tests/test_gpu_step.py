@@ -97,3 +97,62 @@ def test_cg_tma_matches_float4_passes(mp, oracle_mod, monkeypatch, config, shape
     assert abs(out["v4"][0] - out["tma"][0]) <= 1, (out["v4"][0], out["tma"][0])
     assert rel_err(out["tma"][1], out["v4"][1]) <= 1e-5
     assert rel_err(out["tma"][2], out["v4"][2]) <= 1e-5
+
+
+@pytest.mark.parametrize("config,n", [(2, 64), (3, 64)])
+def test_mixed_form_fields_against_fp64_form(mp, oracle_mod, config, n):
+    """One whole step from the same state in the mixed FP32/FP64 form and in
+    the all-FP64 form (projection and heat solve in FP64): every output field
+    -- pressure, velocity faces, temperature, level set -- within 1e-5
+    relative (L2) of the FP64 form's."""
+    from parity_util import rel_l2
+    sim = mp.Sim.from_config(config, n, 9300 + config)
+    blob = sim.checkpoint()
+    p0 = sim.get_params()
+    out = {}
+    for name, prec in (("fp64", mp.PREC_FP64), ("mixed", mp.PREC_MIXED)):
+        sim.set_params(p0)
+        sim.restore(blob)
+        p = sim.get_params(); p.precision = prec; sim.set_params(p)
+        sim.bubblesim()
+        out[name] = {f: sim.get_field(f) for f in ["press", "waterux", "wateruy", "wateruz", "airux", "airuy",
+                                                   "airuz", "tp", "lsmerge"]}
+    for f in out["fp64"]:
+        e = rel_l2(out["mixed"][f], out["fp64"][f])
+        assert e <= 1e-5, f"config {config} {f}: mixed vs FP64 form rel L2 {e:.3e}"
+    sim.close()
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_refined_mixed_pressure_against_fp64(mp, oracle_mod, config):
+    """Mixed-precision iterative refinement (cg_refine_tol): FP32-vector CG
+    corrections with the solution and the true residual in FP64 reach the
+    FP64 solve's pressure to 1e-6 relative at the configuration's 1e-6 stop,
+    and the stop test holds on the FP64 true residual."""
+    sim, _ = make_pair(mp, oracle_mod, config, 64, 199 + config)
+    for st in ["hashAndSortParticles", "addexternalforce"]:
+        getattr(sim, st)()
+    sim.computeLevelset(0.0); sim.sweepLSAndMardGrid()
+    sim.mapvelp2g_bubble()
+    for ph in (1, 0):
+        sim.sweepPhi(ph); sim.sweepU(ph)
+    sim.setWaterBoundaryU(1); sim.setWaterBoundaryU(0)
+    faces = {f: sim.get_field(f) for f in FACE_FIELDS}
+    p0 = sim.get_params()
+    p = sim.get_params()
+    p.precision = mp.PREC_FP64; p.cg_tol = 1e-12; p.cg_max_iter = 8000
+    sim.set_params(p)
+    _, _, rc = sim.project_CG_bubble()
+    assert rc == 0
+    ref = sim.get_field("press").astype(np.float64)
+    for f, a in faces.items():
+        sim.set_field(f, a)
+    p = p0
+    p.cg_refine_tol = 1e-3
+    sim.set_params(p)
+    it, res, rc = sim.project_CG_bubble()
+    assert rc == 0
+    x = sim.get_field("press").astype(np.float64)
+    err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+    assert err <= 1e-6, f"refined mixed vs fp64 relative pressure error {err:.3e} ({it} iterations)"
+    sim.close()
