@@ -108,8 +108,10 @@ static int create_impl(MpCtx* c, const mp_params* p) {
     MP_TRY(dalloc_t(c, &c->cell_cnt, n8 + 1)); MP_TRY(dalloc_t(c, &c->cell_off, n8 + 1));
     MP_CUDA(c, cudaMemset(c->cell_cnt, 0, sizeof(uint32_t) * (n8 + 1)));
     MP_CUDA(c, cudaMemset(c->cell_off, 0, sizeof(uint32_t) * (n8 + 1)));
-    MP_TRY(dalloc_t(c, &c->tmask, n8));
-    MP_CUDA(c, cudaMemset(c->tmask, 0, n8));
+    // type masks are OR-ed in by 32-bit words: whole words
+    const size_t n8w = (n8 + 3) / 4 * 4;
+    MP_TRY(dalloc_t(c, &c->tmask, n8w));
+    MP_CUDA(c, cudaMemset(c->tmask, 0, n8w));
     MP_TRY(dalloc_t(c, &c->u32_scratch, 16));
     // marching cubes tables and buffers
     MP_TRY(dalloc_t(c, &c->mc_numverts, 256)); MP_TRY(dalloc_t(c, &c->mc_tri, 256 * 16));

@@ -156,21 +156,28 @@ __device__ __forceinline__ uint32_t hash_key(float4 q, float gx0, float gy0, flo
     int k = (r.z >= 0 && r.z < d) ? (int)r.z : 0;
     return (uint32_t)(i * hh * d + j * d + k);
 }
-// keys, per-cell counts, and a flag raised when the keys are not already in
-// order (then the stable sort is the identity and the gather can be skipped)
+// keys, per-cell counts, each cell's type mask (which particle types it holds;
+// the cleared mask words take one OR per run of equal keys), and a flag raised
+// when the keys are not already in order (then the stable sort is the
+// identity and the gather can be skipped)
 __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, float gy0, float gz0, float dx,
                              int w, int hh, int d, uint32_t* __restrict__ keys, uint32_t* __restrict__ cnt,
-                             uint32_t* __restrict__ unsorted) {
+                             uint32_t* __restrict__ tmask_words, uint32_t* __restrict__ unsorted) {
     __shared__ uint32_t blk_unsorted;
     if (threadIdx.x == 0) blk_unsorted = 0;
     __syncthreads();
     MP_GRID_LOOP(p, np) {
-        uint32_t key = hash_key(pos[p], gx0, gy0, gz0, dx, w, hh, d);
+        const float4 q = pos[p];
+        uint32_t key = hash_key(q, gx0, gy0, gz0, dx, w, hh, d);
         if (p > 0 && hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d) > key) blk_unsorted = 1u;
         keys[p] = key;
         // one atomic per run of equal keys in the warp (particles arrive nearly sorted)
         unsigned peers = __match_any_sync(__activemask(), key);
-        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(cnt + key, (uint32_t)__popc(peers));
+        const uint32_t bits = __reduce_or_sync(peers, 1u << (pflag(q) & 7));
+        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) {
+            atomicAdd(cnt + key, (uint32_t)__popc(peers));
+            atomicOr(tmask_words + (key >> 2), bits << (8 * (key & 3)));
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0 && blk_unsorted) *unsorted = 1u;   // one store per block
@@ -191,24 +198,11 @@ __global__ void k_scatter(const uint32_t* __restrict__ keys, int np, const uint3
         perm[off[key] + r] = (uint32_t)p;
     }
 }
-// sort each cell's indices ascending (stability of thrust::sort_by_key) and
-// record which particle types the cell holds
-__global__ void k_segsort(const uint32_t* __restrict__ off, int ncell, uint32_t* __restrict__ perm,
-                          const float4* __restrict__ pos, uint8_t* __restrict__ tmask) {
+// sort each cell's indices ascending (stability of thrust::sort_by_key)
+__global__ void k_segsort(const uint32_t* __restrict__ off, int ncell, uint32_t* __restrict__ perm) {
     MP_GRID_LOOP(cc, ncell) {
         const uint32_t s0 = off[cc];
-        uint32_t m = 0;
-        sort_distinct_run(perm, s0, off[cc + 1] - s0, [&](uint32_t v) { m |= 1u << (pflag(__ldg(pos + v)) & 7); });
-        tmask[cc] = (uint8_t)m;
-    }
-}
-// type mask of each cell when the particles are already in cell order
-__global__ void k_tmask_sorted(const uint32_t* __restrict__ off, int ncell, const float4* __restrict__ pos,
-                               uint8_t* __restrict__ tmask) {
-    MP_GRID_LOOP(cc, ncell) {
-        uint32_t m = 0;
-        for (uint32_t s = off[cc]; s < off[cc + 1]; s++) m |= 1u << (pflag(__ldg(pos + s)) & 7);
-        tmask[cc] = (uint8_t)m;
+        sort_distinct_run(perm, s0, off[cc + 1] - s0, [&](uint32_t) {});
     }
 }
 __global__ void k_reorder(const uint32_t* __restrict__ perm, int np,
@@ -228,9 +222,11 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     int ncell = w * hh * d;
     uint32_t* unsorted = c->u32_scratch + 1;
     MP_CUDA(c, cudaMemsetAsync(unsorted, 0, sizeof(uint32_t), c->stream));
+    MP_CUDA(c, cudaMemsetAsync(c->tmask, 0, ((size_t)ncell + 3) / 4 * 4, c->stream));
     if (np > 0) {
         k_hash_count<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->pos, np, c->G.gx0, c->G.gy0, c->G.gz0, dx, w, hh, d,
-                                                                c->keys, c->cell_cnt, unsorted);
+                                                                c->keys, c->cell_cnt,
+                                                                reinterpret_cast<uint32_t*>(c->tmask), unsorted);
         c->launches++;
         MP_CHECK_LAUNCH(c);
     }
@@ -243,9 +239,6 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
         // already in cell order: the stable sort is the identity permutation;
         // the counts still have to run back to zero for the next sort
         MP_CUDA(c, cudaMemsetAsync(c->cell_cnt, 0, sizeof(uint32_t) * ncell, c->stream));
-        k_tmask_sorted<<<mp_blocks(ncell, 256), 256, 0, c->stream>>>(c->cell_off, ncell, c->pos, c->tmask);
-        c->launches++;
-        MP_CHECK_LAUNCH(c);
         return MP_OK;
     }
     if (np > 0) {
@@ -253,7 +246,7 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
         c->launches++;
         MP_CHECK_LAUNCH(c);
     }
-    k_segsort<<<mp_blocks(ncell, 256), 256, 0, c->stream>>>(c->cell_off, ncell, c->perm, c->pos, c->tmask);
+    k_segsort<<<mp_blocks(ncell, 256), 256, 0, c->stream>>>(c->cell_off, ncell, c->perm);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     if (np > 0) {
