@@ -36,7 +36,7 @@ static void free_all(MpCtx* c) {
                     c->gx, c->gy, c->gz, c->gxa, c->gya, c->gza, c->sf, c->Tp, c->Tp_save, c->Tp_old, c->fixedheat,
                     c->cell_tmp, c->mark, c->mark_tmp, c->cg_r, c->cg_p, c->cg_z, c->cg64, c->red, c->scal, c->red_count,
                     c->pos, c->vel, c->heat, c->pos2, c->vel2, c->heat2, c->pdens, c->pprs, c->pscr, c->pscr2,
-                    c->flag_snap, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->scan_tmp, c->u32_scratch,
+                    c->flag_snap, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->air_brick, c->scan_tmp, c->u32_scratch,
                     c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_dens2, c->gfm_beta, c->gfm_s, c->mc_cube, c->mc_vflag, c->mc_vscan,
                     c->mc_compact, c->mc_vverts, c->mc_vvscan, c->mc_emark, c->mc_escan, c->mc_vstart, c->mc_inc,
                     c->mc_fill, c->mc_tmpv, c->pour_pos, c->pour_vel};
@@ -92,7 +92,7 @@ static int create_impl(MpCtx* c, const mp_params* p) {
     MP_TRY(dalloc_t(c, &c->cg64, 5 * n));
     c->red_blocks = mp_blocks((long long)n, 256);
     if (const char* e = getenv("MP_CG_KERNEL")) c->cg_use_tma = strcmp(e, "v4") != 0;
-    if (const char* e = getenv("MP_CG_TMA_CHUNK")) c->cg_tma_chunk = atoi(e);
+    if (const char* e = getenv("MP_CG_TMA_CTAS")) c->cg_tma_ctas = atoi(e);
     MP_TRY(dalloc_t(c, &c->red, (size_t)148 * 32 * 6));
     MP_TRY(dalloc_t(c, &c->scal, 16));
     MP_TRY(dalloc_t(c, &c->red_count, 16));
@@ -108,6 +108,12 @@ static int create_impl(MpCtx* c, const mp_params* p) {
     MP_TRY(dalloc_t(c, &c->cell_cnt, n8 + 1)); MP_TRY(dalloc_t(c, &c->cell_off, n8 + 1));
     MP_CUDA(c, cudaMemset(c->cell_cnt, 0, sizeof(uint32_t) * (n8 + 1)));
     MP_CUDA(c, cudaMemset(c->cell_off, 0, sizeof(uint32_t) * (n8 + 1)));
+    {
+        const size_t bricks = (size_t)((p->nx + 3) / 4) * ((p->ny + 3) / 4) * ((p->nz + 3) / 4);
+        c->air_brick_words = (bricks + 31) / 32;
+        MP_TRY(dalloc_t(c, &c->air_brick, c->air_brick_words));
+        MP_CUDA(c, cudaMemset(c->air_brick, 0, sizeof(uint32_t) * c->air_brick_words));
+    }
     // type masks are OR-ed in by 32-bit words: whole words
     const size_t n8w = (n8 + 3) / 4 * 4;
     MP_TRY(dalloc_t(c, &c->tmask, n8w));

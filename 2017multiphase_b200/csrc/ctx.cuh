@@ -56,9 +56,9 @@ struct MpCtx {
     int red_blocks = 0;
     // CG kernels (tuning knobs read from the environment at mp_create):
     // MP_CG_KERNEL=v4 keeps the float4-group passes where the TMA plane
-    // marching applies; MP_CG_TMA_CHUNK sets its planes per CTA (0: derived)
+    // marching applies; MP_CG_TMA_CTAS sets its CTA count (0: one wave)
     int cg_use_tma = 1;
-    int cg_tma_chunk = 0;
+    int cg_tma_ctas = 0;
     float *gfm_beta = 0;         // ghost-fluid face weights (x, y, z faces), allocated on first use
     float *gfm_s = 0;            // its Jacobi scaling per cell
     // particles
@@ -72,6 +72,8 @@ struct MpCtx {
     uint32_t *keys = 0, *perm = 0;
     uint32_t *cell_cnt = 0, *cell_off = 0;   // sized for the 2x marching-cubes grid
     uint8_t *tmask = 0;
+    uint32_t *air_brick = 0;     // bit per 4x4x4-cell brick holding an AIR/AIRSOLO particle (last sort)
+    size_t air_brick_words = 0;
     uint32_t *scan_tmp = 0;
     size_t scan_tmp_elems = 0;
     uint32_t *u32_scratch = 0;   // small device counters

@@ -32,7 +32,7 @@ __constant__ signed char kWin[125][3] = {
 
 __global__ void __launch_bounds__(256) k_genlevelset(Grid g, Cells cl, const float4* __restrict__ pos,
                                                      float* __restrict__ lsf, float* __restrict__ lsa,
-                                                     int8_t* __restrict__ mark) {
+                                                     int8_t* __restrict__ mark, const uint32_t* __restrict__ air_brick) {
     const uint32_t AIRB = (1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO);
     const uint32_t FLB = (1u << MP_TYPEFLUID) | (1u << MP_TYPESOLID);
     MP_GRID_LOOP(idx, g.n) {
@@ -43,6 +43,23 @@ __global__ void __launch_bounds__(256) k_genlevelset(Grid g, Cells cl, const flo
         float3 gp = (mk3((float)i, (float)j, (float)k) + mk3(0.5f, 0.5f, 0.5f)) * h;
         const float cap2 = 6.25f * h * h * 1.001f;       // beyond 2.5h nothing changes
         float ma2 = __int_as_float(0x7f800000), mf2 = __int_as_float(0x7f800000);
+        // no brick that the window (i-2..i+2, ...) touches holds an air
+        // particle: the air distance stays at its cap, and the search for it
+        // would visit every cell only to find no air
+        bool air_near = false;
+        {
+            const int bw = (g.NZ + 3) / 4, bh = (g.NY + 3) / 4;
+            const int bi0 = max(i - 2, 0) >> 2, bi1 = min(i + 2, g.NX - 1) >> 2;
+            const int bj0 = max(j - 2, 0) >> 2, bj1 = min(j + 2, g.NY - 1) >> 2;
+            const int bk0 = max(k - 2, 0) >> 2, bk1 = min(k + 2, g.NZ - 1) >> 2;
+            for (int bi = bi0; bi <= bi1; bi++)
+                for (int bj = bj0; bj <= bj1; bj++)
+                    for (int bk = bk0; bk <= bk1; bk++) {
+                        const int br = (bi * bh + bj) * bw + bk;
+                        air_near |= (__ldg(air_brick + (br >> 5)) >> (br & 31)) & 1u;
+                    }
+        }
+        if (!air_near) ma2 = 0.0f;   // searched no further; the value is replaced below
         for (int w = 0; w < 125; ++w) {
             int di = kWin[w][0], dj = kWin[w][1], dk = kWin[w][2];
             int a = i + di, b = j + dj, cc = k + dk;
@@ -51,7 +68,9 @@ __global__ void __launch_bounds__(256) k_genlevelset(Grid g, Cells cl, const flo
             float bz = dk == 0 ? 0.f : ((float)abs(dk) - 0.5f);
             float lb2 = (bx * bx + by * by + bz * bz) * h * h * 0.9999f;
             bool wantA = lb2 < fminf(ma2, cap2), wantF = lb2 < fminf(mf2, cap2);
-            if (!wantA && !wantF) continue;
+            // the window is ordered by this bound and the minima only fall:
+            // no later cell is wanted either
+            if (!wantA && !wantF) break;
             int c = cid(g, a, b, cc);
             uint32_t tm = __ldg(cl.tmask + c);
             if (!((wantA && (tm & AIRB)) || (wantF && (tm & FLB)))) continue;
@@ -65,6 +84,7 @@ __global__ void __launch_bounds__(256) k_genlevelset(Grid g, Cells cl, const flo
                 else if (f == MP_TYPEFLUID || f == MP_TYPESOLID) mf2 = fminf(mf2, d2);
             }
         }
+        if (!air_near) ma2 = __int_as_float(0x7f800000);
         float mair = 2.5f * h, mfl = 2.5f * h;
         float da = sqrtf(ma2), df = sqrtf(mf2);
         mair = (da < mair) ? da : mair;
@@ -384,7 +404,8 @@ int k_sweep_pass_swap(MpCtx* c, float** phi, int typeflag) {
 
 int k_levelset(MpCtx* c) {
     KtScope kt(c, MP_KT_LEVELSET);
-    k_genlevelset<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, cells_of(c), c->pos, c->lsfluid, c->lsair, c->mark);
+    k_genlevelset<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, cells_of(c), c->pos, c->lsfluid, c->lsair, c->mark,
+                                                                 c->air_brick);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     return MP_OK;

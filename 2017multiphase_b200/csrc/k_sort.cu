@@ -160,9 +160,12 @@ __device__ __forceinline__ uint32_t hash_key(float4 q, float gx0, float gy0, flo
 // the cleared mask words take one OR per run of equal keys), and a flag raised
 // when the keys are not already in order (then the stable sort is the
 // identity and the gather can be skipped)
+// With `air_words` (the simulation grid's sort), the bit of each 4x4x4-cell
+// brick that holds an AIR or AIRSOLO particle is set as well.
 __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, float gy0, float gz0, float dx,
                              int w, int hh, int d, uint32_t* __restrict__ keys, uint32_t* __restrict__ cnt,
-                             uint32_t* __restrict__ tmask_words, uint32_t* __restrict__ unsorted) {
+                             uint32_t* __restrict__ tmask_words, uint32_t* __restrict__ air_words,
+                             uint32_t* __restrict__ unsorted) {
     __shared__ uint32_t blk_unsorted;
     if (threadIdx.x == 0) blk_unsorted = 0;
     __syncthreads();
@@ -177,6 +180,13 @@ __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, 
         if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) {
             atomicAdd(cnt + key, (uint32_t)__popc(peers));
             atomicOr(tmask_words + (key >> 2), bits << (8 * (key & 3)));
+            if (air_words && (bits & ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO)))) {
+                const uint32_t kk = key % (uint32_t)d, jj = (key / (uint32_t)d) % (uint32_t)hh,
+                               ii = key / ((uint32_t)d * (uint32_t)hh);
+                const uint32_t bw = ((uint32_t)d + 3) / 4, bh = ((uint32_t)hh + 3) / 4;
+                const uint32_t br = ((ii >> 2) * bh + (jj >> 2)) * bw + (kk >> 2);
+                atomicOr(air_words + (br >> 5), 1u << (br & 31));
+            }
         }
     }
     __syncthreads();
@@ -223,10 +233,13 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     uint32_t* unsorted = c->u32_scratch + 1;
     MP_CUDA(c, cudaMemsetAsync(unsorted, 0, sizeof(uint32_t), c->stream));
     MP_CUDA(c, cudaMemsetAsync(c->tmask, 0, ((size_t)ncell + 3) / 4 * 4, c->stream));
+    const bool sim_grid = w == c->G.NX && hh == c->G.NY && d == c->G.NZ;
+    if (sim_grid) MP_CUDA(c, cudaMemsetAsync(c->air_brick, 0, sizeof(uint32_t) * c->air_brick_words, c->stream));
     if (np > 0) {
         k_hash_count<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->pos, np, c->G.gx0, c->G.gy0, c->G.gz0, dx, w, hh, d,
                                                                 c->keys, c->cell_cnt,
-                                                                reinterpret_cast<uint32_t*>(c->tmask), unsorted);
+                                                                reinterpret_cast<uint32_t*>(c->tmask),
+                                                                sim_grid ? c->air_brick : nullptr, unsorted);
         c->launches++;
         MP_CHECK_LAUNCH(c);
     }
