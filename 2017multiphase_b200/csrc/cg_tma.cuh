@@ -152,6 +152,20 @@ __device__ __forceinline__ bool tt_finish(const Red& R, double mine, double* tot
     return tid == 0;
 }
 
+// launch with programmatic stream serialization (the kernel waits with
+// griddepcontrol.wait before it reads the previous launch's results)
+template <typename... KArgs, typename... Args>
+inline cudaError_t tt_launch(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t s,
+                             Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid); cfg.blockDim = dim3(block); cfg.dynamicSmemBytes = smem; cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr; cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 struct TtMaps {
     CUtensorMap a;     // MODE 0: r (halo box)       MODE 1: p (halo box)
     CUtensorMap b;     // MODE 0: p_old (halo box)   MODE 1: x (tile box)
@@ -169,6 +183,10 @@ template <class Op, int MODE>
 __global__ void __launch_bounds__(TT_THREADS, 3)
     k_cg_tma(Op op, const __grid_constant__ TtMaps maps, float* __restrict__ pout, float* __restrict__ x,
              float* __restrict__ r, Red Rd, int tk, int first, int it, int maxiter, int skip_dot) {
+    // launched with programmatic stream serialization: the previous launch on
+    // the stream (the other pass) may still be finishing; its results (the
+    // vectors, the scalars, the stop flag) are visible after this wait
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (Rd.flag[F_DONE] != DONE_RUN) return;
     extern __shared__ unsigned char tt_raw[];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tt_raw) + 127) & ~uintptr_t(127));
@@ -328,6 +346,9 @@ __global__ void __launch_bounds__(TT_THREADS, 3)
         // every thread is done with the window before the next segment writes it
         __syncthreads();
     }
+    // the next pass may be launched now; it waits for this grid's completion
+    // before it reads anything this grid writes
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (tt_fail) {
         // a TMA wait ran out: wait (bounded) for the loads still in flight
         // into this CTA's ring, report the timeout and leave without joining

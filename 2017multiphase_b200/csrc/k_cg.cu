@@ -960,13 +960,15 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
                     const int d = (pa == p0) ? 0 : 1;   // p_old
                     {
                         KtScope kt(c, kt_stencil);
-                        k_cg_tma<Op, 0><<<tgrid, TT_THREADS, tt_smem_bytes<0>(), s>>>(
-                            op, tmaps[d], pb, nullptr, nullptr, Rd, ttk, it == 0 ? 1 : 0, it, maxiter, 0);
+                        MP_CUDA(c, tt_launch(k_cg_tma<Op, 0>, tgrid, TT_THREADS, tt_smem_bytes<0>(), s, op, tmaps[d],
+                                             pb, (float*)nullptr, (float*)nullptr, Rd, ttk, it == 0 ? 1 : 0, it,
+                                             maxiter, 0));
                     }
                     {
                         KtScope kt(c, MP_KT_CG_UPDATE);
-                        k_cg_tma<Op, 1><<<tgrid, TT_THREADS, tt_smem_bytes<1>(), s>>>(
-                            op, tmaps[2 + d], nullptr, x, r, Rd, ttk, 0, it, maxiter, tr ? 1 : 0);
+                        MP_CUDA(c, tt_launch(k_cg_tma<Op, 1>, tgrid, TT_THREADS, tt_smem_bytes<1>(), s, op,
+                                             tmaps[2 + d], (float*)nullptr, x, r, Rd, ttk, 0, it, maxiter,
+                                             tr ? 1 : 0));
                     }
                 } else if (v4) {
                     {
