@@ -46,7 +46,7 @@ SCENE_ALL = 15
 MC_SOLID, MC_FLUID, MC_GAS = 0, 1, 2
 PREC_MIXED, PREC_FP64 = 0, 1
 TOL_REF_ABS, TOL_REL = 0, 1
-KT_CG_STENCIL, KT_CG_UPDATE, KT_P2G, KT_G2P, KT_SORT, KT_LEVELSET, KT_MC_DENS = range(7)
+KT_CG_STENCIL, KT_CG_UPDATE, KT_P2G, KT_G2P, KT_SORT, KT_LEVELSET, KT_MC_DENS, KT_CORRECT = range(8)
 
 # field ids in the order of enum mp_field (mp.h)
 FIELDS = [

@@ -856,6 +856,7 @@ int k_correct_pos(MpCtx* c) {
     int np = c->np();
     if (!np) return MP_OK;
     const mp_params& P = c->P;
+    KtScope kt(c, MP_KT_CORRECT);
     k_correct_pos<<<PB(np)>>>(c->G, cells_of(c), np, c->pos, c->vel, c->pos2, P.correction_radius * c->G.h,
                               P.correction_spring, P.samplespace, P.dt);
     c->launches++;

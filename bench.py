@@ -32,7 +32,8 @@ CG_UPD_BYTES_PER_CELL = 21
 
 def names_kt(mp):
     return {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g",
-            mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
+            mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density",
+            mp.KT_CORRECT: "k_correct_pos"}
 
 
 # DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum),
@@ -234,8 +235,7 @@ def profile_case(args):
     else:
         sim = mp.Sim.from_config(args.config, n, args.seed)
         sim.bubblesim()
-        classes = {mp.KT_CG_STENCIL: "k_cg_dir", mp.KT_CG_UPDATE: "k_cg_upd", mp.KT_P2G: "k_p2g",
-                   mp.KT_G2P: "k_g2p", mp.KT_SORT: "sort", mp.KT_LEVELSET: "k_genlevelset", mp.KT_MC_DENS: "k_mc_density"}
+        classes = names_kt(mp)
         for k in classes:
             sim.kernel_timing(k, True)
         torch.cuda.synchronize()
@@ -422,7 +422,8 @@ def main():
         sim.bubblesim()
     torch.cuda.synchronize()
 
-    classes = [mp.KT_CG_STENCIL, mp.KT_CG_UPDATE, mp.KT_P2G, mp.KT_G2P, mp.KT_SORT, mp.KT_LEVELSET, mp.KT_MC_DENS]
+    classes = [mp.KT_CG_STENCIL, mp.KT_CG_UPDATE, mp.KT_P2G, mp.KT_G2P, mp.KT_SORT, mp.KT_LEVELSET, mp.KT_MC_DENS,
+               mp.KT_CORRECT]
     # the timed region runs with no per-kernel timing events (they would sit
     # between the launches); the per-class breakdown is a separate pass below
     sim.kernel_timing_reset()
@@ -525,7 +526,10 @@ def main():
                           wc["sort_full"] + wc["sort_fast"]),
              mp.KT_LEVELSET: ("k_genlevelset", (13 * npart + 9 * n) * kt[mp.KT_LEVELSET][1], kt[mp.KT_LEVELSET][1]),
              mp.KT_MC_DENS: ("k_mc_density (fused fluid + gas fields at 2x)", (13 * npart + 64 * n) * kt[mp.KT_MC_DENS][1],
-                             kt[mp.KT_MC_DENS][1])}
+                             kt[mp.KT_MC_DENS][1]),
+             # read each position record and neighbour mass, write the corrected record; cell ranges
+             mp.KT_CORRECT: ("k_correct_pos (particle spacing spring)", (36 * npart + 4 * n) * kt[mp.KT_CORRECT][1],
+                             kt[mp.KT_CORRECT][1])}
     dom = max(model, key=lambda k: kt[k][0])
     ms_k = kt[dom][0]
     units = max(model[dom][2], 1)

@@ -218,7 +218,8 @@ typedef struct mp_state {
 #define MP_KT_SORT         4   /* hash + counting sort + reorder            */
 #define MP_KT_LEVELSET     5   /* genlevelset                               */
 #define MP_KT_MC_DENS      6   /* marching-cubes density field              */
-#define MP_KT_COUNT        7
+#define MP_KT_CORRECT      7   /* particle spacing correction (correctpos)  */
+#define MP_KT_COUNT        8
 
 /* ---- parameters ------------------------------------------------------- */
 
