@@ -92,7 +92,7 @@ static int create_impl(MpCtx* c, const mp_params* p) {
     MP_TRY(dalloc_t(c, &c->cg64, 5 * n));
     c->red_blocks = mp_blocks((long long)n, 256);
     if (const char* e = getenv("MP_CG_KERNEL")) c->cg_use_tma = strcmp(e, "v4") != 0;
-    if (const char* e = getenv("MP_CG_TMA_CTAS")) c->cg_tma_ctas = atoi(e);
+    if (const char* e = getenv("MP_CG_TMA_CHUNK")) c->cg_tma_chunk = atoi(e);
     MP_TRY(dalloc_t(c, &c->red, (size_t)148 * 32 * 6));
     MP_TRY(dalloc_t(c, &c->scal, 16));
     MP_TRY(dalloc_t(c, &c->red_count, 16));

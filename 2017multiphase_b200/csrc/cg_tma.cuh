@@ -96,22 +96,6 @@ __device__ __forceinline__ void tt_load(void* dst, const CUtensorMap* map, uint6
         : "memory");
 }
 
-// (double)f, formed from the float's bits with integer operations: the same
-// value as the conversion instruction, which runs on the SM's narrow
-// conversion pipe and bounds these passes when every cell's FP64 product
-// takes one or two of it. Zeros by select; subnormals, infinities and NaNs
-// (never met in practice) take the conversion instruction.
-__device__ __forceinline__ double tt_f2d(float f) {
-    const uint32_t b = __float_as_uint(f);
-    const uint32_t e = (b >> 23) & 0xffu;
-    if ((e == 0u && (b << 1) != 0u) || e == 0xffu) return (double)f;
-    uint32_t hi = (b & 0x80000000u) | ((e + 896u) << 20) | ((b & 0x7fffffu) >> 3);
-    uint32_t lo = b << 29;
-    hi = e == 0u ? (b & 0x80000000u) : hi;
-    lo = e == 0u ? 0u : lo;
-    return __hiloint2double((int)hi, (int)lo);
-}
-
 // the FP64 sum of one value per thread over all blocks of a 3-D grid of
 // TT_THREADS-thread blocks: block partials, then the last block to finish adds
 // them in a fixed order (deterministic); true in thread 0 of that block
@@ -155,10 +139,10 @@ __device__ __forceinline__ bool tt_finish(const Red& R, double mine, double* tot
 // launch with programmatic stream serialization (the kernel waits with
 // griddepcontrol.wait before it reads the previous launch's results)
 template <typename... KArgs, typename... Args>
-inline cudaError_t tt_launch(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t s,
+inline cudaError_t tt_launch(void (*kern)(KArgs...), dim3 grid, int block, size_t smem, cudaStream_t s,
                              Args... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid); cfg.blockDim = dim3(block); cfg.dynamicSmemBytes = smem; cfg.stream = s;
+    cfg.gridDim = grid; cfg.blockDim = dim3(block); cfg.dynamicSmemBytes = smem; cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -175,14 +159,10 @@ struct TtMaps {
 
 // MODE 0: p_new = r + beta p_old (first: r); z = A p_new; p_new . z
 // MODE 1: z = A p; x += alpha p, r -= alpha z; r . r; stop test
-// Work split: the (tile, plane) pairs of the grid, tile-major, are cut into
-// gridDim.x equal contiguous ranges, one per CTA (a range may end one tile and
-// start the next: two segments, each with its own halo planes). With one
-// wave of CTAs every SM then holds the same number of equal shares.
 template <class Op, int MODE>
 __global__ void __launch_bounds__(TT_THREADS, 3)
     k_cg_tma(Op op, const __grid_constant__ TtMaps maps, float* __restrict__ pout, float* __restrict__ x,
-             float* __restrict__ r, Red Rd, int tk, int first, int it, int maxiter, int skip_dot) {
+             float* __restrict__ r, Red Rd, int chunk, int first, int it, int maxiter, int skip_dot) {
     // launched with programmatic stream serialization: the previous launch on
     // the stream (the other pass) may still be finishing; its results (the
     // vectors, the scalars, the stop flag) are visible after this wait
@@ -199,152 +179,132 @@ __global__ void __launch_bounds__(TT_THREADS, 3)
     const Grid& g = op.g;
     const int tid = threadIdx.x;
     const int ty = tid >> 4, tg = tid & 15;
-    const long long units = (long long)tk * ((g.NY + TT_J - 1) / TT_J) * g.NX;
-    const long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
+    const int k0 = blockIdx.x * TT_K, j0 = blockIdx.y * TT_J;
+    const int i0 = blockIdx.z * chunk, i1 = min(i0 + chunk, g.NX);
+    const int kk = k0 + 4 * tg, jj = j0 + ty;
+    const bool inb = kk < g.NZ && jj < g.NY;
     const float bf = (MODE == 0 && !first) ? (float)Rd.scal[S_BETA] : 0.0f;
     const float af = MODE == 1 ? (float)Rd.scal[S_ALPHA] : 0.0f;
     const bool load_b = MODE == 1 || !first;
     const uint32_t tx = MODE == 0 ? (load_b ? 2 * TT_HALO_BYTES : TT_HALO_BYTES) + TT_NB_BYTES
                                   : TT_HALO_BYTES + 2 * TT_TILE_BYTES + TT_NB_BYTES;
+    // planes q = i0-1 .. i1 pass through the ring; plane q uses stage (q - i0 + 1) % NS
+    const int q0 = i0 - 1, nplanes = i1 - i0 + 2;
+
+    auto issue = [&](int t) {   // plane q0 + t into stage t % NS (thread 0)
+        unsigned char* st = sm + (t % TT_NS) * SB;
+        uint64_t* b = bar + (t % TT_NS);
+        const int q = q0 + t;
+        tt_bar_expect(b, tx);
+        if (MODE == 0) {
+            tt_load(st, &maps.a, b, k0 - 4, j0 - 1, q);
+            if (load_b) tt_load(st + TT_HALO_PAD, &maps.b, b, k0 - 4, j0 - 1, q);
+            tt_load(st + 2 * TT_HALO_PAD, &maps.nb, b, k0, j0, q);
+        } else {
+            tt_load(st, &maps.a, b, k0 - 4, j0 - 1, q);
+            tt_load(st + TT_HALO_PAD, &maps.b, b, k0, j0, q);
+            tt_load(st + TT_HALO_PAD + TT_TILE_BYTES, &maps.c, b, k0, j0, q);
+            tt_load(st + TT_HALO_PAD + 2 * TT_TILE_BYTES, &maps.nb, b, k0, j0, q);
+        }
+    };
     if (tid == 0) {
         tt_fail = 0;
         for (int s = 0; s < TT_NS; s++) tt_bar_init(bar + s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int t = 0; t < TT_NS && t < nplanes; t++) issue(t);
     }
     __syncthreads();
 
     double acc = 0;
-    // ring use counted over the whole CTA: plane number n (issued and consumed
-    // in the same order) lives in stage n % NS, phase (n / NS) & 1
-    int issued = 0, consumed = 0;
-    for (long long u = u0; u < u1 && !tt_fail;) {
-        const int tile = (int)(u / g.NX), i0 = (int)(u % g.NX);
-        const int i1 = (int)min((long long)g.NX, (long long)i0 + (u1 - u));
-        u += i1 - i0;
-        const int k0 = (tile % tk) * TT_K, j0 = (tile / tk) * TT_J;
-        const int kk = k0 + 4 * tg, jj = j0 + ty;
-        const bool inb = kk < g.NZ && jj < g.NY;
-        // planes q = i0-1 .. i1 pass through the ring
-        const int q0 = i0 - 1, nplanes = i1 - i0 + 2;
-        const int base = consumed;   // == issued: the ring is empty between segments
-        auto issue = [&](int t) {   // local plane t (plane q0 + t) into its stage (thread 0)
-            const int nidx = base + t;
-            unsigned char* st = sm + (nidx % TT_NS) * SB;
-            uint64_t* b = bar + (nidx % TT_NS);
-            const int q = q0 + t;
-            tt_bar_expect(b, tx);
-            if (MODE == 0) {
-                tt_load(st, &maps.a, b, k0 - 4, j0 - 1, q);
-                if (load_b) tt_load(st + TT_HALO_PAD, &maps.b, b, k0 - 4, j0 - 1, q);
-                tt_load(st + 2 * TT_HALO_PAD, &maps.nb, b, k0, j0, q);
-            } else {
-                tt_load(st, &maps.a, b, k0 - 4, j0 - 1, q);
-                tt_load(st + TT_HALO_PAD, &maps.b, b, k0, j0, q);
-                tt_load(st + TT_HALO_PAD + TT_TILE_BYTES, &maps.c, b, k0, j0, q);
-                tt_load(st + TT_HALO_PAD + 2 * TT_TILE_BYTES, &maps.nb, b, k0, j0, q);
+    // this thread's group of the previous plane: neighbour bytes, x, r
+    uint32_t m_prev = 0;
+    float4 x_prev = make_float4(0, 0, 0, 0), r_prev = x_prev;
+    int t = 0;
+    for (; t < nplanes; t++) {
+        const int q = q0 + t;
+        unsigned char* st = sm + (t % TT_NS) * SB;
+        // every thread waits for the stage itself; a wait that runs out is
+        // seen by all threads after the barrier below
+        const bool ok = tt_bar_wait(bar + (t % TT_NS), (uint32_t)((t / TT_NS) & 1));
+        if (!ok) atomicExch(&tt_fail, 1);
+        // the window plane of q from the stage
+        float4* w = reinterpret_cast<float4*>(win + (t % TT_NW) * (TT_HK * TT_HJ));
+        const float4* sa = reinterpret_cast<const float4*>(st);
+        const float4* sb = reinterpret_cast<const float4*>(st + TT_HALO_PAD);
+        for (int e = tid; ok && e < TT_HK * TT_HJ / 4; e += TT_THREADS) {
+            float4 a = sa[e];
+            if (MODE == 0 && !first) {
+                const float4 b = sb[e];
+                a = make_float4(a.x + bf * b.x, a.y + bf * b.y, a.z + bf * b.z, a.w + bf * b.w);
             }
-        };
-        if (tid == 0)
-            for (int t = 0; t < TT_NS && t < nplanes; t++) issue(t);
-        issued += min(TT_NS, nplanes);
-        // this thread's group of the previous plane: neighbour bytes, x, r
-        uint32_t m_prev = 0;
-        float4 x_prev = make_float4(0, 0, 0, 0), r_prev = x_prev;
-        for (int t = 0; t < nplanes; t++) {
-            const int q = q0 + t;
-            const int nidx = base + t;
-            unsigned char* st = sm + (nidx % TT_NS) * SB;
-            // every thread waits for the stage itself; a wait that runs out is
-            // seen by all threads after the barrier below
-            const bool ok = tt_bar_wait(bar + (nidx % TT_NS), (uint32_t)((nidx / TT_NS) & 1));
-            if (!ok) atomicExch(&tt_fail, 1);
-            // the window plane of q from the stage
-            float4* w = reinterpret_cast<float4*>(win + (t % TT_NW) * (TT_HK * TT_HJ));
-            const float4* sa = reinterpret_cast<const float4*>(st);
-            const float4* sb = reinterpret_cast<const float4*>(st + TT_HALO_PAD);
-            for (int e = tid; ok && e < TT_HK * TT_HJ / 4; e += TT_THREADS) {
-                float4 a = sa[e];
-                if (MODE == 0 && !first) {
-                    const float4 b = sb[e];
-                    a = make_float4(a.x + bf * b.x, a.y + bf * b.y, a.z + bf * b.z, a.w + bf * b.w);
-                }
-                w[e] = a;
-            }
-            // this thread's own group of plane q
-            uint32_t m_cur;
-            float4 x_cur = make_float4(0, 0, 0, 0), r_cur = x_cur;
-            if (MODE == 0) {
-                m_cur = reinterpret_cast<const uint32_t*>(st + 2 * TT_HALO_PAD)[tid];
-            } else {
-                x_cur = reinterpret_cast<const float4*>(st + TT_HALO_PAD)[tid];
-                r_cur = reinterpret_cast<const float4*>(st + TT_HALO_PAD + TT_TILE_BYTES)[tid];
-                m_cur = reinterpret_cast<const uint32_t*>(st + TT_HALO_PAD + 2 * TT_TILE_BYTES)[tid];
-            }
-            // every thread has read the stage: order those reads before the TMA
-            // writes that refill it, and publish the window plane
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (tt_fail) break;
-            consumed++;
-            if (t + TT_NS < nplanes) {
-                if (tid == 0) issue(t + TT_NS);
-                issued++;
-            }
-            // the row of plane q-1 from window planes q-2, q-1, q
-            const int ic = q - 1;
-            if (t >= 2 && inb && (m_prev & 0x80808080u)) {
-                const float* wm = win + ((t - 2) % TT_NW) * (TT_HK * TT_HJ);
-                const float* wc = win + ((t - 1) % TT_NW) * (TT_HK * TT_HJ);
-                const float* wp = win + (t % TT_NW) * (TT_HK * TT_HJ);
-                const int o = (ty + 1) * TT_HK + 4 + 4 * tg;
-                const float4 c = *reinterpret_cast<const float4*>(wc + o);
-                const float4 xp = *reinterpret_cast<const float4*>(wp + o);
-                const float4 xm = *reinterpret_cast<const float4*>(wm + o);
-                const float4 yp = *reinterpret_cast<const float4*>(wc + o + TT_HK);
-                const float4 ym = *reinterpret_cast<const float4*>(wc + o - TT_HK);
-                const float zm = wc[o - 1], zp = wc[o + 4];
-                const float cv[6] = {zm, c.x, c.y, c.z, c.w, zp};
-                const float xpv[4] = {xp.x, xp.y, xp.z, xp.w}, xmv[4] = {xm.x, xm.y, xm.z, xm.w};
-                const float ypv[4] = {yp.x, yp.y, yp.z, yp.w}, ymv[4] = {ym.x, ym.y, ym.z, ym.w};
-                float xov[4] = {x_prev.x, x_prev.y, x_prev.z, x_prev.w};
-                float rov[4] = {r_prev.x, r_prev.y, r_prev.z, r_prev.w};
-                float po[4];
-                const int cidx = (ic * g.NY + jj) * g.NZ + kk;
-                #pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const uint32_t m = (m_prev >> (8 * e)) & 0xffu;
-                    const float cur = cv[e + 1];
-                    po[e] = (m & 0x80) ? cur : 0.0f;
-                    if (m & 0x80) {
-                        float s = op.template start<float>(cidx + e, cur);
-                        s = op.template comb<float>(s, (m & 1) ? cur : xpv[e]);
-                        s = op.template comb<float>(s, (m & 2) ? cur : ypv[e]);
-                        s = op.template comb<float>(s, (m & 4) ? cur : cv[e + 2]);
-                        s = op.template comb<float>(s, (m & 8) ? cur : xmv[e]);
-                        s = op.template comb<float>(s, (m & 16) ? cur : ymv[e]);
-                        s = op.template comb<float>(s, (m & 32) ? cur : cv[e]);
-                        const float z = op.template finish<float>(s);
-                        if (MODE == 0) {
-                            acc += tt_f2d(z) * tt_f2d(cur);
-                        } else {
-                            xov[e] = xov[e] + af * cur;
-                            rov[e] = rov[e] + (-af) * z;
-                            const double rd = tt_f2d(rov[e]);
-                            acc += rd * rd;
-                        }
+            w[e] = a;
+        }
+        // this thread's own group of plane q
+        uint32_t m_cur;
+        float4 x_cur = make_float4(0, 0, 0, 0), r_cur = x_cur;
+        if (MODE == 0) {
+            m_cur = reinterpret_cast<const uint32_t*>(st + 2 * TT_HALO_PAD)[tid];
+        } else {
+            x_cur = reinterpret_cast<const float4*>(st + TT_HALO_PAD)[tid];
+            r_cur = reinterpret_cast<const float4*>(st + TT_HALO_PAD + TT_TILE_BYTES)[tid];
+            m_cur = reinterpret_cast<const uint32_t*>(st + TT_HALO_PAD + 2 * TT_TILE_BYTES)[tid];
+        }
+        // every thread has read stage t: order those reads before the TMA
+        // writes that refill it, and publish the window plane
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tt_fail) break;
+        if (tid == 0 && t + TT_NS < nplanes) issue(t + TT_NS);
+        // the row of plane q-1 from window planes q-2, q-1, q
+        const int ic = q - 1;
+        if (t >= 2 && inb && (m_prev & 0x80808080u)) {
+            const float* wm = win + ((t - 2) % TT_NW) * (TT_HK * TT_HJ);
+            const float* wc = win + ((t - 1) % TT_NW) * (TT_HK * TT_HJ);
+            const float* wp = win + (t % TT_NW) * (TT_HK * TT_HJ);
+            const int o = (ty + 1) * TT_HK + 4 + 4 * tg;
+            const float4 c = *reinterpret_cast<const float4*>(wc + o);
+            const float4 xp = *reinterpret_cast<const float4*>(wp + o);
+            const float4 xm = *reinterpret_cast<const float4*>(wm + o);
+            const float4 yp = *reinterpret_cast<const float4*>(wc + o + TT_HK);
+            const float4 ym = *reinterpret_cast<const float4*>(wc + o - TT_HK);
+            const float zm = wc[o - 1], zp = wc[o + 4];
+            const float cv[6] = {zm, c.x, c.y, c.z, c.w, zp};
+            const float xpv[4] = {xp.x, xp.y, xp.z, xp.w}, xmv[4] = {xm.x, xm.y, xm.z, xm.w};
+            const float ypv[4] = {yp.x, yp.y, yp.z, yp.w}, ymv[4] = {ym.x, ym.y, ym.z, ym.w};
+            float xov[4] = {x_prev.x, x_prev.y, x_prev.z, x_prev.w}, rov[4] = {r_prev.x, r_prev.y, r_prev.z, r_prev.w};
+            float po[4];
+            const int cidx = (ic * g.NY + jj) * g.NZ + kk;
+            #pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const uint32_t m = (m_prev >> (8 * e)) & 0xffu;
+                const float cur = cv[e + 1];
+                po[e] = (m & 0x80) ? cur : 0.0f;
+                if (m & 0x80) {
+                    float s = op.template start<float>(cidx + e, cur);
+                    s = op.template comb<float>(s, (m & 1) ? cur : xpv[e]);
+                    s = op.template comb<float>(s, (m & 2) ? cur : ypv[e]);
+                    s = op.template comb<float>(s, (m & 4) ? cur : cv[e + 2]);
+                    s = op.template comb<float>(s, (m & 8) ? cur : xmv[e]);
+                    s = op.template comb<float>(s, (m & 16) ? cur : ymv[e]);
+                    s = op.template comb<float>(s, (m & 32) ? cur : cv[e]);
+                    const float z = op.template finish<float>(s);
+                    if (MODE == 0) {
+                        acc += (double)z * (double)cur;
+                    } else {
+                        xov[e] = xov[e] + af * cur;
+                        rov[e] = rov[e] + (-af) * z;
+                        acc += (double)rov[e] * (double)rov[e];
                     }
                 }
-                if (MODE == 0) {
-                    reinterpret_cast<float4*>(pout)[cidx >> 2] = make_float4(po[0], po[1], po[2], po[3]);
-                } else {
-                    reinterpret_cast<float4*>(x)[cidx >> 2] = make_float4(xov[0], xov[1], xov[2], xov[3]);
-                    reinterpret_cast<float4*>(r)[cidx >> 2] = make_float4(rov[0], rov[1], rov[2], rov[3]);
-                }
             }
-            m_prev = m_cur; x_prev = x_cur; r_prev = r_cur;
+            if (MODE == 0) {
+                reinterpret_cast<float4*>(pout)[cidx >> 2] = make_float4(po[0], po[1], po[2], po[3]);
+            } else {
+                reinterpret_cast<float4*>(x)[cidx >> 2] = make_float4(xov[0], xov[1], xov[2], xov[3]);
+                reinterpret_cast<float4*>(r)[cidx >> 2] = make_float4(rov[0], rov[1], rov[2], rov[3]);
+            }
         }
-        // every thread is done with the window before the next segment writes it
-        __syncthreads();
+        m_prev = m_cur; x_prev = x_cur; r_prev = r_cur;
     }
     // the next pass may be launched now; it waits for this grid's completion
     // before it reads anything this grid writes
@@ -354,7 +314,7 @@ __global__ void __launch_bounds__(TT_THREADS, 3)
         // into this CTA's ring, report the timeout and leave without joining
         // the sum (the host clears the block counter before the next solve)
         if (tid == 0) {
-            for (int n = consumed; n < issued; n++) tt_bar_wait(bar + (n % TT_NS), (uint32_t)((n / TT_NS) & 1));
+            for (int u = t; u < nplanes && u < t + TT_NS; u++) tt_bar_wait(bar + (u % TT_NS), (uint32_t)((u / TT_NS) & 1));
             Rd.flag[F_DONE] = DONE_TIMEOUT;
         }
         return;

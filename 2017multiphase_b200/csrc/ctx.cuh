@@ -56,9 +56,9 @@ struct MpCtx {
     int red_blocks = 0;
     // CG kernels (tuning knobs read from the environment at mp_create):
     // MP_CG_KERNEL=v4 keeps the float4-group passes where the TMA plane
-    // marching applies; MP_CG_TMA_CTAS sets its CTA count (0: one wave)
+    // marching applies; MP_CG_TMA_CHUNK sets its planes per CTA (0: derived)
     int cg_use_tma = 1;
-    int cg_tma_ctas = 0;
+    int cg_tma_chunk = 0;
     float *gfm_beta = 0;         // ghost-fluid face weights (x, y, z faces), allocated on first use
     float *gfm_s = 0;            // its Jacobi scaling per cell
     // particles

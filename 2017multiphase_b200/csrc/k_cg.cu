@@ -896,7 +896,8 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     bool tma = kF32 && !kGeneral && c->cg_use_tma && gg.NZ % 16 == 0 && al16(x) && al16(r) && al16(p0) &&
                al16(p1) && tt_encoder() != nullptr;
     TtMaps tmaps[4];   // direction with p_old = p0 / p1, update with p = p1 / p0
-    int tgrid = 0, ttk = 0;
+    dim3 tgrid;
+    int tchunk = 0;
     if constexpr (kF32 && !kGeneral) {
         if (tma) {
             tma = tt_encode(&tmaps[0].a, r, gg, 4, TT_HK, TT_HJ) && tt_encode(&tmaps[0].b, p0, gg, 4, TT_HK, TT_HJ) &&
@@ -909,25 +910,19 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
             tma = tma && tt_encode(&tmaps[3].a, p0, gg, 4, TT_HK, TT_HJ);
         }
         if (tma) {
+            // the (k, j) tiles of one chunk of planes run together (their halo
+            // rows meet in L2); chunks sized for one wave of 3 CTAs per SM
+            const int tk = (gg.NZ + TT_K - 1) / TT_K, tj = (gg.NY + TT_J - 1) / TT_J;
+            int nch = std::max(1, (148 * 3) / (tk * tj));
+            tchunk = c->cg_tma_chunk > 0 ? c->cg_tma_chunk : std::max(4, (gg.NX + nch - 1) / nch);
+            tgrid = dim3(tk, tj, (gg.NX + tchunk - 1) / tchunk);
+            if ((long long)tgrid.x * tgrid.y * tgrid.z > 148LL * 32) tma = false;   // the partial-sum slots
+        }
+        if (tma) {
             MP_CUDA(c, cudaFuncSetAttribute(k_cg_tma<Op, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)tt_smem_bytes<0>()));
             MP_CUDA(c, cudaFuncSetAttribute(k_cg_tma<Op, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)tt_smem_bytes<1>()));
-            // one wave: as many CTAs as are resident at once (the fewer of the
-            // two passes' occupancies), each taking an equal share of the
-            // (tile, plane) pairs
-            ttk = (gg.NZ + TT_K - 1) / TT_K;
-            const long long units = (long long)ttk * ((gg.NY + TT_J - 1) / TT_J) * gg.NX;
-            int sms = 0, occ0 = 0, occ1 = 0;
-            MP_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-            MP_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k_cg_tma<Op, 0>, TT_THREADS,
-                                                                     tt_smem_bytes<0>()));
-            MP_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k_cg_tma<Op, 1>, TT_THREADS,
-                                                                     tt_smem_bytes<1>()));
-            long long want = (long long)sms * std::max(1, std::min(occ0, occ1));
-            if (c->cg_tma_ctas > 0) want = c->cg_tma_ctas;
-            tgrid = (int)std::max(1LL, std::min(want, units));
-            if (tgrid > 148 * 32) tma = false;   // the partial-sum slots
         }
     }
     const bool v4 = kF32 && gg.NZ % 4 == 0;
@@ -961,13 +956,13 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
                     {
                         KtScope kt(c, kt_stencil);
                         MP_CUDA(c, tt_launch(k_cg_tma<Op, 0>, tgrid, TT_THREADS, tt_smem_bytes<0>(), s, op, tmaps[d],
-                                             pb, (float*)nullptr, (float*)nullptr, Rd, ttk, it == 0 ? 1 : 0, it,
+                                             pb, (float*)nullptr, (float*)nullptr, Rd, tchunk, it == 0 ? 1 : 0, it,
                                              maxiter, 0));
                     }
                     {
                         KtScope kt(c, MP_KT_CG_UPDATE);
                         MP_CUDA(c, tt_launch(k_cg_tma<Op, 1>, tgrid, TT_THREADS, tt_smem_bytes<1>(), s, op,
-                                             tmaps[2 + d], (float*)nullptr, x, r, Rd, ttk, 0, it, maxiter,
+                                             tmaps[2 + d], (float*)nullptr, x, r, Rd, tchunk, 0, it, maxiter,
                                              tr ? 1 : 0));
                     }
                 } else if (v4) {

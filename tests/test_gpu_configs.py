@@ -22,8 +22,8 @@ and over the configurations' step counts (bubblesim, spray.cpp:979-1233).
 import numpy as np
 import pytest
 
-from parity_util import (bubblesim_stages, check_one_step, compare, drift, grid_params, make_pair, snapshot,
-                         transplant)
+from parity_util import (bubblesim_stages, check_one_step, compare, drift, grid_params, make_pair, rel_err,
+                         snapshot, transplant)
 
 pytestmark = pytest.mark.gpu
 
@@ -106,8 +106,12 @@ def test_drift_over_steps(mp, oracle_mod, config):
         if checks[s] == "exact":
             # the solid-velocity faces are not gathered by the step when no
             # cell holds a SOLID particle (the collision reads them only near
-            # a solid); the oracle fills them anyway
-            bad = compare(g, r, exact=True, skip=("solidux", "soliduy", "soliduz"))
+            # a solid); the oracle fills them anyway. Solubility and gas
+            # content take expf, whose CUDA and host results may differ in the
+            # last bit (the stage tests compare them at 1e-5)
+            bad = compare(g, r, exact=True, skip=("solidux", "soliduy", "soliduz", "solubility", "gascontain"))
+            assert rel_err(g["solubility"], r["solubility"]) <= 1e-5
+            assert rel_err(g["gascontain"], r["gascontain"]) <= 1e-5
             assert not bad, f"config {config} step {s}: not bit-identical: {bad[:3]}"
             continue
         d = drift(g, r)
