@@ -156,38 +156,21 @@ __device__ __forceinline__ uint32_t hash_key(float4 q, float gx0, float gy0, flo
     int k = (r.z >= 0 && r.z < d) ? (int)r.z : 0;
     return (uint32_t)(i * hh * d + j * d + k);
 }
-// keys, per-cell counts, each cell's type mask (which particle types it holds;
-// the cleared mask words take one OR per run of equal keys), and a flag raised
-// when the keys are not already in order (then the stable sort is the
-// identity and the gather can be skipped)
-// With `air_words` (the simulation grid's sort), the bit of each 4x4x4-cell
-// brick that holds an AIR or AIRSOLO particle is set as well.
+// keys, per-cell counts, and a flag raised when the keys are not already in
+// order (then the stable sort is the identity and the gather can be skipped)
 __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, float gy0, float gz0, float dx,
                              int w, int hh, int d, uint32_t* __restrict__ keys, uint32_t* __restrict__ cnt,
-                             uint32_t* __restrict__ tmask_words, uint32_t* __restrict__ air_words,
                              uint32_t* __restrict__ unsorted) {
     __shared__ uint32_t blk_unsorted;
     if (threadIdx.x == 0) blk_unsorted = 0;
     __syncthreads();
     MP_GRID_LOOP(p, np) {
-        const float4 q = pos[p];
-        uint32_t key = hash_key(q, gx0, gy0, gz0, dx, w, hh, d);
+        uint32_t key = hash_key(pos[p], gx0, gy0, gz0, dx, w, hh, d);
         if (p > 0 && hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d) > key) blk_unsorted = 1u;
         keys[p] = key;
         // one atomic per run of equal keys in the warp (particles arrive nearly sorted)
         unsigned peers = __match_any_sync(__activemask(), key);
-        const uint32_t bits = __reduce_or_sync(peers, 1u << (pflag(q) & 7));
-        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) {
-            atomicAdd(cnt + key, (uint32_t)__popc(peers));
-            atomicOr(tmask_words + (key >> 2), bits << (8 * (key & 3)));
-            if (air_words && (bits & ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO)))) {
-                const uint32_t kk = key % (uint32_t)d, jj = (key / (uint32_t)d) % (uint32_t)hh,
-                               ii = key / ((uint32_t)d * (uint32_t)hh);
-                const uint32_t bw = ((uint32_t)d + 3) / 4, bh = ((uint32_t)hh + 3) / 4;
-                const uint32_t br = ((ii >> 2) * bh + (jj >> 2)) * bw + (kk >> 2);
-                atomicOr(air_words + (br >> 5), 1u << (br & 31));
-            }
-        }
+        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(cnt + key, (uint32_t)__popc(peers));
     }
     __syncthreads();
     if (threadIdx.x == 0 && blk_unsorted) *unsorted = 1u;   // one store per block
@@ -215,6 +198,25 @@ __global__ void k_segsort(const uint32_t* __restrict__ off, int ncell, uint32_t*
         sort_distinct_run(perm, s0, off[cc + 1] - s0, [&](uint32_t) {});
     }
 }
+// each cell's type mask (which particle types it holds) from the particles in
+// cell order (coalesced reads), and with `air_words` (the simulation grid's
+// sort) the bit of each 4x4x4-cell brick that holds an AIR or AIRSOLO particle
+__global__ void k_tmask_sorted(const uint32_t* __restrict__ off, int ncell, int w, int hh, int d,
+                               const float4* __restrict__ pos, uint8_t* __restrict__ tmask,
+                               uint32_t* __restrict__ air_words) {
+    MP_GRID_LOOP(cc, ncell) {
+        uint32_t m = 0;
+        for (uint32_t s = off[cc]; s < off[cc + 1]; s++) m |= 1u << (pflag(__ldg(pos + s)) & 7);
+        tmask[cc] = (uint8_t)m;
+        if (air_words && (m & ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO)))) {
+            const uint32_t kk = (uint32_t)cc % (uint32_t)d, jj = ((uint32_t)cc / (uint32_t)d) % (uint32_t)hh,
+                           ii = (uint32_t)cc / ((uint32_t)d * (uint32_t)hh);
+            const uint32_t bw = ((uint32_t)d + 3) / 4, bh = ((uint32_t)hh + 3) / 4;
+            const uint32_t br = ((ii >> 2) * bh + (jj >> 2)) * bw + (kk >> 2);
+            atomicOr(air_words + (br >> 5), 1u << (br & 31));
+        }
+    }
+}
 __global__ void k_reorder(const uint32_t* __restrict__ perm, int np,
                           const float4* __restrict__ p0, const float4* __restrict__ v0, const float4* __restrict__ h0,
                           float4* __restrict__ p1, float4* __restrict__ v1, float4* __restrict__ h1) {
@@ -232,14 +234,18 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     int ncell = w * hh * d;
     uint32_t* unsorted = c->u32_scratch + 1;
     MP_CUDA(c, cudaMemsetAsync(unsorted, 0, sizeof(uint32_t), c->stream));
-    MP_CUDA(c, cudaMemsetAsync(c->tmask, 0, ((size_t)ncell + 3) / 4 * 4, c->stream));
     const bool sim_grid = w == c->G.NX && hh == c->G.NY && d == c->G.NZ;
     if (sim_grid) MP_CUDA(c, cudaMemsetAsync(c->air_brick, 0, sizeof(uint32_t) * c->air_brick_words, c->stream));
+    auto tmask_pass = [&]() -> int {
+        k_tmask_sorted<<<mp_blocks(ncell, 256), 256, 0, c->stream>>>(c->cell_off, ncell, w, hh, d, c->pos, c->tmask,
+                                                                     sim_grid ? c->air_brick : nullptr);
+        c->launches++;
+        MP_CHECK_LAUNCH(c);
+        return MP_OK;
+    };
     if (np > 0) {
         k_hash_count<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->pos, np, c->G.gx0, c->G.gy0, c->G.gz0, dx, w, hh, d,
-                                                                c->keys, c->cell_cnt,
-                                                                reinterpret_cast<uint32_t*>(c->tmask),
-                                                                sim_grid ? c->air_brick : nullptr, unsorted);
+                                                                c->keys, c->cell_cnt, unsorted);
         c->launches++;
         MP_CHECK_LAUNCH(c);
     }
@@ -252,7 +258,7 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
         // already in cell order: the stable sort is the identity permutation;
         // the counts still have to run back to zero for the next sort
         MP_CUDA(c, cudaMemsetAsync(c->cell_cnt, 0, sizeof(uint32_t) * ncell, c->stream));
-        return MP_OK;
+        return tmask_pass();
     }
     if (np > 0) {
         k_scatter<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->keys, np, c->cell_off, c->cell_cnt, c->perm);
@@ -268,7 +274,7 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
         MP_CHECK_LAUNCH(c);
         std::swap(c->pos, c->pos2); std::swap(c->vel, c->vel2); std::swap(c->heat, c->heat2);
     }
-    return MP_OK;
+    return tmask_pass();
 }
 
 int k_hash_sort(MpCtx* c) {
