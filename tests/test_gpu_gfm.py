@@ -1,10 +1,10 @@
 """Ghost-fluid variable-density projection (MP_COEF_GFM) on the GPU.
 
-An extension the north star asks for (the reference's projection is
-constant-coefficient). The GPU form (Jacobi-scaled CG, FP32 vectors, FP64
-dots, stop at the configuration's 1e-6 relative residual) is checked against
-the oracle's FP64 restatement solved to 1e-12 from the same transplanted
-state; at a unit density ratio it is checked against the GPU's own reference
+An extension beyond the reference, whose projection is constant-coefficient.
+The GPU forms (Jacobi-scaled CG: FP32 vectors with FP64 dots, the same with
+mixed-precision refinement, and all-FP64) are checked against the oracle's
+FP64 restatement solved to 1e-12 from the same transplanted state; at a unit
+density ratio the GPU form is checked against the GPU's own reference
 projection.
 """
 import numpy as np
