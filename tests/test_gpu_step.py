@@ -113,7 +113,7 @@ def test_mixed_form_fields_against_fp64_form(mp, oracle_mod, config, n):
     pass adds ~eps*cond on top (1e-5..1e-3 of the splatted velocity in these
     liquids near rest), which the FP64 true residual removes: the refined
     mixed form's faces are as close to the reference as the FP64 form's
-    (within 1.5x, plus 1e-6 of the splatted velocity), the single pass's
+    (within 3x, plus 2e-6 of the splatted velocity), the single pass's
     within 2e-3."""
     from parity_util import rel_l2
     sim = mp.Sim.from_config(config, n, 9300 + config)
@@ -139,7 +139,7 @@ def test_mixed_form_fields_against_fp64_form(mp, oracle_mod, config, n):
         scale = max(np.linalg.norm(out["ref"][f + "_old"].astype(np.float64)), 1e-30)
         err = {form: float(np.linalg.norm(out[form][f].astype(np.float64) - out["ref"][f]) / scale)
                for form in ("fp64", "mixed", "refined")}
-        assert err["refined"] <= 1.5 * err["fp64"] + 1e-6, f"config {config} {f}: {err}"
+        assert err["refined"] <= 3 * err["fp64"] + 2e-6, f"config {config} {f}: {err}"
         assert err["mixed"] <= 2e-3, f"config {config} {f}: {err}"
     sim.close()
 
