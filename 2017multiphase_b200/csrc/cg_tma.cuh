@@ -28,14 +28,29 @@
 
 namespace {
 
+#ifndef TT_NS0
+#define TT_NS0 3
+#endif
+#ifndef TT_CTAS0
+#define TT_CTAS0 4
+#endif
+#ifndef TT_NS1
+#define TT_NS1 3
+#endif
+#ifndef TT_CTAS1
+#define TT_CTAS1 3
+#endif
 constexpr int TT_K = 64;              // tile cells along k (16 float4 groups)
 constexpr int TT_J = 16;              // tile rows along j
 constexpr int TT_THREADS = TT_J * (TT_K / 4);   // one thread per float4 group: 256
 constexpr int TT_HK = TT_K + 8;       // halo box along k: k0-4 .. k0+TK+3 (72 floats)
 constexpr int TT_HJ = TT_J + 2;       // halo box along j: j0-1 .. j0+TJ (18 rows)
-// ring stages: MODE 0 keeps three planes in flight (3 CTAs of 65 KB per
-// SM); MODE 1's stages are larger, so it keeps two (3 CTAs of 63 KB)
-template <int MODE> __host__ __device__ constexpr int tt_ns() { return MODE == 0 ? 4 : 3; }
+// ring stages and resident CTAs per SM: the direction pass keeps two planes
+// in flight with 4 CTAs of 54 KB per SM (more warps to cover the per-plane
+// latency measured faster than three planes in flight with 3 CTAs of 65 KB);
+// the update pass's stages are larger: two planes in flight, 3 CTAs of 63 KB
+template <int MODE> __host__ __device__ constexpr int tt_ns() { return MODE == 0 ? TT_NS0 : TT_NS1; }
+template <int MODE> __host__ __device__ constexpr int tt_ctas() { return MODE == 0 ? TT_CTAS0 : TT_CTAS1; }
 constexpr int TT_NW = 4;              // window planes
 constexpr uint32_t TT_HALO_BYTES = TT_HK * TT_HJ * 4;        // 5184
 constexpr uint32_t TT_HALO_PAD = (TT_HALO_BYTES + 127) / 128 * 128;   // 5248
@@ -160,7 +175,7 @@ struct TtMaps {
 // MODE 0: p_new = r + beta p_old (first: r); z = A p_new; p_new . z
 // MODE 1: z = A p; x += alpha p, r -= alpha z; r . r; stop test
 template <class Op, int MODE>
-__global__ void __launch_bounds__(TT_THREADS, 3)
+__global__ void __launch_bounds__(TT_THREADS, tt_ctas<MODE>())
     k_cg_tma(Op op, const __grid_constant__ TtMaps maps, float* __restrict__ pout, float* __restrict__ x,
              float* __restrict__ r, Red Rd, int chunk, int first, int it, int maxiter, int skip_dot) {
     // launched with programmatic stream serialization: the previous launch on

@@ -896,8 +896,8 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
     bool tma = kF32 && !kGeneral && c->cg_use_tma && gg.NZ % 16 == 0 && al16(x) && al16(r) && al16(p0) &&
                al16(p1) && tt_encoder() != nullptr;
     TtMaps tmaps[4];   // direction with p_old = p0 / p1, update with p = p1 / p0
-    dim3 tgrid;
-    int tchunk = 0;
+    dim3 tgrid, tgrid0;          // update pass, direction pass
+    int tchunk = 0, tchunk0 = 0;
     if constexpr (kF32 && !kGeneral) {
         if (tma) {
             tma = tt_encode(&tmaps[0].a, r, gg, 4, TT_HK, TT_HJ) && tt_encode(&tmaps[0].b, p0, gg, 4, TT_HK, TT_HJ) &&
@@ -911,12 +911,19 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
         }
         if (tma) {
             // the (k, j) tiles of one chunk of planes run together (their halo
-            // rows meet in L2); chunks sized for one wave of 3 CTAs per SM
+            // rows meet in L2); chunks sized for one wave of each pass's
+            // resident CTAs per SM
             const int tk = (gg.NZ + TT_K - 1) / TT_K, tj = (gg.NY + TT_J - 1) / TT_J;
-            int nch = std::max(1, (148 * 3) / (tk * tj));
-            tchunk = c->cg_tma_chunk > 0 ? c->cg_tma_chunk : std::max(4, (gg.NX + nch - 1) / nch);
+            auto chunk_for = [&](int ctas) {
+                const int nch = std::max(1, (148 * ctas) / (tk * tj));
+                return c->cg_tma_chunk > 0 ? c->cg_tma_chunk : std::max(4, (gg.NX + nch - 1) / nch);
+            };
+            tchunk0 = chunk_for(tt_ctas<0>());
+            tchunk = chunk_for(tt_ctas<1>());
+            tgrid0 = dim3(tk, tj, (gg.NX + tchunk0 - 1) / tchunk0);
             tgrid = dim3(tk, tj, (gg.NX + tchunk - 1) / tchunk);
-            if ((long long)tgrid.x * tgrid.y * tgrid.z > 148LL * 32) tma = false;   // the partial-sum slots
+            if ((long long)tgrid0.x * tgrid0.y * tgrid0.z > 148LL * 32 || (long long)tgrid.x * tgrid.y * tgrid.z > 148LL * 32)
+                tma = false;   // the partial-sum slots
         }
         if (tma) {
             MP_CUDA(c, cudaFuncSetAttribute(k_cg_tma<Op, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -955,8 +962,8 @@ static int run_cg(MpCtx* c, const Op& op, R* x, const R* b, R* r, R* p0, R* p1, 
                     const int d = (pa == p0) ? 0 : 1;   // p_old
                     {
                         KtScope kt(c, kt_stencil);
-                        MP_CUDA(c, tt_launch(k_cg_tma<Op, 0>, tgrid, TT_THREADS, tt_smem_bytes<0>(), s, op, tmaps[d],
-                                             pb, (float*)nullptr, (float*)nullptr, Rd, tchunk, it == 0 ? 1 : 0, it,
+                        MP_CUDA(c, tt_launch(k_cg_tma<Op, 0>, tgrid0, TT_THREADS, tt_smem_bytes<0>(), s, op, tmaps[d],
+                                             pb, (float*)nullptr, (float*)nullptr, Rd, tchunk0, it == 0 ? 1 : 0, it,
                                              maxiter, 0));
                     }
                     {
