@@ -35,20 +35,23 @@ namespace {
 #define TT_CTAS0 4
 #endif
 #ifndef TT_NS1
-#define TT_NS1 3
+#define TT_NS1 2
 #endif
 #ifndef TT_CTAS1
-#define TT_CTAS1 3
+#define TT_CTAS1 4
 #endif
 constexpr int TT_K = 64;              // tile cells along k (16 float4 groups)
 constexpr int TT_J = 16;              // tile rows along j
 constexpr int TT_THREADS = TT_J * (TT_K / 4);   // one thread per float4 group: 256
 constexpr int TT_HK = TT_K + 8;       // halo box along k: k0-4 .. k0+TK+3 (72 floats)
 constexpr int TT_HJ = TT_J + 2;       // halo box along j: j0-1 .. j0+TJ (18 rows)
-// ring stages and resident CTAs per SM: the direction pass keeps two planes
-// in flight with 4 CTAs of 54 KB per SM (more warps to cover the per-plane
-// latency measured faster than three planes in flight with 3 CTAs of 65 KB);
-// the update pass's stages are larger: two planes in flight, 3 CTAs of 63 KB
+// ring stages and resident CTAs per SM. Both passes are bound by issue
+// latency at the occupancy shared memory allows, so more resident warps beat
+// deeper prefetch: the direction pass keeps two planes in flight with 4 CTAs
+// of 54 KB per SM (faster than three planes with 3 CTAs of 65 KB, and than
+// one plane with 5 CTAs of 43 KB); the update pass, whose stages are larger,
+// keeps one plane in flight with 4 CTAs of 49 KB (faster than two planes with
+// 3 CTAs of 63 KB)
 template <int MODE> __host__ __device__ constexpr int tt_ns() { return MODE == 0 ? TT_NS0 : TT_NS1; }
 template <int MODE> __host__ __device__ constexpr int tt_ctas() { return MODE == 0 ? TT_CTAS0 : TT_CTAS1; }
 constexpr int TT_NW = 4;              // window planes

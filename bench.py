@@ -40,9 +40,9 @@ def names_kt(mp):
 # as functions of (cells, particles): the capture's bytes scaled by the units a
 # launch processes
 TRAFFIC_PER_LAUNCH = {
-    # the TMA CG passes captured at 256^3: 188.7 MB and 291.9 MB per launch
-    "k_cg_dir": lambda n, np_: 188.71e6 * n / 256 ** 3,
-    "k_cg_upd": lambda n, np_: 291.91e6 * n / 256 ** 3,
+    # the TMA CG passes captured at 256^3: 189.4 MB and 294.5 MB per launch
+    "k_cg_dir": lambda n, np_: 189.36e6 * n / 256 ** 3,
+    "k_cg_upd": lambda n, np_: 294.46e6 * n / 256 ** 3,
     # the MC density pass captured at 128^3 (12.9M particles): 711.9 MB per
     # launch; nodes and particles both grow with the cells
     "k_mc_density": lambda n, np_: 711.91e6 * n / 128 ** 3,
