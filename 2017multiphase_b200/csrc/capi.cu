@@ -160,6 +160,8 @@ static int check_params(const mp_params* p, std::string& err) {
     if (!p) { err = "null params"; return MP_ERR_ARG; }
     if (p->version != MP_PARAMS_VERSION) { err = "params version mismatch"; return MP_ERR_ARG; }
     if (p->nx < 4 || p->ny < 4 || p->nz < 4) { err = "grid must be at least 4^3"; return MP_ERR_ARG; }
+    // row-per-block launches put i and j in the grid's z and y extents
+    if (p->nx > 65534 || p->ny > 65534) { err = "grid x and y extents must be below 65535"; return MP_ERR_ARG; }
     long long n = (long long)p->nx * p->ny * p->nz;
     if (8 * n + 1 > 0x7fffffffLL || 3LL * (2 * p->nx + 1) * (2 * p->ny + 1) * (2 * p->nz + 1) > 0x7fffffffLL) {
         err = "grid too large for 32-bit indexing"; return MP_ERR_ARG;

@@ -101,47 +101,71 @@ __device__ __forceinline__ void solvedistance(float a, float b, float c, float& 
         d = (a + b + c + sqrtf(3 - (a - b) * (a - b) - (a - c) * (a - c) - (b - c) * (b - c))) / 3;
     if (d < x) x = d;
 }
-// one Jacobi pass of sweepphibytype (typeflag >= 0) or sweepphi (typeflag < 0)
-__global__ void k_sweep(Grid g, const float* __restrict__ in, float* __restrict__ out,
-                        const int8_t* __restrict__ mark, int typeflag) {
+// An octant with m = min(a,b,c) >= res cannot lower res, and skips the sqrt
+// and the division, when its result is provably not below res: the result is
+// m + 1 rounded (>= m) when that is not above the maximum; otherwise
+// ((a+b)+c + sqrt(...)) / 3 rounded, which by monotone rounding is at least
+// fl(fl(3m) / 3) (or NaN): that is m itself when 3m is exact
+// (fl(3m) - 2m == m, the subtraction being exact), and at least m - ulp(m)
+// otherwise, so then m two ulps down must still be >= res. sweep_settled(m)
+// is the last two conditions, which depend on m alone.
+__device__ __forceinline__ bool sweep_settled(float m, float res) {
+    const float t = 3.0f * m;
+    if (t - 2.0f * m == m) return true;
+    return m > 1e-30f && __int_as_float(__float_as_int(m) - 2) >= res;
+}
+// one cell of a Jacobi pass of sweepphibytype (typeflag >= 0) or sweepphi
+// (typeflag < 0)
+__device__ __forceinline__ float sweep_cell(const Grid& g, const float* __restrict__ in,
+                                            const int8_t* __restrict__ mark, int typeflag, int i, int j, int k,
+                                            int idx) {
     const int sI = g.NY * g.NZ, sJ = g.NZ;
-    MP_GRID_LOOP(idx, g.n) {
-        float res = in[idx];
-        if (!(typeflag >= 0 && mark[idx] == typeflag)) {
-            int i, j, k; getijk(g, (int)idx, i, j, k);
-            // the six neighbours, each loaded once; octants in the reference's order
-            const bool vx[2] = {i > 0, i < g.NX - 1}, vy[2] = {j > 0, j < g.NY - 1}, vz[2] = {k > 0, k < g.NZ - 1};
-            const float nx[2] = {vx[0] ? __ldg(in + idx - sI) : 0.f, vx[1] ? __ldg(in + idx + sI) : 0.f};
-            const float ny[2] = {vy[0] ? __ldg(in + idx - sJ) : 0.f, vy[1] ? __ldg(in + idx + sJ) : 0.f};
-            const float nz[2] = {vz[0] ? __ldg(in + idx - 1) : 0.f, vz[1] ? __ldg(in + idx + 1) : 0.f};
-            // An octant with m = min(a,b,c) >= res cannot lower res, and skips the
-            // sqrt and the division. Its result is m + 1 rounded (>= m) when that
-            // is not above the maximum; otherwise ((a+b)+c + sqrt(...)) / 3
-            // rounded, which by monotone rounding is at least fl(fl(3m) / 3) (or
-            // NaN): that is m itself when 3m is exact (fl(3m) - 2m == m, the
-            // subtraction being exact), and at least m - ulp(m) otherwise, so
-            // then m two ulps down must still be >= res. The field is unchanged
-            // bit for bit.
-            #pragma unroll
-            for (int a = 0; a < 2; a++)
-            #pragma unroll
-            for (int b = 0; b < 2; b++)
-            #pragma unroll
-            for (int e = 0; e < 2; e++) {
-                if (!(vx[a] && vy[b] && vz[e])) continue;
-                const float m = fminf(nx[a], fminf(ny[b], nz[e]));
-                if (m >= res) {
-                    const float mx = fmaxf(nx[a], fmaxf(ny[b], nz[e]));
-                    if (!(m + 1 > mx)) continue;
-                    const float t = 3.0f * m;
-                    if (t - 2.0f * m == m) continue;
-                    if (m > 1e-30f && __int_as_float(__float_as_int(m) - 2) >= res) continue;
-                }
-                solvedistance(nx[a], ny[b], nz[e], res);
-            }
-        }
-        out[idx] = res;
+    float res = __ldg(in + idx);
+    if (typeflag >= 0 && __ldg(mark + idx) == typeflag) return res;
+    // the six neighbours, each loaded once; octants in the reference's order
+    const bool vx[2] = {i > 0, i < g.NX - 1}, vy[2] = {j > 0, j < g.NY - 1}, vz[2] = {k > 0, k < g.NZ - 1};
+    const float nx[2] = {vx[0] ? __ldg(in + idx - sI) : 0.f, vx[1] ? __ldg(in + idx + sI) : 0.f};
+    const float ny[2] = {vy[0] ? __ldg(in + idx - sJ) : 0.f, vy[1] ? __ldg(in + idx + sJ) : 0.f};
+    const float nz[2] = {vz[0] ? __ldg(in + idx - 1) : 0.f, vz[1] ? __ldg(in + idx + 1) : 0.f};
+    // Every octant's minimum is one of the six values and at least their
+    // minimum m6. When m6 >= res and each of the six values is settled, every
+    // octant is skipped below, so the pass leaves the cell as it is: an exact
+    // test, not a tolerance (a NaN among the six is never settled and takes
+    // the octant loop). Most cells away from the interface take this exit.
+    if (vx[0] && vx[1] && vy[0] && vy[1] && vz[0] && vz[1]) {
+        const float m6 = fminf(fminf(fminf(nx[0], nx[1]), fminf(ny[0], ny[1])), fminf(nz[0], nz[1]));
+        if (m6 >= res && sweep_settled(nx[0], res) && sweep_settled(nx[1], res) && sweep_settled(ny[0], res) &&
+            sweep_settled(ny[1], res) && sweep_settled(nz[0], res) && sweep_settled(nz[1], res))
+            return res;
     }
+    #pragma unroll
+    for (int a = 0; a < 2; a++)
+    #pragma unroll
+    for (int b = 0; b < 2; b++)
+    #pragma unroll
+    for (int e = 0; e < 2; e++) {
+        if (!(vx[a] && vy[b] && vz[e])) continue;
+        const float m = fminf(nx[a], fminf(ny[b], nz[e]));
+        if (m >= res) {
+            const float mx = fmaxf(nx[a], fmaxf(ny[b], nz[e]));
+            if (!(m + 1 > mx)) continue;
+            if (sweep_settled(m, res)) continue;
+        }
+        solvedistance(nx[a], ny[b], nz[e], res);
+    }
+    return res;
+}
+// A block covers one k-row of cells (blockIdx.z = i, blockIdx.y = j), a thread
+// one cell, or two where the row is longer than the blocks along it, so no
+// thread divides to find its cell.
+constexpr int SWEEP_K = 128;
+inline dim3 sweep_grid(int ni, int nj, int nk) { return dim3(std::max(1, nk / SWEEP_K), nj, ni); }
+__global__ void __launch_bounds__(SWEEP_K) k_sweep(Grid g, const float* __restrict__ in, float* __restrict__ out,
+                                                   const int8_t* __restrict__ mark, int typeflag) {
+    const int j = blockIdx.y, i = blockIdx.z;
+    const int row = (i * g.NY + j) * g.NZ;
+    for (int k = blockIdx.x * SWEEP_K + threadIdx.x; k < g.NZ; k += gridDim.x * SWEEP_K)
+        out[row + k] = sweep_cell(g, in, mark, typeflag, i, j, k, row + k);
 }
 // markLS_bigpositive (mode 0), setLSback_bigpositive (1), preparels (2), setLSback (3)
 __global__ void k_ls_prep(int n, float h, float* __restrict__ ls, int8_t* __restrict__ mark, int mode) {
@@ -264,26 +288,17 @@ __device__ __forceinline__ float sweepu_face(const Grid& g, const float* __restr
     if (AX == 1) return wx * in[fyi(g, i + di, j, k)] + wy * in[fyi(g, i, j + dj, k)] + wz * in[fyi(g, i, j, k + dk)];
     return wx * in[fzi(g, i + di, j, k)] + wy * in[fzi(g, i, j + dj, k)] + wz * in[fzi(g, i, j, k + dk)];
 }
-__global__ void k_sweepu(Grid g, const float* __restrict__ ix, const float* __restrict__ iy, const float* __restrict__ iz,
-                         float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz,
-                         const float* __restrict__ ls, const int8_t* __restrict__ mark, int fl) {
-    long long tot = (long long)g.nfx + g.nfy + g.nfz;
-    MP_GRID_LOOP(t, tot) {
-        int i, j, k;
-        if (t < g.nfx) {
-            int idx = (int)t;
-            getijk3(idx, g.NY, g.NZ, i, j, k);
-            ox[idx] = sweepu_face<0>(g, ix, ls, mark, fl, i, j, k, idx);
-        } else if (t < (long long)g.nfx + g.nfy) {
-            int idx = (int)(t - g.nfx);
-            getijk3(idx, g.NY + 1, g.NZ, i, j, k);
-            oy[idx] = sweepu_face<1>(g, iy, ls, mark, fl, i, j, k, idx);
-        } else {
-            int idx = (int)(t - g.nfx - g.nfy);
-            getijk3(idx, g.NY, g.NZ + 1, i, j, k);
-            oz[idx] = sweepu_face<2>(g, iz, ls, mark, fl, i, j, k, idx);
-        }
-    }
+// one pass over the faces of axis AX, laid out as the cells of k_sweep: a block
+// covers one (i, j) row of faces along k
+template <int AX>
+__global__ void __launch_bounds__(SWEEP_K) k_sweepu(Grid g, const float* __restrict__ in, float* __restrict__ out,
+                                                    const float* __restrict__ ls, const int8_t* __restrict__ mark,
+                                                    int fl) {
+    const int j = blockIdx.y, i = blockIdx.z;
+    const int kn = AX == 2 ? g.NZ + 1 : g.NZ;
+    const int row = AX == 0 ? fxi(g, i, j, 0) : (AX == 1 ? fyi(g, i, j, 0) : fzi(g, i, j, 0));
+    for (int k = blockIdx.x * SWEEP_K + threadIdx.x; k < kn; k += gridDim.x * SWEEP_K)
+        out[row + k] = sweepu_face<AX>(g, in, ls, mark, fl, i, j, k, row + k);
 }
 __device__ __forceinline__ float zrule(const Grid& g, const int8_t* mark, int i, int j, int k, float v) {
     if (k <= 1) return 0.0f;
@@ -395,7 +410,8 @@ __global__ void k_flip_air_vacuum(int n, int8_t* __restrict__ mark) {
 static Cells cells_of(MpCtx* c) { return Cells{c->cell_off, c->tmask}; }
 
 int k_sweep_pass_swap(MpCtx* c, float** phi, int typeflag) {
-    k_sweep<<<mp_blocks(c->G.n, 256), 256, 0, c->stream>>>(c->G, *phi, c->cell_tmp, c->mark, typeflag);
+    const Grid& g = c->G;
+    k_sweep<<<sweep_grid(g.NX, g.NY, g.NZ), SWEEP_K, 0, c->stream>>>(g, *phi, c->cell_tmp, c->mark, typeflag);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     std::swap(*phi, c->cell_tmp);
@@ -463,11 +479,13 @@ int k_sweep_phi(MpCtx* c, int phase) {
 int k_sweep_u(MpCtx* c, int phase) {
     float** u = (phase == MP_TYPEAIR) ? c->au : c->wu;
     const float* phi = (phase == MP_TYPEAIR) ? c->phiair : c->phifluid;
-    long long tot = (long long)c->G.nfx + c->G.nfy + c->G.nfz;
+    const Grid& g = c->G;
     for (int it = 0; it < 2; it++) {
-        k_sweepu<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(c->G, u[0], u[1], u[2], c->tmpu[0], c->tmpu[1], c->tmpu[2],
-                                                             phi, c->mark, phase);
-        c->launches++;
+        // the three face sets are independent: each reads only its own input
+        k_sweepu<0><<<sweep_grid(g.NX + 1, g.NY, g.NZ), SWEEP_K, 0, c->stream>>>(g, u[0], c->tmpu[0], phi, c->mark, phase);
+        k_sweepu<1><<<sweep_grid(g.NX, g.NY + 1, g.NZ), SWEEP_K, 0, c->stream>>>(g, u[1], c->tmpu[1], phi, c->mark, phase);
+        k_sweepu<2><<<sweep_grid(g.NX, g.NY, g.NZ + 1), SWEEP_K, 0, c->stream>>>(g, u[2], c->tmpu[2], phi, c->mark, phase);
+        c->launches += 3;
         MP_CHECK_LAUNCH(c);
         for (int a = 0; a < 3; a++) std::swap(u[a], c->tmpu[a]);
     }
