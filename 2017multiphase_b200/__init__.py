@@ -167,6 +167,7 @@ def load_library() -> C.CDLL:
         "mp_adj_record": ([vp, C.c_int, C.c_int], C.c_int),
         "mp_adj_set_targets": ([vp, vp, C.c_int], C.c_int),
         "mp_adj_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+        "mp_adj_order": ([vp, vp], C.c_int),
         "mp_adj_loss": ([vp, C.c_int, vp, C.POINTER(C.c_double)], C.c_int),
         "mp_adj_gradient": ([vp, C.c_int, vp, vp, C.POINTER(C.c_double)], C.c_int),
         "mp_adj_release": ([vp], C.c_int),
@@ -593,6 +594,17 @@ class Sim:
         n = C.c_int(); k = C.c_int()
         _check(self.lib.mp_adj_info(self.ctx, C.byref(n), C.byref(k)), self.ctx)
         return n.value
+
+    def adj_order(self):
+        """Recording index of the particle in each slot of the context now
+        (mp_adj_order), as a CUDA int64 tensor: the engine's particles after
+        the recording, reordered by it, line up with the replay's final state."""
+        import torch
+        n = self.adj_num_particles()
+        ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{torch.cuda.current_device()}")
+        torch.cuda.synchronize()
+        _check(self.lib.mp_adj_order(self.ctx, C.c_void_p(ids.data_ptr())), self.ctx)
+        return ids.to(torch.int64)
 
     def adj_loss(self, v0=None, precision: int = PREC_MIXED) -> float:
         """Loss of the recorded program from initial velocities v0 (a CUDA

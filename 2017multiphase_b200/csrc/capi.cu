@@ -452,7 +452,7 @@ extern "C" int mp_set_tables(void* ctx, const float* randfloat, int nrand, const
 }
 
 // ---------------------------------------------------------------------------
-// adjoint of the FLUID-only step (k_adjoint.cu)
+// adjoint of the FLUID and AIR step (k_adjoint.cu)
 // ---------------------------------------------------------------------------
 extern "C" int mp_adj_record(void* ctx, int nsteps, int checkpoint_every) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_adj_record(c, nsteps, checkpoint_every);
@@ -462,6 +462,11 @@ extern "C" int mp_adj_set_targets(void* ctx, const float* samples3, int nsamples
 }
 extern "C" int mp_adj_info(void* ctx, int* np, int* nsteps) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c); return k_adj_np(c, np, nsteps);
+}
+extern "C" int mp_adj_order(void* ctx, uint32_t* ids) {
+    MpCtx* c = C(ctx); CTX_OR_ARG(c);
+    if (!ids) return MP_ERR_ARG;
+    return k_adj_order(c, ids);
 }
 extern "C" int mp_adj_loss(void* ctx, int precision, const double* v0, double* loss) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);

@@ -213,6 +213,7 @@ int k_adj_record(MpCtx* c, int nsteps, int every);
 int k_adj_set_targets(MpCtx* c, const float* samples3, int nsamples);
 int k_adj_run(MpCtx* c, int precision, const double* v0, double* grad, double* loss);
 int k_adj_np(MpCtx* c, int* np, int* nsteps);
+int k_adj_order(MpCtx* c, uint32_t* ids);
 int k_heat_cg_solve(MpCtx* c, const int8_t* mark, float* x, const float* b, int maxiter, int tolmode, float tol,
                     int* iters, double* res);
 int k_heat_cg_solve(MpCtx* c, const int8_t* mark, double* x, const double* b, int maxiter, int tolmode, float tol,

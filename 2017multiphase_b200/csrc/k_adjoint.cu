@@ -1,16 +1,20 @@
-// k_adjoint.cu — reverse-mode derivative of the water-only dam-break step.
+// k_adjoint.cu — reverse-mode derivative of the FLUID (and AIR) step.
 //
 // The reference has no differentiation. This module differentiates the
 // program the bubblesim step (spray.cpp:979-1233) runs for a scene of FLUID
-// particles only, with the position corrections off:
-//   gravity (addgravityforce_k, spray_k.cu:330)
-//   -> velocity splat to faces (mapvelp2g_k_fluidSolid, spray_k.cu:2809-2866)
+// particles, or of FLUID and AIR particles, with the position corrections and
+// the solo-air stages off:
+//   external forces (addexternalforce: gravity on FLUID, the buoyancy of AIR)
+//   -> velocity splats to faces (mapvelp2g_k_fluidSolid, spray_k.cu:2809-2866,
+//      and mapvelp2g_k_air, spray_k.cu:2894-2937)
 //   -> extrapolation, two Jacobi passes (sweepu_k_bubble, spray_k.cu:3779-3880)
 //   -> wall rules (setWaterBoundaryU_k, spray_k.cu:956-995)
-//   -> projection (cptdivergence_bubble2 + solver_cg_bubble + subGradPress)
+//   -> projection (cptdivergence_bubble2 with the level-set blend at
+//      liquid-air faces, solver_cg_bubble, subGradPress on both fields)
 //   -> extrapolation + wall rules again
-//   -> FLIP/PIC gather (mapvelg2p_flip_bubble, spray_k.cu:3525-3540, blended
-//      with the new grid velocity by flip_alpha as spray_k.cu:3487-3490)
+//   -> FLIP/PIC gather of each phase's field (mapvelg2p_flip_bubble,
+//      spray_k.cu:3525-3540, blended with the new grid velocity by flip_alpha
+//      as spray_k.cu:3487-3490)
 //   -> advection with the wall clamp (CollisionWithSolid_k, spray_k.cu:5276)
 // and, after the last step, the loss sum_s phi(y_s)^2 of the fluid distance
 // field (genlevelset, spray_k.cu:2753-2806) at target points y_s.
@@ -28,7 +32,10 @@
 // particles over nearby faces, cells over nearby samples), so gradients are
 // deterministic. The projection's transpose is a second CG solve on the
 // symmetric pressure matrix. States are checkpointed every `every` steps and
-// recomputed segment by segment during the reverse sweep.
+// recomputed segment by segment during the reverse sweep; each step's
+// intermediates are recomputed from its state just before its transpose, so
+// only one step's are held (the pressure and heat solves of the first replay
+// are kept per step, so the recomputations solve nothing).
 #include "ctx.cuh"
 #include <algorithm>
 #include <cstring>
@@ -58,6 +65,16 @@ struct AdjTape {
     std::vector<int8_t*> mark_h;
     float* T0 = nullptr;                 // initial temperatures (id order)
     float* fixedheat = nullptr;          // the fixed-heat field (b_fixed_heat), or null
+    // the air phase (AIR particles present): each particle's phase (0 FLUID,
+    // 1 AIR; fixed, the program has no AIR <-> AIRSOLO transitions), the splat
+    // masses of each phase (0 for the other phase's particles), and per step
+    // the merged level set (the divergence's blend) and the air extrapolation
+    // distance
+    bool air = false;
+    uint8_t* phase = nullptr;
+    float* mass_w = nullptr;
+    float* mass_a = nullptr;
+    std::vector<float*> lsm, phia;
     // replay / adjoint work, sized for `wesz`-byte elements
     size_t wesz = 0;
     int wk_ns = 0;                       // samples the work was sized for
@@ -105,8 +122,26 @@ __global__ void k_ad_snapshot_T(int n, const uint32_t* __restrict__ ids, const f
                                 float* __restrict__ T) {
     MP_GRID_LOOP(s, n) T[ids[s]] = heat[s].x;
 }
-__global__ void k_ad_count_nonfluid(int n, const float4* __restrict__ pos, uint32_t* cnt) {
-    MP_GRID_LOOP(s, n) if (pflag(pos[s]) != MP_TYPEFLUID) atomicAdd(cnt, 1u);
+// counts the particles that are neither FLUID nor AIR (cnt[0]) and the AIR ones (cnt[2])
+__global__ void k_ad_count_types(int n, const float4* __restrict__ pos, uint32_t* cnt) {
+    MP_GRID_LOOP(s, n) {
+        const int f = pflag(pos[s]);
+        if (f != MP_TYPEFLUID && f != MP_TYPEAIR) atomicAdd(cnt, 1u);
+        else if (f == MP_TYPEAIR) atomicAdd(cnt + 2, 1u);
+    }
+}
+// each particle's phase and per-phase splat mass
+__global__ void k_ad_snapshot_phase(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ pos,
+                                    const float4* __restrict__ vel, uint8_t* __restrict__ phase,
+                                    float* __restrict__ mw, float* __restrict__ ma) {
+    MP_GRID_LOOP(s, n) {
+        const uint32_t id = ids[s];
+        const bool air = pflag(pos[s]) == MP_TYPEAIR;
+        const float m = vel[s].w;
+        phase[id] = air ? 1 : 0;
+        mw[id] = air ? 0.0f : m;
+        ma[id] = air ? m : 0.0f;
+    }
 }
 // nearest FLUID particle of each cell centre within the genlevelset window
 // (2.5 cells; the +-2 cell box in a fixed order, first minimum kept)
@@ -142,6 +177,34 @@ __global__ void k_ad_gravity(int np, const T* __restrict__ v, T* __restrict__ va
         va[3 * p + 2] = v[3 * p + 2] + dtg;
     }
 }
+// addexternalforce for FLUID and AIR particles (k_forces): FLUID v += dt g; AIR
+// v_z -= dt g_z rate bra with rate = max(vmax - v_z, 0) / vmax
+template <class T>
+__global__ void k_ad_forces(int np, const uint8_t* __restrict__ phase, const T* __restrict__ v, T* __restrict__ va,
+                            T dtg, T bra, T vmax) {
+    MP_GRID_LOOP(p, np) {
+        va[3 * p] = v[3 * p]; va[3 * p + 1] = v[3 * p + 1];
+        T vz = v[3 * p + 2];
+        if (phase[p] == 0) vz = vz + dtg;
+        else {
+            T r = vmax - vz;
+            r = r > (T)0 ? r : (T)0;
+            vz = vz - dtg * (r / vmax) * bra;
+        }
+        va[3 * p + 2] = vz;
+    }
+}
+// its transpose, in place on the velocity cotangent (v the step's input)
+template <class T>
+__global__ void k_ad_forces_adj(int np, const uint8_t* __restrict__ phase, const T* __restrict__ v,
+                                const T* __restrict__ vab, T* __restrict__ vb, T dtg, T bra, T vmax) {
+    MP_GRID_LOOP(p, np) {
+        vb[3 * p] = vab[3 * p]; vb[3 * p + 1] = vab[3 * p + 1];
+        T d = (T)1;
+        if (phase[p] != 0 && vmax - v[3 * p + 2] > (T)0) d = (T)1 + dtg * bra / vmax;
+        vb[3 * p + 2] = d * vab[3 * p + 2];
+    }
+}
 template <class T> __device__ __forceinline__ T sharpk(T r2) {
     const T c = (T)1.4f * (T)1.4f;
     T rr = r2 > (T)0.0001f ? r2 : (T)0.0001f;
@@ -161,21 +224,40 @@ __device__ __forceinline__ void face_pos(int ax, int i, int j, int k, float& gx,
     gy = (float)j + (ax == 1 ? 0.0f : 0.5f);
     gz = (float)k + (ax == 2 ? 0.0f : 0.5f);
 }
+// cells holding an AIR particle in a step's recorded order (the air splat and
+// the air faces' gather skip the others, as the engine's air splat skips cells
+// by their type mask)
+__global__ void k_ad_air_cells(int n, const uint32_t* __restrict__ off, const uint32_t* __restrict__ order,
+                               const uint8_t* __restrict__ phase, uint8_t* __restrict__ airc) {
+    MP_GRID_LOOP(c, n) {
+        uint8_t a = 0;
+        for (uint32_t q = off[c]; q < off[c + 1]; q++)
+            if (phase[order[q]]) { a = 1; break; }
+        airc[c] = a;
+    }
+}
+// the splat windows: a face e along its normal takes the cells [e-LO, e+HI],
+// across [-AC, AC]: the water splat (mapvelp2g_k_fluidSolid) [-1, 0] and
+// [-1, 1], the air splat (mapvelp2g_k_air) [-2, 1] and [-2, 2]
+template <int PH> struct SplatWin {
+    static constexpr int LO = PH ? 2 : 1, HI = PH ? 1 : 0, AC = PH ? 2 : 1;
+};
 // splat: per face, the mass-weighted sharp-kernel average of the particles of
-// the cells [i-1,i] along the face normal and [-1,1] across (the order of
-// mapvelp2g_k_fluidSolid's loops)
-template <class T>
+// its window's cells, in the order of the reference's loops; the records hold
+// each particle's phase mass (0 for the other phase, which then adds nothing)
+template <class T, int PH>
 __global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4, const T* __restrict__ vs4,
-                         Fc<T> u, Fc<T> W) {
+                         Fc<T> u, Fc<T> W, const uint8_t* __restrict__ cellmask) {
+    using Wn = SplatWin<PH>;
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
     const T scale = (T)1 / (T)g.h;
     MP_GRID_LOOP(t, tot) {
         int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
         float fx, fy, fz; face_pos(ax, i, j, k, fx, fy, fz);
         T w = 0, s = 0;
-        const int a0 = ax == 0 ? i - 1 : i - 1, a1 = ax == 0 ? i : i + 1;
-        const int b0 = j - 1, b1 = ax == 1 ? j : j + 1;
-        const int c0 = k - 1, c1 = ax == 2 ? k : k + 1;
+        const int a0 = i - (ax == 0 ? Wn::LO : Wn::AC), a1 = i + (ax == 0 ? Wn::HI : Wn::AC);
+        const int b0 = j - (ax == 1 ? Wn::LO : Wn::AC), b1 = j + (ax == 1 ? Wn::HI : Wn::AC);
+        const int c0 = k - (ax == 2 ? Wn::LO : Wn::AC), c1 = k + (ax == 2 ? Wn::HI : Wn::AC);
         for (int a = a0; a <= a1; a++) {
             if (a < 0 || a > g.NX - 1) continue;
             for (int b = b0; b <= b1; b++) {
@@ -183,8 +265,10 @@ __global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ off, const T* __re
                 for (int cc = c0; cc <= c1; cc++) {
                     if (cc < 0 || cc > g.NZ - 1) continue;
                     int c = cid(g, a, b, cc);
+                    if (cellmask && !cellmask[c]) continue;
                     for (uint32_t q = off[c]; q < off[c + 1]; q++) {
                         const T* r = xs4 + 4 * (size_t)q;
+                        if (r[3] == (T)0) continue;   // adds +0 to both sums
                         T dx = r[0] * scale - (T)fx, dy = r[1] * scale - (T)fy, dz = r[2] * scale - (T)fz;
                         T r2 = dx * dx + dy * dy + dz * dz;
                         T wp = r[3] * sharpk(r2);
@@ -209,6 +293,17 @@ __global__ void k_ad_slot_gather(int np, const uint32_t* __restrict__ order, con
         oa[4 * (size_t)s + 3] = mass ? (T)mass[p] : (T)0;
         ob[4 * (size_t)s] = b[3 * p]; ob[4 * (size_t)s + 1] = b[3 * p + 1]; ob[4 * (size_t)s + 2] = b[3 * p + 2];
         ob[4 * (size_t)s + 3] = (T)0;
+    }
+}
+// per-slot records (b xyz, 0) of one phase's particles, zero for the other's
+template <class T>
+__global__ void k_ad_slot_gather_ph(int np, const uint32_t* __restrict__ order, const T* __restrict__ b,
+                                    const uint8_t* __restrict__ phase, int want, T* __restrict__ ob) {
+    MP_GRID_LOOP(s, np) {
+        const uint32_t p = order[s];
+        const bool on = phase[p] == want;
+        ob[4 * (size_t)s] = on ? b[3 * p] : (T)0; ob[4 * (size_t)s + 1] = on ? b[3 * p + 1] : (T)0;
+        ob[4 * (size_t)s + 2] = on ? b[3 * p + 2] : (T)0; ob[4 * (size_t)s + 3] = (T)0;
     }
 }
 template <class T> __global__ void k_ad_copy(long long n, const T* __restrict__ a, T* __restrict__ b) {
@@ -457,6 +552,100 @@ __global__ void k_ad_divT(Grid g, const T* __restrict__ q, Fc<T> ubi, Fc<T> ubo)
         fsel(ubo, ax)[idx] = acc;
     }
 }
+// The two-phase divergence (cptdivergence_bubble2, spray_k.cu:3138-3263): an
+// unknown cell of type m reads across each face the value of its own phase,
+// or, where the neighbour is of the other phase, the blend with theta =
+// -l_c / (l_n - l_c) of the merged level set: theta of its own phase's face
+// velocity and 1 - theta of the other's. blend_coef gives the weights (cw, ca)
+// of the water and air velocities of the face.
+template <class T>
+__device__ __forceinline__ void blend_coef(int m, int mn, T lc, T ln, T& cw, T& ca) {
+    if (m == MP_TYPEFLUID && mn != MP_TYPEAIR) { cw = (T)1; ca = (T)0; return; }
+    if (m == MP_TYPEAIR && mn != MP_TYPEFLUID) { cw = (T)0; ca = (T)1; return; }
+    const T th = ((T)0 - lc) / (ln - lc);
+    if (m == MP_TYPEFLUID) { cw = th; ca = (T)1 - th; }
+    else { cw = (T)1 - th; ca = th; }
+}
+template <class T>
+__device__ __forceinline__ T blend_face(const Grid& g, const int8_t* mark, const float* ls, int m, T lc, int q, T wv,
+                                        T av) {
+    const int mn = mark[q];
+    if (m == MP_TYPEFLUID && mn != MP_TYPEAIR) return wv;
+    if (m == MP_TYPEAIR && mn != MP_TYPEFLUID) return av;
+    const T th = ((T)0 - lc) / ((T)ls[q] - lc);
+    if (m == MP_TYPEFLUID) return th * wv + ((T)1 - th) * av;
+    return th * av + ((T)1 - th) * wv;
+}
+template <class T>
+__global__ void k_ad_div2(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ ls, Fc<T> uw, Fc<T> ua,
+                          T* __restrict__ b) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        T out = 0;
+        if (unknown(g, mark, idx, i, j, k)) {
+            const int m = mark[idx];
+            const T lc = (T)ls[idx];
+            int f;
+            f = fxi(g, i + 1, j, k); T x1 = blend_face<T>(g, mark, ls, m, lc, cid(g, i + 1, j, k), uw.x[f], ua.x[f]);
+            f = fxi(g, i, j, k);     T x0 = blend_face<T>(g, mark, ls, m, lc, cid(g, i - 1, j, k), uw.x[f], ua.x[f]);
+            f = fyi(g, i, j + 1, k); T y1 = blend_face<T>(g, mark, ls, m, lc, cid(g, i, j + 1, k), uw.y[f], ua.y[f]);
+            f = fyi(g, i, j, k);     T y0 = blend_face<T>(g, mark, ls, m, lc, cid(g, i, j - 1, k), uw.y[f], ua.y[f]);
+            f = fzi(g, i, j, k + 1); T z1 = blend_face<T>(g, mark, ls, m, lc, cid(g, i, j, k + 1), uw.z[f], ua.z[f]);
+            f = fzi(g, i, j, k);     T z0 = blend_face<T>(g, mark, ls, m, lc, cid(g, i, j, k - 1), uw.z[f], ua.z[f]);
+            out = (x1 - x0 + y1 - y0 + z1 - z0) / (T)g.h;
+        }
+        b[idx] = out;
+    }
+}
+// pbar = -G^T (ub_w + ub_a) on the unknown cells: both face fields take the
+// same pressure gradient
+template <class T>
+__global__ void k_ad_pbar2(Grid g, const int8_t* __restrict__ mark, Fc<T> uw, Fc<T> ua, T* __restrict__ pb) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        T out = 0;
+        if (unknown(g, mark, idx, i, j, k)) {
+            const int x1 = fxi(g, i + 1, j, k), x0 = fxi(g, i, j, k), y1 = fyi(g, i, j + 1, k), y0 = fyi(g, i, j, k);
+            const int z1 = fzi(g, i, j, k + 1), z0 = fzi(g, i, j, k);
+            out = ((uw.x[x1] + ua.x[x1]) - (uw.x[x0] + ua.x[x0]) + (uw.y[y1] + ua.y[y1]) - (uw.y[y0] + ua.y[y0]) +
+                   (uw.z[z1] + ua.z[z1]) - (uw.z[z0] + ua.z[z0])) / (T)g.h;
+        }
+        pb[idx] = out;
+    }
+}
+// the two-phase divergence's transpose: (ubw, uba)_out = (ubw, uba)_in + D^T q.
+// A face is the upper face of the cell below it (+1/h there) and the lower
+// face of the cell above it (-1/h), each weighted by that cell's blend
+// weights toward the other
+template <class T>
+__global__ void k_ad_divT2(Grid g, const int8_t* __restrict__ mark, const float* __restrict__ ls,
+                           const T* __restrict__ q, Fc<T> wi, Fc<T> ai, Fc<T> wo, Fc<T> ao) {
+    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
+    MP_GRID_LOOP(t, tot) {
+        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
+        int e = ax == 0 ? i : (ax == 1 ? j : k), n = ax == 0 ? g.NX : (ax == 1 ? g.NY : g.NZ);
+        T aw = fsel(wi, ax)[idx], aa = fsel(ai, ax)[idx];
+        const int lo_i = i - (ax == 0), lo_j = j - (ax == 1), lo_k = k - (ax == 2);
+        T sw = 0, sa = 0;
+        if (e > 0) {
+            const int c = cid(g, lo_i, lo_j, lo_k);
+            if (unknown(g, mark, c, lo_i, lo_j, lo_k) && e < n) {
+                T cw, ca; blend_coef<T>(mark[c], mark[cid(g, i, j, k)], (T)ls[c], (T)ls[cid(g, i, j, k)], cw, ca);
+                sw += cw * q[c]; sa += ca * q[c];
+            }
+        }
+        if (e < n) {
+            const int c = cid(g, i, j, k);
+            if (unknown(g, mark, c, i, j, k) && e > 0) {
+                T cw, ca; blend_coef<T>(mark[c], mark[cid(g, lo_i, lo_j, lo_k)], (T)ls[c], (T)ls[cid(g, lo_i, lo_j, lo_k)],
+                                        cw, ca);
+                sw -= cw * q[c]; sa -= ca * q[c];
+            }
+        }
+        fsel(wo, ax)[idx] = aw + sw / (T)g.h;
+        fsel(ao, ax)[idx] = aa + sa / (T)g.h;
+    }
+}
 // trilinear of the face/cell grids (the engine's trilinear) with its gradient
 // in grid units
 template <class T>
@@ -485,11 +674,15 @@ __device__ __forceinline__ T tri(const T* u, T x, T y, T z, int w, int hh, int d
 template <class T> __device__ __forceinline__ void ipos(int ax, T X, T Y, T Z, T& x, T& y, T& z) {
     x = ax == 0 ? X : X - (T)0.5f; y = ax == 1 ? Y : Y - (T)0.5f; z = ax == 2 ? Z : Z - (T)0.5f;
 }
+// mapvelg2p_flip_bubble: each particle reads its own phase's fields (with
+// `phase` null every particle is FLUID)
 template <class T>
-__global__ void k_ad_g2p(Grid g, int np, const T* __restrict__ x, const T* __restrict__ va, Fc<T> uf, Fc<T> du,
-                         T alpha, T* __restrict__ vg) {
+__global__ void k_ad_g2p(Grid g, int np, const T* __restrict__ x, const T* __restrict__ va, Fc<T> ufw, Fc<T> duw,
+                         T alpha, T* __restrict__ vg, const uint8_t* __restrict__ phase, Fc<T> ufa, Fc<T> dua) {
     MP_GRID_LOOP(p, np) {
         T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
+        const bool air = phase && phase[p];
+        const Fc<T> uf = air ? ufa : ufw, du = air ? dua : duw;
         for (int ax = 0; ax < 3; ax++) {
             const int w = ax == 0 ? g.NX + 1 : g.NX, hh = ax == 1 ? g.NY + 1 : g.NY, d = ax == 2 ? g.NZ + 1 : g.NZ;
             T a, b, c; ipos(ax, X, Y, Z, a, b, c);
@@ -632,11 +825,14 @@ __global__ void k_ad_advect_adj(Grid g, int np, const T* __restrict__ x, const T
 // gather part of the particle side of the G2P transpose: vabar and the
 // position derivative of the interpolation
 template <class T>
-__global__ void k_ad_g2p_adj_p(Grid g, int np, const uint32_t* __restrict__ order, const T* __restrict__ x, Fc<T> uf,
-                               Fc<T> du, T alpha, const T* __restrict__ vgb, T* __restrict__ vab, T* __restrict__ xb) {
+__global__ void k_ad_g2p_adj_p(Grid g, int np, const uint32_t* __restrict__ order, const T* __restrict__ x, Fc<T> ufw,
+                               Fc<T> duw, T alpha, const T* __restrict__ vgb, T* __restrict__ vab, T* __restrict__ xb,
+                               const uint8_t* __restrict__ phase, Fc<T> ufa, Fc<T> dua) {
     // particles in sorted order, so neighbouring threads read neighbouring faces
     MP_GRID_LOOP(sl, np) {
         const uint32_t p = order[sl];
+        const bool air = phase && phase[p];
+        const Fc<T> uf = air ? ufa : ufw, du = air ? dua : duw;
         const T ih = (T)1 / (T)g.h;
         T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
         const T cdu = alpha == (T)1 ? (T)1 : alpha, cu = alpha == (T)1 ? (T)0 : (T)1 - alpha;
@@ -662,7 +858,7 @@ __global__ void k_ad_g2p_adj_p(Grid g, int np, const uint32_t* __restrict__ orde
 // decided from the replay's own positions either way.
 template <class T, bool WIDE>
 __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4,
-                               const T* __restrict__ vgs4, Fc<T> q) {
+                               const T* __restrict__ vgs4, Fc<T> q, const uint8_t* __restrict__ cellmask) {
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
     MP_GRID_LOOP(t, tot) {
         int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
@@ -678,6 +874,7 @@ __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ off, const T
                 for (int cc = c0; cc <= c1; cc++) {
                     if (cc < 0 || cc > g.NZ - 1) continue;
                     int c = cid(g, a, b, cc);
+                    if (cellmask && !cellmask[c]) continue;
                     for (uint32_t s = off[c]; s < off[c + 1]; s++) {
                         const T* r = xs4 + 4 * (size_t)s;
                         T X = r[0] / (T)g.h, Y = r[1] / (T)g.h, Z = r[2] / (T)g.h;
@@ -702,7 +899,7 @@ __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ off, const T
 }
 // splat transpose per particle over the faces whose window holds its cell
 // (the particle's cell is the recorded one: window membership is frozen)
-template <class T>
+template <class T, int PH>
 __global__ void k_ad_p2g_adj(Grid g, int np, const uint32_t* __restrict__ order, const T* __restrict__ x,
                              const T* __restrict__ va, const float* __restrict__ mass,
                              const uint32_t* __restrict__ cellof, Fc<T> u, Fc<T> W, Fc<T> ub, T* __restrict__ vab,
@@ -715,13 +912,16 @@ __global__ void k_ad_p2g_adj(Grid g, int np, const uint32_t* __restrict__ order,
         int ca, cb, cc;
         getijk3((int)cellof[p], g.NY, g.NZ, ca, cb, cc);
         const T m = (T)mass[p];
+        if (m == (T)0) continue;   // the other phase's particle: not in this splat
+        using Wn = SplatWin<PH>;
         T vb[3] = {0, 0, 0}, gxs = 0, gys = 0, gzs = 0;
         for (int ax = 0; ax < 3; ax++) {
             const int W_ = ax == 0 ? g.NX + 1 : g.NX, H_ = ax == 1 ? g.NY + 1 : g.NY, D_ = ax == 2 ? g.NZ + 1 : g.NZ;
-            const int i0 = ca, i1 = ax == 0 ? ca + 1 : ca + 1, j0 = cb - (ax == 1 ? 0 : 1), j1 = cb + 1;
-            const int k0 = cc - (ax == 2 ? 0 : 1), k1 = cc + 1;
-            // x-face window: cells [i-1,i] -> faces i in [a, a+1]; across: [-1,1] -> faces [b-1, b+1]
-            const int fi0 = ax == 0 ? i0 : ca - 1, fi1 = ax == 0 ? i1 : ca + 1;
+            // a face e whose window along the normal holds cell c, e-LO <= c <= e+HI,
+            // lies in [c-HI, c+LO]; across, in [c-AC, c+AC]
+            const int fi0 = ca - (ax == 0 ? Wn::HI : Wn::AC), fi1 = ca + (ax == 0 ? Wn::LO : Wn::AC);
+            const int j0 = cb - (ax == 1 ? Wn::HI : Wn::AC), j1 = cb + (ax == 1 ? Wn::LO : Wn::AC);
+            const int k0 = cc - (ax == 2 ? Wn::HI : Wn::AC), k1 = cc + (ax == 2 ? Wn::LO : Wn::AC);
             const T pv = va[3 * p + ax];
             for (int fi = fi0; fi <= fi1; fi++) {
                 if (fi < 0 || fi >= W_) continue;
@@ -1012,8 +1212,11 @@ void k_adj_free(MpCtx* c) {
     for (auto* p : t->order_h) cudaFree(p);
     for (auto* p : t->off_h) cudaFree(p);
     for (auto* p : t->mark_h) cudaFree(p);
+    for (auto* p : t->lsm) cudaFree(p);
+    for (auto* p : t->phia) cudaFree(p);
     for (void* p : {(void*)t->x0, (void*)t->v0, (void*)t->mass, (void*)t->ids, (void*)t->ids2, (void*)t->nearest,
-                    (void*)t->samples, (void*)t->s_off, (void*)t->T0, (void*)t->fixedheat})
+                    (void*)t->samples, (void*)t->s_off, (void*)t->T0, (void*)t->fixedheat, (void*)t->phase,
+                    (void*)t->mass_w, (void*)t->mass_a})
         if (p) cudaFree(p);
     for (void* p : t->wk) if (p) cudaFree(p);
     delete t;
@@ -1046,7 +1249,7 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     const mp_params& P = c->P;
     if (nsteps < 1 || every < 1) { c->err = "adj_record: nsteps and checkpoint interval must be positive"; return MP_ERR_ARG; }
     if (P.b_correct_position || P.b_gen_gas || P.b_melt || P.b_freeze || P.b_solid) {
-        c->err = "adj_record: the adjoint covers the FLUID-only step without position correction, gas, "
+        c->err = "adj_record: the adjoint covers the FLUID and AIR step without position correction, gas, "
                  "melting, freezing or solids";
         return MP_ERR_STATE;
     }
@@ -1060,12 +1263,16 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     }
     const int np = c->np();
     if (np == 0) { c->err = "adj_record: no particles"; return MP_ERR_STATE; }
-    MP_CUDA(c, cudaMemsetAsync(c->u32_scratch + 3, 0, sizeof(uint32_t), c->stream));
-    k_ad_count_nonfluid<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, c->pos, c->u32_scratch + 3);
-    uint32_t nonfluid = 0;
-    MP_CUDA(c, cudaMemcpyAsync(&nonfluid, c->u32_scratch + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    MP_CUDA(c, cudaMemsetAsync(c->u32_scratch + 3, 0, 3 * sizeof(uint32_t), c->stream));
+    k_ad_count_types<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, c->pos, c->u32_scratch + 3);
+    uint32_t cnt[3] = {0, 0, 0};
+    MP_CUDA(c, cudaMemcpyAsync(cnt, c->u32_scratch + 3, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (nonfluid) { c->err = "adj_record: every particle must be FLUID"; return MP_ERR_STATE; }
+    if (cnt[0]) { c->err = "adj_record: every particle must be FLUID or AIR"; return MP_ERR_STATE; }
+    if (cnt[2] && P.b_heat_trans) {
+        c->err = "adj_record: the heat stage is differentiated for FLUID particles only (no AIR)";
+        return MP_ERR_STATE;
+    }
     k_adj_free(c);
     AdjTape* t = new AdjTape();
     c->adj = t;
@@ -1077,6 +1284,13 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     k_ad_iota<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids);
     k_ad_snapshot<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->pos, c->vel, t->x0, t->v0, t->mass);
     ADJ_LAUNCH(c);
+    t->air = cnt[2] != 0;
+    if (t->air) {
+        MP_TRY(amalloc(c, &t->phase, np)); MP_TRY(amalloc(c, &t->mass_w, np)); MP_TRY(amalloc(c, &t->mass_a, np));
+        k_ad_snapshot_phase<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->pos, c->vel, t->phase,
+                                                                       t->mass_w, t->mass_a);
+        ADJ_LAUNCH(c);
+    }
     t->heat = P.b_heat_trans != 0;
     if (t->heat) {
         MP_TRY(amalloc(c, &t->T0, np));
@@ -1101,12 +1315,27 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
         MP_CUDA(c, cudaMemcpyAsync(off, c->cell_off, sizeof(uint32_t) * ((size_t)g.n + 1), cudaMemcpyDeviceToDevice, c->stream));
         MP_CUDA(c, cudaMemcpyAsync(mk, c->mark, g.n, cudaMemcpyDeviceToDevice, c->stream));
         MP_TRY(k_p2g(c));
+        if (t->air) {
+            // bubblesim's order: the air phase's extrapolation first
+            float* lm; float* pa;
+            MP_TRY(amalloc(c, &lm, g.n)); t->lsm.push_back(lm);
+            MP_TRY(amalloc(c, &pa, g.n)); t->phia.push_back(pa);
+            MP_CUDA(c, cudaMemcpyAsync(lm, c->lsmerge, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, c->stream));
+            MP_TRY(k_sweep_phi(c, MP_TYPEAIR));
+            MP_CUDA(c, cudaMemcpyAsync(pa, c->phiair, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, c->stream));
+            MP_TRY(k_sweep_u(c, MP_TYPEAIR));
+        }
         MP_TRY(k_sweep_phi(c, MP_TYPEFLUID));
         MP_CUDA(c, cudaMemcpyAsync(ph, c->phifluid, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, c->stream));
-        MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+        MP_TRY(k_sweep_u(c, MP_TYPEFLUID));
+        if (t->air) MP_TRY(k_set_boundary_u(c, MP_TYPEAIR));
+        MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
         int st = k_project(c, nullptr, nullptr);
         if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
-        MP_TRY(k_sweep_u(c, MP_TYPEFLUID)); MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
+        if (t->air) MP_TRY(k_sweep_u(c, MP_TYPEAIR));
+        MP_TRY(k_sweep_u(c, MP_TYPEFLUID));
+        if (t->air) MP_TRY(k_set_boundary_u(c, MP_TYPEAIR));
+        MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
         MP_TRY(k_g2p(c));
         MP_TRY(sorted_ids(c, t));
         MP_TRY(k_collide_advect(c, true));
@@ -1166,8 +1395,7 @@ int k_adj_set_targets(MpCtx* c, const float* sp, int ns) {
 
 namespace {
 // work layout: element counts per buffer; W_I* hold one step's intermediates
-// per slot (`every` slots: a segment's steps are replayed into them and then
-// reversed without recomputation)
+// (each step is replayed again just before its transpose)
 enum {
     W_XS, W_VS, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
     W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2,
@@ -1177,7 +1405,12 @@ enum {
     // intermediates (cell temperature and weight, extended solution, change;
     // particle temperature before the clamp), scratch, cached solves
     W_T, W_TN, W_TS, W_TB, W_HT1, W_HTC, W_HWC, W_HTE, W_HDT, W_HB, W_HBB, W_HQ, W_HQ1, W_HTEB, W_HTCB, W_HST,
-    W_HS4, W_HCELLOF, W_COUNT
+    W_HS4, W_HCELLOF,
+    // the air phase: its splat's old field, projected field and scratch, its
+    // splat records, and its per-slot intermediates (splat, weights,
+    // extrapolated, final, change; extrapolation choices)
+    W_UOLDA, W_UPROJA, W_A0, W_A1, W_A2, W_S4C, W_IUPA, W_IWTA, W_IUEA, W_IUFA, W_IDUA, W_ISELA, W_ISWA, W_AIRC,
+    W_COUNT
 };
 }
 
@@ -1185,6 +1418,7 @@ enum {
 template <class T> struct Inter {
     T* va; T* vg; Fc<T> up, wt, ue, uf, du; uint8_t* sel; float* sw;
     T* Tc; T* Wc; T* Te; T* dT; T* T1;   // heat stage (when recorded)
+    Fc<T> upa, wta, uea, ufa, dua; uint8_t* sela; float* swa;   // air phase (when recorded)
 };
 
 template <class T> struct Replay {
@@ -1205,6 +1439,12 @@ template <class T> struct Replay {
         const size_t n = t->heat ? (size_t)g.n : 0, npp = t->heat ? (size_t)np : 0;
         I.Tc = a(W_HTC) + j * n; I.Wc = a(W_HWC) + j * n; I.Te = a(W_HTE) + j * n; I.dT = a(W_HDT) + j * n;
         I.T1 = a(W_HT1) + j * npp;
+        const size_t nfa = t->air ? nfs : 0;
+        I.upa = faces_of<T>(a(W_IUPA) + j * nfa, g); I.wta = faces_of<T>(a(W_IWTA) + j * nfa, g);
+        I.uea = faces_of<T>(a(W_IUEA) + j * nfa, g); I.ufa = faces_of<T>(a(W_IUFA) + j * nfa, g);
+        I.dua = faces_of<T>(a(W_IDUA) + j * nfa, g);
+        I.sela = static_cast<uint8_t*>(t->wk[W_ISELA]) + j * nfa;
+        I.swa = static_cast<float*>(t->wk[W_ISWA]) + 3 * j * nfa;
         return I;
     }
     T* seg_T(int s) const { return a(W_TS) + (size_t)s * np; }
@@ -1217,7 +1457,7 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     const Grid& g = c->G;
     const size_t np3 = 3 * (size_t)t->np, nf = (size_t)g.nfx + g.nfy + g.nfz, n = g.n;
     const int nseg = (t->nsteps + t->every - 1) / t->every;
-    const size_t E = (size_t)t->every;
+    const size_t E = 1;   // intermediates of one step at a time (adj_run)
     size_t cnt[W_COUNT], es[W_COUNT];
     for (int w = 0; w < W_COUNT; w++) es[w] = sizeof(T);
     cnt[W_XS] = cnt[W_VS] = np3 * (size_t)(nseg + t->every);   // segment starts, then one segment's steps
@@ -1243,6 +1483,13 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     cnt[W_HST] = hn * (size_t)t->nsteps;
     cnt[W_HS4] = 4 * hp;
     cnt[W_HCELLOF] = hp; es[W_HCELLOF] = sizeof(uint32_t);
+    const size_t af = t->air ? nf : 0;
+    for (int w : {W_UOLDA, W_UPROJA, W_A0, W_A1, W_A2}) cnt[w] = af;
+    cnt[W_S4C] = t->air ? 4 * (size_t)t->np : 0;
+    for (int w : {W_IUPA, W_IWTA, W_IUEA, W_IUFA, W_IDUA}) cnt[w] = af * E;
+    cnt[W_ISELA] = af * E; es[W_ISELA] = 1;
+    cnt[W_ISWA] = 3 * af * E; es[W_ISWA] = sizeof(float);
+    cnt[W_AIRC] = t->air ? n : 0; es[W_AIRC] = 1;
     for (int w = 0; w < W_COUNT; w++) {
         size_t bytes = es[w] * std::max<size_t>(cnt[w], 1);
         cudaError_t e = cudaMalloc(&t->wk[w], bytes);
@@ -1351,15 +1598,34 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     cudaStream_t s = c->stream;
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
     const mp_params& P = c->P;
+    const bool air = t->air;
     k_ad_sweep_sel<<<nbf, 256, 0, s>>>(g, t->phi[k], t->mark[k], MP_TYPEFLUID, I.sel, I.sw);
-    k_ad_gravity<T><<<nbp, 256, 0, s>>>(R.np, v, I.va, (T)P.dt * (T)P.gravity_z);
-    k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, t->mass, R.a(W_S4A), R.a(W_S4B));
-    k_ad_p2g<T><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), I.up, I.wt);
+    if (air) {
+        k_ad_sweep_sel<<<nbf, 256, 0, s>>>(g, t->phia[k], t->mark[k], MP_TYPEAIR, I.sela, I.swa);
+        k_ad_forces<T><<<nbp, 256, 0, s>>>(R.np, t->phase, v, I.va, (T)P.dt * (T)P.gravity_z,
+                                           (T)P.buoyance_rate_air, (T)P.bubble_max_vel);
+    } else {
+        k_ad_gravity<T><<<nbp, 256, 0, s>>>(R.np, v, I.va, (T)P.dt * (T)P.gravity_z);
+    }
+    k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, air ? t->mass_w : t->mass, R.a(W_S4A),
+                                            R.a(W_S4B));
+    k_ad_p2g<T, 0><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), I.up, I.wt, nullptr);
     k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, I.up.x, R.a(W_UOLD));
+    if (air) {
+        uint8_t* airc = static_cast<uint8_t*>(t->wk[W_AIRC]);
+        k_ad_air_cells<<<nbc, 256, 0, s>>>(g.n, t->off[k], t->order[k], t->phase, airc);
+        k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, t->mass_a, R.a(W_S4C), R.a(W_S4B));
+        k_ad_p2g<T, 1><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4C), R.a(W_S4B), I.upa, I.wta, airc);
+        k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, I.upa.x, R.a(W_UOLDA));
+        k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, I.upa, R.f(W_T0), I.sela, I.swa);
+        k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_A0), I.sela, I.swa);
+    }
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, I.up, R.f(W_T0), I.sel, I.sw);
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B0), I.sel, I.sw);
+    if (air) k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_A0), I.uea, t->mark[k]);
     k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), I.ue, t->mark[k]);
-    k_ad_div<T><<<nbc, 256, 0, s>>>(g, t->mark[k], I.ue, R.a(W_CB));
+    if (air) k_ad_div2<T><<<nbc, 256, 0, s>>>(g, t->mark[k], t->lsm[k], I.ue, I.uea, R.a(W_CB));
+    else k_ad_div<T><<<nbc, 256, 0, s>>>(g, t->mark[k], I.ue, R.a(W_CB));
     MP_CHECK_LAUNCH(c);
     T* pk = R.a(W_PST) + (size_t)k * g.n;
     if (solve) {
@@ -1369,11 +1635,21 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
         if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
     }
     k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, pk, I.ue, R.f(W_UPROJ));
+    if (air) {
+        k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, pk, I.uea, R.f(W_UPROJA));
+        k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_UPROJA), R.f(W_A1), I.sela, I.swa);
+        k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_A1), R.f(W_A2), I.sela, I.swa);
+    }
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_UPROJ), R.f(W_B1), I.sel, I.sw);
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), I.sel, I.sw);
+    if (air) {
+        k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_A2), I.ufa, t->mark[k]);
+        k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, I.ufa.x, R.a(W_UOLDA), I.dua.x);
+    }
     k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), I.uf, t->mark[k]);
     k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, I.uf.x, R.a(W_UOLD), I.du.x);
-    k_ad_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.va, I.uf, I.du, (T)P.flip_alpha, I.vg);
+    k_ad_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.va, I.uf, I.du, (T)P.flip_alpha, I.vg, air ? t->phase : nullptr,
+                                    I.ufa, I.dua);
     k_ad_advect<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, xo, vo, (T)P.dt);
     MP_CHECK_LAUNCH(c);
     if (t->heat) MP_TRY(heat_fwd<T>(R, k, xo, Tin, Tout, I, solve));
@@ -1381,8 +1657,9 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
 }
 
 // transpose of a step from its intermediates: (xb, vb) hold the adjoint of the
-// step's outputs on entry and of its inputs on exit
-template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, const T* x1, const T* Tin,
+// step's outputs on entry and of its inputs on exit; v is the step's input
+// velocity (the air force's slope depends on it)
+template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, const T* v, const T* x1, const T* Tin,
                                        const Inter<T>& I, T* xb, T* vb, T* Tb) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
     // the heat stage ran last, on the advected positions x1
@@ -1391,21 +1668,38 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
     const mp_params& P = c->P;
     const T alpha = (T)P.flip_alpha;
+    const bool air = t->air;
     uint32_t* cellof = static_cast<uint32_t*>(t->wk[W_CELLOF]);
     uint32_t* flag = static_cast<uint32_t*>(t->wk[W_FLAG]);
     k_ad_cellof<<<nbc, 256, 0, s>>>(g.n, t->order[k], t->off[k], cellof);
     MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
     k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x, cellof, flag);
     k_ad_advect_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, (T)P.dt, xb, vb, R.a(W_VGB));
-    k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.uf, I.du, alpha, R.a(W_VGB), R.a(W_VAB), xb);
-    k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, R.a(W_VGB), nullptr, R.a(W_S4A), R.a(W_S4B));
+    k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.uf, I.du, alpha, R.a(W_VGB), R.a(W_VAB), xb,
+                                          air ? t->phase : nullptr, I.ufa, I.dua);
+    if (air) {
+        // the face side per phase: each field gathers only its own particles
+        k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, R.a(W_VGB), nullptr, R.a(W_S4A), R.a(W_S4B));
+        k_ad_slot_gather_ph<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], R.a(W_VGB), t->phase, 0, R.a(W_S4B));
+        k_ad_slot_gather_ph<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], R.a(W_VGB), t->phase, 1, R.a(W_S4C));
+    } else {
+        k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, R.a(W_VGB), nullptr, R.a(W_S4A), R.a(W_S4B));
+    }
     MP_CHECK_LAUNCH(c);
     uint32_t wide = 1;
     MP_CUDA(c, cudaMemcpyAsync(&wide, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     MP_CUDA(c, cudaStreamSynchronize(s));
-    // q = I^T vgbar on B0; ufbar = q, uoldbar = -cdu q
-    if (wide) k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0));
-    else k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0));
+    // q = I^T vgbar on B0 (A0 for the air faces); ufbar = q, uoldbar = -cdu q
+    if (wide) k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0), nullptr);
+    else k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0), nullptr);
+    if (air) {
+        // the air cell mask of this step, from its forward replay
+        const uint8_t* airc = static_cast<const uint8_t*>(t->wk[W_AIRC]);
+        if (wide)
+            k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4C), R.f(W_A0), airc);
+        else
+            k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4C), R.f(W_A0), airc);
+    }
     const T cdu = alpha == (T)1 ? (T)1 : alpha;
     // wall rules then the two passes, transposed (B0 -> B1 -> T0 -> B1); the
     // ceiling rule's decision reads the rule's output, equal to its input
@@ -1413,24 +1707,46 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
     k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B0), R.f(W_B1), I.uf, t->mark[k]);
     k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_T0), I.sel, I.sw);
     k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_B1), I.sel, I.sw);
-    // projection: ubar_e = ubar_proj + D^T L^-1 (-G^T ubar_proj)
-    k_ad_pbar<T><<<nbc, 256, 0, s>>>(g, t->mark[k], R.f(W_B1), R.a(W_CB));
+    if (air) {
+        k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_A0), R.f(W_A1), I.ufa, t->mark[k]);
+        k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_A1), R.f(W_T0), I.sela, I.swa);
+        k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_A1), I.sela, I.swa);
+    }
+    // projection: ubar_e = ubar_proj + D^T L^-1 (-G^T ubar_proj), with both
+    // phases' fields taking the one pressure gradient
+    if (air) k_ad_pbar2<T><<<nbc, 256, 0, s>>>(g, t->mark[k], R.f(W_B1), R.f(W_A1), R.a(W_CB));
+    else k_ad_pbar<T><<<nbc, 256, 0, s>>>(g, t->mark[k], R.f(W_B1), R.a(W_CB));
     MP_CHECK_LAUNCH(c);
     int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
     int it = 0; double res = 0;
     int st = k_cg_solve(c, t->mark[k], R.a(W_CQ), R.a(W_CB), maxit, mode, tol, &it, &res);
     if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
-    k_ad_divT<T><<<nbf, 256, 0, s>>>(g, R.a(W_CQ), R.f(W_B1), R.f(W_B2));
+    if (air) {
+        k_ad_divT2<T><<<nbf, 256, 0, s>>>(g, t->mark[k], t->lsm[k], R.a(W_CQ), R.f(W_B1), R.f(W_A1), R.f(W_B2),
+                                          R.f(W_A2));
+        k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_A2), R.f(W_A1), I.uea, t->mark[k]);
+        k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_A1), R.f(W_A2), I.sela, I.swa);
+        k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_A2), R.f(W_A1), I.sela, I.swa);
+        k_ad_axpy<T><<<nbf, 256, 0, s>>>(R.nf, -cdu, R.a(W_A0), R.a(W_A1));
+    } else {
+        k_ad_divT<T><<<nbf, 256, 0, s>>>(g, R.a(W_CQ), R.f(W_B1), R.f(W_B2));
+    }
     k_ad_bound_adj<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), I.ue, t->mark[k]);
     k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), I.sel, I.sw);
     k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), I.sel, I.sw);
     // upbar = that + uoldbar
     k_ad_axpy<T><<<nbf, 256, 0, s>>>(R.nf, -cdu, R.a(W_B0), R.a(W_B1));
-    // splat transpose (vabar += ..., xbar += ...)
-    k_ad_p2g_adj<T><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.va, t->mass, cellof, I.up, I.wt, R.f(W_B1),
-                                        R.a(W_VAB), xb);
-    // gravity: vbar = vabar
-    k_ad_copy<T><<<nbp, 256, 0, s>>>(3LL * R.np, R.a(W_VAB), vb);
+    // splat transposes (vabar += ..., xbar += ...)
+    k_ad_p2g_adj<T, 0><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.va, air ? t->mass_w : t->mass, cellof, I.up,
+                                           I.wt, R.f(W_B1), R.a(W_VAB), xb);
+    if (air)
+        k_ad_p2g_adj<T, 1><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.va, t->mass_a, cellof, I.upa, I.wta,
+                                               R.f(W_A1), R.a(W_VAB), xb);
+    // external forces: vbar = dva/dv^T vabar
+    if (air)
+        k_ad_forces_adj<T><<<nbp, 256, 0, s>>>(R.np, t->phase, v, R.a(W_VAB), vb, (T)P.dt * (T)P.gravity_z,
+                                               (T)P.buoyance_rate_air, (T)P.bubble_max_vel);
+    else k_ad_copy<T><<<nbp, 256, 0, s>>>(3LL * R.np, R.a(W_VAB), vb);
     MP_CHECK_LAUNCH(c);
     return MP_OK;
 }
@@ -1540,8 +1856,7 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
     }
     MP_CHECK_LAUNCH(c);
     // reverse sweep, segment by segment: the segment is replayed from its
-    // start, each step's state and intermediates kept in its slot, then the
-    // steps are reversed
+    // start, each step's state kept in its slot, then the steps are reversed
     for (int sg = nseg - 1; sg >= 0; sg--) {
         const int k0 = sg * E, len = std::min(t->nsteps, k0 + E) - k0;
         MP_CUDA(c, cudaMemcpyAsync(R.seg_x(nseg), ckx[sg], sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
@@ -1551,10 +1866,18 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
         auto xs = [&](int j) { return j < len ? R.seg_x(nseg + j) : R.a(W_XN); };
         auto vs = [&](int j) { return j < len ? R.seg_v(nseg + j) : R.a(W_VN); };
         auto Ts = [&](int j) -> T* { return !t->heat ? nullptr : (j < len ? R.seg_T(nseg + j) : R.a(W_TN)); };
+        // one step's intermediates are kept at a time: the states of the
+        // segment first, then each step is replayed again (its pressure from
+        // the first replay, so no solve) just before its transpose. The replay
+        // is deterministic, so it rewrites the same next state.
+        const Inter<T> I = R.inter(0);
         for (int j = 0; j < len; j++)
-            MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), R.inter(j), false));
-        for (int j = len - 1; j >= 0; j--)
-            MP_TRY(adj_step<T>(R, k0 + j, xs(j), xs(j + 1), Ts(j), R.inter(j), xb, vb, Tb));
+            MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), I, false));
+        for (int j = len - 1; j >= 0; j--) {
+            if (j < len - 1)
+                MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), I, false));
+            MP_TRY(adj_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), Ts(j), I, xb, vb, Tb));
+        }
     }
     if (io.v0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, vb, io.v0b);
     if (io.x0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, xb, io.x0b);
@@ -1617,6 +1940,14 @@ int k_adj_vjp(MpCtx* c, int precision, const mp_grad* in, const mp_grad* dout, m
 int k_adj_ls_loss(MpCtx* c, int precision, const double* xT, double* loss, double* xTb) {
     if (precision == MP_PREC_FP64) return adj_ls_loss<double>(c, xT, loss, xTb);
     return adj_ls_loss<float>(c, xT, loss, xTb);
+}
+int k_adj_order(MpCtx* c, uint32_t* ids) {
+    if (!c->adj) { c->err = "adjoint: record first"; return MP_ERR_STATE; }
+    if (c->np() != c->adj->np) { c->err = "adjoint: the particles changed since the recording"; return MP_ERR_STATE; }
+    MP_CUDA(c, cudaMemcpyAsync(ids, c->adj->ids, sizeof(uint32_t) * (size_t)c->adj->np, cudaMemcpyDeviceToDevice,
+                               c->stream));
+    MP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MP_OK;
 }
 int k_adj_np(MpCtx* c, int* np, int* nsteps) {
     if (!c->adj) { c->err = "adjoint: record first"; return MP_ERR_STATE; }

@@ -351,17 +351,22 @@ def precision_report(sim, mp, stream, fp64_steps):
 
 
 def fwd_adjoint(args, n, local, dist):
-    """Forward + adjoint throughput on the FLUID-only program the adjoint covers
-    (configuration 4, the dam break, at the bench's grid): the recorded engine
-    steps plus the gradient of the loss with respect to the initial particle
-    velocities (FP32 replay and transpose, checkpoints every --adj-every steps),
-    timed with CUDA events on the context's stream, max over ranks."""
+    """Forward + adjoint throughput of the two-phase program the adjoint covers
+    on the bubble column (configuration 5's scene and step at the bench's
+    grid, FLUID and AIR particles, position correction off, without the
+    solo-air stages): the recorded engine steps plus the gradient of the loss
+    with respect to the initial particle velocities (FP32 replay and
+    transpose, checkpoints every --adj-every steps), timed with CUDA events on
+    the context's stream, max over ranks."""
     import importlib
     import torch
     mp = importlib.import_module("2017multiphase_b200")
-    sim = mp.Sim.from_config(4, n, replica_seed(2017004, int(os.environ.get("RANK", "0"))))
+    p = mp.scene_params(5, n)
+    p.b_correct_position = 0
+    p.b_run_mc = 0   # the recorded program extracts no surface
+    sim = mp.Sim.from_config(5, n, replica_seed(2017005, int(os.environ.get("RANK", "0"))), params=p)
     stream = torch.cuda.ExternalStream(sim.stream_handle())
-    targets = mp.dam_break_targets(4096, 2017004, height=0.3)
+    targets = mp.dam_break_targets(4096, 2017005, height=0.7)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -384,8 +389,9 @@ def fwd_adjoint(args, n, local, dist):
            "checkpoint_every": args.adj_every, "fwd_ms_per_step": fwd_ms / args.adj_steps,
            "adjoint_ms_per_step": adj_ms / args.adj_steps, "particles": sim.adj_num_particles(),
            "loss": loss, "grad_norm": float(grad.norm()),
-           "workload": f"dam break {n}^3 (liquid x<0.4, z<0.6, FLUID only, no position correction), "
-                       f"loss = sum phi^2 on 4096 target points at z=0.3, dL/dv0 in FP32"}
+           "workload": f"bubble column {n}^3 (liquid z<0.8 with AIR bubbles; FLUID and AIR, the two-phase "
+                       f"projection; position correction and the solo-air stages off), "
+                       f"loss = sum phi^2 of the fluid level set on 4096 target points at z=0.7, dL/dv0 in FP32"}
     sim.close()
     return res
 

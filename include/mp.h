@@ -534,13 +534,22 @@ typedef struct mp_output {
 int mp_set_output(void* ctx, const mp_output* out);
 
 /* ---- adjoint (no counterpart in the reference) -------------------------------
- * Reverse-mode derivative of the step for a scene of FLUID particles only,
- * with position correction, heat, gas, melting, freezing and solids off
- * (configuration 4, the dam break). mp_adj_record runs `nsteps` engine steps
- * from the current particles (advancing the context) and records the
- * discrete state of each step (splat order and cell ranges, cell marks, the
- * extrapolation distance field, and at the end each cell's nearest particle);
- * the derivative is that of the program with this state held fixed.
+ * Reverse-mode derivative of the step for a scene of FLUID particles, or of
+ * FLUID and AIR particles (bubbles), with position correction, gas, melting,
+ * freezing and solids off (configuration 4, the dam break; configurations 1
+ * and 5 with position correction off). The program is bubblesim's: external
+ * forces (gravity on FLUID, the buoyancy of AIR), the water and air splats,
+ * extrapolation of both fields, wall rules, the two-phase projection (the
+ * level-set blend of cptdivergence_bubble2 at liquid-air faces), the FLIP/PIC
+ * gather of each phase's field and advection; the solo-air stages
+ * (markSoloAirParticle, the drag and SPH forces) are not part of it, so AIR
+ * particles stay AIR. The heat stage (b_heat_trans) is differentiated for
+ * FLUID-only scenes. mp_adj_record runs `nsteps` steps of this program with
+ * the engine's own stages from the current particles (advancing the context)
+ * and records the discrete state of each step (splat order and cell ranges,
+ * cell marks, the merged level set and the extrapolation distance fields,
+ * and at the end each cell's nearest FLUID particle); the derivative is that
+ * of the program with this state held fixed.
  * mp_adj_set_targets takes the target points y_s (host float xyz) of the
  * loss L = sum_s phi(y_s)^2, phi the fluid distance field of genlevelset
  * after the last step. mp_adj_loss replays the program from the recorded
@@ -577,6 +586,12 @@ int mp_step_adjoint(void* ctx, int precision, const mp_grad* in, const mp_grad* 
 int mp_adj_level_set_loss(void* ctx, int precision, const double* pos, double* loss, double* dloss_dpos);
 int mp_adj_set_targets(void* ctx, const float* samples3, int nsamples);
 int mp_adj_info(void* ctx, int* np, int* nsteps);
+/* The recording order of the context's current particles: ids[s] (device,
+ * one uint32 per particle) is the index, in the order the particles had at
+ * mp_adj_record, of the particle now in slot s (mp_download_particles'
+ * order), so the engine's state after the recording can be set beside the
+ * replay's final state. */
+int mp_adj_order(void* ctx, uint32_t* ids);
 int mp_adj_loss(void* ctx, int precision, const double* v0, double* loss);
 int mp_adj_gradient(void* ctx, int precision, const double* v0, double* grad_v0, double* loss);
 int mp_adj_release(void* ctx);
