@@ -34,8 +34,9 @@
 // symmetric pressure matrix. States are checkpointed every `every` steps and
 // recomputed segment by segment during the reverse sweep; each step's
 // intermediates are recomputed from its state just before its transpose, so
-// only one step's are held (the pressure and heat solves of the first replay
-// are kept per step, so the recomputations solve nothing).
+// only one step's are held (the splats and the pressure and heat solves of
+// the first replay are kept per step, so the recomputations neither splat
+// nor solve).
 #include "ctx.cuh"
 #include <algorithm>
 #include <cstring>
@@ -279,6 +280,102 @@ __global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ off, const T* __re
         }
         fsel(W, ax)[idx] = w;
         fsel(u, ax)[idx] = w > (T)0 ? s / w : (T)0;
+    }
+}
+// The same splat with a warp per 32 nodes along k (i, j fixed), a thread per
+// node's three faces: for each column (a, b) of the window the particles of
+// the warp's cells along k are one contiguous range of the recorded order; the
+// warp stages it in shared memory CAP records at a time with coalesced loads,
+// and each lane walks its own part. A face sums the same pairs in the same
+// order as k_ad_p2g (a pair beyond the kernel radius adds +0 there and is
+// skipped here), so the fields are identical.
+template <class T, int PH>
+__global__ void __launch_bounds__(256) k_ad_p2g_w(Grid g, const uint32_t* __restrict__ off,
+                                                  const T* __restrict__ xs4, const T* __restrict__ vs4, Fc<T> u,
+                                                  Fc<T> W, const uint8_t* __restrict__ cellmask) {
+    using Wn = SplatWin<PH>;
+    constexpr int CAP = sizeof(T) == 4 ? 128 : 64;
+    constexpr int R = Wn::AC;   // the union window: [-AC, AC] on every axis (LO == AC, HI <= AC)
+    __shared__ T sm_x[8][CAP][4];
+    __shared__ T sm_v[8][CAP][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const Tiles Tl = make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1);
+    const T scale = (T)1 / (T)g.h;
+    const T cker = (T)1.4f * (T)1.4f;
+    MP_GRID_LOOP(t, Tl.threads()) {
+        int i, j, k;
+        const bool act = tile_ijk(Tl, t, i, j, k);
+        if (!__any_sync(0xffffffffu, act)) continue;
+        const bool hx = act && j < g.NY && k < g.NZ, hy = act && i < g.NX && k < g.NZ, hz = act && i < g.NX && j < g.NY;
+        T wx = 0, sx = 0, wy = 0, sy = 0, wz = 0, sz = 0;
+        const T ti = (T)(float)i, tj = (T)(float)j, tk = (T)(float)k;
+        const T half = (T)0.5f;
+        const int klo = max(k - R, 0), khi = min(k + R, g.NZ - 1), kzhi = min(k + Wn::HI, g.NZ - 1);
+        for (int di = -R; di <= R; di++) {
+            const int a = i + di;
+            if (a < 0 || a > g.NX - 1) continue;   // the same for the whole warp
+            const bool ax = hx && di >= -Wn::LO && di <= Wn::HI;
+            for (int dj = -R; dj <= R; dj++) {
+                const int b = j + dj;
+                if (b < 0 || b > g.NY - 1) continue;
+                const bool ay = hy && dj >= -Wn::LO && dj <= Wn::HI;
+                bool need = (ax || ay || hz) && klo <= khi;
+                const int cb = cid(g, a, b, 0);
+                if (need && cellmask) {
+                    bool any = false;
+                    for (int cc = klo; cc <= khi; cc++) any = any || cellmask[cb + cc];
+                    need = any;
+                }
+                if (!__any_sync(0xffffffffu, need)) continue;
+                uint32_t s0 = 0, s1 = 0, sz1 = 0;
+                if (need) {
+                    s0 = off[cb + klo]; s1 = off[cb + khi + 1];
+                    sz1 = hz ? off[cb + kzhi + 1] : s0;
+                }
+                // the warp's range: the lanes' windows along k overlap, so their
+                // ranges join into one
+                const uint32_t A = __reduce_min_sync(0xffffffffu, need ? s0 : 0xffffffffu);
+                const uint32_t B = __reduce_max_sync(0xffffffffu, need ? s1 : 0u);
+                for (uint32_t c0 = A; c0 < B; c0 += CAP) {
+                    const uint32_t n = min(B - c0, (uint32_t)CAP);
+                    __syncwarp();
+                    for (uint32_t q = lane; q < n; q += 32) {
+                        const T* r = xs4 + 4 * (size_t)(c0 + q);
+                        const T* v = vs4 + 4 * (size_t)(c0 + q);
+                        sm_x[warp][q][0] = r[0]; sm_x[warp][q][1] = r[1]; sm_x[warp][q][2] = r[2];
+                        sm_x[warp][q][3] = r[3];
+                        sm_v[warp][q][0] = v[0]; sm_v[warp][q][1] = v[1]; sm_v[warp][q][2] = v[2];
+                    }
+                    __syncwarp();
+                    if (!need) continue;
+                    const uint32_t lo = max(s0, c0), hi = min(s1, c0 + n);
+                    for (uint32_t p = lo; p < hi; ++p) {
+                        const T m = sm_x[warp][p - c0][3];
+                        if (m == (T)0) continue;   // the other phase: adds +0
+                        const T X = sm_x[warp][p - c0][0] * scale, Y = sm_x[warp][p - c0][1] * scale;
+                        const T Z = sm_x[warp][p - c0][2] * scale;
+                        if (ax) {
+                            const T dx = X - ti, dy = Y - (tj + half), dz = Z - (tk + half);
+                            const T r2 = dx * dx + dy * dy + dz * dz;
+                            if (r2 < cker) { const T wp = m * sharpk(r2); wx += wp; sx += wp * sm_v[warp][p - c0][0]; }
+                        }
+                        if (ay) {
+                            const T dx = X - (ti + half), dy = Y - tj, dz = Z - (tk + half);
+                            const T r2 = dx * dx + dy * dy + dz * dz;
+                            if (r2 < cker) { const T wp = m * sharpk(r2); wy += wp; sy += wp * sm_v[warp][p - c0][1]; }
+                        }
+                        if (hz && p < sz1) {
+                            const T dx = X - (ti + half), dy = Y - (tj + half), dz = Z - tk;
+                            const T r2 = dx * dx + dy * dy + dz * dz;
+                            if (r2 < cker) { const T wp = m * sharpk(r2); wz += wp; sz += wp * sm_v[warp][p - c0][2]; }
+                        }
+                    }
+                }
+            }
+        }
+        if (hx) { const int f = fxi(g, i, j, k); W.x[f] = wx; u.x[f] = wx > (T)0 ? sx / wx : (T)0; }
+        if (hy) { const int f = fyi(g, i, j, k); W.y[f] = wy; u.y[f] = wy > (T)0 ? sy / wy : (T)0; }
+        if (hz) { const int f = fzi(g, i, j, k); W.z[f] = wz; u.z[f] = wz > (T)0 ? sz / wz : (T)0; }
     }
 }
 // particle records in a step's recorded sorted order: (a xyz, mass or 0) and
@@ -1398,8 +1495,8 @@ namespace {
 // (each step is replayed again just before its transpose)
 enum {
     W_XS, W_VS, W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN,
-    W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2,
-    W_IVA, W_IVG, W_IUP, W_IWT, W_IUE, W_IUF, W_IDU, W_ISEL, W_ISW,
+    W_T0, W_UPROJ, W_B0, W_B1, W_B2,
+    W_IVA, W_IVG, W_CUP, W_CWT, W_IUE, W_IUF, W_IDU, W_ISEL, W_ISW,
     W_CB, W_CP, W_CQ, W_PHI, W_SV, W_LOSS, W_CELLOF, W_FLAG, W_S4A, W_S4B, W_PST,
     // heat: temperatures (current, next, segment states, cotangent), per-slot
     // intermediates (cell temperature and weight, extended solution, change;
@@ -1409,7 +1506,7 @@ enum {
     // the air phase: its splat's old field, projected field and scratch, its
     // splat records, and its per-slot intermediates (splat, weights,
     // extrapolated, final, change; extrapolation choices)
-    W_UOLDA, W_UPROJA, W_A0, W_A1, W_A2, W_S4C, W_IUPA, W_IWTA, W_IUEA, W_IUFA, W_IDUA, W_ISELA, W_ISWA, W_AIRC,
+    W_UPROJA, W_A0, W_A1, W_A2, W_S4C, W_CUPA, W_CWTA, W_IUEA, W_IUFA, W_IDUA, W_ISELA, W_ISWA, W_AIRC,
     W_COUNT
 };
 }
@@ -1431,7 +1528,6 @@ template <class T> struct Replay {
         const size_t np3 = 3 * (size_t)np, nfs = (size_t)nf;
         Inter<T> I;
         I.va = a(W_IVA) + j * np3; I.vg = a(W_IVG) + j * np3;
-        I.up = faces_of<T>(a(W_IUP) + j * nfs, g); I.wt = faces_of<T>(a(W_IWT) + j * nfs, g);
         I.ue = faces_of<T>(a(W_IUE) + j * nfs, g); I.uf = faces_of<T>(a(W_IUF) + j * nfs, g);
         I.du = faces_of<T>(a(W_IDU) + j * nfs, g);
         I.sel = static_cast<uint8_t*>(t->wk[W_ISEL]) + j * nfs;
@@ -1440,7 +1536,6 @@ template <class T> struct Replay {
         I.Tc = a(W_HTC) + j * n; I.Wc = a(W_HWC) + j * n; I.Te = a(W_HTE) + j * n; I.dT = a(W_HDT) + j * n;
         I.T1 = a(W_HT1) + j * npp;
         const size_t nfa = t->air ? nfs : 0;
-        I.upa = faces_of<T>(a(W_IUPA) + j * nfa, g); I.wta = faces_of<T>(a(W_IWTA) + j * nfa, g);
         I.uea = faces_of<T>(a(W_IUEA) + j * nfa, g); I.ufa = faces_of<T>(a(W_IUFA) + j * nfa, g);
         I.dua = faces_of<T>(a(W_IDUA) + j * nfa, g);
         I.sela = static_cast<uint8_t*>(t->wk[W_ISELA]) + j * nfa;
@@ -1448,6 +1543,16 @@ template <class T> struct Replay {
         return I;
     }
     T* seg_T(int s) const { return a(W_TS) + (size_t)s * np; }
+    // step k's splats (field and weights of each phase): the first replay
+    // computes them, the later replays of the reverse sweep (same inputs)
+    // read them back
+    Inter<T> with_splat(const Inter<T>& I0, int k) const {
+        Inter<T> I = I0;
+        const size_t ks = (size_t)k * (size_t)nf, ka = t->air ? ks : 0;
+        I.up = faces_of<T>(a(W_CUP) + ks, g); I.wt = faces_of<T>(a(W_CWT) + ks, g);
+        I.upa = faces_of<T>(a(W_CUPA) + ka, g); I.wta = faces_of<T>(a(W_CWTA) + ka, g);
+        return I;
+    }
 };
 
 template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
@@ -1462,9 +1567,10 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     for (int w = 0; w < W_COUNT; w++) es[w] = sizeof(T);
     cnt[W_XS] = cnt[W_VS] = np3 * (size_t)(nseg + t->every);   // segment starts, then one segment's steps
     for (int w : {W_XB, W_VB, W_VAB, W_VGB, W_X, W_V, W_XN, W_VN}) cnt[w] = np3;
-    for (int w : {W_UOLD, W_T0, W_UPROJ, W_B0, W_B1, W_B2}) cnt[w] = nf;
+    for (int w : {W_T0, W_UPROJ, W_B0, W_B1, W_B2}) cnt[w] = nf;
     cnt[W_IVA] = cnt[W_IVG] = np3 * E;
-    for (int w : {W_IUP, W_IWT, W_IUE, W_IUF, W_IDU}) cnt[w] = nf * E;
+    for (int w : {W_IUE, W_IUF, W_IDU}) cnt[w] = nf * E;
+    for (int w : {W_CUP, W_CWT}) cnt[w] = nf * (size_t)t->nsteps;
     cnt[W_ISEL] = nf * E; es[W_ISEL] = 1;
     cnt[W_ISW] = 3 * nf * E; es[W_ISW] = sizeof(float);
     for (int w : {W_CB, W_CP, W_CQ, W_PHI}) cnt[w] = n;
@@ -1484,9 +1590,10 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     cnt[W_HS4] = 4 * hp;
     cnt[W_HCELLOF] = hp; es[W_HCELLOF] = sizeof(uint32_t);
     const size_t af = t->air ? nf : 0;
-    for (int w : {W_UOLDA, W_UPROJA, W_A0, W_A1, W_A2}) cnt[w] = af;
+    for (int w : {W_UPROJA, W_A0, W_A1, W_A2}) cnt[w] = af;
     cnt[W_S4C] = t->air ? 4 * (size_t)t->np : 0;
-    for (int w : {W_IUPA, W_IWTA, W_IUEA, W_IUFA, W_IDUA}) cnt[w] = af * E;
+    for (int w : {W_IUEA, W_IUFA, W_IDUA}) cnt[w] = af * E;
+    for (int w : {W_CUPA, W_CWTA}) cnt[w] = af * (size_t)t->nsteps;
     cnt[W_ISELA] = af * E; es[W_ISELA] = 1;
     cnt[W_ISWA] = 3 * af * E; es[W_ISWA] = sizeof(float);
     cnt[W_AIRC] = t->air ? n : 0; es[W_AIRC] = 1;
@@ -1593,8 +1700,9 @@ template <class T> static int heat_adj(const Replay<T>& R, int k, const T* x1, c
 // The pressure solve's result is stored in pst (first replay) or copied from
 // it (segment replays): the inputs are the same bit for bit, so is the result.
 template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, const T* v, T* xo, T* vo,
-                                       const T* Tin, T* Tout, const Inter<T>& I, bool solve) {
+                                       const T* Tin, T* Tout, const Inter<T>& I0, bool solve) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
+    const Inter<T> I = R.with_splat(I0, k);
     cudaStream_t s = c->stream;
     const int nbp = mp_blocks(R.np, 256), nbf = mp_blocks(R.nf, 256), nbc = mp_blocks(g.n, 256);
     const mp_params& P = c->P;
@@ -1607,16 +1715,21 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     } else {
         k_ad_gravity<T><<<nbp, 256, 0, s>>>(R.np, v, I.va, (T)P.dt * (T)P.gravity_z);
     }
-    k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, air ? t->mass_w : t->mass, R.a(W_S4A),
-                                            R.a(W_S4B));
-    k_ad_p2g<T, 0><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), I.up, I.wt, nullptr);
-    k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, I.up.x, R.a(W_UOLD));
+    // the splats (kept per step: the replays after the first read them back);
+    // each splat stays as it is through the step and is its FLIP old field
+    const int nbw = mp_blocks(make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1).threads(), 256);
+    if (solve) {
+        k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, air ? t->mass_w : t->mass, R.a(W_S4A),
+                                                R.a(W_S4B));
+        k_ad_p2g_w<T, 0><<<nbw, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), I.up, I.wt, nullptr);
+    }
     if (air) {
         uint8_t* airc = static_cast<uint8_t*>(t->wk[W_AIRC]);
         k_ad_air_cells<<<nbc, 256, 0, s>>>(g.n, t->off[k], t->order[k], t->phase, airc);
-        k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, t->mass_a, R.a(W_S4C), R.a(W_S4B));
-        k_ad_p2g<T, 1><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4C), R.a(W_S4B), I.upa, I.wta, airc);
-        k_ad_copy<T><<<nbf, 256, 0, s>>>(R.nf, I.upa.x, R.a(W_UOLDA));
+        if (solve) {
+            k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, t->mass_a, R.a(W_S4C), R.a(W_S4B));
+            k_ad_p2g_w<T, 1><<<nbw, 256, 0, s>>>(g, t->off[k], R.a(W_S4C), R.a(W_S4B), I.upa, I.wta, airc);
+        }
         k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, I.upa, R.f(W_T0), I.sela, I.swa);
         k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_T0), R.f(W_A0), I.sela, I.swa);
     }
@@ -1644,10 +1757,10 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     k_ad_sweepu_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B1), R.f(W_B2), I.sel, I.sw);
     if (air) {
         k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_A2), I.ufa, t->mark[k]);
-        k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, I.ufa.x, R.a(W_UOLDA), I.dua.x);
+        k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, I.ufa.x, I.upa.x, I.dua.x);
     }
     k_ad_bound<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), I.uf, t->mark[k]);
-    k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, I.uf.x, R.a(W_UOLD), I.du.x);
+    k_ad_sub<T><<<nbf, 256, 0, s>>>(R.nf, I.uf.x, I.up.x, I.du.x);
     k_ad_g2p<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.va, I.uf, I.du, (T)P.flip_alpha, I.vg, air ? t->phase : nullptr,
                                     I.ufa, I.dua);
     k_ad_advect<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, xo, vo, (T)P.dt);
@@ -1660,8 +1773,9 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
 // step's outputs on entry and of its inputs on exit; v is the step's input
 // velocity (the air force's slope depends on it)
 template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, const T* v, const T* x1, const T* Tin,
-                                       const Inter<T>& I, T* xb, T* vb, T* Tb) {
+                                       const Inter<T>& I0, T* xb, T* vb, T* Tb) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
+    const Inter<T> I = R.with_splat(I0, k);
     // the heat stage ran last, on the advected positions x1
     if (t->heat) MP_TRY(heat_adj<T>(R, k, x1, Tin, I, Tb, xb));
     cudaStream_t s = c->stream;
