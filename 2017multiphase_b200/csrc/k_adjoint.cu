@@ -525,16 +525,30 @@ __global__ void k_ad_sweepu_adj_s(Grid g, Fc<T> ob, Fc<T> ib, const uint8_t* __r
     }
 }
 // raises *flag when some particle's cell from its replay position differs from
-// its recorded cell (the G2P transpose then searches the wider window)
+// its recorded cell (the G2P transposes then search a wider window), and with
+// `cellbad` marks the recorded cell of each such particle
 template <class T>
 __global__ void k_ad_cell_mismatch(Grid g, int np, const T* __restrict__ x, const uint32_t* __restrict__ cellof,
-                                   uint32_t* flag) {
+                                   uint32_t* flag, uint8_t* __restrict__ cellbad) {
     MP_GRID_LOOP(p, np) {
         int a, b, c; getijk3((int)cellof[p], g.NY, g.NZ, a, b, c);
         const T X = x[3 * p] / (T)g.h, Y = x[3 * p + 1] / (T)g.h, Z = x[3 * p + 2] / (T)g.h;
         bool bad = !(X >= (T)0 && Y >= (T)0 && Z >= (T)0) || (int)X != a || (int)Y != b || (int)Z != c;
+        if (bad && cellbad) cellbad[cellof[p]] = 1;   // every writer stores 1
         if (__any_sync(__activemask(), bad) && (threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1))
             atomicOr(flag, 1u);
+    }
+}
+// near[c]: some cell of c's 3x3x3 neighbourhood holds a particle whose replay
+// cell is not its recorded one
+__global__ void k_ad_dilate(Grid g, const uint8_t* __restrict__ bad, uint8_t* __restrict__ near) {
+    MP_GRID_LOOP(idx, g.n) {
+        int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
+        uint8_t v = 0;
+        for (int a = max(i - 1, 0); a <= min(i + 1, g.NX - 1); a++)
+            for (int b = max(j - 1, 0); b <= min(j + 1, g.NY - 1); b++)
+                for (int cc = max(k - 1, 0); cc <= min(k + 1, g.NZ - 1); cc++) v |= bad[cid(g, a, b, cc)];
+        near[idx] = v;
     }
 }
 // wall rules (setWaterBoundaryU_k), in place; `zceil` marks the top z faces
@@ -950,18 +964,28 @@ __global__ void k_ad_g2p_adj_p(Grid g, int np, const uint32_t* __restrict__ orde
 // face side of the G2P transpose: q_f = sum of w_pf vgbar_p over the particles
 // whose interpolation stencil holds f. Those lie in cells [i-1,i] along the
 // face normal and [-1,1] across of their replay positions; the candidates come
-// from the recorded cell lists, so when some particle's replay cell differs
-// from its recorded one (WIDE) they are taken one cell wider. Membership is
-// decided from the replay's own positions either way.
-template <class T, bool WIDE>
+// from the recorded cell lists, so a face takes its candidates one cell wider
+// when a cell of that wider window holds a particle whose replay cell differs
+// from its recorded one (near[] of the core cells; with near null, every face
+// does). Membership is decided from the replay's own positions either way, and
+// a face's members appear in the same order in both windows.
+template <class T>
 __global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4,
-                               const T* __restrict__ vgs4, Fc<T> q, const uint8_t* __restrict__ cellmask) {
+                               const T* __restrict__ vgs4, Fc<T> q, const uint8_t* __restrict__ cellmask,
+                               const uint8_t* __restrict__ near) {
     const long long tot = (long long)g.nfx + g.nfy + g.nfz;
     MP_GRID_LOOP(t, tot) {
         int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
         const int w = ax == 0 ? g.NX + 1 : g.NX, hh = ax == 1 ? g.NY + 1 : g.NY, d = ax == 2 ? g.NZ + 1 : g.NZ;
         T acc = 0;
-        const int wd = WIDE ? 1 : 0;
+        bool wide = near == nullptr;
+        if (!wide) {
+            for (int a = max(i - 1, 0); a <= min(ax == 0 ? i : i + 1, g.NX - 1) && !wide; a++)
+                for (int b = max(j - 1, 0); b <= min(ax == 1 ? j : j + 1, g.NY - 1) && !wide; b++)
+                    for (int cc = max(k - 1, 0); cc <= min(ax == 2 ? k : k + 1, g.NZ - 1); cc++)
+                        if (near[cid(g, a, b, cc)]) { wide = true; break; }
+        }
+        const int wd = wide ? 1 : 0;
         const int a0 = i - 1 - wd, a1 = (ax == 0 ? i : i + 1) + wd, b0 = j - 1 - wd, b1 = (ax == 1 ? j : j + 1) + wd;
         const int c0 = k - 1 - wd, c1 = (ax == 2 ? k : k + 1) + wd;
         for (int a = a0; a <= a1; a++) {
@@ -1026,12 +1050,14 @@ __global__ void k_ad_p2g_adj(Grid g, int np, const uint32_t* __restrict__ order,
                     if (fj < 0 || fj >= H_) continue;
                     for (int fk = k0; fk <= k1; fk++) {
                         if (fk < 0 || fk >= D_) continue;
-                        int f = face_index(g, ax, fi, fj, fk);
-                        T Wf = fsel(W, ax)[f];
-                        if (!(Wf > (T)0)) continue;
                         float gx, gy, gz; face_pos(ax, fi, fj, fk, gx, gy, gz);
                         T dx = X - (T)gx, dy = Y - (T)gy, dz = Z - (T)gz;
                         T r2 = dx * dx + dy * dy + dz * dz;
+                        // beyond the kernel radius the weight and its slope are zero
+                        if (!(r2 < (T)1.4f * (T)1.4f)) continue;
+                        int f = face_index(g, ax, fi, fj, fk);
+                        T Wf = fsel(W, ax)[f];
+                        if (!(Wf > (T)0)) continue;
                         T k_ = sharpk(r2);
                         T kd = sharpk_d(r2);
                         if (k_ == (T)0 && kd == (T)0) continue;
@@ -1507,6 +1533,7 @@ enum {
     // splat records, and its per-slot intermediates (splat, weights,
     // extrapolated, final, change; extrapolation choices)
     W_UPROJA, W_A0, W_A1, W_A2, W_S4C, W_CUPA, W_CWTA, W_IUEA, W_IUFA, W_IDUA, W_ISELA, W_ISWA, W_AIRC,
+    W_CBAD, W_CNEAR,   // per cell: holds a particle whose replay cell moved; near one
     W_COUNT
 };
 }
@@ -1597,6 +1624,7 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     cnt[W_ISELA] = af * E; es[W_ISELA] = 1;
     cnt[W_ISWA] = 3 * af * E; es[W_ISWA] = sizeof(float);
     cnt[W_AIRC] = t->air ? n : 0; es[W_AIRC] = 1;
+    cnt[W_CBAD] = cnt[W_CNEAR] = n; es[W_CBAD] = es[W_CNEAR] = 1;
     for (int w = 0; w < W_COUNT; w++) {
         size_t bytes = es[w] * std::max<size_t>(cnt[w], 1);
         cudaError_t e = cudaMalloc(&t->wk[w], bytes);
@@ -1665,7 +1693,7 @@ template <class T> static int heat_adj(const Replay<T>& R, int k, const T* x1, c
     uint32_t* flag = static_cast<uint32_t*>(t->wk[W_FLAG]);
     k_ad_cellof<<<nbc, 256, 0, s>>>(g.n, t->order_h[k], t->off_h[k], cellof);
     MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
-    k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x1, cellof, flag);
+    k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x1, cellof, flag, nullptr);
     k_ad_heat_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, x1, I.T1, I.dT, I.Te, a, (T)P.melting_point,
                                                (T)P.boiling_point, Tb, R.a(W_HQ1), xb);
     k_ad_slot_gather1<T><<<nbp, 256, 0, s>>>(R.np, t->order_h[k], x1, R.a(W_HQ1), R.a(W_HS4));
@@ -1787,7 +1815,10 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
     uint32_t* flag = static_cast<uint32_t*>(t->wk[W_FLAG]);
     k_ad_cellof<<<nbc, 256, 0, s>>>(g.n, t->order[k], t->off[k], cellof);
     MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
-    k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x, cellof, flag);
+    uint8_t* cellbad = static_cast<uint8_t*>(t->wk[W_CBAD]);
+    uint8_t* near = static_cast<uint8_t*>(t->wk[W_CNEAR]);
+    MP_CUDA(c, cudaMemsetAsync(cellbad, 0, (size_t)g.n, s));
+    k_ad_cell_mismatch<T><<<nbp, 256, 0, s>>>(g, R.np, x, cellof, flag, cellbad);
     k_ad_advect_adj<T><<<nbp, 256, 0, s>>>(g, R.np, x, I.vg, (T)P.dt, xb, vb, R.a(W_VGB));
     k_ad_g2p_adj_p<T><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.uf, I.du, alpha, R.a(W_VGB), R.a(W_VAB), xb,
                                           air ? t->phase : nullptr, I.ufa, I.dua);
@@ -1800,19 +1831,22 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
         k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, R.a(W_VGB), nullptr, R.a(W_S4A), R.a(W_S4B));
     }
     MP_CHECK_LAUNCH(c);
-    uint32_t wide = 1;
-    MP_CUDA(c, cudaMemcpyAsync(&wide, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    uint32_t anybad = 1;
+    MP_CUDA(c, cudaMemcpyAsync(&anybad, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     MP_CUDA(c, cudaStreamSynchronize(s));
+    // the faces near a particle whose replay cell is not its recorded one take
+    // the wider window (none when no particle changed cell: cellbad is zero)
+    const uint8_t* nearp = cellbad;
+    if (anybad) {
+        k_ad_dilate<<<nbc, 256, 0, s>>>(g, cellbad, near);
+        nearp = near;
+    }
     // q = I^T vgbar on B0 (A0 for the air faces); ufbar = q, uoldbar = -cdu q
-    if (wide) k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0), nullptr);
-    else k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0), nullptr);
+    k_ad_g2p_adj_f<T><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0), nullptr, nearp);
     if (air) {
         // the air cell mask of this step, from its forward replay
         const uint8_t* airc = static_cast<const uint8_t*>(t->wk[W_AIRC]);
-        if (wide)
-            k_ad_g2p_adj_f<T, true><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4C), R.f(W_A0), airc);
-        else
-            k_ad_g2p_adj_f<T, false><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4C), R.f(W_A0), airc);
+        k_ad_g2p_adj_f<T><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4C), R.f(W_A0), airc, nearp);
     }
     const T cdu = alpha == (T)1 ? (T)1 : alpha;
     // wall rules then the two passes, transposed (B0 -> B1 -> T0 -> B1); the
