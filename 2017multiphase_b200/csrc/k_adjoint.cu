@@ -73,6 +73,7 @@ struct AdjTape {
     // distance
     bool air = false;
     uint8_t* phase = nullptr;
+    char* arena = nullptr;               // every step's recorded state, one allocation
     float* mass_w = nullptr;
     float* mass_a = nullptr;
     std::vector<float*> lsm, phia;
@@ -963,59 +964,107 @@ __global__ void k_ad_g2p_adj_p(Grid g, int np, const uint32_t* __restrict__ orde
 }
 // face side of the G2P transpose: q_f = sum of w_pf vgbar_p over the particles
 // whose interpolation stencil holds f. Those lie in cells [i-1,i] along the
-// face normal and [-1,1] across of their replay positions; the candidates come
-// from the recorded cell lists, so a face takes its candidates one cell wider
-// when a cell of that wider window holds a particle whose replay cell differs
-// from its recorded one (near[] of the core cells; with near null, every face
-// does). Membership is decided from the replay's own positions either way, and
-// a face's members appear in the same order in both windows.
+// face normal and [-1,1] across of their replay positions (the water splat's
+// window); the candidates come from the recorded cell lists, so a face takes
+// them one cell wider (the air splat's window) when near[] is set in the
+// 3x3x3 cells around its node, i.e. near a particle whose replay cell is not
+// its recorded one. Membership is decided from the replay's own positions, and
+// a face adds its members in (a, b, c, particle) order in either window.
+// A warp handles 32 nodes along k (i, j fixed), a thread a node's three
+// faces, with the candidates of each column (a, b) staged in shared memory
+// as in k_ad_p2g_w.
 template <class T>
-__global__ void k_ad_g2p_adj_f(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4,
-                               const T* __restrict__ vgs4, Fc<T> q, const uint8_t* __restrict__ cellmask,
-                               const uint8_t* __restrict__ near) {
-    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
-    MP_GRID_LOOP(t, tot) {
-        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
-        const int w = ax == 0 ? g.NX + 1 : g.NX, hh = ax == 1 ? g.NY + 1 : g.NY, d = ax == 2 ? g.NZ + 1 : g.NZ;
-        T acc = 0;
-        bool wide = near == nullptr;
-        if (!wide) {
-            for (int a = max(i - 1, 0); a <= min(ax == 0 ? i : i + 1, g.NX - 1) && !wide; a++)
-                for (int b = max(j - 1, 0); b <= min(ax == 1 ? j : j + 1, g.NY - 1) && !wide; b++)
-                    for (int cc = max(k - 1, 0); cc <= min(ax == 2 ? k : k + 1, g.NZ - 1); cc++)
-                        if (near[cid(g, a, b, cc)]) { wide = true; break; }
-        }
-        const int wd = wide ? 1 : 0;
-        const int a0 = i - 1 - wd, a1 = (ax == 0 ? i : i + 1) + wd, b0 = j - 1 - wd, b1 = (ax == 1 ? j : j + 1) + wd;
-        const int c0 = k - 1 - wd, c1 = (ax == 2 ? k : k + 1) + wd;
-        for (int a = a0; a <= a1; a++) {
-            if (a < 0 || a > g.NX - 1) continue;
-            for (int b = b0; b <= b1; b++) {
+__global__ void __launch_bounds__(256) k_ad_g2p_adj_w(Grid g, const uint32_t* __restrict__ off,
+                                                      const T* __restrict__ xs4, const T* __restrict__ vgs4, Fc<T> q,
+                                                      const uint8_t* __restrict__ cellmask,
+                                                      const uint8_t* __restrict__ near) {
+    constexpr int CAP = sizeof(T) == 4 ? 128 : 64;
+    __shared__ T sm_x[8][CAP][4];
+    __shared__ T sm_v[8][CAP][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const Tiles Tl = make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1);
+    MP_GRID_LOOP(t, Tl.threads()) {
+        int i, j, k;
+        const bool act = tile_ijk(Tl, t, i, j, k);
+        if (!__any_sync(0xffffffffu, act)) continue;
+        const bool hx = act && j < g.NY && k < g.NZ, hy = act && i < g.NX && k < g.NZ, hz = act && i < g.NX && j < g.NY;
+        bool wide = false;
+        if (act)
+            for (int a = max(i - 1, 0); a <= min(i + 1, g.NX - 1); a++)
+                for (int b = max(j - 1, 0); b <= min(j + 1, g.NY - 1); b++)
+                    for (int cc = max(k - 1, 0); cc <= min(k + 1, g.NZ - 1); cc++) wide = wide || near[cid(g, a, b, cc)];
+        // this lane's windows: along the normal [-LO, HI], across [-AC, AC]
+        const int LO = wide ? 2 : 1, HI = wide ? 1 : 0, AC = wide ? 2 : 1;
+        const int R = __reduce_max_sync(0xffffffffu, act ? AC : 1);
+        T qx = 0, qy = 0, qz = 0;
+        const int klo = max(k - AC, 0), khi = min(k + AC, g.NZ - 1), kzhi = min(k + HI, g.NZ - 1);
+        const int W0 = g.NX + 1, H1 = g.NY + 1, D2 = g.NZ + 1;
+        for (int di = -R; di <= R; di++) {
+            const int a = i + di;
+            if (a < 0 || a > g.NX - 1) continue;   // the same for the whole warp
+            const bool ax = hx && di >= -LO && di <= HI, inx = di >= -AC && di <= AC;
+            for (int dj = -R; dj <= R; dj++) {
+                const int b = j + dj;
                 if (b < 0 || b > g.NY - 1) continue;
-                for (int cc = c0; cc <= c1; cc++) {
-                    if (cc < 0 || cc > g.NZ - 1) continue;
-                    int c = cid(g, a, b, cc);
-                    if (cellmask && !cellmask[c]) continue;
-                    for (uint32_t s = off[c]; s < off[c + 1]; s++) {
-                        const T* r = xs4 + 4 * (size_t)s;
-                        T X = r[0] / (T)g.h, Y = r[1] / (T)g.h, Z = r[2] / (T)g.h;
-                        T px, py, pz; ipos(ax, X, Y, Z, px, py, pz);
-                        px = px < (T)0 ? (T)0 : (px > (T)w ? (T)w : px);
-                        py = py < (T)0 ? (T)0 : (py > (T)hh ? (T)hh : py);
-                        pz = pz < (T)0 ? (T)0 : (pz > (T)d ? (T)d : pz);
-                        int bi = (int)(px < (T)(w - 2) ? px : (T)(w - 2));
-                        int bj = (int)(py < (T)(hh - 2) ? py : (T)(hh - 2));
-                        int bk = (int)(pz < (T)(d - 2) ? pz : (T)(d - 2));
-                        int ei = i - bi, ej = j - bj, ek = k - bk;
-                        if (ei < 0 || ei > 1 || ej < 0 || ej > 1 || ek < 0 || ek > 1) continue;
-                        T fx = ei ? px - (T)bi : (T)(bi + 1) - px, fy = ej ? py - (T)bj : (T)(bj + 1) - py;
-                        T fz = ek ? pz - (T)bk : (T)(bk + 1) - pz;
-                        acc += fx * fy * fz * vgs4[4 * (size_t)s + ax];
+                const bool ay = hy && inx && dj >= -LO && dj <= HI;
+                const bool axc = ax && dj >= -AC && dj <= AC;
+                const bool azc = hz && inx && dj >= -AC && dj <= AC;
+                bool need = (axc || ay || azc) && klo <= khi;
+                const int cb = cid(g, a, b, 0);
+                if (need && cellmask) {
+                    bool any = false;
+                    for (int cc = klo; cc <= khi; cc++) any = any || cellmask[cb + cc];
+                    need = any;
+                }
+                if (!__any_sync(0xffffffffu, need)) continue;
+                uint32_t s0 = 0, s1 = 0, sz1 = 0;
+                if (need) {
+                    s0 = off[cb + klo]; s1 = off[cb + khi + 1];
+                    sz1 = azc ? off[cb + kzhi + 1] : s0;
+                }
+                const uint32_t A = __reduce_min_sync(0xffffffffu, need ? s0 : 0xffffffffu);
+                const uint32_t B = __reduce_max_sync(0xffffffffu, need ? s1 : 0u);
+                for (uint32_t c0 = A; c0 < B; c0 += CAP) {
+                    const uint32_t n = min(B - c0, (uint32_t)CAP);
+                    __syncwarp();
+                    for (uint32_t e = lane; e < n; e += 32) {
+                        const T* r = xs4 + 4 * (size_t)(c0 + e);
+                        const T* v = vgs4 + 4 * (size_t)(c0 + e);
+                        sm_x[warp][e][0] = r[0]; sm_x[warp][e][1] = r[1]; sm_x[warp][e][2] = r[2];
+                        sm_v[warp][e][0] = v[0]; sm_v[warp][e][1] = v[1]; sm_v[warp][e][2] = v[2];
+                    }
+                    __syncwarp();
+                    if (!need) continue;
+                    const uint32_t lo = max(s0, c0), hi = min(s1, c0 + n);
+                    for (uint32_t p = lo; p < hi; ++p) {
+                        const T X = sm_x[warp][p - c0][0] / (T)g.h, Y = sm_x[warp][p - c0][1] / (T)g.h;
+                        const T Z = sm_x[warp][p - c0][2] / (T)g.h;
+                        #pragma unroll
+                        for (int f = 0; f < 3; f++) {
+                            const bool on = f == 0 ? axc : (f == 1 ? ay : (azc && p < sz1));
+                            if (!on) continue;
+                            const int w = f == 0 ? W0 : g.NX, hh = f == 1 ? H1 : g.NY, d = f == 2 ? D2 : g.NZ;
+                            T px, py, pz; ipos(f, X, Y, Z, px, py, pz);
+                            px = px < (T)0 ? (T)0 : (px > (T)w ? (T)w : px);
+                            py = py < (T)0 ? (T)0 : (py > (T)hh ? (T)hh : py);
+                            pz = pz < (T)0 ? (T)0 : (pz > (T)d ? (T)d : pz);
+                            const int bi = (int)(px < (T)(w - 2) ? px : (T)(w - 2));
+                            const int bj = (int)(py < (T)(hh - 2) ? py : (T)(hh - 2));
+                            const int bk = (int)(pz < (T)(d - 2) ? pz : (T)(d - 2));
+                            const int ei = i - bi, ej = j - bj, ek = k - bk;
+                            if (ei < 0 || ei > 1 || ej < 0 || ej > 1 || ek < 0 || ek > 1) continue;
+                            const T fx = ei ? px - (T)bi : (T)(bi + 1) - px, fy = ej ? py - (T)bj : (T)(bj + 1) - py;
+                            const T fz = ek ? pz - (T)bk : (T)(bk + 1) - pz;
+                            const T term = fx * fy * fz * sm_v[warp][p - c0][f];
+                            if (f == 0) qx += term; else if (f == 1) qy += term; else qz += term;
+                        }
                     }
                 }
             }
         }
-        fsel(q, ax)[idx] = acc;
+        if (hx) q.x[fxi(g, i, j, k)] = qx;
+        if (hy) q.y[fyi(g, i, j, k)] = qy;
+        if (hz) q.z[fzi(g, i, j, k)] = qz;
     }
 }
 // splat transpose per particle over the faces whose window holds its cell
@@ -1328,18 +1377,10 @@ template <class T> __global__ void k_ad_from_double(long long n, const double* _
 void k_adj_free(MpCtx* c) {
     AdjTape* t = c->adj;
     if (!t) return;
-    for (auto* p : t->order) cudaFree(p);
-    for (auto* p : t->off) cudaFree(p);
-    for (auto* p : t->mark) cudaFree(p);
-    for (auto* p : t->phi) cudaFree(p);
-    for (auto* p : t->order_h) cudaFree(p);
-    for (auto* p : t->off_h) cudaFree(p);
-    for (auto* p : t->mark_h) cudaFree(p);
-    for (auto* p : t->lsm) cudaFree(p);
-    for (auto* p : t->phia) cudaFree(p);
+    // the per-step arrays point into the arena
     for (void* p : {(void*)t->x0, (void*)t->v0, (void*)t->mass, (void*)t->ids, (void*)t->ids2, (void*)t->nearest,
                     (void*)t->samples, (void*)t->s_off, (void*)t->T0, (void*)t->fixedheat, (void*)t->phase,
-                    (void*)t->mass_w, (void*)t->mass_a})
+                    (void*)t->mass_w, (void*)t->mass_a, (void*)t->arena})
         if (p) cudaFree(p);
     for (void* p : t->wk) if (p) cudaFree(p);
     delete t;
@@ -1425,24 +1466,31 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
                                        c->stream));
         }
     }
+    // every step's recorded state in one allocation (allocating per step in
+    // the loop costs more than the copies)
+    const auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t n = (size_t)g.n, snp = (size_t)np;
+    const size_t per = up(4 * snp) + up(4 * (n + 1)) + up(n) + up(4 * n) + (t->air ? 2 * up(4 * n) : 0) +
+                       (t->heat ? up(4 * snp) + up(4 * (n + 1)) + up(n) : 0);
+    MP_TRY(amalloc(c, &t->arena, per * (size_t)nsteps));
     for (int k = 0; k < nsteps; k++) {
+        char* slab = t->arena + per * (size_t)k;
+        auto carve = [&](size_t bytes) { char* q = slab; slab += up(bytes); return q; };
         MP_TRY(sorted_ids(c, t));
         MP_TRY(k_external_force(c));
         MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
-        uint32_t* ord; uint32_t* off; int8_t* mk; float* ph;
-        MP_TRY(amalloc(c, &ord, np)); t->order.push_back(ord);
-        MP_TRY(amalloc(c, &off, (size_t)g.n + 1)); t->off.push_back(off);
-        MP_TRY(amalloc(c, &mk, g.n)); t->mark.push_back(mk);
-        MP_TRY(amalloc(c, &ph, g.n)); t->phi.push_back(ph);
+        uint32_t* ord = reinterpret_cast<uint32_t*>(carve(4 * snp)); t->order.push_back(ord);
+        uint32_t* off = reinterpret_cast<uint32_t*>(carve(4 * (n + 1))); t->off.push_back(off);
+        int8_t* mk = reinterpret_cast<int8_t*>(carve(n)); t->mark.push_back(mk);
+        float* ph = reinterpret_cast<float*>(carve(4 * n)); t->phi.push_back(ph);
         MP_CUDA(c, cudaMemcpyAsync(ord, t->ids, sizeof(uint32_t) * np, cudaMemcpyDeviceToDevice, c->stream));
         MP_CUDA(c, cudaMemcpyAsync(off, c->cell_off, sizeof(uint32_t) * ((size_t)g.n + 1), cudaMemcpyDeviceToDevice, c->stream));
         MP_CUDA(c, cudaMemcpyAsync(mk, c->mark, g.n, cudaMemcpyDeviceToDevice, c->stream));
         MP_TRY(k_p2g(c));
         if (t->air) {
             // bubblesim's order: the air phase's extrapolation first
-            float* lm; float* pa;
-            MP_TRY(amalloc(c, &lm, g.n)); t->lsm.push_back(lm);
-            MP_TRY(amalloc(c, &pa, g.n)); t->phia.push_back(pa);
+            float* lm = reinterpret_cast<float*>(carve(4 * n)); t->lsm.push_back(lm);
+            float* pa = reinterpret_cast<float*>(carve(4 * n)); t->phia.push_back(pa);
             MP_CUDA(c, cudaMemcpyAsync(lm, c->lsmerge, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, c->stream));
             MP_TRY(k_sweep_phi(c, MP_TYPEAIR));
             MP_CUDA(c, cudaMemcpyAsync(pa, c->phiair, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, c->stream));
@@ -1468,10 +1516,9 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
             // the advected particles, a sort, then updateTemperature
             MP_TRY(k_levelset(c)); MP_TRY(k_sweep_ls_mark(c));
             MP_TRY(sorted_ids(c, t));
-            uint32_t* oh; uint32_t* fh; int8_t* mh;
-            MP_TRY(amalloc(c, &oh, np)); t->order_h.push_back(oh);
-            MP_TRY(amalloc(c, &fh, (size_t)g.n + 1)); t->off_h.push_back(fh);
-            MP_TRY(amalloc(c, &mh, g.n)); t->mark_h.push_back(mh);
+            uint32_t* oh = reinterpret_cast<uint32_t*>(carve(4 * snp)); t->order_h.push_back(oh);
+            uint32_t* fh = reinterpret_cast<uint32_t*>(carve(4 * (n + 1))); t->off_h.push_back(fh);
+            int8_t* mh = reinterpret_cast<int8_t*>(carve(n)); t->mark_h.push_back(mh);
             MP_CUDA(c, cudaMemcpyAsync(oh, t->ids, sizeof(uint32_t) * np, cudaMemcpyDeviceToDevice, c->stream));
             MP_CUDA(c, cudaMemcpyAsync(fh, c->cell_off, sizeof(uint32_t) * ((size_t)g.n + 1), cudaMemcpyDeviceToDevice,
                                        c->stream));
@@ -1842,11 +1889,12 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
         nearp = near;
     }
     // q = I^T vgbar on B0 (A0 for the air faces); ufbar = q, uoldbar = -cdu q
-    k_ad_g2p_adj_f<T><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0), nullptr, nearp);
+    const int nbw = mp_blocks(make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1).threads(), 256);
+    k_ad_g2p_adj_w<T><<<nbw, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), R.f(W_B0), nullptr, nearp);
     if (air) {
         // the air cell mask of this step, from its forward replay
         const uint8_t* airc = static_cast<const uint8_t*>(t->wk[W_AIRC]);
-        k_ad_g2p_adj_f<T><<<nbf, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4C), R.f(W_A0), airc, nearp);
+        k_ad_g2p_adj_w<T><<<nbw, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4C), R.f(W_A0), airc, nearp);
     }
     const T cdu = alpha == (T)1 ? (T)1 : alpha;
     // wall rules then the two passes, transposed (B0 -> B1 -> T0 -> B1); the
