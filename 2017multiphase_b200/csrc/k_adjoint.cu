@@ -1067,13 +1067,20 @@ __global__ void __launch_bounds__(256) k_ad_g2p_adj_w(Grid g, const uint32_t* __
         if (hz) q.z[fzi(g, i, j, k)] = qz;
     }
 }
+// per face ub/W of a splat (0 where the face took no weight): the factor every
+// particle of the face's window takes
+template <class T>
+__global__ void k_ad_ub_over_w(long long nf, const T* __restrict__ ub, const T* __restrict__ W, T* __restrict__ o) {
+    MP_GRID_LOOP(t, nf) o[t] = W[t] > (T)0 ? ub[t] / W[t] : (T)0;
+}
 // splat transpose per particle over the faces whose window holds its cell
 // (the particle's cell is the recorded one: window membership is frozen)
 template <class T, int PH>
 __global__ void k_ad_p2g_adj(Grid g, int np, const uint32_t* __restrict__ order, const T* __restrict__ x,
                              const T* __restrict__ va, const float* __restrict__ mass,
-                             const uint32_t* __restrict__ cellof, Fc<T> u, Fc<T> W, Fc<T> ub, T* __restrict__ vab,
+                             const uint32_t* __restrict__ cellof, Fc<T> u, Fc<T> ubw, T* __restrict__ vab,
                              T* __restrict__ xb) {
+    const T cker = (T)1.4f * (T)1.4f;
     const T scale = (T)1 / (T)g.h;
     // particles in sorted order, so neighbouring threads read neighbouring faces
     MP_GRID_LOOP(sl, np) {
@@ -1103,17 +1110,24 @@ __global__ void k_ad_p2g_adj(Grid g, int np, const uint32_t* __restrict__ order,
                         T dx = X - (T)gx, dy = Y - (T)gy, dz = Z - (T)gz;
                         T r2 = dx * dx + dy * dy + dz * dz;
                         // beyond the kernel radius the weight and its slope are zero
-                        if (!(r2 < (T)1.4f * (T)1.4f)) continue;
-                        int f = face_index(g, ax, fi, fj, fk);
-                        T Wf = fsel(W, ax)[f];
-                        if (!(Wf > (T)0)) continue;
-                        T k_ = sharpk(r2);
-                        T kd = sharpk_d(r2);
-                        if (k_ == (T)0 && kd == (T)0) continue;
-                        T u_b = fsel(ub, ax)[f];
-                        vb[ax] += u_b * m * k_ / Wf;
-                        T s = u_b * (pv - fsel(u, ax)[f]) / Wf * m * kd * (T)2 * scale;
-                        gxs += s * dx; gys += s * dy; gzs += s * dz;
+                        if (!(r2 < cker)) continue;
+                        const int f = face_index(g, ax, fi, fj, fk);
+                        // ub/W of the face (0 where the face took no weight)
+                        const T a = fsel(ubw, ax)[f];
+                        if (a == (T)0) continue;
+                        // the kernel c/r2 - 1 and its slope -c/r2^2 (zero below
+                        // the clamp at r2 = 1e-4) from one division
+                        T k_, kd;
+                        if (r2 > (T)0.0001f) {
+                            const T qv = cker / r2;
+                            k_ = qv - (T)1; kd = -qv / r2;
+                            if (!(k_ > (T)0)) continue;
+                        } else {
+                            k_ = cker / (T)0.0001f - (T)1; kd = (T)0;
+                        }
+                        vb[ax] += a * m * k_;
+                        const T sv = (pv - fsel(u, ax)[f]) * a * m * kd * (T)2 * scale;
+                        gxs += sv * dx; gys += sv * dy; gzs += sv * dz;
                     }
                 }
             }
@@ -1932,12 +1946,16 @@ template <class T> static int adj_step(const Replay<T>& R, int k, const T* x, co
     k_ad_sweepu_adj_s<T><<<nbf, 256, 0, s>>>(g, R.f(W_B2), R.f(W_B1), I.sel, I.sw);
     // upbar = that + uoldbar
     k_ad_axpy<T><<<nbf, 256, 0, s>>>(R.nf, -cdu, R.a(W_B0), R.a(W_B1));
-    // splat transposes (vabar += ..., xbar += ...)
+    // splat transposes (vabar += ..., xbar += ...), with ub/W per face on T0
+    // (A2 for the air faces)
+    k_ad_ub_over_w<T><<<nbf, 256, 0, s>>>(R.nf, R.a(W_B1), I.wt.x, R.a(W_T0));
     k_ad_p2g_adj<T, 0><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.va, air ? t->mass_w : t->mass, cellof, I.up,
-                                           I.wt, R.f(W_B1), R.a(W_VAB), xb);
-    if (air)
-        k_ad_p2g_adj<T, 1><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.va, t->mass_a, cellof, I.upa, I.wta,
-                                               R.f(W_A1), R.a(W_VAB), xb);
+                                           R.f(W_T0), R.a(W_VAB), xb);
+    if (air) {
+        k_ad_ub_over_w<T><<<nbf, 256, 0, s>>>(R.nf, R.a(W_A1), I.wta.x, R.a(W_A2));
+        k_ad_p2g_adj<T, 1><<<nbp, 256, 0, s>>>(g, R.np, t->order[k], x, I.va, t->mass_a, cellof, I.upa, R.f(W_A2),
+                                               R.a(W_VAB), xb);
+    }
     // external forces: vbar = dva/dv^T vabar
     if (air)
         k_ad_forces_adj<T><<<nbp, 256, 0, s>>>(R.np, t->phase, v, R.a(W_VAB), vb, (T)P.dt * (T)P.gravity_z,
