@@ -28,9 +28,13 @@ namespace {
 // sharp_kernel(r2, 1.4) is exactly zero once r2 exceeds 1.4^2, and a zero
 // weight adds +-0 to both sums, so such pairs are skipped, and the velocity is
 // read only when some face takes the particle.
+// A face triple whose 5x5x5-cell window touches no 4x4x4-cell brick holding an
+// air particle (the bit map of the last sort) has no pair: its faces take 0,
+// as the walk would give them.
 __global__ void __launch_bounds__(256, 4) k_p2g_air(Grid g, Cells cl, const float4* __restrict__ pos,
                                                     const float4* __restrict__ vel, float* __restrict__ ux,
-                                                    float* __restrict__ uy, float* __restrict__ uz) {
+                                                    float* __restrict__ uy, float* __restrict__ uz,
+                                                    const uint32_t* __restrict__ air_brick) {
     constexpr int R = 2;       // union window -R..R
     constexpr int HI = 1;      // upper bound along the face normal
     const Tiles T = make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1);
@@ -40,6 +44,25 @@ __global__ void __launch_bounds__(256, 4) k_p2g_air(Grid g, Cells cl, const floa
         int i, j, k; if (!tile_ijk(T, t, i, j, k)) continue;
         bool hx = (j < g.NY && k < g.NZ), hy = (i < g.NX && k < g.NZ), hz = (i < g.NX && j < g.NY);
         float wx = 0, sx = 0, wy = 0, sy = 0, wz = 0, sz = 0;
+        bool air_near = false;
+        {
+            const int bw = (g.NZ + 3) / 4, bh = (g.NY + 3) / 4;
+            const int bi0 = max(i - R, 0) >> 2, bi1 = min(i + R, g.NX - 1) >> 2;
+            const int bj0 = max(j - R, 0) >> 2, bj1 = min(j + R, g.NY - 1) >> 2;
+            const int bk0 = max(k - R, 0) >> 2, bk1 = min(k + R, g.NZ - 1) >> 2;
+            for (int bi = bi0; bi <= bi1 && !air_near; bi++)
+                for (int bj = bj0; bj <= bj1 && !air_near; bj++)
+                    for (int bk = bk0; bk <= bk1; bk++) {
+                        const int br = (bi * bh + bj) * bw + bk;
+                        if ((__ldg(air_brick + (br >> 5)) >> (br & 31)) & 1u) { air_near = true; break; }
+                    }
+        }
+        if (!air_near) {
+            if (hx) ux[fxi(g, i, j, k)] = 0.0f;
+            if (hy) uy[fyi(g, i, j, k)] = 0.0f;
+            if (hz) uz[fzi(g, i, j, k)] = 0.0f;
+            continue;
+        }
         const float3 gpx = mk3((float)i, (float)j + 0.5f, (float)k + 0.5f);
         const float3 gpy = mk3((float)i + 0.5f, (float)j, (float)k + 0.5f);
         const float3 gpz = mk3((float)i + 0.5f, (float)j + 0.5f, (float)k);
@@ -370,7 +393,8 @@ int k_p2g_faces(MpCtx* c, float** out, int which) {
         k_p2g_water<P2G_CAP><<<mp_blocks(tot, 256), 256, smem, c->stream>>>(g, cells_of(c), c->pos, c->vel, out[0], out[1], out[2]);
     }
     else
-        k_p2g_air<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g, cells_of(c), c->pos, c->vel, out[0], out[1], out[2]);
+        k_p2g_air<<<mp_blocks(tot, 256), 256, 0, c->stream>>>(g, cells_of(c), c->pos, c->vel, out[0], out[1], out[2],
+                                                              c->air_brick);
     c->launches++;
     MP_CHECK_LAUNCH(c);
     return MP_OK;
