@@ -153,11 +153,32 @@ __global__ void k_ad_nearest(Grid g, Cells cl, const float4* __restrict__ pos, c
         int i, j, k; getijk3(idx, g.NY, g.NZ, i, j, k);
         float h = g.h;
         float3 gp = (mk3((float)i, (float)j, (float)k) + mk3(0.5f, 0.5f, 0.5f)) * h;
-        float best = 6.25f * h * h;
+        const float cap = 6.25f * h * h;
+        // a bound from the 27 nearest cells first: a window cell (di,dj,dk)
+        // holds no particle closer than ((|d|-0.5)h)^2 summed over the axes
+        // (shrunk by 1e-4 relative against the rounding of d2), so the ones
+        // whose bound exceeds it cannot hold the minimum or a tie with it
+        float bound = cap;
+        for (int di = -1; di <= 1; di++) for (int dj = -1; dj <= 1; dj++) for (int dk = -1; dk <= 1; dk++) {
+            int a = i + di, b = j + dj, cc = k + dk;
+            if (a < 0 || a >= g.NX || b < 0 || b >= g.NY || cc < 0 || cc >= g.NZ) continue;
+            int c = cid(g, a, b, cc);
+            for (uint32_t s = cl.off[c]; s < cl.off[c + 1]; s++) {
+                float4 q = pos[s];
+                if (pflag(q) != MP_TYPEFLUID) continue;
+                float3 d = xyz(q) - gp;
+                bound = fminf(bound, dot(d, d));
+            }
+        }
+        // the fixed order of the +-2 box, first minimum kept
+        float best = cap;
         uint32_t who = NONE;
         for (int di = -2; di <= 2; di++) for (int dj = -2; dj <= 2; dj++) for (int dk = -2; dk <= 2; dk++) {
             int a = i + di, b = j + dj, cc = k + dk;
             if (a < 0 || a >= g.NX || b < 0 || b >= g.NY || cc < 0 || cc >= g.NZ) continue;
+            const float bx = di == 0 ? 0.f : ((float)abs(di) - 0.5f), by = dj == 0 ? 0.f : ((float)abs(dj) - 0.5f);
+            const float bz = dk == 0 ? 0.f : ((float)abs(dk) - 0.5f);
+            if ((bx * bx + by * by + bz * bz) * h * h * 0.9999f > bound) continue;
             int c = cid(g, a, b, cc);
             for (uint32_t s = cl.off[c]; s < cl.off[c + 1]; s++) {
                 float4 q = pos[s];
