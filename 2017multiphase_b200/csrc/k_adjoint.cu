@@ -266,51 +266,14 @@ template <int PH> struct SplatWin {
     static constexpr int LO = PH ? 2 : 1, HI = PH ? 1 : 0, AC = PH ? 2 : 1;
 };
 // splat: per face, the mass-weighted sharp-kernel average of the particles of
-// its window's cells, in the order of the reference's loops; the records hold
-// each particle's phase mass (0 for the other phase, which then adds nothing)
-template <class T, int PH>
-__global__ void k_ad_p2g(Grid g, const uint32_t* __restrict__ off, const T* __restrict__ xs4, const T* __restrict__ vs4,
-                         Fc<T> u, Fc<T> W, const uint8_t* __restrict__ cellmask) {
-    using Wn = SplatWin<PH>;
-    const long long tot = (long long)g.nfx + g.nfy + g.nfz;
-    const T scale = (T)1 / (T)g.h;
-    MP_GRID_LOOP(t, tot) {
-        int i, j, k, idx; const int ax = face_decode(g, t, i, j, k, idx);
-        float fx, fy, fz; face_pos(ax, i, j, k, fx, fy, fz);
-        T w = 0, s = 0;
-        const int a0 = i - (ax == 0 ? Wn::LO : Wn::AC), a1 = i + (ax == 0 ? Wn::HI : Wn::AC);
-        const int b0 = j - (ax == 1 ? Wn::LO : Wn::AC), b1 = j + (ax == 1 ? Wn::HI : Wn::AC);
-        const int c0 = k - (ax == 2 ? Wn::LO : Wn::AC), c1 = k + (ax == 2 ? Wn::HI : Wn::AC);
-        for (int a = a0; a <= a1; a++) {
-            if (a < 0 || a > g.NX - 1) continue;
-            for (int b = b0; b <= b1; b++) {
-                if (b < 0 || b > g.NY - 1) continue;
-                for (int cc = c0; cc <= c1; cc++) {
-                    if (cc < 0 || cc > g.NZ - 1) continue;
-                    int c = cid(g, a, b, cc);
-                    if (cellmask && !cellmask[c]) continue;
-                    for (uint32_t q = off[c]; q < off[c + 1]; q++) {
-                        const T* r = xs4 + 4 * (size_t)q;
-                        if (r[3] == (T)0) continue;   // adds +0 to both sums
-                        T dx = r[0] * scale - (T)fx, dy = r[1] * scale - (T)fy, dz = r[2] * scale - (T)fz;
-                        T r2 = dx * dx + dy * dy + dz * dz;
-                        T wp = r[3] * sharpk(r2);
-                        w += wp; s += wp * vs4[4 * (size_t)q + ax];
-                    }
-                }
-            }
-        }
-        fsel(W, ax)[idx] = w;
-        fsel(u, ax)[idx] = w > (T)0 ? s / w : (T)0;
-    }
-}
-// The same splat with a warp per 32 nodes along k (i, j fixed), a thread per
-// node's three faces: for each column (a, b) of the window the particles of
-// the warp's cells along k are one contiguous range of the recorded order; the
-// warp stages it in shared memory CAP records at a time with coalesced loads,
-// and each lane walks its own part. A face sums the same pairs in the same
-// order as k_ad_p2g (a pair beyond the kernel radius adds +0 there and is
-// skipped here), so the fields are identical.
+// its window's cells, in the order of the reference's loops (cells a, b, c
+// ascending, then the particles of a cell); the records hold each particle's
+// phase mass (0 for the other phase, which then adds nothing), and a pair
+// beyond the kernel radius (weight 0) is skipped. A warp handles 32 nodes
+// along k (i, j fixed), a thread a node's three faces: for each column (a, b)
+// of the window the particles of the warp's cells along k are one contiguous
+// range of the recorded order; the warp stages it in shared memory CAP
+// records at a time with coalesced loads, and each lane walks its own part.
 template <class T, int PH>
 __global__ void __launch_bounds__(256) k_ad_p2g_w(Grid g, const uint32_t* __restrict__ off,
                                                   const T* __restrict__ xs4, const T* __restrict__ vs4, Fc<T> u,
