@@ -240,6 +240,24 @@ __device__ __forceinline__ float sweepu_face(const Grid& g, const float* __restr
     float res = in[idx];
     const int e = AX == 0 ? i : (AX == 1 ? j : k), n = AX == 0 ? g.NX : (AX == 1 ? g.NY : g.NZ);
     if (!(e > 1 && e < n - 1 && mark[c0] != fl && mark[c1] != fl)) return res;
+    // A face that is +0, with every neighbour face an octant can read (along
+    // the normal, and across within the grid) +0 as well, stays +0 whatever
+    // octant wins: the weights are non-negative, so the average is +0 too.
+    // Most faces far from the phase (the air field inside the liquid) are so.
+    if (__float_as_uint(res) == 0u) {
+        auto fz = [&](int a, int b, int c) {
+            const float v = AX == 0 ? in[fxi(g, a, b, c)] : (AX == 1 ? in[fyi(g, a, b, c)] : in[fzi(g, a, b, c)]);
+            return __float_as_uint(v) == 0u;
+        };
+        bool zero = true;
+        #pragma unroll
+        for (int d = -1; d <= 1; d += 2) {
+            if (AX == 0 || (i + d >= 0 && i + d <= g.NX - 1)) zero = zero && fz(i + d, j, k);
+            if (AX == 1 || (j + d >= 0 && j + d <= g.NY - 1)) zero = zero && fz(i, j + d, k);
+            if (AX == 2 || (k + d >= 0 && k + d <= g.NZ - 1)) zero = zero && fz(i, j, k + d);
+        }
+        if (zero) return res;
+    }
     const float l0 = ls[c0], l1 = ls[c1];
     // the two cross axes (p, q) of this face axis, in the order the weights are named
     const int sP = AX == 0 ? sJ : sI, sQ = AX == 2 ? sJ : 1;
