@@ -150,7 +150,9 @@ def workload_config(p, npart0, seed, world):
                         f"constant-coefficient projection (the reference's; coef_mode ref), "
                         f"CG rel 1e-6, marching cubes every step",
             "grid": p.nx, "particles": int(npart0), "seed": seed,
-            "l2": "inputs larger than L2 (particle streams alone are ~5 GB)",
+            "l2": (f"inputs larger than L2 (the three particle streams alone are {48 * npart0 / 1e9:.1f} GB)"
+                   if 48 * npart0 > 126e6 else
+                   f"inputs smaller than L2 ({48 * npart0 / 1e6:.0f} MB of particle streams): a reduced grid"),
             "parallelism": f"replicas x{world}"}
 
 
