@@ -260,3 +260,20 @@ def test_heat_autograd_and_fp32_against_fp64(mp):
     rel = float((g32 - g64).norm() / g64.norm())
     assert rel <= 5e-2, f"FP32 heat gradient rel err {rel:.3e}"
     sim.close()
+
+
+def test_replay_reproduces_the_engine_run(mp):
+    """The FP32 replay of the recorded FLUID program runs the engine's
+    arithmetic in the engine's order, so after four steps its final state is
+    the engine's own, bit for bit (mp_adj_order maps the engine's slots)."""
+    import torch
+    sim, v0 = _setup(mp, 32, 4, 2)
+    x0 = sim._x0_recorded
+    parts = sim.download_particles()
+    ids = sim.adj_order().cpu().numpy()
+    xe = np.empty_like(parts["pos"]); ve = np.empty_like(parts["vel"])
+    xe[ids] = parts["pos"]; ve[ids] = parts["vel"]
+    xT, vT = sim.adj_forward(x0, v0, mp.PREC_MIXED)
+    xT = xT.cpu().numpy().astype(np.float32); vT = vT.cpu().numpy().astype(np.float32)
+    assert np.array_equal(xT, xe) and np.array_equal(vT, ve)
+    sim.close()
