@@ -77,6 +77,14 @@ struct AdjTape {
     float* mass_w = nullptr;
     float* mass_a = nullptr;
     std::vector<float*> lsm, phia;
+    // the engine's projection of each step (its right-hand side and pressure),
+    // kept when the engine's solve is the one the FP32 replay runs (mixed
+    // precision, the reference's coefficients, no refinement or periodic true
+    // residual): a replay step whose right-hand side equals the engine's bit
+    // for bit takes the engine's pressure instead of solving again (the solve
+    // is deterministic, so it would give the same)
+    bool eng = false;
+    std::vector<float*> eng_b, eng_p;
     // replay / adjoint work, sized for `wesz`-byte elements
     size_t wesz = 0;
     int wk_ns = 0;                       // samples the work was sized for
@@ -192,6 +200,14 @@ __global__ void k_ad_nearest(Grid g, Cells cl, const float4* __restrict__ pos, c
     }
 }
 
+// raises *flag when a and b differ in some bit
+__global__ void k_ad_differ(int n, const float* __restrict__ a, const float* __restrict__ b, uint32_t* flag) {
+    MP_GRID_LOOP(i, n) {
+        const bool d = __float_as_uint(a[i]) != __float_as_uint(b[i]);
+        if (__any_sync(__activemask(), d) && (threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1))
+            atomicOr(flag, 1u);
+    }
+}
 // ---- replay of the continuous part ----------------------------------------------
 template <class T>
 __global__ void k_ad_gravity(int np, const T* __restrict__ v, T* __restrict__ va, T dtg) {
@@ -1468,8 +1484,10 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     // the loop costs more than the copies)
     const auto up = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t n = (size_t)g.n, snp = (size_t)np;
+    t->eng = P.precision == MP_PREC_MIXED && P.coef_mode == MP_COEF_REF && P.cg_refine_tol == 0.0f &&
+             P.cg_true_residual_every == 0;
     const size_t per = up(4 * snp) + up(4 * (n + 1)) + up(n) + up(4 * n) + (t->air ? 2 * up(4 * n) : 0) +
-                       (t->heat ? up(4 * snp) + up(4 * (n + 1)) + up(n) : 0);
+                       (t->heat ? up(4 * snp) + up(4 * (n + 1)) + up(n) : 0) + (t->eng ? 2 * up(4 * n) : 0);
     MP_TRY(amalloc(c, &t->arena, per * (size_t)nsteps));
     for (int k = 0; k < nsteps; k++) {
         char* slab = t->arena + per * (size_t)k;
@@ -1501,6 +1519,12 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
         MP_TRY(k_set_boundary_u(c, MP_TYPEFLUID));
         int st = k_project(c, nullptr, nullptr);
         if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+        if (t->eng) {
+            float* eb = reinterpret_cast<float*>(carve(4 * n)); t->eng_b.push_back(eb);
+            float* ep = reinterpret_cast<float*>(carve(4 * n)); t->eng_p.push_back(ep);
+            MP_CUDA(c, cudaMemcpyAsync(eb, c->divg, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+            MP_CUDA(c, cudaMemcpyAsync(ep, c->press, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
+        }
         if (t->air) MP_TRY(k_sweep_u(c, MP_TYPEAIR));
         MP_TRY(k_sweep_u(c, MP_TYPEFLUID));
         if (t->air) MP_TRY(k_set_boundary_u(c, MP_TYPEAIR));
@@ -1815,10 +1839,26 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     MP_CHECK_LAUNCH(c);
     T* pk = R.a(W_PST) + (size_t)k * g.n;
     if (solve) {
-        int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
-        int it = 0; double res = 0;
-        int st = k_cg_solve(c, t->mark[k], pk, R.a(W_CB), maxit, mode, tol, &it, &res);
-        if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+        bool same = false;
+        if constexpr (sizeof(T) == sizeof(float)) {
+            if (t->eng) {
+                uint32_t* flag = static_cast<uint32_t*>(t->wk[W_FLAG]) + 1;
+                MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
+                k_ad_differ<<<nbc, 256, 0, s>>>(g.n, reinterpret_cast<const float*>(R.a(W_CB)), t->eng_b[k], flag);
+                uint32_t differ = 1;
+                MP_CUDA(c, cudaMemcpyAsync(&differ, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                MP_CUDA(c, cudaStreamSynchronize(s));
+                same = differ == 0;
+                if (same)
+                    MP_CUDA(c, cudaMemcpyAsync(pk, t->eng_p[k], sizeof(float) * g.n, cudaMemcpyDeviceToDevice, s));
+            }
+        }
+        if (!same) {
+            int mode, maxit; float tol; cg_tol_of<T>(c, mode, tol, maxit);
+            int it = 0; double res = 0;
+            int st = k_cg_solve(c, t->mark[k], pk, R.a(W_CB), maxit, mode, tol, &it, &res);
+            if (st != MP_OK && st != MP_ERR_NOCONVERGE) return st;
+        }
     }
     k_ad_subgrad<T><<<nbf, 256, 0, s>>>(g, pk, I.ue, R.f(W_UPROJ));
     if (air) {
