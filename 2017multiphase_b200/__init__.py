@@ -690,10 +690,12 @@ class Sim:
         return int(self.lib.mp_launch_count(self.ctx))
 
     def work_counts(self) -> Dict[str, int]:
-        """mp_work_counts: sorts that reordered / found the order, CG iterations."""
-        a = (C.c_int64 * 3)()
-        _check(self.lib.mp_work_counts(self.ctx, a, 3), self.ctx)
-        return {"sort_full": int(a[0]), "sort_fast": int(a[1]), "cg_iters": int(a[2])}
+        """mp_work_counts: sorts that reordered / found the order, CG iterations,
+        reverse sweeps from the engine's states / after a full replay."""
+        a = (C.c_int64 * 5)()
+        _check(self.lib.mp_work_counts(self.ctx, a, 5), self.ctx)
+        return {"sort_full": int(a[0]), "sort_fast": int(a[1]), "cg_iters": int(a[2]),
+                "adj_engine": int(a[3]), "adj_replay": int(a[4])}
 
     def stream_handle(self) -> int:
         s = C.c_void_p()

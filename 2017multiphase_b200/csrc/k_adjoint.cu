@@ -85,6 +85,13 @@ struct AdjTape {
     // is deterministic, so it would give the same)
     bool eng = false;
     std::vector<float*> eng_b, eng_p;
+    // the engine's state (positions, velocities in recording order) at the
+    // start of every segment after the first and at the end: at the recorded
+    // inputs the FP32 replay reproduces it bit for bit, so a gradient there
+    // needs no first replay over all steps (each segment's replay checks that
+    // it ends on the engine's state)
+    float* eng_xs = nullptr;
+    float* eng_vs = nullptr;
     // replay / adjoint work, sized for `wesz`-byte elements
     size_t wesz = 0;
     int wk_ns = 0;                       // samples the work was sized for
@@ -1394,7 +1401,7 @@ void k_adj_free(MpCtx* c) {
     // the per-step arrays point into the arena
     for (void* p : {(void*)t->x0, (void*)t->v0, (void*)t->mass, (void*)t->ids, (void*)t->ids2, (void*)t->nearest,
                     (void*)t->samples, (void*)t->s_off, (void*)t->T0, (void*)t->fixedheat, (void*)t->phase,
-                    (void*)t->mass_w, (void*)t->mass_a, (void*)t->arena})
+                    (void*)t->mass_w, (void*)t->mass_a, (void*)t->arena, (void*)t->eng_xs, (void*)t->eng_vs})
         if (p) cudaFree(p);
     for (void* p : t->wk) if (p) cudaFree(p);
     delete t;
@@ -1489,7 +1496,19 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     const size_t per = up(4 * snp) + up(4 * (n + 1)) + up(n) + up(4 * n) + (t->air ? 2 * up(4 * n) : 0) +
                        (t->heat ? up(4 * snp) + up(4 * (n + 1)) + up(n) : 0) + (t->eng ? 2 * up(4 * n) : 0);
     MP_TRY(amalloc(c, &t->arena, per * (size_t)nsteps));
+    const int nseg = (nsteps + every - 1) / every;
+    if (t->eng && !t->heat) {
+        MP_TRY(amalloc(c, &t->eng_xs, 3 * snp * (size_t)nseg));
+        MP_TRY(amalloc(c, &t->eng_vs, 3 * snp * (size_t)nseg));
+    }
+    auto eng_state = [&](int e) -> int {
+        k_ad_snapshot<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->pos, c->vel, t->eng_xs + 3 * snp * e,
+                                                                 t->eng_vs + 3 * snp * e, t->mass);
+        ADJ_LAUNCH(c);
+        return MP_OK;
+    };
     for (int k = 0; k < nsteps; k++) {
+        if (t->eng_xs && k > 0 && k % every == 0) MP_TRY(eng_state(k / every - 1));
         char* slab = t->arena + per * (size_t)k;
         auto carve = [&](size_t bytes) { char* q = slab; slab += up(bytes); return q; };
         MP_TRY(sorted_ids(c, t));
@@ -1550,6 +1569,7 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
         }
         c->S.frame++;
     }
+    if (t->eng_xs) MP_TRY(eng_state(nseg - 1));
     // nearest particle of each cell at the end (cells from the last sort)
     k_ad_nearest<<<mp_blocks(g.n, 256), 256, 0, c->stream>>>(g, Cells{c->cell_off, c->tmask}, c->pos, t->ids, t->nearest);
     ADJ_LAUNCH(c);
@@ -1797,7 +1817,7 @@ template <class T> static int heat_adj(const Replay<T>& R, int k, const T* x1, c
 // The pressure solve's result is stored in pst (first replay) or copied from
 // it (segment replays): the inputs are the same bit for bit, so is the result.
 template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, const T* v, T* xo, T* vo,
-                                       const T* Tin, T* Tout, const Inter<T>& I0, bool solve) {
+                                       const T* Tin, T* Tout, const Inter<T>& I0, bool solve, bool splat) {
     MpCtx* c = R.c; AdjTape* t = R.t; const Grid& g = R.g;
     const Inter<T> I = R.with_splat(I0, k);
     cudaStream_t s = c->stream;
@@ -1815,7 +1835,7 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     // the splats (kept per step: the replays after the first read them back);
     // each splat stays as it is through the step and is its FLIP old field
     const int nbw = mp_blocks(make_tiles(g.NX + 1, g.NY + 1, g.NZ + 1).threads(), 256);
-    if (solve) {
+    if (splat) {
         k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, air ? t->mass_w : t->mass, R.a(W_S4A),
                                                 R.a(W_S4B));
         k_ad_p2g_w<T, 0><<<nbw, 256, 0, s>>>(g, t->off[k], R.a(W_S4A), R.a(W_S4B), I.up, I.wt, nullptr);
@@ -1823,7 +1843,7 @@ template <class T> static int fwd_step(const Replay<T>& R, int k, const T* x, co
     if (air) {
         uint8_t* airc = static_cast<uint8_t*>(t->wk[W_AIRC]);
         k_ad_air_cells<<<nbc, 256, 0, s>>>(g.n, t->off[k], t->order[k], t->phase, airc);
-        if (solve) {
+        if (splat) {
             k_ad_slot_gather<T><<<nbp, 256, 0, s>>>(R.np, t->order[k], x, I.va, t->mass_a, R.a(W_S4C), R.a(W_S4B));
             k_ad_p2g_w<T, 1><<<nbw, 256, 0, s>>>(g, t->off[k], R.a(W_S4C), R.a(W_S4B), I.upa, I.wta, airc);
         }
@@ -2021,7 +2041,18 @@ struct AdjIO {
     double* T0b = nullptr;
 };
 
-template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
+// bit patterns of a and b differ somewhere (*flag raised); T float
+template <class T>
+__global__ void k_ad_differ_t(long long n, const T* __restrict__ a, const float* __restrict__ b, uint32_t* flag) {
+    MP_GRID_LOOP(i, n) {
+        const bool d = __float_as_uint((float)a[i]) != __float_as_uint(b[i]);
+        if (__any_sync(__activemask(), d) && (threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1))
+            atomicOr(flag, 1u);
+    }
+}
+
+template <class T> static int adj_run(MpCtx* c, const AdjIO& io, bool allow_engine = true);
+template <class T> static int adj_run(MpCtx* c, const AdjIO& io, bool allow_engine) {
     AdjTape* t = c->adj;
     if (!t) { c->err = "adjoint: record first (mp_adj_record)"; return MP_ERR_STATE; }
     if (io.loss && !t->nsamples) { c->err = "adjoint: no target samples (mp_adj_set_targets)"; return MP_ERR_STATE; }
@@ -2047,7 +2078,33 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
     const int E = t->every, nseg = (t->nsteps + E - 1) / E;
     std::vector<T*> ckx(nseg), ckv(nseg), ckT(nseg, nullptr);
     const Inter<T> scratch = R.inter(0);
-    for (int k = 0; k < t->nsteps; k++) {
+    // for a gradient at the recorded inputs, the engine's states stand in for
+    // the first replay: the segment starts and the final state come from the
+    // recording, each step's pressure is the engine's, and the splats are
+    // formed when a segment is replayed, which is checked against the
+    // engine's state at its end
+    const bool engine = allow_engine && io.reverse && sizeof(T) == sizeof(float) && t->eng_xs && !io.x0 && !io.v0 &&
+                        !t->heat;
+    const size_t sn = (size_t)c->G.n;
+    if (engine) {
+        for (int sgi = 0; sgi < nseg; sgi++) {
+            ckx[sgi] = R.seg_x(sgi); ckv[sgi] = R.seg_v(sgi);
+            if (sgi == 0) {
+                MP_CUDA(c, cudaMemcpyAsync(ckx[0], x, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
+                MP_CUDA(c, cudaMemcpyAsync(ckv[0], v, sizeof(T) * np3, cudaMemcpyDeviceToDevice, s));
+            } else {
+                k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->eng_xs + (size_t)np3 * (sgi - 1), ckx[sgi]);
+                k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->eng_vs + (size_t)np3 * (sgi - 1), ckv[sgi]);
+            }
+        }
+        k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->eng_xs + (size_t)np3 * (nseg - 1), x);
+        k_ad_from_float<T><<<nb3, 256, 0, s>>>(np3, t->eng_vs + (size_t)np3 * (nseg - 1), v);
+        for (int k = 0; k < t->nsteps; k++)
+            MP_CUDA(c, cudaMemcpyAsync(R.a(W_PST) + (size_t)k * sn, t->eng_p[k], sizeof(float) * sn,
+                                       cudaMemcpyDeviceToDevice, s));
+        MP_CHECK_LAUNCH(c);
+    }
+    for (int k = 0; k < t->nsteps && !engine; k++) {
         if (k % E == 0) {
             int sgi = k / E;
             ckx[sgi] = R.seg_x(sgi); ckv[sgi] = R.seg_v(sgi);
@@ -2058,7 +2115,7 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
                 MP_CUDA(c, cudaMemcpyAsync(ckT[sgi], Tc, sizeof(T) * t->np, cudaMemcpyDeviceToDevice, s));
             }
         }
-        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, Tc, Tn, scratch, true));
+        MP_TRY(fwd_step<T>(R, k, x, v, xn, vn, Tc, Tn, scratch, true, true));
         std::swap(x, xn); std::swap(v, vn); std::swap(Tc, Tn);
     }
     if (io.xT) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, x, io.xT);
@@ -2110,13 +2167,26 @@ template <class T> static int adj_run(MpCtx* c, const AdjIO& io) {
         // is deterministic, so it rewrites the same next state.
         const Inter<T> I = R.inter(0);
         for (int j = 0; j < len; j++)
-            MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), I, false));
+            MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), I, false, engine));
+        if (engine) {
+            // the segment's replay must end on the engine's state; if it does
+            // not, the gradient is taken again with the first replay
+            uint32_t* flag = static_cast<uint32_t*>(t->wk[W_FLAG]) + 2;
+            MP_CUDA(c, cudaMemsetAsync(flag, 0, sizeof(uint32_t), s));
+            k_ad_differ_t<T><<<nb3, 256, 0, s>>>(np3, xs(len), t->eng_xs + (size_t)np3 * sg, flag);
+            k_ad_differ_t<T><<<nb3, 256, 0, s>>>(np3, vs(len), t->eng_vs + (size_t)np3 * sg, flag);
+            uint32_t differ = 1;
+            MP_CUDA(c, cudaMemcpyAsync(&differ, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            MP_CUDA(c, cudaStreamSynchronize(s));
+            if (differ) return adj_run<T>(c, io, false);
+        }
         for (int j = len - 1; j >= 0; j--) {
             if (j < len - 1)
-                MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), I, false));
+                MP_TRY(fwd_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), vs(j + 1), Ts(j), Ts(j + 1), I, false, false));
             MP_TRY(adj_step<T>(R, k0 + j, xs(j), vs(j), xs(j + 1), Ts(j), I, xb, vb, Tb));
         }
     }
+    c->work[engine ? MP_WC_ADJ_ENGINE : MP_WC_ADJ_REPLAY]++;
     if (io.v0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, vb, io.v0b);
     if (io.x0b) k_ad_to_double<T><<<nb3, 256, 0, s>>>(np3, xb, io.x0b);
     if (io.T0b && t->heat) k_ad_to_double<T><<<nb1, 256, 0, s>>>(t->np, Tb, io.T0b);

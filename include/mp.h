@@ -620,11 +620,16 @@ int64_t mp_launch_count(void* ctx);
  * of the measurement: particle sorts that reordered the particles, sorts
  * that found them already in cell order (keys and ranges only), and CG
  * iterations performed (pressure and heat solves; the launches of an
- * iteration batch after the stop test are not iterations). */
+ * iteration batch after the stop test are not iterations); and the adjoint's
+ * reverse sweeps that took the engine's recorded states in place of a first
+ * replay (a gradient at the recorded inputs) and those that replayed every
+ * step first. `n` may be smaller than MP_WC_COUNT. */
 #define MP_WC_SORT_FULL  0
 #define MP_WC_SORT_FAST  1
 #define MP_WC_CG_ITERS   2
-#define MP_WC_COUNT      3
+#define MP_WC_ADJ_ENGINE 3
+#define MP_WC_ADJ_REPLAY 4
+#define MP_WC_COUNT      5
 int mp_work_counts(void* ctx, int64_t* counts, int n);
 
 #ifdef __cplusplus

@@ -277,3 +277,22 @@ def test_replay_reproduces_the_engine_run(mp):
     xT = xT.cpu().numpy().astype(np.float32); vT = vT.cpu().numpy().astype(np.float32)
     assert np.array_equal(xT, xe) and np.array_equal(vT, ve)
     sim.close()
+
+
+def test_gradient_at_the_recorded_inputs_from_the_engine_states(mp):
+    """A gradient at the recorded inputs (NULL initial state) takes its
+    segment starts, final state and pressures from the engine's recorded run
+    instead of a first replay; it equals the gradient from explicit inputs
+    (the full replay) bit for bit, for several checkpoint intervals."""
+    import torch
+    for every in (8, 3):
+        sim, v0 = _setup(mp, 32, 8, every)
+        w0 = sim.work_counts()
+        L1, g1 = sim.adj_gradient(None, mp.PREC_MIXED)
+        w1 = sim.work_counts()
+        L2, g2 = sim.adj_gradient(v0, mp.PREC_MIXED)
+        w2 = sim.work_counts()
+        assert w1["adj_engine"] == w0["adj_engine"] + 1 and w1["adj_replay"] == w0["adj_replay"]
+        assert w2["adj_replay"] == w1["adj_replay"] + 1
+        assert L1 == L2 and torch.equal(g1, g2)
+        sim.close()

@@ -174,3 +174,18 @@ def test_non_cubic_grid(mp):
         ad = float((x0b * d).sum())
         assert abs(fd - ad) <= 1e-4 * max(abs(fd), abs(ad)), f"x direction {i}: fd {fd:.9e} adjoint {ad:.9e}"
     sim.close()
+
+
+def test_gradient_at_the_recorded_inputs_from_the_engine_states(mp):
+    """The two-phase program: the gradient at the recorded inputs, from the
+    engine's recorded states, equals the one from the full replay bit for
+    bit."""
+    import torch
+    sim, x0, v0 = _setup(mp, 1, 32, 4, 2, 2017001, 0.45)
+    w0 = sim.work_counts()
+    L1, g1 = sim.adj_gradient(None, mp.PREC_MIXED)
+    w1 = sim.work_counts()
+    L2, g2 = sim.adj_gradient(v0, mp.PREC_MIXED)
+    assert w1["adj_engine"] == w0["adj_engine"] + 1 and w1["adj_replay"] == w0["adj_replay"]
+    assert L1 == L2 and torch.equal(g1, g2)
+    sim.close()
