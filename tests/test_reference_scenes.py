@@ -14,8 +14,9 @@ import pytest
 
 from conftest import ROOT
 
-# the reference's source directory (MP_REFERENCE_SRC, as oracle/make_refhost.py reads it)
-SPRAY_CPP = os.path.join(os.environ.get("MP_REFERENCE_SRC", "/root/reference/Multiphase/Multiphase"), "spray.cpp")
+# the reference's source directory: the one the oracle's recipe compiles from
+from oracle.make_refhost import DEFAULT_SRC  # noqa: E402
+SPRAY_CPP = os.path.join(DEFAULT_SRC, "spray.cpp")
 
 # reference member -> mp_params field (p) or mp_scene_info field (i)
 PARAM = {
