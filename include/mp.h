@@ -558,7 +558,13 @@ int mp_set_output(void* ctx, const mp_output* out);
  * recorded ones) and returns L; mp_adj_gradient also writes dL/dv0 (device,
  * double xyz). precision: MP_PREC_MIXED replays in FP32 (CG dots in FP64),
  * MP_PREC_FP64 in FP64 with a 1e-13 relative CG stop. States are kept every
- * `checkpoint_every` steps and recomputed segment by segment backwards. */
+ * `checkpoint_every` steps and recomputed segment by segment backwards.
+ * Device memory: the recording holds, per step, the sort order (4 B per
+ * particle) and a few cell fields (~22 B per cell, ~30 B with AIR, plus 8 B
+ * per cell for the engine's projection in the mixed form) and, per segment,
+ * the engine's state (24 B per particle); a gradient in FP32 holds the
+ * checkpoints and one segment's states (24 B per particle each) and one
+ * step's intermediates. */
 int mp_adj_record(void* ctx, int nsteps, int checkpoint_every);
 /* The recorded program as a differentiable map of the particles' initial
  * state to their final state, (x0, v0) -> (xT, vT), with the general
