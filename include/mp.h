@@ -560,8 +560,8 @@ int mp_set_output(void* ctx, const mp_output* out);
  * MP_PREC_FP64 in FP64 with a 1e-13 relative CG stop. States are kept every
  * `checkpoint_every` steps and recomputed segment by segment backwards.
  * Device memory: the recording holds, per step, the sort order (4 B per
- * particle) and a few cell fields (~22 B per cell, ~30 B with AIR, plus 8 B
- * per cell for the engine's projection in the mixed form) and, per segment,
+ * particle) and cell fields (9 B per cell, 17 B with AIR, another 8 B for the
+ * engine's projection in the mixed form, 9 B with the heat stage) and, per segment,
  * the engine's state (24 B per particle); a gradient in FP32 holds the
  * checkpoints and one segment's states (24 B per particle each) and one
  * step's intermediates. */
