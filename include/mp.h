@@ -561,7 +561,8 @@ int mp_set_output(void* ctx, const mp_output* out);
  * `checkpoint_every` steps and recomputed segment by segment backwards.
  * Device memory: the recording holds, per step, the sort order (4 B per
  * particle) and cell fields (9 B per cell, 17 B with AIR, another 8 B for the
- * engine's projection in the mixed form, 9 B with the heat stage) and, per segment,
+ * engine's projection in the mixed form; the heat stage adds its own sort:
+ * 4 B per particle and 5 B per cell) and, per segment,
  * the engine's state (24 B per particle); a gradient in FP32 holds the
  * checkpoints and one segment's states (24 B per particle each) and one
  * step's intermediates. */
