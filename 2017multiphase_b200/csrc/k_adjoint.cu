@@ -995,8 +995,8 @@ __global__ void __launch_bounds__(256) k_ad_g2p_adj_w(Grid g, const uint32_t* __
         const bool act = tile_ijk(Tl, t, i, j, k);
         if (!__any_sync(0xffffffffu, act)) continue;
         const bool hx = act && j < g.NY && k < g.NZ, hy = act && i < g.NX && k < g.NZ, hz = act && i < g.NX && j < g.NY;
-        bool wide = false;
-        if (act)
+        bool wide = near == nullptr;   // no map: every face takes the wider window
+        if (act && near)
             for (int a = max(i - 1, 0); a <= min(i + 1, g.NX - 1); a++)
                 for (int b = max(j - 1, 0); b <= min(j + 1, g.NY - 1); b++)
                     for (int cc = max(k - 1, 0); cc <= min(k + 1, g.NZ - 1); cc++) wide = wide || near[cid(g, a, b, cc)];
