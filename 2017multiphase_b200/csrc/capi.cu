@@ -36,7 +36,7 @@ static void free_all(MpCtx* c) {
                     c->gx, c->gy, c->gz, c->gxa, c->gya, c->gza, c->sf, c->Tp, c->Tp_save, c->Tp_old, c->fixedheat,
                     c->cell_tmp, c->mark, c->mark_tmp, c->cg_r, c->cg_p, c->cg_z, c->cg64, c->red, c->scal, c->red_count,
                     c->pos, c->vel, c->heat, c->pos2, c->vel2, c->heat2, c->pdens, c->pprs, c->pscr, c->pscr2,
-                    c->flag_snap, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->air_brick, c->scan_tmp, c->u32_scratch,
+                    c->flag_snap, c->pflag8, c->pflag8s, c->keys, c->perm, c->cell_cnt, c->cell_off, c->tmask, c->air_brick, c->scan_tmp, c->u32_scratch,
                     c->randf, c->seeds, c->mc_numverts, c->mc_tri, c->mc_dens, c->mc_dens2, c->gfm_beta, c->gfm_s, c->mc_cube, c->mc_vflag, c->mc_vscan,
                     c->mc_compact, c->mc_vverts, c->mc_vvscan, c->mc_emark, c->mc_escan, c->mc_vstart, c->mc_inc,
                     c->mc_fill, c->mc_tmpv, c->pour_pos, c->pour_vel};
@@ -105,6 +105,7 @@ static int create_impl(MpCtx* c, const mp_params* p) {
     size_t n8 = c->P.b_run_mc ? 8 * n : n;
     size_t kcap = std::max(cap, n) + 1;
     MP_TRY(dalloc_t(c, &c->keys, kcap)); MP_TRY(dalloc_t(c, &c->perm, kcap));
+    MP_TRY(dalloc_t(c, &c->pflag8, cap)); MP_TRY(dalloc_t(c, &c->pflag8s, cap));
     MP_TRY(dalloc_t(c, &c->cell_cnt, n8 + 1)); MP_TRY(dalloc_t(c, &c->cell_off, n8 + 1));
     MP_CUDA(c, cudaMemset(c->cell_cnt, 0, sizeof(uint32_t) * (n8 + 1)));
     MP_CUDA(c, cudaMemset(c->cell_off, 0, sizeof(uint32_t) * (n8 + 1)));

@@ -68,6 +68,7 @@ struct MpCtx {
     float4 *pscr = 0;            // per-particle scratch (drag delta, snapshots)
     float4 *pscr2 = 0;
     int8_t *flag_snap = 0;
+    uint8_t *pflag8 = 0, *pflag8s = 0;   // particle types as bytes: from the sort's count pass, and sorted
     // sort
     uint32_t *keys = 0, *perm = 0;
     uint32_t *cell_cnt = 0, *cell_off = 0;   // sized for the 2x marching-cubes grid

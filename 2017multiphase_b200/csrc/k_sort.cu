@@ -156,17 +156,28 @@ __device__ __forceinline__ uint32_t hash_key(float4 q, float gx0, float gy0, flo
     int k = (r.z >= 0 && r.z < d) ? (int)r.z : 0;
     return (uint32_t)(i * hh * d + j * d + k);
 }
-// keys, per-cell counts, and a flag raised when the keys are not already in
-// order (then the stable sort is the identity and the gather can be skipped)
+// keys, per-cell counts, each particle's type as a byte, and a flag raised
+// when the keys are not already in order (then the stable sort is the
+// identity and the gather can be skipped)
 __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, float gy0, float gz0, float dx,
                              int w, int hh, int d, uint32_t* __restrict__ keys, uint32_t* __restrict__ cnt,
-                             uint32_t* __restrict__ unsorted) {
+                             uint32_t* __restrict__ unsorted, uint8_t* __restrict__ types) {
     __shared__ uint32_t blk_unsorted;
     if (threadIdx.x == 0) blk_unsorted = 0;
     __syncthreads();
     MP_GRID_LOOP(p, np) {
-        uint32_t key = hash_key(pos[p], gx0, gy0, gz0, dx, w, hh, d);
-        if (p > 0 && hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d) > key) blk_unsorted = 1u;
+        const float4 q = pos[p];
+        const uint32_t key = hash_key(q, gx0, gy0, gz0, dx, w, hh, d);
+        types[p] = (uint8_t)(pflag(q) & 7);
+        // the previous particle's key: from the lane before (a warp's active
+        // lanes hold consecutive particles from lane 0), lane 0 computes it
+        const unsigned am = __activemask();
+        const uint32_t up = __shfl_up_sync(am, key, 1);
+        const int lane = threadIdx.x & 31;
+        if (p > 0) {
+            const uint32_t prev = lane > 0 ? up : hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d);
+            if (prev > key) blk_unsorted = 1u;
+        }
         keys[p] = key;
         // one atomic per run of equal keys in the warp (particles arrive nearly sorted)
         unsigned peers = __match_any_sync(__activemask(), key);
@@ -198,15 +209,16 @@ __global__ void k_segsort(const uint32_t* __restrict__ off, int ncell, uint32_t*
         sort_distinct_run(perm, s0, off[cc + 1] - s0, [&](uint32_t) {});
     }
 }
-// each cell's type mask (which particle types it holds) from the particles in
-// cell order (coalesced reads), and with `air_words` (the simulation grid's
-// sort) the bit of each 4x4x4-cell brick that holds an AIR or AIRSOLO particle
+// each cell's type mask (which particle types it holds) from the particles'
+// type bytes in cell order (coalesced reads), and with `air_words` (the
+// simulation grid's sort) the bit of each 4x4x4-cell brick that holds an AIR
+// or AIRSOLO particle
 __global__ void k_tmask_sorted(const uint32_t* __restrict__ off, int ncell, int w, int hh, int d,
-                               const float4* __restrict__ pos, uint8_t* __restrict__ tmask,
+                               const uint8_t* __restrict__ types, uint8_t* __restrict__ tmask,
                                uint32_t* __restrict__ air_words) {
     MP_GRID_LOOP(cc, ncell) {
         uint32_t m = 0;
-        for (uint32_t s = off[cc]; s < off[cc + 1]; s++) m |= 1u << (pflag(__ldg(pos + s)) & 7);
+        for (uint32_t s = off[cc]; s < off[cc + 1]; s++) m |= 1u << __ldg(types + s);
         tmask[cc] = (uint8_t)m;
         if (air_words && (m & ((1u << MP_TYPEAIR) | (1u << MP_TYPEAIRSOLO)))) {
             const uint32_t kk = (uint32_t)cc % (uint32_t)d, jj = ((uint32_t)cc / (uint32_t)d) % (uint32_t)hh,
@@ -219,12 +231,14 @@ __global__ void k_tmask_sorted(const uint32_t* __restrict__ off, int ncell, int 
 }
 __global__ void k_reorder(const uint32_t* __restrict__ perm, int np,
                           const float4* __restrict__ p0, const float4* __restrict__ v0, const float4* __restrict__ h0,
-                          float4* __restrict__ p1, float4* __restrict__ v1, float4* __restrict__ h1) {
+                          float4* __restrict__ p1, float4* __restrict__ v1, float4* __restrict__ h1,
+                          const uint8_t* __restrict__ t0, uint8_t* __restrict__ t1) {
     MP_GRID_LOOP(s, np) {
         uint32_t src = perm[s];
         p1[s] = __ldg(p0 + src);
         v1[s] = __ldg(v0 + src);
         h1[s] = __ldg(h0 + src);
+        t1[s] = __ldg(t0 + src);
     }
 }
 }  // namespace
@@ -236,8 +250,8 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     MP_CUDA(c, cudaMemsetAsync(unsorted, 0, sizeof(uint32_t), c->stream));
     const bool sim_grid = w == c->G.NX && hh == c->G.NY && d == c->G.NZ;
     if (sim_grid) MP_CUDA(c, cudaMemsetAsync(c->air_brick, 0, sizeof(uint32_t) * c->air_brick_words, c->stream));
-    auto tmask_pass = [&]() -> int {
-        k_tmask_sorted<<<mp_blocks(ncell, 256), 256, 0, c->stream>>>(c->cell_off, ncell, w, hh, d, c->pos, c->tmask,
+    auto tmask_pass = [&](const uint8_t* types) -> int {
+        k_tmask_sorted<<<mp_blocks(ncell, 256), 256, 0, c->stream>>>(c->cell_off, ncell, w, hh, d, types, c->tmask,
                                                                      sim_grid ? c->air_brick : nullptr);
         c->launches++;
         MP_CHECK_LAUNCH(c);
@@ -245,7 +259,7 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     };
     if (np > 0) {
         k_hash_count<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->pos, np, c->G.gx0, c->G.gy0, c->G.gz0, dx, w, hh, d,
-                                                                c->keys, c->cell_cnt, unsorted);
+                                                                c->keys, c->cell_cnt, unsorted, c->pflag8);
         c->launches++;
         MP_CHECK_LAUNCH(c);
     }
@@ -258,7 +272,7 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
         // already in cell order: the stable sort is the identity permutation;
         // the counts still have to run back to zero for the next sort
         MP_CUDA(c, cudaMemsetAsync(c->cell_cnt, 0, sizeof(uint32_t) * ncell, c->stream));
-        return tmask_pass();
+        return tmask_pass(c->pflag8);
     }
     if (np > 0) {
         k_scatter<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->keys, np, c->cell_off, c->cell_cnt, c->perm);
@@ -269,12 +283,13 @@ static int sort_on_grid(MpCtx* c, float dx, int w, int hh, int d) {
     c->launches++;
     MP_CHECK_LAUNCH(c);
     if (np > 0) {
-        k_reorder<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->perm, np, c->pos, c->vel, c->heat, c->pos2, c->vel2, c->heat2);
+        k_reorder<<<mp_blocks(np, 256), 256, 0, c->stream>>>(c->perm, np, c->pos, c->vel, c->heat, c->pos2, c->vel2, c->heat2,
+                                                             c->pflag8, c->pflag8s);
         c->launches++;
         MP_CHECK_LAUNCH(c);
         std::swap(c->pos, c->pos2); std::swap(c->vel, c->vel2); std::swap(c->heat, c->heat2);
     }
-    return tmask_pass();
+    return tmask_pass(np > 0 ? c->pflag8s : c->pflag8);
 }
 
 int k_hash_sort(MpCtx* c) {
