@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--config", type=int, default=5)
     ap.add_argument("--n", type=int, default=0, help="grid size (0: the configuration's own, 256)")
     ap.add_argument("--seed", type=int, default=2017005)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="steps of the end-to-end measurement (0: as many as --steps, on the same frames)")
     ap.add_argument("--ref-steps", type=int, default=2, help="reference arm: at most this many timed oracle steps")
     ap.add_argument("--ref-warmup", type=int, default=0, help="reference arm: at most this many warm-up steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -398,6 +399,64 @@ def fwd_adjoint(args, n, local, dist):
     return res
 
 
+def e2e_run(mp, args, rank, world, dist, mesh_max):
+    """End to end through the public API with host buffers: a fresh engine
+    from the same configuration and seed (the engine is deterministic, so
+    after the same warm-up it steps through the same frames as the timed
+    region), then `e2e_steps` steps (default: as many as the timed ones),
+    each uploading its host inputs (random table and nucleation cells) from
+    pinned memory and downloading the three extracted meshes into host
+    buffers sized from `mesh_max` (the largest vertex and index counts of the
+    timed steps). Wall clock around the steps, max over ranks."""
+    import numpy as np
+    import torch
+    import ctypes as C
+    steps = args.e2e_steps if args.e2e_steps > 0 else args.steps
+    sim = mp.Sim.from_config(args.config, args.n, replica_seed(args.seed, rank))
+    p = sim.params
+    for _ in range(args.warmup):
+        sim.bubblesim()
+    torch.cuda.synchronize()
+    rf, seeds = mp.scene_tables(p, args.config, replica_seed(args.seed, rank))
+    rf_pin = torch.empty(rf.size, dtype=torch.float32, pin_memory=True).numpy(); rf_pin[:] = rf
+    sd_pin = torch.empty(max(seeds.size, 1), dtype=torch.int32, pin_memory=True).numpy()[:seeds.size]; sd_pin[:] = seeds
+    # twice the largest mesh of the timed steps, which were the same frames
+    # when e2e_steps <= steps (the download reports a capacity error if a
+    # mesh were larger)
+    cap_v = min(p.mc_max_verts, max(2 * mesh_max[0], 1024))
+    cap_i = min(3 * p.mc_max_tris, max(2 * mesh_max[1], 3072))
+    vbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
+    nbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
+    ibuf = torch.empty(cap_i, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    h2d = rf_pin.nbytes + sd_pin.nbytes
+    d2h = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.set_tables(rf_pin, sd_pin)
+        sim.bubblesim()
+        st = sim.state()
+        for s in range(3):
+            nv, ni = st.mc_verts[s], st.mc_indices[s]
+            rc = sim.lib.mp_mc_download(sim.ctx, s, vbuf.ctypes.data_as(C.c_void_p), nbuf.ctypes.data_as(C.c_void_p),
+                                        ibuf.ctypes.data_as(C.c_void_p), cap_v, cap_i)
+            if rc:
+                raise RuntimeError(f"mesh download failed {rc}")
+            d2h += 24 * nv + 4 * ni
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * steps / e2e_s, "unit": "steps/s",
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h / max(steps, 1))}
+    sim.close()
+    return e2e
+
+
 def main():
     args = parse()
     if args.profile_case:
@@ -443,9 +502,12 @@ def main():
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    mesh_max = [0, 0]
     for _ in range(args.steps):
         sim.bubblesim()
-        cg_iters += sim.state().last_cg_iters
+        st = sim.state()
+        cg_iters += st.last_cg_iters
+        mesh_max = [max(mesh_max[0], *st.mc_verts), max(mesh_max[1], *st.mc_indices)]
     e1.record(stream)
     torch.cuda.synchronize()
     if dist:
@@ -471,47 +533,6 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = aggregate_steps_per_s(world, args.steps, t_max)
-
-    # end to end through the public API with host buffers: the step's host
-    # inputs (random table and nucleation cells) go up, the extracted meshes
-    # come back, every step
-    rf, seeds = mp.scene_tables(p, args.config, replica_seed(args.seed, rank))
-    rf_pin = torch.empty(rf.size, dtype=torch.float32, pin_memory=True).numpy(); rf_pin[:] = rf
-    sd_pin = torch.empty(max(seeds.size, 1), dtype=torch.int32, pin_memory=True).numpy()[:seeds.size]; sd_pin[:] = seeds
-    # host mesh buffers: twice the largest mesh of the timed steps (the
-    # download reports a capacity error if a later mesh were larger)
-    st0 = sim.state()
-    cap_v = min(p.mc_max_verts, max(2 * max(st0.mc_verts), 1024))
-    cap_i = min(3 * p.mc_max_tris, max(2 * max(st0.mc_indices), 3072))
-    vbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
-    nbuf = torch.empty((cap_v, 3), dtype=torch.float32, pin_memory=True).numpy()
-    ibuf = torch.empty(cap_i, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-    import ctypes as C
-    h2d = rf_pin.nbytes + sd_pin.nbytes
-    d2h = 0
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        sim.set_tables(rf_pin, sd_pin)
-        sim.bubblesim()
-        st = sim.state()
-        for s in range(3):
-            nv, ni = st.mc_verts[s], st.mc_indices[s]
-            rc = sim.lib.mp_mc_download(sim.ctx, s, vbuf.ctypes.data_as(C.c_void_p), nbuf.ctypes.data_as(C.c_void_p),
-                                        ibuf.ctypes.data_as(C.c_void_p), cap_v, cap_i)
-            if rc:
-                raise RuntimeError(f"mesh download failed {rc}")
-            d2h += 24 * nv + 4 * ni
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
-           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h / max(args.e2e_steps, 1))}
 
     # roofline of the dominant kernel class (by device time in the timed
     # region); algorithmic bytes from the compulsory-traffic model (each byte
@@ -577,12 +598,13 @@ def main():
            "cg_iters_per_step": cg_iters / max(args.steps, 1),
            "mesh": {"verts": [int(v) for v in st.mc_verts], "triangles": [int(v) // 3 for v in st.mc_indices]},
            "kernel_classes": cls_table,
-           "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
+           "e2e": None, "gpu_launches": int(launches), "clocks": clk}
     nx = p.nx
     if args.precision_steps > 0:
         out["precision"] = precision_report(sim, mp, stream, args.precision_steps)
         out["pressure_rel_err"] = out["precision"]["projection"]["mixed"]["pressure_rel_err"]
     sim.close()
+    out["e2e"] = e2e_run(mp, args, rank, world, dist, mesh_max)
     if args.adj_steps > 0:
         out["fwd_adjoint"] = fwd_adjoint(args, nx, local, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
