@@ -165,23 +165,34 @@ __global__ void k_hash_count(const float4* __restrict__ pos, int np, float gx0, 
     __shared__ uint32_t blk_unsorted;
     if (threadIdx.x == 0) blk_unsorted = 0;
     __syncthreads();
-    MP_GRID_LOOP(p, np) {
-        const float4 q = pos[p];
-        const uint32_t key = hash_key(q, gx0, gy0, gz0, dx, w, hh, d);
-        types[p] = (uint8_t)(pflag(q) & 7);
-        // the previous particle's key: from the lane before (a warp's active
-        // lanes hold consecutive particles from lane 0), lane 0 computes it
-        const unsigned am = __activemask();
-        const uint32_t up = __shfl_up_sync(am, key, 1);
-        const int lane = threadIdx.x & 31;
-        if (p > 0) {
-            const uint32_t prev = lane > 0 ? up : hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d);
-            if (prev > key) blk_unsorted = 1u;
+    // a warp-uniform grid-stride loop (blockDim is a multiple of 32): all 32
+    // lanes run every iteration, lane l holding particle p0 + l when it is
+    // below np, so the shuffle that passes each key to the next lane names
+    // the whole warp and lane l - 1 always holds particle p - 1
+    const int lane = threadIdx.x & 31;
+    const int stride = (int)(gridDim.x * blockDim.x);
+    for (int p0 = (int)(blockIdx.x * blockDim.x + (threadIdx.x & ~31u)); p0 < np; p0 += stride) {
+        const int p = p0 + lane;
+        const bool live = p < np;
+        uint32_t key = 0;
+        if (live) {
+            const float4 q = pos[p];
+            key = hash_key(q, gx0, gy0, gz0, dx, w, hh, d);
+            types[p] = (uint8_t)(pflag(q) & 7);
+            keys[p] = key;
         }
-        keys[p] = key;
-        // one atomic per run of equal keys in the warp (particles arrive nearly sorted)
-        unsigned peers = __match_any_sync(__activemask(), key);
-        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(cnt + key, (uint32_t)__popc(peers));
+        const uint32_t up = __shfl_up_sync(0xffffffffu, key, 1);
+        const unsigned lm = __ballot_sync(0xffffffffu, live);
+        if (live) {
+            // the previous particle's key: from the lane before, lane 0 computes it
+            if (p > 0) {
+                const uint32_t prev = lane > 0 ? up : hash_key(pos[p - 1], gx0, gy0, gz0, dx, w, hh, d);
+                if (prev > key) blk_unsorted = 1u;
+            }
+            // one atomic per run of equal keys in the warp (particles arrive nearly sorted)
+            const unsigned peers = __match_any_sync(lm, key);
+            if (lane == __ffs(peers) - 1) atomicAdd(cnt + key, (uint32_t)__popc(peers));
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0 && blk_unsorted) *unsorted = 1u;   // one store per block
