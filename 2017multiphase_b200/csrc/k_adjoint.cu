@@ -1430,6 +1430,8 @@ static int sorted_ids(MpCtx* c, AdjTape* t) {
     return MP_OK;
 }
 
+static int record_tape(MpCtx* c, AdjTape* t, bool air);
+
 int k_adj_record(MpCtx* c, int nsteps, int every) {
     const mp_params& P = c->P;
     if (nsteps < 1 || every < 1) { c->err = "adj_record: nsteps and checkpoint interval must be positive"; return MP_ERR_ARG; }
@@ -1462,6 +1464,17 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     AdjTape* t = new AdjTape();
     c->adj = t;
     t->np = np; t->nsteps = nsteps; t->every = every;
+    const int rc = record_tape(c, t, cnt[2] != 0);
+    // a recording that stopped part-way keeps no tape: its missing steps
+    // hold no state, and a replay would read past the recorded ones
+    if (rc != MP_OK) k_adj_free(c);
+    return rc;
+}
+
+// the snapshots and every step's recorded state, stepping the engine
+static int record_tape(MpCtx* c, AdjTape* t, bool air) {
+    const mp_params& P = c->P;
+    const int np = t->np, nsteps = t->nsteps, every = t->every;
     const Grid& g = c->G;
     MP_TRY(amalloc(c, &t->ids, np)); MP_TRY(amalloc(c, &t->ids2, np));
     MP_TRY(amalloc(c, &t->x0, 3 * (size_t)np)); MP_TRY(amalloc(c, &t->v0, 3 * (size_t)np));
@@ -1469,7 +1482,7 @@ int k_adj_record(MpCtx* c, int nsteps, int every) {
     k_ad_iota<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids);
     k_ad_snapshot<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->pos, c->vel, t->x0, t->v0, t->mass);
     ADJ_LAUNCH(c);
-    t->air = cnt[2] != 0;
+    t->air = air;
     if (t->air) {
         MP_TRY(amalloc(c, &t->phase, np)); MP_TRY(amalloc(c, &t->mass_w, np)); MP_TRY(amalloc(c, &t->mass_a, np));
         k_ad_snapshot_phase<<<mp_blocks(np, 256), 256, 0, c->stream>>>(np, t->ids, c->pos, c->vel, t->phase,

@@ -549,7 +549,10 @@ int mp_set_output(void* ctx, const mp_output* out);
  * and records the discrete state of each step (splat order and cell ranges,
  * cell marks, the merged level set and the extrapolation distance fields,
  * and at the end each cell's nearest FLUID particle); the derivative is that
- * of the program with this state held fixed.
+ * of the program with this state held fixed. A recording that fails (an
+ * MP_ERR_* code from a step or an allocation) keeps no tape, and the context
+ * has advanced by the steps it ran; mp_adj_* calls then return
+ * MP_ERR_STATE until the next mp_adj_record.
  * mp_adj_set_targets takes the target points y_s (host float xyz) of the
  * loss L = sum_s phi(y_s)^2, phi the fluid distance field of genlevelset
  * after the last step. mp_adj_loss replays the program from the recorded
