@@ -1610,7 +1610,9 @@ int k_adj_set_targets(MpCtx* c, const float* sp, int ns) {
     for (int q = 0; q < g.n; q++) off[q + 1] += off[q];
     if (t->samples) cudaFree(t->samples);
     if (t->s_off) cudaFree(t->s_off);
-    t->samples = nullptr; t->s_off = nullptr;
+    // no samples until the new ones are on the device (a failure below
+    // leaves the tape without targets, not with freed ones)
+    t->samples = nullptr; t->s_off = nullptr; t->nsamples = 0;
     MP_TRY(amalloc(c, &t->samples, 3 * (size_t)ns)); MP_TRY(amalloc(c, &t->s_off, (size_t)g.n + 1));
     MP_CUDA(c, cudaMemcpy(t->samples, sorted.data(), sizeof(float) * 3 * ns, cudaMemcpyHostToDevice));
     MP_CUDA(c, cudaMemcpy(t->s_off, off.data(), sizeof(uint32_t) * (g.n + 1), cudaMemcpyHostToDevice));
@@ -1688,6 +1690,9 @@ template <class T> static int adj_work(MpCtx* c, AdjTape* t) {
     if (t->wesz == sizeof(T) && (int)t->wk.size() == W_COUNT && t->wk_ns >= t->nsamples) return MP_OK;
     for (void* p : t->wk) if (p) cudaFree(p);
     t->wk.assign(W_COUNT, nullptr);
+    // marked unusable until every array below is allocated: a failed
+    // allocation leaves null arrays that no later call may take as ready
+    t->wesz = 0; t->wk_ns = 0;
     const Grid& g = c->G;
     const size_t np3 = 3 * (size_t)t->np, nf = (size_t)g.nfx + g.nfy + g.nfz, n = g.n;
     const int nseg = (t->nsteps + t->every - 1) / t->every;
