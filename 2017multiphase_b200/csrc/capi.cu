@@ -434,15 +434,18 @@ extern "C" int mp_set_field(void* ctx, int f, const void* src, size_t bytes) {
 extern "C" int mp_set_tables(void* ctx, const float* randfloat, int nrand, const int32_t* seeds, int nseed) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     if (nrand <= 200 || !randfloat || nseed < 0 || (nseed > 0 && !seeds)) { c->err = "set_tables: need > 200 random values"; return MP_ERR_ARG; }
+    // a table being replaced counts as absent until its new array exists, so
+    // a failed allocation leaves "not set" (which the stages check), not a
+    // size over a freed array
     if (nrand != c->nrand) {
         if (c->randf) cudaFree(c->randf);
-        c->randf = nullptr;
+        c->randf = nullptr; c->nrand = 0;
         MP_TRY(dalloc_t(c, &c->randf, nrand));
         c->nrand = nrand;
     }
     if (nseed != c->nseed || !c->seeds) {
         if (c->seeds) cudaFree(c->seeds);
-        c->seeds = nullptr;
+        c->seeds = nullptr; c->nseed = 0;
         MP_TRY(dalloc_t(c, &c->seeds, std::max(nseed, 1)));
         c->nseed = nseed;
     }
@@ -566,6 +569,10 @@ extern "C" int mp_checkpoint_load(void* ctx, const void* host_src, size_t bytes)
     }
     if (h.np < 0 || h.np > c->P.par_num_max || h.ncell != c->G.n || h.nrand <= 200 || h.nseed < 0) {
         c->err = "checkpoint_load: sizes do not fit this context"; return MP_ERR_ARG;
+    }
+    // the state's particle count is the one every later kernel runs over
+    if (h.state.par_num_now != h.np) {
+        c->err = "checkpoint_load: the state's particle count differs from the stored particles"; return MP_ERR_ARG;
     }
     const size_t need = sizeof(CkptHeader) + 3 * sizeof(float4) * (size_t)h.np + sizeof(float) * (size_t)h.nrand +
                         sizeof(int32_t) * (size_t)h.nseed + 2 * sizeof(float) * (size_t)h.ncell;
