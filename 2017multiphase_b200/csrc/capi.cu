@@ -272,12 +272,20 @@ extern "C" int mp_get_device(void* ctx, int* device) {
 // ---------------------------------------------------------------------------
 // data in / out
 // ---------------------------------------------------------------------------
+// every flag one of the particle types (the stages select on them, and the
+// sort keeps the low three bits as the type)
+static bool flags_valid(const int8_t* flag, int n) {
+    for (int p = 0; p < n; p++)
+        if (flag[p] < 0 || flag[p] >= MP_TYPECNT) return false;
+    return true;
+}
 extern "C" int mp_upload_particles(void* ctx, int n, const float* pos3, const float* vel3, const int8_t* flag,
                                    const float* mass, const float* temp, const float* lheat, const float* sol,
                                    const float* gas) {
     MpCtx* c = C(ctx); CTX_OR_ARG(c);
     if (n < 0 || (n > 0 && (!pos3 || !flag || !mass))) { c->err = "upload: bad arguments"; return MP_ERR_ARG; }
     if (n > c->P.par_num_max) { c->err = "upload: more particles than par_num_max"; return MP_ERR_CAPACITY; }
+    if (!flags_valid(flag, n)) { c->err = "upload: a particle flag is not an MP_TYPE* value"; return MP_ERR_ARG; }
     MP_TRY(k_pack_particles(c, n, pos3, vel3, flag, mass, temp, lheat, sol, gas));
     MP_CUDA(c, cudaStreamSynchronize(c->stream));
     c->S.par_num_now = n;
@@ -420,6 +428,9 @@ extern "C" int mp_set_field(void* ctx, int f, const void* src, size_t bytes) {
         case MP_P_LHEAT: dstp = L.data(); break;
         case MP_P_SOLUBILITY: dstp = so.data(); break;
         default: dstp = ga.data(); break;
+        }
+        if (f == MP_P_FLAG && !flags_valid(static_cast<const int8_t*>(src), np)) {
+            c->err = "set_field: a particle flag is not an MP_TYPE* value"; return MP_ERR_ARG;
         }
         memcpy(dstp, src, bytes);
         MP_TRY(k_pack_particles(c, np, p3.data(), v3.data(), fl.data(), m.data(), T.data(), L.data(), so.data(), ga.data()));

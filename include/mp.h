@@ -255,6 +255,7 @@ int mp_get_device(void* ctx, int* device);
 
 /* Copies n particles from HOST arrays (structure of arrays as in the
  * reference; any of T/L/sol/gas may be NULL = zero). Sets par_num_now.
+ * Every flag must be an MP_TYPE* value (else MP_ERR_ARG, nothing copied).
  * Replaces the H2D copies of initparticle_solidCoupling (spray.cu:465-470). */
 int mp_upload_particles(void* ctx, int n, const float* pos3, const float* vel3,
                         const int8_t* flag, const float* mass, const float* temp,
