@@ -175,6 +175,29 @@ def oracle_steps(config, n, seed, steps, warm, threads=None):
     return times, threads, npart, p
 
 
+def cpu_baseline(config, n, seed, single_n=64):
+    """The GPU arm's `cpu_baseline`: one whole oracle step of the same
+    configuration at n^3 on all host threads (no warm-up), and beside it one
+    whole step on a single host thread at min(single_n, n)^3, a grid that one
+    thread finishes in seconds (reported as measured, not scaled to n^3)."""
+    t0 = time.perf_counter()
+    times, threads, npart, _ = oracle_steps(config, n, seed, 1, 0)
+    out = {"value": 1.0 / times[0], "unit": "steps/s", "cores": threads, "kind": "port",
+           "sample": f"one whole oracle step of the same configuration at {n}^3 ({npart} particles, "
+                     f"{times[0]:.1f} s; {time.perf_counter() - t0:.0f} s with set-up), no warm-up"}
+    n1 = min(single_n, n)
+    try:
+        times1, _, npart1, _ = oracle_steps(config, n1, seed, 1, 0, threads=1)
+    finally:   # the oracle's thread count is process-wide: put it back
+        from oracle import oracle as orc_lib
+        orc_lib.load().or_set_threads(threads)
+    out["single_thread"] = {"value": 1.0 / times1[0], "unit": "steps/s", "cores": 1, "kind": "port",
+                            "sample": f"one whole oracle step of the same configuration at {n1}^3 on one host "
+                                      f"thread ({npart1} particles, {times1[0]:.1f} s), no warm-up; a smaller "
+                                      f"grid, not scaled"}
+    return out
+
+
 def run_reference(args, rank):
     """The reference arm: whole oracle steps of the same configuration at the
     same grid on the host cores. A step at 256^3 takes minutes on the CPU, so
@@ -609,12 +632,7 @@ def main():
         out["fwd_adjoint"] = fwd_adjoint(args, nx, local, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            t0 = time.perf_counter()
-            times, threads, npart, _ = oracle_steps(args.config, nx, args.seed, 1, 0)
-            out["cpu_baseline"] = {"value": 1.0 / times[0], "unit": "steps/s", "cores": threads, "kind": "port",
-                                   "sample": f"one whole oracle step of the same configuration at {nx}^3 "
-                                             f"({npart} particles, {times[0]:.1f} s; "
-                                             f"{time.perf_counter() - t0:.0f} s with set-up), no warm-up"}
+            out["cpu_baseline"] = cpu_baseline(args.config, nx, args.seed)
         except Exception as e:   # the baseline is reported, not required
             out["cpu_baseline"] = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
                                    "sample": f"failed: {e}"}

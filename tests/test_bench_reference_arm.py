@@ -34,3 +34,15 @@ def test_reference_arm_line_and_libraries():
     assert line["config"]["grid"] == 16 and line["config"]["particles"] > 0
     assert not [l for l in libs if os.path.basename(l) == "libmp.so"], libs
     assert [l for l in libs if "oracle" in l], libs
+
+
+def test_cpu_baseline_reports_all_threads_and_one_thread():
+    """The GPU arm's cpu_baseline: a whole oracle step on all host threads and
+    one on a single thread at the smaller of the two grids."""
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    cb = bench.cpu_baseline(5, 16, 2017005, single_n=12)
+    assert cb["value"] > 0 and cb["cores"] >= 1 and cb["kind"] == "port" and "16^3" in cb["sample"]
+    st = cb["single_thread"]
+    assert st["value"] > 0 and st["cores"] == 1 and "12^3" in st["sample"]
