@@ -69,8 +69,11 @@ def copy_state(src, dst):
     dst.set_state(src.state())
 
 
-def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2, dims=None):
+def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2, dims=None, select=None):
     p, parts, rf, seeds = reference_mode(mp, config, n, seed, dims)
+    if select is not None:      # a subset of the configuration's particles
+        keep = select(parts)
+        parts = {k: (None if v is None else np.asarray(v)[keep]) for k, v in parts.items()}
     orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
     orc.upload_particles(**parts)
     orc.set_tables(rf, seeds)
@@ -138,6 +141,33 @@ def test_every_stage_on_a_non_cubic_grid(mp, oracle_mod, refhost, config):
     checked, bad, _ = run_pair(mp, oracle_mod, refhost, config, 16, 2017_706 + config, dims=(16, 24, 20))
     assert not bad, bad
     assert len(checked) >= 60
+
+
+SUBSETS = {
+    "empty": lambda q: np.zeros(0, np.int64),
+    # the FLUID particle nearest the domain centre
+    "one": lambda q: [int(np.argmin(((np.asarray(q["pos"]).reshape(-1, 3) - 0.5) ** 2).sum(1)
+                                    + 10.0 * (np.asarray(q["flag"]) != 0)))],
+    # scattered FLUID and AIR particles: isolated AIR is deleted, FLUID falls alone
+    "sparse": lambda q: np.concatenate([np.where(np.asarray(q["flag"]) == 0)[0][::500],
+                                        np.where(np.asarray(q["flag"]) == 1)[0][::7]]),
+}
+
+
+@pytest.mark.parametrize("subset", sorted(SUBSETS))
+def test_every_stage_on_empty_and_sparse_particle_sets(mp, oracle_mod, refhost, subset):
+    """The rising bubble's scene with no particles, a single FLUID particle, and
+    a sparse scatter of FLUID and AIR particles (cells with one particle, most
+    cells empty, AIR particles without liquid around them): every stage of two
+    frames equals the reference's kernels bit for bit."""
+    checked, bad, orc = run_pair(mp, oracle_mod, refhost, 1, N, 2017_701, select=SUBSETS[subset])
+    assert not bad, bad
+    assert len(checked) >= 40
+    if subset == "empty":
+        assert orc.state().par_num_now == 0
+    if subset == "sparse":
+        flags = orc.download_particles()["flag"]
+        assert len(flags) > 0 and (flags == mp.TYPEFLUID).all()   # the isolated AIR particles were deleted
 
 
 def test_in_place_kernels_write_only_their_own_element(mp, oracle_mod, refhost):
