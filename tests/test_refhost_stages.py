@@ -69,11 +69,10 @@ def copy_state(src, dst):
     dst.set_state(src.state())
 
 
-def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2, dims=None, select=None):
+def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2, dims=None, transform=None):
     p, parts, rf, seeds = reference_mode(mp, config, n, seed, dims)
-    if select is not None:      # a subset of the configuration's particles
-        keep = select(parts)
-        parts = {k: (None if v is None else np.asarray(v)[keep]) for k, v in parts.items()}
+    if transform is not None:   # edited or subset particles of the configuration
+        parts = transform(p, dict(parts))
     orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
     orc.upload_particles(**parts)
     orc.set_tables(rf, seeds)
@@ -143,29 +142,62 @@ def test_every_stage_on_a_non_cubic_grid(mp, oracle_mod, refhost, config):
     assert len(checked) >= 60
 
 
-SUBSETS = {
-    "empty": lambda q: np.zeros(0, np.int64),
+def _subset(keep_fn):
+    def f(p, parts):
+        keep = keep_fn(parts)
+        return {k: (None if v is None else np.asarray(v)[keep]) for k, v in parts.items()}
+    return f
+
+
+def _positions(edit):
+    def f(p, parts):
+        pos = np.asarray(parts["pos"], np.float32).reshape(-1, 3).copy()
+        edit(pos, np.float32(1.0 / p.nx), np.random.default_rng(2017))
+        parts["pos"] = pos
+        return parts
+    return f
+
+
+def _on_faces(pos, h, rng):
+    # a fifth of the particles moved onto the nearest cell face along one axis
+    sel, ax = rng.random(len(pos)) < 0.2, rng.integers(0, 3, len(pos))
+    for a in range(3):
+        m = sel & (ax == a)
+        pos[m, a] = np.round(pos[m, a] / h).astype(np.float32) * h
+
+
+def _outside(pos, h, rng):
+    # one particle in a hundred just outside the box in x
+    sel = rng.random(len(pos)) < 0.01
+    pos[sel, 0] = np.where(rng.random(int(sel.sum())) < 0.5, -0.01, 1.01).astype(np.float32)
+
+
+EDGE_INPUTS = {
+    "empty": _subset(lambda q: np.zeros(0, np.int64)),
     # the FLUID particle nearest the domain centre
-    "one": lambda q: [int(np.argmin(((np.asarray(q["pos"]).reshape(-1, 3) - 0.5) ** 2).sum(1)
-                                    + 10.0 * (np.asarray(q["flag"]) != 0)))],
+    "one": _subset(lambda q: [int(np.argmin(((np.asarray(q["pos"]).reshape(-1, 3) - 0.5) ** 2).sum(1)
+                                            + 10.0 * (np.asarray(q["flag"]) != 0)))]),
     # scattered FLUID and AIR particles: isolated AIR is deleted, FLUID falls alone
-    "sparse": lambda q: np.concatenate([np.where(np.asarray(q["flag"]) == 0)[0][::500],
-                                        np.where(np.asarray(q["flag"]) == 1)[0][::7]]),
+    "sparse": _subset(lambda q: np.concatenate([np.where(np.asarray(q["flag"]) == 0)[0][::500],
+                                                np.where(np.asarray(q["flag"]) == 1)[0][::7]])),
+    "on_cell_faces": _positions(_on_faces),
+    "outside_the_box": _positions(_outside),
 }
 
 
-@pytest.mark.parametrize("subset", sorted(SUBSETS))
-def test_every_stage_on_empty_and_sparse_particle_sets(mp, oracle_mod, refhost, subset):
-    """The rising bubble's scene with no particles, a single FLUID particle, and
-    a sparse scatter of FLUID and AIR particles (cells with one particle, most
-    cells empty, AIR particles without liquid around them): every stage of two
-    frames equals the reference's kernels bit for bit."""
-    checked, bad, orc = run_pair(mp, oracle_mod, refhost, 1, N, 2017_701, select=SUBSETS[subset])
+@pytest.mark.parametrize("case", sorted(EDGE_INPUTS))
+def test_every_stage_on_edge_inputs(mp, oracle_mod, refhost, case):
+    """The rising bubble's scene with no particles, a single FLUID particle, a
+    sparse scatter of FLUID and AIR particles (cells with one particle, most
+    cells empty, AIR without liquid around it), a fifth of the particles
+    exactly on cell faces, and one in a hundred just outside the box: every
+    stage of two frames equals the reference's kernels bit for bit."""
+    checked, bad, orc = run_pair(mp, oracle_mod, refhost, 1, N, 2017_701, transform=EDGE_INPUTS[case])
     assert not bad, bad
     assert len(checked) >= 40
-    if subset == "empty":
+    if case == "empty":
         assert orc.state().par_num_now == 0
-    if subset == "sparse":
+    if case == "sparse":
         flags = orc.download_particles()["flag"]
         assert len(flags) > 0 and (flags == mp.TYPEFLUID).all()   # the isolated AIR particles were deleted
 
