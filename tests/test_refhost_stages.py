@@ -69,10 +69,12 @@ def copy_state(src, dst):
     dst.set_state(src.state())
 
 
-def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2, dims=None, transform=None):
+def run_pair(mp, oracle_mod, refhost, config, n, seed, frames=2, dims=None, transform=None, no_seeds=False):
     p, parts, rf, seeds = reference_mode(mp, config, n, seed, dims)
     if transform is not None:   # edited or subset particles of the configuration
         parts = transform(p, dict(parts))
+    if no_seeds:                # no nucleation cells
+        seeds = np.zeros(0, np.int32)
     orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
     orc.upload_particles(**parts)
     orc.set_tables(rf, seeds)
@@ -200,6 +202,23 @@ def test_every_stage_on_edge_inputs(mp, oracle_mod, refhost, case):
     if case == "sparse":
         flags = orc.download_particles()["flag"]
         assert len(flags) > 0 and (flags == mp.TYPEFLUID).all()   # the isolated AIR particles were deleted
+
+
+@pytest.mark.parametrize("config,case", [(2, "no_nucleation_cells"), (2, "sparse"), (3, "solid_only")])
+def test_phase_change_stages_on_edge_inputs(mp, oracle_mod, refhost, config, case):
+    """Pool boiling with no nucleation cells and with one particle in fifty;
+    melting/freezing with the solid sphere alone (no liquid): every stage of
+    two frames, the heat, gas, melting and freezing stages among them, equals
+    the reference's kernels bit for bit."""
+    transform = {"no_nucleation_cells": None,
+                 "sparse": _subset(lambda q: np.arange(len(q["flag"]))[::50]),
+                 "solid_only": _subset(lambda q: np.where(np.asarray(q["flag"]) == mp.TYPESOLID)[0])}[case]
+    checked, bad, orc = run_pair(mp, oracle_mod, refhost, config, N, 2017_700 + config, transform=transform,
+                                 no_seeds=case == "no_nucleation_cells")
+    assert not bad, bad
+    names = {nm for _, nm in checked}
+    assert "updateTemperature" in names
+    assert ("GenerateGasParticle" in names) if config == 2 else ({"MeltSolid", "Freezing"} <= names)
 
 
 def test_in_place_kernels_write_only_their_own_element(mp, oracle_mod, refhost):
