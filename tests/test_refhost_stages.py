@@ -243,8 +243,8 @@ def test_the_stages_change_the_state(mp, oracle_mod, refhost):
     assert np.abs(orc.get_field("press")).max() > 0 and np.abs(orc.get_field("waterux")).max() > 0
 
 
-@pytest.mark.parametrize("config", [1, 2, 5])
-def test_marching_cubes_equals_the_reference_kernels(mp, oracle_mod, refhost, config):
+@pytest.mark.parametrize("config,case", [(1, None), (2, None), (5, None), (1, "empty"), (1, "one"), (1, "sparse")])
+def test_marching_cubes_equals_the_reference_kernels(mp, oracle_mod, refhost, config, case):
     """preMC and runMC_smooth from the state at the end of a step.  Bit-exact:
     the 2x re-sort, the density field of each surface, classifyVoxel's vertex
     counts, the active voxel, vertex and index counts, and which vertices each
@@ -255,9 +255,12 @@ def test_marching_cubes_equals_the_reference_kernels(mp, oracle_mod, refhost, co
     it from the edge's lower node.  The triangle lists themselves follow the
     generated case table (same crossed edges and counts as tables.h, other
     triangulations in some cases), so smoothing and normals are compared on
-    the oracle's triangles, through the reference's kernels, bit for bit."""
+    the oracle's triangles, through the reference's kernels, bit for bit.
+    Also from the edge inputs with no particles and with a single particle
+    (no surface either way) and from a sparse scatter (isolated blobs)."""
     p, parts, rf, seeds = reference_mode(mp, config, N, 2017_720 + config)
-    _, bad, orc = run_pair(mp, oracle_mod, refhost, config, N, 2017_720 + config, frames=1)
+    _, bad, orc = run_pair(mp, oracle_mod, refhost, config, N, 2017_720 + config, frames=1,
+                           transform=EDGE_INPUTS[case] if case else None)
     assert not bad
     ref = refhost.RefHost(p, mp.FIELD_ID, mp.MPState)
     nvt = np.asarray(mp.mc_tables()[0])
@@ -295,7 +298,8 @@ def test_marching_cubes_equals_the_reference_kernels(mp, oracle_mod, refhost, co
             else:
                 sv, sn = ref.smooth_and_normals(*unsmoothed[surf], 1, p.smooth_iters)
                 assert np.array_equal(sv, ov) and np.array_equal(sn, on), f"smoothing surface {surf}"
-    assert any(len(m[0]) for m in unsmoothed.values())
+    # a lone particle's density stays below the surface level: no mesh
+    assert any(len(m[0]) for m in unsmoothed.values()) == (case not in ("empty", "one"))
 
 
 @pytest.mark.parametrize("config", [1, 5])
