@@ -16,8 +16,11 @@ N = 16
 TF = 0
 
 
-def _pair(mp, oracle_mod, refhost, config, seed, **overrides):
+def _pair(mp, oracle_mod, refhost, config, seed, keep=None, **overrides):
     p, parts, rf, seeds = reference_mode(mp, config, N, seed)
+    if keep is not None:        # a subset of the configuration's particles
+        idx = keep(parts)
+        parts = {k: (None if v is None else np.asarray(v)[idx]) for k, v in parts.items()}
     for k, v in overrides.items():
         setattr(p, k, v)
     orc = oracle_mod.Oracle(p, mp.FIELD_ID, mp.MPState, mc_tables=mp.mc_tables())
@@ -73,6 +76,23 @@ def test_water_mode_stages(mp, oracle_mod, refhost):
         s = orc.state()
         s.frame += 1
         orc.set_state(s)
+
+
+@pytest.mark.parametrize("case", ["empty", "one", "sparse"])
+def test_water_mode_stages_on_edge_inputs(mp, oracle_mod, refhost, case):
+    """watersim's stages on the dam break with no particles, one particle
+    (the block's first) and one particle in forty: bit for bit."""
+    keep = {"empty": lambda q: np.zeros(0, np.int64), "one": lambda q: [0],
+            "sparse": lambda q: np.arange(len(q["flag"]))[::40]}[case]
+    p, orc, ref, _ = _pair(mp, oracle_mod, refhost, 4, 2017_740, keep=keep, b_correct_position=1)
+    for frame in range(2):
+        for st in WATER:
+            bad = _stage(orc, ref, st)
+            assert not bad, (frame, st, bad)
+        s = orc.state()
+        s.frame += 1
+        orc.set_state(s)
+    assert orc.state().par_num_now == {"empty": 0, "one": 1}.get(case, orc.state().par_num_now)
 
 
 def test_heat_only_mode(mp, oracle_mod, refhost):
