@@ -95,9 +95,11 @@ def test_water_mode_stages_on_edge_inputs(mp, oracle_mod, refhost, case):
     assert orc.state().par_num_now == {"empty": 0, "one": 1}.get(case, orc.state().par_num_now)
 
 
-def test_heat_only_mode(mp, oracle_mod, refhost):
-    """initheat_grid's two-disc scene (spray_k.cu:5603-5621) and heatsim steps."""
-    p, orc, ref, _ = _pair(mp, oracle_mod, refhost, 1, 2017_750, b_extend_heat_to_boundary=1)
+@pytest.mark.parametrize("extend", [1, 0])
+def test_heat_only_mode(mp, oracle_mod, refhost, extend):
+    """initheat_grid's two-disc scene (spray_k.cu:5603-5621) and heatsim steps,
+    with the boundary cells' temperature extended from the interior or not."""
+    p, orc, ref, _ = _pair(mp, oracle_mod, refhost, 1, 2017_750, b_extend_heat_to_boundary=extend)
     assert not _stage(orc, ref, ("initheat_grid",))
     for _ in range(3):
         assert not _stage(orc, ref, ("heatsim",))
